@@ -1,0 +1,210 @@
+/*
+ * lepic_gpu.h -- C ABI of the B200 (sm_100a) implementation of the LePIC per-timestep
+ * PIC-MCC loop.  Plain pointers and sizes only; every entry point returns LEPIC_OK (0) or a
+ * negative LEPIC_E* code and never aborts the caller.
+ *
+ * The reference is F77-style Fortran with implicit interfaces (all arguments by reference,
+ * global state in COMMON blocks).  Each entry point below names the reference routine it
+ * replaces.  A Fortran host binds them with ISO_C_BINDING and keeps
+ * its decks, tables and call sites; device state stays resident between calls and host
+ * arrays are exchanged only where a pointer argument is non-NULL.
+ *
+ * Array layouts are the reference's Fortran memory order (first index fastest):
+ *   node arrays  f(0:nx+2, 0:ny+2)         double / int32, index i + j*(nx+3)
+ *   rhs          b(1:nx+1, 1:ny+1)         double, index (i-1) + (j-1)*(nx+1)
+ *   E field      Ei(2, 0:nx+2, 0:ny+2)     double, interleaved (Ex, Ey)
+ *   B field      Bi(4, 0:nx+2, 0:ny+2)     double, interleaved (Bx, By, Bz, |B|)
+ *   particles    vxp(6, n) of one species  double, (x, y, z, vx, vy, vz) per particle
+ *
+ * Threading: one context is used by one host thread at a time.  All device work of a
+ * context is ordered on the context's own CUDA stream (lepic_gpu_stream).  Calls whose
+ * output pointers are all NULL only enqueue work; calls with an output pointer (or stats)
+ * synchronise that stream before returning.
+ */
+#ifndef LEPIC_GPU_H
+#define LEPIC_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LEPIC_OK 0
+#define LEPIC_EINVAL (-1)     /* bad argument or configuration                          */
+#define LEPIC_ENOMEM (-2)     /* device allocation failed                               */
+#define LEPIC_ECUDA (-3)      /* a CUDA runtime call failed                             */
+#define LEPIC_ECAPACITY (-4)  /* a particle array or product list would overflow        */
+#define LEPIC_EDIVERGED (-5)  /* Poisson residual grew 10x: iterative_solver.f90:42-50  */
+#define LEPIC_ETIMEOUT (-6)   /* a bounded device-side wait gave up                     */
+#define LEPIC_ERANGE (-7)     /* Pmax > 1 (collisions.f90:119-123) or a bad cell index  */
+#define LEPIC_ENOTCONV (-8)   /* ncycl V-cycles without reaching eps                    */
+#define LEPIC_ENOKERNEL (-9)  /* the library was not built for this GPU                 */
+
+#define LEPIC_MAXSP 8   /* species (charged + neutral)  */
+#define LEPIC_MAXCOL 64 /* reactions                    */
+
+/* Poisson solve modes for lepic_gpu_iterative_solver */
+#define LEPIC_POISSON_FP64_MG 0   /* the reference's V-cycle (mg.f90) in FP64              */
+#define LEPIC_POISSON_MIXED_IR 1  /* FP32 V-cycles inside FP64 iterative refinement       */
+
+/* Grid selectors for lepic_gpu_get_grid / lepic_gpu_set_grid */
+#define LEPIC_GRID_PHI 0      /* phi(0:nx+2,0:ny+2)                     */
+#define LEPIC_GRID_RHS 1      /* rhs(1:nx+1,1:ny+1)                     */
+#define LEPIC_GRID_EI 2       /* Ei(2,0:nx+2,0:ny+2)                    */
+#define LEPIC_GRID_NP 16      /* + ptype: np(0:nx+2,0:ny+2,ptype)       */
+
+typedef struct lepic_ctx lepic_ctx;
+
+/* Scalars the reference keeps in the COMMON blocks part_info_int/dp_1/dp_2/dp_3 and constants (particle_info.h,
+ * constants.h), plus the device capacities.  Species 0 is the electron, then ions, then
+ * neutrals (negative mass, read_reactions.f90:200-205); indices are 0-based. */
+typedef struct lepic_config {
+    int32_t nx, ny;          /* cells (n(1), n(2)); nodes 1..n+1 plus ghosts 0 and n+2   */
+    double dx, dy, zmax;     /* h(1), h(2) [m]; zmax [m] (1 m when hz < 0)               */
+    double dt;               /* [s]                                                      */
+    double eps0, qe;         /* qe is the float32-rounded 1.60217646e-19 (main.f90:120) */
+    int32_t flag_pbc, flag_spec, flag_nmn;
+    int32_t flag_B;          /* 0: none, 1: constant Bc, 2: map Bi on the field grid      */
+    int32_t flag_B_pos;      /* 1: positive ions unmagnetised (part_expmover.f90:185)    */
+    double Bc[3];
+    int32_t ntype;           /* charged species                                          */
+    int32_t nsp;             /* charged + neutral species                                */
+    double charge[LEPIC_MAXSP], mass[LEPIC_MAXSP], Nm[LEPIC_MAXSP], vt0[LEPIC_MAXSP];
+    double np_mx[LEPIC_MAXSP];    /* neutral densities at the neutral indices            */
+    double nu_uplim[LEPIC_MAXSP]; /* main.f90:494-495                                    */
+    int32_t ns_coll, nsort;       /* main.f90:479-480                                    */
+    int32_t ng;                   /* multigrid levels (main.f90:264-277)                 */
+    int32_t ncycl;                /* maximum V-cycles (main.f90:261)                     */
+    double omega;                 /* SOR factor (iterative_solver.f90:28)                */
+    int64_t capacity[LEPIC_MAXSP];/* particle slots per charged species (nmax)           */
+    uint64_t seed;                /* counter-based RNG key                               */
+    int32_t tile_w, tile_h;       /* sort tile in cells; 0,0 = the reference's row-major
+                                     cell order (sorting.f90:151)                        */
+} lepic_config;
+
+/* Output of read_reactions/ordering (read_reactions.f90:511-697), species 0-based. */
+typedef struct lepic_xs_tables {
+    int32_t npt;               /* sig_npt_mx                                             */
+    int32_t ncol;              /* reactions                                              */
+    const double *sig_Er;      /* [npt]                                                  */
+    const double *sig;         /* [icol*npt + ipt]                                       */
+    const double *Eth;         /* [icol] threshold [eV]                                  */
+    const int32_t *col_info;   /* [icol*10 + k] = col_info(icol, k+1), species 0-based   */
+    const int32_t *p_ncol;     /* [ptype]                                                */
+    const int32_t *sig_list;   /* [ptype*LEPIC_MAXCOL + k], reaction index 0-based       */
+    const double *sigv_mx;     /* [ptype*LEPIC_MAXCOL + icol]                            */
+    int32_t flag_ionrep;
+    double fEk;
+} lepic_xs_tables;
+
+typedef struct lepic_solve_stats {
+    int32_t cycles;            /* V-cycles (k)                                           */
+    int32_t sweeps_fine;       /* SOR sweeps on the finest level                         */
+    double res_l1;             /* the reference's normalised L1 residual                 */
+    double res_l2_rel;         /* ||b - A u||_2 / ||b||_2 over interior nodes, FP64      */
+    double ktot;               /* equivalent fine-grid SOR sweeps (mg.f90:227-229)       */
+} lepic_solve_stats;
+
+typedef struct lepic_push_stats {
+    int64_t np_tot[LEPIC_MAXSP];  /* live particles after the call                     */
+    int64_t n_lost[LEPIC_MAXSP];  /* cumulative wall losses                             */
+    int64_t n_dead[LEPIC_MAXSP];  /* cumulative removals of collision-killed particles  */
+    int64_t n_slots[LEPIC_MAXSP]; /* occupied slots (live + holes until the next sort)  */
+} lepic_push_stats;
+
+typedef struct lepic_mcc_stats {
+    int64_t n_cand[LEPIC_MAXSP];  /* cumulative collision candidates                    */
+    int64_t n_coll[LEPIC_MAXCOL]; /* cumulative real collisions per reaction            */
+    int64_t n_add[LEPIC_MAXSP];   /* cumulative products appended                       */
+    int64_t n_overflow;           /* relative energies above the table's last point     */
+    double nu_max[LEPIC_MAXSP];   /* collisions.f90:98-106                              */
+} lepic_mcc_stats;
+
+/* Synthetic initial load (the one-time load_part.f90:59-224 on the device).  Every sample
+ * places one particle of each charged species at the same position (load_part.f90:141),
+ * positions follow the density profile, velocities are Maxwellian at vt0. */
+typedef struct lepic_load_spec {
+    int64_t n_samples;        /* particles per charged species                          */
+    int32_t profile;          /* 0: uniform, 1: n_floor + (n_peak-n_floor)*gaussian      */
+    double x_load;            /* samples limited to x < x_load [m] (load_part.f90:104)  */
+    double n_peak, n_floor;   /* profile 1 [m^-3]                                        */
+    double sigma;             /* profile 1 Gaussian sigma [m], centred in the box       */
+    uint64_t seed;
+} lepic_load_spec;
+
+/* Version of this ABI. */
+int32_t lepic_gpu_abi_version(void);
+
+/* Creates a context on the current CUDA device.  bcnd: node labels (>0 Dirichlet wall,
+ * -1 interior, -2 Neumann, 0 periodic, <=-4 dielectric) as generate_boundary.f90 leaves
+ * them; phi_init: the wall potentials (generate_boundary.f90:210-216); Bi may be NULL when
+ * flag_B != 2; xs may be NULL (collision-less).  Replaces the device-side half of
+ * main.f90:192-214 (allocation) and main.f90:334-344 (kq). */
+int lepic_gpu_create(const lepic_config *cfg, const int32_t *bcnd, const double *phi_init,
+                     const double *Bi, const lepic_xs_tables *xs, lepic_ctx **out);
+int lepic_gpu_destroy(lepic_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t). */
+void *lepic_gpu_stream(lepic_ctx *ctx);
+/* Waits for the context's stream and reports any device-side error flag as a code. */
+int lepic_gpu_sync(lepic_ctx *ctx);
+/* Text of the last error of this context (valid until the next call). */
+const char *lepic_gpu_last_error(lepic_ctx *ctx);
+
+/* Uploads n particles of one charged species, AoS FP64 as vxp(6,n) (z is not kept).
+ * Replaces the particle half of restart.f90:48-149.  Particles must lie in the box. */
+int lepic_gpu_put_particles(lepic_ctx *ctx, int32_t ptype, const double *vxp, int64_t n);
+/* Downloads the live particles of one species in slot order (holes removed), AoS FP64
+ * with z = 0.  The backup writer main.f90:1102-1139 reads this. */
+int lepic_gpu_get_particles(lepic_ctx *ctx, int32_t ptype, double *vxp, int64_t cap,
+                            int64_t *n_out);
+/* Synthetic initial load on the device (see lepic_load_spec). */
+int lepic_gpu_load_particles(lepic_ctx *ctx, const lepic_load_spec *spec);
+
+/* charge_deposition (part_expmover.f90:520-610) of every charged species into np, after
+ * zeroing it (main.f90:1076); used after a load or a restart. */
+int lepic_gpu_charge_deposition(lepic_ctx *ctx);
+/* np_periodic + calc_rhs (calc_rho.f90:1-77): rhs = -sum charge*np.  rhs_out (nullable)
+ * receives rhs(1:nx+1,1:ny+1). */
+int lepic_gpu_calc_rhs(lepic_ctx *ctx, double *rhs_out);
+/* dens_red (calc_rho.f90:134-199): np_red_out (nullable) receives ntype node grids,
+ * np_mx_out (nullable) the ntype interior maxima. */
+int lepic_gpu_dens_red(lepic_ctx *ctx, double *np_red_out, double *np_mx_out);
+/* iterative_solver (iterative_solver.f90:1-69 -> mg.f90 -> sors.f90) on the device phi.
+ * phi_inout (nullable): uploaded first (warm start) and downloaded after.  eps is the
+ * reference's normalised L1 tolerance for mode 0 and the FP64 relative L2 tolerance
+ * ||b-Au||/||b|| for mode 1.  stats (nullable) forces a sync. */
+int lepic_gpu_iterative_solver(lepic_ctx *ctx, double *phi_inout, double eps, int32_t mode,
+                               lepic_solve_stats *stats);
+/* calc_Efield (Efield.f90:1-128).  Ei_out (nullable) receives Ei(2,0:nx+2,0:ny+2) FP64. */
+int lepic_gpu_calc_efield(lepic_ctx *ctx, double *Ei_out);
+/* part_sorting (sorting.f90:92-251) of one species by cell.  plist_out (nullable,
+ * nx+nx*ny+2 entries) receives Plist(0:pl_max) when the context uses the reference order. */
+int lepic_gpu_part_sorting(lepic_ctx *ctx, int32_t ptype, int32_t *plist_out);
+/* collisions (collisions.f90:1-207, collision_OMP, SCATTER) for every species, neutral
+ * targets, null-collision MCC with a counter-based RNG keyed by (seed, it, species, slot). */
+int lepic_gpu_collisions(lepic_ctx *ctx, int32_t it, lepic_mcc_stats *stats);
+/* part_mover (part_expmover.f90:1-517) fused with charge_deposition (:520-610) for every
+ * charged species: np is zeroed and rebuilt from the moved particles. */
+int lepic_gpu_push_deposit(lepic_ctx *ctx, int32_t it, lepic_push_stats *stats);
+/* One PIC step, the in-scope body of main.f90:818-1090: calc_rhs -> iterative_solver ->
+ * calc_Efield -> part_sorting (MOD(it,nsort)==1) -> collisions (it>1, MOD(it,ns_coll)==1)
+ * -> push_deposit.  eps / mode as lepic_gpu_iterative_solver. */
+int lepic_gpu_step(lepic_ctx *ctx, int32_t it, double eps, int32_t mode);
+
+/* Copies a device grid (LEPIC_GRID_*) to the host, FP64, in the layouts above. */
+int lepic_gpu_get_grid(lepic_ctx *ctx, int32_t which, double *out);
+/* Sets phi (LEPIC_GRID_PHI) or rhs (LEPIC_GRID_RHS) from the host. */
+int lepic_gpu_set_grid(lepic_ctx *ctx, int32_t which, const double *in);
+/* Live particles per species and the cumulative counters. */
+int lepic_gpu_get_push_stats(lepic_ctx *ctx, lepic_push_stats *stats);
+int lepic_gpu_get_mcc_stats(lepic_ctx *ctx, lepic_mcc_stats *stats);
+
+/* Raw device pointers of one species' SoA arrays (for in-process tools and tests):
+ * X, Y are uint32 fixed point in cell units with `shift` fractional bits, VX/VY/VZ float. */
+int lepic_gpu_particle_arrays(lepic_ctx *ctx, int32_t ptype, void **X, void **Y, void **VX,
+                              void **VY, void **VZ, int64_t *n_slots, int32_t *shift);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,175 @@
+"""ctypes mirror of ``include/lepic_gpu.h`` (the C ABI of the sm_100a library).
+
+The structures below must match the header field for field; ``tests/test_capi_cpu.py``
+checks that every symbol the header declares is exported by the shared library.
+The library is the in-tree ``jd_lepic_b200/_lib/liblepic_gpu.so``; if it is missing the
+load fails loudly (there is no CPU fallback of the product path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+MAXSP = 8
+MAXCOL = 64
+
+OK = 0
+EINVAL = -1
+ENOMEM = -2
+ECUDA = -3
+ECAPACITY = -4
+EDIVERGED = -5
+ETIMEOUT = -6
+ERANGE = -7
+ENOTCONV = -8
+ENOKERNEL = -9
+
+ERROR_NAMES = {
+    EINVAL: "LEPIC_EINVAL", ENOMEM: "LEPIC_ENOMEM", ECUDA: "LEPIC_ECUDA",
+    ECAPACITY: "LEPIC_ECAPACITY", EDIVERGED: "LEPIC_EDIVERGED", ETIMEOUT: "LEPIC_ETIMEOUT",
+    ERANGE: "LEPIC_ERANGE", ENOTCONV: "LEPIC_ENOTCONV", ENOKERNEL: "LEPIC_ENOKERNEL",
+}
+
+POISSON_FP64_MG = 0
+POISSON_MIXED_IR = 1
+POISSON_FP64_MG_L2 = 2
+
+GRID_PHI = 0
+GRID_RHS = 1
+GRID_EI = 2
+GRID_NP = 16
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "liblepic_gpu.so")
+
+
+class LepicConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("dx", C.c_double), ("dy", C.c_double), ("zmax", C.c_double),
+        ("dt", C.c_double),
+        ("eps0", C.c_double), ("qe", C.c_double),
+        ("flag_pbc", C.c_int32), ("flag_spec", C.c_int32), ("flag_nmn", C.c_int32),
+        ("flag_B", C.c_int32),
+        ("flag_B_pos", C.c_int32),
+        ("Bc", C.c_double * 3),
+        ("ntype", C.c_int32),
+        ("nsp", C.c_int32),
+        ("charge", C.c_double * MAXSP), ("mass", C.c_double * MAXSP),
+        ("Nm", C.c_double * MAXSP), ("vt0", C.c_double * MAXSP),
+        ("np_mx", C.c_double * MAXSP),
+        ("nu_uplim", C.c_double * MAXSP),
+        ("ns_coll", C.c_int32), ("nsort", C.c_int32),
+        ("ng", C.c_int32),
+        ("ncycl", C.c_int32),
+        ("omega", C.c_double),
+        ("capacity", C.c_int64 * MAXSP),
+        ("seed", C.c_uint64),
+        ("tile_w", C.c_int32), ("tile_h", C.c_int32),
+    ]
+
+
+class LepicXsTables(C.Structure):
+    _fields_ = [
+        ("npt", C.c_int32), ("ncol", C.c_int32),
+        ("sig_Er", C.POINTER(C.c_double)),
+        ("sig", C.POINTER(C.c_double)),
+        ("Eth", C.POINTER(C.c_double)),
+        ("col_info", C.POINTER(C.c_int32)),
+        ("p_ncol", C.POINTER(C.c_int32)),
+        ("sig_list", C.POINTER(C.c_int32)),
+        ("sigv_mx", C.POINTER(C.c_double)),
+        ("flag_ionrep", C.c_int32),
+        ("fEk", C.c_double),
+    ]
+
+
+class LepicSolveStats(C.Structure):
+    _fields_ = [
+        ("cycles", C.c_int32), ("sweeps_fine", C.c_int32),
+        ("res_l1", C.c_double), ("res_l2_rel", C.c_double), ("ktot", C.c_double),
+    ]
+
+
+class LepicPushStats(C.Structure):
+    _fields_ = [
+        ("np_tot", C.c_int64 * MAXSP), ("n_lost", C.c_int64 * MAXSP),
+        ("n_dead", C.c_int64 * MAXSP), ("n_slots", C.c_int64 * MAXSP),
+    ]
+
+
+class LepicMccStats(C.Structure):
+    _fields_ = [
+        ("n_cand", C.c_int64 * MAXSP), ("n_coll", C.c_int64 * MAXCOL),
+        ("n_add", C.c_int64 * MAXSP), ("n_overflow", C.c_int64),
+        ("nu_max", C.c_double * MAXSP),
+    ]
+
+
+class LepicLoadSpec(C.Structure):
+    _fields_ = [
+        ("n_samples", C.c_int64),
+        ("profile", C.c_int32),
+        ("x_load", C.c_double),
+        ("n_peak", C.c_double), ("n_floor", C.c_double),
+        ("sigma", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int32)
+_VP = C.c_void_p
+
+# name -> (restype, argtypes); every function declared in include/lepic_gpu.h
+PROTOTYPES = {
+    "lepic_gpu_abi_version": (C.c_int32, []),
+    "lepic_gpu_create": (C.c_int, [C.POINTER(LepicConfig), _IP, _DP, _DP, C.POINTER(LepicXsTables),
+                                   C.POINTER(_VP)]),
+    "lepic_gpu_destroy": (C.c_int, [_VP]),
+    "lepic_gpu_stream": (_VP, [_VP]),
+    "lepic_gpu_sync": (C.c_int, [_VP]),
+    "lepic_gpu_last_error": (C.c_char_p, [_VP]),
+    "lepic_gpu_put_particles": (C.c_int, [_VP, C.c_int32, _DP, C.c_int64]),
+    "lepic_gpu_get_particles": (C.c_int, [_VP, C.c_int32, _DP, C.c_int64, C.POINTER(C.c_int64)]),
+    "lepic_gpu_load_particles": (C.c_int, [_VP, C.POINTER(LepicLoadSpec)]),
+    "lepic_gpu_charge_deposition": (C.c_int, [_VP]),
+    "lepic_gpu_calc_rhs": (C.c_int, [_VP, _DP]),
+    "lepic_gpu_dens_red": (C.c_int, [_VP, _DP, _DP]),
+    "lepic_gpu_iterative_solver": (C.c_int, [_VP, _DP, C.c_double, C.c_int32, C.POINTER(LepicSolveStats)]),
+    "lepic_gpu_calc_efield": (C.c_int, [_VP, _DP]),
+    "lepic_gpu_part_sorting": (C.c_int, [_VP, C.c_int32, _IP]),
+    "lepic_gpu_collisions": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicMccStats)]),
+    "lepic_gpu_push_deposit": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicPushStats)]),
+    "lepic_gpu_step": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_int32]),
+    "lepic_gpu_get_grid": (C.c_int, [_VP, C.c_int32, _DP]),
+    "lepic_gpu_set_grid": (C.c_int, [_VP, C.c_int32, _DP]),
+    "lepic_gpu_get_push_stats": (C.c_int, [_VP, C.POINTER(LepicPushStats)]),
+    "lepic_gpu_get_mcc_stats": (C.c_int, [_VP, C.POINTER(LepicMccStats)]),
+    "lepic_gpu_particle_arrays": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
+                                            C.POINTER(_VP), C.POINTER(_VP), C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int32)]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the sm_100a library and binds every prototype; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library {path} is missing; run `python -m jd_lepic_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class LepicError(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        super().__init__(f"{where} failed with {ERROR_NAMES.get(code, code)}: {detail}")

@@ -1,0 +1,202 @@
+// field.cu -- charge density to Poisson right-hand side, density reduction, electric field.
+// Compiled with -fmad=false: every FP64 product and sum is rounded as written, so the
+// field values equal the CPU restatement's bit for bit.
+//
+// Roofline: all three are HBM/L2 streams over the (nx+3)(ny+3) node grid:
+//   calc_rhs  reads ntype*8 B (uint64 accumulators) + 1 B mask + 8 B kq, writes 8 B / node
+//   efield    reads 8 B phi (5-point, cached) + 1 B mask, writes 16 B (FP64) + 8 B (FP32)
+#include <algorithm>
+#include "lepic_internal.cuh"
+
+struct RhoParams {
+    int nx, ny, ntype, pbc;
+    const unsigned long long *acc[LEPIC_MAXSP];
+    const double *kq;
+    const int8_t *bc;
+    double k1[LEPIC_MAXSP];      // Nm / (dx dy zmax)
+    double charge[LEPIC_MAXSP];
+};
+
+// np(ix,iy,s) after the periodic fold of calc_rho.f90:1-35.  The reference accumulates
+// kq*(k1*w) per particle; here the exact integer sum of w*2^44 is scaled once.
+__device__ __forceinline__ double np_raw(const RhoParams &P, int s, int ix, int iy) {
+    const long long n = ix + (long long)iy * (P.nx + 3);
+    double w = (double)P.acc[s][n] * 5.684341886080802e-14; // 2^-44
+    return P.kq[n] * (P.k1[s] * w);
+}
+__device__ __forceinline__ double np_val(const RhoParams &P, int s, int ix, int iy) {
+    if (P.pbc) {
+        const int W = P.nx + 3;
+        if (iy == 1 && P.bc[ix + 1 * W] == 0)
+            return 0.5 * (np_raw(P, s, ix, 1) + np_raw(P, s, ix, P.ny + 1));
+        if (iy == P.ny + 1 && P.bc[ix + (P.ny + 1) * W] == 0) {
+            if (P.bc[ix + 1 * W] == 0) return 0.5 * (np_raw(P, s, ix, 1) + np_raw(P, s, ix, P.ny + 1));
+            return np_raw(P, s, ix, 1);
+        }
+    }
+    return np_raw(P, s, ix, iy);
+}
+
+// calc_rho.f90:37-77: rhs(ix,iy) = -sum_ptype charge(ptype)*np(ix,iy,ptype)
+__global__ void k_calc_rhs(RhoParams P, double *rhs) {
+    const long long tot = (long long)(P.nx + 1) * (P.ny + 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(t % (P.nx + 1)) + 1, iy = (int)(t / (P.nx + 1)) + 1;
+        double r = 0.0;
+        for (int s = 0; s < P.ntype; s++) r = r - P.charge[s] * np_val(P, s, ix, iy);
+        rhs[t] = r;
+    }
+}
+
+// calc_rho.f90:134-199: np_red = np (one rank), np_mx = max over bcnd == -1 nodes.
+// The maximum of non-negative doubles is taken on their bit patterns (order-free).
+__global__ void k_dens_red(RhoParams P, double *np_red, unsigned long long *np_mx) {
+    const long long nn = (long long)(P.nx + 3) * (P.ny + 3);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(t % (P.nx + 3)), iy = (int)(t / (P.nx + 3));
+        bool in = ix >= 1 && ix <= P.nx + 1 && iy >= 1 && iy <= P.ny + 1;
+        for (int s = 0; s < P.ntype; s++) {
+            double v = in ? np_val(P, s, ix, iy) : 0.0;
+            np_red[s * nn + t] = v;
+            if (in && P.bc[t] == -1 && v > 0.0) atomicMax(&np_mx[s], (unsigned long long)__double_as_longlong(v));
+        }
+    }
+}
+
+__global__ void k_np_grid(RhoParams P, int s, double *out) {
+    const long long nn = (long long)(P.nx + 3) * (P.ny + 3);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
+         t += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(t % (P.nx + 3)), iy = (int)(t / (P.nx + 3));
+        bool in = ix >= 1 && ix <= P.nx + 1 && iy >= 1 && iy <= P.ny + 1;
+        out[t] = in ? np_val(P, s, ix, iy) : np_raw(P, s, ix, iy);
+    }
+}
+
+static RhoParams rho_params(lepic_ctx *c) {
+    RhoParams P;
+    P.nx = c->cfg.nx; P.ny = c->cfg.ny; P.ntype = c->cfg.ntype; P.pbc = c->cfg.flag_pbc;
+    for (int s = 0; s < LEPIC_MAXSP; s++) { P.acc[s] = nullptr; P.k1[s] = 0; P.charge[s] = 0; }
+    for (int s = 0; s < c->cfg.ntype; s++) {
+        P.acc[s] = c->sp[s].acc;
+        P.k1[s] = c->cfg.Nm[s] / (c->cfg.dx * c->cfg.dy * c->cfg.zmax);
+        P.charge[s] = c->cfg.charge[s];
+    }
+    P.kq = c->kq; P.bc = c->bc8;
+    return P;
+}
+
+int field_calc_rhs(lepic_ctx *c) {
+    RhoParams P = rho_params(c);
+    long long tot = (long long)(c->cfg.nx + 1) * (c->cfg.ny + 1);
+    int grid = (int)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16);
+    k_calc_rhs<<<grid, 256, 0, c->stream>>>(P, c->rhs);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+int field_dens_red(lepic_ctx *c) {
+    RhoParams P = rho_params(c);
+    LCUDA(cudaMemsetAsync(c->np_mx, 0, sizeof(double) * LEPIC_MAXSP, c->stream));
+    int grid = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
+    k_dens_red<<<grid, 256, 0, c->stream>>>(P, c->np_red, (unsigned long long *)c->np_mx);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+int field_np_grid(lepic_ctx *c, int ptype, double *d_out) {
+    RhoParams P = rho_params(c);
+    int grid = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
+    k_np_grid<<<grid, 256, 0, c->stream>>>(P, ptype, d_out);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Efield.f90:1-128.
+// Pass 1 (:19-34): central differences at nodes with bcnd <= 0.
+__global__ void k_efield_interior(int nx, int ny, double h1, double h2, const double *phi,
+                                  const int8_t *bc, double2 *E) {
+    const int W = nx + 3;
+    const long long tot = (long long)(nx + 1) * (ny + 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(t % (nx + 1)) + 1, iy = (int)(t / (nx + 1)) + 1;
+        long long n = ix + (long long)iy * W;
+        if (bc[n] <= 0) {
+            double2 e;
+            e.x = -(phi[n + 1] - phi[n - 1]) / (2.0 * h1);
+            e.y = -(phi[n + W] - phi[n - W]) / (2.0 * h2);
+            E[n] = e;
+        }
+    }
+}
+// Pass 2, Neumann column (:52-63) and periodic rows (:68-82), one thread per row/column.
+__global__ void k_efield_nmn_pbc(int nx, int ny, double h2, const double *phi, const int8_t *bc,
+                                 double2 *E) {
+    const int W = nx + 3;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 1 && t <= ny + 1) { // Neumann: any node of row iy with bcnd == -2
+        int iy = t;
+        for (int ix = 1; ix <= nx + 1; ix++) {
+            if (bc[ix + iy * W] != -2) continue;
+            E[1 + iy * W].x = 0.0;
+            if (iy > 1 && iy < ny + 1)
+                E[1 + iy * W].y = -(phi[1 + (iy + 1) * W] - phi[1 + (iy - 1) * W]) / (2.0 * h2);
+        }
+    }
+    if (t >= 1 && t <= nx + 1) { // periodic: node (ix, 1)
+        int ix = t;
+        int b = bc[ix + 1 * W];
+        if (b == 0 || b == -2) {
+            E[ix + 1 * W].y = -(phi[ix + 2 * W] - phi[ix + ny * W]) / (2.0 * h2);
+            E[ix + 0 * W].y = E[ix + ny * W].y;
+            E[ix + (ny + 1) * W].y = E[ix + 1 * W].y;
+            E[ix + (ny + 2) * W].y = E[ix + 2 * W].y;
+            E[ix + 0 * W].x = E[ix + ny * W].x;
+            E[ix + (ny + 2) * W].x = E[ix + 2 * W].x;
+        }
+    }
+}
+// Pass 2, walls (:87-118): zero, then linear extrapolation from the interior side.  Reads the
+// pass-1 field and writes a second buffer, so every wall node sees the same input.
+__global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *Ein, double2 *Eout,
+                               float2 *Ef) {
+    const int W = nx + 3;
+    const long long nn = (long long)(nx + 3) * (ny + 3);
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn;
+         n += (long long)gridDim.x * blockDim.x) {
+        int ix = (int)(n % W), iy = (int)(n / W);
+        double2 e = Ein[n];
+        if (ix >= 1 && ix <= nx + 1 && iy >= 1 && iy <= ny + 1 && bc[n] >= 1) {
+            e.x = 0.0;
+            e.y = 0.0;
+            // the +-2 neighbours exist only inside the ghost frame (0..n+2)
+            if (bc[n + 1] <= 0) e.x = 2.0 * Ein[n + 1].x - (ix + 2 <= nx + 2 ? Ein[n + 2].x : 0.0);
+            if (bc[n - 1] <= 0) e.x = 2.0 * Ein[n - 1].x - (ix >= 2 ? Ein[n - 2].x : 0.0);
+            if (bc[n + W] <= 0) e.y = 2.0 * Ein[n + W].y - (iy + 2 <= ny + 2 ? Ein[n + 2 * W].y : 0.0);
+            if (bc[n - W] <= 0) e.y = 2.0 * Ein[n - W].y - (iy >= 2 ? Ein[n - 2 * W].y : 0.0);
+        }
+        Eout[n] = e;
+        Ef[n] = make_float2((float)e.x, (float)e.y);
+    }
+}
+
+int field_calc_efield(lepic_ctx *c) {
+    const int nx = c->cfg.nx, ny = c->cfg.ny;
+    long long tot = (long long)(nx + 1) * (ny + 1);
+    int grid = (int)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16);
+    // E (FP64) lives in Ed[0..nn); the second half is the wall-pass output.
+    double2 *E0 = c->Ed, *E1 = c->Ed + c->nn;
+    k_efield_interior<<<grid, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, E0);
+    if (c->cfg.flag_pbc || c->cfg.flag_nmn)
+        k_efield_nmn_pbc<<<div_up(std::max(nx, ny) + 2, 256), 256, 0, c->stream>>>(nx, ny, c->cfg.dy,
+                                                                                   c->phi, c->bc8, E0);
+    int grid2 = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
+    k_efield_walls<<<grid2, 256, 0, c->stream>>>(nx, ny, c->bc8, E0, E1, c->Ef);
+    LCUDA(cudaGetLastError());
+    LCUDA(cudaMemcpyAsync(E0, E1, sizeof(double2) * c->nn, cudaMemcpyDeviceToDevice, c->stream));
+    return LEPIC_OK;
+}

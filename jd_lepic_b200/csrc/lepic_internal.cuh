@@ -1,0 +1,270 @@
+// lepic_internal.cuh -- shared definitions of the sm_100a implementation.
+//
+// HBM layout (one context, one GPU):
+//   particles  per charged species, structure of arrays, two copies (sort ping-pong):
+//              X, Y  uint32 fixed point in cell units: cell = X >> S, offset = X & (2^S-1)
+//              VX, VY, VZ float.  A free slot ("hole") has VX = NaN.  20 B per particle.
+//   grids      node arrays (nx+3)*(ny+3), x fastest (the reference's Fortran order):
+//              phi double, E double2 (FP64 result) + float2 (gather copy), B float4,
+//              deposit accumulators uint64 per species (fixed point 2^-44), bcnd int32 and
+//              an int8 copy, per-cell "all four corners are walls" bytes for the loss test.
+//   multigrid  per level u, b (double) and the FP32 e, r of the mixed-precision cycle.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include "../../include/lepic_gpu.h"
+
+#define LEPIC_DEP_SHIFT 44          // deposit fixed point: weight * 2^44
+#define LEPIC_MAXLEV 16
+
+// device error bits (DevCounters::err)
+#define LERR_CAPACITY 1
+#define LERR_TIMEOUT 2
+#define LERR_RANGE 4
+#define LERR_DIVERGED 8
+#define LERR_NOTCONV 16
+
+struct WorkItem {           // one CTA's share of the push: particles [start, end) of a tile
+    int tile;               // sort tile (-1: no shared-memory window, global atomics)
+    int start, end, pad;
+};
+
+struct Product {            // a particle created by a collision, before its ordered append
+    unsigned long long key; // parent slot * 8 + byproduct index (unique, orders the append)
+    uint32_t X, Y;
+    float vx, vy, vz;
+    int pad;
+};
+
+struct DevCounters {
+    long long n_slots[LEPIC_MAXSP];    // occupied slots (sorted region + appended tail)
+    long long n_sorted[LEPIC_MAXSP];   // end of the region the work list covers
+    long long n_alive[LEPIC_MAXSP];
+    unsigned long long n_lost[LEPIC_MAXSP], n_dead[LEPIC_MAXSP];
+    unsigned long long n_cand[LEPIC_MAXSP], n_add[LEPIC_MAXSP];
+    unsigned long long n_coll[LEPIC_MAXCOL];
+    unsigned long long n_overflow;
+    unsigned int work_next[LEPIC_MAXSP];  // push work-item dispenser
+    int n_items[LEPIC_MAXSP];
+    unsigned int prod_count[LEPIC_MAXSP]; // products waiting for the ordered append
+    int n_big;                            // sort: segments too long for one warp
+    int err;
+    int err_where;
+    // multigrid results
+    int mg_cycles, mg_sweeps_fine;
+    double mg_res_l1, mg_ktot, mg_res_l2, mg_b_l2;
+    unsigned int bar_count, bar_gen;      // grid barrier of the cooperative kernels
+    int abort_flag;                       // set to end every wait of a cooperative kernel
+};
+
+struct MGLevel {
+    int nx, ny;
+    double hx, hy;
+    double *u;       // (nx+3)(ny+3)
+    double *b;       // (nx+1)(ny+1)
+    int8_t *bc;      // (nx+3)(ny+3), bcnd clamped to [-4, 1]
+    float *e32;      // mixed precision correction (nx+3)(ny+3)
+    float *r32;      // mixed precision right-hand side (nx+1)(ny+1)
+};
+
+struct SpeciesBuf {
+    uint32_t *X[2], *Y[2];
+    float *VX[2], *VY[2], *VZ[2];
+    int cur;
+    long long cap;
+    unsigned long long *acc;   // deposit accumulator, one node grid
+    WorkItem *items;
+    int max_items;
+    Product *prod;             // product list
+    int prod_cap;
+};
+
+struct lepic_ctx {
+    lepic_config cfg;
+    int dev = 0, num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int S = 0;                 // fractional bits of the fixed-point positions
+    long long nn = 0;          // nodes (nx+3)(ny+3)
+    int tw = 0, th = 0, ntx = 0, nty = 0, ntiles = 0;
+    long long nkeys = 0;       // ntiles * tw * th
+    // static grids
+    int32_t *bcnd = nullptr;
+    int8_t *bc8 = nullptr;
+    uint8_t *cellwall = nullptr;   // (nx+2)(ny+2) cells, 1 = all corners are walls
+    double *kq = nullptr;
+    float4 *Bf = nullptr;
+    // dynamic grids
+    double *phi = nullptr, *rhs = nullptr;
+    double2 *Ed = nullptr;
+    float2 *Ef = nullptr;
+    double *npd = nullptr;        // FP64 np grids (ntype), filled on demand
+    double *np_red = nullptr;
+    double *np_mx = nullptr;
+    SpeciesBuf sp[LEPIC_MAXSP];
+    // sort scratch
+    int *keys = nullptr, *perm = nullptr, *counts = nullptr, *offsets = nullptr;
+    int *cursor = nullptr, *blocksums = nullptr, *bigseg = nullptr;
+    long long scratch_cap = 0;
+    // multigrid
+    MGLevel lev[LEPIC_MAXLEV];
+    int nlev = 0;
+    double *partials = nullptr;
+    int mg_grid = 0, mg_grid_mixed = 0;
+    // collisions
+    bool has_xs = false;
+    int npt = 0, ncol = 0;
+    double *sig_Er = nullptr, *sig = nullptr, *Eth = nullptr;
+    int *col_info = nullptr;
+    int hsig_list[LEPIC_MAXSP * LEPIC_MAXCOL] = {0};
+    unsigned long long *prod_sort = nullptr;
+    int p_ncol[LEPIC_MAXSP] = {0};
+    double nu_max[LEPIC_MAXSP] = {0};
+    int flag_ionrep = 0;
+    double fEk = 0;
+    // counters
+    DevCounters *dcnt = nullptr;
+    DevCounters *hcnt = nullptr;  // pinned mirror
+    std::string last_err;
+};
+
+// ---------------------------------------------------------------------------------------
+// Counter-based RNG: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), written from the
+// published round function: two 32x32->64 multiplies per round, Weyl key schedule.
+struct U4 { uint32_t x, y, z, w; };
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        U4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+__device__ __forceinline__ double u01(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
+
+// 32-bit integer mix (MurmurHash3 finaliser), used for the stochastic rounding of moves.
+__device__ __forceinline__ uint32_t mix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ void set_err(DevCounters *c, int bit, int where) {
+    atomicOr(&c->err, bit);
+    atomicCAS(&c->err_where, 0, where);
+}
+
+// Bounded software grid barrier for cooperative launches.  Every wait gives up after a
+// clock budget (about 2 s) and then raises LERR_TIMEOUT; any raised error ends all waits.
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_volatile_i32(const int *p) {
+    int v;
+    asm volatile("ld.volatile.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ bool grid_barrier(DevCounters *c, unsigned int nblocks) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned int g = ld_acquire_u32(&c->bar_gen);
+        __threadfence();
+        unsigned int arrived = atomicAdd(&c->bar_count, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            long long t0 = clock64();
+            while (ld_acquire_u32(&c->bar_gen) == g) {
+                if (ld_volatile_i32(&c->abort_flag) != 0) { ok = 0; break; }
+                if (clock64() - t0 > 4000000000LL) {
+                    set_err(c, LERR_TIMEOUT, 900);
+                    atomicExch(&c->abort_flag, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (ld_volatile_i32(&c->abort_flag) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// bitonic sort (all comparators ascending, "flip" form): valid for any n with the missing
+// tail of the power of two treated as +infinity.  sync() separates the stages.
+template <class T, class Sync>
+__device__ void bitonic_sort(T *a, int n, int rank, int size, Sync sync) {
+    int P = 1;
+    while (P < n) P <<= 1;
+    for (int blk = 2; blk <= P; blk <<= 1) {
+        for (int t = rank; t < P / 2; t += size) {
+            int half = blk >> 1;
+            int pos = (t / half) * blk + (t % half);
+            int partner = (pos / blk) * blk + blk - 1 - (pos % blk);
+            if (partner < n) {
+                T x = a[pos], y = a[partner];
+                if (x > y) { a[pos] = y; a[partner] = x; }
+            }
+        }
+        sync();
+        for (int stride = blk >> 2; stride >= 1; stride >>= 1) {
+            for (int t = rank; t < P / 2; t += size) {
+                int pos = (t / stride) * 2 * stride + (t % stride);
+                int partner = pos + stride;
+                if (partner < n) {
+                    T x = a[pos], y = a[partner];
+                    if (x > y) { a[pos] = y; a[partner] = x; }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+struct WarpSync { __device__ void operator()() const { __syncwarp(); } };
+struct BlockSync { __device__ void operator()() const { __syncthreads(); } };
+
+// ---------------------------------------------------------------------------------------
+// Host-side launchers, one translation unit each.
+int field_calc_rhs(lepic_ctx *c);
+int field_dens_red(lepic_ctx *c);
+int field_calc_efield(lepic_ctx *c);
+int field_np_grid(lepic_ctx *c, int ptype, double *d_out);
+int mg_solve(lepic_ctx *c, double eps, int mode);
+int mg_init(lepic_ctx *c);
+int mg_residual_stats(lepic_ctx *c);
+int mg_mixed_solve(lepic_ctx *c, double eps);
+int push_deposit(lepic_ctx *c, int it, bool move);
+int sort_species(lepic_ctx *c, int ptype);
+int mcc_collide(lepic_ctx *c, int it);
+int particles_load(lepic_ctx *c, const lepic_load_spec *spec);
+int particles_put(lepic_ctx *c, int ptype, const double *vxp, long long n);
+int particles_get(lepic_ctx *c, int ptype, double *vxp, long long cap, long long *n_out);
+
+#define LCUDA(call)                                                                     \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            c->last_err = std::string(#call) + ": " + cudaGetErrorString(_e);           \
+            return LEPIC_ECUDA;                                                         \
+        }                                                                               \
+    } while (0)
+
+static inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

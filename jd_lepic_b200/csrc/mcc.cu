@@ -1,0 +1,355 @@
+// mcc.cu -- null-collision Monte Carlo collisions (collisions.f90:1-207, collision_OMP
+// :209-1040) for neutral targets, every ns_coll steps.
+//
+// The reference draws Nc = N*Pmax particles with replacement from one Park-Miller stream.
+// Here every slot draws its own uniform from Philox4x32-10 keyed by (seed, step, species,
+// slot): the slot is a candidate when u < Pmax = nu_max*ns_coll*dt, so the expected number of
+// candidates and the per-particle collision probability sum(nu)*ns_coll*dt are the same, and
+// every result is reproducible run to run.  A candidate then follows collision_OMP exactly:
+// Maxwellian target velocity (load_gauss), centre-of-mass kinematics, cross section by
+// interval search on the union energy grid with linear interpolation, nu/nu_max per reaction,
+// one uniform against the cumulative sum, and the reaction outcome (energy- and momentum-
+// conserving equal-angle scattering, the fixed-split ionization option, charge exchange).
+// The cumulative sum runs over the reactions in ascending nu, as the reference's indexx
+// orders them (that order matters once sum(nu/nu_max) exceeds 1).
+//
+// Products go to a per-species list (unordered atomics) with a unique key parent*8+index;
+// a second kernel sorts each list by key and appends it after the occupied slots, so the
+// particle order after a collision step is deterministic.
+//
+// Roofline: the selection pass generates one Philox block per 4 slots and reads nothing;
+// only candidates (N*Pmax, about 0.3 % of particles) read and write their 20 B record.
+#include <algorithm>
+#include "lepic_internal.cuh"
+
+#define MCC_THREADS 256
+
+struct MccP {
+    int sp, ntype;
+    uint32_t *X, *Y;
+    float *VX, *VY, *VZ;
+    Product *prod[LEPIC_MAXSP];
+    int prod_cap[LEPIC_MAXSP];
+    DevCounters *cnt;
+    double Pmax, nu_max;
+    int ncol_sp;
+    int cols[LEPIC_MAXCOL];
+    const double *sig_Er;
+    int npt;
+    const double *sig;
+    const double *Eth;
+    const int *col_info;
+    double mass[LEPIC_MAXSP], charge[LEPIC_MAXSP], vt0[LEPIC_MAXSP], ndens[LEPIC_MAXSP];
+    double qe, pi;
+    int flag_ionrep;
+    double fEk;
+    uint32_t k0, k1, it;
+};
+
+struct Rng {
+    U4 ctr;
+    uint32_t k0, k1;
+    U4 buf;
+    int used;
+    __device__ double next() {
+        if (used == 4) {
+            buf = philox4x32_10(ctr, k0, k1);
+            ctr.w++;
+            used = 0;
+        }
+        uint32_t v = used == 0 ? buf.x : used == 1 ? buf.y : used == 2 ? buf.z : buf.w;
+        used++;
+        return u01(v);
+    }
+};
+
+// load_gauss.f90:16-39
+__device__ __forceinline__ void load_gauss(double vt, double r1, double r2, double pi, double *a, double *b) {
+    double vp = vt * sqrt(-log(1.0 - r1));
+    double th = 2.0 * pi * r2;
+    double s, c;
+    sincos(th, &s, &c);
+    *a = vp * c;
+    *b = vp * s;
+}
+
+// collisions.f90:485-519: cross section of reaction c at relative energy E (eV); returns
+// -1 when E is outside (E_1, E_npt]
+__device__ __forceinline__ double sigma_at(const MccP &P, int c, double E) {
+    const double *Er = P.sig_Er;
+    const int npt = P.npt;
+    if (!(E > Er[0]) || E > Er[npt - 1]) return -1.0;
+    int lo = 0, hi = npt - 1; // Er[lo] < E <= Er[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (E <= Er[mid]) hi = mid; else lo = mid;
+    }
+    const double *sg = P.sig + (long long)c * npt;
+    double EL = Er[lo], ER = Er[hi], sL = sg[lo], sR = sg[hi];
+    return sL + (E - EL) * (sR - sL) / (ER - EL);
+}
+
+__device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_local) {
+    float fvx = P.VX[slot];
+    if (isnan(fvx)) return;
+    (*n_cand_local)++;
+    const int sp = P.sp;
+    Rng R;
+    R.ctr = U4{(uint32_t)slot, P.it, (uint32_t)sp | 0x4D430000u, 0u};
+    R.k0 = P.k0; R.k1 = P.k1; R.used = 4;
+    const double vx1 = fvx, vy1 = P.VY[slot], vz1 = P.VZ[slot];
+    const double mp = fabs(P.mass[sp]);
+    // per target species: drawn velocity and CM quantities (collision_OMP :336-482)
+    double tvx[LEPIC_MAXSP], tvy[LEPIC_MAXSP], tvz[LEPIC_MAXSP], mu[LEPIC_MAXSP], vr[LEPIC_MAXSP];
+    double vcx[LEPIC_MAXSP], vcy[LEPIC_MAXSP], vcz[LEPIC_MAXSP];
+    unsigned drawn = 0;
+    double nu[LEPIC_MAXCOL];
+    double sum_nu = 0.0;
+    for (int q = 0; q < P.ncol_sp; q++) {
+        const int c = P.cols[q];
+        const int *ci = P.col_info + c * 10;
+        const int n_re = ci[0];
+        const int tt = ci[2 + n_re - 1];
+        nu[q] = 0.0;
+        if (P.charge[tt] != 0.0) continue; // charged targets (DSMC) are not handled here
+        if (!(drawn & (1u << tt))) {
+            double a, b, z, dummy;
+            load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &a, &b);
+            load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &z, &dummy);
+            tvx[tt] = a; tvy[tt] = b; tvz[tt] = z;
+            const double mt = fabs(P.mass[tt]);
+            mu[tt] = mp * mt / (mp + mt);
+            vr[tt] = sqrt((vx1 - a) * (vx1 - a) + (vy1 - b) * (vy1 - b) + (vz1 - z) * (vz1 - z));
+            const double sm = mp + mt;
+            vcx[tt] = (mp * vx1 + mt * a) / sm;
+            vcy[tt] = (mp * vy1 + mt * b) / sm;
+            vcz[tt] = (mp * vz1 + mt * z) / sm;
+            drawn |= 1u << tt;
+        }
+        const double Ekr = (0.5 * mu[tt] * (vr[tt] * vr[tt])) / P.qe;
+        if (Ekr > P.sig_Er[P.npt - 1]) atomicAdd(&P.cnt->n_overflow, 1ull);
+        const double s = sigma_at(P, c, Ekr);
+        if (s < 0.0) continue;
+        nu[q] = P.ndens[tt] * s * vr[tt] / P.nu_max; // :522-532
+        sum_nu = sum_nu + nu[q];
+    }
+    // :619 indexx: reactions ordered by ascending nu (straight insertion, stable); the order
+    // decides the outcome when sum(nu) > 1, i.e. when nu_max was capped (main.f90:494-495)
+    int order[LEPIC_MAXCOL];
+    for (int q = 0; q < P.ncol_sp; q++) {
+        int k = q;
+        while (k > 0 && nu[order[k - 1]] > nu[q]) { order[k] = order[k - 1]; k--; }
+        order[k] = q;
+    }
+    const double r = R.next(); // :624-647
+    if (!(r <= sum_nu)) return;
+    int qsel = -1;
+    double cum = 0.0;
+    for (int k = 0; k < P.ncol_sp; k++) {
+        cum = cum + nu[order[k]];
+        if (r <= cum) { qsel = order[k]; break; }
+    }
+    if (qsel < 0) return;
+    const int c = P.cols[qsel];
+    const int *ci = P.col_info + c * 10;
+    const int n_re = ci[0], n_by = ci[1], rt = ci[2 + n_re + n_by];
+    const int tt = ci[2 + n_re - 1];
+    atomicAdd(&P.cnt->n_coll[c], 1ull);
+    const uint32_t X = P.X[slot], Y = P.Y[slot];
+    if (rt == 4) { // charge exchange :942-1000: the incident ion takes the neutral's velocity
+        for (int ib = 0; ib < n_by; ib++) {
+            int bt = ci[2 + n_re + ib];
+            if (P.mass[bt] <= 0.0) continue;
+            if (bt == sp) {
+                P.VX[slot] = (float)tvx[tt]; P.VY[slot] = (float)tvy[tt]; P.VZ[slot] = (float)tvz[tt];
+            }
+        }
+        return;
+    }
+    const double Eth = P.Eth[c];
+    double Ee = 0.5 * mu[tt] * (vr[tt] * vr[tt]) - Eth * P.qe; // :683
+    int opt_scat = 1;
+    double Ek_b[16];
+    double sum_mass = 0.0, th = 0.0, th_add = 0.0, sin_ph = 0.0, cos_ph = 0.0;
+    for (int q = 0; q < 16; q++) Ek_b[q] = 0.0;
+    bool ion_rep = false;
+    if (rt == 2 && P.flag_ionrep >= 1 && n_by == 3) { // :689-727
+        int cnt_ele = 0, flag_ion = 0;
+        for (int ib = 0; ib < n_by; ib++) {
+            int bt = ci[2 + n_re + ib];
+            if (bt == 0) {
+                cnt_ele++;
+                if (cnt_ele == 1) Ek_b[ib] = P.fEk;
+                if (cnt_ele == 2) Ek_b[ib] = 1.0 - P.fEk;
+            }
+            if (bt != 0 && P.charge[bt] != 0.0) flag_ion = 1;
+        }
+        ion_rep = true;
+        if (cnt_ele == 2 && flag_ion == 1) {
+            opt_scat = 2;
+            Ee = 0.5 * P.mass[0] * (vx1 * vx1 + vy1 * vy1 + vz1 * vz1) - Eth * P.qe;
+            if (Ee < 0.0) Ee = 0.0;
+        }
+    }
+    if (!ion_rep) { // :728-750 (the SCATTER rotation's output is not used by the reference)
+        for (int ib = 0; ib < n_by; ib++) sum_mass = sum_mass + 1.0 / fabs(P.mass[ci[2 + n_re + ib]]);
+        double r0 = R.next(), r1 = R.next();
+        th_add = 2.0 * P.pi / (double)n_by;
+        th = acos(1.0 - 2.0 * r0);
+        sincos(2.0 * P.pi * r1, &sin_ph, &cos_ph);
+    }
+    if (Ee < 0.0) return;
+    bool incident_kept = false;
+    for (int ib = 0; ib < n_by; ib++) { // :767-902
+        const int bt = ci[2 + n_re + ib];
+        if (P.mass[bt] <= 0.0) continue;
+        bool to_incident = false;
+        if (ib == 0 && bt == sp) to_incident = true;
+        if (rt == 1 || rt == 3) {
+            if (bt == sp) to_incident = true;
+            else continue; // a charged target's update (DSMC) is not handled here
+        }
+        double vbx = 0.0, vby = 0.0, vbz = 0.0;
+        if (opt_scat == 1) {
+            double s, cth;
+            sincos(th, &s, &cth);
+            th = th + th_add;
+            const double ex = cth, ey = s * sin_ph, ez = s * cos_ph;
+            const double mb = fabs(P.mass[bt]);
+            const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
+            vbx = vcx[tt] + vp * ex;
+            vby = vcy[tt] + vp * ey;
+            vbz = vcz[tt] + vp * ez;
+        } else if (bt == 0) {
+            double r0 = R.next(), r1 = R.next();
+            double cth = 1.0 - 2.0 * r0, sth = 2.0 * sqrt(r0 * (1.0 - r0));
+            double s, cph;
+            sincos(2.0 * P.pi * r1, &s, &cph);
+            const double vp = sqrt(2.0 * (Ee * Ek_b[ib] / fabs(P.mass[bt])));
+            vbx = vp * cth; vby = vp * sth * s; vbz = vp * sth * cph;
+        } else {
+            double z, dummy;
+            load_gauss(P.vt0[bt], R.next(), R.next(), P.pi, &vbx, &vby);
+            load_gauss(P.vt0[bt], R.next(), R.next(), P.pi, &z, &dummy);
+            vbz = z;
+        }
+        if (to_incident) {
+            incident_kept = true;
+            P.VX[slot] = (float)vbx; P.VY[slot] = (float)vby; P.VZ[slot] = (float)vbz;
+        } else {
+            unsigned int k = atomicAdd(&P.cnt->prod_count[bt], 1u);
+            if ((int)k < P.prod_cap[bt]) {
+                Product pr;
+                pr.key = (unsigned long long)slot * 8ull + (unsigned long long)ib;
+                pr.X = X; pr.Y = Y;
+                pr.vx = (float)vbx; pr.vy = (float)vby; pr.vz = (float)vbz;
+                pr.pad = 0;
+                P.prod[bt][k] = pr;
+            } else {
+                set_err(P.cnt, LERR_CAPACITY, 200);
+            }
+        }
+    }
+    // reactants :908-935: a positive-mass incident that is not byproduct 1 is removed
+    for (int ire = 0; ire < n_re; ire++) {
+        const int ct = ci[2 + ire];
+        if (P.mass[ct] <= 0.0) continue;
+        if (ct == sp && !incident_kept && ire == 0) {
+            P.VX[slot] = __int_as_float(0x7fc00000);
+            atomicAdd(&P.cnt->n_dead[sp], 1ull);
+            atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P) {
+    const long long n = P.cnt->n_slots[P.sp];
+    unsigned int ncand = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * 4; base < n; base += stride) {
+        U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
+        uint32_t v[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            long long slot = base + q;
+            if (slot < n && u01(v[q]) < P.Pmax) collide_one(P, slot, &ncand);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(0xffffffffu, ncand, o);
+    if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&P.cnt->n_cand[P.sp], (unsigned long long)ncand);
+}
+
+// Ordered append of one species' products after its occupied slots (single CTA).
+__global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long long *sortbuf,
+                             uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, long long cap,
+                             DevCounters *cnt) {
+    __shared__ unsigned long long sm[4096];
+    int n = (int)min(cnt->prod_count[sp], (unsigned int)prod_cap);
+    if (n == 0) return;
+    unsigned long long *a = n <= 4096 ? sm : sortbuf;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) a[q] = (prod[q].key << 24) | (unsigned long long)q;
+    __syncthreads();
+    bitonic_sort(a, n, threadIdx.x, blockDim.x, BlockSync());
+    const long long base = cnt->n_slots[sp];
+    int m = n;
+    if (base + m > cap) {
+        m = (int)(cap - base);
+        if (threadIdx.x == 0) set_err(cnt, LERR_CAPACITY, 201);
+    }
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const Product &p = prod[(int)(a[q] & 0xFFFFFFull)];
+        long long s = base + q;
+        X[s] = p.X; Y[s] = p.Y; VX[s] = p.vx; VY[s] = p.vy; VZ[s] = p.vz;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cnt->n_slots[sp] = base + m;
+        cnt->n_alive[sp] += m;
+        cnt->n_add[sp] += (unsigned long long)m;
+        cnt->prod_count[sp] = 0;
+    }
+}
+
+int mcc_collide(lepic_ctx *c, int it) {
+    if (!c->has_xs) return LEPIC_OK;
+    const lepic_config &g = c->cfg;
+    for (int s = 0; s < g.ntype; s++) {
+        if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0) continue;
+        double Pmax = c->nu_max[s] * (double)g.ns_coll * g.dt;
+        if (Pmax > 1.0) { c->last_err = "collision probability Pmax > 1"; return LEPIC_ERANGE; }
+    }
+    for (int s = 0; s < g.ntype; s++) {
+        if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0 || c->nu_max[s] <= 0.0) continue;
+        SpeciesBuf &B = c->sp[s];
+        MccP P;
+        memset(&P, 0, sizeof(P));
+        P.sp = s; P.ntype = g.ntype;
+        P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+        for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
+        P.cnt = c->dcnt;
+        P.nu_max = c->nu_max[s];
+        P.Pmax = c->nu_max[s] * (double)g.ns_coll * g.dt;
+        P.ncol_sp = c->p_ncol[s];
+        for (int q = 0; q < c->p_ncol[s]; q++) P.cols[q] = c->hsig_list[s * LEPIC_MAXCOL + q];
+        P.sig_Er = c->sig_Er; P.npt = c->npt; P.sig = c->sig; P.Eth = c->Eth; P.col_info = c->col_info;
+        for (int t = 0; t < g.nsp; t++) {
+            P.mass[t] = g.mass[t]; P.charge[t] = g.charge[t]; P.vt0[t] = g.vt0[t]; P.ndens[t] = g.np_mx[t];
+        }
+        P.qe = g.qe;
+        P.pi = 4.0 * atan(1.0);
+        P.flag_ionrep = c->flag_ionrep;
+        P.fEk = c->fEk;
+        P.k0 = (uint32_t)g.seed;
+        P.k1 = (uint32_t)(g.seed >> 32) ^ 0xA5A5F00Du;
+        P.it = (uint32_t)it;
+        k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
+        LCUDA(cudaGetLastError());
+    }
+    for (int t = 0; t < g.ntype; t++) {
+        SpeciesBuf &B = c->sp[t];
+        k_mcc_commit<<<1, 1024, 0, c->stream>>>(t, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],
+                                                B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.cap, c->dcnt);
+        LCUDA(cudaGetLastError());
+    }
+    return LEPIC_OK;
+}

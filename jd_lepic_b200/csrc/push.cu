@@ -1,0 +1,270 @@
+// push.cu -- part_mover (part_expmover.f90:1-517) fused with charge_deposition (:520-610).
+//
+// One pass over the particle stream per species and step: read 20 B, write 20 B.
+//   gather   CIC of E (float2 per node, L1/L2-cached) and B at the old position
+//   push     Boris (magnetised) or leap-frog, FP32
+//   move     x += dt*v on uint32 fixed-point positions; the sub-unit remainder is rounded
+//            stochastically (hash of slot, step, axis) so slow particles move unbiased
+//   walls    FLOOR cell -> check_outofbounds -> "all four corners are walls" byte
+//   deposit  integer CIC weights (exact products of the fixed-point offsets, scaled to
+//            2^44) accumulated in a shared-memory uint64 window around the CTA's sort tile
+//            (plus a halo for particles that drifted since the sort); anything outside the
+//            window goes straight to the global uint64 grid.  Integer sums are associative,
+//            so the density is bit-reproducible whatever the atomic order.
+// Work is dispensed dynamically: the sort's per-tile items first, then fixed-size chunks of
+// the unsorted tail (particles created by collisions since the sort).
+//
+// Roofline: 40 B per particle-step of algorithmic HBM traffic (X,Y,VX,VY,VZ read+write).
+#include <algorithm>
+#include "lepic_internal.cuh"
+
+#define PUSH_THREADS 256
+#define PUSH_CHUNK 2048
+
+struct PushP {
+    int nx, ny, S, W;
+    uint32_t *X, *Y;
+    float *VX, *VY, *VZ;
+    const float2 *E;
+    const float4 *B;
+    int bmode;                 // 0 none, 1 constant, 2 map
+    float Bcx, Bcy, Bcz;
+    const uint8_t *cellwall;
+    unsigned long long *acc;
+    const WorkItem *items;
+    DevCounters *cnt;
+    int sp;
+    float k1;                  // dt*q/(2m)
+    float cdx, cdy;            // dt * 2^S / dx
+    int pbc, spec, nmn, negion_nmn;
+    uint32_t step_key;
+    int tw, th, ntx, M, WX, WY, win;
+    int move;
+    long long xlim, ylim;      // nx<<S, ny<<S
+};
+
+__device__ __forceinline__ void deposit(const PushP &P, unsigned long long *win, int ox, int oy,
+                                        bool use_win, uint32_t X, uint32_t Y) {
+    const uint32_t mask = (1u << P.S) - 1u;
+    const uint64_t A = 1ull << P.S;
+    const uint64_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
+    uint64_t w00 = ax * ay, w10 = fx * ay, w11 = fx * fy, w01 = ax * fy;
+    const int sh = 2 * P.S - LEPIC_DEP_SHIFT;
+    if (sh > 0) {
+        const uint64_t half = 1ull << (sh - 1);
+        w00 = (w00 + half) >> sh; w10 = (w10 + half) >> sh; w11 = (w11 + half) >> sh; w01 = (w01 + half) >> sh;
+    } else if (sh < 0) {
+        w00 <<= -sh; w10 <<= -sh; w11 <<= -sh; w01 <<= -sh;
+    }
+    const int ix = (int)(X >> P.S) + 1, iy = (int)(Y >> P.S) + 1; // INT(x/h)+1, x >= 0
+    const int lx = ix - ox, ly = iy - oy;
+    if (use_win && lx >= 0 && lx + 1 < P.WX && ly >= 0 && ly + 1 < P.WY) {
+        unsigned long long *q = win + lx + ly * P.WX;
+        if (w00) atomicAdd(q, (unsigned long long)w00);
+        if (w10) atomicAdd(q + 1, (unsigned long long)w10);
+        if (w11) atomicAdd(q + P.WX + 1, (unsigned long long)w11);
+        if (w01) atomicAdd(q + P.WX, (unsigned long long)w01);
+    } else {
+        unsigned long long *q = P.acc + ix + (long long)iy * P.W;
+        if (w00) atomicAdd(q, (unsigned long long)w00);
+        if (w10) atomicAdd(q + 1, (unsigned long long)w10);
+        if (w11) atomicAdd(q + P.W + 1, (unsigned long long)w11);
+        if (w01) atomicAdd(q + P.W, (unsigned long long)w01);
+    }
+}
+
+__global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
+    extern __shared__ unsigned long long win[];
+    __shared__ int s_tile, s_start, s_end;
+    __shared__ unsigned int s_lost;
+    DevCounters *cnt = P.cnt;
+    const long long n_slots = cnt->n_slots[P.sp], n_sorted = cnt->n_sorted[P.sp];
+    const int n_items = cnt->n_items[P.sp];
+    const uint32_t mask = (1u << P.S) - 1u;
+    const float inv2S = 1.0f / (float)(1u << P.S);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            unsigned int w = atomicAdd(&cnt->work_next[P.sp], 1u);
+            if ((int)w < n_items) {
+                WorkItem it = P.items[w];
+                s_tile = it.tile; s_start = it.start; s_end = it.end;
+            } else {
+                long long st = n_sorted + (long long)(w - n_items) * PUSH_CHUNK;
+                if (st >= n_slots) { s_tile = -2; s_start = s_end = 0; }
+                else { s_tile = -1; s_start = (int)st; s_end = (int)min(st + PUSH_CHUNK, n_slots); }
+            }
+            s_lost = 0;
+        }
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile == -2) break;
+        const bool use_win = P.win && tile >= 0;
+        int ox = 0, oy = 0;
+        if (use_win) {
+            int tx = tile % P.ntx, ty = tile / P.ntx;
+            ox = tx * P.tw + 1 - P.M;
+            oy = ty * P.th + 1 - P.M;
+            for (int q = threadIdx.x; q < P.WX * P.WY; q += blockDim.x) win[q] = 0ull;
+        }
+        __syncthreads();
+        unsigned int lost = 0;
+        for (int i = s_start + threadIdx.x; i < s_end; i += blockDim.x) {
+            float vx = P.VX[i];
+            if (isnan(vx)) continue; // hole
+            uint32_t X = P.X[i], Y = P.Y[i];
+            if (P.move) {
+                float vy = P.VY[i], vz = P.VZ[i];
+                // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
+                const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
+                const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
+                const float px = 1.0f - fx, py = 1.0f - fy;
+                const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
+                const long long n00 = (cx + 1) + (long long)(cy + 1) * P.W;
+                const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
+                const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
+                const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
+                const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
+                bool mag = false;
+                float Bx = 0.f, By = 0.f, Bz = 0.f;
+                if (P.bmode == 1) {
+                    mag = true; Bx = P.Bcx; By = P.Bcy; Bz = P.Bcz;
+                } else if (P.bmode == 2) {
+                    const float4 b00 = __ldg(P.B + n00);
+                    if (b00.w > 1.e-5f) {
+                        const float4 b10 = __ldg(P.B + n00 + 1), b11 = __ldg(P.B + n00 + P.W + 1);
+                        const float4 b01 = __ldg(P.B + n00 + P.W);
+                        Bx = k00 * b00.x + k10 * b10.x + k11 * b11.x + k01 * b01.x;
+                        By = k00 * b00.y + k10 * b10.y + k11 * b11.y + k01 * b01.y;
+                        Bz = k00 * b00.z + k10 * b10.z + k11 * b11.z + k01 * b01.z;
+                        mag = true;
+                    }
+                }
+                const float k1 = P.k1;
+                if (mag) { // Boris, part_expmover.f90:187-206
+                    const float Bt2 = Bx * Bx + By * By + Bz * Bz;
+                    const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+                    const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz;
+                    const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
+                    const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
+                    const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
+                    vx = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
+                    vy = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
+                    vz = v1z + k2 * (v3x * By - v3y * Bx);
+                } else { // leap-frog, :210-211
+                    vx = vx + 2.0f * k1 * Ex;
+                    vy = vy + 2.0f * k1 * Ey;
+                }
+                // move (:216-217) with unbiased stochastic rounding of the sub-unit part
+                const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u ^ P.step_key);
+                const float ux = (float)(h >> 8) * (1.0f / 16777216.0f);
+                const float uy = (float)(mix32(h ^ 0x7F4A7C15u) >> 8) * (1.0f / 16777216.0f);
+                long long Xn = (long long)X + __float2ll_rd(vx * P.cdx + ux);
+                long long Yn = (long long)Y + __float2ll_rd(vy * P.cdy + uy);
+                if (P.pbc) { // :222-241
+                    const long long Ym = P.ylim;
+                    long long k4 = Yn / Ym; // INT: truncation toward zero
+                    if (Yn >= Ym) {
+                        if (P.spec == 0) Yn = Yn - k4 * Ym;
+                        else { Yn = (k4 + 1) * Ym - Yn; vy = -vy; }
+                    }
+                    if (Yn <= 0) {
+                        if (P.spec == 0) Yn = (1 - k4) * Ym + Yn;
+                        else { Yn = k4 * Ym - Yn; vy = -vy; }
+                        if (Yn >= Ym) Yn = 0; // y = ymax exactly is kept as y = 0
+                    }
+                }
+                // FLOOR cell + check_outofbounds + four-corner wall test (:244-258)
+                int ixn = (int)(Xn >> P.S) + 1, iyn = (int)(Yn >> P.S) + 1;
+                ixn = min(max(ixn, 0), P.nx + 1);
+                iyn = min(max(iyn, 0), P.ny + 1);
+                bool is_lost = P.cellwall[ixn + (long long)iyn * (P.nx + 2)] != 0;
+                if (!is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
+                if (is_lost) {
+                    lost++;
+                    P.VX[i] = __int_as_float(0x7fc00000); // the slot becomes a hole
+                    continue;
+                }
+                if (P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
+                if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
+                    set_err(cnt, LERR_RANGE, 100);
+                    Xn = min(max(Xn, 0ll), P.xlim - 1);
+                    Yn = min(max(Yn, 0ll), P.ylim - 1);
+                }
+                X = (uint32_t)Xn;
+                Y = (uint32_t)Yn;
+                P.X[i] = X; P.Y[i] = Y;
+                P.VX[i] = vx; P.VY[i] = vy; P.VZ[i] = vz;
+            }
+            deposit(P, win, ox, oy, use_win, X, Y);
+        }
+        // lost-particle count: one atomic per warp, then per CTA
+        for (int o = 16; o > 0; o >>= 1) lost += __shfl_xor_sync(0xffffffffu, lost, o);
+        if ((threadIdx.x & 31) == 0 && lost) atomicAdd(&s_lost, lost);
+        __syncthreads();
+        if (use_win) {
+            for (int q = threadIdx.x; q < P.WX * P.WY; q += blockDim.x) {
+                unsigned long long v = win[q];
+                if (v) {
+                    int lx = q % P.WX, ly = q / P.WX;
+                    atomicAdd(P.acc + (ox + lx) + (long long)(oy + ly) * P.W, v);
+                }
+            }
+        }
+        if (threadIdx.x == 0 && s_lost) {
+            atomicAdd(&cnt->n_lost[P.sp], (unsigned long long)s_lost);
+            atomicAdd((unsigned long long *)&cnt->n_alive[P.sp], (unsigned long long)(-(long long)s_lost));
+        }
+        __syncthreads();
+    }
+}
+
+int push_deposit(lepic_ctx *c, int it, bool move) {
+    const lepic_config &g = c->cfg;
+    for (int s = 0; s < g.ntype; s++)
+        LCUDA(cudaMemsetAsync(c->sp[s].acc, 0, sizeof(unsigned long long) * c->nn, c->stream));
+    LCUDA(cudaMemsetAsync(c->dcnt->work_next, 0, sizeof(c->dcnt->work_next), c->stream));
+    const double amu = 1.66053886e-27;
+    for (int s = 0; s < g.ntype; s++) {
+        SpeciesBuf &B = c->sp[s];
+        PushP P;
+        memset(&P, 0, sizeof(P));
+        P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
+        P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+        P.E = c->Ef; P.B = c->Bf;
+        P.bmode = g.flag_B;
+        if (g.flag_B_pos == 1 && g.charge[s] > 0.0) P.bmode = 0; // :185
+        P.Bcx = (float)g.Bc[0]; P.Bcy = (float)g.Bc[1]; P.Bcz = (float)g.Bc[2];
+        P.cellwall = c->cellwall;
+        P.acc = B.acc;
+        P.items = B.items;
+        P.cnt = c->dcnt;
+        P.sp = s;
+        P.k1 = (float)(g.dt * g.charge[s] / (2.0 * g.mass[s]));
+        P.cdx = (float)(g.dt * (double)(1u << c->S) / g.dx);
+        P.cdy = (float)(g.dt * (double)(1u << c->S) / g.dy);
+        P.pbc = g.flag_pbc; P.spec = g.flag_spec; P.nmn = g.flag_nmn;
+        P.negion_nmn = (g.charge[s] < 0 && g.mass[s] >= amu && g.flag_nmn == 1) ? 1 : 0;
+        P.step_key = (uint32_t)(g.seed * 0x2545F491ull) ^ ((uint32_t)it * 0x27D4EB2Fu) ^ ((uint32_t)s * 0x165667B1u);
+        P.tw = c->tw; P.th = c->th; P.ntx = c->ntx;
+        P.M = 3;
+        P.WX = c->tw + 1 + 2 * P.M;
+        P.WY = c->th + 1 + 2 * P.M;
+        size_t smem = sizeof(unsigned long long) * (size_t)P.WX * P.WY;
+        P.win = smem <= 64 * 1024 ? 1 : 0;
+        if (!P.win) smem = 0;
+        P.move = move ? 1 : 0;
+        P.xlim = (long long)g.nx << c->S;
+        P.ylim = (long long)g.ny << c->S;
+        static bool attr_set = false;
+        if (!attr_set) {
+            LCUDA(cudaFuncSetAttribute(k_push_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+            attr_set = true;
+        }
+        int occ = 0;
+        LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit, PUSH_THREADS, smem));
+        int grid = c->num_sms * std::max(1, occ);
+        k_push_deposit<<<grid, PUSH_THREADS, smem, c->stream>>>(P);
+        LCUDA(cudaGetLastError());
+    }
+    return LEPIC_OK;
+}

@@ -1,0 +1,268 @@
+// sort.cu -- part_sorting (sorting.f90:92-251): counting sort of one species by cell.
+//
+// The reference (one thread) produces a STABLE order: particles grouped by cell index
+// ic = (ix-1) + nx*(iy-1) + 1, original order kept inside a cell.  Here:
+//   1. keys + histogram        (warp-aggregated atomics on the per-key counts)
+//   2. exclusive scan           (three-phase, fixed order)
+//   3. scatter of slot indices  (atomics: order inside a key is not yet defined)
+//   4. per-key segment sort of the slot indices (bitonic, ascending) -> stable again
+//   5. gather of the 5 SoA fields into the other buffer, holes dropped
+//   6. push work list: per tile, chunks of CHUNK particles
+// so the result is bit-identical to the reference's, independent of thread timing.
+// The key is the reference's cell index when tile_w = nx, tile_h = 1; other tile shapes
+// order cells tile by tile (the push kernel then stages a compact node window per tile).
+//
+// Roofline (per particle per sort): read X,Y (8 B) twice, keys 4+4 B, perm 4+4+4 B, the
+// 20 B record read + written once: ~72 B, amortised over the nsort = 10 step cadence.
+#include <algorithm>
+#include <climits>
+#include "lepic_internal.cuh"
+
+#define SORT_THREADS 256
+#define PUSH_CHUNK 2048
+#define SEG_WARP_MAX 256
+#define SEG_BLOCK_MAX 8192
+
+struct KeyP {
+    int S, nx, ny, tw, th, ntx;
+};
+__device__ __forceinline__ int cell_key(const KeyP &K, uint32_t X, uint32_t Y) {
+    int cx = (int)(X >> K.S), cy = (int)(Y >> K.S);
+    cx = min(max(cx, 0), K.nx - 1);
+    cy = min(max(cy, 0), K.ny - 1);
+    int tx = cx / K.tw, ty = cy / K.th;
+    int lx = cx - tx * K.tw, ly = cy - ty * K.th;
+    return ((ty * K.ntx + tx) * K.th + ly) * K.tw + lx;
+}
+
+__global__ void k_keys_hist(KeyP K, const uint32_t *X, const uint32_t *Y, const float *VX,
+                            const DevCounters *cnt, int sp, int *keys, int *counts) {
+    const long long n = cnt->n_slots[sp];
+    const unsigned lane = threadIdx.x & 31;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
+        long long i = i0 + threadIdx.x;
+        int key = -1;
+        if (i < n && !isnan(VX[i])) key = cell_key(K, X[i], Y[i]);
+        if (i < n) keys[i] = key;
+        unsigned m = __match_any_sync(0xffffffffu, key);
+        if (key >= 0 && lane == (unsigned)(__ffs(m) - 1)) atomicAdd(&counts[key], __popc(m));
+    }
+}
+
+// three-phase exclusive scan of counts[0..n) into offsets[0..n], offsets[n] = total
+#define SCAN_ITEMS 2048
+__global__ void k_scan_blocks(const int *counts, long long n, int *blocksums) {
+    __shared__ int s[SORT_THREADS];
+    long long base = (long long)blockIdx.x * SCAN_ITEMS;
+    int a = 0;
+    for (int k = threadIdx.x; k < SCAN_ITEMS; k += blockDim.x) {
+        long long i = base + k;
+        if (i < n) a += counts[i];
+    }
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = SORT_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) blocksums[blockIdx.x] = s[0];
+}
+__global__ void k_scan_top(int *blocksums, int nb) { // single block, in place, exclusive
+    __shared__ int s[1024];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += 1024) {
+        int i = base + threadIdx.x;
+        int v = (i < nb) ? blocksums[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int t = ((int)threadIdx.x >= o) ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        int incl = s[threadIdx.x];
+        if (i < nb) blocksums[i] = carry + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += incl;
+        __syncthreads();
+    }
+}
+__global__ void k_scan_final(const int *counts, long long n, const int *blocksums, int *offsets) {
+    __shared__ int s[SORT_THREADS];
+    __shared__ int carry;
+    long long base = (long long)blockIdx.x * SCAN_ITEMS;
+    if (threadIdx.x == 0) carry = blocksums[blockIdx.x];
+    __syncthreads();
+    for (int k0 = 0; k0 < SCAN_ITEMS; k0 += blockDim.x) {
+        long long i = base + k0 + threadIdx.x;
+        int v = (i < n) ? counts[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < SORT_THREADS; o <<= 1) {
+            int t = ((int)threadIdx.x >= o) ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        int incl = s[threadIdx.x];
+        if (i < n) offsets[i] = carry + incl - v;
+        if (i == n - 1) offsets[n] = carry + incl;
+        __syncthreads();
+        if (threadIdx.x == SORT_THREADS - 1) carry += incl;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *cursor, int *perm) {
+    const long long n = cnt->n_slots[sp];
+    const unsigned lane = threadIdx.x & 31;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
+        long long i = i0 + threadIdx.x;
+        int key = (i < n) ? keys[i] : -1;
+        unsigned m = __match_any_sync(0xffffffffu, key);
+        int leader = __ffs(m) - 1;
+        int base = 0;
+        if (key >= 0 && (int)lane == leader) base = atomicAdd(&cursor[key], __popc(m));
+        base = __shfl_sync(m, base, leader);
+        if (key >= 0) perm[base + __popc(m & ((1u << lane) - 1u))] = (int)i;
+    }
+}
+
+__global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, int *bigseg,
+                               DevCounters *cnt) {
+    __shared__ int buf[SORT_THREADS / 32][SEG_WARP_MAX];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long k = gw; k < nkeys; k += nw) {
+        int s0 = offsets[k], s1 = offsets[k + 1], n = s1 - s0;
+        if (n <= 1) continue;
+        bool sorted = true;
+        for (int q = lane; q + 1 < n; q += 32)
+            if (perm[s0 + q] > perm[s0 + q + 1]) sorted = false;
+        if (__all_sync(0xffffffffu, sorted)) continue;
+        if (n > SEG_WARP_MAX) {
+            if (lane == 0) {
+                int slot = atomicAdd(&cnt->n_big, 1);
+                bigseg[slot] = (int)k;
+            }
+            continue;
+        }
+        int *a = buf[warp];
+        for (int q = lane; q < n; q += 32) a[q] = perm[s0 + q];
+        __syncwarp();
+        bitonic_sort(a, n, lane, 32, WarpSync());
+        for (int q = lane; q < n; q += 32) perm[s0 + q] = a[q];
+        __syncwarp();
+    }
+}
+
+__global__ void k_segsort_big(const int *offsets, int *perm, const int *bigseg, const DevCounters *cnt) {
+    __shared__ int a[SEG_BLOCK_MAX];
+    const int nbig = cnt->n_big;
+    for (int s = blockIdx.x; s < nbig; s += gridDim.x) {
+        int k = bigseg[s];
+        int s0 = offsets[k], n = offsets[k + 1] - s0;
+        if (n <= SEG_BLOCK_MAX) {
+            for (int q = threadIdx.x; q < n; q += blockDim.x) a[q] = perm[s0 + q];
+            __syncthreads();
+            bitonic_sort(a, n, threadIdx.x, blockDim.x, BlockSync());
+            for (int q = threadIdx.x; q < n; q += blockDim.x) perm[s0 + q] = a[q];
+        } else {
+            bitonic_sort(perm + s0, n, threadIdx.x, blockDim.x, BlockSync());
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_gather(const int *perm, const int *offsets, long long nkeys, const uint32_t *X,
+                         const uint32_t *Y, const float *VX, const float *VY, const float *VZ,
+                         uint32_t *X2, uint32_t *Y2, float *VX2, float *VY2, float *VZ2) {
+    const long long n = offsets[nkeys];
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        int i = perm[j];
+        X2[j] = X[i]; Y2[j] = Y[i]; VX2[j] = VX[i]; VY2[j] = VY[i]; VZ2[j] = VZ[i];
+    }
+}
+
+// per tile: ceil(count / CHUNK) work items; single block, fixed order
+__global__ void k_items(const int *offsets, int ntiles, int keys_per_tile, WorkItem *items,
+                        int max_items, DevCounters *cnt, int sp, long long nkeys) {
+    __shared__ int s[1024];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ntiles; base += 1024) {
+        int t = base + threadIdx.x;
+        int st = 0, en = 0, ni = 0;
+        if (t < ntiles) {
+            st = offsets[(long long)t * keys_per_tile];
+            en = offsets[(long long)(t + 1) * keys_per_tile];
+            ni = (en - st + PUSH_CHUNK - 1) / PUSH_CHUNK;
+        }
+        s[threadIdx.x] = ni;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int v = ((int)threadIdx.x >= o) ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += v;
+            __syncthreads();
+        }
+        int first = carry + s[threadIdx.x] - ni;
+        for (int q = 0; q < ni; q++) {
+            int idx = first + q;
+            if (idx < max_items) {
+                WorkItem w;
+                w.tile = t;
+                w.start = st + q * PUSH_CHUNK;
+                w.end = min(en, st + (q + 1) * PUSH_CHUNK);
+                w.pad = 0;
+                items[idx] = w;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        int nitems = carry;
+        if (nitems > max_items) { set_err(cnt, LERR_CAPACITY, 300); nitems = max_items; }
+        long long total = offsets[nkeys];
+        cnt->n_items[sp] = nitems;
+        cnt->n_slots[sp] = total;
+        cnt->n_sorted[sp] = total;
+        cnt->n_alive[sp] = total;
+    }
+}
+
+int sort_species(lepic_ctx *c, int sp) {
+    SpeciesBuf &B = c->sp[sp];
+    const int cur = B.cur, nxt = 1 - cur;
+    KeyP K{c->S, c->cfg.nx, c->cfg.ny, c->tw, c->th, c->ntx};
+    const long long nk = c->nkeys;
+    int grid = c->num_sms * 8;
+    LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
+    LCUDA(cudaMemsetAsync(&c->dcnt->n_big, 0, sizeof(int), c->stream));
+    k_keys_hist<<<grid, SORT_THREADS, 0, c->stream>>>(K, B.X[cur], B.Y[cur], B.VX[cur], c->dcnt, sp,
+                                                        c->keys, c->counts);
+    int nb = div_up(nk, SCAN_ITEMS);
+    k_scan_blocks<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums);
+    k_scan_top<<<1, 1024, 0, c->stream>>>(c->blocksums, nb);
+    k_scan_final<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums, c->offsets);
+    LCUDA(cudaMemcpyAsync(c->cursor, c->offsets, sizeof(int) * nk, cudaMemcpyDeviceToDevice, c->stream));
+    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, c->dcnt, sp, c->cursor, c->perm);
+    k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, nk, c->perm, c->bigseg, c->dcnt);
+    k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, c->perm, c->bigseg, c->dcnt);
+    k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
+                                                   B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt], B.VX[nxt],
+                                                   B.VY[nxt], B.VZ[nxt]);
+    k_items<<<1, 1024, 0, c->stream>>>(c->offsets, c->ntiles, c->tw * c->th, B.items, B.max_items,
+                                       c->dcnt, sp, nk);
+    LCUDA(cudaGetLastError());
+    B.cur = nxt;
+    return LEPIC_OK;
+}

@@ -1,0 +1,144 @@
+/*
+ * lepic_oracle.h -- CPU FP64 restatement of the LePIC per-step PIC-MCC routines.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the CUDA path: only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.  The product
+ * library (jd_lepic_b200) never links, loads or calls it.
+ *
+ * Parity status: the reference (Fortran 90 + MPI + OpenMP) cannot be compiled in this
+ * environment (no Fortran compiler) and ships no tests, golden vectors or fixtures for
+ * these routines.  Parity against the reference's own outputs is therefore UNPINNED; the
+ * restatement is pinned instead by published known answers (Park-Miller minimal standard
+ * sequence) and analytic known-answer tests (Boris gyration, E x B drift, CIC charge
+ * conservation, manufactured Poisson solutions, MCC rate n*sigma*v).
+ *
+ * Conventions (identical to the reference's Fortran memory order):
+ *   node arrays  f(0:nx+2, 0:ny+2)  ->  f[i + j*(nx+3)], x index fastest
+ *   rhs          b(1:nx+1, 1:ny+1)  ->  b[(i-1) + (j-1)*(nx+1)]
+ *   E field      Ei(2, 0:nx+2, 0:ny+2) -> Ei[2*(i + j*(nx+3)) + c]
+ *   B field      Bi(4, 0:nx+2, 0:ny+2) -> Bi[4*(i + j*(nx+3)) + c]
+ *   particles    vxp(6, np) per species -> vxp[6*k + c], c = x,y,z,vx,vy,vz
+ * Species index 0 is the electron, then ions, then neutrals (negative mass), 0-based.
+ */
+#ifndef LEPIC_ORACLE_H
+#define LEPIC_ORACLE_H
+#include <stdint.h>
+
+#define O_MAXSP 8
+#define O_MAXCOL 64
+
+typedef struct {
+    int nx, ny;
+    double dx, dy, zmax, xmax, ymax, dt;
+    double eps0, qe, pi;
+    int flag_pbc, flag_spec, flag_nmn;
+    int flag_B;            /* 0: no B, 1: constant B (Bc), 2: B map on the field grid (Bi) */
+    int flag_B_pos;        /* 1: positive ions unmagnetised */
+    double Bc[3];
+    int ntype;             /* charged species (electrons first)                */
+    int nsp;               /* charged + neutral species                         */
+    double charge[O_MAXSP], mass[O_MAXSP], Nm[O_MAXSP], vt0[O_MAXSP];
+    double np_mx[O_MAXSP]; /* neutral densities live at the neutral indices     */
+    double nu_uplim[O_MAXSP];
+    int ns_coll, nsort;
+} o_cfg;
+
+typedef struct {
+    int npt;                 /* sig_npt_mx: points of the union energy grid           */
+    int ncol;                /* number of reactions                                    */
+    const double *sig_Er;    /* [npt]                                                  */
+    const double *sig;       /* [icol*npt + ipt]                                       */
+    const double *Eth;       /* [icol] threshold energy, eV                            */
+    const int32_t *col_info; /* [icol*10 + k], the reference's col_info(icol, k+1) with
+                                species entries converted to 0-based indices           */
+    const int32_t *p_ncol;   /* [ptype]                                                */
+    const int32_t *sig_list; /* [ptype*O_MAXCOL + k] reaction index, 0-based           */
+    const double *sigv_mx;   /* [ptype*O_MAXCOL + icol]                                */
+    int flag_ionrep;
+    double fEk;
+} o_xs;
+
+typedef struct {
+    int64_t n_lost;       /* wall / boundary losses            */
+    int64_t n_dead;       /* removed because flag_dead was set */
+} o_push_tally;
+
+typedef struct {
+    int64_t n_cand[O_MAXSP];              /* Nc per species                 */
+    int64_t n_coll[O_MAXCOL];             /* real collisions per reaction   */
+    int64_t n_add[O_MAXSP];               /* products appended per species  */
+    int64_t n_overflow;                   /* Ekr above the table            */
+    double nu_max[O_MAXSP];
+} o_mcc_tally;
+
+/* ran2.f90:1-15 -- Park-Miller minimal standard generator (Schrage). */
+double o_ran2(int32_t *irand);
+/* load_gauss.f90:16-39 */
+void o_load_gauss(double *vx, double *vy, double vt, const double rnd[2]);
+
+/* part_expmover.f90:1-517 (E gather, Boris/leap-frog, move, y wrap, wall loss,
+ * Neumann reflection, flag_dead removal, order-preserving compaction).
+ * Not restated: 3rd-dimension loss model (hz >= 0), dielectric charging, secondary
+ * emission, refluxing (opt_inj = 4), phase-space and power tallies. */
+void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                  const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                  o_push_tally *t);
+
+/* part_expmover.f90:520-610 -- adds into npg (caller zeroes it). */
+void o_charge_deposition(const o_cfg *c, int ptype, const double *vxp, int64_t np_tot,
+                         const double *kq, double *npg);
+
+/* calc_rho.f90:1-35 */
+void o_np_periodic(const o_cfg *c, double *npg, const int32_t *bcnd);
+/* calc_rho.f90:37-77 -- npg holds ntype grids back to back. */
+void o_calc_rhs(const o_cfg *c, const double *npg, double *rhs);
+/* calc_rho.f90:134-199 -- fills np_red (ntype grids) and c->np_mx[0..ntype-1]. */
+void o_dens_red(o_cfg *c, const double *npg, double *np_red, const int32_t *bcnd);
+
+/* Efield.f90:1-128, single-threaded loop order. */
+void o_calc_efield(const o_cfg *c, const double *phi, double *Ei, const int32_t *bcnd);
+
+/* iterative_solver.f90:1-69 with mg.f90 / sors.f90 on one rank.
+ * Returns 0, or -1 when the reference would abort on divergence. */
+typedef struct { int k; double ktot; double res; int sweeps_fine; } o_solve_stats;
+int o_iterative_solver(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
+                       int ng, int ncycl, double eps, o_solve_stats *st);
+/* One red-black SOR smoothing call (sors.f90:1-435), exposed for tests. */
+int o_sor_rb(int nx, int ny, double hx, double hy, double eps0, double *u, const double *b,
+             const int32_t *bcnd, double *res, double omega, double eps, int kmg, int dig,
+             int flag_pbc);
+/* mg.f90 helpers exposed for tests. */
+void o_restriction(int nx, int ny, double hx, double hy, double eps0, const double *u,
+                   const double *b, const int32_t *bcnd, int32_t *bcnd2h, double *r2h,
+                   double *e2h, int flag_pbc, int flag_nmn);
+void o_prolongation(int nx, int ny, double *u, const double *e2h, const int32_t *bcnd);
+
+/* sorting.f90:92-251 with nproc = 1 (stable counting sort by cell).  plist has
+ * pl_max+1 = nx + nx*ny + 2 entries; scratch holds 6*np_tot doubles. */
+void o_part_sorting(const o_cfg *c, double *vxp, int64_t np_tot, int32_t *plist,
+                    double *scratch);
+
+/* indexx.f90:1-88 (Numerical Recipes index sort), 0-based output. */
+void o_indexx(int n, const double *arr, int *indx);
+
+/* collisions.f90:1-207 + collision_OMP :209-1040 + SCATTER :1042-1070 for neutral
+ * targets (null-collision MCC), nproc = 1.  vxp/np_tot/cap/flag_dead are per species.
+ * Products are appended at np_tot + np_add.  Returns 0, -1 on Pmax > 1, -2 when a
+ * species array would exceed its capacity, -3 on a negative collision energy. */
+int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
+                 int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t);
+
+/* SCATTER, collisions.f90:1042-1070 */
+void o_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy, double vz,
+               double costheta, double phi);
+
+/* OpenMP variants used only for the timed CPU baseline: same arithmetic as the serial
+ * routines; the particle array is split into contiguous per-thread slabs with private
+ * density grids, reduced in thread order, like the reference's per-thread slabs. */
+void o_push_deposit_omp(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                        const int32_t *bcnd, const double *kq, double *vxp, int64_t *np_tot,
+                        int8_t *flag_dead, double *npg, int nthreads);
+int o_iterative_solver_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
+                           int ng, int ncycl, double eps, o_solve_stats *st, int nthreads);
+
+#endif

@@ -1,0 +1,312 @@
+"""ctypes wrapper of the CPU FP64 restatement (``lepic_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it; the product package
+``jd_lepic_b200`` never imports it.
+
+Parity against the reference's own outputs is UNPINNED (the Fortran reference cannot be
+built here and ships no golden vectors); the restatement is pinned by the Park-Miller
+published sequence and analytic known-answer tests in ``tests/test_oracle_kat.py``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+MAXSP = 8
+MAXCOL = 64
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "lepic_oracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "lepic_oracle.h"))):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "-s"], check=True, capture_output=True)
+    return LIB
+
+
+class OCfg(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("zmax", C.c_double), ("xmax", C.c_double),
+        ("ymax", C.c_double), ("dt", C.c_double),
+        ("eps0", C.c_double), ("qe", C.c_double), ("pi", C.c_double),
+        ("flag_pbc", C.c_int), ("flag_spec", C.c_int), ("flag_nmn", C.c_int),
+        ("flag_B", C.c_int), ("flag_B_pos", C.c_int),
+        ("Bc", C.c_double * 3),
+        ("ntype", C.c_int), ("nsp", C.c_int),
+        ("charge", C.c_double * MAXSP), ("mass", C.c_double * MAXSP), ("Nm", C.c_double * MAXSP),
+        ("vt0", C.c_double * MAXSP), ("np_mx", C.c_double * MAXSP), ("nu_uplim", C.c_double * MAXSP),
+        ("ns_coll", C.c_int), ("nsort", C.c_int),
+    ]
+
+
+class OXs(C.Structure):
+    _fields_ = [
+        ("npt", C.c_int), ("ncol", C.c_int),
+        ("sig_Er", C.POINTER(C.c_double)), ("sig", C.POINTER(C.c_double)),
+        ("Eth", C.POINTER(C.c_double)), ("col_info", C.POINTER(C.c_int32)),
+        ("p_ncol", C.POINTER(C.c_int32)), ("sig_list", C.POINTER(C.c_int32)),
+        ("sigv_mx", C.POINTER(C.c_double)),
+        ("flag_ionrep", C.c_int), ("fEk", C.c_double),
+    ]
+
+
+class OPushTally(C.Structure):
+    _fields_ = [("n_lost", C.c_int64), ("n_dead", C.c_int64)]
+
+
+class OMccTally(C.Structure):
+    _fields_ = [("n_cand", C.c_int64 * MAXSP), ("n_coll", C.c_int64 * MAXCOL),
+                ("n_add", C.c_int64 * MAXSP), ("n_overflow", C.c_int64), ("nu_max", C.c_double * MAXSP)]
+
+
+class OSolveStats(C.Structure):
+    _fields_ = [("k", C.c_int), ("ktot", C.c_double), ("res", C.c_double), ("sweeps_fine", C.c_int)]
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int32)
+_I8 = C.POINTER(C.c_int8)
+_LP = C.POINTER(C.c_int64)
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        L = C.CDLL(build())
+        L.o_ran2.restype = C.c_double
+        L.o_ran2.argtypes = [C.POINTER(C.c_int32)]
+        L.o_load_gauss.argtypes = [_DP, _DP, C.c_double, _DP]
+        L.o_part_mover.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _LP, _I8,
+                                   C.POINTER(OPushTally)]
+        L.o_charge_deposition.argtypes = [C.POINTER(OCfg), C.c_int, _DP, C.c_int64, _DP, _DP]
+        L.o_np_periodic.argtypes = [C.POINTER(OCfg), _DP, _IP]
+        L.o_calc_rhs.argtypes = [C.POINTER(OCfg), _DP, _DP]
+        L.o_dens_red.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP]
+        L.o_calc_efield.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP]
+        L.o_iterative_solver.restype = C.c_int
+        L.o_iterative_solver.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP, C.c_int, C.c_int, C.c_double,
+                                         C.POINTER(OSolveStats)]
+        L.o_iterative_solver_omp.restype = C.c_int
+        L.o_iterative_solver_omp.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP, C.c_int, C.c_int, C.c_double,
+                                             C.POINTER(OSolveStats), C.c_int]
+        L.o_sor_rb.restype = C.c_int
+        L.o_sor_rb.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _DP, _DP, _IP, _DP,
+                               C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.o_restriction.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _DP, _DP, _IP,
+                                    _IP, _DP, _DP, C.c_int, C.c_int]
+        L.o_prolongation.argtypes = [C.c_int, C.c_int, _DP, _DP, _IP]
+        L.o_part_sorting.argtypes = [C.POINTER(OCfg), _DP, C.c_int64, _IP, _DP]
+        L.o_indexx.argtypes = [C.c_int, _DP, C.POINTER(C.c_int)]
+        L.o_collisions.restype = C.c_int
+        L.o_collisions.argtypes = [C.POINTER(OCfg), C.POINTER(OXs), C.POINTER(_DP), _LP, _LP,
+                                   C.POINTER(_I8), C.POINTER(C.c_int32), C.POINTER(OMccTally)]
+        L.o_scatter.argtypes = [_DP, _DP, _DP, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.o_push_deposit_omp.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _DP, _LP, _I8, _DP,
+                                         C.c_int]
+        _lib = L
+    return _lib
+
+
+def dp(a):
+    return a.ctypes.data_as(_DP) if a is not None else None
+
+
+def ip(a):
+    return a.ctypes.data_as(_IP) if a is not None else None
+
+
+def make_cfg(case, sp) -> OCfg:
+    """o_cfg from a configs.Case and simulation.SpeciesParams (the same inputs the GPU gets)."""
+    from jd_lepic_b200 import deck as dk
+    c = OCfg()
+    c.nx, c.ny = case.nx, case.ny
+    c.dx, c.dy, c.zmax = case.dx, case.dy, case.zmax
+    c.xmax, c.ymax = case.nx * case.dx, case.ny * case.dy
+    c.dt = case.dt
+    c.eps0, c.qe, c.pi = dk.EPS0, dk.QE, 4.0 * math.atan(1.0)
+    c.flag_pbc = c.flag_spec = c.flag_nmn = 0
+    c.flag_B = case.flag_B
+    c.flag_B_pos = 0
+    for k in range(3):
+        c.Bc[k] = case.Bc[k]
+    c.ntype, c.nsp = sp.ntype, sp.nsp
+    for s in range(MAXSP):
+        c.charge[s], c.mass[s], c.Nm[s] = sp.charge[s], sp.mass[s], sp.Nm[s]
+        c.vt0[s], c.np_mx[s], c.nu_uplim[s] = sp.vt0[s], sp.np_mx[s], sp.nu_uplim[s]
+    c.ns_coll, c.nsort = 10, 10
+    return c
+
+
+class XsHolder:
+    """Keeps numpy buffers alive behind an OXs."""
+
+    def __init__(self, t):
+        self.arrs = [np.ascontiguousarray(t.sig_Er), np.ascontiguousarray(t.sig), np.ascontiguousarray(t.Eth),
+                     np.ascontiguousarray(t.col_info, dtype=np.int32), np.ascontiguousarray(t.p_ncol, dtype=np.int32),
+                     np.ascontiguousarray(t.sig_list, dtype=np.int32), np.ascontiguousarray(t.sigv_mx)]
+        a = self.arrs
+        self.xs = OXs(t.npt, t.ncol, dp(a[0]), dp(a[1]), dp(a[2]), ip(a[3]), ip(a[4]), ip(a[5]), dp(a[6]),
+                      t.flag_ionrep, t.fEk)
+
+
+def kq_of(bcnd: np.ndarray) -> np.ndarray:
+    """main.f90:334-344"""
+    return np.where(bcnd != -1, 2.0, 1.0)
+
+
+def mover(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, flag_dead=None):
+    n = C.c_int64(vxp.shape[0])
+    t = OPushTally()
+    fd = flag_dead.ctypes.data_as(_I8) if flag_dead is not None else None
+    lib().o_part_mover(C.byref(cfg), ptype, dp(Ei), dp(Bi), ip(bcnd), dp(vxp), C.byref(n), fd, C.byref(t))
+    return n.value, t
+
+
+def deposit(cfg, ptype, vxp, n, kq, npg):
+    lib().o_charge_deposition(C.byref(cfg), ptype, dp(vxp), n, dp(kq), dp(npg))
+
+
+def calc_rhs(cfg, npg):
+    rhs = np.zeros((cfg.ny + 1, cfg.nx + 1))
+    lib().o_calc_rhs(C.byref(cfg), dp(npg), dp(rhs))
+    return rhs
+
+
+def efield(cfg, phi, bcnd, Ei=None):
+    if Ei is None:
+        Ei = np.zeros((cfg.ny + 3, cfg.nx + 3, 2))
+    lib().o_calc_efield(C.byref(cfg), dp(phi), dp(Ei), ip(bcnd))
+    return Ei
+
+
+def solve(cfg, phi, rhs, bcnd, ng, eps, ncycl=20000, nthreads=1):
+    st = OSolveStats()
+    if nthreads > 1:
+        rc = lib().o_iterative_solver_omp(C.byref(cfg), dp(phi), dp(rhs), ip(bcnd), ng, ncycl, eps, C.byref(st),
+                                          nthreads)
+    else:
+        rc = lib().o_iterative_solver(C.byref(cfg), dp(phi), dp(rhs), ip(bcnd), ng, ncycl, eps, C.byref(st))
+    return rc, st
+
+
+def sort(cfg, vxp, n):
+    pl = np.zeros(cfg.nx + cfg.nx * cfg.ny + 2, dtype=np.int32)
+    scratch = np.zeros((max(n, 1), 6))
+    lib().o_part_sorting(C.byref(cfg), dp(vxp), n, ip(pl), dp(scratch))
+    return pl
+
+
+def ran2_sequence(seed: int, n: int) -> tuple[np.ndarray, int]:
+    s = C.c_int32(seed)
+    out = np.array([lib().o_ran2(C.byref(s)) for _ in range(n)])
+    return out, s.value
+
+
+def l2_residual(cfg, phi, rhs, bcnd):
+    """||b - A u||_2 / ||b - A u_D||_2 over bcnd == -1 nodes (u_D: unknowns zeroed), FP64."""
+    aw = cfg.eps0 / (cfg.dx * cfg.dx)
+    an = cfg.eps0 / (cfg.dy * cfg.dy)
+    ac = -(an + an + aw + aw)
+    u = phi
+    c = u[1:-1, 1:-1]
+    Au = aw * u[1:-1, :-2] + an * u[2:, 1:-1] + an * u[:-2, 1:-1] + aw * u[1:-1, 2:] + ac * c
+    m = bcnd[1:-1, 1:-1] == -1
+    r = rhs - Au
+    w = bcnd > 0
+    ud = np.where(w, u, 0.0)
+    Aud = aw * ud[1:-1, :-2] + an * ud[2:, 1:-1] + an * ud[:-2, 1:-1] + aw * ud[1:-1, 2:]
+    d = rhs - Aud
+    return math.sqrt(float((r[m] ** 2).sum())) / max(math.sqrt(float((d[m] ** 2).sum())), 1e-300)
+
+
+class OracleSimulation:
+    """The reference's step loop (main.f90:818-1090, in-scope routines) on the CPU, FP64."""
+
+    def __init__(self, case, nthreads: int = 1, particles: dict | None = None, seed: int | None = None,
+                 capacity_factor: float = 1.3):
+        from jd_lepic_b200 import deck as dk
+        from jd_lepic_b200.simulation import species_params
+        self.case = case
+        self.deck = dk.read_reactions(case.deck_text, case.ngas)
+        self.tables = dk.ordering(self.deck)
+        self.sp = species_params(case, self.deck)
+        self.cfg = make_cfg(case, self.sp)
+        self.xsh = XsHolder(self.tables)
+        self.nt = nthreads
+        self.bcnd = np.ascontiguousarray(case.bcnd, dtype=np.int32)
+        self.phi = np.ascontiguousarray(case.phi0, dtype=np.float64).copy()
+        self.kq = kq_of(self.bcnd)
+        self.Bi = np.ascontiguousarray(case.Bi) if case.Bi is not None else None
+        self.Ei = np.zeros((case.ny + 3, case.nx + 3, 2))
+        self.ng = case.levels()
+        ntype = self.sp.ntype
+        nn = (case.nx + 3) * (case.ny + 3)
+        self.npg = np.zeros((ntype, case.ny + 3, case.nx + 3))
+        self.seed = C.c_int32(seed if seed is not None else 123456)  # main.f90:530 for iproc = 1
+        self.vxp, self.np_tot, self.cap, self.flag_dead = [], [], [], []
+        for s in range(ntype):
+            arr = particles[s] if particles is not None else None
+            n = arr.shape[0] if arr is not None else 0
+            cap = max(int(n * capacity_factor) + 1024, 1024)
+            buf = np.zeros((cap, 6))
+            if n:
+                buf[:n] = arr
+            self.vxp.append(buf)
+            self.np_tot.append(n)
+            self.cap.append(cap)
+            self.flag_dead.append(np.zeros(cap, dtype=np.int8))
+        self._nn = nn
+        self.deposit_all()
+
+    def deposit_all(self):
+        self.npg[:] = 0.0
+        for s in range(self.sp.ntype):
+            deposit(self.cfg, s, self.vxp[s], self.np_tot[s], self.kq, self.npg[s])
+
+    def step(self, it: int, eps: float | None = None):
+        case = self.case
+        eps = case.eps if eps is None else eps
+        self.rhs = calc_rhs(self.cfg, self.npg)
+        rc, self.solve_stats = solve(self.cfg, self.phi, self.rhs, self.bcnd, self.ng, eps, nthreads=self.nt)
+        if rc != 0:
+            raise RuntimeError("oracle Poisson solve diverged")
+        efield(self.cfg, self.phi, self.bcnd, self.Ei)
+        if it % 10 == 1:
+            for s in range(self.sp.ntype):
+                if self.np_tot[s] > 0:
+                    sort(self.cfg, self.vxp[s], self.np_tot[s])
+        if it > 1 and it % 10 == 1:
+            self.collide()
+        self.npg[:] = 0.0
+        for s in range(self.sp.ntype):
+            n = C.c_int64(self.np_tot[s])
+            lib().o_push_deposit_omp(C.byref(self.cfg), s, dp(self.Ei), dp(self.Bi), ip(self.bcnd), dp(self.kq),
+                                     dp(self.vxp[s]), C.byref(n), self.flag_dead[s].ctypes.data_as(_I8),
+                                     dp(self.npg[s]), self.nt)
+            self.np_tot[s] = n.value
+
+    def collide(self):
+        ntype = self.sp.ntype
+        arrs = (_DP * MAXSP)(*[dp(self.vxp[s]) for s in range(ntype)])
+        npt = (C.c_int64 * MAXSP)(*self.np_tot)
+        cap = (C.c_int64 * MAXSP)(*self.cap)
+        fds = (_I8 * MAXSP)(*[self.flag_dead[s].ctypes.data_as(_I8) for s in range(ntype)])
+        t = OMccTally()
+        rc = lib().o_collisions(C.byref(self.cfg), C.byref(self.xsh.xs), arrs, npt, cap, fds, C.byref(self.seed),
+                                C.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"oracle collisions failed with {rc}")
+        for s in range(ntype):
+            self.np_tot[s] = npt[s]
+        self.mcc = t
+        return t

@@ -1,0 +1,223 @@
+"""Known-answer tests that pin the CPU restatement (the oracle) of the reference routines.
+
+The reference has no tests or golden vectors; these pin the restatement to published values
+(Park-Miller minimal standard) and to analytic physics (Boris rotation, E x B drift, CIC
+charge conservation, discrete Poisson solutions, MCC rate n*sigma*v)."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from jd_lepic_b200 import configs, deck as dk
+from jd_lepic_b200.simulation import species_params
+
+
+def small_case(nx=32, ny=32, ppc=4):
+    return configs.case0(ppc=ppc, nx=nx, ny=ny)
+
+
+def cfg_for(case):
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    sp = species_params(case, d)
+    return O.make_cfg(case, sp), sp
+
+
+def test_ran2_park_miller_minimal_standard(oracle_lib):
+    # ran2.f90:1-15 is Park & Miller's minimal standard; from seed 1 the 10000th state is
+    # 1043618065 (Park & Miller, CACM 31(10), 1988).
+    vals, state = O.ran2_sequence(1, 10000)
+    assert state == 1043618065
+    assert vals[0] == 16807 / 2147483647
+
+
+def test_load_gauss_moments(oracle_lib):
+    rng = np.random.default_rng(1)
+    vt = 3.0
+    xs, ys = [], []
+    L = O.lib()
+    a, b = C.c_double(), C.c_double()
+    for _ in range(20000):
+        r = (C.c_double * 2)(*rng.random(2))
+        L.o_load_gauss(C.byref(a), C.byref(b), vt, r)
+        xs.append(a.value)
+        ys.append(b.value)
+    xs, ys = np.array(xs), np.array(ys)
+    # components are normal with sigma = vt/sqrt(2)
+    assert abs(xs.mean()) < 0.05 and abs(ys.mean()) < 0.05
+    assert abs(xs.std() - vt / math.sqrt(2)) < 0.05
+    assert abs(ys.std() - vt / math.sqrt(2)) < 0.05
+
+
+def _uniform_E(case, ex=0.0, ey=0.0):
+    Ei = np.zeros((case.ny + 3, case.nx + 3, 2))
+    Ei[..., 0] = ex
+    Ei[..., 1] = ey
+    return Ei
+
+
+def test_boris_gyration_angle_and_speed(oracle_lib):
+    case = small_case()
+    case.flag_B = 1
+    case.Bc = (0.0, 0.0, 0.02)
+    cfg, sp = cfg_for(case)
+    Ei = _uniform_E(case)
+    v0 = 1.0e5
+    p = np.array([[0.5 * case.nx * case.dx, 0.5 * case.ny * case.dy, 0.0, v0, 0.0, 0.0]])
+    k1 = case.dt * sp.charge[0] / (2 * sp.mass[0])
+    theta = -2.0 * math.atan(k1 * 0.02)  # Boris rotation per step (q < 0: counter-clockwise)
+    for _ in range(50):
+        n, _t = O.mover(cfg, 0, Ei, None, case.bcnd, p)
+        assert n == 1
+    ang = math.atan2(p[0, 4], p[0, 3])
+    expect = math.remainder(50 * theta, 2 * math.pi)
+    assert abs(math.remainder(ang - expect, 2 * math.pi)) < 1e-9
+    assert abs(math.hypot(p[0, 3], p[0, 4]) - v0) / v0 < 1e-12
+
+
+def test_exb_drift(oracle_lib):
+    case = small_case(64, 64)
+    case.flag_B = 1
+    case.Bc = (0.0, 0.0, 0.05)
+    cfg, sp = cfg_for(case)
+    ex = 1.0e3
+    Ei = _uniform_E(case, ex=ex)
+    p = np.array([[0.5 * case.nx * case.dx, 0.5 * case.ny * case.dy, 0.0, 0.0, 0.0, 0.0]])
+    y0 = p[0, 1]
+    nsteps = 4000
+    for _ in range(nsteps):
+        O.mover(cfg, 0, Ei, None, case.bcnd, p)
+    vd = (p[0, 1] - y0) / (nsteps * case.dt)
+    assert abs(vd - (-ex / 0.05)) / (ex / 0.05) < 0.02  # v_E = E x B / B^2
+
+
+def test_leapfrog_constant_field(oracle_lib):
+    case = small_case()
+    cfg, sp = cfg_for(case)
+    ey = -500.0
+    Ei = _uniform_E(case, ey=ey)
+    p = np.array([[0.5 * case.nx * case.dx, 0.5 * case.ny * case.dy, 0.0, 0.0, 0.0, 0.0]])
+    O.mover(cfg, 0, Ei, None, case.bcnd, p)
+    assert abs(p[0, 4] - sp.charge[0] / sp.mass[0] * ey * case.dt) < 1e-9 * abs(p[0, 4])
+
+
+def test_wall_loss_and_compaction(oracle_lib):
+    case = small_case()
+    cfg, sp = cfg_for(case)
+    Ei = _uniform_E(case)
+    L = case.nx * case.dx
+    p = np.array([[0.5 * L, 0.5 * L, 0, 0, 0, 0],
+                  [0.5 * case.dx, 0.5 * L, 0, -1e8, 0, 0],   # leaves through x = 0
+                  [0.3 * L, 0.6 * L, 0, 0, 0, 0]])
+    n, t = O.mover(cfg, 0, Ei, None, case.bcnd, p)
+    assert n == 2 and t.n_lost == 1
+    assert p[1, 0] == pytest.approx(0.3 * L)  # order-preserving compaction
+
+
+def test_cic_charge_conservation(oracle_lib):
+    case = small_case()
+    cfg, sp = cfg_for(case)
+    rng = np.random.default_rng(3)
+    n = 5000
+    p = np.zeros((n, 6))
+    p[:, 0] = rng.random(n) * case.nx * case.dx
+    p[:, 1] = rng.random(n) * case.ny * case.dy
+    kq = np.ones((case.ny + 3, case.nx + 3))
+    npg = np.zeros_like(kq)
+    O.deposit(cfg, 0, p, n, kq, npg)
+    total = npg.sum() * case.dx * case.dy * case.zmax / sp.Nm[0]
+    assert abs(total - n) < 1e-9 * n
+
+
+def _manufactured(case):
+    nx, ny = case.nx, case.ny
+    i = np.arange(nx + 3) - 1
+    j = np.arange(ny + 3) - 1
+    X, Y = np.meshgrid(i / nx, j / ny)
+    u = 3.0 * np.sin(math.pi * X) * np.sin(2 * math.pi * Y) + 2.0 * X
+    return u
+
+
+def _apply_A(cfg, u):
+    aw = cfg.eps0 / (cfg.dx * cfg.dx)
+    an = cfg.eps0 / (cfg.dy * cfg.dy)
+    ac = -(2 * an + 2 * aw)
+    return aw * u[1:-1, :-2] + an * u[2:, 1:-1] + an * u[:-2, 1:-1] + aw * u[1:-1, 2:] + ac * u[1:-1, 1:-1]
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_mg_manufactured_solution(oracle_lib, n):
+    case = small_case(n, n)
+    cfg, sp = cfg_for(case)
+    ue = _manufactured(case)
+    b = _apply_A(cfg, ue)
+    phi = np.where(case.bcnd >= 1, ue, 0.0)
+    rc, st = O.solve(cfg, phi, b, case.bcnd, case.levels(), 1e-12)
+    assert rc == 0
+    interior = case.bcnd == -1
+    assert np.abs(phi - ue)[interior].max() < 1e-8 * np.abs(ue).max()
+    assert O.l2_residual(cfg, phi, b, case.bcnd) < 1e-10
+
+
+def test_mg_vcycle_contracts(oracle_lib):
+    case = small_case(64, 64)
+    cfg, sp = cfg_for(case)
+    ue = _manufactured(case)
+    b = _apply_A(cfg, ue)
+    phi = np.where(case.bcnd >= 1, ue, 0.0)
+    res = []
+    for k in range(4):
+        rc, st = O.solve(cfg, phi, b, case.bcnd, case.levels(), 1e-30, ncycl=1)
+        res.append(O.l2_residual(cfg, phi, b, case.bcnd))
+    assert all(res[k + 1] < 0.3 * res[k] for k in range(3))
+
+
+def test_sort_stable_by_cell(oracle_lib):
+    case = small_case(16, 16)
+    cfg, sp = cfg_for(case)
+    rng = np.random.default_rng(5)
+    n = 3000
+    p = np.zeros((n, 6))
+    p[:, 0] = rng.random(n) * case.nx * case.dx
+    p[:, 1] = rng.random(n) * case.ny * case.dy
+    p[:, 3] = np.arange(n)  # original index as a tag
+    pl = O.sort(cfg, p, n)
+    ic = (p[:, 0] / case.dx).astype(int) + case.nx * (p[:, 1] / case.dy).astype(int)
+    assert np.all(np.diff(ic) >= 0)
+    for c in np.unique(ic):  # stable inside each cell
+        assert np.all(np.diff(p[ic == c, 3]) > 0)
+    counts = np.bincount(ic, minlength=case.nx * case.ny)
+    assert np.array_equal(pl[1:case.nx * case.ny + 1], np.cumsum(counts))
+
+
+def test_indexx_ascending(oracle_lib):
+    rng = np.random.default_rng(7)
+    for n in (1, 3, 7, 8, 20, 60):
+        a = rng.random(n)
+        idx = (C.c_int * n)()
+        O.lib().o_indexx(n, O.dp(a), idx)
+        assert list(idx) == list(np.argsort(a))
+
+
+def test_mcc_rate_constant_cross_section(oracle_lib):
+    """Null-collision MCC with a constant elastic cross section: the number of real collisions
+    per call is N * n_gas * sigma * v * ns_coll * dt (collisions.f90)."""
+    case = small_case(16, 16)
+    E = dk.energy_grid(1e3, 50)
+    text = dk.write_deck("[Ar+]", 39.95, 0.03, "[Ar]", 0.0258,
+                         [("[e]+[Ar]->[e]+[Ar]", "COLLISION", 0.0, E, dk.sigma_constant(E, 1e-19))])
+    case.deck_text = text
+    n = 200000
+    v = 2.0e6
+    p = np.zeros((n, 6))
+    rng = np.random.default_rng(11)
+    p[:, 0] = rng.random(n) * case.nx * case.dx
+    p[:, 1] = rng.random(n) * case.ny * case.dy
+    p[:, 3] = v
+    sim = O.OracleSimulation(case, particles={0: p, 1: p[:10].copy()}, seed=1)
+    t = sim.collide()
+    nu = case.ngas * 1e-19 * v  # neutral velocity is negligible against v
+    expect = n * nu * 10 * case.dt
+    got = t.n_coll[0]
+    assert abs(got - expect) < 5 * math.sqrt(expect)
