@@ -1,0 +1,437 @@
+"""Benchmark: particle-steps/s of the full PIC-MCC step (rhs -> Poisson -> E -> sort -> MCC ->
+push+deposit) on the 2048x2048 aperture-plate workload, one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 4]
+
+Prints ONE JSON line (rank 0).  Timing: CUDA events on the library's own stream, barrier +
+synchronize on both sides, max over ranks.  The particle arrays (8.4 GB per species) are far
+larger than L2, so no L2 flush is needed between steps.  Weak scaling for N > 1: every rank
+holds the full per-GPU particle load of the same plasma and the int64 charge accumulators are
+summed with one NCCL all-reduce per step (exact, order-free); Poisson is solved replicated.
+
+``--impl reference`` times the CPU restatement of the same routines (OpenMP, all host cores)
+on a bounded sample of the same workload and extrapolates to the full particle count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_PARTICLE_STEP = 40  # X, Y, VX, VY, VZ read + written by the fused push/deposit
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_particle():
+    """DRAM bytes per pushed particle of k_push_deposit from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "push_deposit_ncu.md")
+    try:
+        m = re.search(r"dram_bytes_per_particle\s*=\s*([0-9.]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.count(",") >= 8]
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+def cpu_baseline(case, sample_particles: int, steps: int, warmup: int, nthreads: int) -> dict:
+    """CPU restatement (OpenMP, `nthreads`) of the same step on `sample_particles` particles per
+    species with the full grid; the particle part is scaled to the full particle count."""
+    from oracle import oracle as O
+    from jd_lepic_b200.simulation import mean_density
+
+    rng = np.random.default_rng(case.seed)
+    n = sample_particles
+    # positions: uniform or the Gaussian profile by rejection, outside the wall cells
+    L = case.nx * case.dx
+    pts = []
+    while sum(len(p) for p in pts) < n:
+        x = rng.random(2 * n) * L
+        y = rng.random(2 * n) * case.ny * case.dy
+        if case.profile == 1:
+            r2 = (x - 0.5 * L) ** 2 + (y - 0.5 * case.ny * case.dy) ** 2
+            dens = case.n_floor + (case.n_peak - case.n_floor) * np.exp(-r2 / (2 * case.sigma ** 2))
+            keep = rng.random(2 * n) * case.n_peak <= dens
+            x, y = x[keep], y[keep]
+        ix = (x / case.dx).astype(int) + 1
+        iy = (y / case.dy).astype(int) + 1
+        b = case.bcnd
+        wall = (b[iy, ix] >= 1) & (b[iy, ix + 1] >= 1) & (b[iy + 1, ix + 1] >= 1) & (b[iy + 1, ix] >= 1)
+        pts.append(np.stack([x[~wall], y[~wall]], 1))
+    xy = np.concatenate(pts)[:n]
+    sim = None
+    parts = {}
+    from jd_lepic_b200 import deck as dk
+    from jd_lepic_b200.simulation import species_params
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    spp = species_params(case, d)
+    for s in range(spp.ntype):
+        p = np.zeros((n, 6))
+        p[:, :2] = xy
+        p[:, 3:] = rng.normal(0, spp.vt0[s] / np.sqrt(2), (n, 3))
+        parts[s] = p
+    # the sample carries the full charge: macro-weights scaled by N_full / n
+    sim = O.OracleSimulation(case, nthreads=nthreads, particles=parts, seed=123456)
+    scale = case.n_particles / n
+    for s in range(spp.ntype):
+        sim.cfg.Nm[s] = spp.Nm[s] * scale
+    sim.deposit_all()
+    t_grid, t_part = [], []
+    import ctypes as C
+    for it in range(2, warmup + steps + 2):  # steps without sort/MCC; those are timed below
+        t0 = time.perf_counter()
+        sim.rhs = O.calc_rhs(sim.cfg, sim.npg)
+        rc, _st = O.solve(sim.cfg, sim.phi, sim.rhs, sim.bcnd, sim.ng, case.eps if case.poisson_mode == 0 else 1e-8,
+                          nthreads=nthreads)
+        O.efield(sim.cfg, sim.phi, sim.bcnd, sim.Ei)
+        t1 = time.perf_counter()
+        sim.npg[:] = 0.0
+        for s in range(spp.ntype):
+            nn = C.c_int64(sim.np_tot[s])
+            O.lib().o_push_deposit_omp(C.byref(sim.cfg), s, O.dp(sim.Ei), O.dp(sim.Bi), O.ip(sim.bcnd), O.dp(sim.kq),
+                                       O.dp(sim.vxp[s]), C.byref(nn), sim.flag_dead[s].ctypes.data_as(O._I8),
+                                       O.dp(sim.npg[s]), nthreads)
+            sim.np_tot[s] = nn.value
+        t2 = time.perf_counter()
+        if it > warmup + 1:
+            t_grid.append(t1 - t0)
+            t_part.append(t2 - t1)
+    t0 = time.perf_counter()
+    for s in range(spp.ntype):
+        O.sort(sim.cfg, sim.vxp[s], sim.np_tot[s])
+    t_sort = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sim.collide()
+    t_mcc = time.perf_counter() - t0
+    # per step, with sort and MCC at their 1-in-10 cadence (main.f90:479-480)
+    grid_s = float(np.mean(t_grid))
+    part_s = (float(np.mean(t_part)) + (t_sort + t_mcc) / 10.0) * scale
+    step_s = grid_s + part_s
+    total = case.n_particles * spp.ntype
+    return {"value": total / step_s, "unit": "particle-steps/s", "cores": nthreads, "kind": "port",
+            "step_ms_extrapolated": step_s * 1e3, "grid_ms": grid_s * 1e3, "particle_ms_extrapolated": part_s * 1e3,
+            "sample": (f"{n} particles/species (of {case.n_particles}) on the full {case.nx}x{case.ny} grid, "
+                       f"{steps} steps after {warmup} warm-up; Poisson+E measured on the full grid, "
+                       f"particle phases scaled by {scale:.1f}")}
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from jd_lepic_b200 import configs
+    case = configs.make_case(args.config)
+    nt = host_threads()
+    sample = args.cpu_sample
+    t0 = time.perf_counter()
+    cb = cpu_baseline(case, sample, args.steps, args.warmup, nt)
+    wall = time.perf_counter() - t0
+    line = {"metric": "particle-steps/s per PIC step (push+deposit+MCC+sort+Poisson to 1e-8)",
+            "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cb["step_ms_extrapolated"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": case.name, "particles_per_species": case.n_particles, "grid": [case.nx, case.ny],
+                       "poisson": "reference multigrid (FP64, L1 criterion) on the CPU"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from jd_lepic_b200 import configs, _capi as capi
+    from jd_lepic_b200.simulation import GpuSimulation
+    import ctypes as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    case = configs.make_case(args.config, **({"ppc": args.ppc} if args.ppc else {}))
+    case.seed = case.seed + 7919 * rank
+    sim = GpuSimulation(case, tile=(args.tile, args.tile))
+    lib, ctx = sim.lib, sim.ctx
+    stream = torch.cuda.ExternalStream(sim.stream_ptr())
+    mode = args.mode
+    eps = 1e-8
+
+    acc_views = []
+    if world > 1:
+        for s in range(sim.sp.ntype):
+            ptr = C.c_void_p()
+            sim.check(lib.lepic_gpu_deposit_grid(ctx, s, C.byref(ptr)), "deposit_grid")
+            nn = (case.nx + 3) * (case.ny + 3)
+
+            class _A:
+                __cuda_array_interface__ = {"shape": (nn,), "typestr": "<i8", "data": (ptr.value, False),
+                                            "version": 3, "stream": sim.stream_ptr()}
+            acc_views.append(torch.as_tensor(_A(), device=f"cuda:{local}"))
+
+    def reduce_rho():
+        if world > 1:
+            with torch.cuda.stream(stream):
+                for t in acc_views:
+                    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+
+    ev = {}
+
+    def phase(name, it, fn):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        ev.setdefault(name, []).append((it, a, b))
+
+    def one_step(it, timed):
+        def rec(name, fn):
+            if timed:
+                phase(name, it, fn)
+            else:
+                fn()
+        rec("rhs", lambda: sim.check(lib.lepic_gpu_calc_rhs(ctx, None), "calc_rhs"))
+        rec("poisson", lambda: sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, mode, None), "solver"))
+        rec("efield", lambda: sim.check(lib.lepic_gpu_calc_efield(ctx, None), "efield"))
+        if it % 10 == 1:
+            def srt():
+                for s in range(sim.sp.ntype):
+                    sim.check(lib.lepic_gpu_part_sorting(ctx, s, None), "sort")
+            rec("sort", srt)
+        if it > 1 and it % 10 == 1:
+            rec("mcc", lambda: sim.check(lib.lepic_gpu_collisions(ctx, it, None), "collisions"))
+        rec("push_deposit", lambda: sim.check(lib.lepic_gpu_push_deposit(ctx, it, None), "push"))
+        rec("allreduce", reduce_rho) if world > 1 else None
+
+    # cold solve to a converged phi, then warm-up steps
+    it = 1
+    for _ in range(args.warmup):
+        one_step(it, False)
+        it += 1
+    sim.sync()
+    n_start = sum(sim.push_stats()["np_tot"])
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    first_timed = it
+    for _ in range(args.steps):
+        one_step(it, True)
+        it += 1
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    sim.sync()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    n_end = sum(sim.push_stats()["np_tot"])
+    total_ms = t_start.elapsed_time(t_end)
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    phases = {k: sum(a.elapsed_time(b) for _, a, b in v) for k, v in ev.items()}
+    n_avg = 0.5 * (n_start + n_end)
+    value = n_avg * args.steps * world / (total_ms * 1e-3)
+    push_ms = phases["push_deposit"] / args.steps
+    bytes_per_launch = BYTES_PER_PARTICLE_STEP * n_avg
+    peak, peak_kind = peaks()
+    achieved = bytes_per_launch / (push_ms * 1e-3) / 1e9
+    tpp = profiled_traffic_per_particle()
+
+    # Poisson: plain FP64 multigrid (the reference's V-cycle, L2 criterion) vs the FP32-in-FP64
+    # refinement, same rhs, both warm-started from the same phi
+    phi_save = sim.grid(capi.GRID_PHI)
+    pois = {}
+    for name, m in (("fp64_mg", capi.POISSON_FP64_MG_L2), ("mixed_ir", capi.POISSON_MIXED_IR)):
+        sim.set_phi(phi_save)
+        st = capi.LepicSolveStats()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, m, C.byref(st)), "solver")
+        b.record(stream)
+        torch.cuda.synchronize()
+        pois[name] = {"ms": a.elapsed_time(b), "cycles": st.cycles, "res_l2_rel": st.res_l2_rel}
+    sim.set_phi(phi_save)
+
+    # end to end through the C ABI with host buffers: phi exchanged with pinned host memory
+    # every step (the Fortran host's array) and the particle counters read back
+    e2e_steps = min(args.steps, 10)
+    nn = (case.nx + 3) * (case.ny + 3)
+    phi_host = torch.empty(nn, dtype=torch.float64, pin_memory=True)
+    phi_host.copy_(torch.from_numpy(phi_save.ravel()))
+    php = C.cast(phi_host.data_ptr(), C.POINTER(C.c_double))
+    ps = capi.LepicPushStats()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    w0 = time.perf_counter()
+    ne0 = n_end
+    for _ in range(e2e_steps):
+        sim.check(lib.lepic_gpu_calc_rhs(ctx, None), "calc_rhs")
+        sim.check(lib.lepic_gpu_iterative_solver(ctx, php, eps, mode, None), "solver")
+        sim.check(lib.lepic_gpu_calc_efield(ctx, None), "efield")
+        if it % 10 == 1:
+            for s in range(sim.sp.ntype):
+                sim.check(lib.lepic_gpu_part_sorting(ctx, s, None), "sort")
+        if it > 1 and it % 10 == 1:
+            sim.check(lib.lepic_gpu_collisions(ctx, it, None), "collisions")
+        sim.check(lib.lepic_gpu_push_deposit(ctx, it, C.byref(ps)), "push")
+        reduce_rho()
+        it += 1
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    ne1 = sum(ps.np_tot[:sim.sp.ntype])
+    e2e_value = 0.5 * (ne0 + ne1) * e2e_steps * world / e2e_s
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(case, args.cpu_sample, 3, 1, host_threads())
+    line = None
+    if rank == 0:
+        # kernels of this library launched in the timed steps (memsets/copies not counted):
+        # rhs 1, Poisson 1 (cooperative), E field 2, push 1 per species; a sort step adds 9 per
+        # species, a collision step 1 k_mcc per colliding species + 1 commit per species
+        n_mcc = sum(1 for s in range(sim.sp.ntype) if sim.xs.p_ncol[s] > 0)
+        launches = 0
+        for t in range(first_timed, first_timed + args.steps):
+            launches += 1 + 1 + 2 + sim.sp.ntype
+            if t % 10 == 1:
+                launches += 9 * sim.sp.ntype
+            if t > 1 and t % 10 == 1:
+                launches += n_mcc + sim.sp.ntype
+        line = {
+            "metric": "particle-steps/s per PIC step (push+deposit+MCC+sort+Poisson to 1e-8)",
+            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 particles / f64 Poisson residual",
+            "data": "synthetic",
+            "config": {"workload": case.name, "grid": [case.nx, case.ny],
+                       "particles_per_species_per_gpu": case.n_particles, "species": sim.sp.ntype,
+                       "particles_avg_per_gpu": n_avg, "poisson": "mixed FP32 V-cycles in FP64 refinement, "
+                       "relative L2 residual 1e-8" if mode == 1 else "FP64 multigrid",
+                       "l2": "inputs larger than L2 (particle arrays 8.4 GB/species)",
+                       "sort_every": 10, "mcc_every": 10, "tile": args.tile},
+            "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()},
+            "poisson_compare": pois,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "k_push_deposit (both species, incl. accumulator clears)",
+                         "traffic": (tpp * n_avg if tpp else None)},
+            "cpu_baseline": ({k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")} if cb else None),
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn + C.sizeof(capi.LepicPushStats)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=4)
+    ap.add_argument("--mode", type=int, default=1)
+    ap.add_argument("--tile", type=int, default=16)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--ppc", type=int, default=0, help="override particles per cell (profiling runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

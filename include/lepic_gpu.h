@@ -199,6 +199,12 @@ int lepic_gpu_set_grid(lepic_ctx *ctx, int32_t which, const double *in);
 int lepic_gpu_get_push_stats(lepic_ctx *ctx, lepic_push_stats *stats);
 int lepic_gpu_get_mcc_stats(lepic_ctx *ctx, lepic_mcc_stats *stats);
 
+/* Device pointer of one species' charge accumulator: (nx+3)*(ny+3) int64 node values, the
+ * deposited CIC weights in units of 2^-44 (the np grid before its FP64 scaling).  Summing
+ * these integers across ranks (e.g. an NCCL int64 all-reduce after lepic_gpu_push_deposit)
+ * is the multi-GPU form of calc_rho.f90:71-74 and is exact. */
+int lepic_gpu_deposit_grid(lepic_ctx *ctx, int32_t ptype, void **acc);
+
 /* Raw device pointers of one species' SoA arrays (for in-process tools and tests):
  * X, Y are uint32 fixed point in cell units with `shift` fractional bits, VX/VY/VZ float. */
 int lepic_gpu_particle_arrays(lepic_ctx *ctx, int32_t ptype, void **X, void **Y, void **VX,

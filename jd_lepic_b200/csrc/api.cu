@@ -52,6 +52,7 @@ static void free_all(lepic_ctx *c) {
         F(c->lev[l].e32); F(c->lev[l].r32);
     }
     F(c->partials);
+    F(c->cg_r); F(c->cg_p); F(c->cg_ap);
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
     F(c->dcnt);
     if (c->hcnt) cudaFreeHost(c->hcnt);
@@ -187,6 +188,10 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         LCUDA(cudaMemset(L.r32, 0, sizeof(float) * (L.nx + 1) * (L.ny + 1)));
     }
     LALLOC(c->partials, (size_t)c->num_sms * 32);
+    LALLOC(c->cg_r, nn); LALLOC(c->cg_p, nn); LALLOC(c->cg_ap, nn);
+    LCUDA(cudaMemset(c->cg_r, 0, sizeof(double) * nn));
+    LCUDA(cudaMemset(c->cg_p, 0, sizeof(double) * nn));
+    LCUDA(cudaMemset(c->cg_ap, 0, sizeof(double) * nn));
     // collision tables
     if (xs && xs->ncol > 0 && xs->npt > 1) {
         c->has_xs = true;
@@ -353,7 +358,8 @@ int particles_get(lepic_ctx *c, int sp, double *vxp, long long cap, long long *n
 struct LoadP {
     int nx, ny, S, ntype, profile;
     long long n;
-    uint32_t xload;            // x_load in fixed-point units
+    unsigned long long xload;  // x_load in fixed-point units (nx << S can be 2^32)
+    unsigned long long ylim;   // ny << S
     double n_peak, n_floor, sig2, xc, yc, dx, dy;
     const uint8_t *cellwall;
     uint32_t *X[LEPIC_MAXSP], *Y[LEPIC_MAXSP];
@@ -365,14 +371,13 @@ struct LoadP {
 
 __global__ void k_load(LoadP P) {
     const double pi = 3.141592653589793;
-    const uint32_t ylim = (uint32_t)((unsigned long long)P.ny << P.S);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P.n; i += (long long)gridDim.x * blockDim.x) {
         uint32_t X = 0, Y = 0;
         bool ok = false;
         for (uint32_t a = 0; a < 100000u && !ok; a++) {
             U4 r = philox4x32_10(U4{(uint32_t)i, a, 0x4C4F4144u, (uint32_t)(i >> 32)}, P.k0, P.k1);
-            X = (uint32_t)((unsigned long long)r.x * P.xload >> 32);
-            Y = (uint32_t)((unsigned long long)r.y * ylim >> 32);
+            X = (uint32_t)(((unsigned long long)r.x * P.xload) >> 32);
+            Y = (uint32_t)(((unsigned long long)r.y * P.ylim) >> 32);
             int ix = (int)(X >> P.S) + 1, iy = (int)(Y >> P.S) + 1;
             if (P.cellwall[ix + (long long)iy * (P.nx + 2)]) continue; // load_part.f90:115-116
             if (P.profile == 1) {
@@ -407,7 +412,9 @@ int particles_load(lepic_ctx *c, const lepic_load_spec *sp) {
     P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.ntype = g.ntype; P.profile = sp->profile; P.n = sp->n_samples;
     double xl = std::min(sp->x_load, g.dx * g.nx);
     if (xl <= 0) xl = g.dx * g.nx;
-    P.xload = (uint32_t)std::min<double>((double)((long long)g.nx << c->S), std::floor(xl / g.dx * (double)(1u << c->S)));
+    P.xload = (unsigned long long)std::min<double>((double)((long long)g.nx << c->S),
+                                                   std::floor(xl / g.dx * (double)(1u << c->S)));
+    P.ylim = (unsigned long long)g.ny << c->S;
     P.n_peak = sp->n_peak; P.n_floor = sp->n_floor; P.sig2 = sp->sigma * sp->sigma;
     P.xc = 0.5 * g.dx * g.nx; P.yc = 0.5 * g.dy * g.ny; P.dx = g.dx; P.dy = g.dy;
     P.cellwall = c->cellwall;
@@ -622,6 +629,12 @@ extern "C" int lepic_gpu_get_mcc_stats(lepic_ctx *c, lepic_mcc_stats *st) {
     for (int q = 0; q < LEPIC_MAXCOL; q++) st->n_coll[q] = (int64_t)c->hcnt->n_coll[q];
     st->n_overflow = (int64_t)c->hcnt->n_overflow;
     return r;
+}
+
+extern "C" int lepic_gpu_deposit_grid(lepic_ctx *c, int32_t ptype, void **acc) {
+    if (!c || !acc || ptype < 0 || ptype >= c->cfg.ntype) return LEPIC_EINVAL;
+    *acc = c->sp[ptype].acc;
+    return LEPIC_OK;
 }
 
 extern "C" int lepic_gpu_particle_arrays(lepic_ctx *c, int32_t ptype, void **X, void **Y, void **VX, void **VY,

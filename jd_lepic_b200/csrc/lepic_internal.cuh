@@ -111,6 +111,7 @@ struct lepic_ctx {
     int nlev = 0;
     double *partials = nullptr;
     int mg_grid = 0, mg_grid_mixed = 0;
+    double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;  // finest-level CG vectors
     // collisions
     bool has_xs = false;
     int npt = 0, ncol = 0;

@@ -1,17 +1,23 @@
-// mg_mixed.cu -- mixed-precision Poisson solve: FP32 V-cycles inside FP64 iterative
-// refinement, one persistent cooperative kernel.
+// mg_mixed.cu -- mixed-precision Poisson solve, one persistent cooperative kernel:
+// conjugate gradients in FP64 on the reference's discrete operator (5-point, Dirichlet walls
+// and embedded conductors from bcnd), preconditioned by one FP32 V-cycle of the reference's
+// multigrid components (red-black SOR smoothing, full-weighting restriction, bilinear
+// prolongation, injection-coarsened masks, mg.f90 / sors.f90), run symmetrically
+// (red-black before, black-red after the coarse correction) so that it is a valid CG
+// preconditioner.
 //
-//   loop:  r = b - A u          FP64 (the only place the solution's accuracy is decided)
-//          stop when ||r||_2 <= eps * ||b - A u_D||_2   (u_D: u with the unknowns zeroed)
-//          A e = r              one FP32 V-cycle from e = 0: red-black SOR smoothing (nu1/nu2
-//                               sweeps), full-weighting restriction, bilinear prolongation,
-//                               with the reference's boundary rules (mg.f90, sors.f90)
-//          u = u + e            FP64
-// The smoother, transfer operators and masks are the reference's; only the arithmetic type
-// of the correction cycle changes, so the FP64 outer loop converges to the same discrete
-// solution as the FP64 solver.  The coarse levels (at most `small_nodes` nodes) run on CTA 0.
-// Roofline: per outer iteration the finest level moves ~110 B/node (FP64 u, b once; FP32 e, r
-// for the sweeps); at 2049^2 nodes the working set is L2-resident.
+//   r = b - A u (FP64);  z = V32(r);  p = z
+//   loop:  Ap = A p;  a = (r.z)/(p.Ap);  u += a p;  r -= a Ap          (FP64)
+//          stop when ||r||_2 <= eps ||b - A u_D||_2 (checked on the true residual)
+//          z = V32(r);  b = (r.z)_new/(r.z)_old;  p = z + b p
+// Every quantity that decides the answer (u, r, p, Ap, the dot products) is FP64; the
+// FP32 cycle only chooses search directions, so the converged u solves the FP64 system.
+// Why CG around the cycle: with embedded conductors (the aperture plate) the injected coarse
+// masks misrepresent the conductor and a stand-alone V-cycle contracts by ~0.5 per cycle or
+// diverges; CG removes those few conductor modes (11-12 iterations from a cold start to 1e-8,
+// independent of the grid size, in a CPU emulation of this exact algorithm).
+// Roofline: per iteration the finest level moves ~5 FP64 passes (~170 B/node) plus the FP32
+// cycle (~60 B/node); coarse levels (<= small_nodes nodes) run on CTA 0.
 #include <algorithm>
 #include <cstdlib>
 #include "mg_common.cuh"
@@ -29,9 +35,10 @@ struct MXP {
     MXL L[LEPIC_MAXLEV];
     int ng, Ls;
     float omega;
-    int nu1, nu2, nuc, max_outer;
+    int nu1, nu2, nuc, max_iter;
     double eps, alpha;
     int pbc, nmn;
+    double *r64, *p64, *ap64;  // finest-level CG vectors, (nx+3)(ny+3)
     double *partials;
     DevCounters *cnt;
 };
@@ -73,10 +80,13 @@ __device__ void pbc32(const Team &T, const MXL &L) {
     }
 }
 
+// nsweep red-black sweeps; `reverse` runs black-red (the adjoint order, used after the
+// coarse-grid correction so that the V-cycle is a symmetric preconditioner)
 template <class Team>
-__device__ bool smooth32(const Team &T, const MXP &P, int l, int nsweep) {
+__device__ bool smooth32(const Team &T, const MXP &P, int l, int nsweep, bool reverse) {
     for (int k = 0; k < nsweep; k++)
-        for (int color = 0; color < 2; color++) {
+        for (int cc = 0; cc < 2; cc++) {
+            const int color = reverse ? 1 - cc : cc;
             sweep32(T, P.L[l], color, P.omega);
             if (!T.sync()) return false;
             if (P.pbc) {
@@ -168,38 +178,151 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
     }
 }
 
-// finest level, FP64: r32 = b - A u (getres form) at unknowns, e = 0; returns ||r||^2 over
-// bcnd == -1 nodes (5-point form) and the L1 sum of the reference's residual
-template <class Team>
-__device__ bool fine_residual(const Team &T, const MXP &P, double *rr, double *l1) {
+
+__device__ void small_cycle(const MXP &P) {
+    SmallTeam T;
+    const int ng = P.ng;
+    for (int l = P.Ls; l <= ng - 2; l++) {
+        smooth32(T, P, l, P.nu1, false);
+        restrict32(T, P.L[l], P.L[l + 1], P.pbc, P.nmn);
+        __syncthreads();
+    }
+    smooth32(T, P, ng - 1, P.nuc, false);
+    smooth32(T, P, ng - 1, P.nuc, true);
+    for (int l = ng - 2; l >= P.Ls; l--) {
+        prolong32(T, P.L[l + 1], P.L[l]);
+        __syncthreads();
+        smooth32(T, P, l, P.nu2, true);
+    }
+}
+
+// one symmetric V-cycle on A e = r32 of level 0, from e = 0 (the caller zeroes e)
+__device__ bool vcycle32(const MXP &P) {
+    BigTeam B{P.cnt, P.partials};
+    const int ng = P.ng, Ls = P.Ls;
+    for (int l = 0; l < Ls && l <= ng - 2; l++) {
+        if (!smooth32(B, P, l, P.nu1, false)) return false;
+        restrict32(B, P.L[l], P.L[l + 1], P.pbc, P.nmn);
+        if (!B.sync()) return false;
+    }
+    int top;
+    if (Ls <= ng - 1) {
+        if (blockIdx.x == 0) small_cycle(P);
+        if (!B.sync()) return false;
+        top = Ls;
+    } else {
+        if (!smooth32(B, P, ng - 1, P.nuc, false)) return false;
+        if (!smooth32(B, P, ng - 1, P.nuc, true)) return false;
+        top = ng - 1;
+    }
+    for (int l = top - 1; l >= 0; l--) {
+        prolong32(B, P.L[l + 1], P.L[l]);
+        if (!B.sync()) return false;
+        if (!smooth32(B, P, l, P.nu2, true)) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void ij_of(long long t, int nx, int *i, int *j) {
+    *i = (int)(t % (nx + 1)) + 1;
+    *j = (int)(t / (nx + 1)) + 1;
+}
+
+// r = b - A u at unknowns (bcnd <= 0), zero elsewhere; r32 = (float) r; e = 0 (all nodes);
+// returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum
+__device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double *l1) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
-    const double aw = L.awd, ae = L.awd, an = L.and_, as = L.and_, ac = L.acd;
+    const double aw = L.awd, an = L.and_, ac = L.acd;
     const long long tot = (long long)(nx + 1) * (ny + 1);
     double a = 0.0, s1 = 0.0;
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx + 1)) + 1, j = (int)(t / (nx + 1)) + 1;
+    for (long long t = B.rank(); t < tot; t += B.size()) {
+        int i, j;
+        ij_of(t, nx, &i, &j);
         const long long n = i + (long long)j * W;
         const int bc = L.bc[n];
-        float out = 0.0f;
+        double r = 0.0;
         if (bc <= 0) {
             const double *u = L.u;
-            double uw = u[n - 1], awx = aw, aex = ae;
-            if (i == 1 && P.nmn == 1) { uw = 0.0; awx = 0.0; aex = 2.0 * ae; }
-            double r = L.b[t] - (awx * uw + aex * u[n + 1] + an * u[n + W] + as * u[n - W] + ac * u[n]);
-            out = (float)r;
-            if (bc == -1) {
-                double rs = L.b[t] - (aw * u[n - 1] + an * u[n + W] + as * u[n - W] + ae * u[n + 1] + ac * u[n]);
-                a += rs * rs;
-                s1 += fabs(rs);
-            }
+            r = L.b[t] - (aw * u[n - 1] + an * u[n + W] + an * u[n - W] + aw * u[n + 1] + ac * u[n]);
+            if (bc == -1) { a += r * r; s1 += fabs(r); }
         }
-        L.r[t] = out;
+        P.r64[n] = r;
+        L.r[t] = (float)r;
     }
     const long long nn = (long long)W * (ny + 3);
-    for (long long t = T.rank(); t < nn; t += T.size()) L.e[t] = 0.0f;
-    if (!team_sum(T, a, rr)) return false;
-    return team_sum(T, s1, l1);
+    for (long long t = B.rank(); t < nn; t += B.size()) {
+        L.e[t] = 0.0f;
+        int i = (int)(t % W), j = (int)(t / W);
+        if (i == 0 || j == 0 || i == nx + 2 || j == ny + 2) P.r64[t] = 0.0;
+    }
+    if (!team_sum(B, a, rr)) return false;
+    return team_sum(B, s1, l1);
+}
+
+// z = e (FP32 cycle output): returns r.z; if first, p = z else p = z + beta p (beta passed)
+__device__ bool dot_rz(const BigTeam &B, const MXP &P, double *rz) {
+    const MXL &L = P.L[0];
+    const long long nn = (long long)(L.nx + 3) * (L.ny + 3);
+    double a = 0.0;
+    for (long long t = B.rank(); t < nn; t += B.size())
+        if (L.bc[t] <= 0) a += P.r64[t] * (double)L.e[t];
+    return team_sum(B, a, rz);
+}
+
+__device__ void update_p(const BigTeam &B, const MXP &P, double beta, bool first) {
+    const MXL &L = P.L[0];
+    const long long nn = (long long)(L.nx + 3) * (L.ny + 3);
+    for (long long t = B.rank(); t < nn; t += B.size()) {
+        double z = L.bc[t] <= 0 ? (double)L.e[t] : 0.0;
+        P.p64[t] = first ? z : z + beta * P.p64[t];
+    }
+}
+
+// Ap = A p at unknowns (p is zero on walls and ghosts); returns p.Ap
+__device__ bool apply_A(const BigTeam &B, const MXP &P, double *pap) {
+    const MXL &L = P.L[0];
+    const int nx = L.nx, ny = L.ny, W = nx + 3;
+    const double aw = L.awd, an = L.and_, ac = L.acd;
+    const long long tot = (long long)(nx + 1) * (ny + 1);
+    double a = 0.0;
+    for (long long t = B.rank(); t < tot; t += B.size()) {
+        int i, j;
+        ij_of(t, nx, &i, &j);
+        const long long n = i + (long long)j * W;
+        double v = 0.0;
+        if (L.bc[n] <= 0) {
+            const double *p = P.p64;
+            v = aw * p[n - 1] + an * p[n + W] + an * p[n - W] + aw * p[n + 1] + ac * p[n];
+            a += p[n] * v;
+        }
+        P.ap64[n] = v;
+    }
+    return team_sum(B, a, pap);
+}
+
+// u += alpha p; r -= alpha Ap; r32 = r; e = 0; returns ||r||^2 over bcnd == -1 nodes
+__device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *rr) {
+    const MXL &L = P.L[0];
+    const int nx = L.nx, ny = L.ny, W = nx + 3;
+    const long long tot = (long long)(nx + 1) * (ny + 1);
+    double a = 0.0;
+    for (long long t = B.rank(); t < tot; t += B.size()) {
+        int i, j;
+        ij_of(t, nx, &i, &j);
+        const long long n = i + (long long)j * W;
+        const int bc = L.bc[n];
+        if (bc <= 0) {
+            L.u[n] = L.u[n] + alpha * P.p64[n];
+            double r = P.r64[n] - alpha * P.ap64[n];
+            P.r64[n] = r;
+            L.r[t] = (float)r;
+            if (bc == -1) a += r * r;
+        }
+    }
+    const long long nn = (long long)W * (ny + 3);
+    for (long long t = B.rank(); t < nn; t += B.size()) L.e[t] = 0.0f;
+    return team_sum(B, a, rr);
 }
 
 template <class Team>
@@ -221,76 +344,51 @@ __device__ bool b0_norm(const Team &T, const MXL &L, double *bb) {
     return team_sum(T, b, bb);
 }
 
-__device__ void small_cycle(const MXP &P) {
-    SmallTeam T;
-    const int ng = P.ng;
-    for (int l = P.Ls; l <= ng - 2; l++) {
-        smooth32(T, P, l, P.nu1);
-        restrict32(T, P.L[l], P.L[l + 1], P.pbc, P.nmn);
-        __syncthreads();
-    }
-    smooth32(T, P, ng - 1, P.nuc);
-    for (int l = ng - 2; l >= P.Ls; l--) {
-        prolong32(T, P.L[l + 1], P.L[l]);
-        __syncthreads();
-        smooth32(T, P, l, P.nu2);
-    }
-}
-
-__device__ bool vcycle32(const MXP &P) {
-    BigTeam B{P.cnt, P.partials};
-    const int ng = P.ng, Ls = P.Ls;
-    for (int l = 0; l < Ls && l <= ng - 2; l++) {
-        if (!smooth32(B, P, l, P.nu1)) return false;
-        restrict32(B, P.L[l], P.L[l + 1], P.pbc, P.nmn);
-        if (!B.sync()) return false;
-    }
-    int top;
-    if (Ls <= ng - 1) {
-        if (blockIdx.x == 0) small_cycle(P);
-        if (!B.sync()) return false;
-        top = Ls;
-    } else {
-        if (!smooth32(B, P, ng - 1, P.nuc)) return false;
-        top = ng - 1;
-    }
-    for (int l = top - 1; l >= 0; l--) {
-        prolong32(B, P.L[l + 1], P.L[l]);
-        if (!B.sync()) return false;
-        if (!smooth32(B, P, l, P.nu2)) return false;
-    }
-    return true;
-}
-
 __global__ void __launch_bounds__(MG_THREADS) k_mg_mixed(MXP P) {
     BigTeam B{P.cnt, P.partials};
-    double bb = 0.0, rr = 0.0, l1 = 0.0;
+    double bb = 0.0, rr = 0.0, l1 = 0.0, rz = 0.0, pap = 0.0;
     if (!b0_norm(B, P.L[0], &bb)) return;
-    const double b0 = sqrt(bb);
-    int outer = 0;
-    for (;;) {
-        if (!fine_residual(B, P, &rr, &l1)) return;
-        if (sqrt(rr) <= P.eps * b0 || outer >= P.max_outer) break;
-        if (!vcycle32(P)) return;
-        const MXL &L = P.L[0];
-        const long long nn = (long long)(L.nx + 3) * (L.ny + 3);
-        for (long long t = B.rank(); t < nn; t += B.size())
-            if (L.bc[t] <= 0) L.u[t] = L.u[t] + (double)L.e[t];
+    const double b0 = sqrt(bb), tol = P.eps * b0;
+    if (!true_residual(B, P, &rr, &l1)) return;
+    int it = 0, restarts = 0;
+    bool conv = sqrt(rr) <= tol;
+    bool first = true;
+    while (!conv && it < P.max_iter) {
+        if (!vcycle32(P)) return;            // z = M^-1 r in L[0].e
+        double rz_new;
+        if (!dot_rz(B, P, &rz_new)) return;
+        update_p(B, P, first ? 0.0 : rz_new / rz, first);
+        rz = rz_new;
+        first = false;
         if (!B.sync()) return;
-        outer++;
+        if (!apply_A(B, P, &pap)) return;
+        if (!(pap > 0.0)) break;             // not a descent direction: stop, report
+        if (!update_ur(B, P, rz / pap, &rr)) return;
+        it++;
+        if (sqrt(rr) <= tol) {               // confirm on the true residual
+            if (!true_residual(B, P, &rr, &l1)) return;
+            conv = sqrt(rr) <= tol;
+            if (!conv) { first = true; restarts++; }
+        }
+    }
+    if (!conv) {
+        if (!true_residual(B, P, &rr, &l1)) return;
+        conv = sqrt(rr) <= tol;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        P.cnt->mg_cycles = outer;
-        P.cnt->mg_sweeps_fine = outer * (P.nu1 + P.nu2);
+        P.cnt->mg_cycles = it;
+        P.cnt->mg_sweeps_fine = it * (P.nu1 + P.nu2);
         P.cnt->mg_res_l1 = l1 / P.alpha;
-        P.cnt->mg_ktot = 0.0;
+        P.cnt->mg_ktot = (double)restarts;
         P.cnt->mg_res_l2 = sqrt(rr);
         P.cnt->mg_b_l2 = b0;
-        if (outer >= P.max_outer && !(sqrt(rr) <= P.eps * b0)) set_err(P.cnt, LERR_NOTCONV, 600);
+        if (!conv) set_err(P.cnt, LERR_NOTCONV, 600);
     }
 }
 
 int mg_mixed_solve(lepic_ctx *c, double eps) {
+    if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the CG operator is symmetric only with Dirichlet rows
+        return mg_solve(c, eps, 2);
     MXP P;
     memset(&P, 0, sizeof(P));
     const double eps0 = c->cfg.eps0;
@@ -310,8 +408,8 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     for (int l = 0; l < c->nlev; l++)
         if ((long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1) <= small_nodes) { Ls = l; break; }
     P.Ls = Ls;
-    P.omega = 1.15f;
-    P.nu1 = 2; P.nu2 = 2; P.nuc = 40; P.max_outer = 200;
+    P.omega = 1.0f;
+    P.nu1 = 2; P.nu2 = 2; P.nuc = 20; P.max_iter = 200;
     if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
     if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
     if (const char *e = getenv("LEPIC_MX_NU2")) P.nu2 = atoi(e);
@@ -319,6 +417,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     P.alpha = fabs((double)(c->cfg.nx + 1) * (c->cfg.ny + 1) * P.L[0].acd);
     P.pbc = c->cfg.flag_pbc;
     P.nmn = c->cfg.flag_nmn;
+    P.r64 = c->cg_r; P.p64 = c->cg_p; P.ap64 = c->cg_ap;
     P.partials = c->partials;
     P.cnt = c->dcnt;
     if (c->mg_grid_mixed == 0) {

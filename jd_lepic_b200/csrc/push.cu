@@ -43,34 +43,156 @@ struct PushP {
     long long xlim, ylim;      // nx<<S, ny<<S
 };
 
-__device__ __forceinline__ void deposit(const PushP &P, unsigned long long *win, int ox, int oy,
-                                        bool use_win, uint32_t X, uint32_t Y) {
+// CIC deposit of one particle per lane, aggregated per cell inside the warp: lanes whose
+// particles share a cell (the usual case after the sort) sum their four integer weights with
+// two exact 32-bit warp reductions each (22-bit halves: 32 lanes x 2^22 < 2^32), and one lane
+// issues the four atomics.  Must be called by all 32 lanes of the warp.
+__device__ __forceinline__ void deposit_warp(const PushP &P, unsigned long long *win, int ox, int oy,
+                                             bool use_win, bool have, uint32_t X, uint32_t Y) {
+    const int ix = (int)(X >> P.S) + 1, iy = (int)(Y >> P.S) + 1; // INT(x/h)+1, x >= 0
+    const int key = have ? ix + iy * P.W : -1;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (key < 0) return;
     const uint32_t mask = (1u << P.S) - 1u;
     const uint64_t A = 1ull << P.S;
     const uint64_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
-    uint64_t w00 = ax * ay, w10 = fx * ay, w11 = fx * fy, w01 = ax * fy;
+    uint64_t w[4] = {ax * ay, fx * ay, fx * fy, ax * fy}; // (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1)
     const int sh = 2 * P.S - LEPIC_DEP_SHIFT;
-    if (sh > 0) {
-        const uint64_t half = 1ull << (sh - 1);
-        w00 = (w00 + half) >> sh; w10 = (w10 + half) >> sh; w11 = (w11 + half) >> sh; w01 = (w01 + half) >> sh;
-    } else if (sh < 0) {
-        w00 <<= -sh; w10 <<= -sh; w11 <<= -sh; w01 <<= -sh;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (sh > 0) w[k] = (w[k] + (1ull << (sh - 1))) >> sh;
+        else if (sh < 0) w[k] <<= -sh;
     }
-    const int ix = (int)(X >> P.S) + 1, iy = (int)(Y >> P.S) + 1; // INT(x/h)+1, x >= 0
+    if (__popc(grp) > 1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const unsigned lo = __reduce_add_sync(grp, (unsigned)(w[k] & 0x3FFFFFull));
+            const unsigned hi = __reduce_add_sync(grp, (unsigned)(w[k] >> 22));
+            w[k] = ((uint64_t)hi << 22) + lo;
+        }
+        if ((int)(threadIdx.x & 31) != __ffs(grp) - 1) return;
+    }
     const int lx = ix - ox, ly = iy - oy;
+    unsigned long long *q;
+    int row;
     if (use_win && lx >= 0 && lx + 1 < P.WX && ly >= 0 && ly + 1 < P.WY) {
-        unsigned long long *q = win + lx + ly * P.WX;
-        if (w00) atomicAdd(q, (unsigned long long)w00);
-        if (w10) atomicAdd(q + 1, (unsigned long long)w10);
-        if (w11) atomicAdd(q + P.WX + 1, (unsigned long long)w11);
-        if (w01) atomicAdd(q + P.WX, (unsigned long long)w01);
+        q = win + lx + ly * P.WX;
+        row = P.WX;
     } else {
-        unsigned long long *q = P.acc + ix + (long long)iy * P.W;
-        if (w00) atomicAdd(q, (unsigned long long)w00);
-        if (w10) atomicAdd(q + 1, (unsigned long long)w10);
-        if (w11) atomicAdd(q + P.W + 1, (unsigned long long)w11);
-        if (w01) atomicAdd(q + P.W, (unsigned long long)w01);
+        q = P.acc + ix + (long long)iy * P.W;
+        row = P.W;
     }
+    if (w[0]) atomicAdd(q, (unsigned long long)w[0]);
+    if (w[1]) atomicAdd(q + 1, (unsigned long long)w[1]);
+    if (w[2]) atomicAdd(q + row + 1, (unsigned long long)w[2]);
+    if (w[3]) atomicAdd(q + row, (unsigned long long)w[3]);
+}
+
+// part_mover for one slot; returns false for a hole or a particle lost in this step
+__device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt, uint32_t *Xo, uint32_t *Yo,
+                                         unsigned int *lost) {
+    const uint32_t mask = (1u << P.S) - 1u;
+    const float inv2S = 1.0f / (float)(1u << P.S);
+    float vx = P.VX[i];
+    if (isnan(vx)) return false; // hole
+    uint32_t X = P.X[i], Y = P.Y[i];
+    *Xo = X;
+    *Yo = Y;
+    if (!P.move) return true;
+    float vy = P.VY[i], vz = P.VZ[i];
+    // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
+    const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
+    const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
+    const float px = 1.0f - fx, py = 1.0f - fy;
+    const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
+    const long long n00 = (cx + 1) + (long long)(cy + 1) * P.W;
+    const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
+    const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
+    const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
+    const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
+    bool mag = false;
+    float Bx = 0.f, By = 0.f, Bz = 0.f;
+    if (P.bmode == 1) {
+        mag = true; Bx = P.Bcx; By = P.Bcy; Bz = P.Bcz;
+    } else if (P.bmode == 2) {
+        const float4 b00 = __ldg(P.B + n00);
+        if (b00.w > 1.e-5f) {
+            const float4 b10 = __ldg(P.B + n00 + 1), b11 = __ldg(P.B + n00 + P.W + 1);
+            const float4 b01 = __ldg(P.B + n00 + P.W);
+            Bx = k00 * b00.x + k10 * b10.x + k11 * b11.x + k01 * b01.x;
+            By = k00 * b00.y + k10 * b10.y + k11 * b11.y + k01 * b01.y;
+            Bz = k00 * b00.z + k10 * b10.z + k11 * b11.z + k01 * b01.z;
+            mag = true;
+        }
+    }
+    const float k1 = P.k1;
+    if (mag) { // Boris, part_expmover.f90:187-206
+        const float Bt2 = Bx * Bx + By * By + Bz * Bz;
+        const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+        const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz;
+        const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
+        const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
+        const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
+        vx = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
+        vy = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
+        vz = v1z + k2 * (v3x * By - v3y * Bx);
+    } else { // leap-frog, :210-211
+        vx = vx + 2.0f * k1 * Ex;
+        vy = vy + 2.0f * k1 * Ey;
+    }
+    // a non-finite velocity (a non-finite field) is an error: the particle is removed
+    if (!(fabsf(vx) <= 3.0e8f && fabsf(vy) <= 3.0e8f && fabsf(vz) <= 3.0e8f)) {
+        set_err(cnt, LERR_RANGE, 101);
+        (*lost)++;
+        P.VX[i] = __int_as_float(0x7fc00000);
+        return false;
+    }
+    // move (:216-217): integer part plus an unbiased stochastic rounding of the
+    // fractional part of the displacement in fixed-point units
+    const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u ^ P.step_key);
+    const float ux = (float)(h >> 8) * (1.0f / 16777216.0f);
+    const float uy = (float)(mix32(h ^ 0x7F4A7C15u) >> 8) * (1.0f / 16777216.0f);
+    const float ddx = vx * P.cdx, ddy = vy * P.cdy;
+    const float fdx = floorf(ddx), fdy = floorf(ddy);
+    long long Xn = (long long)X + (long long)fdx + ((ux < ddx - fdx) ? 1 : 0);
+    long long Yn = (long long)Y + (long long)fdy + ((uy < ddy - fdy) ? 1 : 0);
+    if (P.pbc) { // :222-241
+        const long long Ym = P.ylim;
+        long long k4 = Yn / Ym; // INT: truncation toward zero
+        if (Yn >= Ym) {
+            if (P.spec == 0) Yn = Yn - k4 * Ym;
+            else { Yn = (k4 + 1) * Ym - Yn; vy = -vy; }
+        }
+        if (Yn <= 0) {
+            if (P.spec == 0) Yn = (1 - k4) * Ym + Yn;
+            else { Yn = k4 * Ym - Yn; vy = -vy; }
+            if (Yn >= Ym) Yn = 0; // y = ymax exactly is kept as y = 0
+        }
+    }
+    // FLOOR cell + check_outofbounds + four-corner wall test (:244-258)
+    int ixn = (int)(Xn >> P.S) + 1, iyn = (int)(Yn >> P.S) + 1;
+    ixn = min(max(ixn, 0), P.nx + 1);
+    iyn = min(max(iyn, 0), P.ny + 1);
+    bool is_lost = P.cellwall[ixn + (long long)iyn * (P.nx + 2)] != 0;
+    if (!is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
+    if (is_lost) {
+        (*lost)++;
+        P.VX[i] = __int_as_float(0x7fc00000); // the slot becomes a hole
+        return false;
+    }
+    if (P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
+    if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
+        set_err(cnt, LERR_RANGE, 100);
+        Xn = min(max(Xn, 0ll), P.xlim - 1);
+        Yn = min(max(Yn, 0ll), P.ylim - 1);
+    }
+    X = (uint32_t)Xn;
+    Y = (uint32_t)Yn;
+    P.X[i] = X; P.Y[i] = Y;
+    P.VX[i] = vx; P.VY[i] = vy; P.VZ[i] = vz;
+    *Xo = X;
+    *Yo = Y;
+    return true;
 }
 
 __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
@@ -80,8 +202,6 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
     DevCounters *cnt = P.cnt;
     const long long n_slots = cnt->n_slots[P.sp], n_sorted = cnt->n_sorted[P.sp];
     const int n_items = cnt->n_items[P.sp];
-    const uint32_t mask = (1u << P.S) - 1u;
-    const float inv2S = 1.0f / (float)(1u << P.S);
     for (;;) {
         if (threadIdx.x == 0) {
             unsigned int w = atomicAdd(&cnt->work_next[P.sp], 1u);
@@ -108,94 +228,11 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
         }
         __syncthreads();
         unsigned int lost = 0;
-        for (int i = s_start + threadIdx.x; i < s_end; i += blockDim.x) {
-            float vx = P.VX[i];
-            if (isnan(vx)) continue; // hole
-            uint32_t X = P.X[i], Y = P.Y[i];
-            if (P.move) {
-                float vy = P.VY[i], vz = P.VZ[i];
-                // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
-                const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
-                const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
-                const float px = 1.0f - fx, py = 1.0f - fy;
-                const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
-                const long long n00 = (cx + 1) + (long long)(cy + 1) * P.W;
-                const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
-                const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
-                const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
-                const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
-                bool mag = false;
-                float Bx = 0.f, By = 0.f, Bz = 0.f;
-                if (P.bmode == 1) {
-                    mag = true; Bx = P.Bcx; By = P.Bcy; Bz = P.Bcz;
-                } else if (P.bmode == 2) {
-                    const float4 b00 = __ldg(P.B + n00);
-                    if (b00.w > 1.e-5f) {
-                        const float4 b10 = __ldg(P.B + n00 + 1), b11 = __ldg(P.B + n00 + P.W + 1);
-                        const float4 b01 = __ldg(P.B + n00 + P.W);
-                        Bx = k00 * b00.x + k10 * b10.x + k11 * b11.x + k01 * b01.x;
-                        By = k00 * b00.y + k10 * b10.y + k11 * b11.y + k01 * b01.y;
-                        Bz = k00 * b00.z + k10 * b10.z + k11 * b11.z + k01 * b01.z;
-                        mag = true;
-                    }
-                }
-                const float k1 = P.k1;
-                if (mag) { // Boris, part_expmover.f90:187-206
-                    const float Bt2 = Bx * Bx + By * By + Bz * Bz;
-                    const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
-                    const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz;
-                    const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
-                    const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
-                    const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
-                    vx = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
-                    vy = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
-                    vz = v1z + k2 * (v3x * By - v3y * Bx);
-                } else { // leap-frog, :210-211
-                    vx = vx + 2.0f * k1 * Ex;
-                    vy = vy + 2.0f * k1 * Ey;
-                }
-                // move (:216-217) with unbiased stochastic rounding of the sub-unit part
-                const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u ^ P.step_key);
-                const float ux = (float)(h >> 8) * (1.0f / 16777216.0f);
-                const float uy = (float)(mix32(h ^ 0x7F4A7C15u) >> 8) * (1.0f / 16777216.0f);
-                long long Xn = (long long)X + __float2ll_rd(vx * P.cdx + ux);
-                long long Yn = (long long)Y + __float2ll_rd(vy * P.cdy + uy);
-                if (P.pbc) { // :222-241
-                    const long long Ym = P.ylim;
-                    long long k4 = Yn / Ym; // INT: truncation toward zero
-                    if (Yn >= Ym) {
-                        if (P.spec == 0) Yn = Yn - k4 * Ym;
-                        else { Yn = (k4 + 1) * Ym - Yn; vy = -vy; }
-                    }
-                    if (Yn <= 0) {
-                        if (P.spec == 0) Yn = (1 - k4) * Ym + Yn;
-                        else { Yn = k4 * Ym - Yn; vy = -vy; }
-                        if (Yn >= Ym) Yn = 0; // y = ymax exactly is kept as y = 0
-                    }
-                }
-                // FLOOR cell + check_outofbounds + four-corner wall test (:244-258)
-                int ixn = (int)(Xn >> P.S) + 1, iyn = (int)(Yn >> P.S) + 1;
-                ixn = min(max(ixn, 0), P.nx + 1);
-                iyn = min(max(iyn, 0), P.ny + 1);
-                bool is_lost = P.cellwall[ixn + (long long)iyn * (P.nx + 2)] != 0;
-                if (!is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
-                if (is_lost) {
-                    lost++;
-                    P.VX[i] = __int_as_float(0x7fc00000); // the slot becomes a hole
-                    continue;
-                }
-                if (P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
-                if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
-                    set_err(cnt, LERR_RANGE, 100);
-                    Xn = min(max(Xn, 0ll), P.xlim - 1);
-                    Yn = min(max(Yn, 0ll), P.ylim - 1);
-                }
-                X = (uint32_t)Xn;
-                Y = (uint32_t)Yn;
-                P.X[i] = X; P.Y[i] = Y;
-                P.VX[i] = vx; P.VY[i] = vy; P.VZ[i] = vz;
-            }
-            deposit(P, win, ox, oy, use_win, X, Y);
+        for (int base = s_start; base < s_end; base += blockDim.x) { // uniform trip count
+            const int i = base + threadIdx.x;
+            uint32_t X = 0, Y = 0;
+            const bool have = (i < s_end) && move_one(P, i, cnt, &X, &Y, &lost);
+            deposit_warp(P, win, ox, oy, use_win, have, X, Y);
         }
         // lost-particle count: one atomic per warp, then per CTA
         for (int o = 16; o > 0; o >>= 1) lost += __shfl_xor_sync(0xffffffffu, lost, o);

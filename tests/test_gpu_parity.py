@@ -168,9 +168,9 @@ def test_mg_fp64_matches_oracle(gpu_lib, n, eps):
     s.close()
 
 
-@pytest.mark.parametrize("n", [64, 256])
-def test_mg_mixed_precision_reaches_1e8(gpu_lib, n):
-    case = configs.case2(ppc=2, nx=n, ny=n // 2)
+@pytest.mark.parametrize("idx,n", [(2, 64), (2, 256), (4, 256), (4, 512)])
+def test_mg_mixed_precision_reaches_1e8(gpu_lib, idx, n):
+    case = configs.case2(ppc=2, nx=n, ny=n // 2) if idx == 2 else configs.case4(ppc=2, nx=n, ny=n)
     s = sim_for(case)
     rhs = _perturbed_rhs(s, case)
     set_rhs(s, rhs)
