@@ -204,6 +204,10 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         LCUDA(cudaMemcpy(c->col_info, xs->col_info, sizeof(int) * xs->ncol * 10, cudaMemcpyHostToDevice));
         for (int s = 0; s < g.nsp; s++) {
             c->p_ncol[s] = xs->p_ncol[s];
+            if (xs->p_ncol[s] > 16 || xs->p_ncol[s] < 0) {
+                c->last_err = "more than 16 reactions for one incident species";
+                return LEPIC_EINVAL;
+            }
             for (int q = 0; q < xs->p_ncol[s]; q++) c->hsig_list[s * LEPIC_MAXCOL + q] = xs->sig_list[s * LEPIC_MAXCOL + q];
         }
         // collisions.f90:98-106 with neutral targets: nu_max = min(sum n_t*(sigma v)_max, nu_uplim)

@@ -23,6 +23,7 @@
 #include "lepic_internal.cuh"
 
 #define MCC_THREADS 256
+#define MCC_MAX_REACTIONS 16  // reactions per incident species (checked at context creation)
 
 struct MccP {
     int sp, ntype;
@@ -33,7 +34,7 @@ struct MccP {
     DevCounters *cnt;
     double Pmax, nu_max;
     int ncol_sp;
-    int cols[LEPIC_MAXCOL];
+    int cols[MCC_MAX_REACTIONS];
     const double *sig_Er;
     int npt;
     const double *sig;
@@ -103,7 +104,7 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     double tvx[LEPIC_MAXSP], tvy[LEPIC_MAXSP], tvz[LEPIC_MAXSP], mu[LEPIC_MAXSP], vr[LEPIC_MAXSP];
     double vcx[LEPIC_MAXSP], vcy[LEPIC_MAXSP], vcz[LEPIC_MAXSP];
     unsigned drawn = 0;
-    double nu[LEPIC_MAXCOL];
+    double nu[MCC_MAX_REACTIONS];
     double sum_nu = 0.0;
     for (int q = 0; q < P.ncol_sp; q++) {
         const int c = P.cols[q];
@@ -135,7 +136,7 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     }
     // :619 indexx: reactions ordered by ascending nu (straight insertion, stable); the order
     // decides the outcome when sum(nu) > 1, i.e. when nu_max was capped (main.f90:494-495)
-    int order[LEPIC_MAXCOL];
+    int order[MCC_MAX_REACTIONS];
     for (int q = 0; q < P.ncol_sp; q++) {
         int k = q;
         while (k > 0 && nu[order[k - 1]] > nu[q]) { order[k] = order[k - 1]; k--; }

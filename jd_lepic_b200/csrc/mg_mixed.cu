@@ -362,8 +362,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_mixed(MXP P) {
         first = false;
         if (!B.sync()) return;
         if (!apply_A(B, P, &pap)) return;
-        if (!(pap > 0.0)) break;             // not a descent direction: stop, report
-        if (!update_ur(B, P, rz / pap, &rr)) return;
+        // A (eps0 * Laplacian, diagonal -4a) and the V-cycle are both negative definite, so
+        // r.z and p.Ap are both negative and the step length is positive
+        const double alpha = rz / pap;
+        if (!(alpha > 0.0) || !isfinite(alpha)) break; // no descent: stop and report
+        if (!update_ur(B, P, alpha, &rr)) return;
         it++;
         if (sqrt(rr) <= tol) {               // confirm on the true residual
             if (!true_residual(B, P, &rr, &l1)) return;
