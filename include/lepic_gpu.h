@@ -205,6 +205,25 @@ int lepic_gpu_get_mcc_stats(lepic_ctx *ctx, lepic_mcc_stats *stats);
  * is the multi-GPU form of calc_rho.f90:71-74 and is exact. */
 int lepic_gpu_deposit_grid(lepic_ctx *ctx, int32_t ptype, void **acc);
 
+/* Charge deposition that allocates no device memory.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc -- a host whose device memory is reserved up front
+ * and handed out by its own (or another framework's) allocator, or code where the implicit
+ * synchronisation of an allocation is not allowed.  The caller passes device pointers it
+ * owns: X, Y (n fixed-point positions with `shift` fractional bits, as
+ * lepic_gpu_particle_arrays returns them), VX (may be NULL; NaN marks a hole), kq
+ * ((nx+3)*(ny+3) node factors), and np_out ((nx+3)*(ny+3) doubles) which receives
+ * np = kq * k1 * sum of CIC weights, k1 = Nm / (dx*dy*zmax) -- the np grid of
+ * charge_deposition (part_expmover.f90:520-610), identical to the context path.
+ * The temporary uint64 accumulator is a fixed static device array of 2^20 nodes (8 MiB) that
+ * every GPU loading the library keeps until exit; larger grids ((nx+3)*(ny+3) > 2^20) are
+ * rejected with LEPIC_ECAPACITY.  The first call on a device looks up that array's device
+ * address, so make it before any stream capture.  All calls on a device share the array and
+ * each call clears it first: calls that overlap on the GPU race and must be serialised by the
+ * caller.  stream is a cudaStream_t (NULL: the default stream); the call only enqueues work. */
+int lepic_gpu_deposit_noalloc(const uint32_t *X, const uint32_t *Y, const float *VX, int64_t n,
+                              int32_t nx, int32_t ny, int32_t shift, double k1, const double *kq,
+                              double *np_out, void *stream);
+
 /* Raw device pointers of one species' SoA arrays (for in-process tools and tests):
  * X, Y are uint32 fixed point in cell units with `shift` fractional bits, VX/VY/VZ float. */
 int lepic_gpu_particle_arrays(lepic_ctx *ctx, int32_t ptype, void **X, void **Y, void **VX,

@@ -146,6 +146,8 @@ PROTOTYPES = {
     "lepic_gpu_get_push_stats": (C.c_int, [_VP, C.POINTER(LepicPushStats)]),
     "lepic_gpu_get_mcc_stats": (C.c_int, [_VP, C.POINTER(LepicMccStats)]),
     "lepic_gpu_deposit_grid": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
+    "lepic_gpu_deposit_noalloc": (C.c_int, [_VP, _VP, _VP, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                            _VP, _VP, _VP]),
     "lepic_gpu_particle_arrays": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                             C.POINTER(_VP), C.POINTER(_VP), C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int32)]),

@@ -31,6 +31,7 @@ SOURCES = {
     "push.cu": [],
     "sort.cu": [],
     "mcc.cu": [],
+    "noalloc.cu": ["-fmad=false"],
 }
 
 
