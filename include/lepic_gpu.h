@@ -5,7 +5,7 @@
  *
  * The reference is F77-style Fortran with implicit interfaces (all arguments by reference,
  * global state in COMMON blocks).  Each entry point below names the reference routine it
- * replaces.  A Fortran host binds them with ISO_C_BINDING (see INTEGRATION.md) and keeps
+ * replaces.  A Fortran host binds them with ISO_C_BINDING and keeps
  * its decks, tables and call sites; device state stays resident between calls and host
  * arrays are exchanged only where a pointer argument is non-NULL.
  *
@@ -44,7 +44,8 @@ extern "C" {
 
 /* Poisson solve modes for lepic_gpu_iterative_solver */
 #define LEPIC_POISSON_FP64_MG 0   /* the reference's V-cycle (mg.f90) in FP64              */
-#define LEPIC_POISSON_MIXED_IR 1  /* FP32 V-cycles inside FP64 iterative refinement       */
+#define LEPIC_POISSON_MIXED_IR 1  /* FP64 CG preconditioned by an FP32 V-cycle            */
+#define LEPIC_POISSON_FP64_MG_L2 2 /* mode 0's V-cycles, stopped on the L2 relative residual */
 
 /* Grid selectors for lepic_gpu_get_grid / lepic_gpu_set_grid */
 #define LEPIC_GRID_PHI 0      /* phi(0:nx+2,0:ny+2)                     */

@@ -17,7 +17,8 @@
 // diverges; CG removes those few conductor modes (11-12 iterations from a cold start to 1e-8,
 // independent of the grid size, in a CPU emulation of this exact algorithm).
 // Roofline: per iteration the finest level moves ~5 FP64 passes (~170 B/node) plus the FP32
-// cycle (~60 B/node); coarse levels (<= small_nodes nodes) run on CTA 0.
+// cycle (~60 B/node); the coarsest levels that fit together in about 96 KB (e, r and mask)
+// run on CTA 0 out of its shared memory.
 #include <algorithm>
 #include <cstdlib>
 #include "mg_common.cuh"
@@ -41,6 +42,8 @@ struct MXP {
     double *r64, *p64, *ap64;  // finest-level CG vectors, (nx+3)(ny+3)
     double *partials;
     DevCounters *cnt;
+    int soff_e[LEPIC_MAXLEV], soff_r[LEPIC_MAXLEV], soff_b[LEPIC_MAXLEV]; // shared-memory copies
+    int smem_bytes;
 };
 
 template <class Team>
@@ -83,14 +86,14 @@ __device__ void pbc32(const Team &T, const MXL &L) {
 // nsweep red-black sweeps; `reverse` runs black-red (the adjoint order, used after the
 // coarse-grid correction so that the V-cycle is a symmetric preconditioner)
 template <class Team>
-__device__ bool smooth32(const Team &T, const MXP &P, int l, int nsweep, bool reverse) {
+__device__ bool smooth32(const Team &T, const MXP &P, const MXL &L, int nsweep, bool reverse) {
     for (int k = 0; k < nsweep; k++)
         for (int cc = 0; cc < 2; cc++) {
             const int color = reverse ? 1 - cc : cc;
-            sweep32(T, P.L[l], color, P.omega);
+            sweep32(T, L, color, P.omega);
             if (!T.sync()) return false;
             if (P.pbc) {
-                pbc32(T, P.L[l]);
+                pbc32(T, L);
                 if (!T.sync()) return false;
             }
         }
@@ -179,21 +182,58 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
 }
 
 
+// The coarse part of the cycle (levels >= Ls) on CTA 0, with every coarse level's e, r and
+// mask held in shared memory: the restricted r of level Ls comes in from global memory, the
+// correction e of level Ls goes back out, everything in between stays on chip.
+__device__ __forceinline__ MXL smem_level(const MXP &P, unsigned char *base, int l) {
+    MXL S = P.L[l];
+    S.e = (float *)(base + P.soff_e[l]);
+    S.r = (float *)(base + P.soff_r[l]);
+    S.bc = (const int8_t *)(base + P.soff_b[l]);
+    return S;
+}
+
 __device__ void small_cycle(const MXP &P) {
+    extern __shared__ __align__(16) unsigned char mx_smem[];
     SmallTeam T;
-    const int ng = P.ng;
-    for (int l = P.Ls; l <= ng - 2; l++) {
-        smooth32(T, P, l, P.nu1, false);
-        restrict32(T, P.L[l], P.L[l + 1], P.pbc, P.nmn);
+    const int ng = P.ng, Ls = P.Ls;
+    for (int l = Ls; l < ng; l++) {
+        const long long nn = (long long)(P.L[l].nx + 3) * (P.L[l].ny + 3);
+        int8_t *bcs = (int8_t *)(mx_smem + P.soff_b[l]);
+        const int8_t *bcg = P.L[l].bc;
+        for (long long t = threadIdx.x; t < nn; t += blockDim.x) bcs[t] = bcg[t];
+    }
+    {
+        const MXL S = smem_level(P, mx_smem, Ls);
+        const long long nr = (long long)(S.nx + 1) * (S.ny + 1);
+        const long long nn = (long long)(S.nx + 3) * (S.ny + 3);
+        const float *rg = P.L[Ls].r;
+        for (long long t = threadIdx.x; t < nr; t += blockDim.x) S.r[t] = rg[t];
+        for (long long t = threadIdx.x; t < nn; t += blockDim.x) S.e[t] = 0.0f;
+    }
+    __syncthreads();
+    for (int l = Ls; l <= ng - 2; l++) {
+        const MXL F = smem_level(P, mx_smem, l);
+        smooth32(T, P, F, P.nu1, false);
+        restrict32(T, F, smem_level(P, mx_smem, l + 1), P.pbc, P.nmn);
         __syncthreads();
     }
-    smooth32(T, P, ng - 1, P.nuc, false);
-    smooth32(T, P, ng - 1, P.nuc, true);
-    for (int l = ng - 2; l >= P.Ls; l--) {
-        prolong32(T, P.L[l + 1], P.L[l]);
-        __syncthreads();
-        smooth32(T, P, l, P.nu2, true);
+    {
+        const MXL S = smem_level(P, mx_smem, ng - 1);
+        smooth32(T, P, S, P.nuc, false);
+        smooth32(T, P, S, P.nuc, true);
     }
+    for (int l = ng - 2; l >= Ls; l--) {
+        const MXL F = smem_level(P, mx_smem, l);
+        prolong32(T, smem_level(P, mx_smem, l + 1), F);
+        __syncthreads();
+        smooth32(T, P, F, P.nu2, true);
+    }
+    const MXL S = smem_level(P, mx_smem, Ls);
+    const long long nn = (long long)(S.nx + 3) * (S.ny + 3);
+    float *eg = P.L[Ls].e;
+    for (long long t = threadIdx.x; t < nn; t += blockDim.x) eg[t] = S.e[t];
+    __syncthreads();
 }
 
 // one symmetric V-cycle on A e = r32 of level 0, from e = 0 (the caller zeroes e)
@@ -201,7 +241,7 @@ __device__ bool vcycle32(const MXP &P) {
     BigTeam B{P.cnt, P.partials};
     const int ng = P.ng, Ls = P.Ls;
     for (int l = 0; l < Ls && l <= ng - 2; l++) {
-        if (!smooth32(B, P, l, P.nu1, false)) return false;
+        if (!smooth32(B, P, P.L[l], P.nu1, false)) return false;
         restrict32(B, P.L[l], P.L[l + 1], P.pbc, P.nmn);
         if (!B.sync()) return false;
     }
@@ -211,14 +251,14 @@ __device__ bool vcycle32(const MXP &P) {
         if (!B.sync()) return false;
         top = Ls;
     } else {
-        if (!smooth32(B, P, ng - 1, P.nuc, false)) return false;
-        if (!smooth32(B, P, ng - 1, P.nuc, true)) return false;
+        if (!smooth32(B, P, P.L[ng - 1], P.nuc, false)) return false;
+        if (!smooth32(B, P, P.L[ng - 1], P.nuc, true)) return false;
         top = ng - 1;
     }
     for (int l = top - 1; l >= 0; l--) {
         prolong32(B, P.L[l + 1], P.L[l]);
         if (!B.sync()) return false;
-        if (!smooth32(B, P, l, P.nu2, true)) return false;
+        if (!smooth32(B, P, P.L[l], P.nu2, true)) return false;
     }
     return true;
 }
@@ -405,14 +445,35 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
         d.e = a.e32; d.r = a.r32; d.bc = a.bc; d.u = a.u; d.b = a.b;
     }
     P.ng = c->nlev;
-    long long small_nodes = 4500;
-    if (const char *e = getenv("LEPIC_MG_SMALL_NODES")) small_nodes = atoll(e);
+    // the coarsest levels whose e, r and mask fit together in CTA 0's shared-memory budget
+    // run on chip; the finer ones use the whole grid
+    long long budget = 96 * 1024;
+    if (const char *e = getenv("LEPIC_MX_SMEM")) budget = atoll(e);
+    auto level_bytes = [&](int l) {
+        const long long nn = (long long)(c->lev[l].nx + 3) * (c->lev[l].ny + 3);
+        const long long nr = (long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1);
+        return ((nn * 4 + 15) / 16) * 16 + ((nr * 4 + 15) / 16) * 16 + ((nn + 15) / 16) * 16;
+    };
     int Ls = c->nlev;
-    for (int l = 0; l < c->nlev; l++)
-        if ((long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1) <= small_nodes) { Ls = l; break; }
+    long long total = 0;
+    for (int l = c->nlev - 1; l >= 1; l--) {
+        if (total + level_bytes(l) > budget) break;
+        total += level_bytes(l);
+        Ls = l;
+    }
+    long long off = 0;
+    for (int l = Ls; l < c->nlev; l++) {
+        const long long nn = (long long)(c->lev[l].nx + 3) * (c->lev[l].ny + 3);
+        const long long nr = (long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1);
+        P.soff_e[l] = (int)off; off += ((nn * 4 + 15) / 16) * 16;
+        P.soff_r[l] = (int)off; off += ((nr * 4 + 15) / 16) * 16;
+        P.soff_b[l] = (int)off; off += ((nn + 15) / 16) * 16;
+    }
+    P.smem_bytes = (int)off;
     P.Ls = Ls;
     P.omega = 1.0f;
-    P.nu1 = 2; P.nu2 = 2; P.nuc = 20; P.max_iter = 200;
+    P.nu1 = 2; P.nu2 = 2; P.nuc = 8; P.max_iter = 200;
+    if (const char *e = getenv("LEPIC_MX_NUC")) P.nuc = atoi(e);
     if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
     if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
     if (const char *e = getenv("LEPIC_MX_NU2")) P.nu2 = atoi(e);
@@ -423,9 +484,11 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     P.r64 = c->cg_r; P.p64 = c->cg_p; P.ap64 = c->cg_ap;
     P.partials = c->partials;
     P.cnt = c->dcnt;
+    const size_t smem = (size_t)P.smem_bytes;
     if (c->mg_grid_mixed == 0) {
+        LCUDA(cudaFuncSetAttribute(k_mg_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         int occ = 0;
-        LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_mixed, MG_THREADS, 0));
+        LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_mixed, MG_THREADS, smem));
         if (occ < 1) { c->last_err = "mixed multigrid kernel does not fit on an SM"; return LEPIC_ECUDA; }
         int per_sm = 2;
         if (const char *e = getenv("LEPIC_MG_CTAS_PER_SM")) per_sm = atoi(e);
@@ -433,7 +496,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     }
     void *args[] = {&P};
     LCUDA(cudaMemsetAsync(&c->dcnt->bar_count, 0, 3 * sizeof(unsigned int), c->stream));
-    LCUDA(cudaLaunchCooperativeKernel((void *)k_mg_mixed, dim3(c->mg_grid_mixed), dim3(MG_THREADS), args, 0,
+    LCUDA(cudaLaunchCooperativeKernel((void *)k_mg_mixed, dim3(c->mg_grid_mixed), dim3(MG_THREADS), args, smem,
                                       c->stream));
     return LEPIC_OK;
 }

@@ -27,7 +27,6 @@ struct PushP {
     float *VX, *VY, *VZ;
     const float2 *E;
     const float4 *B;
-    int bmode;                 // 0 none, 1 constant, 2 map
     float Bcx, Bcy, Bcz;
     const uint8_t *cellwall;
     unsigned long long *acc;
@@ -39,7 +38,6 @@ struct PushP {
     int pbc, spec, nmn, negion_nmn;
     uint32_t step_key;
     int tw, th, ntx, M, WX, WY, win;
-    int move;
     long long xlim, ylim;      // nx<<S, ny<<S
 };
 
@@ -54,9 +52,10 @@ __device__ __forceinline__ void deposit_warp(const PushP &P, unsigned long long 
     const unsigned grp = __match_any_sync(0xffffffffu, key);
     if (key < 0) return;
     const uint32_t mask = (1u << P.S) - 1u;
-    const uint64_t A = 1ull << P.S;
-    const uint64_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
-    uint64_t w[4] = {ax * ay, fx * ay, fx * fy, ax * fy}; // (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1)
+    const uint32_t A = 1u << P.S;
+    const uint32_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
+    // (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1): 32x32 -> 64-bit products
+    uint64_t w[4] = {(uint64_t)ax * ay, (uint64_t)fx * ay, (uint64_t)fx * fy, (uint64_t)ax * fy};
     const int sh = 2 * P.S - LEPIC_DEP_SHIFT;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -88,33 +87,45 @@ __device__ __forceinline__ void deposit_warp(const PushP &P, unsigned long long 
     if (w[3]) atomicAdd(q + row, (unsigned long long)w[3]);
 }
 
-// part_mover for one slot; returns false for a hole or a particle lost in this step
-__device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt, uint32_t *Xo, uint32_t *Yo,
-                                         unsigned int *lost) {
+struct Part {
+    uint32_t X, Y;
+    float vx, vy, vz;
+};
+
+__device__ __forceinline__ void load_part(const PushP &P, int i, bool ok, Part &p) {
+    if (ok) {
+        p.vx = P.VX[i]; p.X = P.X[i]; p.Y = P.Y[i]; p.vy = P.VY[i]; p.vz = P.VZ[i];
+    } else {
+        p.vx = __int_as_float(0x7fc00000); p.X = 0; p.Y = 0; p.vy = 0.f; p.vz = 0.f;
+    }
+}
+
+// part_mover for one particle already in registers; returns false for a hole or a particle
+// lost in this step (the slot then becomes a hole).  BMODE: 0 no B, 1 constant, 2 map;
+// GEN: the periodic / specular / Neumann boundary options (off in the common deck).
+template <int BMODE, bool GEN>
+__device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCounters *cnt, unsigned int &lost) {
+    if (isnan(p.vx)) return false; // hole
     const uint32_t mask = (1u << P.S) - 1u;
     const float inv2S = 1.0f / (float)(1u << P.S);
-    float vx = P.VX[i];
-    if (isnan(vx)) return false; // hole
-    uint32_t X = P.X[i], Y = P.Y[i];
-    *Xo = X;
-    *Yo = Y;
-    if (!P.move) return true;
-    float vy = P.VY[i], vz = P.VZ[i];
+    uint32_t X = p.X, Y = p.Y;
+    float vx = p.vx, vy = p.vy, vz = p.vz;
     // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
     const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
     const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
     const float px = 1.0f - fx, py = 1.0f - fy;
     const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
-    const long long n00 = (cx + 1) + (long long)(cy + 1) * P.W;
+    const int n00 = (cx + 1) + (cy + 1) * P.W;
     const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
     const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
     const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
     const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
+    const float k1 = P.k1;
     bool mag = false;
     float Bx = 0.f, By = 0.f, Bz = 0.f;
-    if (P.bmode == 1) {
+    if (BMODE == 1) {
         mag = true; Bx = P.Bcx; By = P.Bcy; Bz = P.Bcz;
-    } else if (P.bmode == 2) {
+    } else if (BMODE == 2) {
         const float4 b00 = __ldg(P.B + n00);
         if (b00.w > 1.e-5f) {
             const float4 b10 = __ldg(P.B + n00 + 1), b11 = __ldg(P.B + n00 + P.W + 1);
@@ -125,7 +136,6 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt
             mag = true;
         }
     }
-    const float k1 = P.k1;
     if (mag) { // Boris, part_expmover.f90:187-206
         const float Bt2 = Bx * Bx + By * By + Bz * Bz;
         const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
@@ -143,20 +153,22 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt
     // a non-finite velocity (a non-finite field) is an error: the particle is removed
     if (!(fabsf(vx) <= 3.0e8f && fabsf(vy) <= 3.0e8f && fabsf(vz) <= 3.0e8f)) {
         set_err(cnt, LERR_RANGE, 101);
-        (*lost)++;
+        lost++;
         P.VX[i] = __int_as_float(0x7fc00000);
         return false;
     }
-    // move (:216-217): integer part plus an unbiased stochastic rounding of the
-    // fractional part of the displacement in fixed-point units
-    const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u ^ P.step_key);
-    const float ux = (float)(h >> 8) * (1.0f / 16777216.0f);
-    const float uy = (float)(mix32(h ^ 0x7F4A7C15u) >> 8) * (1.0f / 16777216.0f);
+    // move (:216-217): integer part plus an unbiased stochastic rounding of the fractional part
+    // of the displacement (16-bit uniforms from one integer hash of slot and step)
+    uint32_t h = (uint32_t)i * 0x9E3779B1u ^ P.step_key;
+    h = (h ^ (h >> 16)) * 0x7FEB352Du;
+    h ^= h >> 15;
+    const float ux = (float)(h & 0xFFFFu) * (1.0f / 65536.0f);
+    const float uy = (float)(h >> 16) * (1.0f / 65536.0f);
     const float ddx = vx * P.cdx, ddy = vy * P.cdy;
     const float fdx = floorf(ddx), fdy = floorf(ddy);
-    long long Xn = (long long)X + (long long)fdx + ((ux < ddx - fdx) ? 1 : 0);
-    long long Yn = (long long)Y + (long long)fdy + ((uy < ddy - fdy) ? 1 : 0);
-    if (P.pbc) { // :222-241
+    long long Xn = (long long)X + (long long)((int)fdx + ((ux < ddx - fdx) ? 1 : 0));
+    long long Yn = (long long)Y + (long long)((int)fdy + ((uy < ddy - fdy) ? 1 : 0));
+    if (GEN && P.pbc) { // :222-241
         const long long Ym = P.ylim;
         long long k4 = Yn / Ym; // INT: truncation toward zero
         if (Yn >= Ym) {
@@ -173,14 +185,14 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt
     int ixn = (int)(Xn >> P.S) + 1, iyn = (int)(Yn >> P.S) + 1;
     ixn = min(max(ixn, 0), P.nx + 1);
     iyn = min(max(iyn, 0), P.ny + 1);
-    bool is_lost = P.cellwall[ixn + (long long)iyn * (P.nx + 2)] != 0;
-    if (!is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
+    bool is_lost = P.cellwall[ixn + iyn * (P.nx + 2)] != 0;
+    if (GEN && !is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
     if (is_lost) {
-        (*lost)++;
+        lost++;
         P.VX[i] = __int_as_float(0x7fc00000); // the slot becomes a hole
         return false;
     }
-    if (P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
+    if (GEN && P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
     if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
         set_err(cnt, LERR_RANGE, 100);
         Xn = min(max(Xn, 0ll), P.xlim - 1);
@@ -190,11 +202,14 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, DevCounters *cnt
     Y = (uint32_t)Yn;
     P.X[i] = X; P.Y[i] = Y;
     P.VX[i] = vx; P.VY[i] = vy; P.VZ[i] = vz;
-    *Xo = X;
-    *Yo = Y;
+    p.X = X;
+    p.Y = Y;
     return true;
 }
 
+// Two particles per thread per iteration (two independent load -> push -> store chains in
+// flight), then the two warp-aggregated deposits.
+template <int BMODE, bool GEN, bool MOVE>
 __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
@@ -228,11 +243,22 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
         }
         __syncthreads();
         unsigned int lost = 0;
-        for (int base = s_start; base < s_end; base += blockDim.x) { // uniform trip count
-            const int i = base + threadIdx.x;
-            uint32_t X = 0, Y = 0;
-            const bool have = (i < s_end) && move_one(P, i, cnt, &X, &Y, &lost);
-            deposit_warp(P, win, ox, oy, use_win, have, X, Y);
+        const int end = s_end;
+        for (int base = s_start; base < end; base += 2 * PUSH_THREADS) { // uniform trip count
+            const int i0 = base + threadIdx.x, i1 = i0 + PUSH_THREADS;
+            Part p0, p1;
+            load_part(P, i0, i0 < end, p0);
+            load_part(P, i1, i1 < end, p1);
+            bool h0, h1;
+            if (MOVE) {
+                h0 = move_one<BMODE, GEN>(P, i0, p0, cnt, lost);
+                h1 = move_one<BMODE, GEN>(P, i1, p1, cnt, lost);
+            } else {
+                h0 = !isnan(p0.vx);
+                h1 = !isnan(p1.vx);
+            }
+            deposit_warp(P, win, ox, oy, use_win, h0, p0.X, p0.Y);
+            deposit_warp(P, win, ox, oy, use_win, h1, p1.X, p1.Y);
         }
         // lost-particle count: one atomic per warp, then per CTA
         for (int o = 16; o > 0; o >>= 1) lost += __shfl_xor_sync(0xffffffffu, lost, o);
@@ -255,6 +281,27 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
     }
 }
 
+template <int BMODE, bool GEN, bool MOVE>
+static int launch_one(lepic_ctx *c, PushP &P, size_t smem) {
+    static bool attr_set[64] = {false};
+    if (!attr_set[c->dev & 63]) {
+        LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   64 * 1024));
+        attr_set[c->dev & 63] = true;
+    }
+    int occ = 0;
+    LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE>, PUSH_THREADS, smem));
+    k_push_deposit<BMODE, GEN, MOVE><<<c->num_sms * std::max(1, occ), PUSH_THREADS, smem, c->stream>>>(P);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+template <int BMODE>
+static int launch_b(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
+    if (!move) return launch_one<BMODE, false, false>(c, P, smem);
+    return gen ? launch_one<BMODE, true, true>(c, P, smem) : launch_one<BMODE, false, true>(c, P, smem);
+}
+
 int push_deposit(lepic_ctx *c, int it, bool move) {
     const lepic_config &g = c->cfg;
     for (int s = 0; s < g.ntype; s++)
@@ -268,8 +315,8 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
         P.E = c->Ef; P.B = c->Bf;
-        P.bmode = g.flag_B;
-        if (g.flag_B_pos == 1 && g.charge[s] > 0.0) P.bmode = 0; // :185
+        int bmode = g.flag_B;
+        if (g.flag_B_pos == 1 && g.charge[s] > 0.0) bmode = 0; // :185
         P.Bcx = (float)g.Bc[0]; P.Bcy = (float)g.Bc[1]; P.Bcz = (float)g.Bc[2];
         P.cellwall = c->cellwall;
         P.acc = B.acc;
@@ -289,19 +336,14 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         size_t smem = sizeof(unsigned long long) * (size_t)P.WX * P.WY;
         P.win = smem <= 64 * 1024 ? 1 : 0;
         if (!P.win) smem = 0;
-        P.move = move ? 1 : 0;
         P.xlim = (long long)g.nx << c->S;
         P.ylim = (long long)g.ny << c->S;
-        static bool attr_set = false;
-        if (!attr_set) {
-            LCUDA(cudaFuncSetAttribute(k_push_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-            attr_set = true;
-        }
-        int occ = 0;
-        LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit, PUSH_THREADS, smem));
-        int grid = c->num_sms * std::max(1, occ);
-        k_push_deposit<<<grid, PUSH_THREADS, smem, c->stream>>>(P);
-        LCUDA(cudaGetLastError());
+        const bool gen = P.pbc || P.nmn || P.negion_nmn;
+        int r;
+        if (bmode == 1) r = launch_b<1>(c, P, smem, gen, move);
+        else if (bmode == 2) r = launch_b<2>(c, P, smem, gen, move);
+        else r = launch_b<0>(c, P, smem, gen, move);
+        if (r != LEPIC_OK) return r;
     }
     return LEPIC_OK;
 }

@@ -180,9 +180,13 @@ def test_mg_mixed_precision_reaches_1e8(gpu_lib, idx, n):
     res = O.l2_residual(cfg, st["phi"], rhs, case.bcnd)
     assert res <= 1e-8, res
     assert st["res_l2_rel"] <= 1e-8
-    # same discrete solution as the FP64 solver
-    ref = case.phi0.copy()
-    O.solve(cfg, ref, rhs, case.bcnd, case.levels(), 1e-13)
+    # same discrete solution as the FP64 solver: the oracle's where it finishes in seconds,
+    # else the GPU FP64 V-cycle (itself checked against the oracle above) driven to 1e-12
+    if n <= 256:
+        ref = case.phi0.copy()
+        O.solve(cfg, ref, rhs, case.bcnd, case.levels(), 1e-13)
+    else:
+        ref = s.solve(eps=1e-12, mode=capi.POISSON_FP64_MG_L2, phi=case.phi0.copy())["phi"]
     assert np.abs(st["phi"] - ref).max() <= 1e-5 * np.abs(ref).max()
     s.close()
 
