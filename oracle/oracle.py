@@ -24,9 +24,8 @@ MAXCOL = 64
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "lepic_oracle.c")
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
-            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "lepic_oracle.h"))):
+    srcs = [os.path.join(HERE, f) for f in ("lepic_oracle.c", "lepic_oracle.h", "cnn_oracle.c")]
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", HERE, "-B" if force else "-s"], check=True, capture_output=True)
     return LIB
 
@@ -310,3 +309,44 @@ class OracleSimulation:
             self.np_tot[s] = npt[s]
         self.mcc = t
         return t
+
+
+# ---------------------------------------------------------------------------------------------
+# learned warm-start network (cnn_oracle.c)
+
+CNN_CIN = (2, 16, 16, 32, 32, 64, 64, 64, 64, 64, 32, 16)
+CNN_COUT = (16, 16, 32, 32, 64, 64, 64, 64, 64, 32, 16, 1)
+
+
+def cnn_nparams() -> int:
+    return int(lib().o_cnn_nparams())
+
+
+def cnn_loss_grad(params: np.ndarray, x: np.ndarray, t: np.ndarray, m: np.ndarray, emulate_bf16: bool = True,
+                  want_grad: bool = True):
+    """Forward, energy-norm loss and gradient of the warm-start network on the CPU.
+    x: (N, H, W, 2), t and m: (N, H, W); H and W multiples of 8.  Returns (loss, out, grad)."""
+    L = lib()
+    f = L.o_cnn_loss_grad
+    f.restype = C.c_double
+    f.argtypes = [C.POINTER(C.c_double)] * 4 + [C.c_int] * 4 + [C.POINTER(C.c_double)] * 2
+    N, H, W = t.shape
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    tt = np.ascontiguousarray(t, dtype=np.float64)
+    mm = np.ascontiguousarray(m, dtype=np.float64)
+    out = np.zeros((N, H, W))
+    grad = np.zeros(prm.size) if want_grad else None
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+    loss = f(dp(prm), dp(xx), dp(tt), dp(mm), N, H, W, 1 if emulate_bf16 else 0, dp(out), dp(grad))
+    return loss, out, grad
+
+
+def cnn_init_params(seed: int = 0) -> np.ndarray:
+    """He-normal weights (std sqrt(2 / (9 cin))), zero biases, in the oracle's parameter order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for ci, co in zip(CNN_CIN, CNN_COUT):
+        out.append(rng.standard_normal(co * ci * 9) * np.sqrt(2.0 / (9 * ci)))
+        out.append(np.zeros(co))
+    return np.concatenate(out)
