@@ -206,6 +206,67 @@ def run_reference(args):
     return 0
 
 
+def learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step_fn):
+    import torch
+    import ctypes as C
+    cfg = capi.LepicCnnConfig(enable_training=1, warmup_solves=10 ** 9, steps_warmup=args.learn_train_steps,
+                              train_every=1, steps_after=args.learn_train_steps, crop=args.learn_crop,
+                              batch=args.learn_batch, lr=C.c_float(args.learn_lr), seed=11)
+    sim.check(lib.lepic_gpu_cnn_configure(ctx, C.byref(cfg)), "cnn_configure")
+
+    def timed(fn):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    t_train = timed(lambda: [one_step_fn(it + k, False, capi.POISSON_LEARNED) for k in range(args.learn_steps)])
+    it += args.learn_steps
+    cfg_off = capi.LepicCnnConfig(**{f: getattr(cfg, f) for f, _ in cfg._fields_})
+    cfg_off.enable_training = 0
+    rows = []
+    for k in range(args.learn_ab):
+        sim.check(lib.lepic_gpu_calc_rhs(ctx, None), "calc_rhs")
+        phi_prev = sim.grid(capi.GRID_PHI)
+        row = {}
+        for name, m in (("fp64_mg", capi.POISSON_FP64_MG_L2), ("mixed_pcg", capi.POISSON_MIXED_IR),
+                        ("learned", capi.POISSON_LEARNED), ("learned_train", capi.POISSON_LEARNED)):
+            sim.set_phi(phi_prev)
+            sim.check(lib.lepic_gpu_cnn_configure(ctx, C.byref(cfg if name == "learned_train" else cfg_off)),
+                      "cnn_configure")
+            st = capi.LepicSolveStats()
+            ms = timed(lambda: sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, m, C.byref(st)), "solver"))
+            row[name] = {"ms": ms, "cycles": st.cycles, "res_l2_rel": st.res_l2_rel}
+            if name == "learned":
+                cs = capi.LepicCnnStats()
+                sim.check(lib.lepic_gpu_cnn_stats(ctx, C.byref(cs)), "cnn_stats")
+                row[name]["res_ratio"] = cs.last_res_ratio
+                row[name]["accepted"] = cs.last_accepted
+        rows.append(row)
+        sim.check(lib.lepic_gpu_calc_efield(ctx, None), "efield")
+        sim.check(lib.lepic_gpu_push_deposit(ctx, it, None), "push")
+        it += 1
+    sim.check(lib.lepic_gpu_cnn_configure(ctx, C.byref(cfg_off)), "cnn_configure")
+    mean = lambda name, key: float(np.mean([r[name][key] for r in rows]))
+    out = {"training_pic_steps": args.learn_steps, "training_ms_total": t_train,
+           "train_steps_per_solve": args.learn_train_steps, "crop": args.learn_crop, "batch": args.learn_batch,
+           "ab_steps": args.learn_ab}
+    for name in ("fp64_mg", "mixed_pcg", "learned", "learned_train"):
+        out[name] = {"ms": mean(name, "ms"), "cycles": mean(name, "cycles"),
+                     "res_l2_rel_max": max(r[name]["res_l2_rel"] for r in rows)}
+    out["learned"]["res_ratio"] = mean("learned", "res_ratio")
+    out["learned"]["accepted"] = mean("learned", "accepted")
+    out["online_training_ms_per_solve"] = out["learned_train"]["ms"] - out["learned"]["ms"]
+    out["speedup_learned_vs_fp64_mg"] = out["fp64_mg"]["ms"] / out["learned"]["ms"]
+    out["speedup_learned_vs_mixed_pcg"] = out["mixed_pcg"]["ms"] / out["learned"]["ms"]
+    pois["learned_ab"] = out
+    return it
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -256,14 +317,16 @@ def run_ours(args):
         b.record(stream)
         ev.setdefault(name, []).append((it, a, b))
 
-    def one_step(it, timed):
+    def one_step(it, timed, solve_mode=None):
+        sm = mode if solve_mode is None else solve_mode
+
         def rec(name, fn):
             if timed:
                 phase(name, it, fn)
             else:
                 fn()
         rec("rhs", lambda: sim.check(lib.lepic_gpu_calc_rhs(ctx, None), "calc_rhs"))
-        rec("poisson", lambda: sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, mode, None), "solver"))
+        rec("poisson", lambda: sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, sm, None), "solver"))
         rec("efield", lambda: sim.check(lib.lepic_gpu_calc_efield(ctx, None), "efield"))
         if it % 10 == 1:
             def srt():
@@ -337,6 +400,12 @@ def run_ours(args):
     sim.set_phi(phi_save)
     for start in ("warm", "cold"):
         pois[f"speedup_{start}"] = pois[f"fp64_mg_{start}"]["ms"] / pois[f"mixed_pcg_{start}"]["ms"]
+
+    # learned warm start: PIC steps in the learned mode (online training), then an A/B on the
+    # following steps -- plain FP64 multigrid, the mixed CG and the learned start, each from the
+    # previous step's phi on the same rhs (training off while timed; its cost reported apart)
+    if args.learn_steps > 0:
+        it = learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step)
 
     # end to end through the C ABI with host buffers: phi exchanged with pinned host memory
     # every step (the Fortran host's array) and the particle counters read back
@@ -431,6 +500,12 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learn-steps", type=int, default=60, help="PIC steps of online training before the A/B")
+    ap.add_argument("--learn-ab", type=int, default=4, help="steps of the learned/plain Poisson A/B")
+    ap.add_argument("--learn-train-steps", type=int, default=2, help="Adam steps per learned solve")
+    ap.add_argument("--learn-crop", type=int, default=256)
+    ap.add_argument("--learn-batch", type=int, default=4)
+    ap.add_argument("--learn-lr", type=float, default=2e-3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -46,6 +46,7 @@ extern "C" {
 #define LEPIC_POISSON_FP64_MG 0   /* the reference's V-cycle (mg.f90) in FP64              */
 #define LEPIC_POISSON_MIXED_IR 1  /* FP64 CG preconditioned by an FP32 V-cycle            */
 #define LEPIC_POISSON_FP64_MG_L2 2 /* mode 0's V-cycles, stopped on the L2 relative residual */
+#define LEPIC_POISSON_LEARNED 3   /* mode 1 started from the learned network's prediction   */
 
 /* Grid selectors for lepic_gpu_get_grid / lepic_gpu_set_grid */
 #define LEPIC_GRID_PHI 0      /* phi(0:nx+2,0:ny+2)                     */
@@ -229,6 +230,54 @@ int lepic_gpu_deposit_noalloc(const uint32_t *X, const uint32_t *Y, const float 
  * X, Y are uint32 fixed point in cell units with `shift` fractional bits, VX/VY/VZ float. */
 int lepic_gpu_particle_arrays(lepic_ctx *ctx, int32_t ptype, void **X, void **Y, void **VX,
                               void **VY, void **VZ, int64_t *n_slots, int32_t *shift);
+
+/* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
+ * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network
+ * (3x3 convolutions, channels 16/32/64/64, BF16 tensor-core convolutions with FP32
+ * accumulation) maps (residual of the previous potential b - A phi_prev, scaled by its RMS;
+ * phi_prev scaled) to a correction of phi; the correction is kept only if it lowers the FP64
+ * residual, then mode 1 refines it to the requested residual.  After the solve the network is
+ * trained online (Adam) on crops of the pair it just saw: input -> (phi_solved - phi_prev)
+ * scaled, with the energy norm of the error as the loss.  Periodic or Neumann decks take
+ * mode 1's path for them (the FP64 V-cycle). */
+typedef struct {
+    int32_t enable_training;  /* 0: inference only                                        */
+    int32_t warmup_solves;    /* the first solves train every time ...                    */
+    int32_t steps_warmup;     /* ... with this many Adam steps each                       */
+    int32_t train_every;      /* afterwards every train_every-th solve trains ...          */
+    int32_t steps_after;      /* ... with this many steps                                  */
+    int32_t crop;             /* training crop edge (pixels, multiple of 8)               */
+    int32_t batch;            /* crops per Adam step (1..8)                               */
+    float lr;                 /* Adam learning rate                                       */
+    uint64_t seed;            /* weight initialisation and crop positions                 */
+} lepic_cnn_config;
+
+typedef struct {
+    int64_t solves;           /* learned-mode solves so far                               */
+    int64_t train_steps;      /* Adam steps so far                                        */
+    int32_t last_accepted;    /* 1 if the last prediction was kept                        */
+    double last_res_ratio;    /* ||b - A phi_pred|| / ||b - A phi_prev|| of the last solve */
+    double last_loss;         /* loss of the last training step                           */
+} lepic_cnn_stats;
+
+int lepic_gpu_cnn_configure(lepic_ctx *ctx, const lepic_cnn_config *cfg);
+int lepic_gpu_cnn_stats(lepic_ctx *ctx, lepic_cnn_stats *stats);
+/* the context's network (a handle for the lepic_cnn_* calls below; NULL before the first
+ * learned solve or configure) */
+void *lepic_gpu_cnn_net(lepic_ctx *ctx);
+
+/* The network alone, on the current CUDA device: parameters are FP32, in the order
+ * e0a e0b e1a e1b e2a e2b e3a e3b d2 d1 d0 out, each W[cout][cin][3][3] then b[cout]. */
+int lepic_cnn_create(void **net, uint64_t seed);
+int lepic_cnn_destroy(void *net);
+int lepic_cnn_nparams(void);
+int lepic_cnn_params(void *net, float *params, int64_t n, int32_t set);
+/* forward, loss and gradient for N images of H x W (multiples of 8) of host data:
+ * x [N][H][W][2], t and m [N][H][W] (m 0/1; both NULL: forward only); out [N][H][W]. */
+int lepic_cnn_loss_grad(void *net, const float *x, const float *t, const float *m, int32_t N,
+                        int32_t H, int32_t W, float *out, float *grad, double *loss);
+int lepic_cnn_adam_step(void *net, float lr);
+const char *lepic_cnn_last_error(void *net);
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,7 @@ ERROR_NAMES = {
 POISSON_FP64_MG = 0
 POISSON_MIXED_IR = 1
 POISSON_FP64_MG_L2 = 2
+POISSON_LEARNED = 3
 
 GRID_PHI = 0
 GRID_RHS = 1
@@ -121,6 +122,23 @@ _IP = C.POINTER(C.c_int32)
 _VP = C.c_void_p
 
 # name -> (restype, argtypes); every function declared in include/lepic_gpu.h
+class LepicCnnConfig(C.Structure):
+    _fields_ = [
+        ("enable_training", C.c_int32), ("warmup_solves", C.c_int32), ("steps_warmup", C.c_int32),
+        ("train_every", C.c_int32), ("steps_after", C.c_int32), ("crop", C.c_int32), ("batch", C.c_int32),
+        ("lr", C.c_float), ("seed", C.c_uint64),
+    ]
+
+
+class LepicCnnStats(C.Structure):
+    _fields_ = [
+        ("solves", C.c_int64), ("train_steps", C.c_int64), ("last_accepted", C.c_int32),
+        ("last_res_ratio", C.c_double), ("last_loss", C.c_double),
+    ]
+
+
+_FP = C.POINTER(C.c_float)
+
 PROTOTYPES = {
     "lepic_gpu_abi_version": (C.c_int32, []),
     "lepic_gpu_create": (C.c_int, [C.POINTER(LepicConfig), _IP, _DP, _DP, C.POINTER(LepicXsTables),
@@ -151,6 +169,17 @@ PROTOTYPES = {
     "lepic_gpu_particle_arrays": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                             C.POINTER(_VP), C.POINTER(_VP), C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int32)]),
+    "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),
+    "lepic_gpu_cnn_stats": (C.c_int, [_VP, C.POINTER(LepicCnnStats)]),
+    "lepic_gpu_cnn_net": (_VP, [_VP]),
+    "lepic_cnn_create": (C.c_int, [C.POINTER(_VP), C.c_uint64]),
+    "lepic_cnn_destroy": (C.c_int, [_VP]),
+    "lepic_cnn_nparams": (C.c_int, []),
+    "lepic_cnn_params": (C.c_int, [_VP, _FP, C.c_int64, C.c_int32]),
+    "lepic_cnn_loss_grad": (C.c_int, [_VP, _FP, _FP, _FP, C.c_int32, C.c_int32, C.c_int32, _FP, _FP,
+                                      C.POINTER(C.c_double)]),
+    "lepic_cnn_adam_step": (C.c_int, [_VP, C.c_float]),
+    "lepic_cnn_last_error": (C.c_char_p, [_VP]),
 }
 
 _lib = None

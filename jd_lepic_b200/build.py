@@ -32,6 +32,7 @@ SOURCES = {
     "sort.cu": [],
     "mcc.cu": [],
     "noalloc.cu": ["-fmad=false"],
+    "cnn.cu": [],
 }
 
 

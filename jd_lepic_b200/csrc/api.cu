@@ -7,7 +7,7 @@
 #include <cstring>
 #include <new>
 #include <vector>
-#include "lepic_internal.cuh"
+#include "cnn.cuh"
 
 #define LEPIC_ABI_VERSION 1
 
@@ -124,6 +124,15 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
     LALLOC(c->Ed, 2 * nn); LALLOC(c->Ef, nn);
     LALLOC(c->npd, nn); LALLOC(c->np_red, (size_t)g.ntype * nn); LALLOC(c->np_mx, LEPIC_MAXSP);
     LCUDA(cudaMemcpy(c->phi, phi_init, sizeof(double) * nn, cudaMemcpyHostToDevice));
+    {
+        double m = 0.0;
+        for (long long n = 0; n < nn; n++) m = std::max(m, fabs(phi_init[n]));
+        c->phi_scale = m > 0.0 ? m : 1.0;
+        long long cnt = 0;
+        for (int j = 1; j <= ny + 1; j++)
+            for (int i = 1; i <= nx + 1; i++) cnt += bcnd[i + (long long)j * (nx + 3)] <= 0;
+        c->n_unknown = cnt;
+    }
     LCUDA(cudaMemset(c->rhs, 0, sizeof(double) * (nx + 1) * (ny + 1)));
     LCUDA(cudaMemset(c->Ed, 0, sizeof(double2) * 2 * nn));
     LCUDA(cudaMemset(c->Ef, 0, sizeof(float2) * nn));
@@ -258,6 +267,7 @@ extern "C" int lepic_gpu_create(const lepic_config *cfg, const int32_t *bcnd, co
 extern "C" int lepic_gpu_destroy(lepic_ctx *c) {
     if (!c) return LEPIC_EINVAL;
     cudaStreamSynchronize(c->stream);
+    learn_free(c);
     free_all(c);
     delete c;
     return LEPIC_OK;
@@ -493,6 +503,7 @@ static int solve(lepic_ctx *c, double eps, int mode) {
     if (mode == LEPIC_POISSON_FP64_MG) return mg_solve(c, eps, 0);
     if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps);
     if (mode == 2) return mg_solve(c, eps, 2);
+    if (mode == LEPIC_POISSON_LEARNED) return learned_solve(c, eps);
     c->last_err = "unknown Poisson mode";
     return LEPIC_EINVAL;
 }

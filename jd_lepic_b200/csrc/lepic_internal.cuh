@@ -123,6 +123,10 @@ struct lepic_ctx {
     double nu_max[LEPIC_MAXSP] = {0};
     int flag_ionrep = 0;
     double fEk = 0;
+    // learned warm start (cnn.cu), created on first use
+    void *learn = nullptr;
+    double phi_scale = 1.0;        // max |phi| of the initial potential (network input scale)
+    long long n_unknown = 0;       // nodes with bcnd <= 0
     // counters
     DevCounters *dcnt = nullptr;
     DevCounters *hcnt = nullptr;  // pinned mirror

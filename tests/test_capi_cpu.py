@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "lepic_gpu.h")
 def header_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(lepic_gpu_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(lepic_(?:gpu|cnn)_\w+)\s*\(", text)))
 
 
 @pytest.fixture(scope="module")
@@ -45,7 +45,8 @@ def test_abi_version_without_gpu(lib):
 def test_struct_layouts_match_c():
     structs = {"lepic_config": _capi.LepicConfig, "lepic_xs_tables": _capi.LepicXsTables,
                "lepic_solve_stats": _capi.LepicSolveStats, "lepic_push_stats": _capi.LepicPushStats,
-               "lepic_mcc_stats": _capi.LepicMccStats, "lepic_load_spec": _capi.LepicLoadSpec}
+               "lepic_mcc_stats": _capi.LepicMccStats, "lepic_load_spec": _capi.LepicLoadSpec,
+               "lepic_cnn_config": _capi.LepicCnnConfig, "lepic_cnn_stats": _capi.LepicCnnStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
