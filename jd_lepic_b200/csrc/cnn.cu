@@ -147,11 +147,11 @@ __device__ __forceinline__ uint32_t mask_bf2(uint32_t v, uint32_t m) {
 
 // ---------------------------------------------------------------------------------------
 // convolution parameters
-enum { IN_DIRECT = 0, IN_POOL = 1, IN_UP = 2 };
+enum { IN_DIRECT = 0, IN_POOL = 1, IN_UP = 2, IN_X2 = 3 };  // IN_X2: 2 channels per pixel, zero-padded to CIN
 enum { EPI_RELU = 0, EPI_OUTF = 1, EPI_GRAD = 2 };
 
 struct ConvP {
-    const bf16 *in;      // input tensor [N][inH][inW][CIN]
+    const bf16 *in;      // input tensor [N][inH][inW][CIN] ([N][H][W][2] for IN_X2)
     int in_mode, inH, inW;
     int N, H, W, R;      // output (and convolution input) size; rows per work unit
     const bf16 *w;       // packed weights [tap][CIN/8][COUT][8]
@@ -165,54 +165,105 @@ struct ConvP {
     int *err;
 };
 
-// one input row (pixels x0-1 .. x0+128) into ring slot `slot` of the staging buffer
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// One input row (pixels x0-1 .. x0+128) into ring slot `slot` of the staging buffer.  Plain
+// and upsampled inputs are copied with cp.async (zero-filled outside the image; the caller
+// commits and waits); pooled and 2-channel inputs go through registers, all loads of a
+// thread issued before its stores.
 template <int CIN, int NT>
 __device__ __forceinline__ void load_row(const ConvP &P, unsigned char *s_in, int n, int yy, int x0, int slot) {
     constexpr int NCH = CIN / 8;
+    constexpr int ITEMS = (CONV_PITCH * NCH + NT - 1) / NT;
     const bool row_ok = yy >= 0 && yy < P.H;
-    for (int i = threadIdx.x; i < CONV_PITCH * NCH; i += NT) {
-        const int p = i / NCH, c8 = i - p * NCH;
-        const int xx = x0 - 1 + p;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (row_ok && xx >= 0 && xx < P.W) {
-            if (P.in_mode == IN_DIRECT) {
-                v = __ldg(reinterpret_cast<const uint4 *>(P.in + (((size_t)n * P.inH + yy) * P.inW + xx) * CIN) + c8);
-            } else if (P.in_mode == IN_UP) {
-                v = __ldg(reinterpret_cast<const uint4 *>(
-                              P.in + (((size_t)n * P.inH + (yy >> 1)) * P.inW + (xx >> 1)) * CIN) + c8);
-            } else {
-                const size_t r0 = ((size_t)n * P.inH + 2 * yy) * P.inW + 2 * xx;
-                const uint4 *q0 = reinterpret_cast<const uint4 *>(P.in + r0 * CIN) + c8;
-                const uint4 *q1 = reinterpret_cast<const uint4 *>(P.in + (r0 + P.inW) * CIN) + c8;
-                v = avg4v(__ldg(q0), __ldg(q0 + NCH), __ldg(q1), __ldg(q1 + NCH), 0.25f);
+    unsigned char *base = s_in + (size_t)slot * NCH * CONV_PITCH * 16;
+    if (P.in_mode == IN_DIRECT || P.in_mode == IN_UP) {
+        const int ys = P.in_mode == IN_UP ? (yy >> 1) : yy;
+        for (int i = threadIdx.x; i < CONV_PITCH * NCH; i += NT) {
+            const int p = i / NCH, c8 = i - p * NCH;
+            const int xx = x0 - 1 + p;
+            const bool ok = row_ok && xx >= 0 && xx < P.W;
+            const int xs = P.in_mode == IN_UP ? (xx >> 1) : xx;
+            const bf16 *src = ok ? P.in + (((size_t)n * P.inH + ys) * P.inW + xs) * CIN + 8 * c8 : P.in;
+            cp_async16(smem_u32(base + ((size_t)c8 * CONV_PITCH + p) * 16), src, ok);
+        }
+        return;
+    }
+    constexpr int BATCH = 2;
+#pragma unroll
+    for (int b0 = 0; b0 < ITEMS; b0 += BATCH) {
+        uint4 v[BATCH];
+        int dst[BATCH];
+#pragma unroll
+        for (int k = 0; k < BATCH; k++) {
+            const int i = threadIdx.x + (b0 + k) * NT;
+            v[k] = make_uint4(0u, 0u, 0u, 0u);
+            dst[k] = -1;
+            if (b0 + k < ITEMS && i < CONV_PITCH * NCH) {
+                const int p = i / NCH, c8 = i - p * NCH;
+                const int xx = x0 - 1 + p;
+                dst[k] = (c8 * CONV_PITCH + p) * 16;
+                if (row_ok && xx >= 0 && xx < P.W) {
+                    if (P.in_mode == IN_X2) {
+                        if (c8 == 0)
+                            v[k].x = __ldg(reinterpret_cast<const uint32_t *>(P.in) + ((size_t)n * P.inH + yy) * P.inW + xx);
+                    } else {
+                        const size_t r0 = ((size_t)n * P.inH + 2 * yy) * P.inW + 2 * xx;
+                        const uint4 *q0 = reinterpret_cast<const uint4 *>(P.in + r0 * CIN) + c8;
+                        const uint4 *q1 = reinterpret_cast<const uint4 *>(P.in + (r0 + P.inW) * CIN) + c8;
+                        v[k] = avg4v(__ldg(q0), __ldg(q0 + NCH), __ldg(q1), __ldg(q1 + NCH), 0.25f);
+                    }
+                }
             }
         }
-        *reinterpret_cast<uint4 *>(s_in + ((size_t)(slot * NCH + c8) * CONV_PITCH + p) * 16) = v;
+#pragma unroll
+        for (int k = 0; k < BATCH; k++)
+            if (dst[k] >= 0) *reinterpret_cast<uint4 *>(base + dst[k]) = v[k];
     }
 }
 
 template <int COUT>
-__device__ __forceinline__ void conv_epilogue(const ConvP &P, uint32_t tmem, int n, int y, int x0) {
+__device__ __forceinline__ void conv_epilogue(const ConvP &P, const float *s_bias, uint32_t tmem, int n, int y,
+                                              int x0) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int x = x0 + warp * 32 + lane;
     const bool ok = x < P.W;
-    const size_t pix = ((size_t)n * P.H + y) * P.W + x;
+    const size_t pix = ((size_t)n * P.H + y) * P.W + (ok ? x : 0);
     const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
     if (P.epi == EPI_OUTF) {
         float v[16];
         tmem_ld16(tbase, v);
-        if (ok) P.outf[pix] = v[0] + (P.bias ? P.bias[0] : 0.0f);
+        if (ok) P.outf[pix] = v[0] + s_bias[0];
         return;
     }
+    // the skip (or mask) values of this pixel, fetched before the accumulator reads
+    const bf16 *side = P.epi == EPI_RELU ? P.skip : P.mask;
+    uint4 sd[COUT / 8];
+#pragma unroll
+    for (int k = 0; k < COUT / 8; k++)
+        sd[k] = (side && ok) ? __ldg(reinterpret_cast<const uint4 *>(side + pix * COUT) + k) : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
     for (int c0 = 0; c0 < COUT; c0 += 16) {
         float v[16];
         tmem_ld16(tbase + c0, v);
         if (!ok) continue;
+        const uint32_t sv[8] = {sd[c0 / 8].x, sd[c0 / 8].y, sd[c0 / 8].z, sd[c0 / 8].w,
+                                sd[c0 / 8 + 1].x, sd[c0 / 8 + 1].y, sd[c0 / 8 + 1].z, sd[c0 / 8 + 1].w};
         uint32_t o[8];
         if (P.epi == EPI_RELU) {
 #pragma unroll
-            for (int k = 0; k < 16; k++) v[k] = fmaxf(v[k] + (P.bias ? __ldg(P.bias + c0 + k) : 0.0f), 0.0f);
+            for (int k = 0; k < 16; k += 4) {
+                const float4 b4 = *reinterpret_cast<const float4 *>(s_bias + c0 + k);
+                v[k] = fmaxf(v[k] + b4.x, 0.0f);
+                v[k + 1] = fmaxf(v[k + 1] + b4.y, 0.0f);
+                v[k + 2] = fmaxf(v[k + 2] + b4.z, 0.0f);
+                v[k + 3] = fmaxf(v[k + 3] + b4.w, 0.0f);
+            }
 #pragma unroll
             for (int k = 0; k < 8; k++) o[k] = f2_to_bf2(v[2 * k], v[2 * k + 1]);
             if (P.out) {
@@ -221,9 +272,6 @@ __device__ __forceinline__ void conv_epilogue(const ConvP &P, uint32_t tmem, int
                 dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
             }
             if (P.skip) {
-                const uint4 *sp = reinterpret_cast<const uint4 *>(P.skip + pix * COUT + c0);
-                const uint4 s0 = __ldg(sp), s1 = __ldg(sp + 1);
-                const uint32_t sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
                 uint32_t q[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
@@ -244,11 +292,8 @@ __device__ __forceinline__ void conv_epilogue(const ConvP &P, uint32_t tmem, int
             }
             if (P.out) {
                 if (P.mask) {
-                    const uint4 *mp = reinterpret_cast<const uint4 *>(P.mask + pix * COUT + c0);
-                    const uint4 m0 = __ldg(mp), m1 = __ldg(mp + 1);
-                    const uint32_t mv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
 #pragma unroll
-                    for (int k = 0; k < 8; k++) o[k] = mask_bf2(o[k], mv[k]);
+                    for (int k = 0; k < 8; k++) o[k] = mask_bf2(o[k], sv[k]);
                 }
                 uint4 *dst = reinterpret_cast<uint4 *>(P.out + pix * COUT + c0);
                 dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
@@ -262,7 +307,7 @@ __device__ __forceinline__ void conv_epilogue(const ConvP &P, uint32_t tmem, int
 // one elected thread issues 9 * CIN/16 tcgen05.mma into tensor memory while all threads stage
 // the next input row, then every thread drains its pixel's accumulator row (one TMEM lane).
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(CONV_THREADS) k_conv(ConvP P) {
+__global__ void __launch_bounds__(CONV_THREADS, (CIN == 16 && COUT == 16) ? 10 : 1) k_conv(ConvP P) {
     constexpr int NCH = CIN / 8;
     constexpr int W_BYTES = 9 * CIN * COUT * 2;
     constexpr uint32_t NCOLS = COUT < 32 ? 32 : COUT;
@@ -273,7 +318,9 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(ConvP P) {
     __shared__ __align__(8) uint64_t s_mbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
+    __shared__ __align__(16) float s_bias[COUT];
     const int tid = threadIdx.x;
+    if (tid < COUT) s_bias[tid] = P.bias ? P.bias[tid] : 0.0f;
     if (tid < 32) tmem_alloc(smem_u32(&s_tmem), NCOLS);
     if (tid == 0) {
         mbar_init(smem_u32(&s_mbar), 1);
@@ -302,6 +349,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(ConvP P) {
         load_row<CIN, CONV_THREADS>(P, s_in, n, y0 - 1, x0, (y0) & 3);
         load_row<CIN, CONV_THREADS>(P, s_in, n, y0, x0, (y0 + 1) & 3);
         load_row<CIN, CONV_THREADS>(P, s_in, n, y0 + 1, x0, (y0 + 2) & 3);
+        cp_async_commit();
+        cp_async_wait_all();
         fence_async_smem();
         __syncthreads();
         for (int y = y0; y < y1; y++) {
@@ -322,12 +371,14 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv(ConvP P) {
                 umma_commit(mbar);
             }
             if (y + 1 < y1) load_row<CIN, CONV_THREADS>(P, s_in, n, y + 2, x0, (y + 3) & 3);
-            fence_async_smem();
+            cp_async_commit();
             const bool done = mbar_wait(mbar, phase);
             phase ^= 1u;
             tc_fence_after();
-            if (done) conv_epilogue<COUT>(P, tmem, n, y, x0);
+            if (done) conv_epilogue<COUT>(P, s_bias, tmem, n, y, x0);
             else s_fail = 1;
+            cp_async_wait_all();
+            fence_async_smem();
             tc_fence_before();
             __syncthreads();
             if (s_fail) break;
@@ -381,6 +432,7 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(DwP D) {
     load_row<CIN, DW_THREADS>(P, s_in, n, y0, x0, (y0 + 1) & 3);
     for (int y = y0; y < y1; y++) {
         load_row<CIN, DW_THREADS>(P, s_in, n, y + 1, x0, (y + 2) & 3);
+        cp_async_commit();
         for (int i = tid; i < 128 * (COUT / 8); i += DW_THREADS) {
             const int p = i / (COUT / 8), c8 = i - p * (COUT / 8);
             const int xx = x0 + p;
@@ -388,6 +440,7 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(DwP D) {
             if (xx < P.W) v = __ldg(reinterpret_cast<const uint4 *>(D.G + (((size_t)n * P.H + y) * P.W + xx) * COUT) + c8);
             reinterpret_cast<uint4 *>(s_g)[i] = v;
         }
+        cp_async_wait_all();
         __syncthreads();
         if (active) {
             const int slot = (y + dy) & 3;
@@ -418,21 +471,28 @@ __global__ void __launch_bounds__(DW_THREADS) k_conv_dw(DwP D) {
     if (bias_thr) D.partb[(size_t)u * COUT + tid] = db;
 }
 
-// sum of the per-unit partials (fixed order) into the parameter-gradient vector
+// sum of the per-unit partials into the parameter-gradient vector: one warp per parameter,
+// lane l adds units l, l+32, ... and a fixed shuffle tree combines the lanes (deterministic)
 __global__ void k_dw_reduce(const float *part, const float *partb, int units, int cinp, int coutp, int cin, int cout,
                             float *gw, float *gb) {
     const int nw = cout * cin * 9;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nw + cout; k += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int k = blockIdx.x * wpb + (threadIdx.x >> 5); k < nw + cout; k += gridDim.x * wpb) {
         float s = 0.0f;
         if (k < nw) {
             const int n = k / (cin * 9), r = k - n * cin * 9, c = r / 9, tap = r - 9 * c;
             const size_t src = ((size_t)n * cinp + c) * 9 + tap;
-            for (int u = 0; u < units; u++) s += part[(size_t)u * coutp * cinp * 9 + src];
-            gw[k] = s;
+            for (int u = lane; u < units; u += 32) s += part[(size_t)u * coutp * cinp * 9 + src];
         } else {
             const int n = k - nw;
-            for (int u = 0; u < units; u++) s += partb[(size_t)u * coutp + n];
-            gb[n] = s;
+            for (int u = lane; u < units; u += 32) s += partb[(size_t)u * coutp + n];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            if (k < nw) gw[k] = s;
+            else gb[k - nw] = s;
         }
     }
 }
@@ -512,12 +572,23 @@ __global__ void k_loss(const float *pred, const float *t, const uint8_t *m, int 
     if (threadIdx.x == 0) partial[blockIdx.x] = red[0] * (double)inv;
 }
 
-__global__ void k_sum_partials(const double *partial, int n, double *out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < n; k++) s += partial[k];
-        *out = s;
+// sum of n partials by one block of 256 threads in a fixed order (deterministic)
+__device__ __forceinline__ double block_sum256(const double *partial, int n) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < n; k += 256) s += partial[k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
     }
+    return red[0];
+}
+
+__global__ void __launch_bounds__(256) k_sum_partials(const double *partial, int n, double *out) {
+    const double s = block_sum256(partial, n);
+    if (threadIdx.x == 0) *out = s;
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master parameters
@@ -579,10 +650,7 @@ __global__ void k_crop(const bf16 *x, const float *t, const uint8_t *m, int Hf, 
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < tot; p += (long long)gridDim.x * blockDim.x) {
         const int xx = (int)(p % S), yy = (int)((p / S) % S), b = (int)(p / ((long long)S * S));
         const size_t src = (size_t)(C.oy[b] + yy) * Wf + (C.ox[b] + xx);
-        const uint4 *xs = reinterpret_cast<const uint4 *>(x + src * 16);
-        uint4 *xd = reinterpret_cast<uint4 *>(xc + p * 16);
-        xd[0] = xs[0];
-        xd[1] = xs[1];
+        reinterpret_cast<uint32_t *>(xc)[p] = reinterpret_cast<const uint32_t *>(x)[src];
         tc[p] = t[src];
         mc[p] = m[src];
     }
@@ -602,7 +670,7 @@ __global__ void k_crop(const bf16 *x, const float *t, const uint8_t *m, int Hf, 
 struct Acts {   // activations of one forward pass (N images of H x W)
     int N = 0, H = 0, W = 0;
     bool train = false;
-    bf16 *x = nullptr;                                     // [N][H][W][16]
+    bf16 *x = nullptr;                                     // [N][H][W][2]
     bf16 *e0a, *e0, *e1a, *e1, *e2a, *e2, *e3a, *e3;       // encoder
     bf16 *d2a, *d2, *d1a, *d1, *d0a, *d0;                  // decoder
     float *out = nullptr;                                  // [N][H][W]
@@ -645,28 +713,43 @@ static int grid_for(long long work, int threads, int num_sms) {
     return (int)std::max(1ll, std::min(g, (long long)num_sms * 8));
 }
 
+// resident CTAs per SM for a kernel of `smem` dynamic bytes and `threads` threads, bounded by
+// the shared memory of an SM and, for the convolution, by its 512 tensor-memory columns
+static int ctas_per_sm(CnnNet *net, size_t smem, int threads, int tmem_cols) {
+    int smem_sm = 0;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, net->dev);
+    int k = (int)((size_t)smem_sm / (smem + 1024 + 256));     // + per-CTA reserved and static
+    k = std::min(k, 2048 / threads);
+    if (tmem_cols > 0) k = std::min(k, 512 / tmem_cols);
+    return std::max(1, k);
+}
+
 template <int CIN, int COUT>
 static int launch_conv(CnnNet *net, ConvP &P) {
     const size_t smem = (size_t)9 * CIN * COUT * 2 + (size_t)4 * (CIN / 8) * CONV_PITCH * 16;
-    static int occ[64] = {0};
+    constexpr int NCOLS = COUT < 32 ? 32 : COUT;
+    static int per_sm_cache[64] = {0};
     static std::mutex mu;
-    int o;
+    int per_sm;
     {
         std::lock_guard<std::mutex> lk(mu);
-        if (!occ[net->dev & 63]) {
+        int &c = per_sm_cache[net->dev & 63];
+        if (!c) {
             NCUDA(cudaFuncSetAttribute(k_conv<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int v = 0;
-            NCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_conv<CIN, COUT>, CONV_THREADS, smem));
-            if (v < 1) { net->last_err = "convolution kernel does not fit on an SM"; return LEPIC_ECUDA; }
-            occ[net->dev & 63] = v;
+            NCUDA(cudaFuncSetAttribute(k_conv<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+            c = ctas_per_sm(net, smem, CONV_THREADS, NCOLS);
         }
-        o = occ[net->dev & 63];
+        per_sm = c;
     }
-    // at most 512 tensor-memory columns per SM between the resident CTAs
-    const int per_sm = std::min(o, (int)(512 / (COUT < 32 ? 32 : COUT)));
-    const int nstrip = (P.W + 127) / 128, nrb = (P.H + P.R - 1) / P.R;
-    const long long units = (long long)P.N * nstrip * nrb;
-    const int grid = (int)std::min(units, (long long)net->num_sms * per_sm);
+    // rows per work unit: about one unit per resident CTA (one prologue each, no tail)
+    const int nstrip = (P.W + 127) / 128;
+    const long long slots = (long long)net->num_sms * per_sm;
+    const long long strips = (long long)P.N * nstrip;
+    P.R = (int)std::max(4ll, std::min((long long)P.H, (strips * P.H + slots - 1) / slots));
+    const int nrb = (P.H + P.R - 1) / P.R;
+    const long long units = strips * nrb;
+    const int grid = (int)std::min(units, slots);
     P.err = net->derr;
     k_conv<CIN, COUT><<<grid, CONV_THREADS, smem, net->stream>>>(P);
     NCUDA(cudaGetLastError());
@@ -690,6 +773,8 @@ static int launch_dw(CnnNet *net, DwP &D, int units) {
         std::lock_guard<std::mutex> lk(mu);
         if (!set[net->dev & 63]) {
             NCUDA(cudaFuncSetAttribute(k_conv_dw<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            NCUDA(cudaFuncSetAttribute(k_conv_dw<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
             set[net->dev & 63] = true;
         }
     }
@@ -708,7 +793,7 @@ static int dw_dispatch(CnnNet *net, int cin, int cout, DwP &D, int units) {
     return LEPIC_ENOKERNEL;
 }
 
-static int conv_rows(int H) { return H >= 512 ? 8 : 4; }
+static int conv_rows(int H) { return H >= 1024 ? 16 : H >= 256 ? 8 : 4; }
 
 static ConvP conv_params(const bf16 *in, int mode, int N, int H, int W) {
     ConvP P;
@@ -764,7 +849,7 @@ static int bwd_weights(CnnNet *net, int l, const bf16 *in, int mode, const bf16 
     int r = dw_dispatch(net, cinp, coutp, D, units);
     if (r) return r;
     const int nw = L_COUT[l] * L_CIN[l] * 9 + L_COUT[l];
-    k_dw_reduce<<<grid_for(nw, 256, net->num_sms), 256, 0, net->stream>>>(
+    k_dw_reduce<<<grid_for((long long)nw * 32, 256, net->num_sms), 256, 0, net->stream>>>(
         net->part, net->partb, units, cinp, coutp, L_CIN[l], L_COUT[l], net->grad + net->ow[l], net->grad + net->ob[l]);
     NCUDA(cudaGetLastError());
     return LEPIC_OK;
@@ -781,7 +866,7 @@ static int acts_alloc(CnnNet *net, Acts &A, int N, int H, int W, bool train) {
         return LEPIC_OK;
     };
     int r = 0;
-    r |= bf(p0 * 16, &A.x);
+    r |= bf(p0 * 2, &A.x);
     r |= bf(p0 * 16, &A.e0a); r |= bf(p0 * 16, &A.e0);
     r |= bf(p1 * 32, &A.e1a); r |= bf(p1 * 32, &A.e1);
     r |= bf(p2 * 64, &A.e2a); r |= bf(p2 * 64, &A.e2);
@@ -807,7 +892,7 @@ static int acts_alloc(CnnNet *net, Acts &A, int N, int H, int W, bool train) {
     A.owned.push_back(q);
     A.out = (float *)q;
     if (r) return LEPIC_ECUDA;
-    NCUDA(cudaMemsetAsync(A.x, 0, p0 * 16 * sizeof(bf16), net->stream));
+    NCUDA(cudaMemsetAsync(A.x, 0, p0 * 2 * sizeof(bf16), net->stream));
     return LEPIC_OK;
 }
 
@@ -821,7 +906,7 @@ static void acts_free(Acts &A) {
 static int net_forward(CnnNet *net, Acts &A) {
     const int N = A.N, H = A.H, W = A.W;
     int r;
-    if ((r = fwd_relu(net, 0, A.x, IN_DIRECT, N, H, W, A.e0a, nullptr, nullptr))) return r;
+    if ((r = fwd_relu(net, 0, A.x, IN_X2, N, H, W, A.e0a, nullptr, nullptr))) return r;
     if ((r = fwd_relu(net, 1, A.e0a, IN_DIRECT, N, H, W, A.e0, nullptr, nullptr))) return r;
     if ((r = fwd_relu(net, 2, A.e0, IN_POOL, N, H / 2, W / 2, A.e1a, nullptr, nullptr))) return r;
     if ((r = fwd_relu(net, 3, A.e1a, IN_DIRECT, N, H / 2, W / 2, A.e1, nullptr, nullptr))) return r;
@@ -883,7 +968,7 @@ static int net_backward(CnnNet *net, Acts &A) {
     k_merge<<<elem_grid(net, p0 * 2), 256, 0, net->stream>>>(A.gd0, A.gp1, A.e0, N, H, W, 16, A.ge0);
     if ((r = bwd_weights(net, 1, A.e0a, IN_DIRECT, A.ge0, N, H, W))) return r;
     if ((r = bwd_data(net, 1, A.ge0, N, H, W, A.ge0a, A.e0a, nullptr))) return r;
-    if ((r = bwd_weights(net, 0, A.x, IN_DIRECT, A.ge0a, N, H, W))) return r;
+    if ((r = bwd_weights(net, 0, A.x, IN_X2, A.ge0a, N, H, W))) return r;
     NCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
@@ -892,7 +977,7 @@ static int net_loss(CnnNet *net, Acts &A) {
     const long long np = (long long)A.N * A.H * A.W;
     const int grid = std::min(grid_for(np, 256, net->num_sms), 1024);
     k_loss<<<grid, 256, 0, net->stream>>>(A.out, A.t, A.m, A.N, A.H, A.W, A.G, net->lpart);
-    k_sum_partials<<<1, 32, 0, net->stream>>>(net->lpart, grid, net->dsum);
+    k_sum_partials<<<1, 256, 0, net->stream>>>(net->lpart, grid, net->dsum);
     NCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
@@ -1085,12 +1170,9 @@ extern "C" int lepic_cnn_loss_grad(void *p, const float *x, const float *t, cons
         if ((r = ensure_part(net, N, H, W))) return r;
     }
     const size_t np = (size_t)N * H * W;
-    std::vector<bf16> hx(np * 16, __float2bfloat16_rn(0.0f));
-    for (size_t k = 0; k < np; k++) {
-        hx[k * 16 + 0] = __float2bfloat16_rn(x[2 * k]);
-        hx[k * 16 + 1] = __float2bfloat16_rn(x[2 * k + 1]);
-    }
-    NCUDA(cudaMemcpyAsync(A.x, hx.data(), np * 16 * sizeof(bf16), cudaMemcpyHostToDevice, net->stream));
+    std::vector<bf16> hx(np * 2);
+    for (size_t k = 0; k < np * 2; k++) hx[k] = __float2bfloat16_rn(x[k]);
+    NCUDA(cudaMemcpyAsync(A.x, hx.data(), np * 2 * sizeof(bf16), cudaMemcpyHostToDevice, net->stream));
     std::vector<uint8_t> hm(np, 1);
     if (t) NCUDA(cudaMemcpyAsync(A.t, t, np * sizeof(float), cudaMemcpyHostToDevice, net->stream));
     if (m) {
@@ -1144,18 +1226,17 @@ struct PrepP {
 // r0 = b - A u at unknown nodes (FP64, the solver's operator) into rbuf; sum r0^2 per block
 __global__ void k_prep_resid(PrepP P, float *rbuf, double *partial) {
     __shared__ double red[256];
-    const long long tot = (long long)P.Hc * P.Wc;
+    const int tot = P.Hc * P.Wc;
     const int W = P.nx + 3;
     double acc = 0.0;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < tot; p += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(p % P.Wc), y = (int)(p / P.Wc);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < tot; p += gridDim.x * blockDim.x) {
+        const int y = p / P.Wc, x = p - y * P.Wc;
         float rv = 0.0f;
         if (x <= P.nx && y <= P.ny) {
-            const int i = x + 1, j = y + 1;
-            const long long n = i + (long long)j * W;
+            const int n = (x + 1) + (y + 1) * W;
             if (P.bc[n] <= 0) {
                 const double *u = P.u;
-                const double r = P.b[x + (long long)y * (P.nx + 1)] -
+                const double r = P.b[x + y * (P.nx + 1)] -
                                  (P.aw * u[n - 1] + P.an * u[n + W] + P.an * u[n - W] + P.aw * u[n + 1] + P.ac * u[n]);
                 acc += r * r;
                 rv = (float)r;
@@ -1173,39 +1254,36 @@ __global__ void k_prep_resid(PrepP P, float *rbuf, double *partial) {
 }
 
 // sums the partials (fixed order); scal[0] = ||r||^2, scal[1] = sigma = rms over unknowns
-__global__ void k_prep_sigma(const double *partial, int n, double count, double *scal) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < n; k++) s += partial[k];
+__global__ void __launch_bounds__(256) k_prep_sigma(const double *partial, int n, double count, double *scal) {
+    const double s = block_sum256(partial, n);
+    if (threadIdx.x == 0) {
         scal[0] = s;
         scal[1] = sqrt(s / count);
     }
 }
 
-// network input: channel 0 = r0 / sigma, channel 1 = u / u_scale, channels 2..15 = 0
+// network input: channel 0 = r0 / sigma, channel 1 = u / u_scale
 __global__ void k_prep_input(PrepP P, const float *rbuf, const double *scal, double u_scale, bf16 *xin) {
-    const long long tot = (long long)P.Hc * P.Wc;
+    const int tot = P.Hc * P.Wc;
     const double sig = scal[1];
     const float inv_s = sig > 0.0 ? (float)(1.0 / sig) : 0.0f;
     const float inv_u = (float)(1.0 / u_scale);
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < tot; p += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(p % P.Wc), y = (int)(p / P.Wc);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < tot; p += gridDim.x * blockDim.x) {
+        const int y = p / P.Wc, x = p - y * P.Wc;
         float uv = 0.0f;
-        if (x <= P.nx && y <= P.ny) uv = (float)P.u[(x + 1) + (long long)(y + 1) * (P.nx + 3)] * inv_u;
-        uint4 *dst = reinterpret_cast<uint4 *>(xin + p * 16);
-        dst[0] = make_uint4(f2_to_bf2(rbuf[p] * inv_s, uv), 0u, 0u, 0u);
-        dst[1] = make_uint4(0u, 0u, 0u, 0u);
+        if (x <= P.nx && y <= P.ny) uv = (float)P.u[(x + 1) + (y + 1) * (P.nx + 3)] * inv_u;
+        reinterpret_cast<uint32_t *>(xin)[p] = f2_to_bf2(rbuf[p] * inv_s, uv);
     }
 }
 
 // u += out * sigma / |ac| at unknown nodes (the network's correction, applied in FP64)
 __global__ void k_apply(PrepP P, const float *out, const double *scal, double *u) {
-    const long long tot = (long long)(P.nx + 1) * (P.ny + 1);
+    const int tot = (P.nx + 1) * (P.ny + 1);
     const double f = scal[1] / fabs(P.ac);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (P.nx + 1)), y = (int)(t / (P.nx + 1));
-        const long long n = (x + 1) + (long long)(y + 1) * (P.nx + 3);
-        if (P.bc[n] <= 0) u[n] += (double)out[(long long)y * P.Wc + x] * f;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+        const int y = t / (P.nx + 1), x = t - y * (P.nx + 1);
+        const int n = (x + 1) + (y + 1) * (P.nx + 3);
+        if (P.bc[n] <= 0) u[n] += (double)out[y * P.Wc + x] * f;
     }
 }
 
@@ -1359,7 +1437,7 @@ int learned_solve(lepic_ctx *c, double eps) {
     const double count = c->n_unknown > 0 ? (double)c->n_unknown : 1.0; // counted at create
     LCUDA(cudaMemcpyAsync(L->uprev, c->phi, sizeof(double) * c->nn, cudaMemcpyDeviceToDevice, c->stream));
     k_prep_resid<<<g, 256, 0, c->stream>>>(P, L->rbuf, L->partial);
-    k_prep_sigma<<<1, 32, 0, c->stream>>>(L->partial, g, count, L->scal);
+    k_prep_sigma<<<1, 256, 0, c->stream>>>(L->partial, g, count, L->scal);
     k_prep_input<<<grid_for(np, 256, c->num_sms), 256, 0, c->stream>>>(P, L->rbuf, L->scal, L->u_scale, net->full.x);
     LCUDA(cudaGetLastError());
     r = net_forward(net, net->full);
@@ -1368,7 +1446,7 @@ int learned_solve(lepic_ctx *c, double eps) {
         P, net->full.out, L->scal, c->phi);
     // the new residual norm into scal[2]
     k_prep_resid<<<g, 256, 0, c->stream>>>(P, nullptr, L->partial);
-    k_prep_sigma<<<1, 32, 0, c->stream>>>(L->partial, g, count, L->scal + 2);
+    k_prep_sigma<<<1, 256, 0, c->stream>>>(L->partial, g, count, L->scal + 2);
     k_accept<<<grid_for(c->nn, 256, c->num_sms), 256, 0, c->stream>>>(P, L->scal, L->uprev, c->phi, L->accepted);
     LCUDA(cudaGetLastError());
     r = mg_mixed_solve(c, eps);
