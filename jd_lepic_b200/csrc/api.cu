@@ -69,6 +69,10 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         c->last_err = "invalid configuration";
         return LEPIC_EINVAL;
     }
+    if ((long long)(g.nx + 3) * (g.ny + 3) >= (1ll << 30)) { // node indices are 32-bit in the solvers
+        c->last_err = "grid too large: (nx+3)*(ny+3) must stay below 2^30 nodes";
+        return LEPIC_EINVAL;
+    }
     if ((g.nx % (1 << (g.ng - 1))) != 0 || (g.ny % (1 << (g.ng - 1))) != 0) {
         c->last_err = "nx and ny must be divisible by 2^(ng-1) (main.f90:268-277)";
         return LEPIC_EINVAL;

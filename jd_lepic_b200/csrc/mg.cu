@@ -45,17 +45,15 @@ __device__ void half_sweep(const Team &T, const MGDev &L, int color, double omeg
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
     const int hw = nx / 2 + 1;
-    const long long tot = (long long)(ny + 1) * hw;
-    for (long long w = T.rank(); w < tot; w += T.size()) {
-        int j = (int)(w / hw) + 1;
-        int k = (int)(w % hw);
-        int is = (((j + 1 + color) & 1) != 0) ? 1 : 2;
-        int i = is + 2 * k;
+    for (Walk2 w(T.rank(), T.size(), hw, ny + 1); w.ok(); w.next()) {
+        const int j = w.j + 1;
+        const int is = (((j + 1 + color) & 1) != 0) ? 1 : 2;
+        const int i = is + 2 * w.k;
         if (i > nx + 1) continue;
-        const long long n = i + (long long)j * W;
+        const int n = i + j * W;
         int bc = L.bc[n];
         if (bc > 0) continue;
-        double bij = L.b[(i - 1) + (long long)(j - 1) * (nx + 1)];
+        double bij = L.b[(i - 1) + (j - 1) * (nx + 1)];
         double *u = L.u;
         if (bc == -2) {
             u[n] = (1.0 - omega) * u[n] + omega * (bij - an * u[n + W] - as * u[n - W] - 2.0 * ae * u[n + 1]) / ac;
@@ -71,9 +69,9 @@ __device__ void half_sweep(const Team &T, const MGDev &L, int color, double omeg
 template <class Team>
 __device__ void pbc_rows(const Team &T, const MGDev &L) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
-    for (long long i = T.rank(); i <= nx + 2; i += T.size()) {
-        if (L.bc[i + 1 * W] <= 0) L.u[i] = L.u[i + (long long)ny * W];
-        if (L.bc[i + (long long)(ny + 1) * W] <= 0) L.u[i + (long long)(ny + 1) * W] = L.u[i + W];
+    for (int i = (int)T.rank(); i <= nx + 2; i += (int)T.size()) {
+        if (L.bc[i + 1 * W] <= 0) L.u[i] = L.u[i + ny * W];
+        if (L.bc[i + (ny + 1) * W] <= 0) L.u[i + (ny + 1) * W] = L.u[i + W];
     }
 }
 
@@ -82,11 +80,10 @@ template <class Team>
 __device__ bool residual_l1(const Team &T, const MGDev &L, double *res) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double acc = 0.0;
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx + 1)) + 1, j = (int)(t / (nx + 1)) + 1;
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(T.rank(), T.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int n = (w.k + 1) + (w.j + 1) * W;
         double rij = 0.0;
         if (L.bc[n] == -1) {
             const double *u = L.u;
@@ -134,7 +131,7 @@ __device__ __forceinline__ double getres(const MGDev &L, int ir, int jr, int fla
     const int W = L.nx + 3;
     double aw = L.aw, ae = L.aw, an = L.an, as = L.an;
     const double ac = L.ac;
-    const long long n = ir + (long long)jr * W;
+    const int n = ir + jr * W;
     const double *u = L.u;
     double uij = u[n], un = u[n + W], us = u[n - W], ue = u[n + 1], uw;
     if (ir == 1 && flag == 1) {
@@ -144,7 +141,7 @@ __device__ __forceinline__ double getres(const MGDev &L, int ir, int jr, int fla
     } else {
         uw = u[n - 1];
     }
-    double urhs = L.b[(ir - 1) + (long long)(jr - 1) * (L.nx + 1)];
+    double urhs = L.b[(ir - 1) + (jr - 1) * (L.nx + 1)];
     return urhs - (aw * uw + ae * ue + an * un + as * us + ac * uij);
 }
 
@@ -152,9 +149,9 @@ __device__ __forceinline__ double getres(const MGDev &L, int ir, int jr, int fla
 __device__ __forceinline__ double r_pbc(const MGDev &F, int x, int nmn) {
     const int W = F.nx + 3, ny = F.ny;
     bool set;
-    if (x & 1) set = F.bc[x + (long long)(ny + 1) * W] <= 0;
-    else set = (x - 1 >= 1 && F.bc[x - 1 + (long long)(ny + 1) * W] <= 0) ||
-               (x + 1 <= F.nx + 1 && F.bc[x + 1 + (long long)(ny + 1) * W] <= 0);
+    if (x & 1) set = F.bc[x + (ny + 1) * W] <= 0;
+    else set = (x - 1 >= 1 && F.bc[x - 1 + (ny + 1) * W] <= 0) ||
+               (x + 1 <= F.nx + 1 && F.bc[x + 1 + (ny + 1) * W] <= 0);
     return set ? getres(F, x, ny, nmn) : 0.0;
 }
 
@@ -163,15 +160,15 @@ __device__ __forceinline__ double r_pbc(const MGDev &F, int x, int nmn) {
 template <class Team>
 __device__ void restriction(const Team &T, const MGDev &F, const MGDev &C, int pbc, int nmn) {
     const int nx = F.nx, ny = F.ny, W = nx + 3, nx2 = C.nx, ny2 = C.ny, W2 = nx2 + 3;
-    const long long tot = (long long)(nx2 + 1) * (ny2 + 1);
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx2 + 1)) + 1, j = (int)(t / (nx2 + 1)) + 1;
+    for (Walk2 w(T.rank(), T.size(), nx2 + 1, ny2 + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int i = w.k + 1, j = w.j + 1;
         int ir = 2 * i - 1, jr = 2 * j - 1;
         double out = 0.0;
-        if (C.bc[i + (long long)j * W2] <= 0) {
+        if (C.bc[i + j * W2] <= 0) {
             double r1 = 0, r2 = 0, r3 = 0, r4 = 0, r5 = 0, r6 = 0, r7 = 0, r8 = 0, r9 = 0;
             const int8_t *bc = F.bc;
-#define FB(a, b) bc[(a) + (long long)(b) * W]
+#define FB(a, b) bc[(a) + (b) * W]
             r9 = getres(F, ir, jr, nmn);
             if (ir != nx + 1 && jr != ny + 1)
                 if (FB(ir + 1, jr + 1) <= 0) r1 = getres(F, ir + 1, jr + 1, nmn);
@@ -200,24 +197,23 @@ __device__ void restriction(const Team &T, const MGDev &F, const MGDev &C, int p
         }
         C.b[t] = out;
     }
-    const long long tot2 = (long long)W2 * (ny2 + 3);
-    for (long long t = T.rank(); t < tot2; t += T.size()) C.u[t] = 0.0;
+    const int tot2 = W2 * (ny2 + 3);
+    for (int t = (int)T.rank(); t < tot2; t += (int)T.size()) C.u[t] = 0.0;
 }
 
 // mg.f90:549-616 (each fine node has exactly one writer)
 template <class Team>
 __device__ void prolongation(const Team &T, const MGDev &C, const MGDev &F) {
     const int W = F.nx + 3, nx2 = C.nx, ny2 = C.ny, W2 = nx2 + 3;
-    const long long tot = (long long)(nx2 + 1) * (ny2 + 1);
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx2 + 1)) + 1, j = (int)(t / (nx2 + 1)) + 1;
+    for (Walk2 w(T.rank(), T.size(), nx2 + 1, ny2 + 1); w.ok(); w.next()) {
+        const int i = w.k + 1, j = w.j + 1;
         const double *e = C.u;
-        double r1 = e[i + (long long)j * W2], r2 = e[i + (long long)(j - 1) * W2];
-        double r3 = e[i - 1 + (long long)(j - 1) * W2], r4 = e[i - 1 + (long long)j * W2];
+        double r1 = e[i + j * W2], r2 = e[i + (j - 1) * W2];
+        double r3 = e[i - 1 + (j - 1) * W2], r4 = e[i - 1 + j * W2];
         int ir = 2 * i - 1, jr = 2 * j - 1;
         double *u = F.u;
         const int8_t *bc = F.bc;
-        long long n = ir + (long long)jr * W;
+        const int n = ir + jr * W;
         if (bc[n] <= 0) u[n] = u[n] + r1;
         if (bc[n - W] <= 0) u[n - W] = u[n - W] + (r1 + r2) / 2.0;
         if (bc[n - W - 1] <= 0) u[n - W - 1] = u[n - W - 1] + (r1 + r2 + r3 + r4) / 4.0;
@@ -298,11 +294,10 @@ template <class Team>
 __device__ bool l2_norms(const Team &T, const MGDev &L, double *rr, double *bb) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double a = 0.0, b = 0.0;
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx + 1)) + 1, j = (int)(t / (nx + 1)) + 1;
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(T.rank(), T.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int n = (w.k + 1) + (w.j + 1) * W;
         if (L.bc[n] != -1) continue;
         const double *u = L.u;
         const int8_t *bc = L.bc;
@@ -409,7 +404,7 @@ int mg_init(lepic_ctx *c) {
     int occ = 0;
     LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_solve, MG_THREADS, 0));
     if (occ < 1) { c->last_err = "multigrid kernel does not fit on an SM"; return LEPIC_ECUDA; }
-    int per_sm = 2;
+    int per_sm = 3;
     if (const char *e = getenv("LEPIC_MG_CTAS_PER_SM")) per_sm = atoi(e);
     c->mg_grid = c->num_sms * std::max(1, std::min(occ, per_sm));
     return LEPIC_OK;

@@ -11,7 +11,8 @@
 // Teams: the whole grid (grid barrier) or CTA 0 alone (block barrier).
 struct BigTeam {
     DevCounters *c;
-    double *partials;
+    double *partials;          // 2 * gridDim.x doubles
+    mutable unsigned phase = 0;
     __device__ long long rank() const { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
     __device__ long long size() const { return (long long)gridDim.x * blockDim.x; }
     __device__ bool sync() const { return grid_barrier(c, gridDim.x); }
@@ -20,6 +21,30 @@ struct SmallTeam {
     __device__ long long rank() const { return threadIdx.x; }
     __device__ long long size() const { return blockDim.x; }
     __device__ bool sync() const { __syncthreads(); return true; }
+};
+
+// Grid-stride walk over the (row, column) pairs of a rows x width index range without a
+// division per element: the stride is split once into whole rows and a remainder, and the pair
+// advances incrementally (flat index = row * width + column).
+struct Walk2 {
+    int j, k, dj, dk, width, rows;
+    __device__ __forceinline__ Walk2(long long rank, long long size, int width_, int rows_)
+        : width(width_), rows(rows_) {
+        const long long tot = (long long)width_ * rows_;
+        if (rank >= tot) { j = rows_; k = 0; dj = dk = 0; return; }
+        j = (int)(rank / width_);
+        k = (int)(rank - (long long)j * width_);
+        const long long st = size < tot ? size : tot;
+        dj = (int)(st / width_);
+        dk = (int)(st - (long long)dj * width_);
+    }
+    __device__ __forceinline__ bool ok() const { return j < rows; }
+    __device__ __forceinline__ void next() {
+        k += dk;
+        j += dj;
+        if (k >= width) { k -= width; j++; }
+    }
+    __device__ __forceinline__ int flat() const { return j * width + k; }
 };
 
 // fixed-order block sum; every thread gets the result
@@ -39,14 +64,18 @@ __device__ __forceinline__ double block_sum(double v) {
     return r;
 }
 
+// Consecutive sums alternate between two halves of `partials` (2 * gridDim.x doubles), so a CTA
+// that runs ahead into the next sum never overwrites a partial another CTA is still reading.
 __device__ __forceinline__ bool team_sum(const BigTeam &T, double v, double *out) {
     double b = block_sum(v);
-    if (threadIdx.x == 0) T.partials[blockIdx.x] = b;
+    double *part = T.partials + (T.phase & 1) * gridDim.x;
+    T.phase++;
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
     if (!T.sync()) return false;
     __shared__ double s_tot;
     if (threadIdx.x < 32) {
         double a = 0.0;
-        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) a = a + ((volatile double *)T.partials)[i];
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) a = a + ((volatile double *)part)[i];
         for (int o = 16; o > 0; o >>= 1) a = a + __shfl_xor_sync(0xffffffffu, a, o);
         if (threadIdx.x == 0) s_tot = a;
     }

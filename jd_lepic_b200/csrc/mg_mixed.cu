@@ -52,16 +52,14 @@ __device__ void sweep32(const Team &T, const MXL &L, int color, float omega) {
     const float aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
     const float inv_ac = 1.0f / ac;
     const int hw = nx / 2 + 1;
-    const long long tot = (long long)(ny + 1) * hw;
-    for (long long w = T.rank(); w < tot; w += T.size()) {
-        int j = (int)(w / hw) + 1;
-        int k = (int)(w % hw);
-        int i = ((((j + 1 + color) & 1) != 0) ? 1 : 2) + 2 * k;
+    for (Walk2 w(T.rank(), T.size(), hw, ny + 1); w.ok(); w.next()) {
+        const int j = w.j + 1;
+        const int i = ((((j + 1 + color) & 1) != 0) ? 1 : 2) + 2 * w.k;
         if (i > nx + 1) continue;
-        const long long n = i + (long long)j * W;
+        const int n = i + j * W;
         const int bc = L.bc[n];
         if (bc > 0) continue;
-        const float rij = L.r[(i - 1) + (long long)(j - 1) * (nx + 1)];
+        const float rij = L.r[(i - 1) + (j - 1) * (nx + 1)];
         float *e = L.e;
         float s;
         if (bc == -2) {
@@ -77,9 +75,9 @@ __device__ void sweep32(const Team &T, const MXL &L, int color, float omega) {
 template <class Team>
 __device__ void pbc32(const Team &T, const MXL &L) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
-    for (long long i = T.rank(); i <= nx + 2; i += T.size()) {
-        if (L.bc[i + 1 * W] <= 0) L.e[i] = L.e[i + (long long)ny * W];
-        if (L.bc[i + (long long)(ny + 1) * W] <= 0) L.e[i + (long long)(ny + 1) * W] = L.e[i + W];
+    for (int i = (int)T.rank(); i <= nx + 2; i += (int)T.size()) {
+        if (L.bc[i + 1 * W] <= 0) L.e[i] = L.e[i + ny * W];
+        if (L.bc[i + (ny + 1) * W] <= 0) L.e[i + (ny + 1) * W] = L.e[i + W];
     }
 }
 
@@ -104,21 +102,21 @@ __device__ __forceinline__ float getres32(const MXL &L, int ir, int jr, int flag
     const int W = L.nx + 3;
     float aw = L.aw, ae = L.aw;
     const float an = L.an, as = L.an, ac = L.ac;
-    const long long n = ir + (long long)jr * W;
+    const int n = ir + jr * W;
     const float *e = L.e;
     float uw;
     if (ir == 1 && flag == 1) { uw = 0.0f; aw = 0.0f; ae = 2.0f * ae; }
     else uw = e[n - 1];
-    return L.r[(ir - 1) + (long long)(jr - 1) * (L.nx + 1)] -
+    return L.r[(ir - 1) + (jr - 1) * (L.nx + 1)] -
            (aw * uw + ae * e[n + 1] + an * e[n + W] + as * e[n - W] + ac * e[n]);
 }
 
 __device__ __forceinline__ float rpbc32(const MXL &F, int x, int nmn) {
     const int W = F.nx + 3, ny = F.ny;
     bool set;
-    if (x & 1) set = F.bc[x + (long long)(ny + 1) * W] <= 0;
-    else set = (x - 1 >= 1 && F.bc[x - 1 + (long long)(ny + 1) * W] <= 0) ||
-               (x + 1 <= F.nx + 1 && F.bc[x + 1 + (long long)(ny + 1) * W] <= 0);
+    if (x & 1) set = F.bc[x + (ny + 1) * W] <= 0;
+    else set = (x - 1 >= 1 && F.bc[x - 1 + (ny + 1) * W] <= 0) ||
+               (x + 1 <= F.nx + 1 && F.bc[x + 1 + (ny + 1) * W] <= 0);
     return set ? getres32(F, x, ny, nmn) : 0.0f;
 }
 
@@ -126,14 +124,14 @@ __device__ __forceinline__ float rpbc32(const MXL &F, int x, int nmn) {
 template <class Team>
 __device__ void restrict32(const Team &T, const MXL &F, const MXL &C, int pbc, int nmn) {
     const int nx = F.nx, ny = F.ny, W = nx + 3, nx2 = C.nx, ny2 = C.ny, W2 = nx2 + 3;
-    const long long tot = (long long)(nx2 + 1) * (ny2 + 1);
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx2 + 1)) + 1, j = (int)(t / (nx2 + 1)) + 1;
+    for (Walk2 w(T.rank(), T.size(), nx2 + 1, ny2 + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int i = w.k + 1, j = w.j + 1;
         int ir = 2 * i - 1, jr = 2 * j - 1;
         float out = 0.0f;
-        if (C.bc[i + (long long)j * W2] <= 0) {
+        if (C.bc[i + j * W2] <= 0) {
             const int8_t *bc = F.bc;
-#define FB(a, b) bc[(a) + (long long)(b) * W]
+#define FB(a, b) bc[(a) + (b) * W]
             float r1 = 0, r2 = 0, r3 = 0, r4 = 0, r5 = 0, r6 = 0, r7 = 0, r8 = 0;
             float r9 = getres32(F, ir, jr, nmn);
             if (ir != nx + 1 && jr != ny + 1 && FB(ir + 1, jr + 1) <= 0) r1 = getres32(F, ir + 1, jr + 1, nmn);
@@ -158,20 +156,19 @@ __device__ void restrict32(const Team &T, const MXL &F, const MXL &C, int pbc, i
         }
         C.r[t] = out;
     }
-    const long long tot2 = (long long)W2 * (ny2 + 3);
-    for (long long t = T.rank(); t < tot2; t += T.size()) C.e[t] = 0.0f;
+    const int tot2 = W2 * (ny2 + 3);
+    for (int t = (int)T.rank(); t < tot2; t += (int)T.size()) C.e[t] = 0.0f;
 }
 
 template <class Team>
 __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
     const int W = F.nx + 3, nx2 = C.nx, ny2 = C.ny, W2 = nx2 + 3;
-    const long long tot = (long long)(nx2 + 1) * (ny2 + 1);
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx2 + 1)) + 1, j = (int)(t / (nx2 + 1)) + 1;
+    for (Walk2 w(T.rank(), T.size(), nx2 + 1, ny2 + 1); w.ok(); w.next()) {
+        const int i = w.k + 1, j = w.j + 1;
         const float *e = C.e;
-        float r1 = e[i + (long long)j * W2], r2 = e[i + (long long)(j - 1) * W2];
-        float r3 = e[i - 1 + (long long)(j - 1) * W2], r4 = e[i - 1 + (long long)j * W2];
-        long long n = (2 * i - 1) + (long long)(2 * j - 1) * W;
+        float r1 = e[i + j * W2], r2 = e[i + (j - 1) * W2];
+        float r3 = e[i - 1 + (j - 1) * W2], r4 = e[i - 1 + j * W2];
+        const int n = (2 * i - 1) + (2 * j - 1) * W;
         float *u = F.e;
         const int8_t *bc = F.bc;
         if (bc[n] <= 0) u[n] += r1;
@@ -198,18 +195,18 @@ __device__ void small_cycle(const MXP &P) {
     SmallTeam T;
     const int ng = P.ng, Ls = P.Ls;
     for (int l = Ls; l < ng; l++) {
-        const long long nn = (long long)(P.L[l].nx + 3) * (P.L[l].ny + 3);
+        const int nn = (P.L[l].nx + 3) * (P.L[l].ny + 3);
         int8_t *bcs = (int8_t *)(mx_smem + P.soff_b[l]);
         const int8_t *bcg = P.L[l].bc;
-        for (long long t = threadIdx.x; t < nn; t += blockDim.x) bcs[t] = bcg[t];
+        for (int t = threadIdx.x; t < nn; t += blockDim.x) bcs[t] = bcg[t];
     }
     {
         const MXL S = smem_level(P, mx_smem, Ls);
-        const long long nr = (long long)(S.nx + 1) * (S.ny + 1);
-        const long long nn = (long long)(S.nx + 3) * (S.ny + 3);
+        const int nr = (S.nx + 1) * (S.ny + 1);
+        const int nn = (S.nx + 3) * (S.ny + 3);
         const float *rg = P.L[Ls].r;
-        for (long long t = threadIdx.x; t < nr; t += blockDim.x) S.r[t] = rg[t];
-        for (long long t = threadIdx.x; t < nn; t += blockDim.x) S.e[t] = 0.0f;
+        for (int t = threadIdx.x; t < nr; t += blockDim.x) S.r[t] = rg[t];
+        for (int t = threadIdx.x; t < nn; t += blockDim.x) S.e[t] = 0.0f;
     }
     __syncthreads();
     for (int l = Ls; l <= ng - 2; l++) {
@@ -230,9 +227,9 @@ __device__ void small_cycle(const MXP &P) {
         smooth32(T, P, F, P.nu2, true);
     }
     const MXL S = smem_level(P, mx_smem, Ls);
-    const long long nn = (long long)(S.nx + 3) * (S.ny + 3);
+    const int nn = (S.nx + 3) * (S.ny + 3);
     float *eg = P.L[Ls].e;
-    for (long long t = threadIdx.x; t < nn; t += blockDim.x) eg[t] = S.e[t];
+    for (int t = threadIdx.x; t < nn; t += blockDim.x) eg[t] = S.e[t];
     __syncthreads();
 }
 
@@ -263,10 +260,6 @@ __device__ bool vcycle32(const MXP &P) {
     return true;
 }
 
-__device__ __forceinline__ void ij_of(long long t, int nx, int *i, int *j) {
-    *i = (int)(t % (nx + 1)) + 1;
-    *j = (int)(t / (nx + 1)) + 1;
-}
 
 // r = b - A u at unknowns (bcnd <= 0), zero elsewhere; r32 = (float) r; e = 0 (all nodes);
 // returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum
@@ -274,12 +267,11 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double a = 0.0, s1 = 0.0;
-    for (long long t = B.rank(); t < tot; t += B.size()) {
-        int i, j;
-        ij_of(t, nx, &i, &j);
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int i = w.k + 1, j = w.j + 1;
+        const int n = i + j * W;
         const int bc = L.bc[n];
         double r = 0.0;
         if (bc <= 0) {
@@ -290,11 +282,10 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
         P.r64[n] = r;
         L.r[t] = (float)r;
     }
-    const long long nn = (long long)W * (ny + 3);
-    for (long long t = B.rank(); t < nn; t += B.size()) {
+    for (Walk2 w(B.rank(), B.size(), W, ny + 3); w.ok(); w.next()) {
+        const int t = w.flat();
         L.e[t] = 0.0f;
-        int i = (int)(t % W), j = (int)(t / W);
-        if (i == 0 || j == 0 || i == nx + 2 || j == ny + 2) P.r64[t] = 0.0;
+        if (w.k == 0 || w.j == 0 || w.k == nx + 2 || w.j == ny + 2) P.r64[t] = 0.0;
     }
     if (!team_sum(B, a, rr)) return false;
     return team_sum(B, s1, l1);
@@ -303,17 +294,17 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
 // z = e (FP32 cycle output): returns r.z; if first, p = z else p = z + beta p (beta passed)
 __device__ bool dot_rz(const BigTeam &B, const MXP &P, double *rz) {
     const MXL &L = P.L[0];
-    const long long nn = (long long)(L.nx + 3) * (L.ny + 3);
+    const int nn = (L.nx + 3) * (L.ny + 3);
     double a = 0.0;
-    for (long long t = B.rank(); t < nn; t += B.size())
+    for (int t = (int)B.rank(); t < nn; t += (int)B.size())
         if (L.bc[t] <= 0) a += P.r64[t] * (double)L.e[t];
     return team_sum(B, a, rz);
 }
 
 __device__ void update_p(const BigTeam &B, const MXP &P, double beta, bool first) {
     const MXL &L = P.L[0];
-    const long long nn = (long long)(L.nx + 3) * (L.ny + 3);
-    for (long long t = B.rank(); t < nn; t += B.size()) {
+    const int nn = (L.nx + 3) * (L.ny + 3);
+    for (int t = (int)B.rank(); t < nn; t += (int)B.size()) {
         double z = L.bc[t] <= 0 ? (double)L.e[t] : 0.0;
         P.p64[t] = first ? z : z + beta * P.p64[t];
     }
@@ -324,12 +315,9 @@ __device__ bool apply_A(const BigTeam &B, const MXP &P, double *pap) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double a = 0.0;
-    for (long long t = B.rank(); t < tot; t += B.size()) {
-        int i, j;
-        ij_of(t, nx, &i, &j);
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int n = (w.k + 1) + (w.j + 1) * W;
         double v = 0.0;
         if (L.bc[n] <= 0) {
             const double *p = P.p64;
@@ -345,12 +333,10 @@ __device__ bool apply_A(const BigTeam &B, const MXP &P, double *pap) {
 __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *rr) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double a = 0.0;
-    for (long long t = B.rank(); t < tot; t += B.size()) {
-        int i, j;
-        ij_of(t, nx, &i, &j);
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int n = (w.k + 1) + (w.j + 1) * W;
         const int bc = L.bc[n];
         if (bc <= 0) {
             L.u[n] = L.u[n] + alpha * P.p64[n];
@@ -360,8 +346,8 @@ __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *
             if (bc == -1) a += r * r;
         }
     }
-    const long long nn = (long long)W * (ny + 3);
-    for (long long t = B.rank(); t < nn; t += B.size()) L.e[t] = 0.0f;
+    const int nn = W * (ny + 3);
+    for (int t = (int)B.rank(); t < nn; t += (int)B.size()) L.e[t] = 0.0f;
     return team_sum(B, a, rr);
 }
 
@@ -369,11 +355,10 @@ template <class Team>
 __device__ bool b0_norm(const Team &T, const MXL &L, double *bb) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
     double b = 0.0;
-    for (long long t = T.rank(); t < tot; t += T.size()) {
-        int i = (int)(t % (nx + 1)) + 1, j = (int)(t / (nx + 1)) + 1;
-        const long long n = i + (long long)j * W;
+    for (Walk2 w(T.rank(), T.size(), nx + 1, ny + 1); w.ok(); w.next()) {
+        const int t = w.flat();
+        const int n = (w.k + 1) + (w.j + 1) * W;
         if (L.bc[n] != -1) continue;
         const double *u = L.u;
         const int8_t *bc = L.bc;
@@ -490,7 +475,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
         int occ = 0;
         LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_mixed, MG_THREADS, smem));
         if (occ < 1) { c->last_err = "mixed multigrid kernel does not fit on an SM"; return LEPIC_ECUDA; }
-        int per_sm = 2;
+        int per_sm = 3;
         if (const char *e = getenv("LEPIC_MG_CTAS_PER_SM")) per_sm = atoi(e);
         c->mg_grid_mixed = c->num_sms * std::max(1, std::min(occ, per_sm));
     }
