@@ -27,7 +27,7 @@ SOURCES = {
     "api.cu": [],
     "field.cu": ["-fmad=false"],
     "mg.cu": ["-fmad=false"],
-    "mg_mixed.cu": [],
+    "mg_mixed.cu": ["-fmad=false"],
     "push.cu": [],
     "sort.cu": [],
     "mcc.cu": [],

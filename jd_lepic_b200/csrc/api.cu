@@ -49,7 +49,7 @@ static void free_all(lepic_ctx *c) {
     F(c->keys); F(c->perm); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
     for (int l = 0; l < c->nlev; l++) {
         if (l > 0) { F(c->lev[l].u); F(c->lev[l].b); F(c->lev[l].bc); }
-        F(c->lev[l].e32); F(c->lev[l].r32);
+        F(c->lev[l].e32); F(c->lev[l].e32b); F(c->lev[l].r32);
     }
     F(c->partials);
     F(c->cg_r); F(c->cg_p); F(c->cg_ap);
@@ -196,8 +196,9 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
             LCUDA(cudaMemcpy(L.bc, cur.data(), nnl, cudaMemcpyHostToDevice));
             prev.swap(cur);
         }
-        LALLOC(L.e32, nnl); LALLOC(L.r32, (size_t)(L.nx + 1) * (L.ny + 1));
+        LALLOC(L.e32, nnl); LALLOC(L.e32b, nnl); LALLOC(L.r32, (size_t)(L.nx + 1) * (L.ny + 1));
         LCUDA(cudaMemset(L.e32, 0, sizeof(float) * nnl));
+        LCUDA(cudaMemset(L.e32b, 0, sizeof(float) * nnl));
         LCUDA(cudaMemset(L.r32, 0, sizeof(float) * (L.nx + 1) * (L.ny + 1)));
     }
     LALLOC(c->partials, (size_t)c->num_sms * 32);

@@ -65,6 +65,7 @@ struct MGLevel {
     double *b;       // (nx+1)(ny+1)
     int8_t *bc;      // (nx+3)(ny+3), bcnd clamped to [-4, 1]
     float *e32;      // mixed precision correction (nx+3)(ny+3)
+    float *e32b;     // the pre-smoothed correction of the tiled V-cycle (ping-pong partner)
     float *r32;      // mixed precision right-hand side (nx+1)(ny+1)
 };
 

@@ -28,15 +28,17 @@ struct SmallTeam {
 // advances incrementally (flat index = row * width + column).
 struct Walk2 {
     int j, k, dj, dk, width, rows;
-    __device__ __forceinline__ Walk2(long long rank, long long size, int width_, int rows_)
+    // 32-bit throughout: team sizes and node counts stay below 2^31 (checked at create)
+    __device__ __forceinline__ Walk2(long long rank_, long long size_, int width_, int rows_)
         : width(width_), rows(rows_) {
-        const long long tot = (long long)width_ * rows_;
+        const unsigned rank = (unsigned)rank_, size = (unsigned)size_, w = (unsigned)width_;
+        const unsigned tot = w * (unsigned)rows_;
         if (rank >= tot) { j = rows_; k = 0; dj = dk = 0; return; }
-        j = (int)(rank / width_);
-        k = (int)(rank - (long long)j * width_);
-        const long long st = size < tot ? size : tot;
-        dj = (int)(st / width_);
-        dk = (int)(st - (long long)dj * width_);
+        j = (int)(rank / w);
+        k = (int)(rank - (unsigned)j * w);
+        const unsigned st = size < tot ? size : tot;
+        dj = (int)(st / w);
+        dk = (int)(st - (unsigned)dj * w);
     }
     __device__ __forceinline__ bool ok() const { return j < rows; }
     __device__ __forceinline__ void next() {

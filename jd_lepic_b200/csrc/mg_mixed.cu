@@ -28,6 +28,7 @@ struct MXL {
     float aw, an, ac;         // FP32 stencil of this level
     double awd, and_, acd;    // FP64 stencil (finest level only)
     float *e, *r;
+    float *e2;                // tiled cycle: the pre-smoothed e between the down and up passes
     const int8_t *bc;
     double *u, *b;
 };
@@ -44,6 +45,8 @@ struct MXP {
     DevCounters *cnt;
     int soff_e[LEPIC_MAXLEV], soff_r[LEPIC_MAXLEV], soff_b[LEPIC_MAXLEV]; // shared-memory copies
     int smem_bytes;
+    int tiled;       // 1: the big levels smooth in shared-memory tiles (temporal blocking)
+    int tile_cap;    // nodes a tile region may hold
 };
 
 template <class Team>
@@ -179,6 +182,252 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
 }
 
 
+// ---------------------------------------------------------------------------------------
+// Temporal blocking of the big levels.  A CTA takes a TX x TY tile of updatable nodes, loads
+// e, r and the mask of the tile plus a halo of H nodes into shared memory, and runs all K
+// half-sweeps of a smoothing stage there: half-sweep h updates the nodes at least h + 1 nodes
+// inside the (unclamped) region, so after K half-sweeps the tile itself holds exactly the
+// values the grid-wide sweeps would produce (every node sees the same operations in the same
+// colour order).  Down: smoothing then the restriction of the coarse nodes whose fine centre
+// lies in the tile (H = K + 2).  Up: the prolongation of the region, then smoothing (H = K).
+// One grid barrier per level and direction instead of one per half-sweep.  Tiles read their
+// halo from one buffer and write their result to the other (e -> e2 down, e2 -> e up), so a
+// tile never sees a neighbour's finished values.
+#define MX_TX 64
+#define MX_TY 32
+
+struct Region {
+    int i0, j0, i1, j1;      // tile interior [i0, i1) x [j0, j1) (updatable nodes)
+    int ri0, rj0, RW, RH;    // region origin and size (clamped to the node array)
+    int H;
+    float *e, *r;
+    int8_t *b;
+    float *ce;               // the coarse nodes the region's prolongation reads
+    __device__ __forceinline__ int at(int i, int j) const { return (i - ri0) + (j - rj0) * RW; }
+};
+
+__device__ __forceinline__ Region make_region(const MXL &L, int tile, int H, unsigned char *smem, int cap) {
+    Region g;
+    const int nx = L.nx, ny = L.ny;
+    const int ntx = (nx + 1 + MX_TX - 1) / MX_TX;
+    const int ti = tile % ntx, tj = tile / ntx;
+    g.i0 = 1 + ti * MX_TX;
+    g.j0 = 1 + tj * MX_TY;
+    g.i1 = min(g.i0 + MX_TX, nx + 2);
+    g.j1 = min(g.j0 + MX_TY, ny + 2);
+    g.H = H;
+    g.ri0 = max(g.i0 - H, 0);
+    g.rj0 = max(g.j0 - H, 0);
+    g.RW = min(g.i1 + H, nx + 3) - g.ri0;
+    g.RH = min(g.j1 + H, ny + 3) - g.rj0;
+    g.e = (float *)smem;
+    g.r = g.e + cap;
+    g.b = (int8_t *)(g.r + cap);
+    g.ce = (float *)((int8_t *)g.b + cap);   // cap is a multiple of 4
+    return g;
+}
+
+#define MX_BATCH 4   // elements per thread whose loads are all issued before their stores
+
+// e (from e_src, or zeros when e_src is null), mask and (at updatable nodes) r of the region
+// into shared memory, MX_BATCH elements per thread per round with all loads issued first
+__device__ __forceinline__ void region_load(const MXL &L, const float *e_src, const Region &g) {
+    const int W = L.nx + 3;
+    Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH);
+    while (w.ok()) {
+        int q[MX_BATCH];
+        float ev[MX_BATCH], rv[MX_BATCH];
+        int bv[MX_BATCH];
+#pragma unroll
+        for (int u = 0; u < MX_BATCH; u++) {
+            q[u] = -1;
+            if (w.ok()) {
+                const int i = g.ri0 + w.k, j = g.rj0 + w.j;
+                const int n = i + j * W;
+                q[u] = w.flat();
+                ev[u] = e_src ? e_src[n] : 0.0f;
+                bv[u] = L.bc[n];
+                rv[u] = (i >= 1 && i <= L.nx + 1 && j >= 1 && j <= L.ny + 1) ? L.r[(i - 1) + (j - 1) * (L.nx + 1)]
+                                                                              : 0.0f;
+                w.next();
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < MX_BATCH; u++)
+            if (q[u] >= 0) {
+                g.e[q[u]] = ev[u];
+                g.b[q[u]] = (int8_t)bv[u];
+                g.r[q[u]] = rv[u];
+            }
+    }
+}
+
+// the coarse nodes (ci0.., cj0..) the prolongation of the region reads, into g.ce
+__device__ __forceinline__ void coarse_load(const MXL &C, const Region &g, int ci0, int cj0, int CW, int CH) {
+    const int W2 = C.nx + 3;
+    Walk2 w(threadIdx.x, blockDim.x, CW, CH);
+    while (w.ok()) {
+        int q[MX_BATCH];
+        float v[MX_BATCH];
+#pragma unroll
+        for (int u = 0; u < MX_BATCH; u++) {
+            q[u] = -1;
+            if (w.ok()) {
+                q[u] = w.flat();
+                v[u] = C.e[(ci0 + w.k) + (cj0 + w.j) * W2];
+                w.next();
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < MX_BATCH; u++)
+            if (q[u] >= 0) g.ce[q[u]] = v[u];
+    }
+}
+
+// the tile (and, for a tile on the border, the ghost nodes beside it) from shared memory to
+// e_dst: the tiles together write every node of the level exactly once
+__device__ __forceinline__ void region_store(const MXL &L, const Region &g, float *e_dst) {
+    const int W = L.nx + 3;
+    const int wi0 = g.i0 == 1 ? 0 : g.i0, wj0 = g.j0 == 1 ? 0 : g.j0;
+    const int wi1 = g.i1 == L.nx + 2 ? L.nx + 3 : g.i1, wj1 = g.j1 == L.ny + 2 ? L.ny + 3 : g.j1;
+    for (Walk2 w(threadIdx.x, blockDim.x, wi1 - wi0, wj1 - wj0); w.ok(); w.next()) {
+        const int i = wi0 + w.k, j = wj0 + w.j;
+        e_dst[i + j * W] = g.e[g.at(i, j)];
+    }
+}
+
+// half-sweep h of colour `color` on the region (the same update as sweep32)
+__device__ __forceinline__ void region_half_sweep(const MXL &L, const Region &g, int h, int color, float omega) {
+    const int nx = L.nx, ny = L.ny;
+    const float aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
+    const float inv_ac = 1.0f / ac;
+    // nodes at least h + 1 inside the unclamped region, within the updatable range
+    const int lo_i = max(g.i0 - g.H + h + 1, 1), hi_i = min(g.i1 + g.H - h - 1, nx + 2);
+    const int lo_j = max(g.j0 - g.H + h + 1, 1), hi_j = min(g.j1 + g.H - h - 1, ny + 2);
+    if (lo_i >= hi_i || lo_j >= hi_j) return;
+    const int hw = (hi_i - lo_i + 1) / 2 + 1;
+    const int RW = g.RW;
+    for (Walk2 w(threadIdx.x, blockDim.x, hw, hi_j - lo_j); w.ok(); w.next()) {
+        const int j = lo_j + w.j;
+        int i = lo_i + 2 * w.k;
+        if (((i + j + 1 + color) & 1) != 0) i++;   // colour 0: i + j odd; colour 1: i + j even
+        if (i >= hi_i) continue;
+        const int q = g.at(i, j);
+        const int bc = g.b[q];
+        if (bc > 0) continue;
+        float s;
+        if (bc == -2) {
+            s = g.r[q] - an * g.e[q + RW] - as * g.e[q - RW] - 2.0f * ae * g.e[q + 1];
+        } else {
+            if (bc == 0 && j == ny + 1) continue;
+            s = g.r[q] - aw * g.e[q - 1] - an * g.e[q + RW] - as * g.e[q - RW] - ae * g.e[q + 1];
+        }
+        g.e[q] = (1.0f - omega) * g.e[q] + omega * s * inv_ac;
+    }
+}
+
+// getres32 on the region (no Neumann column: the CG path has no Neumann or periodic decks)
+__device__ __forceinline__ float region_res(const MXL &L, const Region &g, int i, int j) {
+    const float aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
+    const int q = g.at(i, j), RW = g.RW;
+    return g.r[q] - (aw * g.e[q - 1] + ae * g.e[q + 1] + an * g.e[q + RW] + as * g.e[q - RW] + ac * g.e[q]);
+}
+
+// smoothing + restriction of level l into level l + 1 (C.r), tile by tile; the coarse e is
+// not zeroed: the next level's pass starts from zeros itself
+__device__ void tiled_down(const BigTeam &, const MXP &P, int l) {
+    extern __shared__ __align__(16) unsigned char mx_smem[];
+    const MXL &F = P.L[l], &C = P.L[l + 1];
+    const int nx = F.nx, ny = F.ny, nx2 = C.nx, W2 = nx2 + 3;
+    const int K = 2 * P.nu1, H = K + 2;
+    const int ntiles = ((nx + 1 + MX_TX - 1) / MX_TX) * ((ny + 1 + MX_TY - 1) / MX_TY);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const Region g = make_region(F, tile, H, mx_smem, P.tile_cap);
+        region_load(F, nullptr, g);   // every level of the cycle starts from e = 0
+        __syncthreads();
+        for (int h = 0; h < K; h++) {
+            region_half_sweep(F, g, h, h & 1, P.omega);
+            __syncthreads();
+        }
+        // coarse nodes whose fine centre (2i-1, 2j-1) lies in the tile
+        const int ic0 = (g.i0 + 2) / 2, ic1 = g.i1 / 2 + 1, jc0 = (g.j0 + 2) / 2, jc1 = g.j1 / 2 + 1;
+        for (Walk2 w(threadIdx.x, blockDim.x, ic1 - ic0, jc1 - jc0); w.ok(); w.next()) {
+            const int i = ic0 + w.k, j = jc0 + w.j;
+            const int ir = 2 * i - 1, jr = 2 * j - 1;
+            float out = 0.0f;
+            if (C.bc[i + j * W2] <= 0) {
+#define RB(x_, y_) g.b[g.at(x_, y_)]
+                float r1 = 0, r2 = 0, r3 = 0, r4 = 0, r5 = 0, r6 = 0, r7 = 0, r8 = 0;
+                const float r9 = region_res(F, g, ir, jr);
+                if (ir != nx + 1 && jr != ny + 1 && RB(ir + 1, jr + 1) <= 0) r1 = region_res(F, g, ir + 1, jr + 1);
+                if (ir != nx + 1 && RB(ir + 1, jr) <= 0) r2 = region_res(F, g, ir + 1, jr);
+                if (RB(ir + 1, jr - 1) <= 0 && ir != nx + 1 && jr != 1) r3 = region_res(F, g, ir + 1, jr - 1);
+                if (RB(ir, jr - 1) <= 0 && jr != 1) r4 = region_res(F, g, ir, jr - 1);
+                if (RB(ir - 1, jr - 1) <= 0 && ir != 1 && jr != 1) r5 = region_res(F, g, ir - 1, jr - 1);
+                if (RB(ir - 1, jr) <= 0 && ir != 1) r6 = region_res(F, g, ir - 1, jr);
+                if (RB(ir - 1, jr + 1) <= 0 && ir != 1 && jr != ny + 1) r7 = region_res(F, g, ir - 1, jr + 1);
+                if (RB(ir, jr + 1) <= 0 && jr != ny + 1) r8 = region_res(F, g, ir, jr + 1);
+#undef RB
+                out = (4.0f * r9 + 2.0f * (r2 + r4 + r6 + r8) + r1 + r3 + r5 + r7) * 0.0625f;
+            }
+            C.r[(i - 1) + (j - 1) * (nx2 + 1)] = out;
+        }
+        // the smoothed tile into the partner buffer: neighbouring tiles still read F.e as halo
+        region_store(F, g, F.e2);
+        __syncthreads();
+    }
+}
+
+// prolongation of level l + 1 into level l + smoothing, tile by tile
+__device__ void tiled_up(const BigTeam &, const MXP &P, int l) {
+    extern __shared__ __align__(16) unsigned char mx_smem[];
+    const MXL &F = P.L[l], &C = P.L[l + 1];
+    const int nx = F.nx, ny = F.ny;
+    const int K = 2 * P.nu2, H = K;
+    const int ntiles = ((nx + 1 + MX_TX - 1) / MX_TX) * ((ny + 1 + MX_TY - 1) / MX_TY);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const Region g = make_region(F, tile, H, mx_smem, P.tile_cap);
+        region_load(F, F.e2, g);
+        const int ci0 = g.ri0 / 2, cj0 = g.rj0 / 2;
+        const int ci1 = min((g.ri0 + g.RW + 1) / 2, C.nx + 2), cj1 = min((g.rj0 + g.RH + 1) / 2, C.ny + 2);
+        const int CW = ci1 - ci0 + 1, CH = cj1 - cj0 + 1;
+        coarse_load(C, g, ci0, cj0, CW, CH);
+        __syncthreads();
+        // prolong32 written per fine node: each fine node (i, j), 0 <= i <= nx+1, 0 <= j <= ny+1,
+        // takes the correction of the one coarse node prolong32 assigns it, in the same order
+        for (Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH); w.ok(); w.next()) {
+            const int i = g.ri0 + w.k, j = g.rj0 + w.j;
+            if (i > nx + 1 || j > ny + 1) continue;
+            const int q = w.flat();
+            if (g.b[q] > 0) continue;
+            const int i2 = (i + 2) / 2, j2 = (j + 2) / 2;    // the coarse node whose stencil holds (i, j)
+            const float *e = g.ce + (i2 - ci0) + (j2 - cj0) * CW;
+            const float r1 = e[0];
+            const bool io = (i & 1) != 0, jo = (j & 1) != 0;
+            if (io && jo) {
+                g.e[q] += r1;
+            } else if (io) {
+                const float r2 = e[-CW];
+                g.e[q] += 0.5f * (r1 + r2);
+            } else if (jo) {
+                const float r4 = e[-1];
+                g.e[q] += 0.5f * (r1 + r4);
+            } else {
+                const float r2 = e[-CW], r3 = e[-1 - CW], r4 = e[-1];
+                g.e[q] += 0.25f * (r1 + r2 + r3 + r4);
+            }
+        }
+        __syncthreads();
+        for (int h = 0; h < K; h++) {
+            region_half_sweep(F, g, h, 1 - (h & 1), P.omega);
+            __syncthreads();
+        }
+        // the tile (with the ghost nodes the prolongation touched) back into F.e
+        region_store(F, g, F.e);
+        __syncthreads();
+    }
+}
+
 // The coarse part of the cycle (levels >= Ls) on CTA 0, with every coarse level's e, r and
 // mask held in shared memory: the restricted r of level Ls comes in from global memory, the
 // correction e of level Ls goes back out, everything in between stays on chip.
@@ -237,6 +486,19 @@ __device__ void small_cycle(const MXP &P) {
 __device__ bool vcycle32(const MXP &P) {
     BigTeam B{P.cnt, P.partials};
     const int ng = P.ng, Ls = P.Ls;
+    if (P.tiled) { // Ls <= ng - 1: the small cycle takes the coarse levels
+        for (int l = 0; l < Ls; l++) {
+            tiled_down(B, P, l);
+            if (!B.sync()) return false;
+        }
+        if (blockIdx.x == 0) small_cycle(P);
+        if (!B.sync()) return false;
+        for (int l = Ls - 1; l >= 0; l--) {
+            tiled_up(B, P, l);
+            if (!B.sync()) return false;
+        }
+        return true;
+    }
     for (int l = 0; l < Ls && l <= ng - 2; l++) {
         if (!smooth32(B, P, P.L[l], P.nu1, false)) return false;
         restrict32(B, P.L[l], P.L[l + 1], P.pbc, P.nmn);
@@ -346,8 +608,10 @@ __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *
             if (bc == -1) a += r * r;
         }
     }
-    const int nn = W * (ny + 3);
-    for (int t = (int)B.rank(); t < nn; t += (int)B.size()) L.e[t] = 0.0f;
+    if (!P.tiled) { // the grid-wide cycle starts from the zeroed e; the tiled one loads zeros itself
+        const int nn = W * (ny + 3);
+        for (int t = (int)B.rank(); t < nn; t += (int)B.size()) L.e[t] = 0.0f;
+    }
     return team_sum(B, a, rr);
 }
 
@@ -369,7 +633,7 @@ __device__ bool b0_norm(const Team &T, const MXL &L, double *bb) {
     return team_sum(T, b, bb);
 }
 
-__global__ void __launch_bounds__(MG_THREADS) k_mg_mixed(MXP P) {
+__global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
     BigTeam B{P.cnt, P.partials};
     double bb = 0.0, rr = 0.0, l1 = 0.0, rz = 0.0, pap = 0.0;
     if (!b0_norm(B, P.L[0], &bb)) return;
@@ -427,7 +691,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
         double aw = eps0 / (a.hx * a.hx), an = eps0 / (a.hy * a.hy), ac = -(an + an + aw + aw);
         d.awd = aw; d.and_ = an; d.acd = ac;
         d.aw = (float)aw; d.an = (float)an; d.ac = (float)ac;
-        d.e = a.e32; d.r = a.r32; d.bc = a.bc; d.u = a.u; d.b = a.b;
+        d.e = a.e32; d.e2 = a.e32b; d.r = a.r32; d.bc = a.bc; d.u = a.u; d.b = a.b;
     }
     P.ng = c->nlev;
     // the coarsest levels whose e, r and mask fit together in CTA 0's shared-memory budget
@@ -454,7 +718,6 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
         P.soff_r[l] = (int)off; off += ((nr * 4 + 15) / 16) * 16;
         P.soff_b[l] = (int)off; off += ((nn + 15) / 16) * 16;
     }
-    P.smem_bytes = (int)off;
     P.Ls = Ls;
     P.omega = 1.0f;
     P.nu1 = 2; P.nu2 = 2; P.nuc = 8; P.max_iter = 200;
@@ -462,6 +725,14 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
     if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
     if (const char *e = getenv("LEPIC_MX_NU2")) P.nu2 = atoi(e);
+    // tiles: region (TX + 2H) x (TY + 2H) with H = 2 nu + 2 (down) or 2 nu (up); e, r (FP32)
+    // and the mask per node, sharing the dynamic shared memory with the small cycle
+    const int Hmax = 2 * std::max(P.nu1 + 1, P.nu2);
+    P.tile_cap = (MX_TX + 2 * Hmax) * (MX_TY + 2 * Hmax);
+    const long long coarse_cap = (long long)((MX_TX + 2 * Hmax) / 2 + 3) * ((MX_TY + 2 * Hmax) / 2 + 3);
+    const long long tile_bytes = (long long)P.tile_cap * 9 + coarse_cap * 4 + 16;
+    P.tiled = (Ls <= c->nlev - 1 && Ls >= 1 && !getenv("LEPIC_MX_UNTILED") && tile_bytes <= 64 * 1024) ? 1 : 0;
+    P.smem_bytes = (int)std::max(off, P.tiled ? tile_bytes : 0ll);
     P.eps = eps;
     P.alpha = fabs((double)(c->cfg.nx + 1) * (c->cfg.ny + 1) * P.L[0].acd);
     P.pbc = c->cfg.flag_pbc;
