@@ -146,9 +146,12 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         SpeciesBuf &B = c->sp[s];
         B.cap = g.capacity[s];
         maxcap = std::max(maxcap, B.cap);
+        // storage rounded up to whole groups of 8 slots: the push reads and writes 8 consecutive
+        // slots per thread with 16-byte vectors (the capacity itself is unchanged)
+        const long long cap8 = (B.cap + 7) / 8 * 8;
         for (int k = 0; k < 2; k++) {
-            LALLOC(B.X[k], B.cap); LALLOC(B.Y[k], B.cap);
-            LALLOC(B.VX[k], B.cap); LALLOC(B.VY[k], B.cap); LALLOC(B.VZ[k], B.cap);
+            LALLOC(B.X[k], cap8); LALLOC(B.Y[k], cap8);
+            LALLOC(B.VX[k], cap8); LALLOC(B.VY[k], cap8); LALLOC(B.VZ[k], cap8);
         }
         B.cur = 0;
         LALLOC(B.acc, nn);

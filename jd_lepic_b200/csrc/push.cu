@@ -41,36 +41,26 @@ struct PushP {
     long long xlim, ylim;      // nx<<S, ny<<S
 };
 
-// CIC deposit of one particle per lane, aggregated per cell inside the warp: lanes whose
-// particles share a cell (the usual case after the sort) sum their four integer weights with
-// two exact 32-bit warp reductions each (22-bit halves: 32 lanes x 2^22 < 2^32), and one lane
-// issues the four atomics.  Must be called by all 32 lanes of the warp.
-__device__ __forceinline__ void deposit_warp(const PushP &P, unsigned long long *win, int ox, int oy,
-                                             bool use_win, bool have, uint32_t X, uint32_t Y) {
-    const int ix = (int)(X >> P.S) + 1, iy = (int)(Y >> P.S) + 1; // INT(x/h)+1, x >= 0
-    const int key = have ? ix + iy * P.W : -1;
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    if (key < 0) return;
+#define PUSH_G 4    // consecutive slots per thread: one 16-byte vector per array
+
+// CIC weights of one particle: exact integer products of the fixed-point offsets, scaled to
+// 2^LEPIC_DEP_SHIFT, for (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1)
+__device__ __forceinline__ void cic_weights(const PushP &P, uint32_t X, uint32_t Y, uint64_t *w) {
     const uint32_t mask = (1u << P.S) - 1u;
     const uint32_t A = 1u << P.S;
     const uint32_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
-    // (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1): 32x32 -> 64-bit products
-    uint64_t w[4] = {(uint64_t)ax * ay, (uint64_t)fx * ay, (uint64_t)fx * fy, (uint64_t)ax * fy};
+    w[0] = (uint64_t)ax * ay; w[1] = (uint64_t)fx * ay; w[2] = (uint64_t)fx * fy; w[3] = (uint64_t)ax * fy;
     const int sh = 2 * P.S - LEPIC_DEP_SHIFT;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if (sh > 0) w[k] = (w[k] + (1ull << (sh - 1))) >> sh;
         else if (sh < 0) w[k] <<= -sh;
     }
-    if (__popc(grp) > 1) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const unsigned lo = __reduce_add_sync(grp, (unsigned)(w[k] & 0x3FFFFFull));
-            const unsigned hi = __reduce_add_sync(grp, (unsigned)(w[k] >> 22));
-            w[k] = ((uint64_t)hi << 22) + lo;
-        }
-        if ((int)(threadIdx.x & 31) != __ffs(grp) - 1) return;
-    }
+}
+
+// the four accumulators of cell (ix, iy): the CTA's shared-memory window or the global grid
+__device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win, int ox, int oy, bool use_win,
+                                         int ix, int iy, const uint64_t *w) {
     const int lx = ix - ox, ly = iy - oy;
     unsigned long long *q;
     int row;
@@ -87,29 +77,35 @@ __device__ __forceinline__ void deposit_warp(const PushP &P, unsigned long long 
     if (w[3]) atomicAdd(q + row, (unsigned long long)w[3]);
 }
 
-struct Part {
-    uint32_t X, Y;
-    float vx, vy, vz;
-};
-
-__device__ __forceinline__ void load_part(const PushP &P, int i, bool ok, Part &p) {
-    if (ok) {
-        p.vx = P.VX[i]; p.X = P.X[i]; p.Y = P.Y[i]; p.vy = P.VY[i]; p.vz = P.VZ[i];
-    } else {
-        p.vx = __int_as_float(0x7fc00000); p.X = 0; p.Y = 0; p.vy = 0.f; p.vz = 0.f;
+// The last run of every lane, aggregated over the warp: lanes whose runs share a cell (the
+// usual case after the sort) add their sums with exact 32-bit warp reductions of 24-bit
+// halves (a run holds at most PUSH_G <= 8 weights <= 2^44 each, so a half stays below 2^24
+// and 32 of them below 2^29), and one lane issues the atomics.  Called by all 32 lanes.
+__device__ __forceinline__ void flush_warp(const PushP &P, unsigned long long *win, int ox, int oy, bool use_win,
+                                           int key, int ix, int iy, uint64_t *w) {
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (key < 0) return;
+    if (__popc(grp) > 1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const unsigned lo = __reduce_add_sync(grp, (unsigned)(w[k] & 0xFFFFFFull));
+            const unsigned hi = __reduce_add_sync(grp, (unsigned)(w[k] >> 24));
+            w[k] = ((uint64_t)hi << 24) + lo;
+        }
+        if ((int)(threadIdx.x & 31) != __ffs(grp) - 1) return;
     }
+    add_cell(P, win, ox, oy, use_win, ix, iy, w);
 }
 
-// part_mover for one particle already in registers; returns false for a hole or a particle
-// lost in this step (the slot then becomes a hole).  BMODE: 0 no B, 1 constant, 2 map;
+// part_mover for one particle in registers; returns false for a hole or a particle lost in
+// this step (its VX becomes NaN: the slot is a hole).  BMODE: 0 no B, 1 constant, 2 map;
 // GEN: the periodic / specular / Neumann boundary options (off in the common deck).
 template <int BMODE, bool GEN>
-__device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCounters *cnt, unsigned int &lost) {
-    if (isnan(p.vx)) return false; // hole
+__device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, uint32_t &Y, float &vx, float &vy,
+                                          float &vz, DevCounters *cnt, unsigned int &lost) {
+    if (isnan(vx)) return false; // hole
     const uint32_t mask = (1u << P.S) - 1u;
     const float inv2S = 1.0f / (float)(1u << P.S);
-    uint32_t X = p.X, Y = p.Y;
-    float vx = p.vx, vy = p.vy, vz = p.vz;
     // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
     const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
     const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
@@ -136,25 +132,26 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCoun
             mag = true;
         }
     }
+    float ux0 = vx, uy0 = vy, uz0 = vz;
     if (mag) { // Boris, part_expmover.f90:187-206
         const float Bt2 = Bx * Bx + By * By + Bz * Bz;
         const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
-        const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz;
+        const float v1x = ux0 + k1 * Ex, v1y = uy0 + k1 * Ey, v1z = uz0;
         const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
         const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
         const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
-        vx = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
-        vy = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
-        vz = v1z + k2 * (v3x * By - v3y * Bx);
+        ux0 = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
+        uy0 = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
+        uz0 = v1z + k2 * (v3x * By - v3y * Bx);
     } else { // leap-frog, :210-211
-        vx = vx + 2.0f * k1 * Ex;
-        vy = vy + 2.0f * k1 * Ey;
+        ux0 = ux0 + 2.0f * k1 * Ex;
+        uy0 = uy0 + 2.0f * k1 * Ey;
     }
     // a non-finite velocity (a non-finite field) is an error: the particle is removed
-    if (!(fabsf(vx) <= 3.0e8f && fabsf(vy) <= 3.0e8f && fabsf(vz) <= 3.0e8f)) {
+    if (!(fabsf(ux0) <= 3.0e8f && fabsf(uy0) <= 3.0e8f && fabsf(uz0) <= 3.0e8f)) {
         set_err(cnt, LERR_RANGE, 101);
         lost++;
-        P.VX[i] = __int_as_float(0x7fc00000);
+        vx = __int_as_float(0x7fc00000);
         return false;
     }
     // move (:216-217): integer part plus an unbiased stochastic rounding of the fractional part
@@ -164,7 +161,7 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCoun
     h ^= h >> 15;
     const float ux = (float)(h & 0xFFFFu) * (1.0f / 65536.0f);
     const float uy = (float)(h >> 16) * (1.0f / 65536.0f);
-    const float ddx = vx * P.cdx, ddy = vy * P.cdy;
+    const float ddx = ux0 * P.cdx, ddy = uy0 * P.cdy;
     const float fdx = floorf(ddx), fdy = floorf(ddy);
     long long Xn = (long long)X + (long long)((int)fdx + ((ux < ddx - fdx) ? 1 : 0));
     long long Yn = (long long)Y + (long long)((int)fdy + ((uy < ddy - fdy) ? 1 : 0));
@@ -173,11 +170,11 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCoun
         long long k4 = Yn / Ym; // INT: truncation toward zero
         if (Yn >= Ym) {
             if (P.spec == 0) Yn = Yn - k4 * Ym;
-            else { Yn = (k4 + 1) * Ym - Yn; vy = -vy; }
+            else { Yn = (k4 + 1) * Ym - Yn; uy0 = -uy0; }
         }
         if (Yn <= 0) {
             if (P.spec == 0) Yn = (1 - k4) * Ym + Yn;
-            else { Yn = k4 * Ym - Yn; vy = -vy; }
+            else { Yn = k4 * Ym - Yn; uy0 = -uy0; }
             if (Yn >= Ym) Yn = 0; // y = ymax exactly is kept as y = 0
         }
     }
@@ -189,10 +186,10 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCoun
     if (GEN && !is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
     if (is_lost) {
         lost++;
-        P.VX[i] = __int_as_float(0x7fc00000); // the slot becomes a hole
+        vx = __int_as_float(0x7fc00000); // the slot becomes a hole
         return false;
     }
-    if (GEN && P.nmn && Xn <= 0) { Xn = -Xn; vx = -vx; } // :454-459
+    if (GEN && P.nmn && Xn <= 0) { Xn = -Xn; ux0 = -ux0; } // :454-459
     if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
         set_err(cnt, LERR_RANGE, 100);
         Xn = min(max(Xn, 0ll), P.xlim - 1);
@@ -200,31 +197,34 @@ __device__ __forceinline__ bool move_one(const PushP &P, int i, Part &p, DevCoun
     }
     X = (uint32_t)Xn;
     Y = (uint32_t)Yn;
-    P.X[i] = X; P.Y[i] = Y;
-    P.VX[i] = vx; P.VY[i] = vy; P.VZ[i] = vz;
-    p.X = X;
-    p.Y = Y;
+    vx = ux0; vy = uy0; vz = uz0;
     return true;
 }
 
-// Two particles per thread per iteration (two independent load -> push -> store chains in
-// flight), then the two warp-aggregated deposits.
+// Each thread takes PUSH_G consecutive slots per iteration (one 16-byte vector load and store
+// per array): after the sort consecutive particles mostly share a cell, so the deposit
+// accumulates runs of equal cells in registers and only the last run of a thread goes
+// through the warp aggregation; a run that ends earlier goes straight to the accumulators.
+// A work item's range is rounded down to multiples of 8 slots at both ends, so consecutive items
+// still tile the slot array exactly; particles a rounded range takes from a neighbouring
+// tile reach the global grid when they fall outside the window.
 template <int BMODE, bool GEN, bool MOVE>
-__global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
+__global__ void __launch_bounds__(PUSH_THREADS, 3) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
     __shared__ unsigned int s_lost;
     DevCounters *cnt = P.cnt;
     const long long n_slots = cnt->n_slots[P.sp], n_sorted = cnt->n_sorted[P.sp];
     const int n_items = cnt->n_items[P.sp];
+    const long long tail0 = n_sorted & ~7ll;
     for (;;) {
         if (threadIdx.x == 0) {
             unsigned int w = atomicAdd(&cnt->work_next[P.sp], 1u);
             if ((int)w < n_items) {
                 WorkItem it = P.items[w];
-                s_tile = it.tile; s_start = it.start; s_end = it.end;
+                s_tile = it.tile; s_start = it.start & ~7; s_end = it.end & ~7;
             } else {
-                long long st = n_sorted + (long long)(w - n_items) * PUSH_CHUNK;
+                long long st = tail0 + (long long)(w - n_items) * PUSH_CHUNK;
                 if (st >= n_slots) { s_tile = -2; s_start = s_end = 0; }
                 else { s_tile = -1; s_start = (int)st; s_end = (int)min(st + PUSH_CHUNK, n_slots); }
             }
@@ -244,21 +244,55 @@ __global__ void __launch_bounds__(PUSH_THREADS) k_push_deposit(PushP P) {
         __syncthreads();
         unsigned int lost = 0;
         const int end = s_end;
-        for (int base = s_start; base < end; base += 2 * PUSH_THREADS) { // uniform trip count
-            const int i0 = base + threadIdx.x, i1 = i0 + PUSH_THREADS;
-            Part p0, p1;
-            load_part(P, i0, i0 < end, p0);
-            load_part(P, i1, i1 < end, p1);
-            bool h0, h1;
-            if (MOVE) {
-                h0 = move_one<BMODE, GEN>(P, i0, p0, cnt, lost);
-                h1 = move_one<BMODE, GEN>(P, i1, p1, cnt, lost);
-            } else {
-                h0 = !isnan(p0.vx);
-                h1 = !isnan(p1.vx);
+        for (int base = s_start; base < end; base += PUSH_G * PUSH_THREADS) { // uniform trip count
+            const int g = base + PUSH_G * threadIdx.x;
+            const bool grp_ok = g < end;
+            uint32_t X[PUSH_G], Y[PUSH_G];
+            float vx[PUSH_G], vy[PUSH_G], vz[PUSH_G];
+            if (grp_ok) {   // storage is whole groups of 8: the last, partial group is masked below
+                const uint4 x0 = *reinterpret_cast<const uint4 *>(P.X + g);
+                const uint4 y0 = *reinterpret_cast<const uint4 *>(P.Y + g);
+                const float4 a0 = *reinterpret_cast<const float4 *>(P.VX + g);
+                const float4 b0 = *reinterpret_cast<const float4 *>(P.VY + g);
+                const float4 c0 = *reinterpret_cast<const float4 *>(P.VZ + g);
+                X[0] = x0.x; X[1] = x0.y; X[2] = x0.z; X[3] = x0.w;
+                Y[0] = y0.x; Y[1] = y0.y; Y[2] = y0.z; Y[3] = y0.w;
+                vx[0] = a0.x; vx[1] = a0.y; vx[2] = a0.z; vx[3] = a0.w;
+                vy[0] = b0.x; vy[1] = b0.y; vy[2] = b0.z; vy[3] = b0.w;
+                vz[0] = c0.x; vz[1] = c0.y; vz[2] = c0.z; vz[3] = c0.w;
             }
-            deposit_warp(P, win, ox, oy, use_win, h0, p0.X, p0.Y);
-            deposit_warp(P, win, ox, oy, use_win, h1, p1.X, p1.Y);
+            int rkey = -1, rix = 0, riy = 0;   // the current run of equal cells
+            uint64_t rw[4] = {0, 0, 0, 0};
+            if (grp_ok) {
+#pragma unroll
+                for (int p = 0; p < PUSH_G; p++) {
+                    const int i = g + p;
+                    if (i >= end) break;
+                    bool alive;
+                    if (MOVE) alive = move_regs<BMODE, GEN>(P, i, X[p], Y[p], vx[p], vy[p], vz[p], cnt, lost);
+                    else alive = !isnan(vx[p]);
+                    if (!alive) continue;
+                    const int ix = (int)(X[p] >> P.S) + 1, iy = (int)(Y[p] >> P.S) + 1; // INT(x/h)+1, x >= 0
+                    const int key = ix + iy * P.W;
+                    uint64_t w[4];
+                    cic_weights(P, X[p], Y[p], w);
+                    if (key != rkey) {
+                        if (rkey >= 0) add_cell(P, win, ox, oy, use_win, rix, riy, rw);
+                        rkey = key; rix = ix; riy = iy;
+                        rw[0] = w[0]; rw[1] = w[1]; rw[2] = w[2]; rw[3] = w[3];
+                    } else {
+                        rw[0] += w[0]; rw[1] += w[1]; rw[2] += w[2]; rw[3] += w[3];
+                    }
+                }
+                if (MOVE) {
+                    *reinterpret_cast<uint4 *>(P.X + g) = make_uint4(X[0], X[1], X[2], X[3]);
+                    *reinterpret_cast<uint4 *>(P.Y + g) = make_uint4(Y[0], Y[1], Y[2], Y[3]);
+                    *reinterpret_cast<float4 *>(P.VX + g) = make_float4(vx[0], vx[1], vx[2], vx[3]);
+                    *reinterpret_cast<float4 *>(P.VY + g) = make_float4(vy[0], vy[1], vy[2], vy[3]);
+                    *reinterpret_cast<float4 *>(P.VZ + g) = make_float4(vz[0], vz[1], vz[2], vz[3]);
+                }
+            }
+            flush_warp(P, win, ox, oy, use_win, rkey, rix, riy, rw);
         }
         // lost-particle count: one atomic per warp, then per CTA
         for (int o = 16; o > 0; o >>= 1) lost += __shfl_xor_sync(0xffffffffu, lost, o);
