@@ -102,7 +102,7 @@ __device__ __forceinline__ void flush_warp(const PushP &P, unsigned long long *w
 // GEN: the periodic / specular / Neumann boundary options (off in the common deck).
 template <int BMODE, bool GEN>
 __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, uint32_t &Y, float &vx, float &vy,
-                                          float &vz, DevCounters *cnt, unsigned int &lost) {
+                                          float &vz, DevCounters *cnt, unsigned int &lost, int &ixo, int &iyo) {
     if (isnan(vx)) return false; // hole
     const uint32_t mask = (1u << P.S) - 1u;
     const float inv2S = 1.0f / (float)(1u << P.S);
@@ -114,6 +114,8 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     const int n00 = (cx + 1) + (cy + 1) * P.W;
     const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
     const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
+    // the wall byte of the current cell, fetched with the field (independent of the move)
+    const bool wall_now = !GEN && __ldg(P.cellwall + (cx + 1) + (cy + 1) * (P.nx + 2)) != 0;
     const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
     const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
     const float k1 = P.k1;
@@ -163,8 +165,21 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     const float uy = (float)(h >> 16) * (1.0f / 65536.0f);
     const float ddx = ux0 * P.cdx, ddy = uy0 * P.cdy;
     const float fdx = floorf(ddx), fdy = floorf(ddy);
-    long long Xn = (long long)X + (long long)((int)fdx + ((ux < ddx - fdx) ? 1 : 0));
-    long long Yn = (long long)Y + (long long)((int)fdy + ((uy < ddy - fdy) ? 1 : 0));
+    const int dX = (int)fdx + ((ux < ddx - fdx) ? 1 : 0);
+    const int dY = (int)fdy + ((uy < ddy - fdy) ? 1 : 0);
+    if (!GEN) {
+        // a particle that stays in its cell (the common case) and whose cell is not a wall cell
+        // is neither lost nor out of range (a wrap of the 32-bit sum always changes the cell)
+        const uint32_t Xs = X + (uint32_t)dX, Ys = Y + (uint32_t)dY;
+        if (!wall_now && (Xs >> P.S) == (uint32_t)cx && (Ys >> P.S) == (uint32_t)cy) {
+            X = Xs; Y = Ys;
+            vx = ux0; vy = uy0; vz = uz0;
+            ixo = cx + 1; iyo = cy + 1;
+            return true;
+        }
+    }
+    long long Xn = (long long)X + (long long)dX;
+    long long Yn = (long long)Y + (long long)dY;
     if (GEN && P.pbc) { // :222-241
         const long long Ym = P.ylim;
         long long k4 = Yn / Ym; // INT: truncation toward zero
@@ -198,6 +213,8 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     X = (uint32_t)Xn;
     Y = (uint32_t)Yn;
     vx = ux0; vy = uy0; vz = uz0;
+    ixo = (int)(X >> P.S) + 1;
+    iyo = (int)(Y >> P.S) + 1;
     return true;
 }
 
@@ -269,10 +286,15 @@ __global__ void __launch_bounds__(PUSH_THREADS, 3) k_push_deposit(PushP P) {
                     const int i = g + p;
                     if (i >= end) break;
                     bool alive;
-                    if (MOVE) alive = move_regs<BMODE, GEN>(P, i, X[p], Y[p], vx[p], vy[p], vz[p], cnt, lost);
-                    else alive = !isnan(vx[p]);
+                    int ix, iy;   // the deposit cell INT(x/h)+1 (x >= 0)
+                    if (MOVE) {
+                        alive = move_regs<BMODE, GEN>(P, i, X[p], Y[p], vx[p], vy[p], vz[p], cnt, lost, ix, iy);
+                    } else {
+                        alive = !isnan(vx[p]);
+                        ix = (int)(X[p] >> P.S) + 1;
+                        iy = (int)(Y[p] >> P.S) + 1;
+                    }
                     if (!alive) continue;
-                    const int ix = (int)(X[p] >> P.S) + 1, iy = (int)(Y[p] >> P.S) + 1; // INT(x/h)+1, x >= 0
                     const int key = ix + iy * P.W;
                     uint64_t w[4];
                     cic_weights(P, X[p], Y[p], w);
