@@ -139,7 +139,7 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
     }
     LCUDA(cudaMemset(c->rhs, 0, sizeof(double) * (nx + 1) * (ny + 1)));
     LCUDA(cudaMemset(c->Ed, 0, sizeof(double2) * 2 * nn));
-    LCUDA(cudaMemset(c->Ef, 0, sizeof(float2) * nn));
+    LCUDA(cudaMemset(c->Ef, 0, sizeof(float4) * nn));
     // particles
     long long maxcap = 0;
     for (int s = 0; s < g.ntype; s++) {

@@ -163,7 +163,7 @@ __global__ void k_efield_nmn_pbc(int nx, int ny, double h2, const double *phi, c
 // Pass 2, walls (:87-118): zero, then linear extrapolation from the interior side.  Reads the
 // pass-1 field and writes a second buffer, so every wall node sees the same input.
 __global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *Ein, double2 *Eout,
-                               float2 *Ef) {
+                               float4 *Ef) {
     const int W = nx + 3;
     const long long nn = (long long)(nx + 3) * (ny + 3);
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn;
@@ -180,7 +180,12 @@ __global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *
             if (bc[n - W] <= 0) e.y = 2.0 * Ein[n - W].y - (iy >= 2 ? Ein[n - 2 * W].y : 0.0);
         }
         Eout[n] = e;
-        Ef[n] = make_float2((float)e.x, (float)e.y);
+        // FP32 gather copy in node pairs: node n is the first half of pair n and the second
+        // half of pair n - 1, so the push reads two adjacent nodes with one 16-byte load
+        const float2 f = make_float2((float)e.x, (float)e.y);
+        float2 *half = reinterpret_cast<float2 *>(Ef);
+        half[2 * n] = f;
+        if (n > 0) half[2 * n - 1] = f;
     }
 }
 

@@ -98,7 +98,7 @@ struct lepic_ctx {
     // dynamic grids
     double *phi = nullptr, *rhs = nullptr;
     double2 *Ed = nullptr;
-    float2 *Ef = nullptr;
+    float4 *Ef = nullptr;         // gather copy in node pairs: (Ex, Ey)[n], (Ex, Ey)[n+1]
     double *npd = nullptr;        // FP64 np grids (ntype), filled on demand
     double *np_red = nullptr;
     double *np_mx = nullptr;

@@ -19,15 +19,16 @@
 #include "lepic_internal.cuh"
 
 #define PUSH_THREADS 256
-#define PUSH_CHUNK 2048
+#define PUSH_CHUNK 8192
 
 struct PushP {
     int nx, ny, S, W;
     uint32_t *X, *Y;
     float *VX, *VY, *VZ;
-    const float2 *E;
+    const float4 *E;           // node pairs: (Ex, Ey)[n], (Ex, Ey)[n+1]
     const float4 *B;
     float Bcx, Bcy, Bcz;
+    float k2c;                 // the Boris factor of the constant field (BMODE 1)
     const uint8_t *cellwall;
     unsigned long long *acc;
     const WorkItem *items;
@@ -112,12 +113,11 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     const float px = 1.0f - fx, py = 1.0f - fy;
     const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
     const int n00 = (cx + 1) + (cy + 1) * P.W;
-    const float2 e00 = __ldg(P.E + n00), e10 = __ldg(P.E + n00 + 1);
-    const float2 e11 = __ldg(P.E + n00 + P.W + 1), e01 = __ldg(P.E + n00 + P.W);
+    const float4 r0 = __ldg(P.E + n00), r1 = __ldg(P.E + n00 + P.W);   // nodes n00, +1 and +W, +W+1
     // the wall byte of the current cell, fetched with the field (independent of the move)
     const bool wall_now = !GEN && __ldg(P.cellwall + (cx + 1) + (cy + 1) * (P.nx + 2)) != 0;
-    const float Ex = k00 * e00.x + k10 * e10.x + k11 * e11.x + k01 * e01.x;
-    const float Ey = k00 * e00.y + k10 * e10.y + k11 * e11.y + k01 * e01.y;
+    const float Ex = k00 * r0.x + k10 * r0.z + k11 * r1.z + k01 * r1.x;
+    const float Ey = k00 * r0.y + k10 * r0.w + k11 * r1.w + k01 * r1.y;
     const float k1 = P.k1;
     bool mag = false;
     float Bx = 0.f, By = 0.f, Bz = 0.f;
@@ -136,8 +136,13 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     }
     float ux0 = vx, uy0 = vy, uz0 = vz;
     if (mag) { // Boris, part_expmover.f90:187-206
-        const float Bt2 = Bx * Bx + By * By + Bz * Bz;
-        const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+        float k2;
+        if (BMODE == 1) {
+            k2 = P.k2c;   // constant field: computed once per launch
+        } else {
+            const float Bt2 = Bx * Bx + By * By + Bz * Bz;
+            k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+        }
         const float v1x = ux0 + k1 * Ex, v1y = uy0 + k1 * Ey, v1z = uz0;
         const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
         const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
@@ -374,6 +379,11 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         int bmode = g.flag_B;
         if (g.flag_B_pos == 1 && g.charge[s] > 0.0) bmode = 0; // :185
         P.Bcx = (float)g.Bc[0]; P.Bcy = (float)g.Bc[1]; P.Bcz = (float)g.Bc[2];
+        {
+            const float k1f = (float)(g.dt * g.charge[s] / (2.0 * g.mass[s]));
+            const float Bt2 = P.Bcx * P.Bcx + P.Bcy * P.Bcy + P.Bcz * P.Bcz;
+            P.k2c = k1f * (2.0f / (1.0f + k1f * k1f * Bt2));
+        }
         P.cellwall = c->cellwall;
         P.acc = B.acc;
         P.items = B.items;
