@@ -19,7 +19,7 @@
 #include "lepic_internal.cuh"
 
 #define PUSH_THREADS 256
-#define PUSH_CHUNK 8192
+#define PUSH_CHUNK 16384
 
 struct PushP {
     int nx, ny, S, W;

@@ -19,7 +19,7 @@
 #include "lepic_internal.cuh"
 
 #define SORT_THREADS 256
-#define PUSH_CHUNK 8192
+#define PUSH_CHUNK 16384
 #define SEG_WARP_MAX 256
 #define SEG_BLOCK_MAX 8192
 
