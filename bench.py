@@ -465,8 +465,9 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": case.name, "grid": [case.nx, case.ny],
                        "particles_per_species_per_gpu": case.n_particles, "species": sim.sp.ntype,
-                       "particles_avg_per_gpu": n_avg, "poisson": "mixed FP32 V-cycles in FP64 refinement, "
-                       "relative L2 residual 1e-8" if mode == 1 else "FP64 multigrid",
+                       "particles_avg_per_gpu": n_avg, "poisson": {1: "FP64 CG preconditioned by an FP32 V-cycle, relative L2 residual 1e-8",
+                                   3: "learned warm start + FP64 CG with the FP32 V-cycle, relative L2 "
+                                      "residual 1e-8"}.get(mode, "FP64 multigrid"),
                        "l2": "inputs larger than L2 (particle arrays 8.4 GB/species)",
                        "sort_every": 10, "mcc_every": 10, "tile": args.tile},
             "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()},
