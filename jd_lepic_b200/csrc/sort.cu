@@ -131,6 +131,30 @@ __global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *
     }
 }
 
+// ascending bitonic sort of 64 values held two per lane (index lane and lane + 32), padded with
+// INT_MAX; the compare-exchange partner of index i at stride j is i ^ j: a shuffle for j < 32,
+// the lane's other register for j = 32
+__device__ __forceinline__ void warp_sort64(int &v0, int &v1, int lane) {
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j == 32) {
+                const int lo = min(v0, v1), hi = max(v0, v1);
+                v0 = lo;
+                v1 = hi;
+            } else {
+                const int p0 = __shfl_xor_sync(0xffffffffu, v0, j);
+                const int p1 = __shfl_xor_sync(0xffffffffu, v1, j);
+                const bool lower = (lane & j) == 0;
+                const bool asc0 = (lane & k) == 0, asc1 = ((lane + 32) & k) == 0;
+                v0 = (lower == asc0) ? min(v0, p0) : max(v0, p0);
+                v1 = (lower == asc1) ? min(v1, p1) : max(v1, p1);
+            }
+        }
+    }
+}
+
 __global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, int *bigseg,
                                DevCounters *cnt) {
     __shared__ int buf[SORT_THREADS / 32][SEG_WARP_MAX];
@@ -140,6 +164,14 @@ __global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, i
     for (long long k = gw; k < nkeys; k += nw) {
         int s0 = offsets[k], s1 = offsets[k + 1], n = s1 - s0;
         if (n <= 1) continue;
+        if (n <= 64) {   // the common case: in registers, no shared memory
+            int v0 = lane < n ? perm[s0 + lane] : INT_MAX;
+            int v1 = lane + 32 < n ? perm[s0 + lane + 32] : INT_MAX;
+            warp_sort64(v0, v1, lane);
+            if (lane < n) perm[s0 + lane] = v0;
+            if (lane + 32 < n) perm[s0 + lane + 32] = v1;
+            continue;
+        }
         bool sorted = true;
         for (int q = lane; q + 1 < n; q += 32)
             if (perm[s0 + q] > perm[s0 + q + 1]) sorted = false;
@@ -178,14 +210,34 @@ __global__ void k_segsort_big(const int *offsets, int *perm, const int *bigseg, 
     }
 }
 
+// four consecutive outputs per thread: one 16-byte permutation load, twenty independent
+// gathers, 16-byte stores (the slot arrays are allocated in whole groups of 8)
 __global__ void k_gather(const int *perm, const int *offsets, long long nkeys, const uint32_t *X,
                          const uint32_t *Y, const float *VX, const float *VY, const float *VZ,
                          uint32_t *X2, uint32_t *Y2, float *VX2, float *VY2, float *VZ2) {
     const long long n = offsets[nkeys];
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
-         j += (long long)gridDim.x * blockDim.x) {
-        int i = perm[j];
-        X2[j] = X[i]; Y2[j] = Y[i]; VX2[j] = VX[i]; VY2[j] = VY[i]; VZ2[j] = VZ[i];
+    const long long ng = (n + 3) / 4;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ng;
+         g += (long long)gridDim.x * blockDim.x) {
+        const long long j = 4 * g;
+        if (j + 4 <= n) {
+            const int4 p = *reinterpret_cast<const int4 *>(perm + j);
+            const uint4 x = make_uint4(X[p.x], X[p.y], X[p.z], X[p.w]);
+            const uint4 y = make_uint4(Y[p.x], Y[p.y], Y[p.z], Y[p.w]);
+            const float4 a = make_float4(VX[p.x], VX[p.y], VX[p.z], VX[p.w]);
+            const float4 b = make_float4(VY[p.x], VY[p.y], VY[p.z], VY[p.w]);
+            const float4 c = make_float4(VZ[p.x], VZ[p.y], VZ[p.z], VZ[p.w]);
+            *reinterpret_cast<uint4 *>(X2 + j) = x;
+            *reinterpret_cast<uint4 *>(Y2 + j) = y;
+            *reinterpret_cast<float4 *>(VX2 + j) = a;
+            *reinterpret_cast<float4 *>(VY2 + j) = b;
+            *reinterpret_cast<float4 *>(VZ2 + j) = c;
+        } else {
+            for (long long q = j; q < n; q++) {
+                const int i = perm[q];
+                X2[q] = X[i]; Y2[q] = Y[i]; VX2[q] = VX[i]; VY2[q] = VY[i]; VZ2[q] = VZ[i];
+            }
+        }
     }
 }
 
