@@ -231,7 +231,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
 // still tile the slot array exactly; particles a rounded range takes from a neighbouring
 // tile reach the global grid when they fall outside the window.
 template <int BMODE, bool GEN, bool MOVE>
-__global__ void __launch_bounds__(PUSH_THREADS, 3) k_push_deposit(PushP P) {
+__global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
     __shared__ unsigned int s_lost;
