@@ -47,6 +47,7 @@ struct MXP {
     int smem_bytes;
     int tiled;       // 1: the big levels smooth in shared-memory tiles (temporal blocking)
     int tile_cap;    // nodes a tile region may hold
+    int tx[LEPIC_MAXLEV], ty[LEPIC_MAXLEV];   // tile size per level
 };
 
 template <class Team>
@@ -193,7 +194,7 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
 // One grid barrier per level and direction instead of one per half-sweep.  Tiles read their
 // halo from one buffer and write their result to the other (e -> e2 down, e2 -> e up), so a
 // tile never sees a neighbour's finished values.
-#define MX_TX 64
+#define MX_TX 64     // the largest tile; coarser levels use 32 x 16 or 16 x 8 (host choice)
 #define MX_TY 32
 
 struct Region {
@@ -206,15 +207,16 @@ struct Region {
     __device__ __forceinline__ int at(int i, int j) const { return (i - ri0) + (j - rj0) * RW; }
 };
 
-__device__ __forceinline__ Region make_region(const MXL &L, int tile, int H, unsigned char *smem, int cap) {
+__device__ __forceinline__ Region make_region(const MXL &L, int tile, int TX, int TY, int H, unsigned char *smem,
+                                              int cap) {
     Region g;
     const int nx = L.nx, ny = L.ny;
-    const int ntx = (nx + 1 + MX_TX - 1) / MX_TX;
+    const int ntx = (nx + 1 + TX - 1) / TX;
     const int ti = tile % ntx, tj = tile / ntx;
-    g.i0 = 1 + ti * MX_TX;
-    g.j0 = 1 + tj * MX_TY;
-    g.i1 = min(g.i0 + MX_TX, nx + 2);
-    g.j1 = min(g.j0 + MX_TY, ny + 2);
+    g.i0 = 1 + ti * TX;
+    g.j0 = 1 + tj * TY;
+    g.i1 = min(g.i0 + TX, nx + 2);
+    g.j1 = min(g.j0 + TY, ny + 2);
     g.H = H;
     g.ri0 = max(g.i0 - H, 0);
     g.rj0 = max(g.j0 - H, 0);
@@ -340,9 +342,10 @@ __device__ void tiled_down(const BigTeam &, const MXP &P, int l) {
     const MXL &F = P.L[l], &C = P.L[l + 1];
     const int nx = F.nx, ny = F.ny, nx2 = C.nx, W2 = nx2 + 3;
     const int K = 2 * P.nu1, H = K + 2;
-    const int ntiles = ((nx + 1 + MX_TX - 1) / MX_TX) * ((ny + 1 + MX_TY - 1) / MX_TY);
+    const int TX = P.tx[l], TY = P.ty[l];
+    const int ntiles = ((nx + 1 + TX - 1) / TX) * ((ny + 1 + TY - 1) / TY);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const Region g = make_region(F, tile, H, mx_smem, P.tile_cap);
+        const Region g = make_region(F, tile, TX, TY, H, mx_smem, P.tile_cap);
         region_load(F, nullptr, g);   // every level of the cycle starts from e = 0
         __syncthreads();
         for (int h = 0; h < K; h++) {
@@ -384,9 +387,10 @@ __device__ void tiled_up(const BigTeam &, const MXP &P, int l) {
     const MXL &F = P.L[l], &C = P.L[l + 1];
     const int nx = F.nx, ny = F.ny;
     const int K = 2 * P.nu2, H = K;
-    const int ntiles = ((nx + 1 + MX_TX - 1) / MX_TX) * ((ny + 1 + MX_TY - 1) / MX_TY);
+    const int TX = P.tx[l], TY = P.ty[l];
+    const int ntiles = ((nx + 1 + TX - 1) / TX) * ((ny + 1 + TY - 1) / TY);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const Region g = make_region(F, tile, H, mx_smem, P.tile_cap);
+        const Region g = make_region(F, tile, TX, TY, H, mx_smem, P.tile_cap);
         region_load(F, F.e2, g);
         const int ci0 = g.ri0 / 2, cj0 = g.rj0 / 2;
         const int ci1 = min((g.ri0 + g.RW + 1) / 2, C.nx + 2), cj1 = min((g.rj0 + g.RH + 1) / 2, C.ny + 2);
@@ -729,6 +733,22 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     // and the mask per node, sharing the dynamic shared memory with the small cycle
     const int Hmax = 2 * std::max(P.nu1 + 1, P.nu2);
     P.tile_cap = (MX_TX + 2 * Hmax) * (MX_TY + 2 * Hmax);
+    {
+        // per level the largest tile that still gives every CTA of the grid a tile: on the
+        // coarse levels a small tile is a short dependency chain for the CTA that holds it
+        const int grid_est = c->mg_grid_mixed > 0 ? c->mg_grid_mixed : c->num_sms * 3;
+        for (int l = 0; l < c->nlev; l++) {
+            int tx = MX_TX, ty = MX_TY;
+            while (tx > 16) {
+                const long long nt = (long long)((c->lev[l].nx + 1 + tx - 1) / tx) * ((c->lev[l].ny + 1 + ty - 1) / ty);
+                if (nt >= grid_est) break;
+                tx /= 2;
+                ty /= 2;
+            }
+            P.tx[l] = tx;
+            P.ty[l] = ty;
+        }
+    }
     const long long coarse_cap = (long long)((MX_TX + 2 * Hmax) / 2 + 3) * ((MX_TY + 2 * Hmax) / 2 + 3);
     const long long tile_bytes = (long long)P.tile_cap * 9 + coarse_cap * 4 + 16;
     P.tiled = (Ls <= c->nlev - 1 && Ls >= 1 && !getenv("LEPIC_MX_UNTILED") && tile_bytes <= 64 * 1024) ? 1 : 0;
