@@ -241,7 +241,11 @@ def learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step_f
             st = capi.LepicSolveStats()
             ms = timed(lambda: sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, m, C.byref(st)), "solver"))
             row[name] = {"ms": ms, "cycles": st.cycles, "res_l2_rel": st.res_l2_rel}
-            if name == "learned":
+            if name == "fp64_mg":
+                phi_ref = sim.grid(capi.GRID_PHI)
+            if name == "learned":   # the same discrete solution as the FP64 multigrid's
+                phi_l = sim.grid(capi.GRID_PHI)
+                row[name]["phi_rel_err_vs_fp64"] = float(np.abs(phi_l - phi_ref).max() / np.abs(phi_ref).max())
                 cs = capi.LepicCnnStats()
                 sim.check(lib.lepic_gpu_cnn_stats(ctx, C.byref(cs)), "cnn_stats")
                 row[name]["res_ratio"] = cs.last_res_ratio
@@ -259,6 +263,7 @@ def learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step_f
         out[name] = {"ms": mean(name, "ms"), "cycles": mean(name, "cycles"),
                      "res_l2_rel_max": max(r[name]["res_l2_rel"] for r in rows)}
     out["learned"]["res_ratio"] = mean("learned", "res_ratio")
+    out["learned"]["phi_rel_err_vs_fp64_max"] = max(r["learned"]["phi_rel_err_vs_fp64"] for r in rows)
     out["learned"]["accepted"] = mean("learned", "accepted")
     out["online_training_ms_per_solve"] = out["learned_train"]["ms"] - out["learned"]["ms"]
     out["speedup_learned_vs_fp64_mg"] = out["fp64_mg"]["ms"] / out["learned"]["ms"]
