@@ -286,7 +286,10 @@ def run_ours(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    case = configs.make_case(args.config, **({"ppc": args.ppc} if args.ppc else {}))
+    kw = {"ppc": args.ppc} if args.ppc else {}
+    if args.nx:
+        kw.update(nx=args.nx, ny=args.nx)
+    case = configs.make_case(args.config, **kw)
     case.seed = case.seed + 7919 * rank
     sim = GpuSimulation(case, tile=(args.tile, args.tile))
     lib, ctx = sim.lib, sim.ctx
@@ -505,6 +508,7 @@ def main():
     ap.add_argument("--tile", type=int, default=16)
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell (profiling runs)")
+    ap.add_argument("--nx", type=int, default=0, help="override the grid to nx x nx cells (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learn-steps", type=int, default=60, help="PIC steps of online training before the A/B")
     ap.add_argument("--learn-ab", type=int, default=4, help="steps of the learned/plain Poisson A/B")
