@@ -190,7 +190,9 @@ int lepic_gpu_collisions(lepic_ctx *ctx, int32_t it, lepic_mcc_stats *stats);
 int lepic_gpu_push_deposit(lepic_ctx *ctx, int32_t it, lepic_push_stats *stats);
 /* One PIC step, the in-scope body of main.f90:818-1090: calc_rhs -> iterative_solver ->
  * calc_Efield -> part_sorting (MOD(it,nsort)==1) -> collisions (it>1, MOD(it,ns_coll)==1)
- * -> push_deposit.  eps / mode as lepic_gpu_iterative_solver. */
+ * -> [eheating, MOD(it,ns_heat)==0] -> push_deposit -> [part_injection, MOD(it,ns_inj)==0],
+ * the bracketed source steps only after lepic_gpu_set_sources.  eps / mode as
+ * lepic_gpu_iterative_solver. */
 int lepic_gpu_step(lepic_ctx *ctx, int32_t it, double eps, int32_t mode);
 
 /* Copies a device grid (LEPIC_GRID_*) to the host, FP64, in the layouts above. */
@@ -230,6 +232,89 @@ int lepic_gpu_deposit_noalloc(const uint32_t *X, const uint32_t *Y, const float 
  * X, Y are uint32 fixed point in cell units with `shift` fractional bits, VX/VY/VZ float. */
 int lepic_gpu_particle_arrays(lepic_ctx *ctx, int32_t ptype, void **X, void **Y, void **VX,
                               void **VY, void **VZ, int64_t *n_slots, int32_t *shift);
+
+/* ---- particle sources: electron heating and volume injection ---------------------------
+ * The rest of the reference's per-step particle region (main.f90:1033-1068) on the device:
+ * eheating (e_heating.f90:1-112) before the mover, part_injection (part_injection.f90:1-237)
+ * after it, and the heating-region tallies that charge_deposition keeps for the
+ * self-consistent electron temperature (part_expmover.f90:583-605, main.f90:984-1011).
+ * Random numbers come from counter-based streams keyed by (seed, step, species, slot or
+ * injected index), so a run is reproducible whatever the launch shape. */
+#define LEPIC_MAXICP 16   /* heating bands along y (n_icp) */
+
+/* The deck values of read_input.f90:43-55 and :80-97 and main.f90:493-500, lengths in
+ * metres (after the reference's cm -> m and ABS). */
+typedef struct lepic_source_config {
+    int32_t flag_c;            /* 0: slit |x-xa| <= dr, yl_pow <= y <= yr_pow; 1: disk
+                                  (x-xa)^2 + (y-ymax/2)^2 <= dr^2 (xa, dr from xl/xr_pow)  */
+    double xl_pow, xr_pow, yl_pow, yr_pow;
+    /* eheating */
+    int32_t flag_heat;         /* nu_h >= 0 in the deck                                    */
+    int32_t ns_heat;           /* heating every ns_heat steps (MOD(it,ns_heat) == 0)       */
+    int32_t eheat_type;        /* 1: velocity replaced by a Maxwellian draw; 2: increment  */
+    int32_t flag_gpp;          /* 1: Gaussian power profile, nu = 9 Pabs_cor <nu> e^(-9r^2/dr^2) */
+    int32_t n_icp;             /* bands along y (1..LEPIC_MAXICP)                          */
+    int32_t te_update;         /* 1: lepic_gpu_step updates vt itself before each heating
+                                  from this context's tallies (main.f90:984-1011 on one
+                                  rank); 0: the host sets vt (lepic_gpu_set_heating)      */
+    double nudt;               /* nu_h * ns_heat * dt (main.f90:493)                       */
+    double nu_h;               /* [1/s]                                                    */
+    double Pabs[LEPIC_MAXICP]; /* absorbed power per band [W]; Pabs[0] > 0 turns on the
+                                  region tallies and the self-consistent temperature       */
+    double Pabs_cor;           /* Gaussian-profile correction (main.f90:1305-1306)         */
+    double vt[LEPIC_MAXICP];   /* heating thermal speed per band [m/s] (main.f90:1010)     */
+    /* part_injection */
+    int32_t flag_inj;          /* I_inj >= 0 in the deck                                   */
+    int32_t ns_inj;            /* injection every ns_inj steps (MOD(it,ns_inj) == 0)       */
+    int32_t opt_inj;           /* +-1: fixed current; +-2: a pair per lost positive ion;
+                                  < 0: Gaussian loading.  +-3 / +-4 are not supported.     */
+    int32_t flag_Tp;           /* 1: electrons injected at THm (|opt_inj| <= 2)            */
+    int32_t flag_diffsrc;      /* 1: tally -Nm q phi at each injected particle (P_loss(1)) */
+    int32_t tag_neg;           /* 0-based negative-ion species, -1 if none                 */
+    int32_t nproc_mpi;         /* ranks sharing I_inj (one context per rank)               */
+    double I_inj;              /* [A]                                                      */
+    double THm;                /* [eV]                                                     */
+    double ni0[LEPIC_MAXSP];   /* charged-species fractions (read_reactions.f90, main.f90:180) */
+    uint64_t seed;             /* key of the heating and injection streams                 */
+} lepic_source_config;
+
+/* Cumulative tallies since the context was created or last reset; the reference's names. */
+typedef struct lepic_source_tally {
+    double P_heat;                   /* P_loss(2,1): sum 0.5 Nm m (v_new^2 - v_old^2) [J]   */
+    int64_t n_heated;                /* heating events                                     */
+    int64_t n_heat_calls;            /* eheating calls                                     */
+    double P_inj[LEPIC_MAXSP];       /* P_loss(4,ptype): sum 0.5 Nm m v^2 of injected [J]  */
+    double P_src[LEPIC_MAXSP];       /* P_loss(1,ptype): sum -Nm q phi (flag_diffsrc) [J]  */
+    int64_t n_inj[LEPIC_MAXSP];      /* particles injected                                 */
+    int64_t n_inj_last[LEPIC_MAXSP]; /* N_inj of the last injection call                   */
+    int32_t n_icp;
+    int64_t Nh[LEPIC_MAXICP];        /* electrons in the heating region, per band, at the
+                                        last tally (charge_deposition's Nh)                */
+    double sum_dEk[LEPIC_MAXICP];    /* their kinetic energy 0.5 Nm m v^2 (eheat_type 1)   */
+    double vt[LEPIC_MAXICP];         /* heating thermal speed in use                       */
+} lepic_source_tally;
+
+/* Sets (or replaces) the source configuration; flag_heat = flag_inj = 0 turns both off.
+ * lepic_gpu_step then runs eheating before the push and part_injection after it at their
+ * cadences, as main.f90:1033-1068 does. */
+int lepic_gpu_set_sources(lepic_ctx *ctx, const lepic_source_config *cfg);
+/* The host-side temperature update (main.f90:984-1011, e.g. after an MPI reduction of the
+ * tallies): new heating speeds per band (n_icp entries) and the Gaussian-profile factor. */
+int lepic_gpu_set_heating(lepic_ctx *ctx, const double *vt, int32_t n_icp, double Pabs_cor);
+/* eheating (e_heating.f90:1-112) of the electrons at step it (the caller checks the
+ * cadence).  Enqueues only. */
+int lepic_gpu_eheating(lepic_ctx *ctx, int32_t it);
+/* part_injection (part_injection.f90:1-237) of every charged species at step it, in the
+ * species order of main.f90:1057-1064, followed by the deposit of the injected particles
+ * into np (they are deposited in the step they are born, main.f90:1069-1085).  The counts
+ * are computed on the device (fixed current, or the positive-ion losses since the last
+ * injection for |opt_inj| = 2).  Enqueues only. */
+int lepic_gpu_part_injection(lepic_ctx *ctx, int32_t it);
+/* charge_deposition's heating-region tallies (Nh, sum_dEk per band) of the current
+ * electrons.  Enqueues only; lepic_gpu_source_tallies reads them. */
+int lepic_gpu_heating_tally(lepic_ctx *ctx);
+/* Reads the tallies (synchronises); reset != 0 zeroes the cumulative ones afterwards. */
+int lepic_gpu_source_tallies(lepic_ctx *ctx, lepic_source_tally *out, int32_t reset);
 
 /* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
  * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network

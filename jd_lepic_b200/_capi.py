@@ -137,6 +137,32 @@ class LepicCnnStats(C.Structure):
     ]
 
 
+MAXICP = 16
+
+
+class LepicSourceConfig(C.Structure):
+    _fields_ = [
+        ("flag_c", C.c_int32), ("xl_pow", C.c_double), ("xr_pow", C.c_double), ("yl_pow", C.c_double),
+        ("yr_pow", C.c_double),
+        ("flag_heat", C.c_int32), ("ns_heat", C.c_int32), ("eheat_type", C.c_int32), ("flag_gpp", C.c_int32),
+        ("n_icp", C.c_int32), ("te_update", C.c_int32),
+        ("nudt", C.c_double), ("nu_h", C.c_double), ("Pabs", C.c_double * MAXICP), ("Pabs_cor", C.c_double),
+        ("vt", C.c_double * MAXICP),
+        ("flag_inj", C.c_int32), ("ns_inj", C.c_int32), ("opt_inj", C.c_int32), ("flag_Tp", C.c_int32),
+        ("flag_diffsrc", C.c_int32), ("tag_neg", C.c_int32), ("nproc_mpi", C.c_int32),
+        ("I_inj", C.c_double), ("THm", C.c_double), ("ni0", C.c_double * MAXSP), ("seed", C.c_uint64),
+    ]
+
+
+class LepicSourceTally(C.Structure):
+    _fields_ = [
+        ("P_heat", C.c_double), ("n_heated", C.c_int64), ("n_heat_calls", C.c_int64),
+        ("P_inj", C.c_double * MAXSP), ("P_src", C.c_double * MAXSP), ("n_inj", C.c_int64 * MAXSP),
+        ("n_inj_last", C.c_int64 * MAXSP), ("n_icp", C.c_int32), ("Nh", C.c_int64 * MAXICP),
+        ("sum_dEk", C.c_double * MAXICP), ("vt", C.c_double * MAXICP),
+    ]
+
+
 _FP = C.POINTER(C.c_float)
 
 PROTOTYPES = {
@@ -169,6 +195,12 @@ PROTOTYPES = {
     "lepic_gpu_particle_arrays": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.POINTER(_VP), C.POINTER(_VP),
                                             C.POINTER(_VP), C.POINTER(_VP), C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int32)]),
+    "lepic_gpu_set_sources": (C.c_int, [_VP, C.POINTER(LepicSourceConfig)]),
+    "lepic_gpu_set_heating": (C.c_int, [_VP, _DP, C.c_int32, C.c_double]),
+    "lepic_gpu_eheating": (C.c_int, [_VP, C.c_int32]),
+    "lepic_gpu_part_injection": (C.c_int, [_VP, C.c_int32]),
+    "lepic_gpu_heating_tally": (C.c_int, [_VP]),
+    "lepic_gpu_source_tallies": (C.c_int, [_VP, C.POINTER(LepicSourceTally), C.c_int32]),
     "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),
     "lepic_gpu_cnn_stats": (C.c_int, [_VP, C.POINTER(LepicCnnStats)]),
     "lepic_gpu_cnn_net": (_VP, [_VP]),

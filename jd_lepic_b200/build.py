@@ -33,6 +33,7 @@ SOURCES = {
     "mcc.cu": [],
     "noalloc.cu": ["-fmad=false"],
     "cnn.cu": [],
+    "sources.cu": ["-fmad=false"],
 }
 
 

@@ -9,7 +9,7 @@
 #include <vector>
 #include "cnn.cuh"
 
-#define LEPIC_ABI_VERSION 1
+#define LEPIC_ABI_VERSION 2
 
 extern "C" int32_t lepic_gpu_abi_version(void) { return LEPIC_ABI_VERSION; }
 
@@ -276,6 +276,7 @@ extern "C" int lepic_gpu_destroy(lepic_ctx *c) {
     if (!c) return LEPIC_EINVAL;
     cudaStreamSynchronize(c->stream);
     learn_free(c);
+    sources_free(c);
     free_all(c);
     delete c;
     return LEPIC_OK;
@@ -590,7 +591,9 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
             if ((r = sort_species(c, s)) != LEPIC_OK) return r;
     if (it > 1 && g.ns_coll > 0 && it % g.ns_coll == 1)
         if ((r = mcc_collide(c, it)) != LEPIC_OK) return r;
-    return push_deposit(c, it, true);
+    if ((r = sources_before_push(c, it)) != LEPIC_OK) return r;
+    if ((r = push_deposit(c, it, true)) != LEPIC_OK) return r;
+    return sources_after_push(c, it);
 }
 
 extern "C" int lepic_gpu_get_grid(lepic_ctx *c, int32_t which, double *out) {

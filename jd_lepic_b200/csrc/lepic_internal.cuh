@@ -128,6 +128,8 @@ struct lepic_ctx {
     void *learn = nullptr;
     double phi_scale = 1.0;        // max |phi| of the initial potential (network input scale)
     long long n_unknown = 0;       // nodes with bcnd <= 0
+    // particle sources (sources.cu), created by lepic_gpu_set_sources
+    void *src = nullptr;
     // counters
     DevCounters *dcnt = nullptr;
     DevCounters *hcnt = nullptr;  // pinned mirror
@@ -263,6 +265,9 @@ int mcc_collide(lepic_ctx *c, int it);
 int particles_load(lepic_ctx *c, const lepic_load_spec *spec);
 int particles_put(lepic_ctx *c, int ptype, const double *vxp, long long n);
 int particles_get(lepic_ctx *c, int ptype, double *vxp, long long cap, long long *n_out);
+int sources_before_push(lepic_ctx *c, int it);
+int sources_after_push(lepic_ctx *c, int it);
+void sources_free(lepic_ctx *c);
 
 #define LCUDA(call)                                                                     \
     do {                                                                                \

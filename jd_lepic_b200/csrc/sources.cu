@@ -1,0 +1,696 @@
+// sources.cu -- the particle sources of the per-step region: electron heating
+// (e_heating.f90:1-112), the heating-region tallies of charge_deposition
+// (part_expmover.f90:583-605) with the self-consistent temperature update
+// (main.f90:984-1011), and volume injection (part_injection.f90:1-237).
+//
+// Random numbers: Philox4x32-10 streams keyed by the source seed, one counter per decision
+// (slot and step for heating; species, injected index, attempt and step for injection), so
+// every particle's draws are independent of the launch shape and of the other particles.
+// The reference draws from one sequential ran2 stream per OpenMP thread; the two differ in
+// which numbers are drawn, not in the distributions (the oracle holds both forms).
+//
+// Tallies are summed per thread in FP64, reduced per CTA by a fixed tree, and the CTA
+// partials of a fixed grid are added in CTA order by one finishing CTA: the sums do not
+// depend on scheduling, so a run is bit-reproducible.
+//
+// Roofline (HBM): heating and the tally read X, Y of every electron slot (8 B) and the
+// velocities of the electrons in the heating region (12 B); heating writes the velocities of
+// the heated ones (12 B).  Injection writes 20 B per injected particle plus 4 atomics.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include "lepic_internal.cuh"
+
+#define SRC_THREADS 256
+#define SRC_BLOCKS 296          // fixed grid of the tallying kernels (bit-reproducible sums)
+#define INJ_THREADS 128
+#define INJ_BLOCKS 64
+#define INJ_MAX_ATTEMPTS 65536  // rejection-sampling attempts per injected particle
+
+#define TAG_HEAT 0x48454154u    // heating decision
+#define TAG_HEATV 0x48564C31u   // heating velocity
+#define TAG_INJN 0x494E4A4Eu    // injection count rounding
+#define TAG_INJP 0x494E4A50u    // injection position attempt
+#define TAG_INJV 0x494E4A56u    // injection velocity
+
+// device tallies and per-call state of the sources
+struct SrcDev {
+    double P_heat;
+    unsigned long long n_heated, n_heat_calls;
+    double P_inj[LEPIC_MAXSP], P_src[LEPIC_MAXSP];
+    unsigned long long n_inj[LEPIC_MAXSP], n_inj_last[LEPIC_MAXSP];
+    unsigned long long lost_mark[LEPIC_MAXSP];  // n_lost at the last injection (|opt_inj| = 2)
+    long long inj_start[LEPIC_MAXSP];           // first slot of this call's injected particles
+    long long inj_count[LEPIC_MAXSP];
+    long long Nh[LEPIC_MAXICP];
+    double sum_dEk[LEPIC_MAXICP];
+    double vt[LEPIC_MAXICP];
+    double Pabs[LEPIC_MAXICP];
+};
+
+struct SrcState {
+    lepic_source_config cfg;
+    SrcDev *d = nullptr;
+    double *part = nullptr;      // SRC_BLOCKS * (2 * LEPIC_MAXICP) CTA partials
+    int tally_it = INT_MIN;      // the step whose end the last region tally reflects
+};
+
+// The region of read_input.f90:43-55: slit or disk, centre xa, half width dr.
+struct Region {
+    int disk;
+    double xl, xr, yl, yr, xa, dr, ymid;
+};
+
+static Region make_region(const lepic_source_config &s, const lepic_config &g) {
+    Region R;
+    R.disk = s.flag_c;
+    R.xl = s.xl_pow; R.xr = s.xr_pow; R.yl = s.yl_pow; R.yr = s.yr_pow;
+    R.xa = (s.xl_pow + s.xr_pow) / 2.0;
+    R.dr = (s.xr_pow - s.xl_pow) / 2.0;
+    R.ymid = (double)g.ny * g.dy / 2.0;
+    return R;
+}
+
+static SrcState *state(lepic_ctx *c) { return (SrcState *)c->src; }
+
+__device__ __forceinline__ void gauss_pair(double vt, uint32_t a, uint32_t b, double *x, double *y) {
+    // load_gauss.f90:16-39: vp = vt sqrt(-ln(1-r1)), th = 2 pi r2
+    const double pi = 3.141592653589793;
+    const double vp = vt * sqrt(-log(1.0 - u01(a)));
+    double s, co;
+    sincos(2.0 * pi * u01(b), &s, &co);
+    *x = vp * co;
+    *y = vp * s;
+}
+
+// one CTA's sums of NV values per thread (in shared memory, column = thread), reduced by a
+// fixed tree and written to the CTA's partial row
+template <int NT>
+__device__ void cta_reduce_rows(double *col, int nv, double *out_row) {
+    __syncthreads();
+    for (int h = NT / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h)
+            for (int v = 0; v < nv; v++) col[v * NT + threadIdx.x] += col[v * NT + threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < nv; v++) out_row[v] = col[v * NT];
+}
+
+// ---------------------------------------------------------------------------------------
+// eheating (e_heating.f90:33-108) over the electron slots
+struct HeatP {
+    const uint32_t *X, *Y;
+    float *VX, *VY, *VZ;
+    const DevCounters *cnt;
+    const SrcDev *src;
+    Region R;
+    double ux, uy, ymax, dt, nudt, Pabs_cor, Ek;  // Ek = 0.5 Nm m
+    double vt_const;                             // > 0: every band heats at this speed
+    int n_icp, gpp, type;
+    uint32_t it, k0, k1;
+};
+
+__global__ void __launch_bounds__(SRC_THREADS) k_eheat(HeatP P, double *part) {
+    __shared__ double col[2 * SRC_THREADS];
+    const long long n = P.cnt->n_slots[0];
+    double dE = 0.0, cntd = 0.0;
+    const double dr2 = P.R.dr * P.R.dr;
+    for (long long k = blockIdx.x * (long long)SRC_THREADS + threadIdx.x; k < n;
+         k += (long long)SRC_BLOCKS * SRC_THREADS) {
+        const double x = (double)P.X[k] * P.ux, y = (double)P.Y[k] * P.uy;
+        double rp2;
+        bool in;
+        if (P.R.disk == 0) {
+            rp2 = (x - P.R.xa) * (x - P.R.xa);
+            in = rp2 <= dr2 && y >= P.R.yl && y <= P.R.yr;
+        } else {
+            rp2 = (x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid);
+            in = rp2 <= dr2;
+        }
+        if (!in) continue;
+        const float vx = P.VX[k];
+        if (isnan(vx)) continue;  // hole
+        double nu_tmp = P.nudt / P.dt;
+        if (P.gpp) nu_tmp = (P.nudt / P.dt) * 9.0 * P.Pabs_cor * exp(-9.0 * rp2 / dr2);
+        const U4 r = philox4x32_10(U4{(uint32_t)k, (uint32_t)(k >> 32), TAG_HEAT, P.it}, P.k0, P.k1);
+        if (!(u01(r.x) <= nu_tmp * P.dt)) continue;
+        const float vy = P.VY[k], vz = P.VZ[k];
+        int band = (int)(P.n_icp * y / P.ymax);
+        band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
+        const double vt = P.vt_const > 0.0 ? P.vt_const : P.src->vt[band];
+        const U4 q = philox4x32_10(U4{(uint32_t)k, (uint32_t)(k >> 32), TAG_HEATV, P.it}, P.k0, P.k1);
+        double dvx, dvy, dvz, unused;
+        gauss_pair(vt, q.x, q.y, &dvx, &dvy);
+        gauss_pair(vt, q.z, q.w, &dvz, &unused);
+        const double v2old = (double)vx * vx + (double)vy * vy + (double)vz * vz;
+        float nx_, ny_, nz_;
+        if (P.type == 1) {
+            nx_ = (float)dvx; ny_ = (float)dvy; nz_ = (float)dvz;
+        } else {
+            nx_ = (float)((double)vx + dvx); ny_ = (float)((double)vy + dvy); nz_ = (float)((double)vz + dvz);
+        }
+        P.VX[k] = nx_; P.VY[k] = ny_; P.VZ[k] = nz_;
+        dE += P.Ek * ((double)nx_ * nx_ + (double)ny_ * ny_ + (double)nz_ * nz_ - v2old);
+        cntd += 1.0;
+    }
+    col[threadIdx.x] = dE;
+    col[SRC_THREADS + threadIdx.x] = cntd;
+    cta_reduce_rows<SRC_THREADS>(col, 2, part + 2 * blockIdx.x);
+}
+
+// heating-region tally of charge_deposition (part_expmover.f90:583-605)
+struct TallyP {
+    const uint32_t *X, *Y;
+    const float *VX, *VY, *VZ;
+    const DevCounters *cnt;
+    Region R;
+    double ux, uy, ymax, Ek;
+    int n_icp, type;
+};
+
+__global__ void __launch_bounds__(SRC_THREADS) k_heat_tally(TallyP P, double *part) {
+    extern __shared__ double col[];   // [2 * n_icp][SRC_THREADS]: Nh then sum_dEk per band
+    const int nv = 2 * P.n_icp;
+    for (int v = 0; v < nv; v++) col[v * SRC_THREADS + threadIdx.x] = 0.0;
+    const long long n = P.cnt->n_slots[0];
+    const double dr2 = P.R.dr * P.R.dr;
+    for (long long k = blockIdx.x * (long long)SRC_THREADS + threadIdx.x; k < n;
+         k += (long long)SRC_BLOCKS * SRC_THREADS) {
+        const double x = (double)P.X[k] * P.ux, y = (double)P.Y[k] * P.uy;
+        if (P.R.disk == 0) {
+            if (x < P.R.xl || x > P.R.xr || y < P.R.yl || y > P.R.yr) continue;
+        } else {
+            if ((x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) > dr2) continue;
+        }
+        const float vx = P.VX[k];
+        if (isnan(vx)) continue;
+        int band = (int)(P.n_icp * y / P.ymax);
+        band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
+        col[band * SRC_THREADS + threadIdx.x] += 1.0;
+        if (P.type == 1) {
+            const float vy = P.VY[k], vz = P.VZ[k];
+            col[(P.n_icp + band) * SRC_THREADS + threadIdx.x] +=
+                P.Ek * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+        }
+    }
+    cta_reduce_rows<SRC_THREADS>(col, nv, part + (size_t)nv * blockIdx.x);
+}
+
+// sums the CTA partials in CTA order: dst[v] (+)= sum_b part[b*nv + v]
+__global__ void k_src_finish(const double *part, int nblocks, int nv, double *dst, int accumulate) {
+    const int v = threadIdx.x;
+    if (v >= nv) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; b++) s += part[(size_t)b * nv + v];
+    dst[v] = accumulate ? dst[v] + s : s;
+}
+
+__global__ void k_heat_finish(const double *part, SrcDev *src) {
+    if (threadIdx.x != 0) return;
+    double dE = 0.0, cnt = 0.0;
+    for (int b = 0; b < SRC_BLOCKS; b++) { dE += part[2 * b]; cnt += part[2 * b + 1]; }
+    src->P_heat += dE;
+    src->n_heated += (unsigned long long)cnt;
+    src->n_heat_calls += 1;
+}
+
+__global__ void k_tally_finish(const double *part, int n_icp, SrcDev *src) {
+    const int v = threadIdx.x;
+    const int nv = 2 * n_icp;
+    if (v >= nv) return;
+    double s = 0.0;
+    for (int b = 0; b < SRC_BLOCKS; b++) s += part[(size_t)b * nv + v];
+    if (v < n_icp) src->Nh[v] = (long long)s;
+    else src->sum_dEk[v - n_icp] = s;
+}
+
+// main.f90:1003-1010 for one rank: Te from the tallies, vt = sqrt(2 qe Te / |m|)
+__global__ void k_te_update(SrcDev *src, int n_icp, int type, double nu_h, double Nm, double qe, double mass) {
+    const int b = threadIdx.x;
+    if (b >= n_icp) return;
+    const long long nh = src->Nh[b];
+    if (nh <= 0) return;  // the reference divides by zero here; the previous speed is kept
+    double Te;
+    if (type == 1) Te = (2.0 / 3.0) * (src->sum_dEk[b] + src->Pabs[b] / nu_h) / (Nm * qe * (double)nh);
+    else Te = (2.0 / 3.0) * (src->Pabs[b] / nu_h) / (Nm * qe * (double)nh);
+    src->vt[b] = sqrt(2.0 * qe * Te / fabs(mass));
+}
+
+// ---------------------------------------------------------------------------------------
+// part_injection (part_injection.f90:49-233)
+struct InjPlanP {
+    DevCounters *cnt;
+    SrcDev *src;
+    int ntype, opt2, tag_neg;
+    long long cap[LEPIC_MAXSP];
+    double dN_fixed[LEPIC_MAXSP];  // |opt_inj| = 1: I_inj ns_inj dt ni0 / (qe Nm(1)) / nproc_mpi
+    double ni0[LEPIC_MAXSP];
+    uint32_t it, k0, k1;
+};
+
+// the counts of part_injection.f90:49-75 for every species, in the order of main.f90:1058
+__global__ void k_inj_plan(InjPlanP P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long lost[LEPIC_MAXSP];
+    for (int s = 0; s < P.ntype; s++) lost[s] = (long long)(P.cnt->n_lost[s] - P.src->lost_mark[s]);
+    long long pos_lost = 0;  // SUM(N_inj(2:ntype)) - N_inj(tag_neg)
+    for (int s = 1; s < P.ntype; s++)
+        if (s != P.tag_neg) pos_lost += lost[s];
+    for (int s = 0; s < P.ntype; s++) {
+        long long N;
+        bool draw = true;
+        double dN = 0.0;
+        if (P.opt2) {
+            if (s == 0 || s == P.tag_neg) dN = P.ni0[s] * (double)pos_lost;
+            else { N = lost[s]; draw = false; }  // the positive ion's own losses
+        } else {
+            dN = P.dN_fixed[s];
+        }
+        if (draw) {
+            N = (long long)dN;
+            const U4 r = philox4x32_10(U4{(uint32_t)s, 0u, TAG_INJN, P.it}, P.k0, P.k1);
+            if (u01(r.x) <= dN - (double)N) N += 1;
+        }
+        const long long start = P.cnt->n_slots[s];
+        if (start + N > P.cap[s]) {  // part_injection.f90:146-150
+            set_err(P.cnt, LERR_CAPACITY, 700 + s);
+            N = 0;
+        }
+        P.src->inj_start[s] = start;
+        P.src->inj_count[s] = N;
+        P.src->n_inj[s] += (unsigned long long)N;
+        P.src->n_inj_last[s] = (unsigned long long)N;
+        P.cnt->n_slots[s] = start + N;
+        P.cnt->n_alive[s] += N;
+    }
+    for (int s = 0; s < P.ntype; s++) P.src->lost_mark[s] = P.cnt->n_lost[s];
+}
+
+struct InjP {
+    SrcDev *src;
+    DevCounters *cnt;
+    int ntype, nx, ny, S, W;
+    int opt, slit, flag_nmn, diffsrc;
+    Region R;
+    double dx, dy, xmax, ymax;
+    double vt[LEPIC_MAXSP], Ek[LEPIC_MAXSP], qphi[LEPIC_MAXSP];  // qphi = -Nm q
+    const uint8_t *cellwall;
+    const double *phi;
+    uint32_t *X[LEPIC_MAXSP], *Y[LEPIC_MAXSP];
+    float *VX[LEPIC_MAXSP], *VY[LEPIC_MAXSP], *VZ[LEPIC_MAXSP];
+    unsigned long long *acc[LEPIC_MAXSP];
+    uint32_t it, k0, k1;
+};
+
+__device__ __forceinline__ void inj_cic(int S, uint32_t X, uint32_t Y, uint64_t *w) {
+    // the push's integer CIC weights (exact products of the offsets, scaled to 2^44)
+    const uint32_t mask = (1u << S) - 1u, A = 1u << S;
+    const uint32_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
+    w[0] = (uint64_t)ax * ay; w[1] = (uint64_t)fx * ay; w[2] = (uint64_t)fx * fy; w[3] = (uint64_t)ax * fy;
+    const int sh = 2 * S - LEPIC_DEP_SHIFT;
+    for (int k = 0; k < 4; k++) {
+        if (sh > 0) w[k] = (w[k] + (1ull << (sh - 1))) >> sh;
+        else if (sh < 0) w[k] <<= -sh;
+    }
+}
+
+__global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
+    __shared__ double col[2 * LEPIC_MAXSP * INJ_THREADS];  // P_inj then P_src per species
+    for (int v = 0; v < 2 * LEPIC_MAXSP; v++) col[v * INJ_THREADS + threadIdx.x] = 0.0;
+    long long total = 0;
+    for (int s = 0; s < P.ntype; s++) total += P.src->inj_count[s];
+    const double dr2 = P.R.dr * P.R.dr;
+    for (long long t = blockIdx.x * (long long)INJ_THREADS + threadIdx.x; t < total;
+         t += (long long)INJ_BLOCKS * INJ_THREADS) {
+        int s = 0;
+        long long j = t;
+        while (j >= P.src->inj_count[s]) { j -= P.src->inj_count[s]; s++; }
+        // position: part_injection.f90:85-137, redrawn until the cell is not all walls
+        double x = 0.0, y = 0.0;
+        int ix = 1, iy = 1;
+        bool ok = false;
+        for (uint32_t a = 0; a < INJ_MAX_ATTEMPTS && !ok; a++) {
+            const U4 r = philox4x32_10(U4{(uint32_t)j, (a << 3) | (uint32_t)s, TAG_INJP, P.it}, P.k0, P.k1);
+            if (P.opt > 0) {
+                x = u01(r.x) * (P.R.xl - P.R.xr) + P.R.xr;
+                if (P.R.disk) {
+                    y = u01(r.y) * (2.0 * P.R.dr) + P.R.ymid - P.R.dr;
+                    if ((x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) > dr2) continue;
+                }
+            } else if (!P.R.disk) {
+                double g0, g1;
+                gauss_pair(P.R.dr, r.x, r.y, &g0, &g1);
+                x = g0 + P.R.xa;
+                if (P.flag_nmn == 1 && P.R.xa == 0.0) x = fabs(x);
+                if (x < P.R.xa - 4.0 * P.R.dr || x > P.R.xa + 4.0 * P.R.dr || x < 0.0 || x > P.xmax) continue;
+            } else {
+                double g0, g1;
+                gauss_pair(P.R.dr, r.x, r.y, &g0, &g1);
+                x = g0 + P.R.xa;
+                y = g1 + P.R.ymid;
+                if ((x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) > 4.0 * dr2 || x < 0.0 ||
+                    x > P.xmax || y < 0.0 || y > P.ymax)
+                    continue;
+            }
+            if (!P.R.disk) y = u01(r.z) * (P.R.yl - P.R.yr) + P.R.yr;
+            ix = (int)(x / P.dx) + 1;
+            iy = (int)(y / P.dy) + 1;
+            ix = ix < 1 ? 1 : (ix > P.nx + 1 ? P.nx + 1 : ix);
+            iy = iy < 1 ? 1 : (iy > P.ny + 1 ? P.ny + 1 : iy);
+            if (P.cellwall[ix + (long long)iy * (P.nx + 2)]) continue;
+            ok = true;
+        }
+        const long long slot = P.src->inj_start[s] + j;
+        if (!ok) {  // a region with no room: the slot stays a hole and the call fails
+            set_err(P.cnt, LERR_RANGE, 710 + s);
+            P.VX[s][slot] = __int_as_float(0x7fc00000);
+            P.X[s][slot] = 0; P.Y[s][slot] = 0; P.VY[s][slot] = 0.f; P.VZ[s][slot] = 0.f;
+            continue;
+        }
+        // velocity: part_injection.f90:152-194, with its draw order: the first particle of a
+        // call takes (vx, vy) and vz from the second pair (so vz = vx), the next takes its own
+        // (vx, vy) and the saved second component of the previous particle's second pair
+        const double vt = P.vt[s];
+        const U4 q = philox4x32_10(U4{(uint32_t)j, (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
+        double vx, vy, vz;
+        if ((j & 1) == 0) {
+            gauss_pair(vt, q.z, q.w, &vx, &vy);
+            vz = vx;
+        } else {
+            gauss_pair(vt, q.x, q.y, &vx, &vy);
+            const U4 qp = philox4x32_10(U4{(uint32_t)(j - 1), (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
+            double unused;
+            gauss_pair(vt, qp.z, qp.w, &unused, &vz);
+        }
+        // fixed point: x/h truncated, so the cell is the reference's INT(x/h)
+        const double fx = x / P.dx * (double)(1u << P.S), fy = y / P.dy * (double)(1u << P.S);
+        const long long xl = ((long long)P.nx << P.S) - 1, yl = ((long long)P.ny << P.S) - 1;
+        const uint32_t Xf = (uint32_t)min((long long)fx, xl), Yf = (uint32_t)min((long long)fy, yl);
+        const float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
+        P.X[s][slot] = Xf; P.Y[s][slot] = Yf;
+        P.VX[s][slot] = fvx; P.VY[s][slot] = fvy; P.VZ[s][slot] = fvz;
+        // deposit (the injected particle is in this step's np)
+        uint64_t w[4];
+        inj_cic(P.S, Xf, Yf, w);
+        const long long n00 = (long long)((Xf >> P.S) + 1) + (long long)((Yf >> P.S) + 1) * P.W;
+        unsigned long long *a = P.acc[s];
+        if (w[0]) atomicAdd(a + n00, (unsigned long long)w[0]);
+        if (w[1]) atomicAdd(a + n00 + 1, (unsigned long long)w[1]);
+        if (w[2]) atomicAdd(a + n00 + P.W + 1, (unsigned long long)w[2]);
+        if (w[3]) atomicAdd(a + n00 + P.W, (unsigned long long)w[3]);
+        col[s * INJ_THREADS + threadIdx.x] +=
+            P.Ek[s] * ((double)fvx * fvx + (double)fvy * fvy + (double)fvz * fvz);
+        if (P.diffsrc) {  // part_injection.f90:216-231
+            const double px = ((double)ix * P.dx - x) / P.dx, py = ((double)iy * P.dy - y) / P.dy;
+            const long long m = ix + (long long)iy * P.W;
+            const double phip = px * py * P.phi[m] + (1.0 - px) * py * P.phi[m + 1] +
+                                (1.0 - px) * (1.0 - py) * P.phi[m + P.W + 1] + px * (1.0 - py) * P.phi[m + P.W];
+            col[(LEPIC_MAXSP + s) * INJ_THREADS + threadIdx.x] += P.qphi[s] * phip;
+        }
+    }
+    cta_reduce_rows<INJ_THREADS>(col, 2 * LEPIC_MAXSP, part + (size_t)2 * LEPIC_MAXSP * blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+static void keys(const lepic_source_config &s, uint32_t *k0, uint32_t *k1) {
+    *k0 = (uint32_t)s.seed;
+    *k1 = (uint32_t)(s.seed >> 32) ^ 0x53524331u;
+}
+
+void sources_free(lepic_ctx *c) {
+    SrcState *S = state(c);
+    if (!S) return;
+    if (S->d) cudaFree(S->d);
+    if (S->part) cudaFree(S->part);
+    delete S;
+    c->src = nullptr;
+}
+
+static int check_config(lepic_ctx *c, const lepic_source_config &s) {
+    const lepic_config &g = c->cfg;
+    const double xmax = g.nx * g.dx, ymax = g.ny * g.dy;
+    auto bad = [&](const char *m) { c->last_err = std::string("sources: ") + m; return LEPIC_EINVAL; };
+    if (!s.flag_heat && !s.flag_inj) return LEPIC_OK;
+    if (s.flag_c != 0 && s.flag_c != 1) return bad("flag_c must be 0 or 1");
+    if (!(s.xl_pow >= 0 && s.xr_pow > s.xl_pow)) return bad("need 0 <= xl_pow < xr_pow");
+    const double xa = (s.xl_pow + s.xr_pow) / 2.0, dr = (s.xr_pow - s.xl_pow) / 2.0;
+    if (s.flag_c == 0) {
+        if (s.xr_pow > xmax || !(s.yl_pow >= 0 && s.yr_pow >= s.yl_pow && s.yr_pow <= ymax))
+            return bad("slit region outside the box");
+    } else if (xa + dr > xmax || ymax / 2.0 - dr < 0.0) {
+        return bad("disk region outside the box");
+    }
+    if (s.flag_heat) {
+        if (s.ns_heat < 1) return bad("ns_heat < 1");
+        if (s.eheat_type != 1 && s.eheat_type != 2) return bad("eheat_type must be 1 or 2");
+        if (s.n_icp < 1 || s.n_icp > LEPIC_MAXICP) return bad("n_icp out of range");
+        if (!(s.nudt >= 0.0 && s.nudt <= 1.0)) return bad("nu*dt > 1 (main.f90:519-523)");
+        if (s.flag_gpp && s.nudt * 9.0 * s.Pabs_cor > 1.0) return bad("nu0*dt > 1 for the Gaussian profile");
+        if (s.te_update && !(s.nu_h > 0.0)) return bad("te_update needs nu_h > 0");
+        for (int b = 0; b < s.n_icp; b++)
+            if (!(s.vt[b] >= 0.0)) return bad("vt must be >= 0");
+    }
+    if (s.flag_inj) {
+        if (s.ns_inj < 1) return bad("ns_inj < 1");
+        const int a = std::abs(s.opt_inj);
+        if (a != 1 && a != 2) return bad("opt_inj must be +-1 or +-2 (beam and cathode options are not built)");
+        if (s.nproc_mpi < 1) return bad("nproc_mpi < 1");
+        if (s.tag_neg < -1 || s.tag_neg >= g.ntype || s.tag_neg == 0) return bad("tag_neg out of range");
+        if (s.I_inj < 0.0) return bad("I_inj < 0");
+    }
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_set_sources(lepic_ctx *c, const lepic_source_config *cfg) {
+    if (!c || !cfg) return LEPIC_EINVAL;
+    int r = check_config(c, *cfg);
+    if (r != LEPIC_OK) return r;
+    SrcState *S = state(c);
+    if (!S) {
+        S = new (std::nothrow) SrcState;
+        if (!S) return LEPIC_ENOMEM;
+        c->src = S;
+        if (cudaMalloc((void **)&S->d, sizeof(SrcDev)) != cudaSuccess ||
+            cudaMalloc((void **)&S->part, sizeof(double) * SRC_BLOCKS * 2 * LEPIC_MAXICP) != cudaSuccess) {
+            c->last_err = "sources: cudaMalloc failed";
+            sources_free(c);
+            return LEPIC_ENOMEM;
+        }
+        LCUDA(cudaMemsetAsync(S->d, 0, sizeof(SrcDev), c->stream));
+    }
+    S->cfg = *cfg;
+    S->tally_it = INT_MIN;
+    // heating speeds, and the loss mark from which |opt_inj| = 2 counts
+    LCUDA(cudaMemcpyAsync(S->d->vt, cfg->vt, sizeof(double) * LEPIC_MAXICP, cudaMemcpyHostToDevice, c->stream));
+    LCUDA(cudaMemcpyAsync(S->d->Pabs, cfg->Pabs, sizeof(double) * LEPIC_MAXICP, cudaMemcpyHostToDevice, c->stream));
+    LCUDA(cudaMemcpyAsync(S->d->lost_mark, c->dcnt->n_lost, sizeof(unsigned long long) * LEPIC_MAXSP,
+                          cudaMemcpyDeviceToDevice, c->stream));
+    LCUDA(cudaStreamSynchronize(c->stream));
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_set_heating(lepic_ctx *c, const double *vt, int32_t n_icp, double Pabs_cor) {
+    if (!c || !vt || !state(c)) return LEPIC_EINVAL;
+    SrcState *S = state(c);
+    if (n_icp != S->cfg.n_icp) { c->last_err = "set_heating: n_icp differs from the source config"; return LEPIC_EINVAL; }
+    for (int b = 0; b < n_icp; b++)
+        if (!(vt[b] >= 0.0)) return LEPIC_EINVAL;
+    if (S->cfg.flag_gpp && S->cfg.nudt * 9.0 * Pabs_cor > 1.0) {
+        c->last_err = "nu0*dt > 1 for the Gaussian profile (main.f90:1308-1311)";
+        return LEPIC_EINVAL;
+    }
+    S->cfg.Pabs_cor = Pabs_cor;
+    for (int b = 0; b < n_icp; b++) S->cfg.vt[b] = vt[b];
+    LCUDA(cudaMemcpyAsync(S->d->vt, S->cfg.vt, sizeof(double) * LEPIC_MAXICP, cudaMemcpyHostToDevice, c->stream));
+    LCUDA(cudaStreamSynchronize(c->stream));
+    return LEPIC_OK;
+}
+
+static int run_heating(lepic_ctx *c, int it) {
+    SrcState *S = state(c);
+    const lepic_source_config &s = S->cfg;
+    const lepic_config &g = c->cfg;
+    SpeciesBuf &B = c->sp[0];
+    HeatP P;
+    memset(&P, 0, sizeof(P));
+    P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+    P.cnt = c->dcnt; P.src = S->d;
+    P.R = make_region(s, g);
+    P.ux = g.dx * std::ldexp(1.0, -c->S); P.uy = g.dy * std::ldexp(1.0, -c->S);
+    P.ymax = g.ny * g.dy; P.dt = g.dt; P.nudt = s.nudt; P.Pabs_cor = s.Pabs_cor;
+    P.Ek = 0.5 * g.Nm[0] * g.mass[0];
+    P.vt_const = s.flag_inj ? g.vt0[0] : 0.0;  // main.f90:1034
+    P.n_icp = s.n_icp; P.gpp = s.flag_gpp; P.type = s.eheat_type;
+    P.it = (uint32_t)it;
+    keys(s, &P.k0, &P.k1);
+    k_eheat<<<SRC_BLOCKS, SRC_THREADS, 0, c->stream>>>(P, S->part);
+    LCUDA(cudaGetLastError());
+    k_heat_finish<<<1, 32, 0, c->stream>>>(S->part, S->d);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+static int run_tally(lepic_ctx *c) {
+    SrcState *S = state(c);
+    const lepic_source_config &s = S->cfg;
+    const lepic_config &g = c->cfg;
+    SpeciesBuf &B = c->sp[0];
+    TallyP P;
+    memset(&P, 0, sizeof(P));
+    P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+    P.cnt = c->dcnt;
+    P.R = make_region(s, g);
+    P.ux = g.dx * std::ldexp(1.0, -c->S); P.uy = g.dy * std::ldexp(1.0, -c->S);
+    P.ymax = g.ny * g.dy;
+    P.Ek = 0.5 * g.Nm[0] * g.mass[0];
+    P.n_icp = std::max(1, std::min(s.n_icp, LEPIC_MAXICP));
+    P.type = s.eheat_type;
+    const size_t smem = sizeof(double) * 2 * P.n_icp * SRC_THREADS;
+    static bool attr[64] = {false};
+    if (!attr[c->dev & 63]) {
+        LCUDA(cudaFuncSetAttribute(k_heat_tally, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(double) * 2 * LEPIC_MAXICP * SRC_THREADS)));
+        attr[c->dev & 63] = true;
+    }
+    k_heat_tally<<<SRC_BLOCKS, SRC_THREADS, smem, c->stream>>>(P, S->part);
+    LCUDA(cudaGetLastError());
+    k_tally_finish<<<1, 2 * LEPIC_MAXICP, 0, c->stream>>>(S->part, P.n_icp, S->d);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+static int run_injection(lepic_ctx *c, int it) {
+    SrcState *S = state(c);
+    const lepic_source_config &s = S->cfg;
+    const lepic_config &g = c->cfg;
+    InjPlanP Q;
+    memset(&Q, 0, sizeof(Q));
+    Q.cnt = c->dcnt; Q.src = S->d; Q.ntype = g.ntype;
+    Q.opt2 = std::abs(s.opt_inj) == 2;
+    Q.tag_neg = s.tag_neg;
+    for (int sp = 0; sp < g.ntype; sp++) {
+        Q.cap[sp] = c->sp[sp].cap;
+        Q.ni0[sp] = s.ni0[sp];
+        Q.dN_fixed[sp] = s.I_inj * s.ns_inj * g.dt * s.ni0[sp] / (g.qe * g.Nm[0]) / (double)s.nproc_mpi;
+    }
+    Q.it = (uint32_t)it;
+    keys(s, &Q.k0, &Q.k1);
+    k_inj_plan<<<1, 32, 0, c->stream>>>(Q);
+    LCUDA(cudaGetLastError());
+
+    InjP P;
+    memset(&P, 0, sizeof(P));
+    P.src = S->d; P.cnt = c->dcnt; P.ntype = g.ntype;
+    P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
+    P.opt = s.opt_inj; P.flag_nmn = g.flag_nmn; P.diffsrc = s.flag_diffsrc;
+    P.R = make_region(s, g);
+    P.dx = g.dx; P.dy = g.dy; P.xmax = g.nx * g.dx; P.ymax = g.ny * g.dy;
+    for (int sp = 0; sp < g.ntype; sp++) {
+        double vt = g.vt0[sp];
+        if (std::abs(s.opt_inj) <= 2 && s.flag_Tp == 1 && sp == 0) vt = std::sqrt(2.0 * g.qe * s.THm / std::fabs(g.mass[0]));
+        P.vt[sp] = vt;
+        P.Ek[sp] = 0.5 * g.Nm[sp] * g.mass[sp];
+        P.qphi[sp] = -g.Nm[sp] * g.charge[sp];
+        SpeciesBuf &B = c->sp[sp];
+        P.X[sp] = B.X[B.cur]; P.Y[sp] = B.Y[B.cur];
+        P.VX[sp] = B.VX[B.cur]; P.VY[sp] = B.VY[B.cur]; P.VZ[sp] = B.VZ[B.cur];
+        P.acc[sp] = B.acc;
+    }
+    P.cellwall = c->cellwall;
+    P.phi = c->phi;
+    P.it = (uint32_t)it;
+    keys(s, &P.k0, &P.k1);
+    k_inject<<<INJ_BLOCKS, INJ_THREADS, 0, c->stream>>>(P, S->part);
+    LCUDA(cudaGetLastError());
+    // P_inj[] and P_src[] are adjacent in SrcDev: one finishing pass adds both
+    static_assert(offsetof(SrcDev, P_src) == offsetof(SrcDev, P_inj) + sizeof(double) * LEPIC_MAXSP, "layout");
+    k_src_finish<<<1, 2 * LEPIC_MAXSP, 0, c->stream>>>(S->part, INJ_BLOCKS, 2 * LEPIC_MAXSP, S->d->P_inj, 1);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+static int te_update(lepic_ctx *c) {
+    SrcState *S = state(c);
+    const lepic_source_config &s = S->cfg;
+    const lepic_config &g = c->cfg;
+    k_te_update<<<1, LEPIC_MAXICP, 0, c->stream>>>(S->d, s.n_icp, s.eheat_type, s.nu_h, g.Nm[0], g.qe, g.mass[0]);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_eheating(lepic_ctx *c, int32_t it) {
+    if (!c || !state(c) || !state(c)->cfg.flag_heat) return LEPIC_EINVAL;
+    return run_heating(c, it);
+}
+
+extern "C" int lepic_gpu_part_injection(lepic_ctx *c, int32_t it) {
+    if (!c || !state(c) || !state(c)->cfg.flag_inj) return LEPIC_EINVAL;
+    return run_injection(c, it);
+}
+
+extern "C" int lepic_gpu_heating_tally(lepic_ctx *c) {
+    if (!c || !state(c)) return LEPIC_EINVAL;
+    return run_tally(c);
+}
+
+extern "C" int lepic_gpu_source_tallies(lepic_ctx *c, lepic_source_tally *out, int32_t reset) {
+    if (!c || !out || !state(c)) return LEPIC_EINVAL;
+    SrcState *S = state(c);
+    SrcDev h;
+    LCUDA(cudaMemcpyAsync(&h, S->d, sizeof(SrcDev), cudaMemcpyDeviceToHost, c->stream));
+    int r = lepic_gpu_sync(c);
+    memset(out, 0, sizeof(*out));
+    out->P_heat = h.P_heat;
+    out->n_heated = (int64_t)h.n_heated;
+    out->n_heat_calls = (int64_t)h.n_heat_calls;
+    for (int s = 0; s < LEPIC_MAXSP; s++) {
+        out->P_inj[s] = h.P_inj[s];
+        out->P_src[s] = h.P_src[s];
+        out->n_inj[s] = (int64_t)h.n_inj[s];
+        out->n_inj_last[s] = (int64_t)h.n_inj_last[s];
+    }
+    out->n_icp = S->cfg.n_icp;
+    for (int b = 0; b < LEPIC_MAXICP; b++) {
+        out->Nh[b] = h.Nh[b];
+        out->sum_dEk[b] = h.sum_dEk[b];
+        out->vt[b] = h.vt[b];
+    }
+    if (reset) {
+        SrcDev z = h;
+        z.P_heat = 0.0; z.n_heated = 0; z.n_heat_calls = 0;
+        for (int s = 0; s < LEPIC_MAXSP; s++) { z.P_inj[s] = 0.0; z.P_src[s] = 0.0; z.n_inj[s] = 0; }
+        LCUDA(cudaMemcpyAsync(S->d, &z, sizeof(SrcDev), cudaMemcpyHostToDevice, c->stream));
+        LCUDA(cudaStreamSynchronize(c->stream));
+    }
+    return r;
+}
+
+// The source steps of lepic_gpu_step around the push (main.f90:984-1011, 1033-1068).
+int sources_before_push(lepic_ctx *c, int it) {
+    SrcState *S = state(c);
+    if (!S || !S->cfg.flag_heat || it % S->cfg.ns_heat != 0) return LEPIC_OK;
+    const lepic_source_config &s = S->cfg;
+    if (s.te_update && s.Pabs[0] > 0.0 && !s.flag_inj) {
+        int r;
+        if (S->tally_it != it - 1 && (r = run_tally(c)) != LEPIC_OK) return r;
+        if ((r = te_update(c)) != LEPIC_OK) return r;
+    }
+    return run_heating(c, it);
+}
+
+int sources_after_push(lepic_ctx *c, int it) {
+    SrcState *S = state(c);
+    if (!S) return LEPIC_OK;
+    const lepic_source_config &s = S->cfg;
+    int r;
+    if (s.flag_inj && it % s.ns_inj == 0)
+        if ((r = run_injection(c, it)) != LEPIC_OK) return r;
+    if (s.flag_heat && s.Pabs[0] > 0.0 && (it + 1) % s.ns_heat == 0) {
+        if ((r = run_tally(c)) != LEPIC_OK) return r;
+        S->tally_it = it;
+    }
+    return LEPIC_OK;
+}

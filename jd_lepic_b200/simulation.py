@@ -243,6 +243,33 @@ class GpuSimulation:
         return {"n_cand": list(st.n_cand[:n]), "n_coll": list(st.n_coll[:self.xs.ncol]),
                 "n_add": list(st.n_add[:n]), "n_overflow": st.n_overflow, "nu_max": list(st.nu_max[:n])}
 
+    # particle sources (e_heating.f90, part_injection.f90) -------------------------------
+    def set_sources(self, cfg: capi.LepicSourceConfig):
+        self._src_cfg = cfg
+        self.check(self.lib.lepic_gpu_set_sources(self.ctx, C.byref(cfg)), "set_sources")
+
+    def set_heating(self, vt, Pabs_cor: float = 1.0):
+        a = np.ascontiguousarray(vt, dtype=np.float64)
+        self.check(self.lib.lepic_gpu_set_heating(self.ctx, _dp(a), a.shape[0], Pabs_cor), "set_heating")
+
+    def eheating(self, it: int):
+        self.check(self.lib.lepic_gpu_eheating(self.ctx, it), "eheating")
+
+    def inject(self, it: int):
+        self.check(self.lib.lepic_gpu_part_injection(self.ctx, it), "part_injection")
+
+    def heating_tally(self):
+        self.check(self.lib.lepic_gpu_heating_tally(self.ctx), "heating_tally")
+
+    def source_tallies(self, reset: bool = False) -> dict:
+        t = capi.LepicSourceTally()
+        self.check(self.lib.lepic_gpu_source_tallies(self.ctx, C.byref(t), 1 if reset else 0), "source_tallies")
+        n, b = self.sp.ntype, t.n_icp
+        return {"P_heat": t.P_heat, "n_heated": t.n_heated, "n_heat_calls": t.n_heat_calls,
+                "P_inj": list(t.P_inj[:n]), "P_src": list(t.P_src[:n]), "n_inj": list(t.n_inj[:n]),
+                "n_inj_last": list(t.n_inj_last[:n]), "Nh": list(t.Nh[:b]), "sum_dEk": list(t.sum_dEk[:b]),
+                "vt": list(t.vt[:b])}
+
     def stream_ptr(self) -> int:
         return self.lib.lepic_gpu_stream(self.ctx) or 0
 

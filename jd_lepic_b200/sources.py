@@ -1,0 +1,74 @@
+"""Deck values of the particle sources -> ``lepic_source_config``.
+
+The conversions the reference applies while reading its input deck and starting up:
+the heating region in cm with a negative x bound selecting the disk (read_input.f90:43-55),
+the driver count, absorbed powers and heating frequency (read_input.f90:80-89), the injected
+current and its option (read_input.f90:90-98), the injected-electron temperature THm whose
+sign selects flag_Tp (read_input.f90:147-151), and the derived heating parameters nudt,
+eheat_type and flag_gpp (main.f90:493-500).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+from . import _capi as capi
+
+
+@dataclass
+class SourceDeck:
+    heat_region_cm: tuple = (0.0, 0.0, 0.0, 0.0)  # xl_pow, xr_pow, yl_pow, yr_pow [cm]
+    n_icp: int = 1                                  # drivers (< 0: iterative Pabs)
+    Pabs: tuple = (0.0,)                            # absorbed power per driver [W] (<= 0: fixed Te)
+    nu_h: float = -1.0                              # heating frequency [1/s] (< 0: off)
+    I_inj: float = -1.0                             # injected current [A] (< 0: off)
+    opt_inj: int = 1                                # 1 fixed current, 2 pair per lost ion, < 0 Gaussian
+    THm: float = 0.0                                # [eV]; < 0 sets flag_Tp
+    ns_heat: int = 4
+    ns_inj: int = 1
+    ni0: tuple = (1.0,)                             # charged-species fractions
+    tag_neg: int = -1                               # 0-based negative-ion species, -1 none
+    flag_diffsrc: int = 0
+    nproc_mpi: int = 1
+    te_update: int = 1
+    vt: tuple = field(default_factory=tuple)        # initial heating speed per band [m/s]
+    seed: int = 12345
+
+
+def source_config(d: SourceDeck, dt: float, vt0_e: float) -> capi.LepicSourceConfig:
+    """The lepic_source_config of a deck; vt0_e is the electron vt0 (the initial heating speed
+    when the deck gives none, and the constant one when particles are injected)."""
+    c = capi.LepicSourceConfig()
+    xl, xr, yl, yr = (v * 1e-2 for v in d.heat_region_cm)
+    c.flag_c = 1 if (xl < 0.0 or xr < 0.0) else 0
+    c.xl_pow, c.xr_pow, c.yl_pow, c.yr_pow = abs(xl), abs(xr), yl, yr
+    n_icp = abs(int(d.n_icp))
+    if not 1 <= n_icp <= capi.MAXICP:
+        raise ValueError(f"n_icp={d.n_icp} out of range")
+    c.n_icp = n_icp
+    c.flag_heat = 0 if d.nu_h < 0.0 else 1
+    c.nu_h = max(d.nu_h, 0.0)
+    c.ns_heat = d.ns_heat
+    c.nudt = c.nu_h * (d.ns_heat * dt)
+    pabs = list(d.Pabs) + [d.Pabs[-1]] * (n_icp - len(d.Pabs))
+    for b in range(n_icp):
+        c.Pabs[b] = pabs[b]
+    c.eheat_type = 1
+    c.flag_gpp = 1 if (d.opt_inj < 0 and pabs[0] > 0.0) else 0
+    c.Pabs_cor = 1.0
+    vt = list(d.vt) if d.vt else [vt0_e] * n_icp
+    for b in range(n_icp):
+        c.vt[b] = vt[b] if b < len(vt) else vt[-1]
+    c.te_update = d.te_update if pabs[0] > 0.0 else 0
+    c.flag_inj = 0 if d.I_inj < 0.0 else 1
+    c.I_inj = 0.0 if (d.I_inj < 0.0 or abs(d.opt_inj) == 2) else d.I_inj
+    c.opt_inj = d.opt_inj
+    c.ns_inj = d.ns_inj
+    c.flag_Tp = 1 if d.THm < 0.0 else 0
+    c.THm = abs(d.THm)
+    c.flag_diffsrc = d.flag_diffsrc
+    c.tag_neg = d.tag_neg
+    c.nproc_mpi = d.nproc_mpi
+    for s, v in enumerate(d.ni0[:capi.MAXSP]):
+        c.ni0[s] = v
+    c.seed = d.seed
+    return c

@@ -141,4 +141,53 @@ void o_push_deposit_omp(const o_cfg *c, int ptype, const double *Ei, const doubl
 int o_iterative_solver_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
                            int ng, int ncycl, double eps, o_solve_stats *st, int nthreads);
 
+/* ---- particle sources: e_heating.f90, part_injection.f90 ----------------------------------
+ * Two forms of each routine.  The plain form restates the reference's draw order from one
+ * sequential ran2 stream (the vz_sav / x_sav pairing of consecutive particles included).
+ * The _ctr form is the same algorithm fed by the counter-based Philox4x32-10 streams the
+ * device path draws from (one counter per slot or injected particle and step), so the
+ * device's results can be checked particle by particle; it also rounds the stored state
+ * the way the device keeps it (FP32 velocities; fixed-point positions with S fractional
+ * bits when S > 0). */
+#define O_MAXICP 16
+typedef struct {
+    int flag_c;                 /* 0 slit, 1 disk (read_input.f90:48-51)               */
+    double xl_pow, xr_pow, yl_pow, yr_pow;
+    int eheat_type, flag_gpp, n_icp;
+    double nudt, Pabs_cor;
+    int opt_inj, flag_Tp, flag_diffsrc, tag_neg, nproc_mpi, ns_inj;
+    double I_inj, THm;
+    double ni0[O_MAXSP];
+} o_src;
+
+/* Philox4x32-10 (Salmon et al., SC'11) and the device's (0,1) mapping (v + 0.5) 2^-32 */
+void o_philox4x32_10(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]);
+double o_u01(uint32_t v);
+
+/* e_heating.f90:1-112 on the electrons vxp(6,n); vt[n_icp]; ran2 sequence. */
+void o_eheating(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const double *vt,
+                int32_t *iseed, double *P_heat, int64_t *n_heated);
+void o_eheating_ctr(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const double *vt,
+                    uint64_t seed, int32_t it, double *P_heat, int64_t *n_heated);
+/* the heating-region tallies of charge_deposition (part_expmover.f90:583-605) */
+void o_heat_tally(const o_cfg *c, const o_src *s, const double *vxp, int64_t n, int64_t *Nh,
+                  double *sum_dEk);
+/* main.f90:1003-1010 for one band; returns vt (the old value when Nh = 0) */
+double o_te_update(const o_cfg *c, int eheat_type, double Pabs, double nu_h, int64_t Nh,
+                   double sum_dEk, double vt_old);
+
+/* part_injection.f90:1-237 for one species: N_inj[ntype] holds the losses counted by the
+ * mover (|opt_inj| = 2) and receives this call's count; particles are appended to vxp
+ * from *np (capacity cap).  Returns 0, or -2 when the capacity would be exceeded. */
+int o_part_injection(const o_cfg *c, const o_src *s, int ptype, const int32_t *bcnd,
+                     const double *phi, int64_t *N_inj, double *vxp, int64_t *np, int64_t cap,
+                     int32_t *iseed, double *P_inj, double *P_src);
+/* the device's form over all charged species in order: lost[ntype] are the losses since the
+ * last injection; vxp[s] / np[s] / cap[s] per species; count[s] receives N_inj.  Returns 0,
+ * -2 on capacity, -3 when a particle finds no free cell in 65536 attempts. */
+int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, const double *phi,
+                         const int64_t *lost, uint64_t seed, int32_t it, int S, double **vxp,
+                         int64_t *np, const int64_t *cap, int64_t *count, double *P_inj,
+                         double *P_src);
+
 #endif

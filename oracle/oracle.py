@@ -24,7 +24,7 @@ MAXCOL = 64
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("lepic_oracle.c", "lepic_oracle.h", "cnn_oracle.c")]
+    srcs = [os.path.join(HERE, f) for f in ("lepic_oracle.c", "lepic_oracle.h", "cnn_oracle.c", "sources_oracle.c")]
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", HERE, "-B" if force else "-s"], check=True, capture_output=True)
     return LIB
@@ -64,6 +64,20 @@ class OPushTally(C.Structure):
 class OMccTally(C.Structure):
     _fields_ = [("n_cand", C.c_int64 * MAXSP), ("n_coll", C.c_int64 * MAXCOL),
                 ("n_add", C.c_int64 * MAXSP), ("n_overflow", C.c_int64), ("nu_max", C.c_double * MAXSP)]
+
+
+MAXICP = 16
+
+
+class OSrc(C.Structure):
+    _fields_ = [
+        ("flag_c", C.c_int), ("xl_pow", C.c_double), ("xr_pow", C.c_double), ("yl_pow", C.c_double),
+        ("yr_pow", C.c_double), ("eheat_type", C.c_int), ("flag_gpp", C.c_int), ("n_icp", C.c_int),
+        ("nudt", C.c_double), ("Pabs_cor", C.c_double),
+        ("opt_inj", C.c_int), ("flag_Tp", C.c_int), ("flag_diffsrc", C.c_int), ("tag_neg", C.c_int),
+        ("nproc_mpi", C.c_int), ("ns_inj", C.c_int), ("I_inj", C.c_double), ("THm", C.c_double),
+        ("ni0", C.c_double * MAXSP),
+    ]
 
 
 class OSolveStats(C.Structure):
@@ -112,6 +126,22 @@ def lib() -> C.CDLL:
         L.o_scatter.argtypes = [_DP, _DP, _DP, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.o_push_deposit_omp.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _DP, _LP, _I8, _DP,
                                          C.c_int]
+        _U32 = C.POINTER(C.c_uint32)
+        L.o_philox4x32_10.argtypes = [_U32, C.c_uint32, C.c_uint32, _U32]
+        L.o_u01.restype = C.c_double
+        L.o_u01.argtypes = [C.c_uint32]
+        L.o_eheating.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), _DP, C.c_int64, _DP, C.POINTER(C.c_int32), _DP, _LP]
+        L.o_eheating_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), _DP, C.c_int64, _DP, C.c_uint64, C.c_int32,
+                                     _DP, _LP]
+        L.o_heat_tally.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), _DP, C.c_int64, _LP, _DP]
+        L.o_te_update.restype = C.c_double
+        L.o_te_update.argtypes = [C.POINTER(OCfg), C.c_int, C.c_double, C.c_double, C.c_int64, C.c_double, C.c_double]
+        L.o_part_injection.restype = C.c_int
+        L.o_part_injection.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), C.c_int, _IP, _DP, _LP, _DP, _LP, C.c_int64,
+                                       C.POINTER(C.c_int32), _DP, _DP]
+        L.o_part_injection_ctr.restype = C.c_int
+        L.o_part_injection_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), _IP, _DP, _LP, C.c_uint64, C.c_int32,
+                                           C.c_int, C.POINTER(_DP), _LP, _LP, _LP, _DP, _DP]
         _lib = L
     return _lib
 
@@ -350,3 +380,79 @@ def cnn_init_params(seed: int = 0) -> np.ndarray:
         out.append(rng.standard_normal(co * ci * 9) * np.sqrt(2.0 / (9 * ci)))
         out.append(np.zeros(co))
     return np.concatenate(out)
+
+
+# ---- particle sources (e_heating.f90, part_injection.f90) -------------------------------
+def philox(ctr, key) -> tuple[int, int, int, int]:
+    """Philox4x32-10 of a 4-word counter and a 2-word key."""
+    c = (C.c_uint32 * 4)(*[int(v) & 0xFFFFFFFF for v in ctr])
+    o = (C.c_uint32 * 4)()
+    lib().o_philox4x32_10(c, int(key[0]) & 0xFFFFFFFF, int(key[1]) & 0xFFFFFFFF, o)
+    return tuple(int(v) for v in o)
+
+
+def make_src(sc) -> OSrc:
+    """o_src from a lepic_source_config (ctypes structure of the product's C ABI)."""
+    o = OSrc()
+    for f in ("flag_c", "xl_pow", "xr_pow", "yl_pow", "yr_pow", "eheat_type", "flag_gpp", "n_icp", "nudt",
+              "Pabs_cor", "opt_inj", "flag_Tp", "flag_diffsrc", "tag_neg", "nproc_mpi", "ns_inj", "I_inj", "THm"):
+        setattr(o, f, getattr(sc, f))
+    for s in range(MAXSP):
+        o.ni0[s] = sc.ni0[s]
+    return o
+
+
+def eheating(cfg, src, vxp, vt, *, iseed=None, seed=None, it=0):
+    """e_heating.f90 on vxp (n, 6) in place.  iseed: the reference's ran2 form; seed/it: the
+    device's counter streams.  Returns (P_heat, n_heated[, iseed])."""
+    vt = np.ascontiguousarray(vt, dtype=np.float64)
+    P = C.c_double(0.0)
+    nh = C.c_int64(0)
+    if iseed is not None:
+        sd = C.c_int32(iseed)
+        lib().o_eheating(C.byref(cfg), C.byref(src), dp(vxp), vxp.shape[0], dp(vt), C.byref(sd), C.byref(P),
+                         C.byref(nh))
+        return P.value, nh.value, sd.value
+    lib().o_eheating_ctr(C.byref(cfg), C.byref(src), dp(vxp), vxp.shape[0], dp(vt), seed, it, C.byref(P), C.byref(nh))
+    return P.value, nh.value
+
+
+def heat_tally(cfg, src, vxp):
+    Nh = np.zeros(MAXICP, dtype=np.int64)
+    E = np.zeros(MAXICP)
+    lib().o_heat_tally(C.byref(cfg), C.byref(src), dp(vxp), vxp.shape[0], Nh.ctypes.data_as(_LP), dp(E))
+    return Nh[:src.n_icp], E[:src.n_icp]
+
+
+def te_update(cfg, eheat_type, Pabs, nu_h, Nh, sum_dEk, vt_old):
+    return lib().o_te_update(C.byref(cfg), eheat_type, Pabs, nu_h, int(Nh), sum_dEk, vt_old)
+
+
+def part_injection(cfg, src, ptype, bcnd, phi, N_inj, vxp, n, iseed):
+    """The reference's form for one species (ran2).  N_inj (int64[ntype]) in/out; vxp (cap, 6)
+    receives the particles from row n.  Returns (rc, n, P_inj, P_src, iseed)."""
+    nn = C.c_int64(n)
+    sd = C.c_int32(iseed)
+    Pi, Ps = C.c_double(0.0), C.c_double(0.0)
+    rc = lib().o_part_injection(C.byref(cfg), C.byref(src), ptype, ip(bcnd), dp(phi), N_inj.ctypes.data_as(_LP),
+                                dp(vxp), C.byref(nn), vxp.shape[0], C.byref(sd), C.byref(Pi), C.byref(Ps))
+    return rc, nn.value, Pi.value, Ps.value, sd.value
+
+
+def part_injection_ctr(cfg, src, bcnd, phi, lost, seed, it, S, vxp_list, n_list):
+    """The device's form for every charged species.  vxp_list[s] (cap_s, 6) arrays receive the
+    particles from row n_list[s].  Returns (rc, n, count, P_inj, P_src)."""
+    ns = cfg.ntype
+    lost = np.ascontiguousarray(np.resize(np.asarray(lost, dtype=np.int64), MAXSP))
+    ptrs = (_DP * MAXSP)(*[dp(v) for v in vxp_list] + [None] * (MAXSP - ns))
+    npa = np.zeros(MAXSP, dtype=np.int64)
+    npa[:ns] = n_list
+    cap = np.zeros(MAXSP, dtype=np.int64)
+    cap[:ns] = [v.shape[0] for v in vxp_list]
+    cnt = np.zeros(MAXSP, dtype=np.int64)
+    Pi = np.zeros(MAXSP)
+    Ps = np.zeros(MAXSP)
+    rc = lib().o_part_injection_ctr(C.byref(cfg), C.byref(src), ip(bcnd), dp(phi), lost.ctypes.data_as(_LP), seed,
+                                    it, S, ptrs, npa.ctypes.data_as(_LP), cap.ctypes.data_as(_LP),
+                                    cnt.ctypes.data_as(_LP), dp(Pi), dp(Ps))
+    return rc, npa[:ns].copy(), cnt[:ns].copy(), Pi[:ns].copy(), Ps[:ns].copy()

@@ -1,0 +1,385 @@
+/*
+ * sources_oracle.c -- CPU FP64 restatement of the reference's particle sources:
+ * eheating (e_heating.f90:1-112), the heating-region tallies of charge_deposition
+ * (part_expmover.f90:583-605), the temperature update (main.f90:1003-1010) and
+ * part_injection (part_injection.f90:1-237, options |opt_inj| = 1, 2).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path (see lepic_oracle.h).
+ * Parity against the reference's own outputs is unpinned (no Fortran compiler here, and
+ * the reference ships no tests for these routines); the tests pin the restatement with the
+ * published Philox4x32-10 known answers and with distribution checks.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "lepic_oracle.h"
+
+#define TAG_HEAT 0x48454154u
+#define TAG_HEATV 0x48564C31u
+#define TAG_INJN 0x494E4A4Eu
+#define TAG_INJP 0x494E4A50u
+#define TAG_INJV 0x494E4A56u
+#define MAX_ATTEMPTS 65536u
+
+/* Philox4x32-10: ten rounds of two 32x32->64 multiplies, Weyl key schedule */
+void o_philox4x32_10(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)M0 * c0, p1 = (uint64_t)M1 * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += W0;
+        k1 += W1;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+double o_u01(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
+
+static void draw4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint64_t seed, uint32_t out[4]) {
+    const uint32_t ctr[4] = {a, b, c, d};
+    o_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x53524331u, out);
+}
+
+/* load_gauss with the two uniforms of a counter draw */
+static void gauss_u(double vt, uint32_t a, uint32_t b, double *x, double *y) {
+    const double rnd[2] = {o_u01(a), o_u01(b)};
+    o_load_gauss(x, y, vt, rnd);
+}
+
+static int band_of(const o_cfg *c, const o_src *s, double y) {
+    int b = (int)(s->n_icp * y / c->ymax);
+    if (b < 0) b = 0;
+    if (b >= s->n_icp) b = s->n_icp - 1;
+    return b;
+}
+
+/* the heating test of e_heating.f90:51-65; returns 1 inside, with rp2 */
+static int heat_region(const o_cfg *c, const o_src *s, double x, double y, double *rp2) {
+    const double xa = (s->xl_pow + s->xr_pow) / 2.0, dr = (s->xr_pow - s->xl_pow) / 2.0;
+    if (s->flag_c == 0) {
+        *rp2 = (x - xa) * (x - xa);
+        return *rp2 <= dr * dr && y >= s->yl_pow && y <= s->yr_pow;
+    }
+    *rp2 = (x - xa) * (x - xa) + (y - c->ymax / 2.0) * (y - c->ymax / 2.0);
+    return *rp2 <= dr * dr;
+}
+
+/* e_heating.f90:33-108 */
+void o_eheating(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const double *vt,
+                int32_t *iseed, double *P_heat, int64_t *n_heated) {
+    const double dr = (s->xr_pow - s->xl_pow) / 2.0;
+    double vz_sav = 0.0;
+    double nu_tmp = s->nudt / c->dt;
+    for (int64_t i = 0; i < n; i++) {
+        double *p = vxp + 6 * i;
+        double rp2;
+        if (!heat_region(c, s, p[0], p[1], &rp2)) continue;
+        if (s->flag_gpp == 1) nu_tmp = (s->nudt / c->dt) * 9.0 * s->Pabs_cor * exp(-9.0 * rp2 / (dr * dr));
+        double rnd[2];
+        rnd[0] = o_ran2(iseed);
+        if (rnd[0] <= nu_tmp * c->dt) {
+            const double v2old = p[3] * p[3] + p[4] * p[4] + p[5] * p[5];
+            const int b = band_of(c, s, p[1]);
+            double dvx, dvy, dvz;
+            rnd[0] = o_ran2(iseed);
+            rnd[1] = o_ran2(iseed);
+            o_load_gauss(&dvx, &dvy, vt[b], rnd);
+            if (vz_sav == 0.0) {
+                rnd[0] = o_ran2(iseed);
+                rnd[1] = o_ran2(iseed);
+                o_load_gauss(&dvz, &vz_sav, vt[b], rnd);
+            } else {
+                dvz = vz_sav;
+                vz_sav = 0.0;
+            }
+            if (s->eheat_type == 1) {
+                p[3] = dvx; p[4] = dvy; p[5] = dvz;
+            } else {
+                p[3] += dvx; p[4] += dvy; p[5] += dvz;
+            }
+            *P_heat += 0.5 * c->Nm[0] * c->mass[0] * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] - v2old);
+            (*n_heated)++;
+        }
+    }
+}
+
+/* the same with the device's streams: decision (slot, step), then one velocity draw */
+void o_eheating_ctr(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const double *vt,
+                    uint64_t seed, int32_t it, double *P_heat, int64_t *n_heated) {
+    const double dr = (s->xr_pow - s->xl_pow) / 2.0;
+    const double Ek = 0.5 * c->Nm[0] * c->mass[0];
+    for (int64_t k = 0; k < n; k++) {
+        double *p = vxp + 6 * k;
+        double rp2;
+        if (!heat_region(c, s, p[0], p[1], &rp2)) continue;
+        double nu_tmp = s->nudt / c->dt;
+        if (s->flag_gpp == 1) nu_tmp = (s->nudt / c->dt) * 9.0 * s->Pabs_cor * exp(-9.0 * rp2 / (dr * dr));
+        uint32_t r[4], q[4];
+        draw4((uint32_t)k, (uint32_t)((uint64_t)k >> 32), TAG_HEAT, (uint32_t)it, seed, r);
+        if (!(o_u01(r[0]) <= nu_tmp * c->dt)) continue;
+        const int b = band_of(c, s, p[1]);
+        draw4((uint32_t)k, (uint32_t)((uint64_t)k >> 32), TAG_HEATV, (uint32_t)it, seed, q);
+        double dvx, dvy, dvz, unused;
+        gauss_u(vt[b], q[0], q[1], &dvx, &dvy);
+        gauss_u(vt[b], q[2], q[3], &dvz, &unused);
+        const double v2old = p[3] * p[3] + p[4] * p[4] + p[5] * p[5];
+        if (s->eheat_type == 1) {
+            p[3] = (float)dvx; p[4] = (float)dvy; p[5] = (float)dvz;
+        } else {
+            p[3] = (float)(p[3] + dvx); p[4] = (float)(p[4] + dvy); p[5] = (float)(p[5] + dvz);
+        }
+        *P_heat += Ek * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5] - v2old);
+        (*n_heated)++;
+    }
+}
+
+/* part_expmover.f90:583-605 */
+void o_heat_tally(const o_cfg *c, const o_src *s, const double *vxp, int64_t n, int64_t *Nh,
+                  double *sum_dEk) {
+    const double xa = (s->xl_pow + s->xr_pow) / 2.0, dr = (s->xr_pow - s->xl_pow) / 2.0;
+    for (int b = 0; b < s->n_icp; b++) { Nh[b] = 0; sum_dEk[b] = 0.0; }
+    for (int64_t i = 0; i < n; i++) {
+        const double *p = vxp + 6 * i;
+        const double x = p[0], y = p[1];
+        if (s->flag_c == 0) {
+            if (x < s->xl_pow || x > s->xr_pow || y < s->yl_pow || y > s->yr_pow) continue;
+        } else if ((x - xa) * (x - xa) + (y - c->ymax / 2.0) * (y - c->ymax / 2.0) > dr * dr) {
+            continue;
+        }
+        const int b = band_of(c, s, y);
+        Nh[b]++;
+        if (s->eheat_type == 1) sum_dEk[b] += 0.5 * c->Nm[0] * c->mass[0] * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5]);
+    }
+}
+
+double o_te_update(const o_cfg *c, int eheat_type, double Pabs, double nu_h, int64_t Nh, double sum_dEk,
+                   double vt_old) {
+    if (Nh <= 0) return vt_old;
+    double Te;
+    if (eheat_type == 1) Te = (2.0 / 3.0) * (sum_dEk + Pabs / nu_h) / (c->Nm[0] * c->qe * (double)Nh);
+    else Te = (2.0 / 3.0) * (Pabs / nu_h) / (c->Nm[0] * c->qe * (double)Nh);
+    return sqrt(2.0 * c->qe * Te / fabs(c->mass[0]));
+}
+
+/* the cell test of part_injection.f90:131-137: 1 when all four corners are walls */
+static int all_walls(const o_cfg *c, const int32_t *bcnd, int ix, int iy) {
+    const int W = c->nx + 3;
+    return bcnd[ix + iy * W] >= 1 && bcnd[ix + 1 + iy * W] >= 1 && bcnd[ix + 1 + (iy + 1) * W] >= 1 &&
+           bcnd[ix + (iy + 1) * W] >= 1;
+}
+
+static double inj_vt(const o_cfg *c, const o_src *s, int ptype) {
+    double vt = c->vt0[ptype];
+    if (abs(s->opt_inj) <= 2 && s->flag_Tp == 1 && ptype == 0) vt = sqrt(2.0 * c->qe * s->THm / fabs(c->mass[0]));
+    return vt;
+}
+
+/* part_injection.f90:216-231 */
+static double phi_at(const o_cfg *c, const double *phi, int ix, int iy, double x, double y) {
+    const int W = c->nx + 3;
+    const double px = (ix * c->dx - x) / c->dx, py = (iy * c->dy - y) / c->dy;
+    return px * py * phi[ix + iy * W] + (1.0 - px) * py * phi[ix + 1 + iy * W] +
+           (1.0 - px) * (1.0 - py) * phi[ix + 1 + (iy + 1) * W] + px * (1.0 - py) * phi[ix + (iy + 1) * W];
+}
+
+/* the count of part_injection.f90:49-75 before its stochastic rounding; *draw = 0 when the
+ * count is an exact loss count (positive ions under |opt_inj| = 2) */
+static double inj_dN(const o_cfg *c, const o_src *s, int ptype, const int64_t *lost, int *draw) {
+    *draw = 1;
+    if (abs(s->opt_inj) == 2) {
+        if (ptype == 0 || ptype == s->tag_neg) {
+            int64_t t = 0;
+            for (int q = 1; q < c->ntype; q++)
+                if (q != s->tag_neg) t += lost[q];
+            return s->ni0[ptype] * (double)t;
+        }
+        *draw = 0;
+        return (double)lost[ptype];
+    }
+    return s->I_inj * s->ns_inj * c->dt * s->ni0[ptype] / (c->qe * c->Nm[0]) / (double)s->nproc_mpi;
+}
+
+int o_part_injection(const o_cfg *c, const o_src *s, int ptype, const int32_t *bcnd,
+                     const double *phi, int64_t *N_inj, double *vxp, int64_t *np, int64_t cap,
+                     int32_t *iseed, double *P_inj, double *P_src) {
+    const double xa = (s->xl_pow + s->xr_pow) / 2.0, dr = (s->xr_pow - s->xl_pow) / 2.0;
+    const double ymid = c->ymax / 2.0;
+    double vz_sav = 0.0, x_sav = 0.0;
+    int draw;
+    const double dN = inj_dN(c, s, ptype, N_inj, &draw);
+    if (draw) {
+        int64_t N = (int64_t)dN;
+        if (o_ran2(iseed) <= dN - (double)N) N += 1;
+        N_inj[ptype] = N;
+    }
+    const double vt = inj_vt(c, s, ptype);
+    for (int64_t i = 0; i < N_inj[ptype]; i++) {
+        double x = 0.0, y = 0.0, rnd[2];
+        int ix, iy;
+        for (;;) { /* label 70 */
+            if (s->opt_inj > 0) {
+                for (;;) { /* label 60 */
+                    x = o_ran2(iseed) * (s->xl_pow - s->xr_pow) + s->xr_pow;
+                    if (s->flag_c != 1) break;
+                    y = o_ran2(iseed) * (2.0 * dr) + ymid - dr;
+                    if (!((x - xa) * (x - xa) + (y - ymid) * (y - ymid) > dr * dr)) break;
+                }
+            } else if (s->flag_c == 0) {
+                for (;;) { /* label 50 */
+                    if (x_sav == 0) {
+                        rnd[0] = o_ran2(iseed);
+                        rnd[1] = o_ran2(iseed);
+                        o_load_gauss(&x, &x_sav, dr, rnd);
+                        x = x + xa;
+                        x_sav = x_sav + xa;
+                    } else {
+                        x = x_sav;
+                        x_sav = 0.0;
+                    }
+                    if (c->flag_nmn == 1 && xa == 0.0) x = fabs(x);
+                    if (!(x < xa - 4.0 * dr || x > xa + 4.0 * dr || x < 0.0 || x > c->xmax)) break;
+                }
+            } else {
+                for (;;) { /* label 40 */
+                    rnd[0] = o_ran2(iseed);
+                    rnd[1] = o_ran2(iseed);
+                    o_load_gauss(&x, &y, dr, rnd);
+                    x = x + xa;
+                    y = y + ymid;
+                    if (!((x - xa) * (x - xa) + (y - ymid) * (y - ymid) > 4.0 * dr * dr || x < 0.0 ||
+                          x > c->xmax || y < 0.0 || y > c->ymax))
+                        break;
+                }
+            }
+            if (s->flag_c == 0) y = o_ran2(iseed) * (s->yl_pow - s->yr_pow) + s->yr_pow;
+            (void)o_ran2(iseed); /* z */
+            ix = (int)(x / c->dx) + 1;
+            iy = (int)(y / c->dy) + 1;
+            if (!all_walls(c, bcnd, ix, iy)) break;
+        }
+        if (*np + 1 > cap) return -2;
+        double *p = vxp + 6 * (*np);
+        (*np)++;
+        double vx, vy, vz;
+        rnd[0] = o_ran2(iseed);
+        rnd[1] = o_ran2(iseed);
+        o_load_gauss(&vx, &vy, vt, rnd);
+        if (vz_sav == 0.0) {
+            rnd[0] = o_ran2(iseed);
+            rnd[1] = o_ran2(iseed);
+            o_load_gauss(&vx, &vy, vt, rnd);
+            vz = vx;
+            vz_sav = vy;
+        } else {
+            vz = vz_sav;
+            vz_sav = 0.0;
+        }
+        p[0] = x; p[1] = y; p[2] = 0.0;
+        p[3] = vx; p[4] = vy; p[5] = vz;
+        *P_inj += 0.5 * c->Nm[ptype] * c->mass[ptype] * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5]);
+        if (s->flag_diffsrc == 1) *P_src -= c->Nm[ptype] * c->charge[ptype] * phi_at(c, phi, ix, iy, x, y);
+    }
+    return 0;
+}
+
+int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, const double *phi,
+                         const int64_t *lost, uint64_t seed, int32_t it, int S, double **vxp,
+                         int64_t *np, const int64_t *cap, int64_t *count, double *P_inj,
+                         double *P_src) {
+    const double xa = (s->xl_pow + s->xr_pow) / 2.0, dr = (s->xr_pow - s->xl_pow) / 2.0;
+    const double ymid = c->ymax / 2.0;
+    const uint32_t U = (uint32_t)it;
+    int rc = 0;
+    for (int sp = 0; sp < c->ntype; sp++) {
+        int draw;
+        const double dN = inj_dN(c, s, sp, lost, &draw);
+        int64_t N = draw ? (int64_t)dN : lost[sp];
+        if (draw) {
+            uint32_t r[4];
+            draw4((uint32_t)sp, 0u, TAG_INJN, U, seed, r);
+            if (o_u01(r[0]) <= dN - (double)N) N += 1;
+        }
+        if (np[sp] + N > cap[sp]) { rc = -2; N = 0; }
+        count[sp] = N;
+    }
+    for (int sp = 0; sp < c->ntype; sp++) {
+        const double vt = inj_vt(c, s, sp);
+        const double Ek = 0.5 * c->Nm[sp] * c->mass[sp];
+        for (int64_t j = 0; j < count[sp]; j++) {
+            double x = 0.0, y = 0.0;
+            int ix = 1, iy = 1, ok = 0;
+            for (uint32_t a = 0; a < MAX_ATTEMPTS && !ok; a++) {
+                uint32_t r[4];
+                draw4((uint32_t)j, (a << 3) | (uint32_t)sp, TAG_INJP, U, seed, r);
+                if (s->opt_inj > 0) {
+                    x = o_u01(r[0]) * (s->xl_pow - s->xr_pow) + s->xr_pow;
+                    if (s->flag_c == 1) {
+                        y = o_u01(r[1]) * (2.0 * dr) + ymid - dr;
+                        if ((x - xa) * (x - xa) + (y - ymid) * (y - ymid) > dr * dr) continue;
+                    }
+                } else if (s->flag_c == 0) {
+                    double g0, g1;
+                    gauss_u(dr, r[0], r[1], &g0, &g1);
+                    x = g0 + xa;
+                    if (c->flag_nmn == 1 && xa == 0.0) x = fabs(x);
+                    if (x < xa - 4.0 * dr || x > xa + 4.0 * dr || x < 0.0 || x > c->xmax) continue;
+                } else {
+                    double g0, g1;
+                    gauss_u(dr, r[0], r[1], &g0, &g1);
+                    x = g0 + xa;
+                    y = g1 + ymid;
+                    if ((x - xa) * (x - xa) + (y - ymid) * (y - ymid) > 4.0 * dr * dr || x < 0.0 || x > c->xmax ||
+                        y < 0.0 || y > c->ymax)
+                        continue;
+                }
+                if (s->flag_c == 0) y = o_u01(r[2]) * (s->yl_pow - s->yr_pow) + s->yr_pow;
+                ix = (int)(x / c->dx) + 1;
+                iy = (int)(y / c->dy) + 1;
+                if (ix < 1) ix = 1;
+                if (ix > c->nx + 1) ix = c->nx + 1;
+                if (iy < 1) iy = 1;
+                if (iy > c->ny + 1) iy = c->ny + 1;
+                if (all_walls(c, bcnd, ix, iy)) continue;
+                ok = 1;
+            }
+            if (!ok) return -3;
+            uint32_t q[4];
+            draw4((uint32_t)j, (uint32_t)sp, TAG_INJV, U, seed, q);
+            double vx, vy, vz;
+            if ((j & 1) == 0) {
+                gauss_u(vt, q[2], q[3], &vx, &vy);
+                vz = vx;
+            } else {
+                uint32_t qp[4];
+                double unused;
+                gauss_u(vt, q[0], q[1], &vx, &vy);
+                draw4((uint32_t)(j - 1), (uint32_t)sp, TAG_INJV, U, seed, qp);
+                gauss_u(vt, qp[2], qp[3], &unused, &vz);
+            }
+            double *p = vxp[sp] + 6 * (np[sp] + j);
+            if (S > 0) {
+                const double sc = ldexp(1.0, S);
+                double fx = floor(x / c->dx * sc), fy = floor(y / c->dy * sc);
+                const double xl = ldexp((double)c->nx, S) - 1.0, yl = ldexp((double)c->ny, S) - 1.0;
+                if (fx > xl) fx = xl;
+                if (fy > yl) fy = yl;
+                p[0] = fx * (c->dx * ldexp(1.0, -S));
+                p[1] = fy * (c->dy * ldexp(1.0, -S));
+                p[3] = (float)vx; p[4] = (float)vy; p[5] = (float)vz;
+            } else {
+                p[0] = x; p[1] = y;
+                p[3] = vx; p[4] = vy; p[5] = vz;
+            }
+            p[2] = 0.0;
+            P_inj[sp] += Ek * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5]);
+            if (s->flag_diffsrc == 1) P_src[sp] += (-c->Nm[sp] * c->charge[sp]) * phi_at(c, phi, ix, iy, x, y);
+        }
+        np[sp] += count[sp];
+    }
+    return rc;
+}
