@@ -272,6 +272,69 @@ def learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step_f
     return it
 
 
+def sources_measure(args, sim, lib, ctx, stream, it, case):
+    """eheating, the heating-region tally and part_injection (the per-step particle sources)
+    on the workload's own electron population, each entry point timed with CUDA events on
+    the library's stream over args.steps calls after 3 untimed ones.  Heating region: the slit
+    0.1 L <= x <= 0.6 L over the full height; nu_h = 5e8 /s (nu*dt*ns_heat = 2e-3 at dt = 1e-12 s,
+    ns_heat = 4); 65536 particles injected per species and call (fixed current, uniform slit).
+    Algorithmic bytes: heating 8 B per electron slot (X, Y) + 4 B per electron in the region
+    (VX, the hole test) + 20 B per heated electron (VY, VZ read, three velocities written);
+    the tally 8 B per slot + 12 B per electron in the region."""
+    import ctypes as C
+    import torch
+    from jd_lepic_b200 import _capi as capi, sources as S
+    from jd_lepic_b200 import deck as dk
+    Lcm, Hcm = case.nx * case.dx * 100.0, case.ny * case.dy * 100.0
+    n_inj = 65536
+    I_inj = n_inj * dk.QE * sim.sp.Nm[0] / case.dt
+    sc = S.source_config(S.SourceDeck(heat_region_cm=(0.1 * Lcm, 0.6 * Lcm, 0.0, Hcm), nu_h=5.0e8, Pabs=(0.0,),
+                                      I_inj=I_inj, opt_inj=1, ni0=(1.0, 1.0), ns_heat=4, seed=2024),
+                         case.dt, sim.sp.vt0[0])
+    sim.set_sources(sc)
+    reps = max(3, args.steps)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    n_slots = sim.push_stats()["n_slots"][0]
+    t0 = sim.source_tallies()
+    heat_ms = timed(lambda: sim.check(lib.lepic_gpu_eheating(ctx, it), "eheating"))
+    t1 = sim.source_tallies()
+    n_heated = (t1["n_heated"] - t0["n_heated"]) / (t1["n_heat_calls"] - t0["n_heat_calls"])
+    tally_ms = timed(lambda: sim.check(lib.lepic_gpu_heating_tally(ctx), "heating_tally"))
+    n_in = sum(sim.source_tallies()["Nh"])
+    c0 = sim.source_tallies()["n_inj"]
+    inj_ms = timed(lambda: sim.check(lib.lepic_gpu_part_injection(ctx, it), "part_injection"))
+    c1 = sim.source_tallies()["n_inj"]
+    sim.sync()
+    peak, peak_kind = peaks()
+    heat_bytes = 8 * n_slots + 4 * n_in + 20 * n_heated
+    tally_bytes = 8 * n_slots + 12 * n_in
+    heat_gbs = heat_bytes / (heat_ms * 1e-3) / 1e9
+    tally_gbs = tally_bytes / (tally_ms * 1e-3) / 1e9
+    return {
+        "electron_slots": n_slots, "in_region": n_in, "heated_per_call": n_heated,
+        "eheating": {"ms": heat_ms, "achieved_gbs": heat_gbs, "frac": heat_gbs / peak,
+                     "algorithmic_bytes": heat_bytes, "kernels": "k_eheat + k_finish"},
+        "heating_tally": {"ms": tally_ms, "achieved_gbs": tally_gbs, "frac": tally_gbs / peak,
+                          "algorithmic_bytes": tally_bytes, "kernels": "k_heat_tally + k_finish"},
+        "part_injection": {"ms": inj_ms, "injected_per_call": [(b - a) / (reps + 3) for a, b in zip(c0, c1)],
+                           "kernels": "k_inj_plan + k_inject + k_finish"},
+        "peak_gbs": peak, "peak_kind": peak_kind, "calls_timed": reps,
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -449,6 +512,8 @@ def run_ours(args):
     ne1 = sum(ps.np_tot[:sim.sp.ntype])
     e2e_value = 0.5 * (ne0 + ne1) * e2e_steps * world / e2e_s
 
+    src = sources_measure(args, sim, lib, ctx, stream, it, case) if not args.no_sources else None
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(case, args.cpu_sample, 3, 1, host_threads())
@@ -489,6 +554,7 @@ def run_ours(args):
                     "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn + C.sizeof(capi.LepicPushStats)},
             "gpu_launches": launches,
             "clocks": clk,
+            "sources": src,
         }
         print(json.dumps(line))
     sim.close()
@@ -510,6 +576,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell (profiling runs)")
     ap.add_argument("--nx", type=int, default=0, help="override the grid to nx x nx cells (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sources", action="store_true", help="skip the particle-source kernel timings")
     ap.add_argument("--learn-steps", type=int, default=60, help="PIC steps of online training before the A/B")
     ap.add_argument("--learn-ab", type=int, default=4, help="steps of the learned/plain Poisson A/B")
     ap.add_argument("--learn-train-steps", type=int, default=2, help="Adam steps per learned solve")

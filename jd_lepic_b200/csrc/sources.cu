@@ -4,7 +4,8 @@
 // (main.f90:984-1011), and volume injection (part_injection.f90:1-237).
 //
 // Random numbers: Philox4x32-10 streams keyed by the source seed, one counter per decision
-// (slot and step for heating; species, injected index, attempt and step for injection), so
+// (group of 4 slots and step for the heating decision, one word per slot; slot and step for
+// the new velocity; species, injected index, attempt and step for injection), so
 // every particle's draws are independent of the launch shape and of the other particles.
 // The reference draws from one sequential ran2 stream per OpenMP thread; the two differ in
 // which numbers are drawn, not in the distributions (the oracle holds both forms).
@@ -23,7 +24,8 @@
 #include "lepic_internal.cuh"
 
 #define SRC_THREADS 256
-#define SRC_BLOCKS 296          // fixed grid of the tallying kernels (bit-reproducible sums)
+#define SRC_BLOCKS 592          // fixed grids of the scanning kernels (bit-reproducible sums):
+#define HEAT_BLOCKS 444         // 4 and 3 CTAs per SM of a B200
 #define INJ_THREADS 128
 #define INJ_BLOCKS 64
 #define INJ_MAX_ATTEMPTS 65536  // rejection-sampling attempts per injected particle
@@ -57,18 +59,62 @@ struct SrcState {
 };
 
 // The region of read_input.f90:43-55: slit or disk, centre xa, half width dr.
+// For the slit, the tests are monotone in the fixed-point X and Y (x = X ux is monotone, and
+// so is each side of (x - xa)^2), so the host turns them into exact integer intervals by a
+// binary search over the same FP64 expressions the device would evaluate: the kernels then
+// compare integers, with the same result bit for bit.
 struct Region {
     int disk;
     double xl, xr, yl, yr, xa, dr, ymid;
+    uint32_t hx0, hx1, hy0, hy1;    // slit heating test (e_heating.f90:52-54): X, Y intervals
+    uint32_t tx0, tx1, ty0, ty1;    // slit tally test (part_expmover.f90:585-587); lo > hi: empty
 };
 
-static Region make_region(const lepic_source_config &s, const lepic_config &g) {
+// first X in [a, b] where pred turns true (pred false then true on [a, b]); b + 1 if never
+template <class F>
+static long long first_true(long long a, long long b, F pred) {
+    long long lo = a, hi = b + 1;
+    while (lo < hi) {
+        const long long m = lo + (hi - lo) / 2;
+        if (pred(m)) hi = m;
+        else lo = m + 1;
+    }
+    return lo;
+}
+
+static Region make_region(const lepic_source_config &s, const lepic_config &g, int S) {
     Region R;
     R.disk = s.flag_c;
     R.xl = s.xl_pow; R.xr = s.xr_pow; R.yl = s.yl_pow; R.yr = s.yr_pow;
     R.xa = (s.xl_pow + s.xr_pow) / 2.0;
     R.dr = (s.xr_pow - s.xl_pow) / 2.0;
     R.ymid = (double)g.ny * g.dy / 2.0;
+    const double ux = g.dx * std::ldexp(1.0, -S), uy = g.dy * std::ldexp(1.0, -S);
+    const long long xm = ((long long)g.nx << S) - 1, ym = ((long long)g.ny << S) - 1;
+    const double dr2 = R.dr * R.dr;
+    auto xv = [&](long long X) { return (double)X * ux; };
+    auto yv = [&](long long Y) { return (double)Y * uy; };
+    // heating: (x - xa)^2 <= dr^2 around the centre, yl <= y <= yr
+    auto hin = [&](long long X) { const double x = xv(X); return (x - R.xa) * (x - R.xa) <= dr2; };
+    const long long xc = std::min(xm, std::max(0ll, (long long)std::llround(R.xa / ux)));
+    // intervals [lo, hi] of [0, 2^32); an empty one is stored as lo = 1, hi = 0
+    auto put = [](long long lo, long long hi, uint32_t &a, uint32_t &b) {
+        if (lo > hi) { a = 1; b = 0; }
+        else { a = (uint32_t)lo; b = (uint32_t)hi; }
+    };
+    long long h0 = 1, h1 = 0;
+    if (hin(xc)) {
+        h0 = first_true(0, xc, hin);
+        h1 = first_true(xc, xm, [&](long long X) { return !hin(X); }) - 1;
+    }
+    put(h0, h1, R.hx0, R.hx1);
+    put(first_true(0, ym, [&](long long Y) { return yv(Y) >= R.yl; }),
+        first_true(0, ym, [&](long long Y) { return yv(Y) > R.yr; }) - 1, R.hy0, R.hy1);
+    // tally: xl <= x <= xr, yl <= y <= yr
+    put(first_true(0, xm, [&](long long X) { return xv(X) >= R.xl; }),
+        first_true(0, xm, [&](long long X) { return xv(X) > R.xr; }) - 1, R.tx0, R.tx1);
+    R.ty0 = R.hy0;
+    R.ty1 = R.hy1;
     return R;
 }
 
@@ -99,7 +145,9 @@ __device__ void cta_reduce_rows(double *col, int nv, double *out_row) {
 }
 
 // ---------------------------------------------------------------------------------------
-// eheating (e_heating.f90:33-108) over the electron slots
+// eheating (e_heating.f90:33-108) over the electron slots.  Each thread takes groups of 4
+// consecutive slots (one 16-byte load of X and of Y per group, two groups in flight); only
+// the electrons in the region load VX (the hole test), only the heated ones VY, VZ.
 struct HeatP {
     const uint32_t *X, *Y;
     float *VX, *VY, *VZ;
@@ -112,51 +160,104 @@ struct HeatP {
     uint32_t it, k0, k1;
 };
 
-__global__ void __launch_bounds__(SRC_THREADS) k_eheat(HeatP P, double *part) {
+// the new velocity of a heated electron (e_heating.f90:67-103); returns its energy gain.
+// Out of line: the rare path keeps its registers away from the scan loop.
+__device__ __noinline__ double heat_apply(float *VX, float *VY, float *VZ, long long k, double vt, int type, double Ek,
+                                          uint32_t it, uint32_t k0, uint32_t k1) {
+    const float vx = VX[k], vy = VY[k], vz = VZ[k];
+    const U4 q = philox4x32_10(U4{(uint32_t)k, (uint32_t)(k >> 32), TAG_HEATV, it}, k0, k1);
+    double dvx, dvy, dvz, unused;
+    gauss_pair(vt, q.x, q.y, &dvx, &dvy);
+    gauss_pair(vt, q.z, q.w, &dvz, &unused);
+    const double v2old = (double)vx * vx + (double)vy * vy + (double)vz * vz;
+    float nx_, ny_, nz_;
+    if (type == 1) {
+        nx_ = (float)dvx; ny_ = (float)dvy; nz_ = (float)dvz;
+    } else {
+        nx_ = (float)((double)vx + dvx); ny_ = (float)((double)vy + dvy); nz_ = (float)((double)vz + dvz);
+    }
+    VX[k] = nx_; VY[k] = ny_; VZ[k] = nz_;
+    return Ek * ((double)nx_ * nx_ + (double)ny_ * ny_ + (double)nz_ * nz_ - v2old);
+}
+
+// the heating region test of e_heating.f90:51-58 (the slit as integer intervals)
+__device__ __forceinline__ bool heat_in(const HeatP &P, uint32_t Xk, uint32_t Yk, double dr2) {
+    if (P.R.disk == 0) return Xk >= P.R.hx0 && Xk <= P.R.hx1 && Yk >= P.R.hy0 && Yk <= P.R.hy1;
+    const double x = (double)Xk * P.ux, y = (double)Yk * P.uy;
+    return (x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) <= dr2;
+}
+// rp2 as the reference forms it, for the Gaussian profile
+__device__ __forceinline__ double heat_rp2(const HeatP &P, uint32_t Xk, uint32_t Yk) {
+    const double x = (double)Xk * P.ux;
+    if (P.R.disk == 0) return (x - P.R.xa) * (x - P.R.xa);
+    const double y = (double)Yk * P.uy;
+    return (x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid);
+}
+
+// one group of 4 consecutive slots (k0 = 4 g): the region and hole tests give a candidate
+// mask; if it is not empty, one Philox draw decides the group (slot k takes word k & 3)
+__device__ __forceinline__ void heat_group(const HeatP &P, long long k0, const uint32_t *xs, const uint32_t *ys,
+                                           long long n, double dr2, double &dE, unsigned &cnt) {
+    unsigned mask = 0;
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+        if (k0 + p < n && heat_in(P, xs[p], ys[p], dr2) && !isnan(P.VX[k0 + p])) mask |= 1u << p;  // NaN: a hole
+    if (!mask) return;
+    const long long g = k0 >> 2;
+    const U4 r = philox4x32_10(U4{(uint32_t)g, (uint32_t)(g >> 32), TAG_HEAT, P.it}, P.k0, P.k1);
+    const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        if (!(mask >> p & 1u)) continue;
+        double nu_tmp = P.nudt / P.dt;
+        if (P.gpp) nu_tmp = (P.nudt / P.dt) * 9.0 * P.Pabs_cor * exp(-9.0 * heat_rp2(P, xs[p], ys[p]) / dr2);
+        if (!(u01(w[p]) <= nu_tmp * P.dt)) continue;
+        int band = 0;
+        if (P.n_icp > 1) {
+            band = (int)(P.n_icp * ((double)ys[p] * P.uy) / P.ymax);
+            band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
+        }
+        const double vt = P.vt_const > 0.0 ? P.vt_const : P.src->vt[band];
+        dE += heat_apply(P.VX, P.VY, P.VZ, k0 + p, vt, P.type, P.Ek, P.it, P.k0, P.k1);
+        cnt++;
+    }
+}
+
+// the slot groups of one thread, software-pipelined: the next group's X, Y (one 16-byte
+// load each) are issued before the current group is processed; f(k0, xs, ys)
+template <int NBLK, class F>
+__device__ __forceinline__ void scan_groups(const uint32_t *X, const uint32_t *Y, long long n, F f) {
+    const long long ngroups = (n + 3) >> 2;
+    const long long stride = (long long)NBLK * SRC_THREADS;
+    long long g = blockIdx.x * (long long)SRC_THREADS + threadIdx.x;
+    if (g >= ngroups) return;
+    // storage is whole groups of 8 slots: a group's vector stays inside the allocation
+    uint4 xc = __ldcs(reinterpret_cast<const uint4 *>(X) + g), yc = __ldcs(reinterpret_cast<const uint4 *>(Y) + g);
+    for (; g < ngroups; g += stride) {
+        const long long h = g + stride;
+        uint4 xn = xc, yn = yc;
+        if (h < ngroups) {
+            xn = __ldcs(reinterpret_cast<const uint4 *>(X) + h);
+            yn = __ldcs(reinterpret_cast<const uint4 *>(Y) + h);
+        }
+        const uint32_t xs[4] = {xc.x, xc.y, xc.z, xc.w}, ys[4] = {yc.x, yc.y, yc.z, yc.w};
+        f(g << 2, xs, ys);
+        xc = xn;
+        yc = yn;
+    }
+}
+
+__global__ void __launch_bounds__(SRC_THREADS, 3) k_eheat(HeatP P, double *part) {
     __shared__ double col[2 * SRC_THREADS];
     const long long n = P.cnt->n_slots[0];
-    double dE = 0.0, cntd = 0.0;
+    double dE = 0.0;
+    unsigned cnt = 0;
     const double dr2 = P.R.dr * P.R.dr;
-    for (long long k = blockIdx.x * (long long)SRC_THREADS + threadIdx.x; k < n;
-         k += (long long)SRC_BLOCKS * SRC_THREADS) {
-        const double x = (double)P.X[k] * P.ux, y = (double)P.Y[k] * P.uy;
-        double rp2;
-        bool in;
-        if (P.R.disk == 0) {
-            rp2 = (x - P.R.xa) * (x - P.R.xa);
-            in = rp2 <= dr2 && y >= P.R.yl && y <= P.R.yr;
-        } else {
-            rp2 = (x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid);
-            in = rp2 <= dr2;
-        }
-        if (!in) continue;
-        const float vx = P.VX[k];
-        if (isnan(vx)) continue;  // hole
-        double nu_tmp = P.nudt / P.dt;
-        if (P.gpp) nu_tmp = (P.nudt / P.dt) * 9.0 * P.Pabs_cor * exp(-9.0 * rp2 / dr2);
-        const U4 r = philox4x32_10(U4{(uint32_t)k, (uint32_t)(k >> 32), TAG_HEAT, P.it}, P.k0, P.k1);
-        if (!(u01(r.x) <= nu_tmp * P.dt)) continue;
-        const float vy = P.VY[k], vz = P.VZ[k];
-        int band = (int)(P.n_icp * y / P.ymax);
-        band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
-        const double vt = P.vt_const > 0.0 ? P.vt_const : P.src->vt[band];
-        const U4 q = philox4x32_10(U4{(uint32_t)k, (uint32_t)(k >> 32), TAG_HEATV, P.it}, P.k0, P.k1);
-        double dvx, dvy, dvz, unused;
-        gauss_pair(vt, q.x, q.y, &dvx, &dvy);
-        gauss_pair(vt, q.z, q.w, &dvz, &unused);
-        const double v2old = (double)vx * vx + (double)vy * vy + (double)vz * vz;
-        float nx_, ny_, nz_;
-        if (P.type == 1) {
-            nx_ = (float)dvx; ny_ = (float)dvy; nz_ = (float)dvz;
-        } else {
-            nx_ = (float)((double)vx + dvx); ny_ = (float)((double)vy + dvy); nz_ = (float)((double)vz + dvz);
-        }
-        P.VX[k] = nx_; P.VY[k] = ny_; P.VZ[k] = nz_;
-        dE += P.Ek * ((double)nx_ * nx_ + (double)ny_ * ny_ + (double)nz_ * nz_ - v2old);
-        cntd += 1.0;
-    }
+    scan_groups<HEAT_BLOCKS>(P.X, P.Y, n, [&](long long k0, const uint32_t *xs, const uint32_t *ys) {
+        heat_group(P, k0, xs, ys, n, dr2, dE, cnt);
+    });
     col[threadIdx.x] = dE;
-    col[SRC_THREADS + threadIdx.x] = cntd;
+    col[SRC_THREADS + threadIdx.x] = (double)cnt;
     cta_reduce_rows<SRC_THREADS>(col, 2, part + 2 * blockIdx.x);
 }
 
@@ -170,60 +271,70 @@ struct TallyP {
     int n_icp, type;
 };
 
-__global__ void __launch_bounds__(SRC_THREADS) k_heat_tally(TallyP P, double *part) {
+__global__ void __launch_bounds__(SRC_THREADS, 4) k_heat_tally(TallyP P, double *part) {
     extern __shared__ double col[];   // [2 * n_icp][SRC_THREADS]: Nh then sum_dEk per band
     const int nv = 2 * P.n_icp;
     for (int v = 0; v < nv; v++) col[v * SRC_THREADS + threadIdx.x] = 0.0;
     const long long n = P.cnt->n_slots[0];
     const double dr2 = P.R.dr * P.R.dr;
-    for (long long k = blockIdx.x * (long long)SRC_THREADS + threadIdx.x; k < n;
-         k += (long long)SRC_BLOCKS * SRC_THREADS) {
-        const double x = (double)P.X[k] * P.ux, y = (double)P.Y[k] * P.uy;
-        if (P.R.disk == 0) {
-            if (x < P.R.xl || x > P.R.xr || y < P.R.yl || y > P.R.yr) continue;
-        } else {
-            if ((x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) > dr2) continue;
+    scan_groups<SRC_BLOCKS>(P.X, P.Y, n, [&](long long k0, const uint32_t *xs, const uint32_t *ys) {
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const long long k = k0 + p;
+            if (k >= n) break;
+            if (P.R.disk == 0) {
+                if (xs[p] < P.R.tx0 || xs[p] > P.R.tx1 || ys[p] < P.R.ty0 || ys[p] > P.R.ty1) continue;
+            } else {
+                const double x = (double)xs[p] * P.ux, y = (double)ys[p] * P.uy;
+                if ((x - P.R.xa) * (x - P.R.xa) + (y - P.R.ymid) * (y - P.R.ymid) > dr2) continue;
+            }
+            const float vx = P.VX[k];
+            if (isnan(vx)) continue;
+            int band = 0;
+            if (P.n_icp > 1) {
+                band = (int)(P.n_icp * ((double)ys[p] * P.uy) / P.ymax);
+                band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
+            }
+            col[band * SRC_THREADS + threadIdx.x] += 1.0;
+            if (P.type == 1) {
+                const float vy = P.VY[k], vz = P.VZ[k];
+                col[(P.n_icp + band) * SRC_THREADS + threadIdx.x] +=
+                    P.Ek * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
         }
-        const float vx = P.VX[k];
-        if (isnan(vx)) continue;
-        int band = (int)(P.n_icp * y / P.ymax);
-        band = band < 0 ? 0 : (band >= P.n_icp ? P.n_icp - 1 : band);
-        col[band * SRC_THREADS + threadIdx.x] += 1.0;
-        if (P.type == 1) {
-            const float vy = P.VY[k], vz = P.VZ[k];
-            col[(P.n_icp + band) * SRC_THREADS + threadIdx.x] +=
-                P.Ek * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
-        }
-    }
+    });
     cta_reduce_rows<SRC_THREADS>(col, nv, part + (size_t)nv * blockIdx.x);
 }
 
-// sums the CTA partials in CTA order: dst[v] (+)= sum_b part[b*nv + v]
-__global__ void k_src_finish(const double *part, int nblocks, int nv, double *dst, int accumulate) {
-    const int v = threadIdx.x;
-    if (v >= nv) return;
+// Sums column v of the CTA partials part[b * nv + v] (b < nblocks) in a fixed order -- one
+// CTA per value, a fixed stride per thread, then a fixed tree -- and applies the sum.
+#define FIN_HEAT 0    // v = 0: P_heat +=, v = 1: n_heated +=, calls += 1
+#define FIN_TALLY 1   // v < n_icp: Nh[v] =, else sum_dEk[v - n_icp] =
+#define FIN_INJ 2     // v < MAXSP: P_inj[v] +=, else P_src[v - MAXSP] +=
+__global__ void __launch_bounds__(256) k_finish(const double *part, int nblocks, int nv, int kind, SrcDev *src) {
+    __shared__ double red[256];
+    const int v = blockIdx.x;
     double s = 0.0;
-    for (int b = 0; b < nblocks; b++) s += part[(size_t)b * nv + v];
-    dst[v] = accumulate ? dst[v] + s : s;
-}
-
-__global__ void k_heat_finish(const double *part, SrcDev *src) {
+    for (int b = threadIdx.x; b < nblocks; b += 256) s += part[(size_t)b * nv + v];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
     if (threadIdx.x != 0) return;
-    double dE = 0.0, cnt = 0.0;
-    for (int b = 0; b < SRC_BLOCKS; b++) { dE += part[2 * b]; cnt += part[2 * b + 1]; }
-    src->P_heat += dE;
-    src->n_heated += (unsigned long long)cnt;
-    src->n_heat_calls += 1;
-}
-
-__global__ void k_tally_finish(const double *part, int n_icp, SrcDev *src) {
-    const int v = threadIdx.x;
-    const int nv = 2 * n_icp;
-    if (v >= nv) return;
-    double s = 0.0;
-    for (int b = 0; b < SRC_BLOCKS; b++) s += part[(size_t)b * nv + v];
-    if (v < n_icp) src->Nh[v] = (long long)s;
-    else src->sum_dEk[v - n_icp] = s;
+    s = red[0];
+    if (kind == FIN_HEAT) {
+        if (v == 0) src->P_heat += s;
+        else { src->n_heated += (unsigned long long)s; src->n_heat_calls += 1; }
+    } else if (kind == FIN_TALLY) {
+        const int nb = nv / 2;
+        if (v < nb) src->Nh[v] = (long long)s;
+        else src->sum_dEk[v - nb] = s;
+    } else {
+        if (v < LEPIC_MAXSP) src->P_inj[v] += s;
+        else src->P_src[v - LEPIC_MAXSP] += s;
+    }
 }
 
 // main.f90:1003-1010 for one rank: Te from the tallies, vt = sqrt(2 qe Te / |m|)
@@ -518,7 +629,7 @@ static int run_heating(lepic_ctx *c, int it) {
     memset(&P, 0, sizeof(P));
     P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
     P.cnt = c->dcnt; P.src = S->d;
-    P.R = make_region(s, g);
+    P.R = make_region(s, g, c->S);
     P.ux = g.dx * std::ldexp(1.0, -c->S); P.uy = g.dy * std::ldexp(1.0, -c->S);
     P.ymax = g.ny * g.dy; P.dt = g.dt; P.nudt = s.nudt; P.Pabs_cor = s.Pabs_cor;
     P.Ek = 0.5 * g.Nm[0] * g.mass[0];
@@ -526,9 +637,9 @@ static int run_heating(lepic_ctx *c, int it) {
     P.n_icp = s.n_icp; P.gpp = s.flag_gpp; P.type = s.eheat_type;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);
-    k_eheat<<<SRC_BLOCKS, SRC_THREADS, 0, c->stream>>>(P, S->part);
+    k_eheat<<<HEAT_BLOCKS, SRC_THREADS, 0, c->stream>>>(P, S->part);
     LCUDA(cudaGetLastError());
-    k_heat_finish<<<1, 32, 0, c->stream>>>(S->part, S->d);
+    k_finish<<<2, 256, 0, c->stream>>>(S->part, HEAT_BLOCKS, 2, FIN_HEAT, S->d);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
@@ -542,7 +653,7 @@ static int run_tally(lepic_ctx *c) {
     memset(&P, 0, sizeof(P));
     P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
     P.cnt = c->dcnt;
-    P.R = make_region(s, g);
+    P.R = make_region(s, g, c->S);
     P.ux = g.dx * std::ldexp(1.0, -c->S); P.uy = g.dy * std::ldexp(1.0, -c->S);
     P.ymax = g.ny * g.dy;
     P.Ek = 0.5 * g.Nm[0] * g.mass[0];
@@ -557,7 +668,7 @@ static int run_tally(lepic_ctx *c) {
     }
     k_heat_tally<<<SRC_BLOCKS, SRC_THREADS, smem, c->stream>>>(P, S->part);
     LCUDA(cudaGetLastError());
-    k_tally_finish<<<1, 2 * LEPIC_MAXICP, 0, c->stream>>>(S->part, P.n_icp, S->d);
+    k_finish<<<2 * P.n_icp, 256, 0, c->stream>>>(S->part, SRC_BLOCKS, 2 * P.n_icp, FIN_TALLY, S->d);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
@@ -586,7 +697,7 @@ static int run_injection(lepic_ctx *c, int it) {
     P.src = S->d; P.cnt = c->dcnt; P.ntype = g.ntype;
     P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
     P.opt = s.opt_inj; P.flag_nmn = g.flag_nmn; P.diffsrc = s.flag_diffsrc;
-    P.R = make_region(s, g);
+    P.R = make_region(s, g, c->S);
     P.dx = g.dx; P.dy = g.dy; P.xmax = g.nx * g.dx; P.ymax = g.ny * g.dy;
     for (int sp = 0; sp < g.ntype; sp++) {
         double vt = g.vt0[sp];
@@ -605,9 +716,7 @@ static int run_injection(lepic_ctx *c, int it) {
     keys(s, &P.k0, &P.k1);
     k_inject<<<INJ_BLOCKS, INJ_THREADS, 0, c->stream>>>(P, S->part);
     LCUDA(cudaGetLastError());
-    // P_inj[] and P_src[] are adjacent in SrcDev: one finishing pass adds both
-    static_assert(offsetof(SrcDev, P_src) == offsetof(SrcDev, P_inj) + sizeof(double) * LEPIC_MAXSP, "layout");
-    k_src_finish<<<1, 2 * LEPIC_MAXSP, 0, c->stream>>>(S->part, INJ_BLOCKS, 2 * LEPIC_MAXSP, S->d->P_inj, 1);
+    k_finish<<<2 * LEPIC_MAXSP, 256, 0, c->stream>>>(S->part, INJ_BLOCKS, 2 * LEPIC_MAXSP, FIN_INJ, S->d);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }

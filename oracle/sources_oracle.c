@@ -108,7 +108,8 @@ void o_eheating(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const do
     }
 }
 
-/* the same with the device's streams: decision (slot, step), then one velocity draw */
+/* the same with the device's streams: the decision from word k & 3 of the draw of slot group
+ * k / 4 and the step, then one velocity draw per heated slot */
 void o_eheating_ctr(const o_cfg *c, const o_src *s, double *vxp, int64_t n, const double *vt,
                     uint64_t seed, int32_t it, double *P_heat, int64_t *n_heated) {
     const double dr = (s->xr_pow - s->xl_pow) / 2.0;
@@ -120,8 +121,9 @@ void o_eheating_ctr(const o_cfg *c, const o_src *s, double *vxp, int64_t n, cons
         double nu_tmp = s->nudt / c->dt;
         if (s->flag_gpp == 1) nu_tmp = (s->nudt / c->dt) * 9.0 * s->Pabs_cor * exp(-9.0 * rp2 / (dr * dr));
         uint32_t r[4], q[4];
-        draw4((uint32_t)k, (uint32_t)((uint64_t)k >> 32), TAG_HEAT, (uint32_t)it, seed, r);
-        if (!(o_u01(r[0]) <= nu_tmp * c->dt)) continue;
+        const uint64_t g = (uint64_t)k >> 2;   /* one draw per group of 4 slots, word k & 3 */
+        draw4((uint32_t)g, (uint32_t)(g >> 32), TAG_HEAT, (uint32_t)it, seed, r);
+        if (!(o_u01(r[k & 3]) <= nu_tmp * c->dt)) continue;
         const int b = band_of(c, s, p[1]);
         draw4((uint32_t)k, (uint32_t)((uint64_t)k >> 32), TAG_HEATV, (uint32_t)it, seed, q);
         double dvx, dvy, dvz, unused;

@@ -270,3 +270,45 @@ def test_source_errors(gpu_lib):
         assert len(sim.get_particles(0)) == 10
     finally:
         sim.close()
+
+
+def test_region_edges_exact(gpu_lib):
+    """Particles on the fixed-point values around every edge of the slit: with nu*dt = 1 every
+    electron of the region is heated, so the heated set and the tally counts show the region
+    test itself, which must equal the oracle's FP64 test exactly."""
+    case = make_case()
+    cfg, sp = oracle_cfg(case)
+    sim = GpuSimulation(case, load=False, capacity=200000)
+    try:
+        Sb = shift_of(sim)
+        ux = case.dx * 2.0 ** -Sb
+        sc = S.source_config(S.SourceDeck(heat_region_cm=(0.1234567, 0.4123457, 0.0987654, 0.5012345),
+                                          nu_h=1.0 / (4 * case.dt), I_inj=-1.0), case.dt, sp.vt0[0])
+        assert sc.nudt == pytest.approx(1.0)
+        xa, dr = (sc.xl_pow + sc.xr_pow) / 2, (sc.xr_pow - sc.xl_pow) / 2
+        xe = [sc.xl_pow, sc.xr_pow, xa - dr, xa + dr, xa]
+        ye = [sc.yl_pow, sc.yr_pow, 0.5 * case.ny * case.dy]
+        Xs = np.unique(np.concatenate([np.round(np.array(xe) / ux).astype(np.int64)[:, None] + np.arange(-3, 4)]))
+        Ys = np.unique(np.concatenate([np.round(np.array(ye) / ux).astype(np.int64)[:, None] + np.arange(-3, 4)]))
+        XX, YY = np.meshgrid(Xs, Ys)
+        v = np.zeros((XX.size, 6))
+        v[:, 0] = XX.ravel() * ux
+        v[:, 1] = YY.ravel() * ux
+        v[:, 3:] = 1.0
+        sim.put_particles(0, v)
+        sim.set_sources(sc)
+        p0 = sim.get_particles(0)
+        assert np.array_equal(p0[:, :2], v[:, :2])
+        sim.heating_tally()
+        sim.eheating(4)
+        p1 = sim.get_particles(0)
+        t = sim.source_tallies()
+        o = p0.copy()
+        _, nh = O.eheating(cfg, O.make_src(sc), o, vt_used(sc, sp), seed=sc.seed, it=4)
+        heated_o = np.any(o[:, 3:] != p0[:, 3:], axis=1)
+        heated_d = np.any(p1[:, 3:] != p0[:, 3:], axis=1)
+        assert 0 < heated_o.sum() < len(v) and np.array_equal(heated_o, heated_d)
+        Nh, _ = O.heat_tally(cfg, O.make_src(sc), p0)
+        assert t["Nh"] == list(Nh)
+    finally:
+        sim.close()
