@@ -273,8 +273,8 @@ def learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step_f
 
 
 def sources_measure(args, sim, lib, ctx, stream, it, case):
-    """eheating, the heating-region tally and part_injection (the per-step particle sources)
-    on the workload's own electron population, each entry point timed with CUDA events on
+    """eheating, the heating-region tally, part_injection and part_flux_emitter (the per-step
+    particle sources) on the workload's own electron population, each entry point timed with CUDA events on
     the library's stream over args.steps calls after 3 untimed ones.  Heating region: the slit
     0.1 L <= x <= 0.6 L over the full height; nu_h = 5e8 /s (nu*dt*ns_heat = 2e-3 at dt = 1e-12 s,
     ns_heat = 4); 65536 particles injected per species and call (fixed current, uniform slit).
@@ -317,6 +317,20 @@ def sources_measure(args, sim, lib, ctx, stream, it, case):
     c0 = sim.source_tallies()["n_inj"]
     inj_ms = timed(lambda: sim.check(lib.lepic_gpu_part_injection(ctx, it), "part_injection"))
     c1 = sim.source_tallies()["n_inj"]
+    # part_flux_emitter of electrons (THm = 1 eV) from the plasma-side face of the aperture
+    # plate at x = 0.8 L, 65536 per call
+    i0 = int(round(0.8 * case.nx)) + 1
+    ap = max(5, int(round(40 * case.nx / 2048)))
+    Lgrd = case.ny * case.dy - (ap // 2) * case.dy * 3
+    js = n_inj * dk.QE * sim.sp.Nm[0] / (case.zmax * Lgrd * case.dt)
+    sc.js = js
+    sc.ptype_fx, sc.tag_b, sc.ns_Hm, sc.n_holes = 0, -1, 1, 3
+    sc.xg1, sc.Lg, sc.Lh = (i0 - 0.5) * case.dx, case.ny * case.dy, (ap // 2) * case.dy
+    sc.THm = 1.0
+    sim.set_sources(sc)
+    e0 = sim.source_tallies()["n_emit"][0]
+    emit_ms = timed(lambda: sim.check(lib.lepic_gpu_flux_emitter(ctx, it), "flux_emitter"))
+    e1 = sim.source_tallies()["n_emit"][0]
     sim.sync()
     peak, peak_kind = peaks()
     heat_bytes = 8 * n_slots + 4 * n_in + 20 * n_heated
@@ -331,6 +345,7 @@ def sources_measure(args, sim, lib, ctx, stream, it, case):
                           "algorithmic_bytes": tally_bytes, "kernels": "k_heat_tally + k_finish"},
         "part_injection": {"ms": inj_ms, "injected_per_call": [(b - a) / (reps + 3) for a, b in zip(c0, c1)],
                            "kernels": "k_inj_plan + k_inject + k_finish"},
+        "flux_emitter": {"ms": emit_ms, "emitted_per_call": (e1 - e0) / (reps + 3), "kernels": "k_emit (one CTA)"},
         "peak_gbs": peak, "peak_kind": peak_kind, "calls_timed": reps,
     }
 

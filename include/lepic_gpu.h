@@ -190,8 +190,9 @@ int lepic_gpu_collisions(lepic_ctx *ctx, int32_t it, lepic_mcc_stats *stats);
 int lepic_gpu_push_deposit(lepic_ctx *ctx, int32_t it, lepic_push_stats *stats);
 /* One PIC step, the in-scope body of main.f90:818-1090: calc_rhs -> iterative_solver ->
  * calc_Efield -> part_sorting (MOD(it,nsort)==1) -> collisions (it>1, MOD(it,ns_coll)==1)
- * -> [eheating, MOD(it,ns_heat)==0] -> push_deposit -> [part_injection, MOD(it,ns_inj)==0],
- * the bracketed source steps only after lepic_gpu_set_sources.  eps / mode as
+ * -> [eheating, MOD(it,ns_heat)==0] -> push_deposit -> [part_injection, MOD(it,ns_inj)==0]
+ * -> [part_flux_emitter, js > 0 and (ns_Hm == 1 or MOD(it,ns_Hm) == 1)], the bracketed
+ * source steps only after lepic_gpu_set_sources.  eps / mode as
  * lepic_gpu_iterative_solver. */
 int lepic_gpu_step(lepic_ctx *ctx, int32_t it, double eps, int32_t mode);
 
@@ -275,7 +276,18 @@ typedef struct lepic_source_config {
     double I_inj;              /* [A]                                                      */
     double THm;                /* [eV]                                                     */
     double ni0[LEPIC_MAXSP];   /* charged-species fractions (read_reactions.f90, main.f90:180) */
-    uint64_t seed;             /* key of the heating and injection streams                 */
+    uint64_t seed;             /* key of the heating, injection and emission streams       */
+    /* part_flux_emitter (part_flux_emitter.f90:1-217): surface emission from the grid plane
+     * x = xg1 of the deck (read_input.f90:142-151, generate_boundary.f90:246-271) */
+    double js;                 /* emitted current density [A/m^2] (jne*10); <= 0: off      */
+    int32_t ptype_fx;          /* 0-based emitted species                                  */
+    int32_t tag_b;             /* 0-based species of the chamfer-emitted particles, -1 none */
+    int32_t ns_Hm;             /* emission when ns_Hm == 1 or MOD(it, ns_Hm) == 1          */
+    int32_t n_holes;
+    double xg1, Lg, Lh;        /* grid plane, grid length, hole half size [m] (Lh rounded
+                                  to the cell as generate_boundary.f90:267-270 does)       */
+    int32_t flag_chmfrd;       /* chamfered aperture (generate_boundary.f90:110-116)       */
+    double chmfrd[4];          /* chmfrd_array: x1, x2, (ymax/2 - y1), (ymax/2 - y2) [m]   */
 } lepic_source_config;
 
 /* Cumulative tallies since the context was created or last reset; the reference's names. */
@@ -292,6 +304,10 @@ typedef struct lepic_source_tally {
                                         last tally (charge_deposition's Nh)                */
     double sum_dEk[LEPIC_MAXICP];    /* their kinetic energy 0.5 Nm m v^2 (eheat_type 1)   */
     double vt[LEPIC_MAXICP];         /* heating thermal speed in use                       */
+    int64_t n_emit[LEPIC_MAXSP];     /* particles emitted by part_flux_emitter (cumulative) */
+    int64_t n_emit_last[LEPIC_MAXSP];/* ... by its last call                                */
+    int64_t n_emit_out;              /* emitted, then outside the box after their first
+                                        partial move: counted as wall losses (n_lost)      */
 } lepic_source_tally;
 
 /* Sets (or replaces) the source configuration; flag_heat = flag_inj = 0 turns both off.
@@ -310,6 +326,10 @@ int lepic_gpu_eheating(lepic_ctx *ctx, int32_t it);
  * are computed on the device (fixed current, or the positive-ion losses since the last
  * injection for |opt_inj| = 2).  Enqueues only. */
 int lepic_gpu_part_injection(lepic_ctx *ctx, int32_t it);
+/* part_flux_emitter (part_flux_emitter.f90:1-217) at step it (the caller checks the
+ * cadence): the emitted particles are appended after the deposit (main.f90:1093-1096), so
+ * they enter np with the next push.  Enqueues only. */
+int lepic_gpu_flux_emitter(lepic_ctx *ctx, int32_t it);
 /* charge_deposition's heating-region tallies (Nh, sum_dEk per band) of the current
  * electrons.  Enqueues only; lepic_gpu_source_tallies reads them. */
 int lepic_gpu_heating_tally(lepic_ctx *ctx);

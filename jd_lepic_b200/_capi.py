@@ -151,6 +151,9 @@ class LepicSourceConfig(C.Structure):
         ("flag_inj", C.c_int32), ("ns_inj", C.c_int32), ("opt_inj", C.c_int32), ("flag_Tp", C.c_int32),
         ("flag_diffsrc", C.c_int32), ("tag_neg", C.c_int32), ("nproc_mpi", C.c_int32),
         ("I_inj", C.c_double), ("THm", C.c_double), ("ni0", C.c_double * MAXSP), ("seed", C.c_uint64),
+        ("js", C.c_double), ("ptype_fx", C.c_int32), ("tag_b", C.c_int32), ("ns_Hm", C.c_int32),
+        ("n_holes", C.c_int32), ("xg1", C.c_double), ("Lg", C.c_double), ("Lh", C.c_double),
+        ("flag_chmfrd", C.c_int32), ("chmfrd", C.c_double * 4),
     ]
 
 
@@ -160,6 +163,7 @@ class LepicSourceTally(C.Structure):
         ("P_inj", C.c_double * MAXSP), ("P_src", C.c_double * MAXSP), ("n_inj", C.c_int64 * MAXSP),
         ("n_inj_last", C.c_int64 * MAXSP), ("n_icp", C.c_int32), ("Nh", C.c_int64 * MAXICP),
         ("sum_dEk", C.c_double * MAXICP), ("vt", C.c_double * MAXICP),
+        ("n_emit", C.c_int64 * MAXSP), ("n_emit_last", C.c_int64 * MAXSP), ("n_emit_out", C.c_int64),
     ]
 
 
@@ -200,6 +204,7 @@ PROTOTYPES = {
     "lepic_gpu_eheating": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_part_injection": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_heating_tally": (C.c_int, [_VP]),
+    "lepic_gpu_flux_emitter": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_source_tallies": (C.c_int, [_VP, C.POINTER(LepicSourceTally), C.c_int32]),
     "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),
     "lepic_gpu_cnn_stats": (C.c_int, [_VP, C.POINTER(LepicCnnStats)]),

@@ -35,6 +35,10 @@
 #define TAG_INJN 0x494E4A4Eu    // injection count rounding
 #define TAG_INJP 0x494E4A50u    // injection position attempt
 #define TAG_INJV 0x494E4A56u    // injection velocity
+#define TAG_FXN 0x46584E31u     // emission count rounding
+#define TAG_FXP 0x46585031u     // emission attempt position
+#define TAG_FXV 0x46585631u     // emission velocity and time offset
+#define EMIT_THREADS 512
 
 // device tallies and per-call state of the sources
 struct SrcDev {
@@ -49,6 +53,7 @@ struct SrcDev {
     double sum_dEk[LEPIC_MAXICP];
     double vt[LEPIC_MAXICP];
     double Pabs[LEPIC_MAXICP];
+    unsigned long long n_emit[LEPIC_MAXSP], n_emit_last[LEPIC_MAXSP], n_emit_out;
 };
 
 struct SrcState {
@@ -525,6 +530,172 @@ __global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
 }
 
 // ---------------------------------------------------------------------------------------
+// part_flux_emitter (part_flux_emitter.f90:21-214).  Attempts are numbered a = 0, 1, ... and
+// processed in order, 512 per round by one CTA; each draws from its own stream.  An attempt
+// on a wall face (part_flux_emitter.f90:141-144) adds to the counts of plasma nodes on its
+// left and right; those counts run over all attempts of the call, and the attempt is kept
+// when they differ (the flux direction: part_flux_emitter.f90:145-157).  Block prefix sums
+// give every attempt its running counts and every kept attempt its particle index, so the
+// result is the sequential algorithm's; the call stops at the Nh-th particle.
+struct EmitP {
+    DevCounters *cnt;
+    SrcDev *src;
+    int nx, ny, S, W;
+    double dx, dy, xmax, ymax, ns_dt;
+    double xg1, Lg, y1c, th_c;
+    int n_icp, chamfer;
+    int sp[2];                      // species of flat-surface and chamfer emission
+    double dNh;
+    double vt[2], Ek[2];
+    long long cap[2];
+    const int32_t *bcnd;
+    uint32_t *X[2], *Y[2];
+    float *VX[2], *VY[2], *VZ[2];
+    long long max_attempts_extra;
+    uint32_t it, k0, k1;
+};
+
+// exclusive prefix (in thread order) and block total of a predicate
+__device__ __forceinline__ int block_prefix(bool p, int *wcnt, int &total) {
+    const unsigned b = __ballot_sync(0xffffffffu, p);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wcnt[w] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < EMIT_THREADS / 32; i++) {
+        const int c = wcnt[i];
+        off += i < w ? c : 0;
+        tot += c;
+    }
+    __syncthreads();
+    total = tot;
+    return off + __popc(b & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
+    __shared__ int wcnt[EMIT_THREADS / 32];
+    __shared__ long long s_l, s_r, s_tot, s_n[2], s_start[2], s_Nh, s_out[2];
+    __shared__ double red[2][EMIT_THREADS];
+    const double pi = 3.141592653589793;
+    if (threadIdx.x == 0) {
+        long long N = (long long)P.dNh;
+        const U4 r = philox4x32_10(U4{0u, 0u, TAG_FXN, P.it}, P.k0, P.k1);  // part_flux_emitter.f90:47-51
+        if (u01(r.x) <= P.dNh - (double)N) N += 1;
+        s_Nh = N;
+        s_l = s_r = s_tot = 0;
+        for (int q = 0; q < 2; q++) { s_n[q] = 0; s_out[q] = 0; s_start[q] = P.cnt->n_slots[P.sp[q]]; }
+    }
+    __syncthreads();
+    const long long Nh = s_Nh;
+    const long long max_att = 64 * Nh + P.max_attempts_extra;
+    double e[2] = {0.0, 0.0};
+    for (long long base = 0; s_tot < Nh && base < max_att; base += EMIT_THREADS) {
+        const long long a = base + threadIdx.x;
+        bool wall = false, lh = false, rh = false;
+        int q = 0;
+        double x = P.xg1, y = 0.0, th = pi / 2.0;
+        if (a < max_att) {
+            const U4 r = philox4x32_10(U4{(uint32_t)a, (uint32_t)(a >> 32), TAG_FXP, P.it}, P.k0, P.k1);
+            y = P.n_icp == 1 ? (P.ymax - P.Lg) / 2.0 + P.Lg * u01(r.x) : P.ymax * (1.0 - u01(r.x));
+            const double h2 = P.ymax / 2.0;
+            if (P.chamfer && ((y <= h2 && y > P.y1c) || (y > h2 && fabs(P.ymax - y) > P.y1c))) {
+                q = 1;  // part_flux_emitter.f90:114-133
+                double thp = P.th_c, d0 = y - P.y1c, d1 = P.y1c;
+                if (y > h2) { thp = -P.th_c; d0 = fabs(y - P.ymax) - P.y1c; d1 = P.ymax - P.y1c; }
+                x = P.xg1 + d0 * cos(thp);
+                y = d1 + d0 * sin(thp);
+            }
+            // the rotation of the velocity (part_flux_emitter.f90:187-193), on the moved point
+            if (P.chamfer && ((y <= h2 && y > P.y1c) || (y > h2 && fabs(P.ymax - y) > P.y1c)))
+                th = y > h2 ? pi / 2.0 + P.th_c : P.th_c;
+            const int ix = (int)(x / P.dx) + 1, iy = (int)(y / P.dy) + 1;
+            if (ix >= 1 && ix <= P.nx + 1 && iy >= 1 && iy <= P.ny + 1) {  // INT truncates toward 0
+                const int32_t *b = P.bcnd;
+                const long long m = ix + (long long)iy * P.W;
+                wall = (b[m] >= 1 && b[m + P.W] >= 1) || (b[m + 1] >= 1 && b[m + 1 + P.W] >= 1);
+                lh = wall && b[m - 1] == -1;
+                rh = wall && b[m + 1] == -1;
+            }
+        }
+        int tl, tr, tacc, tacc1;
+        const long long cl = s_l + block_prefix(lh, wcnt, tl) + (lh ? 1 : 0);
+        const long long cr = s_r + block_prefix(rh, wcnt, tr) + (rh ? 1 : 0);
+        const bool acc = wall && cl != cr;
+        const double dir = cl > cr ? 1.0 : -1.0;
+        const long long j = s_tot + block_prefix(acc, wcnt, tacc);
+        const int qe = (P.sp[1] != P.sp[0]) ? q : 0;   // the particle's species slot
+        const long long idx1 = block_prefix(acc && qe == 1, wcnt, tacc1);
+        const long long idx0 = (j - s_tot) - idx1;      // accepted before it with qe == 0
+        if (acc && j < Nh) {
+            const long long slot = s_start[qe] + s_n[qe] + (qe ? idx1 : idx0);
+            const U4 v = philox4x32_10(U4{(uint32_t)j, (uint32_t)(j >> 32), TAG_FXV, P.it}, P.k0, P.k1);
+            const double vt = P.vt[qe];
+            const double vx = dir * vt * sqrt(-log(1.0 - u01(v.x)));
+            double vy, vz;
+            gauss_pair(vt, v.y, v.z, &vy, &vz);
+            const double vxt = -vx * sin(th) + vy * cos(th), vyt = vx * cos(th) + vy * sin(th);
+            const double dt_tmp = u01(v.w) * P.ns_dt;
+            const double xn = x + vxt * dt_tmp, yn = y + vyt * dt_tmp;
+            const float fvx = (float)vxt, fvy = (float)vyt, fvz = (float)vz;
+            e[qe] += P.Ek[qe] * ((double)fvx * fvx + (double)fvy * fvy + (double)fvz * fvz);
+            if (slot >= P.cap[qe]) {
+                set_err(P.cnt, LERR_CAPACITY, 720 + qe);
+            } else if (xn < 0.0 || xn >= P.xmax || yn < 0.0 || yn >= P.ymax) {
+                // outside the box after the partial move: a wall loss of the next push
+                P.VX[qe][slot] = __int_as_float(0x7fc00000);
+                P.X[qe][slot] = 0; P.Y[qe][slot] = 0; P.VY[qe][slot] = 0.f; P.VZ[qe][slot] = 0.f;
+                atomicAdd((unsigned long long *)&s_out[qe], 1ull);
+            } else {
+                const double fx = xn / P.dx * (double)(1u << P.S), fy = yn / P.dy * (double)(1u << P.S);
+                const long long xl = ((long long)P.nx << P.S) - 1, yl = ((long long)P.ny << P.S) - 1;
+                P.X[qe][slot] = (uint32_t)min((long long)fx, xl);
+                P.Y[qe][slot] = (uint32_t)min((long long)fy, yl);
+                P.VX[qe][slot] = fvx; P.VY[qe][slot] = fvy; P.VZ[qe][slot] = fvz;
+            }
+        }
+        // the created particles of this round per species: those with j < Nh
+        const long long made = min((long long)tacc, Nh - s_tot);
+        int m1;
+        block_prefix(acc && j < Nh && qe == 1, wcnt, m1);
+        if (threadIdx.x == 0) {
+            s_l += tl;
+            s_r += tr;
+            s_tot += made;
+            s_n[1] += m1;
+            s_n[0] += made - m1;
+        }
+        __syncthreads();
+    }
+    if (s_tot < Nh && threadIdx.x == 0) set_err(P.cnt, LERR_RANGE, 730);  // no wall face found
+    // energy of the emitted particles (P_loss(4)), reduced by a fixed tree
+    red[0][threadIdx.x] = e[0];
+    red[1][threadIdx.x] = e[1];
+    __syncthreads();
+    for (int h = EMIT_THREADS / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + h];
+            red[1][threadIdx.x] += red[1][threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int nq = P.sp[1] != P.sp[0] ? 2 : 1;
+        for (int q = 0; q < nq; q++) {
+            const int sp = P.sp[q];
+            const long long n = min(s_n[q], P.cap[q] - s_start[q]);
+            P.cnt->n_slots[sp] = s_start[q] + n;
+            P.cnt->n_alive[sp] += n - s_out[q];
+            P.cnt->n_lost[sp] += (unsigned long long)s_out[q];
+            P.src->n_emit[sp] += (unsigned long long)n;
+            P.src->n_emit_last[sp] = (unsigned long long)n;
+            P.src->n_emit_out += (unsigned long long)s_out[q];
+            P.src->P_inj[sp] += red[q][0];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // host side
 static void keys(const lepic_source_config &s, uint32_t *k0, uint32_t *k1) {
     *k0 = (uint32_t)s.seed;
@@ -544,6 +715,17 @@ static int check_config(lepic_ctx *c, const lepic_source_config &s) {
     const lepic_config &g = c->cfg;
     const double xmax = g.nx * g.dx, ymax = g.ny * g.dy;
     auto bad = [&](const char *m) { c->last_err = std::string("sources: ") + m; return LEPIC_EINVAL; };
+    if (s.js > 0.0) {
+        if (s.ptype_fx < 0 || s.ptype_fx >= g.ntype) return bad("ptype_fx out of range");
+        if (s.tag_b < -1 || s.tag_b >= g.ntype) return bad("tag_b out of range");
+        if (s.ns_Hm < 1) return bad("ns_Hm < 1");
+        if (s.n_icp < 1 || s.n_icp > LEPIC_MAXICP) return bad("n_icp out of range");
+        if (!(s.xg1 >= 0.0) || !(s.Lg > 0.0) || !(s.Lh >= 0.0) || s.n_holes < 0) return bad("emitter grid");
+        if (s.Lh >= std::min(s.Lg, ymax)) return bad("Lh >= Lg (generate_boundary.f90:249-254)");
+        if (!(s.THm > 0.0)) return bad("THm must be > 0 for the emitter");
+        if (s.nproc_mpi < 1) return bad("nproc_mpi < 1");
+        if (s.flag_chmfrd && s.chmfrd[1] == s.chmfrd[0] && s.chmfrd[3] == s.chmfrd[2]) return bad("chamfer of zero length");
+    }
     if (!s.flag_heat && !s.flag_inj) return LEPIC_OK;
     if (s.flag_c != 0 && s.flag_c != 1) return bad("flag_c must be 0 or 1");
     if (!(s.xl_pow >= 0 && s.xr_pow > s.xl_pow)) return bad("need 0 <= xl_pow < xr_pow");
@@ -721,6 +903,51 @@ static int run_injection(lepic_ctx *c, int it) {
     return LEPIC_OK;
 }
 
+static int run_emitter(lepic_ctx *c, int it) {
+    SrcState *S = state(c);
+    const lepic_source_config &s = S->cfg;
+    const lepic_config &g = c->cfg;
+    EmitP P;
+    memset(&P, 0, sizeof(P));
+    P.cnt = c->dcnt; P.src = S->d;
+    P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
+    P.dx = g.dx; P.dy = g.dy; P.xmax = g.nx * g.dx; P.ymax = g.ny * g.dy;
+    P.ns_dt = (double)s.ns_Hm * g.dt;
+    P.xg1 = std::min(s.xg1, P.xmax);
+    P.Lg = std::min(s.Lg, P.ymax);
+    P.n_icp = s.n_icp;
+    // part_flux_emitter.f90:21-46: current I = js zmax Lgrd, particles per call
+    double Lgrd = s.n_icp * (P.Lg - s.Lh * s.n_holes);
+    P.chamfer = (s.ptype_fx == s.tag_neg && s.flag_chmfrd == 1) ? 1 : 0;
+    if (P.chamfer) {
+        const double x1 = s.chmfrd[0], x2 = s.chmfrd[1], y1 = s.chmfrd[2], y2 = s.chmfrd[3];
+        const double d = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+        P.th_c = std::acos((x2 - x1) / d);
+        P.y1c = y1;
+        Lgrd = 2.0 * (y1 + d);
+        if (Lgrd > P.ymax) { c->last_err = "flux emitter: Lgrd > ymax (part_flux_emitter.f90:38-41)"; return LEPIC_EINVAL; }
+    }
+    P.dNh = s.js * g.zmax * Lgrd * P.ns_dt / (g.Nm[s.ptype_fx] * g.qe) / (double)s.nproc_mpi;
+    P.sp[0] = s.ptype_fx;
+    P.sp[1] = (P.chamfer && s.tag_b >= 0) ? s.tag_b : s.ptype_fx;
+    for (int q = 0; q < 2; q++) {
+        const int sp = P.sp[q];
+        P.vt[q] = std::sqrt(2.0 * g.qe * s.THm / std::fabs(g.mass[sp]));  // part_flux_emitter.f90:178
+        P.Ek[q] = 0.5 * g.Nm[sp] * g.mass[sp];
+        P.cap[q] = c->sp[sp].cap;
+        SpeciesBuf &B = c->sp[sp];
+        P.X[q] = B.X[B.cur]; P.Y[q] = B.Y[B.cur];
+        P.VX[q] = B.VX[B.cur]; P.VY[q] = B.VY[B.cur]; P.VZ[q] = B.VZ[B.cur];
+    }
+    P.bcnd = c->bcnd;
+    P.max_attempts_extra = 65536;
+    P.it = (uint32_t)it;
+    keys(s, &P.k0, &P.k1);
+    k_emit<<<1, EMIT_THREADS, 0, c->stream>>>(P);
+    LCUDA(cudaGetLastError());
+    return LEPIC_OK;
+}
+
 static int te_update(lepic_ctx *c) {
     SrcState *S = state(c);
     const lepic_source_config &s = S->cfg;
@@ -738,6 +965,11 @@ extern "C" int lepic_gpu_eheating(lepic_ctx *c, int32_t it) {
 extern "C" int lepic_gpu_part_injection(lepic_ctx *c, int32_t it) {
     if (!c || !state(c) || !state(c)->cfg.flag_inj) return LEPIC_EINVAL;
     return run_injection(c, it);
+}
+
+extern "C" int lepic_gpu_flux_emitter(lepic_ctx *c, int32_t it) {
+    if (!c || !state(c) || !(state(c)->cfg.js > 0.0)) return LEPIC_EINVAL;
+    return run_emitter(c, it);
 }
 
 extern "C" int lepic_gpu_heating_tally(lepic_ctx *c) {
@@ -767,10 +999,16 @@ extern "C" int lepic_gpu_source_tallies(lepic_ctx *c, lepic_source_tally *out, i
         out->sum_dEk[b] = h.sum_dEk[b];
         out->vt[b] = h.vt[b];
     }
+    for (int s2 = 0; s2 < LEPIC_MAXSP; s2++) {
+        out->n_emit[s2] = (int64_t)h.n_emit[s2];
+        out->n_emit_last[s2] = (int64_t)h.n_emit_last[s2];
+    }
+    out->n_emit_out = (int64_t)h.n_emit_out;
     if (reset) {
         SrcDev z = h;
         z.P_heat = 0.0; z.n_heated = 0; z.n_heat_calls = 0;
-        for (int s = 0; s < LEPIC_MAXSP; s++) { z.P_inj[s] = 0.0; z.P_src[s] = 0.0; z.n_inj[s] = 0; }
+        for (int s = 0; s < LEPIC_MAXSP; s++) { z.P_inj[s] = 0.0; z.P_src[s] = 0.0; z.n_inj[s] = 0; z.n_emit[s] = 0; }
+        z.n_emit_out = 0;
         LCUDA(cudaMemcpyAsync(S->d, &z, sizeof(SrcDev), cudaMemcpyHostToDevice, c->stream));
         LCUDA(cudaStreamSynchronize(c->stream));
     }
@@ -797,6 +1035,8 @@ int sources_after_push(lepic_ctx *c, int it) {
     int r;
     if (s.flag_inj && it % s.ns_inj == 0)
         if ((r = run_injection(c, it)) != LEPIC_OK) return r;
+    if (s.js > 0.0 && (s.ns_Hm == 1 || it % s.ns_Hm == 1))  // main.f90:1093-1096
+        if ((r = run_emitter(c, it)) != LEPIC_OK) return r;
     if (s.flag_heat && s.Pabs[0] > 0.0 && (it + 1) % s.ns_heat == 0) {
         if ((r = run_tally(c)) != LEPIC_OK) return r;
         S->tally_it = it;

@@ -258,6 +258,9 @@ class GpuSimulation:
     def inject(self, it: int):
         self.check(self.lib.lepic_gpu_part_injection(self.ctx, it), "part_injection")
 
+    def flux_emitter(self, it: int):
+        self.check(self.lib.lepic_gpu_flux_emitter(self.ctx, it), "flux_emitter")
+
     def heating_tally(self):
         self.check(self.lib.lepic_gpu_heating_tally(self.ctx), "heating_tally")
 
@@ -268,7 +271,8 @@ class GpuSimulation:
         return {"P_heat": t.P_heat, "n_heated": t.n_heated, "n_heat_calls": t.n_heat_calls,
                 "P_inj": list(t.P_inj[:n]), "P_src": list(t.P_src[:n]), "n_inj": list(t.n_inj[:n]),
                 "n_inj_last": list(t.n_inj_last[:n]), "Nh": list(t.Nh[:b]), "sum_dEk": list(t.sum_dEk[:b]),
-                "vt": list(t.vt[:b])}
+                "vt": list(t.vt[:b]), "n_emit": list(t.n_emit[:n]), "n_emit_last": list(t.n_emit_last[:n]),
+                "n_emit_out": t.n_emit_out}
 
     def stream_ptr(self) -> int:
         return self.lib.lepic_gpu_stream(self.ctx) or 0

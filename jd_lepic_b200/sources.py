@@ -9,6 +9,7 @@ eheat_type and flag_gpp (main.f90:493-500).
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 
 from . import _capi as capi
@@ -32,11 +33,21 @@ class SourceDeck:
     te_update: int = 1
     vt: tuple = field(default_factory=tuple)        # initial heating speed per band [m/s]
     seed: int = 12345
+    # part_flux_emitter: jne [mA/cm^2] (<= 0: off), emitted species, grid plane and holes [cm]
+    jne: float = 0.0
+    ptype_fx: int = 0
+    tag_b: int = -1                                 # 0-based chamfer-emitted species, -1 none
+    xg1_cm: float = 0.0
+    Lg_cm: float = 0.0
+    Lh_cm: float = 0.0
+    n_holes: int = 0
+    chamfer_m: tuple = ()                           # chmfrd_array (x1, x2, ymax/2-y1, ymax/2-y2) [m]
 
 
-def source_config(d: SourceDeck, dt: float, vt0_e: float) -> capi.LepicSourceConfig:
+def source_config(d: SourceDeck, dt: float, vt0_e: float, dy: float = 0.0) -> capi.LepicSourceConfig:
     """The lepic_source_config of a deck; vt0_e is the electron vt0 (the initial heating speed
-    when the deck gives none, and the constant one when particles are injected)."""
+    when the deck gives none, and the constant one when particles are injected); dy the cell
+    height, to which the hole size is rounded down (generate_boundary.f90:267-270)."""
     c = capi.LepicSourceConfig()
     xl, xr, yl, yr = (v * 1e-2 for v in d.heat_region_cm)
     c.flag_c = 1 if (xl < 0.0 or xr < 0.0) else 0
@@ -71,4 +82,16 @@ def source_config(d: SourceDeck, dt: float, vt0_e: float) -> capi.LepicSourceCon
     for s, v in enumerate(d.ni0[:capi.MAXSP]):
         c.ni0[s] = v
     c.seed = d.seed
+    c.js = d.jne * 10.0 if d.jne > 0.0 else 0.0     # mA/cm^2 -> A/m^2 (part_flux_emitter.f90:22)
+    c.ptype_fx = d.ptype_fx
+    c.tag_b = d.tag_b
+    c.ns_Hm = 1                                       # main.f90:496
+    c.n_holes = d.n_holes
+    c.xg1, c.Lg = d.xg1_cm * 1e-2, d.Lg_cm * 1e-2
+    Lh = d.Lh_cm * 1e-2
+    c.Lh = math.floor(Lh / dy) * dy if dy > 0.0 else Lh
+    if d.chamfer_m:
+        c.flag_chmfrd = 1
+        for k in range(4):
+            c.chmfrd[k] = d.chamfer_m[k]
     return c

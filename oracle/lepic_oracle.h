@@ -190,4 +190,26 @@ int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, co
                          int64_t *np, const int64_t *cap, int64_t *count, double *P_inj,
                          double *P_src);
 
+/* part_flux_emitter (part_flux_emitter.f90:1-217), nproc = 1.  Emits into species
+ * sp_fx (flat surface) and sp_b (chamfer, = sp_fx when there is no chamfer species) at the
+ * grid plane xg1.  vxp[s] / np[s] / cap[s] per species; count[s] receives the particles
+ * emitted.  The _ctr form draws from the device's streams (attempt a, particle j) and
+ * stores the device's state (FP32 velocities, fixed-point positions with S bits when
+ * S > 0, NaN vx for a particle outside the box after its partial move, counted in *n_out).
+ * Returns 0, -2 on capacity, -3 when the attempts run out. */
+typedef struct {
+    double js, xg1, Lg, Lh;
+    int n_holes, ns_Hm, n_icp, nproc_mpi;
+    int chamfer;                /* ptype_fx == tag_neg and flag_chmfrd              */
+    double chmfrd[4];
+    int sp_fx, sp_b;
+    double THm;
+} o_emit;
+int o_part_flux_emitter(const o_cfg *c, const o_emit *e, const int32_t *bcnd, double **vxp,
+                        int64_t *np, const int64_t *cap, int32_t *iseed, int64_t *count,
+                        double *P_inj);
+int o_part_flux_emitter_ctr(const o_cfg *c, const o_emit *e, const int32_t *bcnd, uint64_t seed,
+                            int32_t it, int S, double **vxp, int64_t *np, const int64_t *cap,
+                            int64_t *count, double *P_inj, int64_t *n_out);
+
 #endif

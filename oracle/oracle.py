@@ -80,6 +80,15 @@ class OSrc(C.Structure):
     ]
 
 
+class OEmit(C.Structure):
+    _fields_ = [
+        ("js", C.c_double), ("xg1", C.c_double), ("Lg", C.c_double), ("Lh", C.c_double),
+        ("n_holes", C.c_int), ("ns_Hm", C.c_int), ("n_icp", C.c_int), ("nproc_mpi", C.c_int),
+        ("chamfer", C.c_int), ("chmfrd", C.c_double * 4), ("sp_fx", C.c_int), ("sp_b", C.c_int),
+        ("THm", C.c_double),
+    ]
+
+
 class OSolveStats(C.Structure):
     _fields_ = [("k", C.c_int), ("ktot", C.c_double), ("res", C.c_double), ("sweeps_fine", C.c_int)]
 
@@ -142,6 +151,12 @@ def lib() -> C.CDLL:
         L.o_part_injection_ctr.restype = C.c_int
         L.o_part_injection_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OSrc), _IP, _DP, _LP, C.c_uint64, C.c_int32,
                                            C.c_int, C.POINTER(_DP), _LP, _LP, _LP, _DP, _DP]
+        L.o_part_flux_emitter.restype = C.c_int
+        L.o_part_flux_emitter.argtypes = [C.POINTER(OCfg), C.POINTER(OEmit), _IP, C.POINTER(_DP), _LP, _LP,
+                                          C.POINTER(C.c_int32), _LP, _DP]
+        L.o_part_flux_emitter_ctr.restype = C.c_int
+        L.o_part_flux_emitter_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OEmit), _IP, C.c_uint64, C.c_int32, C.c_int,
+                                              C.POINTER(_DP), _LP, _LP, _LP, _DP, _LP]
         _lib = L
     return _lib
 
@@ -456,3 +471,47 @@ def part_injection_ctr(cfg, src, bcnd, phi, lost, seed, it, S, vxp_list, n_list)
                                     it, S, ptrs, npa.ctypes.data_as(_LP), cap.ctypes.data_as(_LP),
                                     cnt.ctypes.data_as(_LP), dp(Pi), dp(Ps))
     return rc, npa[:ns].copy(), cnt[:ns].copy(), Pi[:ns].copy(), Ps[:ns].copy()
+
+
+def make_emit(sc) -> OEmit:
+    """o_emit from a lepic_source_config."""
+    o = OEmit()
+    for f in ("js", "xg1", "Lg", "Lh", "n_holes", "ns_Hm", "n_icp", "nproc_mpi", "THm"):
+        setattr(o, f, getattr(sc, f))
+    o.chamfer = 1 if (sc.ptype_fx == sc.tag_neg and sc.flag_chmfrd == 1) else 0
+    for k in range(4):
+        o.chmfrd[k] = sc.chmfrd[k]
+    o.sp_fx = sc.ptype_fx
+    o.sp_b = sc.tag_b if (o.chamfer and sc.tag_b >= 0) else sc.ptype_fx
+    return o
+
+
+def _emit_args(cfg, vxp_list, n_list):
+    ns = cfg.ntype
+    ptrs = (_DP * MAXSP)(*[dp(v) for v in vxp_list] + [None] * (MAXSP - ns))
+    npa = np.zeros(MAXSP, dtype=np.int64)
+    npa[:ns] = n_list
+    cap = np.zeros(MAXSP, dtype=np.int64)
+    cap[:ns] = [v.shape[0] for v in vxp_list]
+    return ptrs, npa, cap, np.zeros(MAXSP, dtype=np.int64), np.zeros(MAXSP)
+
+
+def flux_emitter(cfg, emit, bcnd, vxp_list, n_list, iseed):
+    """The reference's form (ran2).  Returns (rc, n, count, P_inj, iseed)."""
+    ptrs, npa, cap, cnt, Pi = _emit_args(cfg, vxp_list, n_list)
+    sd = C.c_int32(iseed)
+    rc = lib().o_part_flux_emitter(C.byref(cfg), C.byref(emit), ip(bcnd), ptrs, npa.ctypes.data_as(_LP),
+                                   cap.ctypes.data_as(_LP), C.byref(sd), cnt.ctypes.data_as(_LP), dp(Pi))
+    ns = cfg.ntype
+    return rc, npa[:ns].copy(), cnt[:ns].copy(), Pi[:ns].copy(), sd.value
+
+
+def flux_emitter_ctr(cfg, emit, bcnd, seed, it, S, vxp_list, n_list):
+    """The device's form.  Returns (rc, n, count, P_inj, n_out)."""
+    ptrs, npa, cap, cnt, Pi = _emit_args(cfg, vxp_list, n_list)
+    out = C.c_int64(0)
+    rc = lib().o_part_flux_emitter_ctr(C.byref(cfg), C.byref(emit), ip(bcnd), seed, it, S, ptrs,
+                                       npa.ctypes.data_as(_LP), cap.ctypes.data_as(_LP), cnt.ctypes.data_as(_LP),
+                                       dp(Pi), C.byref(out))
+    ns = cfg.ntype
+    return rc, npa[:ns].copy(), cnt[:ns].copy(), Pi[:ns].copy(), out.value

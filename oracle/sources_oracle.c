@@ -385,3 +385,174 @@ int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, co
     }
     return rc;
 }
+
+/* ---- part_flux_emitter.f90 ------------------------------------------------------------ */
+#define TAG_FXN 0x46584E31u
+#define TAG_FXP 0x46585031u
+#define TAG_FXV 0x46585631u
+
+typedef struct {
+    double xg1, Lg, y1c, th_c, dNh;
+} emit_geo;
+
+/* part_flux_emitter.f90:21-46 (nproc = 1) and generate_boundary.f90:246-248 */
+static int emit_setup(const o_cfg *c, const o_emit *e, emit_geo *g) {
+    g->xg1 = e->xg1 > c->xmax ? c->xmax : e->xg1;
+    g->Lg = e->Lg > c->ymax ? c->ymax : e->Lg;
+    double Lgrd = e->n_icp * (g->Lg - e->Lh * e->n_holes);
+    g->y1c = 0.0;
+    g->th_c = 0.0;
+    if (e->chamfer) {
+        const double x1 = e->chmfrd[0], x2 = e->chmfrd[1], y1 = e->chmfrd[2], y2 = e->chmfrd[3];
+        const double d = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+        g->th_c = acos((x2 - x1) / d);
+        g->y1c = y1;
+        Lgrd = 2.0 * (y1 + d);
+        if (Lgrd > c->ymax) return -1;
+    }
+    const double I_sec = e->js * c->zmax * Lgrd;
+    g->dNh = I_sec * ((double)e->ns_Hm * c->dt) / (c->Nm[e->sp_fx] * c->qe) / (double)e->nproc_mpi;
+    return 0;
+}
+
+static int on_chamfer(const o_cfg *c, const emit_geo *g, double y) {
+    return (y <= c->ymax / 2.0 && y > g->y1c) || (y > c->ymax / 2.0 && fabs(c->ymax - y) > g->y1c);
+}
+
+/* the emission point of one attempt (part_flux_emitter.f90:103-136): returns the species slot
+ * q (1: chamfer), the point, the velocity rotation angle and the cell; 0 if off the grid */
+static int emit_point(const o_cfg *c, const o_emit *e, const emit_geo *g, double r, int *q, double *x,
+                      double *y, double *th, int *ix, int *iy) {
+    const double pi = 4.0 * atan(1.0);
+    *x = g->xg1;
+    *y = e->n_icp == 1 ? (c->ymax - g->Lg) / 2.0 + g->Lg * r : c->ymax * (1.0 - r);
+    *q = 0;
+    if (e->chamfer && on_chamfer(c, g, *y)) {
+        *q = 1;
+        double thp = g->th_c, d0 = *y - g->y1c, d1 = g->y1c;
+        if (*y > c->ymax / 2.0) {
+            thp = -g->th_c;
+            d0 = fabs(*y - c->ymax) - g->y1c;
+            d1 = c->ymax - g->y1c;
+        }
+        *x = g->xg1 + d0 * cos(thp);
+        *y = d1 + d0 * sin(thp);
+    }
+    *th = pi / 2.0;
+    if (e->chamfer && on_chamfer(c, g, *y)) *th = *y > c->ymax / 2.0 ? pi / 2.0 + g->th_c : g->th_c;
+    *ix = (int)(*x / c->dx) + 1;
+    *iy = (int)(*y / c->dy) + 1;
+    return *ix >= 1 && *ix <= c->nx + 1 && *iy >= 1 && *iy <= c->ny + 1;
+}
+
+/* the wall-face test and the running plasma-side counts (part_flux_emitter.f90:141-161);
+ * returns 1 when the attempt is kept, with its direction */
+static int emit_accept(const o_cfg *c, const int32_t *b, int ix, int iy, int64_t *cl, int64_t *cr, double *dir) {
+    const int W = c->nx + 3;
+    const int m = ix + iy * W;
+    if (!((b[m] >= 1 && b[m + W] >= 1) || (b[m + 1] >= 1 && b[m + 1 + W] >= 1))) return 0;
+    if (b[m - 1] == -1) (*cl)++;
+    if (b[m + 1] == -1) (*cr)++;
+    if (*cl == *cr) return 0;
+    *dir = *cl > *cr ? 1.0 : -1.0;
+    return 1;
+}
+
+int o_part_flux_emitter(const o_cfg *c, const o_emit *e, const int32_t *bcnd, double **vxp,
+                        int64_t *np, const int64_t *cap, int32_t *iseed, int64_t *count,
+                        double *P_inj) {
+    emit_geo g;
+    if (emit_setup(c, e, &g)) return -1;
+    int64_t Nh = (int64_t)g.dNh;
+    if (o_ran2(iseed) <= g.dNh - (double)Nh) Nh += 1;
+    int64_t cl = 0, cr = 0;
+    const int64_t max_att = 64 * Nh + 65536;
+    int64_t att = 0;
+    for (int s = 0; s < c->ntype; s++) count[s] = 0;
+    for (int64_t i = 0; i < Nh; i++) {
+        double x, y, th, dir = 1.0;
+        int q, ix, iy;
+        for (;;) { /* label 90 */
+            if (att++ >= max_att) return -3;
+            const double r = o_ran2(iseed);
+            const int ok = emit_point(c, e, &g, r, &q, &x, &y, &th, &ix, &iy);
+            (void)o_ran2(iseed); /* z_inj */
+            if (ok && emit_accept(c, bcnd, ix, iy, &cl, &cr, &dir)) break;
+        }
+        const int sp = q ? e->sp_b : e->sp_fx;
+        if (np[sp] + 1 > cap[sp]) return -2;
+        const double vt = sqrt(2.0 * c->qe * e->THm / fabs(c->mass[sp]));
+        double rnd[2], vy, vz;
+        const double vx = dir * vt * sqrt(-log(1 - o_ran2(iseed)));
+        rnd[0] = o_ran2(iseed);
+        rnd[1] = o_ran2(iseed);
+        o_load_gauss(&vy, &vz, vt, rnd);
+        const double vxt = -vx * sin(th) + vy * cos(th), vyt = vx * cos(th) + vy * sin(th);
+        const double dt_tmp = o_ran2(iseed) * ((double)e->ns_Hm * c->dt);
+        double *p = vxp[sp] + 6 * np[sp];
+        p[0] = x + vxt * dt_tmp; p[1] = y + vyt * dt_tmp; p[2] = 0.0;
+        p[3] = vxt; p[4] = vyt; p[5] = vz;
+        np[sp]++;
+        count[sp]++;
+        P_inj[sp] += 0.5 * c->Nm[sp] * c->mass[sp] * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5]);
+    }
+    return 0;
+}
+
+int o_part_flux_emitter_ctr(const o_cfg *c, const o_emit *e, const int32_t *bcnd, uint64_t seed,
+                            int32_t it, int S, double **vxp, int64_t *np, const int64_t *cap,
+                            int64_t *count, double *P_inj, int64_t *n_out) {
+    emit_geo g;
+    if (emit_setup(c, e, &g)) return -1;
+    const uint32_t U = (uint32_t)it;
+    uint32_t r[4];
+    draw4(0u, 0u, TAG_FXN, U, seed, r);
+    int64_t Nh = (int64_t)g.dNh;
+    if (o_u01(r[0]) <= g.dNh - (double)Nh) Nh += 1;
+    int64_t cl = 0, cr = 0, j = 0;
+    const int64_t max_att = 64 * Nh + 65536;
+    for (int s = 0; s < c->ntype; s++) count[s] = 0;
+    *n_out = 0;
+    for (int64_t a = 0; j < Nh && a < max_att; a++) {
+        double x, y, th, dir = 1.0;
+        int q, ix, iy;
+        draw4((uint32_t)a, (uint32_t)((uint64_t)a >> 32), TAG_FXP, U, seed, r);
+        if (!emit_point(c, e, &g, o_u01(r[0]), &q, &x, &y, &th, &ix, &iy)) continue;
+        if (!emit_accept(c, bcnd, ix, iy, &cl, &cr, &dir)) continue;
+        const int sp = q ? e->sp_b : e->sp_fx;
+        uint32_t v[4];
+        draw4((uint32_t)j, (uint32_t)((uint64_t)j >> 32), TAG_FXV, U, seed, v);
+        j++;
+        if (np[sp] + 1 > cap[sp]) return -2;
+        const double vt = sqrt(2.0 * c->qe * e->THm / fabs(c->mass[sp]));
+        const double vx = dir * vt * sqrt(-log(1.0 - o_u01(v[0])));
+        double vy, vz;
+        gauss_u(vt, v[1], v[2], &vy, &vz);
+        const double vxt = -vx * sin(th) + vy * cos(th), vyt = vx * cos(th) + vy * sin(th);
+        const double dt_tmp = o_u01(v[3]) * ((double)e->ns_Hm * c->dt);
+        const double xn = x + vxt * dt_tmp, yn = y + vyt * dt_tmp;
+        const float fvx = (float)vxt, fvy = (float)vyt, fvz = (float)vz;
+        P_inj[sp] += 0.5 * c->Nm[sp] * c->mass[sp] * ((double)fvx * fvx + (double)fvy * fvy + (double)fvz * fvz);
+        count[sp]++;
+        if (xn < 0.0 || xn >= c->xmax || yn < 0.0 || yn >= c->ymax) {
+            (*n_out)++;   /* a hole on the device: not among the live particles */
+            continue;
+        }
+        double *p = vxp[sp] + 6 * np[sp];
+        if (S > 0) {
+            const double sc = ldexp(1.0, S);
+            double fx = floor(xn / c->dx * sc), fy = floor(yn / c->dy * sc);
+            const double xl = ldexp((double)c->nx, S) - 1.0, yl = ldexp((double)c->ny, S) - 1.0;
+            if (fx > xl) fx = xl;
+            if (fy > yl) fy = yl;
+            p[0] = fx * (c->dx * ldexp(1.0, -S));
+            p[1] = fy * (c->dy * ldexp(1.0, -S));
+        } else {
+            p[0] = xn; p[1] = yn;
+        }
+        p[2] = 0.0;
+        p[3] = fvx; p[4] = fvy; p[5] = fvz;
+        np[sp]++;
+    }
+    return j < Nh ? -3 : 0;
+}

@@ -312,3 +312,92 @@ def test_region_edges_exact(gpu_lib):
         assert t["Nh"] == list(Nh)
     finally:
         sim.close()
+
+
+def plate_case(left=True, holes=((20, 26), (38, 44))):
+    case = configs.case0(ppc=4, nx=NX, ny=NX)
+    b = np.array(case.bcnd, dtype=np.int32, copy=True)
+    b[5:61, 40:44] = 1
+    for h0, h1 in holes:
+        b[h0:h1 + 1, 40:44] = -1
+    if not left:
+        b[2:case.ny + 1, 2:40] = 1
+    case.bcnd = b
+    case.phi0 = configs.potentials(b, {1: 0.0})
+    return case
+
+
+EMIT_CASES = [dict(left=True), dict(left=False),
+              dict(left=True, chamfer=True)]
+
+
+@pytest.mark.parametrize("kw", EMIT_CASES)
+def test_flux_emitter_matches_oracle(gpu_lib, kw):
+    left, chamfer = kw["left"], kw.get("chamfer", False)
+    case = plate_case(left, holes=((28, 36),) if chamfer else ((20, 26), (38, 44)))
+    cfg, sp = oracle_cfg(case)
+    sim = GpuSimulation(case, load=False, capacity=100000)
+    try:
+        rng = np.random.default_rng(8)
+        e = rand_particles(case, 3000, 9, 1e5)
+        sim.put_particles(0, e)
+        sim.put_particles(1, rand_particles(case, 3000, 10, 1e2))
+        xg1 = (39.5 if left else 42.5) * case.dx
+        extra = dict(tag_neg=1, ptype_fx=1, tag_b=0, chamfer_m=(39.5 * case.dx, 43.5 * case.dx, 2.0e-3, 2.6e-3),
+                     n_holes=1) if chamfer else {}
+        deck = dict(jne=1.0e5, ptype_fx=0, THm=5.0, xg1_cm=xg1 * 100, Lg_cm=55 * case.dy * 100,
+                    Lh_cm=3 * case.dy * 100, n_holes=2, nu_h=-1.0, I_inj=-1.0, seed=77)
+        deck.update(extra)
+        sc = S.source_config(S.SourceDeck(**deck), case.dt, sp.vt0[0], case.dy)
+        sim.set_sources(sc)
+        before = [sim.get_particles(s) for s in (0, 1)]
+        sim.flux_emitter(5)
+        after = [sim.get_particles(s) for s in (0, 1)]
+        t = sim.source_tallies()
+        Sb = shift_of(sim)
+        vx = [np.zeros((len(before[s]) + 40000, 6)) for s in (0, 1)]
+        for s in (0, 1):
+            vx[s][:len(before[s])] = before[s]
+        rc, n, cnt, Pi, nout = O.flux_emitter_ctr(cfg, O.make_emit(sc), np.ascontiguousarray(case.bcnd, np.int32),
+                                                  sc.seed, 5, Sb, vx, [len(b) for b in before])
+        assert rc == 0 and sum(cnt) > 2000
+        assert t["n_emit_last"] == list(cnt) and t["n_emit_out"] == nout
+        if chamfer:
+            assert cnt[0] > 0 and cnt[1] > 0
+        unit = case.dx * 2.0 ** -Sb
+        for s in (0, 1):
+            assert np.array_equal(after[s][:len(before[s])], before[s])
+            new, ref = after[s][len(before[s]):], vx[s][len(before[s]):n[s]]
+            assert len(new) == len(ref)
+            if len(new):
+                assert np.abs(new[:, :2] - ref[:, :2]).max() <= unit * 1.0001
+                float_match(ref[:, 3:], new[:, 3:])
+            assert t["P_inj"][s] == pytest.approx(Pi[s], rel=1e-9, abs=0.0)
+        ps = sim.push_stats()
+        assert ps["n_lost"] == [0, 0] or sum(ps["n_lost"]) == nout
+    finally:
+        sim.close()
+
+
+def test_step_runs_the_emitter(gpu_lib):
+    case = plate_case(True)
+    case.poisson_mode = 1
+    case.eps = 1e-8
+    cfg, sp = oracle_cfg(case)
+    sim = GpuSimulation(case, load=False, capacity=200000)
+    try:
+        sim.put_particles(0, rand_particles(case, 20000, 11, 1e5))
+        sim.put_particles(1, rand_particles(case, 20000, 12, 1e2))
+        sim.deposit()
+        sc = S.source_config(S.SourceDeck(jne=2.0e4, ptype_fx=0, THm=5.0, xg1_cm=39.5 * case.dx * 100,
+                                          Lg_cm=55 * case.dy * 100, Lh_cm=3 * case.dy * 100, n_holes=2,
+                                          nu_h=-1.0, I_inj=-1.0, seed=5), case.dt, sp.vt0[0], case.dy)
+        sim.set_sources(sc)
+        per = []
+        for it in range(1, 5):
+            sim.step(it)
+            per.append(sim.source_tallies()["n_emit_last"][0])
+        t = sim.source_tallies()
+        assert min(per) > 0 and t["n_emit"][0] == sum(per)
+    finally:
+        sim.close()

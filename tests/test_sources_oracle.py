@@ -285,3 +285,95 @@ def test_source_deck_conversions():
     assert c.flag_Tp == 1 and c.THm == 3.0
     off = S.source_config(S.SourceDeck(nu_h=-1.0, I_inj=-1.0), 1e-11, 1.0e6)
     assert off.flag_heat == 0 and off.flag_inj == 0 and off.flag_c == 0
+
+
+# ---- part_flux_emitter -----------------------------------------------------------------
+def plate_with_holes(case, i0=40, width=4, j0=5, j1=60, holes=((20, 26), (38, 44)), plasma_left=True):
+    """A grid plate of wall nodes i0..i0+width-1, rows j0..j1, with apertures; the far side of
+    the plate is walled off when plasma_left is False so that the plasma is on the right."""
+    b = np.array(case.bcnd, dtype=np.int32, copy=True)
+    b[j0:j1 + 1, i0:i0 + width] = 1
+    for h0, h1 in holes:
+        b[h0:h1 + 1, i0:i0 + width] = -1
+    if not plasma_left:
+        b[2:case.ny + 1, 2:i0] = 1
+    return b
+
+
+def emit_cfg(sp, case, **kw):
+    d = dict(jne=1.0e5, ptype_fx=0, THm=5.0, xg1_cm=39.5 * case.dx * 100, Lg_cm=55 * case.dy * 100,
+             Lh_cm=3 * case.dy * 100, n_holes=2, nu_h=-1.0, I_inj=-1.0)
+    d.update(kw)
+    return S.source_config(S.SourceDeck(**d), case.dt, sp.vt0[0], case.dy)
+
+
+@pytest.mark.parametrize("left", [True, False])
+def test_flux_emitter_reference_form(oracle_lib, left):
+    case, cfg, sp = setup(64, 64)
+    b = plate_with_holes(case, plasma_left=left)
+    # the emission plane inside the plate's face cell on the plasma side
+    xg1 = (39.5 if left else 42.5) * case.dx
+    sc = emit_cfg(sp, case, xg1_cm=xg1 * 100)
+    em = O.make_emit(sc)
+    v = [np.zeros((50000, 6)), np.zeros((10, 6))]
+    rc, n, cnt, Pi, _ = O.flux_emitter(cfg, em, b, v, [0, 0], 4242)
+    Lgrd = 1 * (55 * case.dy - 3 * case.dy * 2)
+    dNh = sc.js * cfg.zmax * Lgrd * case.dt / (sp.Nm[0] * dk.QE)
+    assert rc == 0 and cnt[0] in (int(dNh), int(dNh) + 1) and cnt[0] > 5000 and cnt[1] == 0
+    p = v[0][:n[0]]
+    vt = math.sqrt(2 * dk.QE * 5.0 / abs(sp.mass[0]))
+    if left:   # the flux leaves the plate towards the plasma side
+        assert np.all(p[:, 3] < 0) and np.all(p[:, 0] <= xg1 + 1e-12)
+    else:
+        assert np.all(p[:, 3] > 0) and np.all(p[:, 0] >= xg1 - 1e-12)
+    # the normal component is the Rayleigh speed of a half-Maxwellian flux, mean vt sqrt(pi)/2
+    assert abs(np.abs(p[:, 3]).mean() / (vt * math.sqrt(math.pi) / 2) - 1) < 0.03
+    assert abs(p[:, 4].std() / (vt / math.sqrt(2)) - 1) < 0.03
+    assert abs(p[:, 5].std() / (vt / math.sqrt(2)) - 1) < 0.03
+    # nothing is emitted from the apertures
+    iy = (p[:, 1] / case.dy).astype(int) + 1
+    assert not np.any((iy >= 21) & (iy <= 25)) and not np.any((iy >= 39) & (iy <= 43))
+    assert Pi[0] == pytest.approx(0.5 * sp.Nm[0] * sp.mass[0] * (p[:, 3:] ** 2).sum(), rel=1e-9)
+
+
+def test_flux_emitter_two_forms_agree(oracle_lib):
+    case, cfg, sp = setup(64, 64)
+    b = plate_with_holes(case)
+    sc = emit_cfg(sp, case)
+    em = O.make_emit(sc)
+    va = [np.zeros((50000, 6)), np.zeros((10, 6))]
+    vb = [np.zeros((50000, 6)), np.zeros((10, 6))]
+    rc, na, ca, Pa, _ = O.flux_emitter(cfg, em, b, va, [0, 0], 99)
+    rc2, nb, cb, Pb, nout = O.flux_emitter_ctr(cfg, em, b, 17, 3, 0, vb, [0, 0])
+    assert rc == 0 and rc2 == 0 and abs(ca[0] - cb[0]) <= 1 and nout == 0
+    pa, pb = va[0][:na[0]], vb[0][:nb[0]]
+    for k in (1, 3, 4, 5):
+        assert abs(pa[:, k].mean() - pb[:, k].mean()) < 5 * pa[:, k].std() / math.sqrt(len(pa))
+        assert abs(pa[:, k].std() / pb[:, k].std() - 1) < 0.04
+    assert Pa[0] == pytest.approx(Pb[0], rel=0.04)
+
+
+def test_flux_emitter_chamfer_species(oracle_lib):
+    case, cfg, sp = setup(64, 64)
+    b = plate_with_holes(case, holes=((28, 36),))
+    ymax = case.ny * case.dy
+    # a chamfered aperture edge: from (x1, ymax/2 - y1) to (x2, ymax/2 - y2)
+    ch = (39.5 * case.dx, 43.5 * case.dx, 2.0e-3, 2.6e-3)     # Lgrd = 2 (y1 + d) = 5.44 mm < ymax
+    sc = emit_cfg(sp, case, tag_neg=1, ptype_fx=1, tag_b=0, chamfer_m=ch, n_holes=1, I_inj=-1.0)
+    em = O.make_emit(sc)
+    assert em.chamfer == 1 and em.sp_fx == 1 and em.sp_b == 0
+    v = [np.zeros((100000, 6)), np.zeros((100000, 6))]
+    rc, n, cnt, Pi, _ = O.flux_emitter_ctr(cfg, em, b, 5, 1, 0, v, [0, 0])
+    assert rc == 0 and cnt[0] > 0 and cnt[1] > 0       # both surfaces emit
+    d = math.hypot(ch[1] - ch[0], ch[3] - ch[2])
+    Lgrd = 2 * (ch[2] + d)
+    dNh = sc.js * cfg.zmax * Lgrd * case.dt / (sp.Nm[1] * dk.QE)
+    assert cnt.sum() in (int(dNh), int(dNh) + 1)
+
+
+def test_emitter_deck_conversion():
+    case, cfg, sp = setup(64, 64)
+    sc = emit_cfg(sp, case, Lh_cm=3.5 * case.dy * 100)
+    assert sc.js == pytest.approx(1.0e6) and sc.ns_Hm == 1
+    assert sc.Lh == pytest.approx(3 * case.dy)          # rounded down to the cell
+    assert sc.xg1 == pytest.approx(39.5 * case.dx)
