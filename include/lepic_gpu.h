@@ -189,11 +189,11 @@ int lepic_gpu_collisions(lepic_ctx *ctx, int32_t it, lepic_mcc_stats *stats);
  * charged species: np is zeroed and rebuilt from the moved particles. */
 int lepic_gpu_push_deposit(lepic_ctx *ctx, int32_t it, lepic_push_stats *stats);
 /* One PIC step, the in-scope body of main.f90:818-1090: calc_rhs -> iterative_solver ->
- * calc_Efield -> part_sorting (MOD(it,nsort)==1) -> collisions (it>1, MOD(it,ns_coll)==1)
- * -> [eheating, MOD(it,ns_heat)==0] -> push_deposit -> [part_injection, MOD(it,ns_inj)==0]
- * -> [part_flux_emitter, js > 0 and (ns_Hm == 1 or MOD(it,ns_Hm) == 1)], the bracketed
- * source steps only after lepic_gpu_set_sources.  eps / mode as
- * lepic_gpu_iterative_solver. */
+ * calc_Efield -> part_sorting (MOD(it,nsort)==1) -> [averages, MOD(it,navg)==1]
+ * -> collisions (it>1, MOD(it,ns_coll)==1) -> [eheating, MOD(it,ns_heat)==0] -> push_deposit
+ * -> [part_injection, MOD(it,ns_inj)==0] -> [part_flux_emitter, js > 0 and (ns_Hm == 1 or
+ * MOD(it,ns_Hm) == 1)]; the averages only after lepic_gpu_set_avg, the source steps only after
+ * lepic_gpu_set_sources.  eps / mode as lepic_gpu_iterative_solver. */
 int lepic_gpu_step(lepic_ctx *ctx, int32_t it, double eps, int32_t mode);
 
 /* Copies a device grid (LEPIC_GRID_*) to the host, FP64, in the layouts above. */
@@ -335,6 +335,20 @@ int lepic_gpu_flux_emitter(lepic_ctx *ctx, int32_t it);
 int lepic_gpu_heating_tally(lepic_ctx *ctx);
 /* Reads the tallies (synchronises); reset != 0 zeroes the cumulative ones afterwards. */
 int lepic_gpu_source_tallies(lepic_ctx *ctx, lepic_source_tally *out, int32_t reset);
+
+/* ---- averaging diagnostics ------------------------------------------------------------
+ * part_moments (utils.f90:1-131) + calc_avg (utils.f90:133-266) + the potential and field
+ * averages (main.f90:935-947) on the device, so the averages need no host transfer until the
+ * host writes them.  The source/sink columns of data_pavg (6, 7: ss2D) stay zero. */
+/* Allocates (or re-allocates and zeroes) the averages on the coarse grid na = n / size_na
+ * (read_input.f90:109-111); navg > 0 makes lepic_gpu_step take one sample when
+ * MOD(it,navg) == 1, after the sort (main.f90:906). */
+int lepic_gpu_set_avg(lepic_ctx *ctx, int32_t size_na, int32_t navg);
+/* One averaging sample now (enqueues only). */
+int lepic_gpu_calc_avg(lepic_ctx *ctx);
+/* Reads data_pavg(7, na1+1, na2+1, ntype) and phi_avg(3, 0:nx+2, 0:ny+2) (each nullable) and
+ * the sample count cnt_avg; reset != 0 zeroes them afterwards (main.f90:1290-1296). */
+int lepic_gpu_get_avg(lepic_ctx *ctx, double *data_pavg, double *phi_avg, int32_t *cnt_avg, int32_t reset);
 
 /* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
  * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network

@@ -206,6 +206,9 @@ PROTOTYPES = {
     "lepic_gpu_heating_tally": (C.c_int, [_VP]),
     "lepic_gpu_flux_emitter": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_source_tallies": (C.c_int, [_VP, C.POINTER(LepicSourceTally), C.c_int32]),
+    "lepic_gpu_set_avg": (C.c_int, [_VP, C.c_int32, C.c_int32]),
+    "lepic_gpu_calc_avg": (C.c_int, [_VP]),
+    "lepic_gpu_get_avg": (C.c_int, [_VP, _DP, _DP, C.POINTER(C.c_int32), C.c_int32]),
     "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),
     "lepic_gpu_cnn_stats": (C.c_int, [_VP, C.POINTER(LepicCnnStats)]),
     "lepic_gpu_cnn_net": (_VP, [_VP]),

@@ -34,6 +34,7 @@ SOURCES = {
     "noalloc.cu": ["-fmad=false"],
     "cnn.cu": [],
     "sources.cu": ["-fmad=false"],
+    "diag.cu": ["-fmad=false"],
 }
 
 

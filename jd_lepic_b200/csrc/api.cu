@@ -277,6 +277,7 @@ extern "C" int lepic_gpu_destroy(lepic_ctx *c) {
     cudaStreamSynchronize(c->stream);
     learn_free(c);
     sources_free(c);
+    avg_free(c);
     free_all(c);
     delete c;
     return LEPIC_OK;
@@ -589,6 +590,7 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
     if (g.nsort > 0 && it % g.nsort == 1)
         for (int s = 0; s < g.ntype; s++)
             if ((r = sort_species(c, s)) != LEPIC_OK) return r;
+    if ((r = avg_step(c, it)) != LEPIC_OK) return r;  // main.f90:906-949
     if (it > 1 && g.ns_coll > 0 && it % g.ns_coll == 1)
         if ((r = mcc_collide(c, it)) != LEPIC_OK) return r;
     if ((r = sources_before_push(c, it)) != LEPIC_OK) return r;

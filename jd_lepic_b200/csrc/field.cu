@@ -6,36 +6,7 @@
 //   calc_rhs  reads ntype*8 B (uint64 accumulators) + 1 B mask + 8 B kq, writes 8 B / node
 //   efield    reads 8 B phi (5-point, cached) + 1 B mask, writes 16 B (FP64) + 8 B (FP32)
 #include <algorithm>
-#include "lepic_internal.cuh"
-
-struct RhoParams {
-    int nx, ny, ntype, pbc;
-    const unsigned long long *acc[LEPIC_MAXSP];
-    const double *kq;
-    const int8_t *bc;
-    double k1[LEPIC_MAXSP];      // Nm / (dx dy zmax)
-    double charge[LEPIC_MAXSP];
-};
-
-// np(ix,iy,s) after the periodic fold of calc_rho.f90:1-35.  The reference accumulates
-// kq*(k1*w) per particle; here the exact integer sum of w*2^44 is scaled once.
-__device__ __forceinline__ double np_raw(const RhoParams &P, int s, int ix, int iy) {
-    const long long n = ix + (long long)iy * (P.nx + 3);
-    double w = (double)P.acc[s][n] * 5.684341886080802e-14; // 2^-44
-    return P.kq[n] * (P.k1[s] * w);
-}
-__device__ __forceinline__ double np_val(const RhoParams &P, int s, int ix, int iy) {
-    if (P.pbc) {
-        const int W = P.nx + 3;
-        if (iy == 1 && P.bc[ix + 1 * W] == 0)
-            return 0.5 * (np_raw(P, s, ix, 1) + np_raw(P, s, ix, P.ny + 1));
-        if (iy == P.ny + 1 && P.bc[ix + (P.ny + 1) * W] == 0) {
-            if (P.bc[ix + 1 * W] == 0) return 0.5 * (np_raw(P, s, ix, 1) + np_raw(P, s, ix, P.ny + 1));
-            return np_raw(P, s, ix, 1);
-        }
-    }
-    return np_raw(P, s, ix, iy);
-}
+#include "rho.cuh"
 
 // calc_rho.f90:37-77: rhs(ix,iy) = -sum_ptype charge(ptype)*np(ix,iy,ptype)
 __global__ void k_calc_rhs(RhoParams P, double *rhs) {
@@ -73,19 +44,6 @@ __global__ void k_np_grid(RhoParams P, int s, double *out) {
         bool in = ix >= 1 && ix <= P.nx + 1 && iy >= 1 && iy <= P.ny + 1;
         out[t] = in ? np_val(P, s, ix, iy) : np_raw(P, s, ix, iy);
     }
-}
-
-static RhoParams rho_params(lepic_ctx *c) {
-    RhoParams P;
-    P.nx = c->cfg.nx; P.ny = c->cfg.ny; P.ntype = c->cfg.ntype; P.pbc = c->cfg.flag_pbc;
-    for (int s = 0; s < LEPIC_MAXSP; s++) { P.acc[s] = nullptr; P.k1[s] = 0; P.charge[s] = 0; }
-    for (int s = 0; s < c->cfg.ntype; s++) {
-        P.acc[s] = c->sp[s].acc;
-        P.k1[s] = c->cfg.Nm[s] / (c->cfg.dx * c->cfg.dy * c->cfg.zmax);
-        P.charge[s] = c->cfg.charge[s];
-    }
-    P.kq = c->kq; P.bc = c->bc8;
-    return P;
 }
 
 int field_calc_rhs(lepic_ctx *c) {

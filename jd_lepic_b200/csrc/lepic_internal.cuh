@@ -130,6 +130,8 @@ struct lepic_ctx {
     long long n_unknown = 0;       // nodes with bcnd <= 0
     // particle sources (sources.cu), created by lepic_gpu_set_sources
     void *src = nullptr;
+    // averaging diagnostics (diag.cu), created by lepic_gpu_set_avg
+    void *avg = nullptr;
     // counters
     DevCounters *dcnt = nullptr;
     DevCounters *hcnt = nullptr;  // pinned mirror
@@ -268,6 +270,8 @@ int particles_get(lepic_ctx *c, int ptype, double *vxp, long long cap, long long
 int sources_before_push(lepic_ctx *c, int it);
 int sources_after_push(lepic_ctx *c, int it);
 void sources_free(lepic_ctx *c);
+int avg_step(lepic_ctx *c, int it);
+void avg_free(lepic_ctx *c);
 
 #define LCUDA(call)                                                                     \
     do {                                                                                \

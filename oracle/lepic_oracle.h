@@ -212,4 +212,12 @@ int o_part_flux_emitter_ctr(const o_cfg *c, const o_emit *e, const int32_t *bcnd
                             int32_t it, int S, double **vxp, int64_t *np, const int64_t *cap,
                             int64_t *count, double *P_inj, int64_t *n_out);
 
+/* part_moments (utils.f90:1-131): p_mts(4, 0:na1+2, 0:na2+2) of one species, index
+ * m*ncell + ix + iy*(na1+3), ncell = (na1+3)(na2+3), na = n/size_na; zeroed first. */
+void o_part_moments(const o_cfg *c, int size_na, int ptype, const double *vxp, int64_t n, const double *kq,
+                    double *p_mts);
+/* calc_avg (utils.f90:133-266) for one species: npg its np(0:nx+2, 0:ny+2); accumulates
+ * data_pavg(7, na1+1, na2+1, ntype). */
+void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const double *p_mts, double *data_pavg);
+
 #endif

@@ -24,7 +24,8 @@ MAXCOL = 64
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("lepic_oracle.c", "lepic_oracle.h", "cnn_oracle.c", "sources_oracle.c")]
+    srcs = [os.path.join(HERE, f) for f in ("lepic_oracle.c", "lepic_oracle.h", "cnn_oracle.c", "sources_oracle.c",
+                                            "diag_oracle.c")]
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", HERE, "-B" if force else "-s"], check=True, capture_output=True)
     return LIB
@@ -157,6 +158,8 @@ def lib() -> C.CDLL:
         L.o_part_flux_emitter_ctr.restype = C.c_int
         L.o_part_flux_emitter_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OEmit), _IP, C.c_uint64, C.c_int32, C.c_int,
                                               C.POINTER(_DP), _LP, _LP, _LP, _DP, _LP]
+        L.o_part_moments.argtypes = [C.POINTER(OCfg), C.c_int, C.c_int, _DP, C.c_int64, _DP, _DP]
+        L.o_calc_avg.argtypes = [C.POINTER(OCfg), C.c_int, C.c_int, _DP, _DP, _DP]
         _lib = L
     return _lib
 
@@ -515,3 +518,16 @@ def flux_emitter_ctr(cfg, emit, bcnd, seed, it, S, vxp_list, n_list):
                                        dp(Pi), C.byref(out))
     ns = cfg.ntype
     return rc, npa[:ns].copy(), cnt[:ns].copy(), Pi[:ns].copy(), out.value
+
+
+# ---- averaging diagnostics (utils.f90) ---------------------------------------------------
+def part_moments(cfg, size_na, ptype, vxp, kq):
+    na1, na2 = cfg.nx // size_na, cfg.ny // size_na
+    p = np.zeros((4, na2 + 3, na1 + 3))
+    lib().o_part_moments(C.byref(cfg), size_na, ptype, dp(np.ascontiguousarray(vxp)), vxp.shape[0], dp(kq), dp(p))
+    return p
+
+
+def calc_avg(cfg, size_na, ptype, npg, p_mts, data_pavg):
+    """data_pavg: (ntype, na2+1, na1+1, 7) array, accumulated in place."""
+    lib().o_calc_avg(C.byref(cfg), size_na, ptype, dp(np.ascontiguousarray(npg)), dp(p_mts), dp(data_pavg))

@@ -1,0 +1,102 @@
+"""Averaging diagnostics on the B200 (part_moments + calc_avg + the potential and field
+averages) against the FP64 restatement.  The device sums in FP64 with atomics, so the check
+is to 1e-12 of each component's largest magnitude."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from jd_lepic_b200 import _capi as capi, configs, deck as dk
+from jd_lepic_b200.simulation import GpuSimulation, species_params
+
+pytestmark = pytest.mark.gpu
+
+NX = 64
+
+
+def get_avg(sim, size_na, reset=False):
+    na = NX // size_na
+    data = np.zeros((sim.sp.ntype, na + 1, na + 1, 7))
+    phi = np.zeros((NX + 3, NX + 3, 3))
+    cnt = C.c_int32()
+    sim.check(sim.lib.lepic_gpu_get_avg(sim.ctx, data.ctypes.data_as(C.POINTER(C.c_double)),
+                                        phi.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt), 1 if reset else 0),
+              "get_avg")
+    return data, phi, cnt.value
+
+
+def close(a, b, tol=1e-12):
+    scale = max(np.abs(b).max(), 1e-300)
+    assert np.abs(a - b).max() <= tol * scale, (np.abs(a - b).max(), scale)
+
+
+@pytest.mark.parametrize("size_na", [1, 2, 4])
+def test_averages_match_oracle(gpu_lib, size_na):
+    case = configs.case0(ppc=4, nx=NX, ny=NX)
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    sp = species_params(case, d)
+    cfg = O.make_cfg(case, sp)
+    sim = GpuSimulation(case, load=False, capacity=400000)
+    try:
+        rng = np.random.default_rng(size_na)
+        for s, vs in ((0, 1.0e6), (1, 5.0e2)):
+            n = 200000
+            v = np.zeros((n, 6))
+            v[:, 0] = rng.random(n) * case.nx * case.dx * 0.999
+            v[:, 1] = rng.random(n) * case.ny * case.dy * 0.999
+            v[:, 3:] = rng.normal(0.0, vs, (n, 3)).astype(np.float32)
+            v[:, 3] += vs
+            sim.put_particles(s, v)
+        sim.sort(0)
+        sim.sort(1)
+        sim.deposit()
+        phi = rng.random((case.ny + 3, case.nx + 3))
+        sim.set_phi(phi)
+        E = sim.efield()
+        sim.check(sim.lib.lepic_gpu_set_avg(sim.ctx, size_na, 0), "set_avg")
+        sim.check(sim.lib.lepic_gpu_calc_avg(sim.ctx), "calc_avg")
+        sim.check(sim.lib.lepic_gpu_calc_avg(sim.ctx), "calc_avg")
+        data, phi_avg, cnt = get_avg(sim, size_na)
+        assert cnt == 2
+        kq = O.kq_of(np.asarray(case.bcnd))
+        na = NX // size_na
+        ref = np.zeros((sp.ntype, na + 1, na + 1, 7))
+        for s in (0, 1):
+            p = sim.get_particles(s)
+            pm = O.part_moments(cfg, size_na, s, p, kq)
+            npg = sim.grid(capi.GRID_NP + s)
+            O.calc_avg(cfg, size_na, s, npg, pm, ref)
+            O.calc_avg(cfg, size_na, s, npg, pm, ref)
+        for s in (0, 1):
+            for q in (0, 2, 3, 4):
+                close(data[s, ..., q], ref[s, ..., q])
+            close(data[s, ..., 1], ref[s, ..., 1], 1e-9)   # Tp: a difference of two close terms
+        assert np.array_equal(phi_avg[..., 0], 2 * phi)
+        assert np.array_equal(phi_avg[..., 1:], 2 * E)
+        assert np.all(data[..., 5:] == 0.0)
+        # reset
+        get_avg(sim, size_na, reset=True)
+        data2, phi2, cnt2 = get_avg(sim, size_na)
+        assert cnt2 == 0 and not data2.any() and not phi2.any()
+    finally:
+        sim.close()
+
+
+def test_step_takes_averages_at_navg(gpu_lib):
+    case = configs.case0(ppc=8, nx=NX, ny=NX)
+    case.poisson_mode = 1
+    case.eps = 1e-8
+    sim = GpuSimulation(case)
+    try:
+        sim.check(sim.lib.lepic_gpu_set_avg(sim.ctx, 2, 5), "set_avg")
+        for it in range(1, 12):
+            sim.step(it)
+        data, phi, cnt = get_avg(sim, 2)
+        assert cnt == 3                                   # it = 1, 6, 11
+        assert data[..., 0].sum() > 0 and np.isfinite(data).all()
+        # the averaged electron temperature is near the loaded 2 eV
+        te = data[0, 4:-4, 4:-4, 1] / cnt
+        assert 1.5 < np.median(te) < 2.5
+    finally:
+        sim.close()
