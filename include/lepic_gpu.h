@@ -350,6 +350,35 @@ int lepic_gpu_calc_avg(lepic_ctx *ctx);
  * the sample count cnt_avg; reset != 0 zeroes them afterwards (main.f90:1290-1296). */
 int lepic_gpu_get_avg(lepic_ctx *ctx, double *data_pavg, double *phi_avg, int32_t *cnt_avg, int32_t reset);
 
+/* Loss, power and collision tallies, cumulative since the context was created or the last
+ * reset: part_mover's p_mac and P_loss(1) (part_expmover.f90:316-427), collisions' P_loss(3)
+ * and cnt_col (collisions.f90:533-543, 896-899, 980-983, 1025-1033; the removal of a killed
+ * incident, part_expmover.f90:83-96, is counted when it is killed), and the sources' P_loss(2)
+ * and P_loss(4) (see lepic_source_tally).  FP64 sums made with device atomics: they agree with
+ * an ordered FP64 sum to rounding, not bit for bit. */
+#define LEPIC_MAXLABEL 16   /* wall labels kept apart (bcnd values, larger ones in the last) */
+#define LEPIC_MAXRG 8       /* x-regions of cnt_col (nm_rg)                               */
+typedef struct lepic_tallies {
+    int64_t n_loss[LEPIC_MAXSP][LEPIC_MAXLABEL]; /* p_mac(ptype, np_loss, igrid): wall losses by
+                                                    the label bcnd(ix,iy) of the loss cell   */
+    double P_w[LEPIC_MAXSP][LEPIC_MAXLABEL];     /* p_mac(ptype, P_w, igrid): their 0.5 Nm m v^2 [J] */
+    double P_loss[4][LEPIC_MAXSP];               /* P_loss(1..4, ptype) [J]: 1 wall losses (+ the
+                                                    injection's -Nm q phi term), 2 heating, 3
+                                                    collisions, 4 injection and emission      */
+    double cnt_col[3][LEPIC_MAXCOL][LEPIC_MAXRG];/* cnt_col(1..3, icol, i_rg): sum nu over the
+                                                    candidates, candidate count, sum 1/np_tot_rg
+                                                    over the collisions                       */
+    int32_t n_rg;
+} lepic_tallies;
+
+/* The x-regions of the collision tallies (read_input.f90:120-128; main.f90:316-328): n_rg
+ * ranges [xl_rg, xr_rg] and one [yl_rg, yr_rg], metres.  n_rg = 0: none. */
+int lepic_gpu_set_regions(lepic_ctx *ctx, int32_t n_rg, const double *xl_rg, const double *xr_rg,
+                          double yl_rg, double yr_rg);
+/* Reads the tallies (synchronises); reset != 0 zeroes them and the sources' power tallies
+ * afterwards (main.f90:1296-1300). */
+int lepic_gpu_get_tallies(lepic_ctx *ctx, lepic_tallies *out, int32_t reset);
+
 /* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
  * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network
  * (3x3 convolutions, channels 16/32/64/64, BF16 tensor-core convolutions with FP32

@@ -167,6 +167,18 @@ class LepicSourceTally(C.Structure):
     ]
 
 
+MAXLABEL = 16
+MAXRG = 8
+
+
+class LepicTallies(C.Structure):
+    _fields_ = [
+        ("n_loss", (C.c_int64 * MAXLABEL) * MAXSP), ("P_w", (C.c_double * MAXLABEL) * MAXSP),
+        ("P_loss", (C.c_double * MAXSP) * 4), ("cnt_col", ((C.c_double * MAXRG) * MAXCOL) * 3),
+        ("n_rg", C.c_int32),
+    ]
+
+
 _FP = C.POINTER(C.c_float)
 
 PROTOTYPES = {
@@ -207,6 +219,8 @@ PROTOTYPES = {
     "lepic_gpu_flux_emitter": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_source_tallies": (C.c_int, [_VP, C.POINTER(LepicSourceTally), C.c_int32]),
     "lepic_gpu_set_avg": (C.c_int, [_VP, C.c_int32, C.c_int32]),
+    "lepic_gpu_set_regions": (C.c_int, [_VP, C.c_int32, _DP, _DP, C.c_double, C.c_double]),
+    "lepic_gpu_get_tallies": (C.c_int, [_VP, C.POINTER(LepicTallies), C.c_int32]),
     "lepic_gpu_calc_avg": (C.c_int, [_VP]),
     "lepic_gpu_get_avg": (C.c_int, [_VP, _DP, _DP, C.POINTER(C.c_int32), C.c_int32]),
     "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),

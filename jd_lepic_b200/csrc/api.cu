@@ -54,7 +54,7 @@ static void free_all(lepic_ctx *c) {
     F(c->partials);
     F(c->cg_r); F(c->cg_p); F(c->cg_ap);
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
-    F(c->dcnt);
+    F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac);
     if (c->hcnt) cudaFreeHost(c->hcnt);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -246,6 +246,10 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
     }
     LALLOC(c->dcnt, 1);
     LCUDA(cudaMemset(c->dcnt, 0, sizeof(DevCounters)));
+    LALLOC(c->tally, 1);
+    LCUDA(cudaMemset(c->tally, 0, sizeof(TallyDev)));
+    LALLOC(c->rg_scratch, 2 * LEPIC_MAXRG);
+    LALLOC(c->rg_kfac, LEPIC_MAXSP);
     LCUDA(cudaMallocHost((void **)&c->hcnt, sizeof(DevCounters)));
     memset(c->hcnt, 0, sizeof(DevCounters));
     int r = mg_init(c);

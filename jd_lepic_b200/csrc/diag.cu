@@ -268,3 +268,59 @@ int avg_step(lepic_ctx *c, int it) {
     if (!A || A->navg < 1 || it % A->navg != 1) return LEPIC_OK;
     return avg_sample(c);
 }
+
+// ---------------------------------------------------------------------------------------
+// loss, power and collision tallies (the device side lives in push.cu, mcc.cu, sources.cu)
+extern "C" int lepic_gpu_set_regions(lepic_ctx *c, int32_t n_rg, const double *xl_rg, const double *xr_rg,
+                                     double yl_rg, double yr_rg) {
+    if (!c || n_rg < 0 || n_rg > LEPIC_MAXRG || (n_rg > 0 && (!xl_rg || !xr_rg))) return LEPIC_EINVAL;
+    const lepic_config &g = c->cfg;
+    const double xmax = g.nx * g.dx, ymax = g.ny * g.dy;
+    for (int i = 0; i < n_rg; i++) {  // main.f90:319-324
+        const double xl = std::max(xl_rg[i], 0.0), xr = std::min(xr_rg[i], xmax);
+        c->ixl_rg[i] = (int)std::lround(xl / g.dx) + 1;
+        c->ixr_rg[i] = (int)std::lround(xr / g.dx) + 1;
+    }
+    c->iyl_rg = (int)std::lround(std::max(yl_rg, 0.0) / g.dy) + 1;  // :325-328
+    c->iyr_rg = (int)std::lround(std::min(yr_rg, ymax) / g.dy) + 1;
+    c->n_rg = n_rg;
+    return LEPIC_OK;
+}
+
+int sources_power(lepic_ctx *c, double *P_heat, double *P_inj, double *P_src);
+int sources_reset_power(lepic_ctx *c);
+
+extern "C" int lepic_gpu_get_tallies(lepic_ctx *c, lepic_tallies *out, int32_t reset) {
+    if (!c || !out) return LEPIC_EINVAL;
+    TallyDev *h = new (std::nothrow) TallyDev;
+    if (!h) return LEPIC_ENOMEM;
+    cudaError_t e = cudaMemcpyAsync(h, c->tally, sizeof(TallyDev), cudaMemcpyDeviceToHost, c->stream);
+    int r = e == cudaSuccess ? lepic_gpu_sync(c) : LEPIC_ECUDA;
+    const lepic_config &g = c->cfg;
+    memset(out, 0, sizeof(*out));
+    double P_heat = 0.0, P_inj[LEPIC_MAXSP] = {0}, P_src[LEPIC_MAXSP] = {0};
+    if (r == LEPIC_OK) r = sources_power(c, &P_heat, P_inj, P_src);
+    for (int s = 0; s < g.ntype; s++) {
+        const double Ek = 0.5 * g.Nm[s] * g.mass[s];
+        double lost = 0.0;
+        for (int l = 0; l < LEPIC_MAXLABEL; l++) {
+            out->n_loss[s][l] = (int64_t)h->n_loss[s][l];
+            out->P_w[s][l] = Ek * h->v2_loss[s][l];
+            lost += out->P_w[s][l];
+        }
+        out->P_loss[0][s] = lost + P_src[s];
+        out->P_loss[1][s] = s == 0 ? P_heat : 0.0;
+        out->P_loss[2][s] = h->P3[s];
+        out->P_loss[3][s] = P_inj[s];
+    }
+    memcpy(out->cnt_col, h->cnt_col, sizeof(out->cnt_col));
+    out->n_rg = c->n_rg;
+    delete h;
+    if (r == LEPIC_OK && reset) {
+        // the per-step inv_np_rg stays; everything cumulative is zeroed
+        LCUDA(cudaMemsetAsync(c->tally, 0, offsetof(TallyDev, inv_np_rg), c->stream));
+        r = sources_reset_power(c);
+        if (r == LEPIC_OK) LCUDA(cudaStreamSynchronize(c->stream));
+    }
+    return r;
+}

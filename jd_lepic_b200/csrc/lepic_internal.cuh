@@ -58,6 +58,16 @@ struct DevCounters {
     int abort_flag;                       // set to end every wait of a cooperative kernel
 };
 
+// Loss, power and collision tallies (part_mover's p_mac and P_loss(1), collisions' P_loss(3)
+// and cnt_col), cumulative since the context was created or the tallies were reset.
+struct TallyDev {
+    unsigned long long n_loss[LEPIC_MAXSP][LEPIC_MAXLABEL];
+    double v2_loss[LEPIC_MAXSP][LEPIC_MAXLABEL];     // sum of v^2 [m^2/s^2]
+    double P3[LEPIC_MAXSP];                           // collisions' energy change [J]
+    double cnt_col[3][LEPIC_MAXCOL][LEPIC_MAXRG];
+    double inv_np_rg[LEPIC_MAXSP][LEPIC_MAXRG];       // 1/np_tot_rg of the current collision step
+};
+
 struct MGLevel {
     int nx, ny;
     double hx, hy;
@@ -134,6 +144,12 @@ struct lepic_ctx {
     void *avg = nullptr;
     // counters
     DevCounters *dcnt = nullptr;
+    TallyDev *tally = nullptr;
+    // x-regions of the collision tallies (main.f90:316-328), node indices
+    int n_rg = 0, iyl_rg = 0, iyr_rg = 0;
+    int ixl_rg[LEPIC_MAXRG] = {0}, ixr_rg[LEPIC_MAXRG] = {0};
+    int *rg_scratch = nullptr;     // device copy of ixl_rg, ixr_rg
+    double *rg_kfac = nullptr;     // dx dy zmax / Nm per species
     DevCounters *hcnt = nullptr;  // pinned mirror
     std::string last_err;
 };

@@ -20,7 +20,7 @@
 // Roofline: the selection pass generates one Philox block per 4 slots and reads nothing;
 // only candidates (N*Pmax, about 0.3 % of particles) read and write their 20 B record.
 #include <algorithm>
-#include "lepic_internal.cuh"
+#include "rho.cuh"
 
 #define MCC_THREADS 256
 #define MCC_MAX_REACTIONS 16  // reactions per incident species (checked at context creation)
@@ -45,7 +45,24 @@ struct MccP {
     int flag_ionrep;
     double fEk;
     uint32_t k0, k1, it;
+    // tallies: P_loss(3) and cnt_col over the x-regions (collisions.f90:533-543, 896-899, 1025-1033)
+    TallyDev *tal;
+    double Ek_half[LEPIC_MAXSP];      // 0.5 Nm m
+    int S, n_rg, iyl, iyr;
+    int ixl[LEPIC_MAXRG], ixr[LEPIC_MAXRG];
 };
+
+// the first x-region holding the cell (ix, iy) (collisions.f90:535-537), -1 if none
+__device__ __forceinline__ int region_of(const MccP &P, int ix, int iy) {
+    if (iy < P.iyl || iy > P.iyr) return -1;
+    for (int r = 0; r < P.n_rg; r++)
+        if (ix >= P.ixl[r] && ix <= P.ixr[r]) return r;
+    return -1;
+}
+
+__device__ __forceinline__ double v2f(float a, float b, float c) {
+    return (double)a * a + (double)b * b + (double)c * c;
+}
 
 struct Rng {
     U4 ctr;
@@ -100,6 +117,8 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     R.k0 = P.k0; R.k1 = P.k1; R.used = 4;
     const double vx1 = fvx, vy1 = P.VY[slot], vz1 = P.VZ[slot];
     const double mp = fabs(P.mass[sp]);
+    int rg = -1;
+    if (P.n_rg > 0) rg = region_of(P, (int)(P.X[slot] >> P.S) + 1, (int)(P.Y[slot] >> P.S) + 1);
     // per target species: drawn velocity and CM quantities (collision_OMP :336-482)
     double tvx[LEPIC_MAXSP], tvy[LEPIC_MAXSP], tvz[LEPIC_MAXSP], mu[LEPIC_MAXSP], vr[LEPIC_MAXSP];
     double vcx[LEPIC_MAXSP], vcy[LEPIC_MAXSP], vcz[LEPIC_MAXSP];
@@ -133,6 +152,10 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
         if (s < 0.0) continue;
         nu[q] = P.ndens[tt] * s * vr[tt] / P.nu_max; // :522-532
         sum_nu = sum_nu + nu[q];
+        if (rg >= 0) { // :535-543
+            atomicAdd(&P.tal->cnt_col[0][c][rg], nu[q] * P.nu_max);
+            atomicAdd(&P.tal->cnt_col[1][c][rg], 1.0);
+        }
     }
     // :619 indexx: reactions ordered by ascending nu (straight insertion, stable); the order
     // decides the outcome when sum(nu) > 1, i.e. when nu_max was capped (main.f90:494-495)
@@ -156,13 +179,17 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     const int n_re = ci[0], n_by = ci[1], rt = ci[2 + n_re + n_by];
     const int tt = ci[2 + n_re - 1];
     atomicAdd(&P.cnt->n_coll[c], 1ull);
+    if (rg >= 0) atomicAdd(&P.tal->cnt_col[2][c][rg], P.tal->inv_np_rg[sp][rg]); // :1026-1033
     const uint32_t X = P.X[slot], Y = P.Y[slot];
+    const double v2in = v2f(fvx, (float)vy1, (float)vz1);
     if (rt == 4) { // charge exchange :942-1000: the incident ion takes the neutral's velocity
         for (int ib = 0; ib < n_by; ib++) {
             int bt = ci[2 + n_re + ib];
             if (P.mass[bt] <= 0.0) continue;
             if (bt == sp) {
-                P.VX[slot] = (float)tvx[tt]; P.VY[slot] = (float)tvy[tt]; P.VZ[slot] = (float)tvz[tt];
+                const float a = (float)tvx[tt], b = (float)tvy[tt], cz = (float)tvz[tt];
+                P.VX[slot] = a; P.VY[slot] = b; P.VZ[slot] = cz;
+                atomicAdd(&P.tal->P3[sp], P.Ek_half[sp] * (v2f(a, b, cz) - v2in)); // :980-983
             }
         }
         return;
@@ -234,6 +261,8 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
             load_gauss(P.vt0[bt], R.next(), R.next(), P.pi, &z, &dummy);
             vbz = z;
         }
+        // P_loss(3) += 0.5 Nm m (v_new^2 - v_old^2), v_old = 0 for a created particle (:821-828, :896-899)
+        atomicAdd(&P.tal->P3[bt], P.Ek_half[bt] * (v2f((float)vbx, (float)vby, (float)vbz) - (to_incident ? v2in : 0.0)));
         if (to_incident) {
             incident_kept = true;
             P.VX[slot] = (float)vbx; P.VY[slot] = (float)vby; P.VZ[slot] = (float)vbz;
@@ -256,6 +285,7 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
         const int ct = ci[2 + ire];
         if (P.mass[ct] <= 0.0) continue;
         if (ct == sp && !incident_kept && ire == 0) {
+            atomicAdd(&P.tal->P3[sp], -P.Ek_half[sp] * v2in);  // removal in the mover (part_expmover.f90:91-95)
             P.VX[slot] = __int_as_float(0x7fc00000);
             atomicAdd(&P.cnt->n_dead[sp], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
@@ -311,8 +341,44 @@ __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long 
     }
 }
 
+// np_tot_rg (collisions.f90:143-154): the particles of a species in each x-region from the
+// density, k * sum of np over the region's nodes, k = dx dy zmax / Nm; one CTA per (species,
+// region), a fixed-order sum.  Stores 1 / np_tot_rg (0 for an empty region).
+__global__ void k_region_np(RhoParams R, int n_rg, int iyl, int iyr, const int *ixl, const int *ixr,
+                            const double *kfac, TallyDev *tal) {
+    __shared__ double red[256];
+    const int s = blockIdx.x / LEPIC_MAXRG, r = blockIdx.x % LEPIC_MAXRG;
+    if (r >= n_rg || s >= R.ntype) return;
+    const int w = ixr[r] - ixl[r] + 1, h = iyr - iyl + 1;
+    double acc = 0.0;
+    for (long long t = threadIdx.x; t < (long long)w * h; t += blockDim.x)
+        acc += np_val(R, s, ixl[r] + (int)(t % w), iyl + (int)(t / w));
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double np = kfac[s] * red[0];
+        tal->inv_np_rg[s][r] = np > 0.0 ? 1.0 / np : 0.0;
+    }
+}
+
 int mcc_collide(lepic_ctx *c, int it) {
     if (!c->has_xs) return LEPIC_OK;
+    if (c->n_rg > 0) {
+        RhoParams R = rho_params(c);
+        double kfac[LEPIC_MAXSP] = {0};
+        for (int s = 0; s < c->cfg.ntype; s++) kfac[s] = c->cfg.dx * c->cfg.dy * c->cfg.zmax / c->cfg.Nm[s];
+        LCUDA(cudaMemcpyAsync(c->rg_scratch, c->ixl_rg, sizeof(int) * LEPIC_MAXRG, cudaMemcpyHostToDevice, c->stream));
+        LCUDA(cudaMemcpyAsync(c->rg_scratch + LEPIC_MAXRG, c->ixr_rg, sizeof(int) * LEPIC_MAXRG, cudaMemcpyHostToDevice,
+                              c->stream));
+        LCUDA(cudaMemcpyAsync(c->rg_kfac, kfac, sizeof(double) * LEPIC_MAXSP, cudaMemcpyHostToDevice, c->stream));
+        k_region_np<<<LEPIC_MAXSP * LEPIC_MAXRG, 256, 0, c->stream>>>(R, c->n_rg, c->iyl_rg, c->iyr_rg, c->rg_scratch,
+                                                                     c->rg_scratch + LEPIC_MAXRG, c->rg_kfac, c->tally);
+        LCUDA(cudaGetLastError());
+    }
     const lepic_config &g = c->cfg;
     for (int s = 0; s < g.ntype; s++) {
         if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0) continue;
@@ -343,6 +409,11 @@ int mcc_collide(lepic_ctx *c, int it) {
         P.k0 = (uint32_t)g.seed;
         P.k1 = (uint32_t)(g.seed >> 32) ^ 0xA5A5F00Du;
         P.it = (uint32_t)it;
+        P.tal = c->tally;
+        for (int t = 0; t < g.ntype; t++) P.Ek_half[t] = 0.5 * g.Nm[t] * g.mass[t];
+        P.S = c->S;
+        P.n_rg = c->n_rg; P.iyl = c->iyl_rg; P.iyr = c->iyr_rg;
+        for (int r = 0; r < LEPIC_MAXRG; r++) { P.ixl[r] = c->ixl_rg[r]; P.ixr[r] = c->ixr_rg[r]; }
         k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
         LCUDA(cudaGetLastError());
     }

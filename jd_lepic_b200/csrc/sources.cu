@@ -1043,3 +1043,23 @@ int sources_after_push(lepic_ctx *c, int it) {
     }
     return LEPIC_OK;
 }
+
+// the sources' power tallies for lepic_gpu_get_tallies (zeros when no sources are set)
+int sources_power(lepic_ctx *c, double *P_heat, double *P_inj, double *P_src) {
+    SrcState *S = state(c);
+    if (!S) return LEPIC_OK;
+    SrcDev h;
+    LCUDA(cudaMemcpyAsync(&h, S->d, sizeof(SrcDev), cudaMemcpyDeviceToHost, c->stream));
+    LCUDA(cudaStreamSynchronize(c->stream));
+    *P_heat = h.P_heat;
+    for (int s = 0; s < LEPIC_MAXSP; s++) { P_inj[s] = h.P_inj[s]; P_src[s] = h.P_src[s]; }
+    return LEPIC_OK;
+}
+
+int sources_reset_power(lepic_ctx *c) {
+    SrcState *S = state(c);
+    if (!S) return LEPIC_OK;
+    LCUDA(cudaMemsetAsync(&S->d->P_heat, 0, sizeof(double), c->stream));
+    LCUDA(cudaMemsetAsync(S->d->P_inj, 0, sizeof(double) * 2 * LEPIC_MAXSP, c->stream));  // P_inj, P_src
+    return LEPIC_OK;
+}

@@ -136,9 +136,16 @@ void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
             flag_lost = 1;
         else if (c->charge[ptype] < 0 && c->mass[ptype] >= amu && xp < 0.0 && c->flag_nmn == 1)
             flag_lost = 3;
-        if (flag_lost >= 1) { /* :314 */
+        if (flag_lost >= 1) { /* :314-427 */
             np_lost++;
-            if (t) t->n_lost++;
+            if (t) {
+                t->n_lost++;
+                int igrid = flag_lost == 1 ? bcnd[NODE(ix, iy, nx)] : 0;
+                if (igrid < 0) igrid = 0;
+                if (igrid > 15) igrid = 15;
+                t->n_loss[igrid]++;
+                t->v2_loss[igrid] += vx * vx + vy * vy + vz * vz;
+            }
             continue;
         }
         if (c->flag_nmn == 1 && xp <= 0.0) { /* :454-459 specular reflection */

@@ -61,6 +61,10 @@ typedef struct {
 typedef struct {
     int64_t n_lost;       /* wall / boundary losses            */
     int64_t n_dead;       /* removed because flag_dead was set */
+    int64_t n_loss[16];   /* p_mac(ptype, np_loss, igrid), igrid = bcnd(ix,iy) of a wall
+                             loss (part_expmover.f90:338), 0 for the other losses; labels
+                             above 15 in the last                                   */
+    double v2_loss[16];   /* sum of the lost particles' v^2 per igrid (P_w / 0.5 Nm m) */
 } o_push_tally;
 
 typedef struct {

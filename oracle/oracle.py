@@ -59,7 +59,8 @@ class OXs(C.Structure):
 
 
 class OPushTally(C.Structure):
-    _fields_ = [("n_lost", C.c_int64), ("n_dead", C.c_int64)]
+    _fields_ = [("n_lost", C.c_int64), ("n_dead", C.c_int64), ("n_loss", C.c_int64 * 16),
+                ("v2_loss", C.c_double * 16)]
 
 
 class OMccTally(C.Structure):

@@ -62,3 +62,39 @@ def test_moments_back_step_and_bounds(oracle_lib):
     jx = pm[1]
     assert jx.sum() == pytest.approx(k1 * 2 * case.dx / case.dt * 1.0, rel=1e-12)
     assert jx[8, 10] == pytest.approx(k1 * 0.25 * 2 * case.dx / case.dt, rel=1e-12)
+
+
+def test_mover_loss_tallies_by_wall_label(oracle_lib):
+    """Particles thrown at the walls of the aperture-plate geometry (left wall label 3, plate
+    2, other walls 1): p_mac counts each loss under the label of its cell and its v^2."""
+    case = configs.case4(ppc=1, nx=64, ny=64)
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    sp = species_params(case, d)
+    cfg = O.make_cfg(case, sp)
+    cfg.flag_B = 0
+    b = np.ascontiguousarray(case.bcnd, dtype=np.int32)
+    i0 = int(round(0.8 * 64)) + 1          # plate's first node
+    v = []
+    ex = {1: 0, 2: 0, 3: 0}
+    v2 = {1: 0.0, 2: 0.0, 3: 0.0}
+    rng = np.random.default_rng(4)
+    for k in range(300):
+        y = (10.3 + rng.random() * 3) * case.dy
+        speed = (3.0 + 0.5 * rng.random()) * case.dx / case.dt   # lands inside the 4-cell plate
+        kind = k % 4
+        if kind == 0:   # into the left wall
+            p = (0.2 * case.dx, y, 0, -speed, 0, 0); ex[3] += 1; v2[3] += speed ** 2
+        elif kind == 1:  # into the plate's left face
+            p = ((i0 - 1.3) * case.dx, y, 0, speed, 0, 0); ex[2] += 1; v2[2] += speed ** 2
+        elif kind == 2:  # into the top wall
+            p = (20.4 * case.dx, 63.8 * case.dy, 0, 0, speed, 0); ex[1] += 1; v2[1] += speed ** 2
+        else:            # stays inside
+            p = (30.5 * case.dx, 30.5 * case.dy, 0, 0.1 * case.dx / case.dt, 0, 0)
+        v.append(p)
+    vxp = np.array(v, dtype=np.float64)
+    Ei = np.zeros((case.ny + 3, case.nx + 3, 2))
+    n, t = O.mover(cfg, 0, Ei, None, b, vxp)
+    assert n == 75 and t.n_lost == 225
+    for lab in (1, 2, 3):
+        assert t.n_loss[lab] == ex[lab]
+        assert t.v2_loss[lab] == pytest.approx(v2[lab], rel=1e-12)
