@@ -287,11 +287,27 @@ extern "C" int lepic_gpu_set_regions(lepic_ctx *c, int32_t n_rg, const double *x
     return LEPIC_OK;
 }
 
+// takes the loss holes not yet seen by a sort into the tallies and turns them into plain holes
+__global__ void k_loss_scan(const uint32_t *X, const uint32_t *Y, float *VX, const float *VY, const float *VZ,
+                            const int32_t *bcnd, TallyDev *tal, const DevCounters *cnt, int sp) {
+    const long long n = cnt->n_slots[sp];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float vx = VX[i];
+        if (isnan(vx) && loss_hole_tally(tal, sp, bcnd, vx, X[i], Y[i], VY[i], VZ[i])) VX[i] = __int_as_float(HOLE_NAN);
+    }
+}
+
 int sources_power(lepic_ctx *c, double *P_heat, double *P_inj, double *P_src);
 int sources_reset_power(lepic_ctx *c);
 
 extern "C" int lepic_gpu_get_tallies(lepic_ctx *c, lepic_tallies *out, int32_t reset) {
     if (!c || !out) return LEPIC_EINVAL;
+    for (int s = 0; s < c->cfg.ntype; s++) {
+        SpeciesBuf &B = c->sp[s];
+        k_loss_scan<<<c->num_sms * 8, 256, 0, c->stream>>>(B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur],
+                                                           c->bcnd, c->tally, c->dcnt, s);
+        LCUDA(cudaGetLastError());
+    }
     TallyDev *h = new (std::nothrow) TallyDev;
     if (!h) return LEPIC_ENOMEM;
     cudaError_t e = cudaMemcpyAsync(h, c->tally, sizeof(TallyDev), cudaMemcpyDeviceToHost, c->stream);

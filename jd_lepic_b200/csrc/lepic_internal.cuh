@@ -68,6 +68,26 @@ struct TallyDev {
     double inv_np_rg[LEPIC_MAXSP][LEPIC_MAXRG];       // 1/np_tot_rg of the current collision step
 };
 
+// A particle lost in the push leaves a hole that keeps its loss until the sort or a tally read
+// takes it (part_expmover.f90:314-427): VX = a NaN with payload LOSS_NAN_WALL (a wall loss,
+// igrid = bcnd of the loss cell) or LOSS_NAN_OTHER (igrid 0), X = the loss cell's node index,
+// Y = the bits of the new vx, VY, VZ = the new vy, vz.  Any other hole is the plain NaN.
+#define LOSS_NAN_WALL 0x7fc00001
+#define LOSS_NAN_OTHER 0x7fc00002
+#define HOLE_NAN 0x7fc00000
+
+// adds a fresh loss hole to p_mac (count and v^2 per label); returns true if it was one
+__device__ __forceinline__ bool loss_hole_tally(TallyDev *T, int sp, const int32_t *bcnd, float vx, uint32_t X,
+                                                uint32_t Y, float vy, float vz) {
+    const int bits = __float_as_int(vx);
+    if (bits != LOSS_NAN_WALL && bits != LOSS_NAN_OTHER) return false;
+    const int lab = bits == LOSS_NAN_WALL ? min(max(bcnd[X], 0), LEPIC_MAXLABEL - 1) : 0;
+    const float ux = __uint_as_float(Y);
+    atomicAdd(&T->n_loss[sp][lab], 1ull);
+    atomicAdd(&T->v2_loss[sp][lab], (double)ux * ux + (double)vy * vy + (double)vz * vz);
+    return true;
+}
+
 struct MGLevel {
     int nx, ny;
     double hx, hy;

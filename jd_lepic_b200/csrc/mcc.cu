@@ -286,7 +286,7 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
         if (P.mass[ct] <= 0.0) continue;
         if (ct == sp && !incident_kept && ire == 0) {
             atomicAdd(&P.tal->P3[sp], -P.Ek_half[sp] * v2in);  // removal in the mover (part_expmover.f90:91-95)
-            P.VX[slot] = __int_as_float(0x7fc00000);
+            P.VX[slot] = __int_as_float(HOLE_NAN);
             atomicAdd(&P.cnt->n_dead[sp], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
         }

@@ -30,9 +30,6 @@ struct PushP {
     float Bcx, Bcy, Bcz;
     float k2c;                 // the Boris factor of the constant field (BMODE 1)
     const uint8_t *cellwall;
-    const int32_t *bcnd;       // wall labels: the loss tallies' igrid
-    unsigned long long *loss_n;// p_mac(ptype, np_loss, 0:LEPIC_MAXLABEL-1) of this species
-    double *loss_v2;           // sum of v^2 of the lost particles, per label
     unsigned long long *acc;
     const WorkItem *items;
     DevCounters *cnt;
@@ -161,7 +158,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     if (!(fabsf(ux0) <= 3.0e8f && fabsf(uy0) <= 3.0e8f && fabsf(uz0) <= 3.0e8f)) {
         set_err(cnt, LERR_RANGE, 101);
         lost++;
-        vx = __int_as_float(0x7fc00000);
+        vx = __int_as_float(HOLE_NAN);
         return false;
     }
     // move (:216-217): integer part plus an unbiased stochastic rounding of the fractional part
@@ -209,13 +206,14 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     if (GEN && !is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
     if (is_lost) {
         lost++;
-        // p_mac(ptype, np_loss | P_w, igrid), igrid = bcnd(ix, iy) of a wall loss's cell (:338),
-        // 0 for the other losses (:399), larger labels in the last entry (:418-427)
+        // the slot becomes a hole that keeps its loss for the tallies (lepic_internal.cuh,
+        // loss_hole_tally): X = the loss cell's node, Y = the new vx, VY, VZ = the new vy, vz,
+        // VX = a NaN whose payload marks a fresh wall loss (1) or another loss (2)
         const bool wall = !GEN || P.cellwall[ixn + iyn * (P.nx + 2)] != 0;
-        const int lab = wall ? min(max(__ldg(P.bcnd + ixn + iyn * P.W), 0), LEPIC_MAXLABEL - 1) : 0;
-        atomicAdd(P.loss_n + lab, 1ull);
-        atomicAdd(P.loss_v2 + lab, (double)ux0 * ux0 + (double)uy0 * uy0 + (double)uz0 * uz0);
-        vx = __int_as_float(0x7fc00000); // the slot becomes a hole
+        X = (uint32_t)(ixn + iyn * P.W);
+        Y = __float_as_uint(ux0);
+        vy = uy0; vz = uz0;
+        vx = __int_as_float(wall ? LOSS_NAN_WALL : LOSS_NAN_OTHER);
         return false;
     }
     if (GEN && P.nmn && Xn <= 0) { Xn = -Xn; ux0 = -ux0; } // :454-459
@@ -394,9 +392,6 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
             P.k2c = k1f * (2.0f / (1.0f + k1f * k1f * Bt2));
         }
         P.cellwall = c->cellwall;
-        P.bcnd = c->bcnd;
-        P.loss_n = c->tally->n_loss[s];
-        P.loss_v2 = c->tally->v2_loss[s];
         P.acc = B.acc;
         P.items = B.items;
         P.cnt = c->dcnt;

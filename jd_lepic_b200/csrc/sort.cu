@@ -35,14 +35,21 @@ __device__ __forceinline__ int cell_key(const KeyP &K, uint32_t X, uint32_t Y) {
     return ((ty * K.ntx + tx) * K.th + ly) * K.tw + lx;
 }
 
-__global__ void k_keys_hist(KeyP K, const uint32_t *X, const uint32_t *Y, const float *VX,
-                            const DevCounters *cnt, int sp, int *keys, int *counts) {
+// the key pass also takes the loss holes of the pushes since the last sort into the tallies
+// (the sort drops the holes)
+__global__ void k_keys_hist(KeyP K, const uint32_t *X, const uint32_t *Y, const float *VX, const float *VY,
+                            const float *VZ, const int32_t *bcnd, TallyDev *tal, const DevCounters *cnt, int sp,
+                            int *keys, int *counts) {
     const long long n = cnt->n_slots[sp];
     const unsigned lane = threadIdx.x & 31;
     for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
         long long i = i0 + threadIdx.x;
         int key = -1;
-        if (i < n && !isnan(VX[i])) key = cell_key(K, X[i], Y[i]);
+        if (i < n) {
+            const float vx = VX[i];
+            if (!isnan(vx)) key = cell_key(K, X[i], Y[i]);
+            else loss_hole_tally(tal, sp, bcnd, vx, X[i], Y[i], VY[i], VZ[i]);
+        }
         if (i < n) keys[i] = key;
         unsigned m = __match_any_sync(0xffffffffu, key);
         if (key >= 0 && lane == (unsigned)(__ffs(m) - 1)) atomicAdd(&counts[key], __popc(m));
@@ -299,8 +306,8 @@ int sort_species(lepic_ctx *c, int sp) {
     int grid = c->num_sms * 8;
     LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
     LCUDA(cudaMemsetAsync(&c->dcnt->n_big, 0, sizeof(int), c->stream));
-    k_keys_hist<<<grid, SORT_THREADS, 0, c->stream>>>(K, B.X[cur], B.Y[cur], B.VX[cur], c->dcnt, sp,
-                                                        c->keys, c->counts);
+    k_keys_hist<<<grid, SORT_THREADS, 0, c->stream>>>(K, B.X[cur], B.Y[cur], B.VX[cur], B.VY[cur], B.VZ[cur],
+                                                        c->bcnd, c->tally, c->dcnt, sp, c->keys, c->counts);
     int nb = div_up(nk, SCAN_ITEMS);
     k_scan_blocks<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums);
     k_scan_top<<<1, 1024, 0, c->stream>>>(c->blocksums, nb);

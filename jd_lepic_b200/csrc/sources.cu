@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
         const long long slot = P.src->inj_start[s] + j;
         if (!ok) {  // a region with no room: the slot stays a hole and the call fails
             set_err(P.cnt, LERR_RANGE, 710 + s);
-            P.VX[s][slot] = __int_as_float(0x7fc00000);
+            P.VX[s][slot] = __int_as_float(HOLE_NAN);
             P.X[s][slot] = 0; P.Y[s][slot] = 0; P.VY[s][slot] = 0.f; P.VZ[s][slot] = 0.f;
             continue;
         }
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
                 set_err(P.cnt, LERR_CAPACITY, 720 + qe);
             } else if (xn < 0.0 || xn >= P.xmax || yn < 0.0 || yn >= P.ymax) {
                 // outside the box after the partial move: a wall loss of the next push
-                P.VX[qe][slot] = __int_as_float(0x7fc00000);
+                P.VX[qe][slot] = __int_as_float(HOLE_NAN);
                 P.X[qe][slot] = 0; P.Y[qe][slot] = 0; P.VY[qe][slot] = 0.f; P.VZ[qe][slot] = 0.f;
                 atomicAdd((unsigned long long *)&s_out[qe], 1ull);
             } else {
