@@ -379,6 +379,20 @@ int lepic_gpu_set_regions(lepic_ctx *ctx, int32_t n_rg, const double *xl_rg, con
  * afterwards (main.f90:1296-1300). */
 int lepic_gpu_get_tallies(lepic_ctx *ctx, lepic_tallies *out, int32_t reset);
 
+/* ---- particle backup (main.f90:1102-1139, restart.f90:48-149) ---------------------------
+ * The reference's particlesNNN.bak: Fortran unformatted sequential records (4-byte length
+ * markers; records over 2^31-9 bytes split into subrecords as the Intel and GNU runtimes do):
+ * (time, gtype, Pabs_cor), np_tot(1:ntype, 1:nproc), then vxp(6, np_tot) per iproc and ptype,
+ * FP64.  Written and read in chunks between the device and pinned host buffers. */
+/* Writes the live particles of every charged species (slot order, holes skipped; nproc = 1;
+ * z written as 0). */
+int lepic_gpu_write_backup(lepic_ctx *ctx, const char *path, double time, int32_t gtype, double Pabs_cor);
+/* Reads a backup written with any nproc (a species' blocks are appended in file order, as
+ * restart.f90:101-133 does for a different thread count) after the occupied slots, then
+ * deposits every species into np (restart_OMP).  time, gtype, Pabs_cor (nullable) receive the
+ * header.  LEPIC_ECAPACITY if the particles do not fit (restart.f90:117-121). */
+int lepic_gpu_read_backup(lepic_ctx *ctx, const char *path, double *time, int32_t *gtype, double *Pabs_cor);
+
 /* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
  * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network
  * (3x3 convolutions, channels 16/32/64/64, BF16 tensor-core convolutions with FP32

@@ -35,6 +35,7 @@ SOURCES = {
     "cnn.cu": [],
     "sources.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
+    "backup.cu": [],
 }
 
 

@@ -274,6 +274,17 @@ class GpuSimulation:
                 "vt": list(t.vt[:b]), "n_emit": list(t.n_emit[:n]), "n_emit_last": list(t.n_emit_last[:n]),
                 "n_emit_out": t.n_emit_out}
 
+    # particle backup (main.f90:1102-1139, restart.f90:48-149) ---------------------------
+    def write_backup(self, path: str, time: float = 0.0, gtype: int = 0, Pabs_cor: float = 1.0):
+        self.check(self.lib.lepic_gpu_write_backup(self.ctx, path.encode(), time, gtype, Pabs_cor), "write_backup")
+
+    def read_backup(self, path: str):
+        t, pc = C.c_double(), C.c_double()
+        gt = C.c_int32()
+        self.check(self.lib.lepic_gpu_read_backup(self.ctx, path.encode(), C.byref(t), C.byref(gt), C.byref(pc)),
+                   "read_backup")
+        return t.value, gt.value, pc.value
+
     def stream_ptr(self) -> int:
         return self.lib.lepic_gpu_stream(self.ctx) or 0
 

@@ -1,0 +1,87 @@
+"""The particle backup (particlesNNN.bak) written from and read into the device, against the
+record-format checker (oracle/fortran_records.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import fortran_records as FR
+from jd_lepic_b200 import _capi as capi, configs
+from jd_lepic_b200.simulation import GpuSimulation
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def small_subrecords(monkeypatch):
+    # 1000-byte subrecords: every particle record of these tests is split
+    monkeypatch.setenv("LEPIC_FORTRAN_MAX_SUBRECORD", "1000")
+
+
+def test_write_then_read_round_trip(gpu_lib, tmp_path, small_subrecords):
+    case = configs.case0(ppc=4, nx=64, ny=64)
+    a = GpuSimulation(case)
+    b = GpuSimulation(case, load=False)
+    try:
+        a.push(1)                                   # some particles are lost: holes are skipped
+        a.deposit()
+        path = str(tmp_path / "particles000.bak")
+        a.write_backup(path, 3.5e-7, 2, 0.875)
+        t, g, pc, np_tot, parts = FR.read_backup(path, 2)
+        assert (t, g, pc) == (3.5e-7, 2, 0.875) and np_tot.shape == (1, 2)
+        live = [a.get_particles(s) for s in (0, 1)]
+        assert np_tot[0].tolist() == [len(live[0]), len(live[1])] == a.push_stats()["np_tot"]
+        assert os.path.getsize(path) > 48 * len(live[0])
+        for s in (0, 1):
+            assert np.array_equal(parts[s][0], live[s])          # z is written as 0
+        t2 = b.read_backup(path)
+        assert t2 == (3.5e-7, 2, 0.875)
+        for s in (0, 1):
+            assert np.array_equal(b.get_particles(s), live[s])
+            assert np.array_equal(b.grid(capi.GRID_NP + s), a.grid(capi.GRID_NP + s))
+    finally:
+        a.close()
+        b.close()
+
+
+def test_read_file_of_two_threads(gpu_lib, tmp_path, small_subrecords):
+    case = configs.case0(ppc=4, nx=64, ny=64)
+    sim = GpuSimulation(case, load=False)
+    try:
+        rng = np.random.default_rng(2)
+
+        def block(n):
+            v = np.zeros((n, 6))
+            v[:, 0] = rng.random(n) * case.nx * case.dx * 0.999
+            v[:, 1] = rng.random(n) * case.ny * case.dy * 0.999
+            v[:, 2] = rng.random(n)
+            v[:, 3:] = rng.normal(0, 1e5, (n, 3)).astype(np.float32)
+            return v
+        blocks = [[block(300), block(50)], [block(200), block(0)]]
+        path = str(tmp_path / "p.bak")
+        FR.write_backup(path, 1.0, 7, 1.0, blocks, max_sub=1000)
+        sim.read_backup(path)
+        unit = case.dx * 2.0 ** -21
+        for s in (0, 1):
+            got = sim.get_particles(s)
+            ref = np.concatenate([blocks[0][s], blocks[1][s]])
+            assert len(got) == len(ref)
+            assert np.abs(got[:, :2] - ref[:, :2]).max() <= unit
+            assert np.array_equal(got[:, 3:], ref[:, 3:])
+    finally:
+        sim.close()
+
+
+def test_read_beyond_capacity(gpu_lib, tmp_path):
+    case = configs.case0(ppc=4, nx=64, ny=64)
+    sim = GpuSimulation(case, load=False, capacity=100)
+    try:
+        v = np.zeros((150, 6))
+        v[:, 0] = 1e-4
+        v[:, 1] = 1e-4
+        path = str(tmp_path / "big.bak")
+        FR.write_backup(path, 0.0, 0, 1.0, [[v, v[:10]]])
+        assert sim.lib.lepic_gpu_read_backup(sim.ctx, path.encode(), None, None, None) == capi.ECAPACITY
+        assert sim.push_stats()["np_tot"] == [0, 0]
+    finally:
+        sim.close()
