@@ -44,7 +44,7 @@ static void free_all(lepic_ctx *c) {
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
         for (int k = 0; k < 2; k++) { F(B.X[k]); F(B.Y[k]); F(B.VX[k]); F(B.VY[k]); F(B.VZ[k]); }
-        F(B.acc); F(B.items); F(B.prod);
+        F(B.acc); F(B.items); F(B.prod); F(B.cell_off); F(B.claim);
     }
     F(c->keys); F(c->perm); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
     for (int l = 0; l < c->nlev; l++) {
@@ -54,7 +54,7 @@ static void free_all(lepic_ctx *c) {
     F(c->partials);
     F(c->cg_r); F(c->cg_p); F(c->cg_ap);
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
-    F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac);
+    F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac); F(c->sigv_mx_d); F(c->nu_max_d);
     if (c->hcnt) cudaFreeHost(c->hcnt);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -238,6 +238,28 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
             }
             c->nu_max[s] = std::min(nu, g.nu_uplim[s]);
         }
+        for (int ic = 0; ic < xs->ncol && ic < LEPIC_MAXCOL; ic++) {
+            const int n_re = xs->col_info[ic * 10 + 0];
+            c->hcol_tt[ic] = xs->col_info[ic * 10 + 2 + n_re - 1];
+        }
+        // charged targets (DSMC): per-cell lists of the target species and a claim per slot
+        for (int s = 0; s < g.ntype; s++)
+            for (int q = 0; q < c->p_ncol[s]; q++) {
+                const int ic = c->hsig_list[s * LEPIC_MAXCOL + q];
+                const int n_re = xs->col_info[ic * 10 + 0];
+                const int tt = xs->col_info[ic * 10 + 2 + n_re - 1];
+                if (tt < g.ntype && g.charge[tt] != 0.0 && g.mass[s] > 0.0) {
+                    c->dsmc = true;
+                    SpeciesBuf &T = c->sp[tt];
+                    if (!T.cell_off) LALLOC(T.cell_off, c->nkeys + 1);
+                    if (!T.claim) LALLOC(T.claim, T.cap);
+                }
+            }
+        LALLOC(c->sigv_mx_d, LEPIC_MAXSP * LEPIC_MAXCOL);
+        LALLOC(c->nu_max_d, LEPIC_MAXSP);
+        LCUDA(cudaMemcpy(c->sigv_mx_d, xs->sigv_mx, sizeof(double) * LEPIC_MAXSP * LEPIC_MAXCOL, cudaMemcpyHostToDevice));
+        for (int s = 0; s < LEPIC_MAXSP; s++)
+            if (c->sp[s].cell_off) LCUDA(cudaMemset(c->sp[s].cell_off, 0, sizeof(int) * (c->nkeys + 1)));
         c->flag_ionrep = xs->flag_ionrep;
         c->fEk = xs->fEk;
         int pmax = 1;

@@ -100,6 +100,8 @@ struct MGLevel {
 };
 
 struct SpeciesBuf {
+    int *cell_off = nullptr;   // per-key start offsets of the last sort (DSMC target lists)
+    int *claim = nullptr;      // DSMC: the incident slot that holds each target slot
     uint32_t *X[2], *Y[2];
     float *VX[2], *VY[2], *VZ[2];
     int cur;
@@ -145,6 +147,10 @@ struct lepic_ctx {
     double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;  // finest-level CG vectors
     // collisions
     bool has_xs = false;
+    bool dsmc = false;             // a reaction has a charged target (collisions.f90:339-418)
+    double *sigv_mx_d = nullptr;   // [ptype*LEPIC_MAXCOL + icol]
+    double *nu_max_d = nullptr;    // per species, formed on the device each collision step
+    int hcol_tt[LEPIC_MAXCOL] = {0};  // target species of each reaction
     int npt = 0, ncol = 0;
     double *sig_Er = nullptr, *sig = nullptr, *Eth = nullptr;
     int *col_info = nullptr;
@@ -282,6 +288,15 @@ __device__ void bitonic_sort(T *a, int n, int rank, int size, Sync sync) {
             sync();
         }
     }
+}
+
+// the sort key of cell (cx, cy): tile-major, then row-major inside the tile (sort.cu)
+__device__ __forceinline__ int sort_cell_key(int cx, int cy, int nx, int ny, int tw, int th, int ntx) {
+    cx = min(max(cx, 0), nx - 1);
+    cy = min(max(cy, 0), ny - 1);
+    const int tx = cx / tw, ty = cy / th;
+    const int lx = cx - tx * tw, ly = cy - ty * th;
+    return ((ty * ntx + tx) * th + ly) * tw + lx;
 }
 
 struct WarpSync { __device__ void operator()() const { __syncwarp(); } };

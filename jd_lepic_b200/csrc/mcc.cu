@@ -50,7 +50,38 @@ struct MccP {
     double Ek_half[LEPIC_MAXSP];      // 0.5 Nm m
     int S, n_rg, iyl, iyr;
     int ixl[LEPIC_MAXRG], ixr[LEPIC_MAXRG];
+    // DSMC with charged targets (collisions.f90:339-418, 524-528): the targets' cell lists of
+    // the last sort, their velocities, the claims and the dens_red densities
+    int dsmc, nx, ny, tw, th, ntx, W;
+    long long nn;
+    const int *toff[LEPIC_MAXSP];
+    float *TVX[LEPIC_MAXSP], *TVY[LEPIC_MAXSP], *TVZ[LEPIC_MAXSP];
+    int *claim[LEPIC_MAXSP];
+    const double *np_red;
+    const double *nu_max_d;   // the device's nu_max of this step (DSMC), else nu_max above
+    double ns_coll_dt;
 };
+
+#define TAG_DSMC 0x44534D43u
+
+// collisions.f90:339-403: a target of species tt for an incident in cell (cx, cy), uniform in
+// the incident's cell, else in the first non-empty of its x+1, x-1, y+1, y-1 neighbours (inside
+// the grid); -1 if none.  u: the draw (slot, step, TAG_DSMC ^ tt).
+__device__ __forceinline__ long long pick_target(const MccP &P, int tt, int cx, int cy, uint32_t u) {
+    const int ddx[5] = {0, 1, -1, 0, 0}, ddy[5] = {0, 0, 0, 1, -1};
+    for (int k = 0; k < 5; k++) {
+        const int x = cx + ddx[k], y = cy + ddy[k];
+        if (x < 0 || x >= P.nx || y < 0 || y >= P.ny) continue;
+        const int key = sort_cell_key(x, y, P.nx, P.ny, P.tw, P.th, P.ntx);
+        const long long a = P.toff[tt][key], b = P.toff[tt][key + 1];
+        if (b > a) return a + (long long)(u01(u) * (double)(b - a));
+    }
+    return -1;
+}
+
+__device__ __forceinline__ uint32_t dsmc_draw(const MccP &P, long long slot, int tt) {
+    return philox4x32_10(U4{(uint32_t)slot, P.it, TAG_DSMC ^ (uint32_t)tt, (uint32_t)P.sp}, P.k0, P.k1).x;
+}
 
 // the first x-region holding the cell (ix, iy) (collisions.f90:535-537), -1 if none
 __device__ __forceinline__ int region_of(const MccP &P, int ix, int iy) {
@@ -107,7 +138,7 @@ __device__ __forceinline__ double sigma_at(const MccP &P, int c, double E) {
     return sL + (E - EL) * (sR - sL) / (ER - EL);
 }
 
-__device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_local) {
+__device__ void collide_one(const MccP &P, long long slot, double nu_max, unsigned int *n_cand_local) {
     float fvx = P.VX[slot];
     if (isnan(fvx)) return;
     (*n_cand_local)++;
@@ -122,7 +153,13 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     // per target species: drawn velocity and CM quantities (collision_OMP :336-482)
     double tvx[LEPIC_MAXSP], tvy[LEPIC_MAXSP], tvz[LEPIC_MAXSP], mu[LEPIC_MAXSP], vr[LEPIC_MAXSP];
     double vcx[LEPIC_MAXSP], vcy[LEPIC_MAXSP], vcz[LEPIC_MAXSP];
+    long long tslot[LEPIC_MAXSP];   // the DSMC target of a charged target species (-1: none)
+    double np_t[LEPIC_MAXSP];
+#pragma unroll
+    for (int t = 0; t < LEPIC_MAXSP; t++) tslot[t] = -1;
     unsigned drawn = 0;
+    int cx = 0, cy = 0;
+    if (P.dsmc) { cx = (int)(P.X[slot] >> P.S); cy = (int)(P.Y[slot] >> P.S); }
     double nu[MCC_MAX_REACTIONS];
     double sum_nu = 0.0;
     for (int q = 0; q < P.ncol_sp; q++) {
@@ -131,11 +168,26 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
         const int n_re = ci[0];
         const int tt = ci[2 + n_re - 1];
         nu[q] = 0.0;
-        if (P.charge[tt] != 0.0) continue; // charged targets (DSMC) are not handled here
+        const bool charged = P.charge[tt] != 0.0;
+        if (charged && (!P.dsmc || tt == sp)) continue; // like-particle DSMC is not handled
         if (!(drawn & (1u << tt))) {
             double a, b, z, dummy;
-            load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &a, &b);
-            load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &z, &dummy);
+            if (!charged) {
+                load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &a, &b);
+                load_gauss(P.vt0[tt], R.next(), R.next(), P.pi, &z, &dummy);
+                tslot[tt] = -1;
+                np_t[tt] = P.ndens[tt];
+            } else {
+                // the target particle (:339-403) if this candidate holds its claim, and the
+                // target density at the incident's cell (:524-528)
+                long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
+                if (t >= 0 && (P.claim[tt][t] != (int)slot || isnan(P.TVX[tt][t]))) t = -1;
+                tslot[tt] = t;
+                a = b = z = 0.0;
+                if (t >= 0) { a = P.TVX[tt][t]; b = P.TVY[tt][t]; z = P.TVZ[tt][t]; }
+                const long long m = (cx + 1) + (long long)(cy + 1) * P.W + tt * P.nn;
+                np_t[tt] = 0.25 * (P.np_red[m] + P.np_red[m + 1] + P.np_red[m + P.W] + P.np_red[m + P.W + 1]);
+            }
             tvx[tt] = a; tvy[tt] = b; tvz[tt] = z;
             const double mt = fabs(P.mass[tt]);
             mu[tt] = mp * mt / (mp + mt);
@@ -146,14 +198,15 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
             vcz[tt] = (mp * vz1 + mt * z) / sm;
             drawn |= 1u << tt;
         }
+        if (charged && tslot[tt] < 0) continue;  // no target for this species (:389-398)
         const double Ekr = (0.5 * mu[tt] * (vr[tt] * vr[tt])) / P.qe;
         if (Ekr > P.sig_Er[P.npt - 1]) atomicAdd(&P.cnt->n_overflow, 1ull);
         const double s = sigma_at(P, c, Ekr);
         if (s < 0.0) continue;
-        nu[q] = P.ndens[tt] * s * vr[tt] / P.nu_max; // :522-532
+        nu[q] = np_t[tt] * s * vr[tt] / nu_max; // :522-532
         sum_nu = sum_nu + nu[q];
         if (rg >= 0) { // :535-543
-            atomicAdd(&P.tal->cnt_col[0][c][rg], nu[q] * P.nu_max);
+            atomicAdd(&P.tal->cnt_col[0][c][rg], nu[q] * nu_max);
             atomicAdd(&P.tal->cnt_col[1][c][rg], 1.0);
         }
     }
@@ -190,6 +243,12 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
                 const float a = (float)tvx[tt], b = (float)tvy[tt], cz = (float)tvz[tt];
                 P.VX[slot] = a; P.VY[slot] = b; P.VZ[slot] = cz;
                 atomicAdd(&P.tal->P3[sp], P.Ek_half[sp] * (v2f(a, b, cz) - v2in)); // :980-983
+            } else if (bt == tt && P.charge[tt] != 0.0 && tslot[tt] >= 0) {
+                // a charged target takes the incident's velocity (:955-978)
+                const long long t = tslot[tt];
+                const double v2t = v2f(P.TVX[tt][t], P.TVY[tt][t], P.TVZ[tt][t]);
+                P.TVX[tt][t] = fvx; P.TVY[tt][t] = (float)vy1; P.TVZ[tt][t] = (float)vz1;
+                atomicAdd(&P.tal->P3[tt], P.Ek_half[tt] * (v2in - v2t));
             }
         }
         return;
@@ -231,11 +290,12 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
     for (int ib = 0; ib < n_by; ib++) { // :767-902
         const int bt = ci[2 + n_re + ib];
         if (P.mass[bt] <= 0.0) continue;
-        bool to_incident = false;
+        bool to_incident = false, to_target = false;
         if (ib == 0 && bt == sp) to_incident = true;
         if (rt == 1 || rt == 3) {
             if (bt == sp) to_incident = true;
-            else continue; // a charged target's update (DSMC) is not handled here
+            else if (bt == tt && P.charge[tt] != 0.0 && tslot[tt] >= 0) to_target = true;  // :794-797
+            else continue;
         }
         double vbx = 0.0, vby = 0.0, vbz = 0.0;
         if (opt_scat == 1) {
@@ -260,6 +320,13 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
             load_gauss(P.vt0[bt], R.next(), R.next(), P.pi, &vbx, &vby);
             load_gauss(P.vt0[bt], R.next(), R.next(), P.pi, &z, &dummy);
             vbz = z;
+        }
+        if (to_target) {
+            const long long t = tslot[tt];
+            const double v2t = v2f(P.TVX[tt][t], P.TVY[tt][t], P.TVZ[tt][t]);
+            atomicAdd(&P.tal->P3[tt], P.Ek_half[tt] * (v2f((float)vbx, (float)vby, (float)vbz) - v2t));
+            P.TVX[tt][t] = (float)vbx; P.TVY[tt][t] = (float)vby; P.TVZ[tt][t] = (float)vbz;
+            continue;
         }
         // P_loss(3) += 0.5 Nm m (v_new^2 - v_old^2), v_old = 0 for a created particle (:821-828, :896-899)
         atomicAdd(&P.tal->P3[bt], P.Ek_half[bt] * (v2f((float)vbx, (float)vby, (float)vbz) - (to_incident ? v2in : 0.0)));
@@ -290,11 +357,23 @@ __device__ void collide_one(const MccP &P, long long slot, unsigned int *n_cand_
             atomicAdd(&P.cnt->n_dead[sp], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
         }
+        if (ire == 1 && ct == tt && P.charge[tt] != 0.0 && tslot[tt] >= 0 && rt != 1 && rt != 3) {
+            const long long t = tslot[tt];  // a charged target that is not a byproduct dies (:921-930)
+            atomicAdd(&P.tal->P3[tt], -P.Ek_half[tt] * v2f(P.TVX[tt][t], P.TVY[tt][t], P.TVZ[tt][t]));
+            P.TVX[tt][t] = __int_as_float(HOLE_NAN);
+            atomicAdd(&P.cnt->n_dead[tt], 1ull);
+            atomicAdd((unsigned long long *)&P.cnt->n_alive[tt], (unsigned long long)-1ll);
+        }
     }
 }
 
+// the collision probability of this step: the host's (neutral targets) or the device's
+// nu_max (charged targets: it depends on the densities, collisions.f90:98-117)
+__device__ __forceinline__ double step_nu_max(const MccP &P) { return P.dsmc ? P.nu_max_d[P.sp] : P.nu_max; }
+
 __global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P) {
     const long long n = P.cnt->n_slots[P.sp];
+    const double nu_max = step_nu_max(P), Pmax = P.dsmc ? nu_max * P.ns_coll_dt : P.Pmax;
     unsigned int ncand = 0;
     const long long stride = (long long)gridDim.x * blockDim.x * 4;
     for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * 4; base < n; base += stride) {
@@ -303,11 +382,62 @@ __global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             long long slot = base + q;
-            if (slot < n && u01(v[q]) < P.Pmax) collide_one(P, slot, &ncand);
+            if (slot < n && u01(v[q]) < Pmax) collide_one(P, slot, nu_max, &ncand);
         }
     }
     for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(0xffffffffu, ncand, o);
     if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&P.cnt->n_cand[P.sp], (unsigned long long)ncand);
+}
+
+// DSMC claims: every candidate of this step picks its charged targets as collide_one will and
+// claims them with the smallest incident slot, so that a target takes part in one collision
+// of the step (the winner is independent of the order the threads run in).
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc_claim(MccP P) {
+    const long long n = P.cnt->n_slots[P.sp];
+    const double Pmax = step_nu_max(P) * P.ns_coll_dt;
+    const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * 4; base < n; base += stride) {
+        U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
+        uint32_t v[4] = {r.x, r.y, r.z, r.w};
+        for (int q = 0; q < 4; q++) {
+            const long long slot = base + q;
+            if (slot >= n || !(u01(v[q]) < Pmax) || isnan(P.VX[slot])) continue;
+            const int cx = (int)(P.X[slot] >> P.S), cy = (int)(P.Y[slot] >> P.S);
+            unsigned done = 0;
+            for (int k = 0; k < P.ncol_sp; k++) {
+                const int *ci = P.col_info + P.cols[k] * 10;
+                const int tt = ci[2 + ci[0] - 1];
+                if (P.charge[tt] == 0.0 || tt == P.sp || (done & (1u << tt))) continue;
+                done |= 1u << tt;
+                const long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
+                if (t >= 0) atomicMin(P.claim[tt] + t, (int)slot);
+            }
+        }
+    }
+}
+
+// nu_max of every species from the densities of this step (collisions.f90:98-123)
+struct NuMaxP {
+    int ntype, p_ncol[LEPIC_MAXSP];
+    int cols[LEPIC_MAXSP][MCC_MAX_REACTIONS], tt[LEPIC_MAXSP][MCC_MAX_REACTIONS];
+    double np_mx_neutral[LEPIC_MAXSP], charge[LEPIC_MAXSP], nu_uplim[LEPIC_MAXSP], ns_coll_dt;
+    const double *sigv_mx, *np_mx_charged;
+    double *nu_max;
+    DevCounters *cnt;
+};
+__global__ void k_nu_max(NuMaxP P) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int s = 0; s < P.ntype; s++) {
+        double nu = 0.0;
+        for (int q = 0; q < P.p_ncol[s]; q++) {
+            const int t = P.tt[s][q];
+            const double n = P.charge[t] != 0.0 ? P.np_mx_charged[t] : P.np_mx_neutral[t];
+            nu = nu + n * P.sigv_mx[s * LEPIC_MAXCOL + P.cols[s][q]];
+        }
+        nu = fmin(nu, P.nu_uplim[s]);
+        P.nu_max[s] = nu;
+        if (nu * P.ns_coll_dt > 1.0) set_err(P.cnt, LERR_RANGE, 210);  // :119-123
+    }
 }
 
 // Ordered append of one species' products after its occupied slots (single CTA).
@@ -380,13 +510,40 @@ int mcc_collide(lepic_ctx *c, int it) {
         LCUDA(cudaGetLastError());
     }
     const lepic_config &g = c->cfg;
-    for (int s = 0; s < g.ntype; s++) {
-        if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0) continue;
-        double Pmax = c->nu_max[s] * (double)g.ns_coll * g.dt;
-        if (Pmax > 1.0) { c->last_err = "collision probability Pmax > 1"; return LEPIC_ERANGE; }
+    if (!c->dsmc) {
+        for (int s = 0; s < g.ntype; s++) {
+            if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0) continue;
+            double Pmax = c->nu_max[s] * (double)g.ns_coll * g.dt;
+            if (Pmax > 1.0) { c->last_err = "collision probability Pmax > 1"; return LEPIC_ERANGE; }
+        }
+    } else {
+        // charged targets: dens_red (main.f90:970) for the densities and their maxima, then
+        // nu_max on the device (collisions.f90:98-123)
+        int r = field_dens_red(c);
+        if (r != LEPIC_OK) return r;
+        NuMaxP N;
+        memset(&N, 0, sizeof(N));
+        N.ntype = g.ntype;
+        for (int s = 0; s < g.ntype; s++) {
+            N.p_ncol[s] = g.mass[s] > 0.0 ? c->p_ncol[s] : 0;
+            for (int q = 0; q < c->p_ncol[s]; q++) {
+                const int ic = c->hsig_list[s * LEPIC_MAXCOL + q];
+                N.cols[s][q] = ic;
+                N.tt[s][q] = c->hcol_tt[ic];
+            }
+            N.nu_uplim[s] = g.nu_uplim[s];
+        }
+        for (int t = 0; t < g.nsp; t++) { N.np_mx_neutral[t] = g.np_mx[t]; N.charge[t] = g.charge[t]; }
+        N.ns_coll_dt = (double)g.ns_coll * g.dt;
+        N.sigv_mx = c->sigv_mx_d;
+        N.np_mx_charged = c->np_mx;
+        N.nu_max = c->nu_max_d;
+        N.cnt = c->dcnt;
+        k_nu_max<<<1, 32, 0, c->stream>>>(N);
+        LCUDA(cudaGetLastError());
     }
     for (int s = 0; s < g.ntype; s++) {
-        if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0 || c->nu_max[s] <= 0.0) continue;
+        if (c->p_ncol[s] == 0 || g.mass[s] <= 0.0 || (!c->dsmc && c->nu_max[s] <= 0.0)) continue;
         SpeciesBuf &B = c->sp[s];
         MccP P;
         memset(&P, 0, sizeof(P));
@@ -414,6 +571,31 @@ int mcc_collide(lepic_ctx *c, int it) {
         P.S = c->S;
         P.n_rg = c->n_rg; P.iyl = c->iyl_rg; P.iyr = c->iyr_rg;
         for (int r = 0; r < LEPIC_MAXRG; r++) { P.ixl[r] = c->ixl_rg[r]; P.ixr[r] = c->ixr_rg[r]; }
+        if (c->dsmc) {
+            P.dsmc = 1;
+            P.nx = g.nx; P.ny = g.ny; P.tw = c->tw; P.th = c->th; P.ntx = c->ntx; P.W = g.nx + 3; P.nn = c->nn;
+            for (int t = 0; t < g.ntype; t++) {
+                SpeciesBuf &T = c->sp[t];
+                P.toff[t] = T.cell_off;
+                P.TVX[t] = T.VX[T.cur]; P.TVY[t] = T.VY[T.cur]; P.TVZ[t] = T.VZ[T.cur];
+                P.claim[t] = T.claim;
+            }
+            P.np_red = c->np_red;
+            P.nu_max_d = c->nu_max_d;
+            P.ns_coll_dt = (double)g.ns_coll * g.dt;
+            bool any = false;
+            for (int q = 0; q < c->p_ncol[s]; q++) {
+                const int t = c->hcol_tt[c->hsig_list[s * LEPIC_MAXCOL + q]];
+                if (t < g.ntype && g.charge[t] != 0.0 && t != s && c->sp[t].claim) {
+                    LCUDA(cudaMemsetAsync(c->sp[t].claim, 0x7f, sizeof(int) * c->sp[t].cap, c->stream));
+                    any = true;
+                }
+            }
+            if (any) {
+                k_mcc_claim<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
+                LCUDA(cudaGetLastError());
+            }
+        }
         k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
         LCUDA(cudaGetLastError());
     }

@@ -27,12 +27,7 @@ struct KeyP {
     int S, nx, ny, tw, th, ntx;
 };
 __device__ __forceinline__ int cell_key(const KeyP &K, uint32_t X, uint32_t Y) {
-    int cx = (int)(X >> K.S), cy = (int)(Y >> K.S);
-    cx = min(max(cx, 0), K.nx - 1);
-    cy = min(max(cy, 0), K.ny - 1);
-    int tx = cx / K.tw, ty = cy / K.th;
-    int lx = cx - tx * K.tw, ly = cy - ty * K.th;
-    return ((ty * K.ntx + tx) * K.th + ly) * K.tw + lx;
+    return sort_cell_key((int)(X >> K.S), (int)(Y >> K.S), K.nx, K.ny, K.tw, K.th, K.ntx);
 }
 
 // the key pass also takes the loss holes of the pushes since the last sort into the tallies
@@ -322,6 +317,9 @@ int sort_species(lepic_ctx *c, int sp) {
     k_items<<<1, 1024, 0, c->stream>>>(c->offsets, c->ntiles, c->tw * c->th, B.items, B.max_items,
                                        c->dcnt, sp, nk);
     LCUDA(cudaGetLastError());
+    // the cell lists of this order (sorting.f90's Plist) for the DSMC target search
+    if (B.cell_off)
+        LCUDA(cudaMemcpyAsync(B.cell_off, c->offsets, sizeof(int) * (nk + 1), cudaMemcpyDeviceToDevice, c->stream));
     B.cur = nxt;
     return LEPIC_OK;
 }

@@ -276,6 +276,20 @@ def argon_deck(ion_temp: float = 0.03, gas_temp_k: float = 300.0) -> str:
     return write_deck("[Ar+]", 39.95, ion_temp, "[Ar]", kT, reac)
 
 
+def argon_dsmc_deck(sigma: float = 2.0e-15, e_cut: float = 20.0, ion_temp: float = 0.03,
+                    gas_temp_k: float = 300.0, with_neutral: bool = False) -> str:
+    """Electron-ion elastic scattering on the ions themselves (a charged target, collisions by
+    DSMC; the first reaction of the reference's argon set), sigma constant up to e_cut eV and
+    zero above; optionally with the e-Ar elastic reaction on the background gas."""
+    E = energy_grid()
+    sig = np.where(np.asarray(E) <= e_cut, sigma, 0.0)
+    reac = [("[e]+[Ar+]->[e]+[Ar+]", "COLLISION", 0.0, E, sig)]
+    if with_neutral:
+        reac.append(("[e]+[Ar]->[e]+[Ar]", "COLLISION", 0.0, E, sigma_constant(E, 1.0e-19)))
+    kT = KB * gas_temp_k / QE
+    return write_deck("[Ar+]", 39.95, ion_temp, "[Ar]", kT, reac)
+
+
 def helium_deck(ion_temp: float = 0.03, gas_temp_k: float = 300.0) -> str:
     """Synthetic helium set: e-He elastic 6e-20 m^2; excitation 19.8 eV (peak 2e-21 m^2 at
     40 eV); ionization 24.6 eV (Lotz, peak 3.5e-21 m^2); He+-He charge exchange 3e-19 m^2."""
