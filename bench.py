@@ -52,9 +52,10 @@ def profiled_traffic_per_particle():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms from before the warm-up
+    (nvidia-smi takes a moment to start) and kept for the timed region only (its timestamps)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -62,6 +63,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -69,25 +71,45 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t = time.time()
+        while time.time() - t < 10.0 and os.path.getsize(self.path) == 0:   # first sample written
+            time.sleep(0.05)
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def stop(self) -> dict:
+        import datetime
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
         self.proc.terminate()
         self.proc.wait(timeout=10)
-        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.count(",") >= 8]
+        rows = [[f.strip() for f in l.split(",")] for l in open(self.path).read().strip().splitlines()
+                if l.count(",") >= 9]
         os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+
+        def stamp(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return None
+        inside = [r for r in rows if stamp(r) is not None and self.t0 is not None and self.t0 <= stamp(r) <= self.t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in inside if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        reasons = sorted({names[k] for r in inside for k in range(4) if "Active" in r[6 + k] and "Not" not in r[6 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(inside)}
 
 
 # ------------------------------------------------------------------------------------------
@@ -189,7 +211,8 @@ def run_reference(args):
     nt = host_threads()
     sample = args.cpu_sample
     t0 = time.perf_counter()
-    cb = cpu_baseline(case, sample, args.steps, args.warmup, nt)
+    # each step is a bounded sample; at most 20 timed steps keep the run within minutes
+    cb = cpu_baseline(case, sample, min(args.steps, 20), min(args.warmup, 3), nt)
     wall = time.perf_counter() - t0
     line = {"metric": "particle-steps/s per PIC step (push+deposit+MCC+sort+Poisson to 1e-8)",
             "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -425,17 +448,18 @@ def run_ours(args):
         rec("allreduce", reduce_rho) if world > 1 else None
 
     # cold solve to a converged phi, then warm-up steps
+    clocks = ClockSampler(local)
+    clocks.start()
     it = 1
     for _ in range(args.warmup):
         one_step(it, False)
         it += 1
     sim.sync()
     n_start = sum(sim.push_stats()["np_tot"])
-    clocks = ClockSampler(local)
-    clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    clocks.mark_start()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
@@ -445,6 +469,7 @@ def run_ours(args):
         it += 1
     t_end.record(stream)
     torch.cuda.synchronize()
+    clocks.mark_end()
     sim.sync()
     if world > 1:
         dist.barrier()
@@ -581,7 +606,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=4)
