@@ -557,7 +557,7 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
     return team_sum(B, s1, l1);
 }
 
-// z = e (FP32 cycle output): returns r.z; if first, p = z else p = z + beta p (beta passed)
+// z = e (FP32 cycle output): returns r.z
 __device__ bool dot_rz(const BigTeam &B, const MXP &P, double *rz) {
     const MXL &L = P.L[0];
     const int nn = (L.nx + 3) * (L.ny + 3);
@@ -567,32 +567,34 @@ __device__ bool dot_rz(const BigTeam &B, const MXP &P, double *rz) {
     return team_sum(B, a, rz);
 }
 
-__device__ void update_p(const BigTeam &B, const MXP &P, double beta, bool first) {
-    const MXL &L = P.L[0];
-    const int nn = (L.nx + 3) * (L.ny + 3);
-    for (int t = (int)B.rank(); t < nn; t += (int)B.size()) {
-        double z = L.bc[t] <= 0 ? (double)L.e[t] : 0.0;
-        P.p64[t] = first ? z : z + beta * P.p64[t];
-    }
-}
-
-// Ap = A p at unknowns (p is zero on walls and ghosts); returns p.Ap
-__device__ bool apply_A(const BigTeam &B, const MXP &P, double *pap) {
+// p = z + beta p and q = A p in one pass: A p_new = A z + beta A p_old, so q = A z + beta q
+// needs z's neighbours but not p's, and no barrier separates the p update from the stencil
+// (z = e at unknowns, 0 on walls and ghosts; p and q are 0 on walls).  Returns p.q.
+__device__ bool update_pq(const BigTeam &B, const MXP &P, double beta, bool first, double *pq) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
     double a = 0.0;
     for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
         const int n = (w.k + 1) + (w.j + 1) * W;
-        double v = 0.0;
-        if (L.bc[n] <= 0) {
-            const double *p = P.p64;
-            v = aw * p[n - 1] + an * p[n + W] + an * p[n - W] + aw * p[n + 1] + ac * p[n];
-            a += p[n] * v;
+        if (L.bc[n] > 0) {
+            P.p64[n] = 0.0;
+            P.ap64[n] = 0.0;
+            continue;
         }
-        P.ap64[n] = v;
+        const int8_t *bc = L.bc;
+        const float *e = L.e;
+        const double z = (double)e[n];
+        const double zw = bc[n - 1] <= 0 ? (double)e[n - 1] : 0.0, ze = bc[n + 1] <= 0 ? (double)e[n + 1] : 0.0;
+        const double zs = bc[n - W] <= 0 ? (double)e[n - W] : 0.0, zn = bc[n + W] <= 0 ? (double)e[n + W] : 0.0;
+        const double Az = aw * zw + an * zn + an * zs + aw * ze + ac * z;
+        const double p = first ? z : z + beta * P.p64[n];
+        const double q = first ? Az : Az + beta * P.ap64[n];
+        P.p64[n] = p;
+        P.ap64[n] = q;
+        a += p * q;
     }
-    return team_sum(B, a, pap);
+    return team_sum(B, a, pq);
 }
 
 // u += alpha p; r -= alpha Ap; r32 = r; e = 0; returns ||r||^2 over bcnd == -1 nodes
@@ -650,11 +652,9 @@ __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
         if (!vcycle32(P)) return;            // z = M^-1 r in L[0].e
         double rz_new;
         if (!dot_rz(B, P, &rz_new)) return;
-        update_p(B, P, first ? 0.0 : rz_new / rz, first);
+        if (!update_pq(B, P, first ? 0.0 : rz_new / rz, first, &pap)) return;
         rz = rz_new;
         first = false;
-        if (!B.sync()) return;
-        if (!apply_A(B, P, &pap)) return;
         // A (eps0 * Laplacian, diagonal -4a) and the V-cycle are both negative definite, so
         // r.z and p.Ap are both negative and the step length is positive
         const double alpha = rz / pap;
