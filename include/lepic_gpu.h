@@ -159,6 +159,15 @@ int lepic_gpu_put_particles(lepic_ctx *ctx, int32_t ptype, const double *vxp, in
  * with z = 0.  The backup writer main.f90:1102-1139 reads this. */
 int lepic_gpu_get_particles(lepic_ctx *ctx, int32_t ptype, double *vxp, int64_t cap,
                             int64_t *n_out);
+/* The same with the reference's own particle array vxp(6, nmax, ntype, nproc) and
+ * np_tot(ntype, nproc) (main.f90:192-214): put concatenates a species' slabs in slab order
+ * (replacing its particles); get deals a species' live particles to the nproc slabs in equal
+ * parts in slot order, as sorting.f90:92-251 rebalances them (LEPIC_ECAPACITY if a slab would
+ * exceed nmax). */
+int lepic_gpu_put_particles_slabs(lepic_ctx *ctx, const double *vxp, const int32_t *np_tot, int64_t nmax,
+                                  int32_t ntype, int32_t nproc);
+int lepic_gpu_get_particles_slabs(lepic_ctx *ctx, double *vxp, int32_t *np_tot, int64_t nmax, int32_t ntype,
+                                  int32_t nproc);
 /* Synthetic initial load on the device (see lepic_load_spec). */
 int lepic_gpu_load_particles(lepic_ctx *ctx, const lepic_load_spec *spec);
 

@@ -192,6 +192,8 @@ PROTOTYPES = {
     "lepic_gpu_put_particles": (C.c_int, [_VP, C.c_int32, _DP, C.c_int64]),
     "lepic_gpu_get_particles": (C.c_int, [_VP, C.c_int32, _DP, C.c_int64, C.POINTER(C.c_int64)]),
     "lepic_gpu_load_particles": (C.c_int, [_VP, C.POINTER(LepicLoadSpec)]),
+    "lepic_gpu_put_particles_slabs": (C.c_int, [_VP, _DP, _IP, C.c_int64, C.c_int32, C.c_int32]),
+    "lepic_gpu_get_particles_slabs": (C.c_int, [_VP, _DP, _IP, C.c_int64, C.c_int32, C.c_int32]),
     "lepic_gpu_charge_deposition": (C.c_int, [_VP]),
     "lepic_gpu_calc_rhs": (C.c_int, [_VP, _DP]),
     "lepic_gpu_dens_red": (C.c_int, [_VP, _DP, _DP]),

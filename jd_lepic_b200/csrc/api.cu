@@ -494,6 +494,57 @@ extern "C" int lepic_gpu_put_particles(lepic_ctx *c, int32_t ptype, const double
     if (!c || ptype < 0 || ptype >= c->cfg.ntype || (n > 0 && !vxp)) return LEPIC_EINVAL;
     return particles_put(c, ptype, vxp, n);
 }
+// The reference's own particle array vxp(6, nmax, ntype, nproc) with np_tot(ntype, nproc): a
+// species' slabs are concatenated in slab order on the way in; on the way out its live
+// particles are dealt to the nproc slabs in equal parts, in slot order, as sorting.f90:92-251
+// rebalances them.
+extern "C" int lepic_gpu_put_particles_slabs(lepic_ctx *c, const double *vxp, const int32_t *np_tot, int64_t nmax,
+                                             int32_t ntype, int32_t nproc) {
+    if (!c || !vxp || !np_tot || nmax < 0 || ntype != c->cfg.ntype || nproc < 1) return LEPIC_EINVAL;
+    for (int s = 0; s < ntype; s++) {
+        long long n = 0;
+        for (int p = 0; p < nproc; p++) {
+            const int32_t k = np_tot[s + (long long)ntype * p];
+            if (k < 0 || k > nmax) { c->last_err = "np_tot outside 0..nmax"; return LEPIC_EINVAL; }
+            n += k;
+        }
+        std::vector<double> buf((size_t)6 * n);
+        long long o = 0;
+        for (int p = 0; p < nproc; p++) {
+            const int32_t k = np_tot[s + (long long)ntype * p];
+            const double *src = vxp + 6 * nmax * ((long long)s + (long long)ntype * p);
+            std::memcpy(buf.data() + 6 * o, src, sizeof(double) * 6 * (size_t)k);
+            o += k;
+        }
+        int r = particles_put(c, s, buf.data(), n);
+        if (r != LEPIC_OK) return r;
+    }
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_get_particles_slabs(lepic_ctx *c, double *vxp, int32_t *np_tot, int64_t nmax,
+                                             int32_t ntype, int32_t nproc) {
+    if (!c || !vxp || !np_tot || nmax < 0 || ntype != c->cfg.ntype || nproc < 1) return LEPIC_EINVAL;
+    for (int s = 0; s < ntype; s++) {
+        long long n = 0;
+        int r = particles_get(c, s, nullptr, 0, &n);
+        if (r != LEPIC_OK) return r;
+        if ((n + nproc - 1) / nproc > nmax) { c->last_err = "a slab would exceed nmax"; return LEPIC_ECAPACITY; }
+        std::vector<double> buf((size_t)6 * std::max(n, 1ll));
+        r = particles_get(c, s, buf.data(), n, &n);
+        if (r != LEPIC_OK) return r;
+        long long o = 0;
+        for (int p = 0; p < nproc; p++) {
+            const long long k = n / nproc + (p < n % nproc ? 1 : 0);
+            double *dst = vxp + 6 * nmax * ((long long)s + (long long)ntype * p);
+            std::memcpy(dst, buf.data() + 6 * o, sizeof(double) * 6 * (size_t)k);
+            np_tot[s + (long long)ntype * p] = (int32_t)k;
+            o += k;
+        }
+    }
+    return LEPIC_OK;
+}
+
 extern "C" int lepic_gpu_get_particles(lepic_ctx *c, int32_t ptype, double *vxp, int64_t cap, int64_t *n_out) {
     if (!c || ptype < 0 || ptype >= c->cfg.ntype) return LEPIC_EINVAL;
     long long n = 0;

@@ -85,3 +85,41 @@ def test_read_beyond_capacity(gpu_lib, tmp_path):
         assert sim.push_stats()["np_tot"] == [0, 0]
     finally:
         sim.close()
+
+
+def test_slab_layout_put_get(gpu_lib):
+    """vxp(6, nmax, ntype, nproc) with np_tot(ntype, nproc), the reference's own arrays."""
+    import ctypes as C
+    case = configs.case0(ppc=4, nx=64, ny=64)
+    sim = GpuSimulation(case, load=False)
+    try:
+        rng = np.random.default_rng(3)
+        nmax, ntype, nproc = 500, 2, 3
+        vxp = np.zeros((nproc, ntype, nmax, 6))          # Fortran vxp(6, nmax, ntype, nproc)
+        np_tot = np.zeros((nproc, ntype), dtype=np.int32)  # Fortran np_tot(ntype, nproc)
+        for p in range(nproc):
+            for s in range(ntype):
+                k = int(rng.integers(0, nmax))
+                np_tot[p, s] = k
+                u = np.zeros((k, 6))
+                # positions on the fixed-point grid, FP32 velocities: the round trip is exact
+                u[:, 0] = np.floor(rng.random(k) * case.nx * 2 ** 21) * case.dx * 2.0 ** -21
+                u[:, 1] = np.floor(rng.random(k) * case.ny * 2 ** 21) * case.dy * 2.0 ** -21
+                u[:, 3:] = rng.normal(0, 1e5, (k, 3)).astype(np.float32)
+                vxp[p, s, :k] = u
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        sim.check(sim.lib.lepic_gpu_put_particles_slabs(sim.ctx, dp(vxp), ip(np_tot), nmax, ntype, nproc), "put_slabs")
+        for s in range(ntype):
+            ref = np.concatenate([vxp[p, s, :np_tot[p, s]] for p in range(nproc)])
+            assert np.array_equal(sim.get_particles(s), ref)
+        out = np.zeros_like(vxp)
+        nt = np.zeros_like(np_tot)
+        sim.check(sim.lib.lepic_gpu_get_particles_slabs(sim.ctx, dp(out), ip(nt), nmax, ntype, nproc), "get_slabs")
+        for s in range(ntype):
+            total = np_tot[:, s].sum()
+            assert nt[:, s].sum() == total and nt[:, s].max() - nt[:, s].min() <= 1
+            got = np.concatenate([out[p, s, :nt[p, s]] for p in range(nproc)])
+            assert np.array_equal(got, np.concatenate([vxp[p, s, :np_tot[p, s]] for p in range(nproc)]))
+    finally:
+        sim.close()
