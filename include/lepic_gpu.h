@@ -276,8 +276,9 @@ typedef struct lepic_source_config {
     /* part_injection */
     int32_t flag_inj;          /* I_inj >= 0 in the deck                                   */
     int32_t ns_inj;            /* injection every ns_inj steps (MOD(it,ns_inj) == 0)       */
-    int32_t opt_inj;           /* +-1: fixed current; +-2: a pair per lost positive ion;
-                                  < 0: Gaussian loading.  +-3 / +-4 are not supported.     */
+    int32_t opt_inj;           /* +-1: fixed current; +-2: a pair per lost positive ion; +-3:
+                                  electron beam along z; +-4: emission from the cathode at
+                                  x = 0 with a shifted-Maxwellian flux; < 0: Gaussian loading */
     int32_t flag_Tp;           /* 1: electrons injected at THm (|opt_inj| <= 2)            */
     int32_t flag_diffsrc;      /* 1: tally -Nm q phi at each injected particle (P_loss(1)) */
     int32_t tag_neg;           /* 0-based negative-ion species, -1 if none                 */
@@ -297,6 +298,7 @@ typedef struct lepic_source_config {
                                   to the cell as generate_boundary.f90:267-270 does)       */
     int32_t flag_chmfrd;       /* chamfered aperture (generate_boundary.f90:110-116)       */
     double chmfrd[4];          /* chmfrd_array: x1, x2, (ymax/2 - y1), (ymax/2 - y2) [m]   */
+    double th_B;               /* angle of B to the x axis for opt_inj = 4 (main.f90:450-452) */
 } lepic_source_config;
 
 /* Cumulative tallies since the context was created or last reset; the reference's names. */

@@ -153,7 +153,7 @@ class LepicSourceConfig(C.Structure):
         ("I_inj", C.c_double), ("THm", C.c_double), ("ni0", C.c_double * MAXSP), ("seed", C.c_uint64),
         ("js", C.c_double), ("ptype_fx", C.c_int32), ("tag_b", C.c_int32), ("ns_Hm", C.c_int32),
         ("n_holes", C.c_int32), ("xg1", C.c_double), ("Lg", C.c_double), ("Lh", C.c_double),
-        ("flag_chmfrd", C.c_int32), ("chmfrd", C.c_double * 4),
+        ("flag_chmfrd", C.c_int32), ("chmfrd", C.c_double * 4), ("th_B", C.c_double),
     ]
 
 

@@ -54,6 +54,10 @@ class Case:
     ng: int = 0
     zmax: float = 1.0
     seed: int = 1
+    # boundary options (read_input.f90): periodic y, specular y walls with it, Neumann at x = 0
+    flag_pbc: int = 0
+    flag_spec: int = 0
+    flag_nmn: int = 0
     extra: dict = field(default_factory=dict)
 
     @property

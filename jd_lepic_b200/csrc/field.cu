@@ -91,12 +91,14 @@ __global__ void k_efield_interior(int nx, int ny, double h1, double h2, const do
         }
     }
 }
-// Pass 2, Neumann column (:52-63) and periodic rows (:68-82), one thread per row/column.
+// Pass 2, periodic rows (:68-82) when part == 0, then the Neumann column (:52-63) when
+// part == 1; one thread per column / row.  The reference visits row 1 first, so its periodic
+// copies read column 1 before the Neumann step zeroes Ex there: two launches keep that order.
 __global__ void k_efield_nmn_pbc(int nx, int ny, double h2, const double *phi, const int8_t *bc,
-                                 double2 *E) {
+                                 double2 *E, int part) {
     const int W = nx + 3;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 1 && t <= ny + 1) { // Neumann: any node of row iy with bcnd == -2
+    if (part == 1 && t >= 1 && t <= ny + 1) { // Neumann: any node of row iy with bcnd == -2
         int iy = t;
         for (int ix = 1; ix <= nx + 1; ix++) {
             if (bc[ix + iy * W] != -2) continue;
@@ -105,7 +107,7 @@ __global__ void k_efield_nmn_pbc(int nx, int ny, double h2, const double *phi, c
                 E[1 + iy * W].y = -(phi[1 + (iy + 1) * W] - phi[1 + (iy - 1) * W]) / (2.0 * h2);
         }
     }
-    if (t >= 1 && t <= nx + 1) { // periodic: node (ix, 1)
+    if (part == 0 && t >= 1 && t <= nx + 1) { // periodic: node (ix, 1)
         int ix = t;
         int b = bc[ix + 1 * W];
         if (b == 0 || b == -2) {
@@ -154,9 +156,10 @@ int field_calc_efield(lepic_ctx *c) {
     // E (FP64) lives in Ed[0..nn); the second half is the wall-pass output.
     double2 *E0 = c->Ed, *E1 = c->Ed + c->nn;
     k_efield_interior<<<grid, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, E0);
-    if (c->cfg.flag_pbc || c->cfg.flag_nmn)
-        k_efield_nmn_pbc<<<div_up(std::max(nx, ny) + 2, 256), 256, 0, c->stream>>>(nx, ny, c->cfg.dy,
-                                                                                   c->phi, c->bc8, E0);
+    if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the passes test the labels, as Efield.f90:43-82 does
+        for (int part = 0; part < 2; part++)
+            k_efield_nmn_pbc<<<div_up(std::max(nx, ny) + 2, 256), 256, 0, c->stream>>>(nx, ny, c->cfg.dy,
+                                                                                       c->phi, c->bc8, E0, part);
     int grid2 = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
     k_efield_walls<<<grid2, 256, 0, c->stream>>>(nx, ny, c->bc8, E0, E1, c->Ef);
     LCUDA(cudaGetLastError());

@@ -35,6 +35,8 @@
 #define TAG_INJN 0x494E4A4Eu    // injection count rounding
 #define TAG_INJP 0x494E4A50u    // injection position attempt
 #define TAG_INJV 0x494E4A56u    // injection velocity
+#define TAG_INJF 0x494E4A46u    // opt_inj = 4: shifted-flux attempt
+#define TAG_INJG 0x494E4A47u    // opt_inj = 4: transverse velocity and time offset
 #define TAG_FXN 0x46584E31u     // emission count rounding
 #define TAG_FXP 0x46585031u     // emission attempt position
 #define TAG_FXV 0x46585631u     // emission velocity and time offset
@@ -359,7 +361,7 @@ __global__ void k_te_update(SrcDev *src, int n_icp, int type, double nu_h, doubl
 struct InjPlanP {
     DevCounters *cnt;
     SrcDev *src;
-    int ntype, opt2, tag_neg;
+    int ntype, opt2, tag_neg, electrons_only;
     long long cap[LEPIC_MAXSP];
     double dN_fixed[LEPIC_MAXSP];  // |opt_inj| = 1: I_inj ns_inj dt ni0 / (qe Nm(1)) / nproc_mpi
     double ni0[LEPIC_MAXSP];
@@ -389,6 +391,7 @@ __global__ void k_inj_plan(InjPlanP P) {
             const U4 r = philox4x32_10(U4{(uint32_t)s, 0u, TAG_INJN, P.it}, P.k0, P.k1);
             if (u01(r.x) <= dN - (double)N) N += 1;
         }
+        if (P.electrons_only && s > 0) N = 0;  // part_injection.f90:77-79
         const long long start = P.cnt->n_slots[s];
         if (start + N > P.cap[s]) {  // part_injection.f90:146-150
             set_err(P.cnt, LERR_CAPACITY, 700 + s);
@@ -409,6 +412,8 @@ struct InjP {
     DevCounters *cnt;
     int ntype, nx, ny, S, W;
     int opt, slit, flag_nmn, diffsrc;
+    double vb[LEPIC_MAXSP], fmax[LEPIC_MAXSP];   // |opt_inj| = 3, 4: beam speed, flux maximum
+    double sin_thB, cos_thB, ns_dt;
     Region R;
     double dx, dy, xmax, ymax;
     double vt[LEPIC_MAXSP], Ek[LEPIC_MAXSP], qphi[LEPIC_MAXSP];  // qphi = -Nm q
@@ -489,16 +494,49 @@ __global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
         // call takes (vx, vy) and vz from the second pair (so vz = vx), the next takes its own
         // (vx, vy) and the saved second component of the previous particle's second pair
         const double vt = P.vt[s];
-        const U4 q = philox4x32_10(U4{(uint32_t)j, (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
         double vx, vy, vz;
-        if ((j & 1) == 0) {
-            gauss_pair(vt, q.z, q.w, &vx, &vy);
-            vz = vx;
+        if (P.opt == 4 || P.opt == -4) {
+            // part_injection.f90:161-178: vx from the shifted-Maxwellian flux about vb cos(th_B)
+            // (acceptance-rejection, :239-265), (vy, vz) Maxwellian with vy += vb sin(th_B), and
+            // the particle moved off the cathode at x = 0 by vx times a random part of ns_inj dt
+            const double vbt = P.vb[s] * P.cos_thB;
+            const double vm = fmax(0.0, vbt - 4.0 * vt), vpm = vbt + 4.0 * vt;
+            bool got = false;
+            vx = vy = vz = 0.0;
+            for (uint32_t a = 0; a < INJ_MAX_ATTEMPTS && !got; a++) {
+                const U4 f = philox4x32_10(U4{(uint32_t)j, (a << 3) | (uint32_t)s, TAG_INJF, P.it}, P.k0, P.k1);
+                const double v = vm + u01(f.x) * (vpm - vm);
+                const double fv = v * exp(-(v - vbt) * (v - vbt) / (vt * vt));
+                if (u01(f.y) > fv / P.fmax[s]) continue;
+                gauss_pair(vt, f.z, f.w, &vy, &vz);
+                const U4 g2 = philox4x32_10(U4{(uint32_t)j, (a << 3) | (uint32_t)s, TAG_INJG, P.it}, P.k0, P.k1);
+                const double xn = v * (u01(g2.x) * P.ns_dt);
+                if (xn < 0.0 || xn > P.xmax) continue;
+                vx = v;
+                vy = vy + P.vb[s] * P.sin_thB;
+                x = xn;
+                got = true;
+            }
+            if (!got) {
+                set_err(P.cnt, LERR_RANGE, 720 + s);
+                P.VX[s][slot] = __int_as_float(HOLE_NAN);
+                P.X[s][slot] = 0; P.Y[s][slot] = 0; P.VY[s][slot] = 0.f; P.VZ[s][slot] = 0.f;
+                continue;
+            }
+            ix = (int)floor(x / P.dx) + 1;
+            ix = ix < 1 ? 1 : (ix > P.nx + 1 ? P.nx + 1 : ix);
         } else {
-            gauss_pair(vt, q.x, q.y, &vx, &vy);
-            const U4 qp = philox4x32_10(U4{(uint32_t)(j - 1), (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
-            double unused;
-            gauss_pair(vt, qp.z, qp.w, &unused, &vz);
+            const U4 q = philox4x32_10(U4{(uint32_t)j, (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
+            if ((j & 1) == 0) {
+                gauss_pair(vt, q.z, q.w, &vx, &vy);
+                vz = vx;
+            } else {
+                gauss_pair(vt, q.x, q.y, &vx, &vy);
+                const U4 qp = philox4x32_10(U4{(uint32_t)(j - 1), (uint32_t)s, TAG_INJV, P.it}, P.k0, P.k1);
+                double unused;
+                gauss_pair(vt, qp.z, qp.w, &unused, &vz);
+            }
+            if (P.opt == 3 || P.opt == -3) vz = vz + P.vb[s];  // :202 beam along z
         }
         // fixed point: x/h truncated, so the cell is the reference's INT(x/h)
         const double fx = x / P.dx * (double)(1u << P.S), fy = y / P.dy * (double)(1u << P.S);
@@ -749,7 +787,13 @@ static int check_config(lepic_ctx *c, const lepic_source_config &s) {
     if (s.flag_inj) {
         if (s.ns_inj < 1) return bad("ns_inj < 1");
         const int a = std::abs(s.opt_inj);
-        if (a != 1 && a != 2) return bad("opt_inj must be +-1 or +-2 (beam and cathode options are not built)");
+        if (a < 1 || a > 4) return bad("opt_inj must be +-1 .. +-4");
+        if (a >= 3 && !(s.THm >= 0.0)) return bad("THm < 0");
+        if (a == 4) {
+            if (!std::isfinite(s.th_B)) return bad("th_B is not finite");
+            for (int sp = 0; sp < g.ntype; sp++)
+                if (!(g.vt0[sp] > 0.0)) return bad("opt_inj 4 needs vt0 > 0 (init_shifted_maxwellian_flux)");
+        }
         if (s.nproc_mpi < 1) return bad("nproc_mpi < 1");
         if (s.tag_neg < -1 || s.tag_neg >= g.ntype || s.tag_neg == 0) return bad("tag_neg out of range");
         if (s.I_inj < 0.0) return bad("I_inj < 0");
@@ -864,6 +908,7 @@ static int run_injection(lepic_ctx *c, int it) {
     Q.cnt = c->dcnt; Q.src = S->d; Q.ntype = g.ntype;
     Q.opt2 = std::abs(s.opt_inj) == 2;
     Q.tag_neg = s.tag_neg;
+    Q.electrons_only = std::abs(s.opt_inj) == 3 || (std::abs(s.opt_inj) == 4 && g.flag_nmn == 0);
     for (int sp = 0; sp < g.ntype; sp++) {
         Q.cap[sp] = c->sp[sp].cap;
         Q.ni0[sp] = s.ni0[sp];
@@ -881,10 +926,21 @@ static int run_injection(lepic_ctx *c, int it) {
     P.opt = s.opt_inj; P.flag_nmn = g.flag_nmn; P.diffsrc = s.flag_diffsrc;
     P.R = make_region(s, g, c->S);
     P.dx = g.dx; P.dy = g.dy; P.xmax = g.nx * g.dx; P.ymax = g.ny * g.dy;
+    P.sin_thB = std::sin(s.th_B); P.cos_thB = std::cos(s.th_B);
+    P.ns_dt = (double)s.ns_inj * g.dt;
     for (int sp = 0; sp < g.ntype; sp++) {
         double vt = g.vt0[sp];
         if (std::abs(s.opt_inj) <= 2 && s.flag_Tp == 1 && sp == 0) vt = std::sqrt(2.0 * g.qe * s.THm / std::fabs(g.mass[0]));
         P.vt[sp] = vt;
+        // part_injection.f90:34-47 and init_shifted_maxwellian_flux (:267-290)
+        if (std::abs(s.opt_inj) == 3 || std::abs(s.opt_inj) == 4) {
+            double vb = std::sqrt(2.0 * g.qe * s.THm / std::fabs(g.mass[sp]));
+            if (std::abs(s.opt_inj) == 4 && sp == 0 && g.flag_nmn == 1) vb = 0.0;  // half-Maxwellian flux
+            P.vb[sp] = vb;
+            const double v0 = g.vt0[sp];
+            const double vmax = (vb + std::sqrt(vb * vb + 2.0 * v0 * v0)) / 2.0;
+            P.fmax[sp] = vmax * std::exp(-(vmax - vb) * (vmax - vb) / (v0 * v0));
+        }
         P.Ek[sp] = 0.5 * g.Nm[sp] * g.mass[sp];
         P.qphi[sp] = -g.Nm[sp] * g.charge[sp];
         SpeciesBuf &B = c->sp[sp];

@@ -94,7 +94,7 @@ class GpuSimulation:
         cfg.nx, cfg.ny = case.nx, case.ny
         cfg.dx, cfg.dy, cfg.zmax, cfg.dt = case.dx, case.dy, case.zmax, case.dt
         cfg.eps0, cfg.qe = dk.EPS0, dk.QE
-        cfg.flag_pbc = cfg.flag_spec = cfg.flag_nmn = 0
+        cfg.flag_pbc, cfg.flag_spec, cfg.flag_nmn = case.flag_pbc, case.flag_spec, case.flag_nmn
         cfg.flag_B = case.flag_B
         cfg.flag_B_pos = 0
         for k in range(3):

@@ -22,7 +22,8 @@ class SourceDeck:
     Pabs: tuple = (0.0,)                            # absorbed power per driver [W] (<= 0: fixed Te)
     nu_h: float = -1.0                              # heating frequency [1/s] (< 0: off)
     I_inj: float = -1.0                             # injected current [A] (< 0: off)
-    opt_inj: int = 1                                # 1 fixed current, 2 pair per lost ion, < 0 Gaussian
+    opt_inj: int = 1                                # 1 fixed current, 2 pair per lost ion, 3 beam along z,
+                                                    # 4 cathode emission at x = 0; < 0 Gaussian
     THm: float = 0.0                                # [eV]; < 0 sets flag_Tp
     ns_heat: int = 4
     ns_inj: int = 1
@@ -42,6 +43,15 @@ class SourceDeck:
     Lh_cm: float = 0.0
     n_holes: int = 0
     chamfer_m: tuple = ()                           # chmfrd_array (x1, x2, ymax/2-y1, ymax/2-y2) [m]
+    th_B: float = 0.0                               # |opt_inj| = 4: angle of B to the x axis [rad]
+
+
+def cathode_angle(opt_inj: int, flag_nmn: int, Bx11: float, By11: float) -> float:
+    """th_B of main.f90:450-452: atan(By/Bx) of the field at node (1, 1) when the cathode
+    option runs with the Neumann boundary and Bx is not zero, else 0."""
+    if opt_inj == 4 and flag_nmn == 1 and abs(Bx11) > 0.0:
+        return math.atan(By11 / Bx11)
+    return 0.0
 
 
 def source_config(d: SourceDeck, dt: float, vt0_e: float, dy: float = 0.0) -> capi.LepicSourceConfig:
@@ -90,6 +100,7 @@ def source_config(d: SourceDeck, dt: float, vt0_e: float, dy: float = 0.0) -> ca
     c.xg1, c.Lg = d.xg1_cm * 1e-2, d.Lg_cm * 1e-2
     Lh = d.Lh_cm * 1e-2
     c.Lh = math.floor(Lh / dy) * dy if dy > 0.0 else Lh
+    c.th_B = d.th_B if abs(d.opt_inj) == 4 else 0.0
     if d.chamfer_m:
         c.flag_chmfrd = 1
         for k in range(4):

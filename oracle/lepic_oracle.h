@@ -162,6 +162,7 @@ typedef struct {
     int opt_inj, flag_Tp, flag_diffsrc, tag_neg, nproc_mpi, ns_inj;
     double I_inj, THm;
     double ni0[O_MAXSP];
+    double th_B;                /* opt_inj = 4: angle of B to the x axis (main.f90:450-452) */
 } o_src;
 
 /* Philox4x32-10 (Salmon et al., SC'11) and the device's (0,1) mapping (v + 0.5) 2^-32 */

@@ -78,7 +78,7 @@ class OSrc(C.Structure):
         ("nudt", C.c_double), ("Pabs_cor", C.c_double),
         ("opt_inj", C.c_int), ("flag_Tp", C.c_int), ("flag_diffsrc", C.c_int), ("tag_neg", C.c_int),
         ("nproc_mpi", C.c_int), ("ns_inj", C.c_int), ("I_inj", C.c_double), ("THm", C.c_double),
-        ("ni0", C.c_double * MAXSP),
+        ("ni0", C.c_double * MAXSP), ("th_B", C.c_double),
     ]
 
 
@@ -182,7 +182,7 @@ def make_cfg(case, sp) -> OCfg:
     c.xmax, c.ymax = case.nx * case.dx, case.ny * case.dy
     c.dt = case.dt
     c.eps0, c.qe, c.pi = dk.EPS0, dk.QE, 4.0 * math.atan(1.0)
-    c.flag_pbc = c.flag_spec = c.flag_nmn = 0
+    c.flag_pbc, c.flag_spec, c.flag_nmn = case.flag_pbc, case.flag_spec, case.flag_nmn
     c.flag_B = case.flag_B
     c.flag_B_pos = 0
     for k in range(3):
@@ -222,6 +222,12 @@ def mover(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, flag_dead=None):
 
 def deposit(cfg, ptype, vxp, n, kq, npg):
     lib().o_charge_deposition(C.byref(cfg), ptype, dp(vxp), n, dp(kq), dp(npg))
+
+
+def np_periodic(cfg, npg, bcnd):
+    """calc_rho.f90:1-35 on npg (ntype, ny+3, nx+3) in place."""
+    assert npg.flags.c_contiguous and npg.shape[0] >= cfg.ntype
+    lib().o_np_periodic(C.byref(cfg), dp(npg), ip(np.ascontiguousarray(bcnd, dtype=np.int32)))
 
 
 def calc_rhs(cfg, npg):
@@ -414,7 +420,7 @@ def make_src(sc) -> OSrc:
     """o_src from a lepic_source_config (ctypes structure of the product's C ABI)."""
     o = OSrc()
     for f in ("flag_c", "xl_pow", "xr_pow", "yl_pow", "yr_pow", "eheat_type", "flag_gpp", "n_icp", "nudt",
-              "Pabs_cor", "opt_inj", "flag_Tp", "flag_diffsrc", "tag_neg", "nproc_mpi", "ns_inj", "I_inj", "THm"):
+              "Pabs_cor", "opt_inj", "flag_Tp", "flag_diffsrc", "tag_neg", "nproc_mpi", "ns_inj", "I_inj", "THm", "th_B"):
         setattr(o, f, getattr(sc, f))
     for s in range(MAXSP):
         o.ni0[s] = sc.ni0[s]

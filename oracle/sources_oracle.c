@@ -2,7 +2,7 @@
  * sources_oracle.c -- CPU FP64 restatement of the reference's particle sources:
  * eheating (e_heating.f90:1-112), the heating-region tallies of charge_deposition
  * (part_expmover.f90:583-605), the temperature update (main.f90:1003-1010) and
- * part_injection (part_injection.f90:1-237, options |opt_inj| = 1, 2).
+ * part_injection (part_injection.f90:1-290, options |opt_inj| = 1 .. 4).
  *
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path (see lepic_oracle.h).
  * Parity against the reference's own outputs is unpinned (no Fortran compiler here, and
@@ -19,6 +19,8 @@
 #define TAG_INJN 0x494E4A4Eu
 #define TAG_INJP 0x494E4A50u
 #define TAG_INJV 0x494E4A56u
+#define TAG_INJF 0x494E4A46u
+#define TAG_INJG 0x494E4A47u
 #define MAX_ATTEMPTS 65536u
 
 /* Philox4x32-10: ten rounds of two 32x32->64 multiplies, Weyl key schedule */
@@ -181,6 +183,37 @@ static double inj_vt(const o_cfg *c, const o_src *s, int ptype) {
     return vt;
 }
 
+/* the beam speed and the flux maximum of part_injection.f90:34-47 and
+ * init_shifted_maxwellian_flux (part_injection.f90:267-290) */
+static void inj_beam(const o_cfg *c, const o_src *s, int ptype, double *vb, double *fmax) {
+    *vb = 0.0;
+    *fmax = 0.0;
+    const int a = abs(s->opt_inj);
+    if (a != 3 && a != 4) return;
+    *vb = sqrt(2.0 * c->qe * s->THm / fabs(c->mass[ptype]));
+    if (a == 4 && ptype == 0 && c->flag_nmn == 1) *vb = 0.0;
+    const double v0 = c->vt0[ptype];
+    const double vmax = (*vb + sqrt(*vb * *vb + 2.0 * v0 * v0)) / 2.0;
+    *fmax = vmax * exp(-(vmax - *vb) * (vmax - *vb) / (v0 * v0));
+}
+
+/* part_injection.f90:77-79: no ions under the beam, nor under cathode emission without the
+ * divertor option */
+static int inj_electrons_only(const o_cfg *c, const o_src *s) {
+    return abs(s->opt_inj) == 3 || (abs(s->opt_inj) == 4 && c->flag_nmn == 0);
+}
+
+/* shifted_maxwellian_flux (part_injection.f90:239-265) from a ran2 stream */
+static double shifted_flux_ran2(double vb, double vt, double fmax, int32_t *iseed) {
+    const double vm = vb - 4.0 * vt > 0.0 ? vb - 4.0 * vt : 0.0, vp = vb + 4.0 * vt;
+    for (;;) {
+        const double r1 = o_ran2(iseed), r2 = o_ran2(iseed);
+        const double v = vm + r1 * (vp - vm);
+        const double f = v * exp(-(v - vb) * (v - vb) / (vt * vt));
+        if (!(r2 > f / fmax)) return v;
+    }
+}
+
 /* part_injection.f90:216-231 */
 static double phi_at(const o_cfg *c, const double *phi, int ix, int iy, double x, double y) {
     const int W = c->nx + 3;
@@ -219,7 +252,11 @@ int o_part_injection(const o_cfg *c, const o_src *s, int ptype, const int32_t *b
         if (o_ran2(iseed) <= dN - (double)N) N += 1;
         N_inj[ptype] = N;
     }
+    if (inj_electrons_only(c, s))
+        for (int q = 1; q < c->ntype; q++) N_inj[q] = 0;
     const double vt = inj_vt(c, s, ptype);
+    double vb, fmx;
+    inj_beam(c, s, ptype, &vb, &fmx);
     for (int64_t i = 0; i < N_inj[ptype]; i++) {
         double x = 0.0, y = 0.0, rnd[2];
         int ix, iy;
@@ -268,19 +305,35 @@ int o_part_injection(const o_cfg *c, const o_src *s, int ptype, const int32_t *b
         double *p = vxp + 6 * (*np);
         (*np)++;
         double vx, vy, vz;
-        rnd[0] = o_ran2(iseed);
-        rnd[1] = o_ran2(iseed);
-        o_load_gauss(&vx, &vy, vt, rnd);
-        if (vz_sav == 0.0) {
+        if (abs(s->opt_inj) == 4) { /* part_injection.f90:161-178 */
+            const double vb_tmp = vb * cos(s->th_B);
+            for (;;) { /* label 75 */
+                vx = shifted_flux_ran2(vb_tmp, vt, fmx, iseed);
+                rnd[0] = o_ran2(iseed);
+                rnd[1] = o_ran2(iseed);
+                o_load_gauss(&vy, &vz, vt, rnd);
+                vy = vy + vb * sin(s->th_B);
+                const double dt_tmp = o_ran2(iseed) * ((double)s->ns_inj * c->dt);
+                x = vx * dt_tmp;
+                if (!(x < 0.0 || x > c->xmax)) break;
+            }
+            ix = (int)floor(x / c->dx) + 1;
+        } else {
             rnd[0] = o_ran2(iseed);
             rnd[1] = o_ran2(iseed);
             o_load_gauss(&vx, &vy, vt, rnd);
-            vz = vx;
-            vz_sav = vy;
-        } else {
-            vz = vz_sav;
-            vz_sav = 0.0;
+            if (vz_sav == 0.0) {
+                rnd[0] = o_ran2(iseed);
+                rnd[1] = o_ran2(iseed);
+                o_load_gauss(&vx, &vy, vt, rnd);
+                vz = vx;
+                vz_sav = vy;
+            } else {
+                vz = vz_sav;
+                vz_sav = 0.0;
+            }
         }
+        if (abs(s->opt_inj) == 3) vz = vz + vb; /* part_injection.f90:202 */
         p[0] = x; p[1] = y; p[2] = 0.0;
         p[3] = vx; p[4] = vy; p[5] = vz;
         *P_inj += 0.5 * c->Nm[ptype] * c->mass[ptype] * (p[3] * p[3] + p[4] * p[4] + p[5] * p[5]);
@@ -306,12 +359,15 @@ int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, co
             draw4((uint32_t)sp, 0u, TAG_INJN, U, seed, r);
             if (o_u01(r[0]) <= dN - (double)N) N += 1;
         }
+        if (sp > 0 && inj_electrons_only(c, s)) N = 0;
         if (np[sp] + N > cap[sp]) { rc = -2; N = 0; }
         count[sp] = N;
     }
     for (int sp = 0; sp < c->ntype; sp++) {
         const double vt = inj_vt(c, s, sp);
         const double Ek = 0.5 * c->Nm[sp] * c->mass[sp];
+        double vb, fmx;
+        inj_beam(c, s, sp, &vb, &fmx);
         for (int64_t j = 0; j < count[sp]; j++) {
             double x = 0.0, y = 0.0;
             int ix = 1, iy = 1, ok = 0;
@@ -350,18 +406,46 @@ int o_part_injection_ctr(const o_cfg *c, const o_src *s, const int32_t *bcnd, co
                 ok = 1;
             }
             if (!ok) return -3;
-            uint32_t q[4];
-            draw4((uint32_t)j, (uint32_t)sp, TAG_INJV, U, seed, q);
-            double vx, vy, vz;
-            if ((j & 1) == 0) {
-                gauss_u(vt, q[2], q[3], &vx, &vy);
-                vz = vx;
+            double vx = 0.0, vy = 0.0, vz = 0.0;
+            if (abs(s->opt_inj) == 4) {
+                /* one attempt = one flux draw (TAG_INJF: v, its acceptance, vy, vz) and one
+                 * time offset (TAG_INJG); a rejection or an x outside [0, xmax] starts the next */
+                const double vbt = vb * cos(s->th_B);
+                const double vm = vbt - 4.0 * vt > 0.0 ? vbt - 4.0 * vt : 0.0, vpm = vbt + 4.0 * vt;
+                int got = 0;
+                for (uint32_t a = 0; a < MAX_ATTEMPTS && !got; a++) {
+                    uint32_t f[4], g[4];
+                    draw4((uint32_t)j, (a << 3) | (uint32_t)sp, TAG_INJF, U, seed, f);
+                    const double v = vm + o_u01(f[0]) * (vpm - vm);
+                    const double fv = v * exp(-(v - vbt) * (v - vbt) / (vt * vt));
+                    if (o_u01(f[1]) > fv / fmx) continue;
+                    gauss_u(vt, f[2], f[3], &vy, &vz);
+                    draw4((uint32_t)j, (a << 3) | (uint32_t)sp, TAG_INJG, U, seed, g);
+                    const double xn = v * (o_u01(g[0]) * ((double)s->ns_inj * c->dt));
+                    if (xn < 0.0 || xn > c->xmax) continue;
+                    vx = v;
+                    vy = vy + vb * sin(s->th_B);
+                    x = xn;
+                    got = 1;
+                }
+                if (!got) return -3;
+                ix = (int)floor(x / c->dx) + 1;
+                if (ix < 1) ix = 1;
+                if (ix > c->nx + 1) ix = c->nx + 1;
             } else {
-                uint32_t qp[4];
-                double unused;
-                gauss_u(vt, q[0], q[1], &vx, &vy);
-                draw4((uint32_t)(j - 1), (uint32_t)sp, TAG_INJV, U, seed, qp);
-                gauss_u(vt, qp[2], qp[3], &unused, &vz);
+                uint32_t q[4];
+                draw4((uint32_t)j, (uint32_t)sp, TAG_INJV, U, seed, q);
+                if ((j & 1) == 0) {
+                    gauss_u(vt, q[2], q[3], &vx, &vy);
+                    vz = vx;
+                } else {
+                    uint32_t qp[4];
+                    double unused;
+                    gauss_u(vt, q[0], q[1], &vx, &vy);
+                    draw4((uint32_t)(j - 1), (uint32_t)sp, TAG_INJV, U, seed, qp);
+                    gauss_u(vt, qp[2], qp[3], &unused, &vz);
+                }
+                if (abs(s->opt_inj) == 3) vz = vz + vb;
             }
             double *p = vxp[sp] + 6 * (np[sp] + j);
             if (S > 0) {

@@ -136,13 +136,19 @@ def test_heating_tally_and_temperature_update(gpu_lib):
         sim.close()
 
 
-INJ_CASES = [(1, (0.08, 0.4, 0.08, 0.56)), (1, (-0.12, -0.44, 0, 0)), (-1, (0.16, 0.32, 0.08, 0.56)),
-             (-1, (-0.2, -0.4, 0, 0))]
+INJ_CASES = [(1, (0.08, 0.4, 0.08, 0.56), {}), (1, (-0.12, -0.44, 0, 0), {}),
+             (-1, (0.16, 0.32, 0.08, 0.56), {}), (-1, (-0.2, -0.4, 0, 0), {}),
+             (3, (0.08, 0.4, 0.08, 0.56), dict(THm=4.0)),
+             (4, (0.08, 0.4, 0.08, 0.56), dict(THm=4.0)),
+             (4, (0.0, 0.3, 0.08, 0.56), dict(THm=4.0, nmn=1, th_B=0.6)),
+             (-4, (0.0, 0.3, 0.08, 0.56), dict(THm=2.0, nmn=1, th_B=-0.3))]
 
 
-@pytest.mark.parametrize("opt,region", INJ_CASES)
-def test_injection_matches_oracle(gpu_lib, opt, region):
+@pytest.mark.parametrize("opt,region,extra", INJ_CASES)
+def test_injection_matches_oracle(gpu_lib, opt, region, extra):
+    extra = dict(extra)
     case = make_case(plate=True)
+    case.flag_nmn = extra.pop("nmn", 0)
     cfg, sp = oracle_cfg(case)
     sim = GpuSimulation(case, load=False, capacity=100000)
     try:
@@ -152,7 +158,7 @@ def test_injection_matches_oracle(gpu_lib, opt, region):
         sim.set_phi(phi)
         sim.deposit()
         sc = S.source_config(S.SourceDeck(heat_region_cm=region, I_inj=2000.0, opt_inj=opt, ni0=(1.0, 1.0),
-                                          flag_diffsrc=1, nu_h=-1.0, seed=99), case.dt, sp.vt0[0])
+                                          flag_diffsrc=1, nu_h=-1.0, seed=99, **extra), case.dt, sp.vt0[0])
         sim.set_sources(sc)
         before = [sim.get_particles(s) for s in (0, 1)]
         sim.inject(6)
@@ -166,11 +172,16 @@ def test_injection_matches_oracle(gpu_lib, opt, region):
                                                   phi, [0, 0], sc.seed, 6, Sb, vx, [len(b) for b in before])
         assert rc == 0
         assert t["n_inj_last"] == list(cnt) and cnt[0] > 1000
+        # part_injection.f90:77-79: no ions under the beam, nor from the cathode without Neumann
+        assert (cnt[1] == 0) == (abs(opt) == 3 or (abs(opt) == 4 and case.flag_nmn == 0))
         unit = case.dx * 2.0 ** -Sb
         for s in (0, 1):
             assert len(after[s]) == len(before[s]) + cnt[s]
             assert np.array_equal(after[s][:len(before[s])], before[s])
             new, ref = after[s][len(before[s]):], vx[s][len(before[s]):n[s]]
+            if cnt[s] == 0:
+                assert t["P_inj"][s] == 0.0
+                continue
             assert np.abs(new[:, :2] - ref[:, :2]).max() <= unit * 1.0001
             float_match(ref[:, 3:], new[:, 3:])
             assert t["P_inj"][s] == pytest.approx(Pi[s], rel=1e-9)
@@ -253,7 +264,7 @@ def test_source_errors(gpu_lib):
     sim = GpuSimulation(case, load=False, capacity=1000)
     try:
         lib = sim.lib
-        bad = S.source_config(S.SourceDeck(heat_region_cm=(0.1, 0.3, 0.1, 0.3), I_inj=1.0, opt_inj=3),
+        bad = S.source_config(S.SourceDeck(heat_region_cm=(0.1, 0.3, 0.1, 0.3), I_inj=1.0, opt_inj=5),
                               case.dt, sp.vt0[0])
         assert lib.lepic_gpu_set_sources(sim.ctx, C.byref(bad)) == capi.EINVAL
         bad = S.source_config(S.SourceDeck(heat_region_cm=(0.1, 3.0, 0.1, 0.3), I_inj=1.0), case.dt, sp.vt0[0])

@@ -273,6 +273,89 @@ def test_injection_two_forms_agree_in_distribution(oracle_lib):
     assert np.all(pb[0::2, 5] == pb[0::2, 3])
 
 
+def flux_mean(vb, vt):
+    """The mean of v under the shifted-Maxwellian flux v exp(-(v - vb)^2 / vt^2) on
+    [max(0, vb - 4 vt), vb + 4 vt] (part_injection.f90:239-265)."""
+    v = np.linspace(max(0.0, vb - 4 * vt), vb + 4 * vt, 200001)
+    f = v * np.exp(-(v - vb) ** 2 / vt ** 2)
+    return float((v * f).sum() / f.sum())
+
+
+@pytest.mark.parametrize("nmn", [0, 1])
+def test_injection_beam_and_cathode_reference_form(oracle_lib, nmn):
+    """|opt_inj| = 3: electrons only, vz shifted by the beam speed; |opt_inj| = 4: the flux
+    along +x from the cathode at x = 0 (electrons half-Maxwellian with Neumann), positions
+    x = vx * U(0, ns_inj dt), vy shifted by vb sin(th_B); ions only with Neumann."""
+    case, cfg, sp = setup()
+    cfg.flag_nmn = nmn
+    b = np.array(case.bcnd, dtype=np.int32)
+    phi = np.zeros((case.ny + 3, case.nx + 3))
+    THm, thB = 3.0, 0.4
+    for opt in (3, 4):
+        sc = src_cfg(sp, case.dt, heat_region_cm=(0.04, 0.28, 0.04, 0.28), I_inj=1600.0, opt_inj=opt,
+                     ni0=(1.0, 1.0), THm=THm, th_B=thB, ns_inj=2)
+        src = O.make_src(sc)
+        assert src.th_B == (thB if opt == 4 else 0.0)
+        for ptype in (0, 1):
+            N_inj = np.zeros(8, dtype=np.int64)
+            vxp = np.zeros((40000, 6))
+            rc, n, Pi, Ps, _ = O.part_injection(cfg, src, ptype, b, phi, N_inj, vxp, 0, 31 + ptype)
+            assert rc == 0
+            ions_off = opt == 3 or nmn == 0
+            if ptype == 1 and ions_off:
+                assert n == 0 and N_inj[1] == 0
+                continue
+            assert n > 3000
+            p = vxp[:n]
+            vt = sp.vt0[ptype]
+            vb = math.sqrt(2 * dk.QE * THm / abs(sp.mass[ptype]))
+            if opt == 3:
+                assert abs(p[:, 5].mean() - vb) < 5 * vt / math.sqrt(2 * n)
+                assert np.all(p[0::2, 5] - vb == pytest.approx(p[0::2, 3], abs=1e-9 * vb))
+                continue
+            if opt == 4 and ptype == 0 and nmn == 1:
+                vb = 0.0
+            vbt = vb * math.cos(thB)
+            assert p[:, 3].min() >= max(0.0, vbt - 4 * vt) and p[:, 3].max() <= vbt + 4 * vt
+            m = flux_mean(vbt, vt)
+            assert abs(p[:, 3].mean() - m) < 5 * p[:, 3].std() / math.sqrt(n)
+            assert abs(p[:, 4].mean() - vb * math.sin(thB)) < 5 * vt / math.sqrt(2 * n) + 1e-12
+            assert abs(p[:, 5].mean()) < 5 * vt / math.sqrt(2 * n)
+            t = p[:, 0] / p[:, 3]
+            ns_dt = 2 * case.dt
+            assert t.min() >= 0.0 and t.max() <= ns_dt * (1 + 1e-12)
+            assert abs(t.mean() / (ns_dt / 2) - 1) < 0.05
+            assert Pi == pytest.approx(0.5 * sp.Nm[ptype] * sp.mass[ptype] * (p[:, 3:] ** 2).sum(), rel=1e-9)
+
+
+def test_cathode_two_forms_agree_in_distribution(oracle_lib):
+    case, cfg, sp = setup()
+    cfg.flag_nmn = 1
+    b = np.array(case.bcnd, dtype=np.int32)
+    phi = np.zeros((case.ny + 3, case.nx + 3))
+    sc = src_cfg(sp, case.dt, heat_region_cm=(0.0, 0.2, 0.04, 0.28), I_inj=6000.0, opt_inj=4, ni0=(1.0, 1.0),
+                 THm=5.0, th_B=-0.7)
+    src = O.make_src(sc)
+    N_inj = np.zeros(8, dtype=np.int64)
+    va = np.zeros((30000, 6))
+    rc, na, *_ = O.part_injection(cfg, src, 1, b, phi, N_inj, va, 0, 77)
+    vb_ = [np.zeros((30000, 6)), np.zeros((30000, 6))]
+    rc2, nb, cnt, *_ = O.part_injection_ctr(cfg, src, b, phi, [0, 0], 5, 4, 0, vb_, [0, 0])
+    assert rc == 0 and rc2 == 0 and abs(na - cnt[1]) <= 1 and na > 5000
+    pa, pb = va[:na], vb_[1][:cnt[1]]
+    for k in (0, 1, 3, 4, 5):
+        se = math.sqrt(pa[:, k].var() / na + pb[:, k].var() / cnt[1])
+        assert abs(pa[:, k].mean() - pb[:, k].mean()) < 5 * se
+        assert abs(pa[:, k].std() / pb[:, k].std() - 1) < 0.05
+
+
+def test_cathode_angle():
+    assert S.cathode_angle(4, 1, 0.02, 0.01) == pytest.approx(math.atan(0.5))
+    assert S.cathode_angle(4, 0, 0.02, 0.01) == 0.0
+    assert S.cathode_angle(-4, 1, 0.02, 0.01) == 0.0        # main.f90:450: opt_inj .eq. 4
+    assert S.cathode_angle(4, 1, 0.0, 0.01) == 0.0
+
+
 # ---- deck conversions ------------------------------------------------------------------
 def test_source_deck_conversions():
     d = S.SourceDeck(heat_region_cm=(-1.0, -3.0, 0.5, 2.5), n_icp=-2, Pabs=(100.0, 50.0), nu_h=1.0e7,
