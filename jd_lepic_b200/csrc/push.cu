@@ -28,7 +28,8 @@ struct PushP {
     const float4 *E;           // node pairs: (Ex, Ey)[n], (Ex, Ey)[n+1]
     const float4 *B;
     float Bcx, Bcy, Bcz;
-    float k2c;                 // the Boris factor of the constant field (BMODE 1)
+    float tcx, tcy, tcz;       // constant field (BMODE 1): t = k1 B and s = k2 B of the Boris
+    float scx, scy, scz;       // rotation, k2 = 2 k1 / (1 + k1^2 |B|^2)
     const uint8_t *cellwall;
     unsigned long long *acc;
     const WorkItem *items;
@@ -36,6 +37,7 @@ struct PushP {
     int sp;
     float k1;                  // dt*q/(2m)
     float cdx, cdy;            // dt * 2^S / dx
+    float inv2S;               // 2^-S
     int pbc, spec, nmn, negion_nmn;
     uint32_t step_key;
     int tw, th, ntx, M, WX, WY, win;
@@ -59,6 +61,24 @@ __device__ __forceinline__ void cic_weights(const PushP &P, uint32_t X, uint32_t
     }
 }
 
+// The node weights of a run from its moments: n particles with offsets fx, fy summed as
+// sx = sum fx, sy = sum fy, sxy = sum fx fy give sum (A-fx)(A-fy), sum fx (A-fy), sum fx fy,
+// sum (A-fx) fy (A = 2^S).  Used when 2S <= LEPIC_DEP_SHIFT: every product is then exact and
+// only shifted up, so the run's weights equal the sum of its particles' cic_weights bit for
+// bit, for two 32-bit adds, one 32x32 product and one 64-bit add per particle.
+__device__ __forceinline__ void mom_weights(const PushP &P, uint32_t n, uint32_t sx, uint32_t sy, uint64_t sxy,
+                                            uint64_t *w) {
+    const int S = P.S;
+    const uint64_t Asx = (uint64_t)sx << S, Asy = (uint64_t)sy << S;
+    w[2] = sxy;
+    w[1] = Asx - sxy;
+    w[3] = Asy - sxy;
+    w[0] = ((uint64_t)n << (2 * S)) - Asx - Asy + sxy;
+    const int up = LEPIC_DEP_SHIFT - 2 * S;
+#pragma unroll
+    for (int k = 0; k < 4; k++) w[k] <<= up;
+}
+
 // the four accumulators of cell (ix, iy): the CTA's shared-memory window or the global grid
 __device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win, int ox, int oy, bool use_win,
                                          int ix, int iy, const uint64_t *w) {
@@ -72,30 +92,10 @@ __device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win
         q = P.acc + ix + (long long)iy * P.W;
         row = P.W;
     }
-    if (w[0]) atomicAdd(q, (unsigned long long)w[0]);
-    if (w[1]) atomicAdd(q + 1, (unsigned long long)w[1]);
-    if (w[2]) atomicAdd(q + row + 1, (unsigned long long)w[2]);
-    if (w[3]) atomicAdd(q + row, (unsigned long long)w[3]);
-}
-
-// The last run of every lane, aggregated over the warp: lanes whose runs share a cell (the
-// usual case after the sort) add their sums with exact 32-bit warp reductions of 24-bit
-// halves (a run holds at most PUSH_G <= 8 weights <= 2^44 each, so a half stays below 2^24
-// and 32 of them below 2^29), and one lane issues the atomics.  Called by all 32 lanes.
-__device__ __forceinline__ void flush_warp(const PushP &P, unsigned long long *win, int ox, int oy, bool use_win,
-                                           int key, int ix, int iy, uint64_t *w) {
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    if (key < 0) return;
-    if (__popc(grp) > 1) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const unsigned lo = __reduce_add_sync(grp, (unsigned)(w[k] & 0xFFFFFFull));
-            const unsigned hi = __reduce_add_sync(grp, (unsigned)(w[k] >> 24));
-            w[k] = ((uint64_t)hi << 24) + lo;
-        }
-        if ((int)(threadIdx.x & 31) != __ffs(grp) - 1) return;
-    }
-    add_cell(P, win, ox, oy, use_win, ix, iy, w);
+    atomicAdd(q, (unsigned long long)w[0]);
+    atomicAdd(q + 1, (unsigned long long)w[1]);
+    atomicAdd(q + row + 1, (unsigned long long)w[2]);
+    atomicAdd(q + row, (unsigned long long)w[3]);
 }
 
 // part_mover for one particle in registers; returns false for a hole or a particle lost in
@@ -106,7 +106,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
                                           float &vz, DevCounters *cnt, unsigned int &lost, int &ixo, int &iyo) {
     if (isnan(vx)) return false; // hole
     const uint32_t mask = (1u << P.S) - 1u;
-    const float inv2S = 1.0f / (float)(1u << P.S);
+    const float inv2S = P.inv2S;
     // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
     const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
     const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
@@ -135,43 +135,47 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         }
     }
     float ux0 = vx, uy0 = vy, uz0 = vz;
-    if (mag) { // Boris, part_expmover.f90:187-206
-        float k2;
-        if (BMODE == 1) {
-            k2 = P.k2c;   // constant field: computed once per launch
+    if (mag) { // Boris, part_expmover.f90:187-206, with t = k1 B and s = k2 B
+        float tx, ty, tz, sx, sy, sz;
+        if (BMODE == 1) {   // constant field: t and s computed once per launch
+            tx = P.tcx; ty = P.tcy; tz = P.tcz;
+            sx = P.scx; sy = P.scy; sz = P.scz;
         } else {
             const float Bt2 = Bx * Bx + By * By + Bz * Bz;
-            k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+            const float k2 = k1 * (2.0f / (1.0f + k1 * k1 * Bt2));
+            tx = k1 * Bx; ty = k1 * By; tz = k1 * Bz;
+            sx = k2 * Bx; sy = k2 * By; sz = k2 * Bz;
         }
-        const float v1x = ux0 + k1 * Ex, v1y = uy0 + k1 * Ey, v1z = uz0;
-        const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
-        const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
-        const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
-        ux0 = v1x + k2 * (v3y * Bz - v3z * By) + k1 * Ex;
-        uy0 = v1y + k2 * (v3z * Bx - v3x * Bz) + k1 * Ey;
-        uz0 = v1z + k2 * (v3x * By - v3y * Bx);
+        const float v1x = fmaf(k1, Ex, ux0), v1y = fmaf(k1, Ey, uy0), v1z = uz0;
+        // v3 = v1 + v1 x t;  u = v1 + v3 x s + k1 E
+        const float v3x = fmaf(v1y, tz, fmaf(-v1z, ty, v1x));
+        const float v3y = fmaf(v1z, tx, fmaf(-v1x, tz, v1y));
+        const float v3z = fmaf(v1x, ty, fmaf(-v1y, tx, v1z));
+        ux0 = fmaf(v3y, sz, fmaf(-v3z, sy, fmaf(k1, Ex, v1x)));
+        uy0 = fmaf(v3z, sx, fmaf(-v3x, sz, fmaf(k1, Ey, v1y)));
+        uz0 = fmaf(v3x, sy, fmaf(-v3y, sx, v1z));
     } else { // leap-frog, :210-211
         ux0 = ux0 + 2.0f * k1 * Ex;
         uy0 = uy0 + 2.0f * k1 * Ey;
     }
-    // a non-finite velocity (a non-finite field) is an error: the particle is removed
-    if (!(fabsf(ux0) <= 3.0e8f && fabsf(uy0) <= 3.0e8f && fabsf(uz0) <= 3.0e8f)) {
+    // a speed above 3e8 m/s or a non-finite velocity (a non-finite field) is an error: the
+    // particle is removed (a NaN component makes the comparison false)
+    if (!(ux0 * ux0 + uy0 * uy0 + uz0 * uz0 <= 9.0e16f)) {
         set_err(cnt, LERR_RANGE, 101);
         lost++;
         vx = __int_as_float(HOLE_NAN);
         return false;
     }
-    // move (:216-217): integer part plus an unbiased stochastic rounding of the fractional part
-    // of the displacement (16-bit uniforms from one integer hash of slot and step)
+    // move (:216-217) in fixed-point units: the displacement rounded stochastically,
+    // floor(d + u) with u uniform on [0, 1) in steps of 2^-16 (one integer hash of slot and
+    // step), which rounds up with probability frac(d) and so moves slow particles unbiased
     uint32_t h = (uint32_t)i * 0x9E3779B1u ^ P.step_key;
     h = (h ^ (h >> 16)) * 0x7FEB352Du;
     h ^= h >> 15;
     const float ux = (float)(h & 0xFFFFu) * (1.0f / 65536.0f);
     const float uy = (float)(h >> 16) * (1.0f / 65536.0f);
-    const float ddx = ux0 * P.cdx, ddy = uy0 * P.cdy;
-    const float fdx = floorf(ddx), fdy = floorf(ddy);
-    const int dX = (int)fdx + ((ux < ddx - fdx) ? 1 : 0);
-    const int dY = (int)fdy + ((uy < ddy - fdy) ? 1 : 0);
+    const int dX = __float2int_rd(fmaf(ux0, P.cdx, ux));
+    const int dY = __float2int_rd(fmaf(uy0, P.cdy, uy));
     if (!GEN) {
         // a particle that stays in its cell (the common case) and whose cell is not a wall cell
         // is neither lost nor out of range (a wrap of the 32-bit sum always changes the cell)
@@ -232,12 +236,11 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
 
 // Each thread takes PUSH_G consecutive slots per iteration (one 16-byte vector load and store
 // per array): after the sort consecutive particles mostly share a cell, so the deposit
-// accumulates runs of equal cells in registers and only the last run of a thread goes
-// through the warp aggregation; a run that ends earlier goes straight to the accumulators.
+// accumulates runs of equal cells in registers and adds each run to the accumulators once.
 // A work item's range is rounded down to multiples of 8 slots at both ends, so consecutive items
 // still tile the slot array exactly; particles a rounded range takes from a neighbouring
 // tile reach the global grid when they fall outside the window.
-template <int BMODE, bool GEN, bool MOVE>
+template <int BMODE, bool GEN, bool MOVE, bool MOM>
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
@@ -291,7 +294,8 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                 vz[0] = c0.x; vz[1] = c0.y; vz[2] = c0.z; vz[3] = c0.w;
             }
             int rkey = -1, rix = 0, riy = 0;   // the current run of equal cells
-            uint64_t rw[4] = {0, 0, 0, 0};
+            uint64_t rw[4] = {0, 0, 0, 0};     // its weights, or (MOM) its moments n, sx, sy, sxy
+            const uint32_t fmask = (1u << P.S) - 1u;
             if (grp_ok) {
 #pragma unroll
                 for (int p = 0; p < PUSH_G; p++) {
@@ -308,6 +312,22 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                     }
                     if (!alive) continue;
                     const int key = ix + iy * P.W;
+                    if (MOM) {
+                        const uint32_t fx = X[p] & fmask, fy = Y[p] & fmask;
+                        const uint64_t fxy = (uint64_t)fx * fy;
+                        if (key != rkey) {
+                            if (rkey >= 0) {
+                                uint64_t w[4];
+                                mom_weights(P, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3], w);
+                                add_cell(P, win, ox, oy, use_win, rix, riy, w);
+                            }
+                            rkey = key; rix = ix; riy = iy;
+                            rw[0] = 1; rw[1] = fx; rw[2] = fy; rw[3] = fxy;
+                        } else {
+                            rw[0] += 1; rw[1] += fx; rw[2] += fy; rw[3] += fxy;
+                        }
+                        continue;
+                    }
                     uint64_t w[4];
                     cic_weights(P, X[p], Y[p], w);
                     if (key != rkey) {
@@ -326,7 +346,19 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                     *reinterpret_cast<float4 *>(P.VZ + g) = make_float4(vz[0], vz[1], vz[2], vz[3]);
                 }
             }
-            flush_warp(P, win, ox, oy, use_win, rkey, rix, riy, rw);
+            // every lane adds its last run itself: lanes whose runs share a cell (the usual case
+            // after the sort) meet at the same shared-memory words, and the serialised atomics
+            // cost less issue than any warp-level combination of the runs (a group-masked warp
+            // reduction measured 16 % slower on the whole push, a segmented shuffle scan 4 %)
+            if (rkey >= 0) {
+                if (MOM) {
+                    uint64_t w[4];
+                    mom_weights(P, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3], w);
+                    add_cell(P, win, ox, oy, use_win, rix, riy, w);
+                } else {
+                    add_cell(P, win, ox, oy, use_win, rix, riy, rw);
+                }
+            }
         }
         // lost-particle count: one atomic per warp, then per CTA
         for (int o = 16; o > 0; o >>= 1) lost += __shfl_xor_sync(0xffffffffu, lost, o);
@@ -349,25 +381,33 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     }
 }
 
-template <int BMODE, bool GEN, bool MOVE>
+template <int BMODE, bool GEN, bool MOVE, bool MOM>
 static int launch_one(lepic_ctx *c, PushP &P, size_t smem) {
     static bool attr_set[64] = {false};
     if (!attr_set[c->dev & 63]) {
-        LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   64 * 1024));
+        LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE, MOM>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         attr_set[c->dev & 63] = true;
     }
     int occ = 0;
-    LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE>, PUSH_THREADS, smem));
-    k_push_deposit<BMODE, GEN, MOVE><<<c->num_sms * std::max(1, occ), PUSH_THREADS, smem, c->stream>>>(P);
+    LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE, MOM>, PUSH_THREADS,
+                                                        smem));
+    k_push_deposit<BMODE, GEN, MOVE, MOM><<<c->num_sms * std::max(1, occ), PUSH_THREADS, smem, c->stream>>>(P);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
 
+template <int BMODE, bool MOM>
+static int launch_m(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
+    if (!move) return launch_one<BMODE, false, false, MOM>(c, P, smem);
+    return gen ? launch_one<BMODE, true, true, MOM>(c, P, smem) : launch_one<BMODE, false, true, MOM>(c, P, smem);
+}
+
+// moments deposit where the weights are exact (2S <= LEPIC_DEP_SHIFT, grids of 1024 and up)
 template <int BMODE>
 static int launch_b(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
-    if (!move) return launch_one<BMODE, false, false>(c, P, smem);
-    return gen ? launch_one<BMODE, true, true>(c, P, smem) : launch_one<BMODE, false, true>(c, P, smem);
+    return 2 * P.S <= LEPIC_DEP_SHIFT ? launch_m<BMODE, true>(c, P, smem, gen, move)
+                                      : launch_m<BMODE, false>(c, P, smem, gen, move);
 }
 
 int push_deposit(lepic_ctx *c, int it, bool move) {
@@ -389,7 +429,9 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         {
             const float k1f = (float)(g.dt * g.charge[s] / (2.0 * g.mass[s]));
             const float Bt2 = P.Bcx * P.Bcx + P.Bcy * P.Bcy + P.Bcz * P.Bcz;
-            P.k2c = k1f * (2.0f / (1.0f + k1f * k1f * Bt2));
+            const float k2 = k1f * (2.0f / (1.0f + k1f * k1f * Bt2));
+            P.tcx = k1f * P.Bcx; P.tcy = k1f * P.Bcy; P.tcz = k1f * P.Bcz;
+            P.scx = k2 * P.Bcx; P.scy = k2 * P.Bcy; P.scz = k2 * P.Bcz;
         }
         P.cellwall = c->cellwall;
         P.acc = B.acc;
@@ -399,6 +441,7 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         P.k1 = (float)(g.dt * g.charge[s] / (2.0 * g.mass[s]));
         P.cdx = (float)(g.dt * (double)(1u << c->S) / g.dx);
         P.cdy = (float)(g.dt * (double)(1u << c->S) / g.dy);
+        P.inv2S = 1.0f / (float)(1u << c->S);
         P.pbc = g.flag_pbc; P.spec = g.flag_spec; P.nmn = g.flag_nmn;
         P.negion_nmn = (g.charge[s] < 0 && g.mass[s] >= amu && g.flag_nmn == 1) ? 1 : 0;
         P.step_key = (uint32_t)(g.seed * 0x2545F491ull) ^ ((uint32_t)it * 0x27D4EB2Fu) ^ ((uint32_t)s * 0x165667B1u);

@@ -100,6 +100,41 @@ def test_push_and_deposit_match_oracle(gpu_lib, bmode):
     s.close()
 
 
+@pytest.mark.parametrize("nx", [1024, 2048])
+def test_push_and_deposit_large_grid(gpu_lib, nx):
+    """Grids of 1024 and up (S <= 22) deposit through per-run moments: exact integer weights,
+    so the density must equal the oracle's FP64 CIC to 1e-12 and be bit-reproducible."""
+    case = configs.case0(ppc=1, nx=nx, ny=nx)
+    case.flag_B, case.Bc = 1, (0.0, 0.0, 0.005)
+    grids = []
+    for rep in range(2):
+        s = sim_for(case, tile=(16, 16))
+        s.set_phi(smooth_phi(case))
+        E = s.efield()
+        s.sort(0)
+        s.sort(1)
+        cfg = oracle_cfg(case, s)
+        p0 = [s.get_particles(k) for k in range(2)]
+        s.push(1)
+        p_all = [s.get_particles(k) for k in range(2)]
+        grids.append([s.grid(capi.GRID_NP + k) for k in range(2)])
+        if rep == 0:
+            kq = O.kq_of(case.bcnd)
+            for sp in range(2):
+                ref = p0[sp].copy()
+                n_ref, _ = O.mover(cfg, sp, E, case.Bi, case.bcnd, ref)
+                got = p_all[sp]
+                assert abs(got.shape[0] - n_ref) <= 2
+                if got.shape[0] == n_ref:
+                    assert np.abs(got[:, :2] - ref[:n_ref, :2]).max() <= 1e-6 * case.dx
+                npg = np.zeros((case.ny + 3, case.nx + 3))
+                O.deposit(cfg, sp, got, got.shape[0], kq, npg)
+                assert np.abs(grids[0][sp] - npg).max() <= 1e-12 * np.abs(npg).max()
+        s.close()
+    for k in range(2):
+        assert np.array_equal(grids[0][k], grids[1][k])
+
+
 def test_deposit_bit_reproducible(gpu_lib, small):
     grids = []
     for _ in range(2):
