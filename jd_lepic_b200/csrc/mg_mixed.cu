@@ -527,6 +527,26 @@ __device__ bool vcycle32(const MXP &P) {
 }
 
 
+// The FP64 passes walk FB nodes per thread at a time and issue all their loads before any
+// arithmetic: a thread holds ~40 nodes of the 2049^2 level, and one node at a time leaves
+// each pass waiting on ~40 memory latencies in a row.  The sums keep the walk order.  The
+// five-point passes take two nodes at a time (the kernel's 80 registers), the others four.
+#define FB 4
+#define FB5 2
+
+// the next FB interior positions of the walk: flat index t over (nx+1)(ny+1), node index n
+// over (nx+3)(ny+3); v = false past the end (n = t = 0, read but never written)
+template <int NB>
+__device__ __forceinline__ void walk_batch(Walk2 &w, int W, int *t, int *n, bool *v) {
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        v[u] = w.ok();
+        t[u] = v[u] ? w.flat() : 0;
+        n[u] = v[u] ? (w.k + 1) + (w.j + 1) * W : 0;
+        if (v[u]) w.next();
+    }
+}
+
 // r = b - A u at unknowns (bcnd <= 0), zero elsewhere; r32 = (float) r; e = 0 (all nodes);
 // returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum
 __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double *l1) {
@@ -534,24 +554,37 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
     double a = 0.0, s1 = 0.0;
-    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
-        const int t = w.flat();
-        const int i = w.k + 1, j = w.j + 1;
-        const int n = i + j * W;
-        const int bc = L.bc[n];
-        double r = 0.0;
-        if (bc <= 0) {
-            const double *u = L.u;
-            r = L.b[t] - (aw * u[n - 1] + an * u[n + W] + an * u[n - W] + aw * u[n + 1] + ac * u[n]);
-            if (bc == -1) { a += r * r; s1 += fabs(r); }
+    Walk2 w(B.rank(), B.size(), nx + 1, ny + 1);
+    while (w.ok()) {
+        int t[FB5], n[FB5];
+        bool v[FB5];
+        walk_batch<FB5>(w, W, t, n, v);
+        int bc[FB5];
+        double bb[FB5], uc[FB5], uw[FB5], ue[FB5], us[FB5], un[FB5];
+        const double *u = L.u;
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            bc[k] = v[k] ? L.bc[n[k]] : 1;
+            bb[k] = L.b[t[k]];
+            uc[k] = u[n[k]]; uw[k] = u[n[k] - 1 + (v[k] ? 0 : 1)]; ue[k] = u[n[k] + 1];
+            us[k] = v[k] ? u[n[k] - W] : 0.0; un[k] = u[n[k] + W];
         }
-        P.r64[n] = r;
-        L.r[t] = (float)r;
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            if (!v[k]) continue;
+            double r = 0.0;
+            if (bc[k] <= 0) {
+                r = bb[k] - (aw * uw[k] + an * un[k] + an * us[k] + aw * ue[k] + ac * uc[k]);
+                if (bc[k] == -1) { a += r * r; s1 += fabs(r); }
+            }
+            P.r64[n[k]] = r;
+            L.r[t[k]] = (float)r;
+        }
     }
-    for (Walk2 w(B.rank(), B.size(), W, ny + 3); w.ok(); w.next()) {
-        const int t = w.flat();
+    for (Walk2 w2(B.rank(), B.size(), W, ny + 3); w2.ok(); w2.next()) {
+        const int t = w2.flat();
         L.e[t] = 0.0f;
-        if (w.k == 0 || w.j == 0 || w.k == nx + 2 || w.j == ny + 2) P.r64[t] = 0.0;
+        if (w2.k == 0 || w2.j == 0 || w2.k == nx + 2 || w2.j == ny + 2) P.r64[t] = 0.0;
     }
     if (!team_sum(B, a, rr)) return false;
     return team_sum(B, s1, l1);
@@ -561,9 +594,24 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
 __device__ bool dot_rz(const BigTeam &B, const MXP &P, double *rz) {
     const MXL &L = P.L[0];
     const int nn = (L.nx + 3) * (L.ny + 3);
+    const int st = (int)B.size();
     double a = 0.0;
-    for (int t = (int)B.rank(); t < nn; t += (int)B.size())
-        if (L.bc[t] <= 0) a += P.r64[t] * (double)L.e[t];
+    for (int t0 = (int)B.rank(); t0 < nn; t0 += FB * st) {
+        int bc[FB];
+        double r[FB];
+        float e[FB];
+#pragma unroll
+        for (int k = 0; k < FB; k++) {
+            const int t = t0 + k * st;
+            const bool v = t < nn;
+            bc[k] = v ? L.bc[t] : 1;
+            r[k] = v ? P.r64[t] : 0.0;
+            e[k] = v ? L.e[t] : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < FB; k++)
+            if (bc[k] <= 0) a += r[k] * (double)e[k];
+    }
     return team_sum(B, a, rz);
 }
 
@@ -575,24 +623,45 @@ __device__ bool update_pq(const BigTeam &B, const MXP &P, double beta, bool firs
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
     double a = 0.0;
-    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
-        const int n = (w.k + 1) + (w.j + 1) * W;
-        if (L.bc[n] > 0) {
-            P.p64[n] = 0.0;
-            P.ap64[n] = 0.0;
-            continue;
-        }
+    Walk2 w(B.rank(), B.size(), nx + 1, ny + 1);
+    while (w.ok()) {
+        int t[FB5], n[FB5];
+        bool v[FB5];
+        walk_batch<FB5>(w, W, t, n, v);
         const int8_t *bc = L.bc;
         const float *e = L.e;
-        const double z = (double)e[n];
-        const double zw = bc[n - 1] <= 0 ? (double)e[n - 1] : 0.0, ze = bc[n + 1] <= 0 ? (double)e[n + 1] : 0.0;
-        const double zs = bc[n - W] <= 0 ? (double)e[n - W] : 0.0, zn = bc[n + W] <= 0 ? (double)e[n + W] : 0.0;
-        const double Az = aw * zw + an * zn + an * zs + aw * ze + ac * z;
-        const double p = first ? z : z + beta * P.p64[n];
-        const double q = first ? Az : Az + beta * P.ap64[n];
-        P.p64[n] = p;
-        P.ap64[n] = q;
-        a += p * q;
+        int b0[FB5], bw[FB5], be[FB5], bs[FB5], bn[FB5];
+        float z0[FB5], zw[FB5], ze[FB5], zs[FB5], zn[FB5];
+        double p0[FB5], q0[FB5];
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            const int m = n[k];
+            const int ms = v[k] ? m - W : m;
+            b0[k] = v[k] ? bc[m] : 1;
+            bw[k] = bc[m - 1 + (v[k] ? 0 : 1)]; be[k] = bc[m + 1]; bs[k] = bc[ms]; bn[k] = bc[m + W];
+            z0[k] = e[m]; zw[k] = e[m - 1 + (v[k] ? 0 : 1)]; ze[k] = e[m + 1]; zs[k] = e[ms]; zn[k] = e[m + W];
+            p0[k] = P.p64[m];
+            q0[k] = P.ap64[m];
+        }
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            if (!v[k]) continue;
+            const int m = n[k];
+            if (b0[k] > 0) {
+                P.p64[m] = 0.0;
+                P.ap64[m] = 0.0;
+                continue;
+            }
+            const double z = (double)z0[k];
+            const double dzw = bw[k] <= 0 ? (double)zw[k] : 0.0, dze = be[k] <= 0 ? (double)ze[k] : 0.0;
+            const double dzs = bs[k] <= 0 ? (double)zs[k] : 0.0, dzn = bn[k] <= 0 ? (double)zn[k] : 0.0;
+            const double Az = aw * dzw + an * dzn + an * dzs + aw * dze + ac * z;
+            const double p = first ? z : z + beta * p0[k];
+            const double q = first ? Az : Az + beta * q0[k];
+            P.p64[m] = p;
+            P.ap64[m] = q;
+            a += p * q;
+        }
     }
     return team_sum(B, a, pq);
 }
@@ -602,16 +671,26 @@ __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     double a = 0.0;
-    for (Walk2 w(B.rank(), B.size(), nx + 1, ny + 1); w.ok(); w.next()) {
-        const int t = w.flat();
-        const int n = (w.k + 1) + (w.j + 1) * W;
-        const int bc = L.bc[n];
-        if (bc <= 0) {
-            L.u[n] = L.u[n] + alpha * P.p64[n];
-            double r = P.r64[n] - alpha * P.ap64[n];
-            P.r64[n] = r;
-            L.r[t] = (float)r;
-            if (bc == -1) a += r * r;
+    Walk2 w(B.rank(), B.size(), nx + 1, ny + 1);
+    while (w.ok()) {
+        int t[FB], n[FB];
+        bool v[FB];
+        walk_batch<FB>(w, W, t, n, v);
+        int bc[FB];
+        double uu[FB], pp[FB], r0[FB], ap[FB];
+#pragma unroll
+        for (int k = 0; k < FB; k++) {
+            bc[k] = v[k] ? L.bc[n[k]] : 1;
+            uu[k] = L.u[n[k]]; pp[k] = P.p64[n[k]]; r0[k] = P.r64[n[k]]; ap[k] = P.ap64[n[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < FB; k++) {
+            if (bc[k] > 0) continue;
+            L.u[n[k]] = uu[k] + alpha * pp[k];
+            const double r = r0[k] - alpha * ap[k];
+            P.r64[n[k]] = r;
+            L.r[t[k]] = (float)r;
+            if (bc[k] == -1) a += r * r;
         }
     }
     if (!P.tiled) { // the grid-wide cycle starts from the zeroed e; the tiled one loads zeros itself
@@ -626,15 +705,31 @@ __device__ bool b0_norm(const Team &T, const MXL &L, double *bb) {
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_;
     double b = 0.0;
-    for (Walk2 w(T.rank(), T.size(), nx + 1, ny + 1); w.ok(); w.next()) {
-        const int t = w.flat();
-        const int n = (w.k + 1) + (w.j + 1) * W;
-        if (L.bc[n] != -1) continue;
+    Walk2 w(T.rank(), T.size(), nx + 1, ny + 1);
+    while (w.ok()) {
+        int t[FB5], n[FB5];
+        bool v[FB5];
+        walk_batch<FB5>(w, W, t, n, v);
         const double *u = L.u;
         const int8_t *bc = L.bc;
-        double d = L.b[t] - ((bc[n - 1] > 0 ? aw * u[n - 1] : 0.0) + (bc[n + W] > 0 ? an * u[n + W] : 0.0) +
-                             (bc[n - W] > 0 ? an * u[n - W] : 0.0) + (bc[n + 1] > 0 ? aw * u[n + 1] : 0.0));
-        b += d * d;
+        int b0[FB5], bw[FB5], be[FB5], bs[FB5], bn[FB5];
+        double bv[FB5], uw[FB5], ue[FB5], us[FB5], un[FB5];
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            const int m = n[k];
+            const int ms = v[k] ? m - W : m, mw = v[k] ? m - 1 : m;
+            b0[k] = v[k] ? bc[m] : 1;
+            bw[k] = bc[mw]; be[k] = bc[m + 1]; bs[k] = bc[ms]; bn[k] = bc[m + W];
+            bv[k] = L.b[t[k]];
+            uw[k] = u[mw]; ue[k] = u[m + 1]; us[k] = u[ms]; un[k] = u[m + W];
+        }
+#pragma unroll
+        for (int k = 0; k < FB5; k++) {
+            if (b0[k] != -1) continue;
+            double d = bv[k] - ((bw[k] > 0 ? aw * uw[k] : 0.0) + (bn[k] > 0 ? an * un[k] : 0.0) +
+                                (bs[k] > 0 ? an * us[k] : 0.0) + (be[k] > 0 ? aw * ue[k] : 0.0));
+            b += d * d;
+        }
     }
     return team_sum(T, b, bb);
 }
@@ -700,7 +795,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     P.ng = c->nlev;
     // the coarsest levels whose e, r and mask fit together in CTA 0's shared-memory budget
     // run on chip; the finer ones use the whole grid
-    long long budget = 96 * 1024;
+    long long budget = 20 * 1024;  // levels of 32^2 nodes and coarser (measured best at 2048^2)
     if (const char *e = getenv("LEPIC_MX_SMEM")) budget = atoll(e);
     auto level_bytes = [&](int l) {
         const long long nn = (long long)(c->lev[l].nx + 3) * (c->lev[l].ny + 3);
@@ -724,7 +819,9 @@ int mg_mixed_solve(lepic_ctx *c, double eps) {
     }
     P.Ls = Ls;
     P.omega = 1.0f;
-    P.nu1 = 2; P.nu2 = 2; P.nuc = 8; P.max_iter = 200;
+    // three sweeps before and after the coarse correction: a warm 2048^2 solve needs 3 CG
+    // iterations instead of 5 with two, and an iteration costs 1.3x as much
+    P.nu1 = 3; P.nu2 = 3; P.nuc = 8; P.max_iter = 200;
     if (const char *e = getenv("LEPIC_MX_NUC")) P.nuc = atoi(e);
     if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
     if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
