@@ -279,6 +279,21 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
         for (int base = s_start; base < end; base += PUSH_G * PUSH_THREADS) { // uniform trip count
             const int g = base + PUSH_G * threadIdx.x;
             const bool grp_ok = g < end;
+            // the CTA's next iteration of the five arrays into L2 with bulk (TMA) prefetches, so
+            // its vector loads meet L2 instead of HBM latency (push 3.76 -> 3.57 ms per step on
+            // the 2048^2 bench; staging the stream in shared memory through mbarriers measured
+            // 3.83, per-thread prefetches 3.58)
+            if (MOVE && threadIdx.x == 0) {
+                const int bn = base + PUSH_G * PUSH_THREADS;
+                if (bn < end) {
+                    const uint32_t nb = (uint32_t)((min(PUSH_G * PUSH_THREADS, end - bn) + 7) & ~7) * 4u;
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.X + bn), "r"(nb) : "memory");
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.Y + bn), "r"(nb) : "memory");
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VX + bn), "r"(nb) : "memory");
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VY + bn), "r"(nb) : "memory");
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VZ + bn), "r"(nb) : "memory");
+                }
+            }
             uint32_t X[PUSH_G], Y[PUSH_G];
             float vx[PUSH_G], vy[PUSH_G], vz[PUSH_G];
             if (grp_ok) {   // storage is whole groups of 8: the last, partial group is masked below
