@@ -4,8 +4,10 @@
 // ic = (ix-1) + nx*(iy-1) + 1, original order kept inside a cell.  Here:
 //   1. keys + histogram        (warp-aggregated atomics on the per-key counts)
 //   2. exclusive scan           (three-phase, fixed order)
-//   3. scatter of slot indices  (atomics: order inside a key is not yet defined)
-//   4. per-key segment sort of the slot indices (bitonic, ascending) -> stable again
+//   3. scatter of slot indices  (atomics; each warp takes a contiguous chunk in slot order, so
+//                               a key comes out of order only where it straddles chunks)
+//   4. per-key segment sort of the slot indices (bitonic, ascending; segments already in
+//      order are skipped) -> stable again
 //   5. gather of the 5 SoA fields into the other buffer, holes dropped
 //   6. push work list: per tile, chunks of CHUNK particles
 // so the result is bit-identical to the reference's, independent of thread timing.
@@ -31,23 +33,42 @@ __device__ __forceinline__ int cell_key(const KeyP &K, uint32_t X, uint32_t Y) {
 }
 
 // the key pass also takes the loss holes of the pushes since the last sort into the tallies
-// (the sort drops the holes)
+// (the sort drops the holes).  Four consecutive slots per thread: one 16-byte load per array
+// (storage is whole groups of 8 slots), so each thread has its loads in flight together;
+// equal keys of a warp add their count with one atomic.
 __global__ void k_keys_hist(KeyP K, const uint32_t *X, const uint32_t *Y, const float *VX, const float *VY,
                             const float *VZ, const int32_t *bcnd, TallyDev *tal, const DevCounters *cnt, int sp,
                             int *keys, int *counts) {
     const long long n = cnt->n_slots[sp];
-    const unsigned lane = threadIdx.x & 31;
-    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
-        long long i = i0 + threadIdx.x;
-        int key = -1;
-        if (i < n) {
-            const float vx = VX[i];
-            if (!isnan(vx)) key = cell_key(K, X[i], Y[i]);
-            else loss_hole_tally(tal, sp, bcnd, vx, X[i], Y[i], VY[i], VZ[i]);
+    const long long ng = (n + 3) / 4;
+    for (long long g0 = blockIdx.x * (long long)blockDim.x; g0 < ng; g0 += (long long)gridDim.x * blockDim.x) {
+        const long long g = g0 + threadIdx.x;
+        int key[4] = {-1, -1, -1, -1};
+        if (g < ng) {
+            const long long i = 4 * g;
+            const uint4 x = *reinterpret_cast<const uint4 *>(X + i);
+            const uint4 y = *reinterpret_cast<const uint4 *>(Y + i);
+            const float4 v = *reinterpret_cast<const float4 *>(VX + i);
+            const uint32_t xs[4] = {x.x, x.y, x.z, x.w}, ys[4] = {y.x, y.y, y.z, y.w};
+            const float vs[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                if (i + p >= n) break;
+                if (!isnan(vs[p])) key[p] = cell_key(K, xs[p], ys[p]);
+                else loss_hole_tally(tal, sp, bcnd, vs[p], xs[p], ys[p], VY[i + p], VZ[i + p]);
+            }
+            if (i + 4 <= n) {
+                *reinterpret_cast<int4 *>(keys + i) = make_int4(key[0], key[1], key[2], key[3]);
+            } else {
+                for (int p = 0; p < 4 && i + p < n; p++) keys[i + p] = key[p];
+            }
         }
-        if (i < n) keys[i] = key;
-        unsigned m = __match_any_sync(0xffffffffu, key);
-        if (key >= 0 && lane == (unsigned)(__ffs(m) - 1)) atomicAdd(&counts[key], __popc(m));
+        const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const unsigned m = __match_any_sync(0xffffffffu, key[p]);
+            if (key[p] >= 0 && lane == (unsigned)(__ffs(m) - 1)) atomicAdd(&counts[key[p]], __popc(m));
+        }
     }
 }
 
@@ -118,18 +139,28 @@ __global__ void k_scan_final(const int *counts, long long n, const int *blocksum
     }
 }
 
+// Each warp scatters a contiguous chunk of SCATTER_CHUNK slots in slot order, so inside a chunk
+// the slots of a key reach their segment in ascending order; only a key whose slots straddle
+// chunks can come out of order (the segment sort below checks every segment and sorts those).
+#define SCATTER_CHUNK 1024
 __global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *cursor, int *perm) {
     const long long n = cnt->n_slots[sp];
     const unsigned lane = threadIdx.x & 31;
-    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
-        long long i = i0 + threadIdx.x;
-        int key = (i < n) ? keys[i] : -1;
-        unsigned m = __match_any_sync(0xffffffffu, key);
-        int leader = __ffs(m) - 1;
-        int base = 0;
-        if (key >= 0 && (int)lane == leader) base = atomicAdd(&cursor[key], __popc(m));
-        base = __shfl_sync(m, base, leader);
-        if (key >= 0) perm[base + __popc(m & ((1u << lane) - 1u))] = (int)i;
+    const long long nchunks = (n + SCATTER_CHUNK - 1) / SCATTER_CHUNK;
+    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c = gw; c < nchunks; c += nw) {
+        const long long c1 = min((c + 1) * SCATTER_CHUNK, n);
+        for (long long i0 = c * SCATTER_CHUNK; i0 < c1; i0 += 32) {
+            const long long i = i0 + lane;
+            const int key = (i < c1) ? keys[i] : -1;
+            const unsigned m = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (key >= 0 && (int)lane == leader) base = atomicAdd(&cursor[key], __popc(m));
+            base = __shfl_sync(m, base, leader);
+            if (key >= 0) perm[base + __popc(m & ((1u << lane) - 1u))] = (int)i;
+        }
     }
 }
 
@@ -169,6 +200,11 @@ __global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, i
         if (n <= 64) {   // the common case: in registers, no shared memory
             int v0 = lane < n ? perm[s0 + lane] : INT_MAX;
             int v1 = lane + 32 < n ? perm[s0 + lane + 32] : INT_MAX;
+            // already ascending (the chunked scatter leaves most segments so): nothing to do
+            const int n0 = __shfl_down_sync(0xffffffffu, v0, 1), n1 = __shfl_down_sync(0xffffffffu, v1, 1);
+            const int f1 = __shfl_sync(0xffffffffu, v1, 0);
+            const bool ok = (lane == 31 ? v0 <= f1 : v0 <= n0) && (lane == 31 || v1 <= n1);
+            if (__all_sync(0xffffffffu, ok)) continue;
             warp_sort64(v0, v1, lane);
             if (lane < n) perm[s0 + lane] = v0;
             if (lane + 32 < n) perm[s0 + lane + 32] = v1;
