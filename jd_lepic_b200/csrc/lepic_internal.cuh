@@ -49,6 +49,7 @@ struct DevCounters {
     int n_items[LEPIC_MAXSP];
     unsigned int prod_count[LEPIC_MAXSP]; // products waiting for the ordered append
     int n_big;                            // sort: segments too long for one warp
+    unsigned int n_cand_list;             // collisions: candidates of the species being treated
     int err;
     int err_where;
     // multigrid results

@@ -17,8 +17,9 @@
 // a second kernel sorts each list by key and appends it after the occupied slots, so the
 // particle order after a collision step is deterministic.
 //
-// Roofline: the selection pass generates one Philox block per 4 slots and reads nothing;
-// only candidates (N*Pmax, about 0.3 % of particles) read and write their 20 B record.
+// Roofline: the selection pass generates one Philox block per 4 slots and reads nothing (it
+// writes the candidate list); only candidates (N*Pmax, about 0.3 % of particles) read and
+// write their 20 B record, one candidate per thread.
 #include <algorithm>
 #include "rho.cuh"
 
@@ -371,20 +372,52 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
 // nu_max (charged targets: it depends on the densities, collisions.f90:98-117)
 __device__ __forceinline__ double step_nu_max(const MccP &P) { return P.dsmc ? P.nu_max_d[P.sp] : P.nu_max; }
 
-__global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P) {
+// Selection: every slot's uniform against Pmax (one Philox block per 4 slots); the candidates
+// are compacted into a list (one atomic per warp).  The list's order does not matter: every
+// draw of a collision is keyed by its slot, a DSMC target goes to the smallest claiming slot,
+// and products are sorted before they are appended.
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc_select(MccP P, int *cand) {
     const long long n = P.cnt->n_slots[P.sp];
-    const double nu_max = step_nu_max(P), Pmax = P.dsmc ? nu_max * P.ns_coll_dt : P.Pmax;
-    unsigned int ncand = 0;
+    const double Pmax = P.dsmc ? step_nu_max(P) * P.ns_coll_dt : P.Pmax;
+    const unsigned lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x * 4;
-    for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * 4; base < n; base += stride) {
-        U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
-        uint32_t v[4] = {r.x, r.y, r.z, r.w};
+    for (long long base0 = blockIdx.x * (long long)blockDim.x * 4; base0 < n; base0 += stride) {  // uniform trip count
+        const long long base = base0 + 4 * (long long)threadIdx.x;
+        unsigned mask = 0;
+        if (base < n) {
+            const U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
+            const uint32_t v[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            long long slot = base + q;
-            if (slot < n && u01(v[q]) < Pmax) collide_one(P, slot, nu_max, &ncand);
+            for (int q = 0; q < 4; q++)
+                if (base + q < n && u01(v[q]) < Pmax) mask |= 1u << q;
         }
+        const int c = __popc(mask);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned wbase = 0;
+        if (lane == 31 && total) wbase = atomicAdd(&P.cnt->n_cand_list, (unsigned)total);
+        wbase = __shfl_sync(0xffffffffu, wbase, 31);
+        const long long off = (long long)wbase + incl - c;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if ((mask >> q) & 1u) cand[off + __popc(mask & ((1u << q) - 1u))] = (int)(base + q);
     }
+}
+
+// The collisions of the listed candidates, one per thread: a candidate runs the whole of
+// collision_OMP (target draw, interval search, scattering), which on a warp of slots where
+// one in ~300 is a candidate would run with one lane active.
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P, const int *cand) {
+    const long long m = P.cnt->n_cand_list;
+    const double nu_max = step_nu_max(P);
+    unsigned int ncand = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        collide_one(P, cand[i], nu_max, &ncand);
     for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(0xffffffffu, ncand, o);
     if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&P.cnt->n_cand[P.sp], (unsigned long long)ncand);
 }
@@ -392,26 +425,20 @@ __global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P) {
 // DSMC claims: every candidate of this step picks its charged targets as collide_one will and
 // claims them with the smallest incident slot, so that a target takes part in one collision
 // of the step (the winner is independent of the order the threads run in).
-__global__ void __launch_bounds__(MCC_THREADS) k_mcc_claim(MccP P) {
-    const long long n = P.cnt->n_slots[P.sp];
-    const double Pmax = step_nu_max(P) * P.ns_coll_dt;
-    const long long stride = (long long)gridDim.x * blockDim.x * 4;
-    for (long long base = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * 4; base < n; base += stride) {
-        U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
-        uint32_t v[4] = {r.x, r.y, r.z, r.w};
-        for (int q = 0; q < 4; q++) {
-            const long long slot = base + q;
-            if (slot >= n || !(u01(v[q]) < Pmax) || isnan(P.VX[slot])) continue;
-            const int cx = (int)(P.X[slot] >> P.S), cy = (int)(P.Y[slot] >> P.S);
-            unsigned done = 0;
-            for (int k = 0; k < P.ncol_sp; k++) {
-                const int *ci = P.col_info + P.cols[k] * 10;
-                const int tt = ci[2 + ci[0] - 1];
-                if (P.charge[tt] == 0.0 || tt == P.sp || (done & (1u << tt))) continue;
-                done |= 1u << tt;
-                const long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
-                if (t >= 0) atomicMin(P.claim[tt] + t, (int)slot);
-            }
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc_claim(MccP P, const int *cand) {
+    const long long m = P.cnt->n_cand_list;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const long long slot = cand[i];
+        if (isnan(P.VX[slot])) continue;
+        const int cx = (int)(P.X[slot] >> P.S), cy = (int)(P.Y[slot] >> P.S);
+        unsigned done = 0;
+        for (int k = 0; k < P.ncol_sp; k++) {
+            const int *ci = P.col_info + P.cols[k] * 10;
+            const int tt = ci[2 + ci[0] - 1];
+            if (P.charge[tt] == 0.0 || tt == P.sp || (done & (1u << tt))) continue;
+            done |= 1u << tt;
+            const long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
+            if (t >= 0) atomicMin(P.claim[tt] + t, (int)slot);
         }
     }
 }
@@ -547,6 +574,7 @@ int mcc_collide(lepic_ctx *c, int it) {
         SpeciesBuf &B = c->sp[s];
         MccP P;
         memset(&P, 0, sizeof(P));
+        bool claims = false;   // a charged target species of this incident gets DSMC claims
         P.sp = s; P.ntype = g.ntype;
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
         for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
@@ -583,20 +611,23 @@ int mcc_collide(lepic_ctx *c, int it) {
             P.np_red = c->np_red;
             P.nu_max_d = c->nu_max_d;
             P.ns_coll_dt = (double)g.ns_coll * g.dt;
-            bool any = false;
             for (int q = 0; q < c->p_ncol[s]; q++) {
                 const int t = c->hcol_tt[c->hsig_list[s * LEPIC_MAXCOL + q]];
                 if (t < g.ntype && g.charge[t] != 0.0 && t != s && c->sp[t].claim) {
                     LCUDA(cudaMemsetAsync(c->sp[t].claim, 0x7f, sizeof(int) * c->sp[t].cap, c->stream));
-                    any = true;
+                    claims = true;
                 }
             }
-            if (any) {
-                k_mcc_claim<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
-                LCUDA(cudaGetLastError());
-            }
         }
-        k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
+        // candidates (the sort's key buffer holds the list: one int per slot at most)
+        LCUDA(cudaMemsetAsync(&c->dcnt->n_cand_list, 0, sizeof(unsigned int), c->stream));
+        k_mcc_select<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P, c->keys);
+        LCUDA(cudaGetLastError());
+        if (c->dsmc && claims) {
+            k_mcc_claim<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P, c->keys);
+            LCUDA(cudaGetLastError());
+        }
+        k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P, c->keys);
         LCUDA(cudaGetLastError());
     }
     for (int t = 0; t < g.ntype; t++) {
