@@ -350,7 +350,12 @@ int lepic_gpu_source_tallies(lepic_ctx *ctx, lepic_source_tally *out, int32_t re
 /* ---- averaging diagnostics ------------------------------------------------------------
  * part_moments (utils.f90:1-131) + calc_avg (utils.f90:133-266) + the potential and field
  * averages (main.f90:935-947) on the device, so the averages need no host transfer until the
- * host writes them.  The source/sink columns of data_pavg (6, 7: ss2D) stay zero. */
+ * host writes them.  While averaging is configured the device also keeps ss2D with the
+ * reference's default plt_src = 0: per species and node a count of macroparticles made
+ * (injection, part_injection.f90:205; emission, part_flux_emitter.f90:175; collision
+ * products, collisions.f90:809) and removed (wall losses at the nearest node,
+ * part_expmover.f90:327-332; collision removals, collisions.f90:931); each sample adds them
+ * times Nm/Vc to data_pavg's source/sink columns (6, 7) and zeroes them (main.f90:929-931). */
 /* Allocates (or re-allocates and zeroes) the averages on the coarse grid na = n / size_na
  * (read_input.f90:109-111); navg > 0 makes lepic_gpu_step take one sample when
  * MOD(it,navg) == 1, after the sort (main.f90:906). */
@@ -360,6 +365,9 @@ int lepic_gpu_calc_avg(lepic_ctx *ctx);
 /* Reads data_pavg(7, na1+1, na2+1, ntype) and phi_avg(3, 0:nx+2, 0:ny+2) (each nullable) and
  * the sample count cnt_avg; reset != 0 zeroes them afterwards (main.f90:1290-1296). */
 int lepic_gpu_get_avg(lepic_ctx *ctx, double *data_pavg, double *phi_avg, int32_t *cnt_avg, int32_t reset);
+/* Reads the current ss2D(2, 0:nx+2, 0:ny+2, ntype) counts (one rank; synchronises).  Replaces
+ * the host's copy of ss2D between calc_avg calls (main.f90:90, 209, 242, 931). */
+int lepic_gpu_get_source_maps(lepic_ctx *ctx, double *ss2D);
 
 /* Loss, power and collision tallies, cumulative since the context was created or the last
  * reset: part_mover's p_mac and P_loss(1) (part_expmover.f90:316-427), collisions' P_loss(3)

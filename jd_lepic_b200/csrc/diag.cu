@@ -12,6 +12,7 @@
 // Roofline: 20 B per particle read (X, Y, VX, VY, VZ) per averaging sample, every navg steps.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 #include "rho.cuh"
 
 struct AvgState {
@@ -132,6 +133,8 @@ struct AvgP {
     const double *p_mts;
     double *data;        // data_pavg(7, na1+1, na2+1, ntype)
     double m_over_qe;
+    const unsigned int *ss_src, *ss_sink;   // this species' ss2D counts (plt_src = 0)
+    double k_ss;                            // Nm / Vc, Vc = dx dy zmax (utils.f90:168, 200-204)
 };
 
 __global__ void k_calc_avg(AvgP P) {
@@ -152,6 +155,9 @@ __global__ void k_calc_avg(AvgP P) {
         double Tp = 0.0;
         if (np_ > 0) Tp = P.m_over_qe * (1.0 / 3.0) * (p1 / np_ - (jx * jx + jy * jy + jz * jz) / (np_ * np_));
         if (Tp > 0) d[1] += Tp;  // :251 (corners, few particles)
+        const long long f = ixf + (long long)iyf * (P.R.nx + 3);   // sour_avg, sink_avg (:200-204)
+        d[5] += (double)P.ss_src[f] * P.k_ss;
+        d[6] += (double)P.ss_sink[f] * P.k_ss;
     }
 }
 
@@ -167,6 +173,7 @@ __global__ void k_phi_avg(const double *phi, const double2 *E, long long nn, dou
 }
 
 void avg_free(lepic_ctx *c) {
+    if (c->ss_map) { cudaFree(c->ss_map); c->ss_map = nullptr; }
     AvgState *A = avg_state(c);
     if (!A) return;
     if (A->p_mts) cudaFree(A->p_mts);
@@ -192,13 +199,15 @@ extern "C" int lepic_gpu_set_avg(lepic_ctx *c, int32_t size_na, int32_t navg) {
     const size_t nd = (size_t)7 * (A->na1 + 1) * (A->na2 + 1) * g.ntype;
     if (cudaMalloc((void **)&A->p_mts, sizeof(double) * 4 * A->ncell * g.ntype) != cudaSuccess ||
         cudaMalloc((void **)&A->data, sizeof(double) * nd) != cudaSuccess ||
-        cudaMalloc((void **)&A->phi_avg, sizeof(double) * 3 * c->nn) != cudaSuccess) {
+        cudaMalloc((void **)&A->phi_avg, sizeof(double) * 3 * c->nn) != cudaSuccess ||
+        cudaMalloc((void **)&c->ss_map, sizeof(unsigned int) * 2 * g.ntype * c->nn) != cudaSuccess) {
         avg_free(c);
         c->last_err = "set_avg: cudaMalloc failed";
         return LEPIC_ENOMEM;
     }
     LCUDA(cudaMemsetAsync(A->data, 0, sizeof(double) * nd, c->stream));
     LCUDA(cudaMemsetAsync(A->phi_avg, 0, sizeof(double) * 3 * c->nn, c->stream));
+    LCUDA(cudaMemsetAsync(c->ss_map, 0, sizeof(unsigned int) * 2 * g.ntype * c->nn, c->stream));
     LCUDA(cudaStreamSynchronize(c->stream));
     return LEPIC_OK;
 }
@@ -233,9 +242,14 @@ int avg_sample(lepic_ctx *c) {
         P.p_mts = A->p_mts + (size_t)4 * A->ncell * s;
         P.data = A->data;
         P.m_over_qe = g.mass[s] / g.qe;
+        P.ss_src = c->ss_map + (size_t)(2 * s) * c->nn;
+        P.ss_sink = c->ss_map + (size_t)(2 * s + 1) * c->nn;
+        P.k_ss = g.Nm[s] / (g.dx * g.dy * g.zmax);
         k_calc_avg<<<(int)std::min<long long>(div_up(nodes, 256), (long long)c->num_sms * 8), 256, 0, c->stream>>>(P);
         LCUDA(cudaGetLastError());
     }
+    // main.f90:931: the counts start again after each sample
+    LCUDA(cudaMemsetAsync(c->ss_map, 0, sizeof(unsigned int) * 2 * g.ntype * c->nn, c->stream));
     k_phi_avg<<<(int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 8), 256, 0, c->stream>>>(
         c->phi, c->Ed, c->nn, A->phi_avg);
     LCUDA(cudaGetLastError());
@@ -261,6 +275,22 @@ extern "C" int lepic_gpu_get_avg(lepic_ctx *c, double *data_pavg, double *phi_av
         A->cnt = 0;
     }
     return lepic_gpu_sync(c);
+}
+
+// ss2D(2, 0:nx+2, 0:ny+2, ntype) of one rank as the reference holds it between samples
+extern "C" int lepic_gpu_get_source_maps(lepic_ctx *c, double *ss2D) {
+    if (!c || !ss2D) return LEPIC_EINVAL;
+    if (!c->ss_map) { c->last_err = "source maps need lepic_gpu_set_avg"; return LEPIC_EINVAL; }
+    const int nt = c->cfg.ntype;
+    const long long nn = c->nn;
+    std::vector<unsigned int> h((size_t)2 * nt * nn);
+    LCUDA(cudaMemcpyAsync(h.data(), c->ss_map, sizeof(unsigned int) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    int r = lepic_gpu_sync(c);
+    if (r) return r;
+    for (int s = 0; s < nt; s++)
+        for (long long n = 0; n < nn; n++)
+            for (int k = 0; k < 2; k++) ss2D[k + 2 * (n + nn * s)] = (double)h[(size_t)(2 * s + k) * nn + n];
+    return LEPIC_OK;
 }
 
 int avg_step(lepic_ctx *c, int it) {

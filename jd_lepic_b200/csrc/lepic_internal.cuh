@@ -169,6 +169,10 @@ struct lepic_ctx {
     void *src = nullptr;
     // averaging diagnostics (diag.cu), created by lepic_gpu_set_avg
     void *avg = nullptr;
+    // ss2D with plt_src = 0: per species a source and a sink count per node, [(2 sp + k) nn
+    // + node], k = 0 source, 1 sink; accumulated between averaging samples while averaging is
+    // configured (null otherwise)
+    unsigned int *ss_map = nullptr;
     // counters
     DevCounters *dcnt = nullptr;
     TallyDev *tally = nullptr;

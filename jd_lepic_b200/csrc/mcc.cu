@@ -28,6 +28,9 @@
 
 struct MccP {
     int sp, ntype;
+    unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
+    long long ss_nn;
+    int ss_W;
     uint32_t *X, *Y;
     float *VX, *VY, *VZ;
     Product *prod[LEPIC_MAXSP];
@@ -335,6 +338,8 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             incident_kept = true;
             P.VX[slot] = (float)vbx; P.VY[slot] = (float)vby; P.VZ[slot] = (float)vbz;
         } else {
+            if (P.ss_map)   // collisions.f90:809: a created particle at the incident's (ix, iy)
+                atomicAdd(P.ss_map + (size_t)(2 * bt) * P.ss_nn + ((X >> P.S) + 1) + (long long)((Y >> P.S) + 1) * P.ss_W, 1u);
             unsigned int k = atomicAdd(&P.cnt->prod_count[bt], 1u);
             if ((int)k < P.prod_cap[bt]) {
                 Product pr;
@@ -355,6 +360,9 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
         if (ct == sp && !incident_kept && ire == 0) {
             atomicAdd(&P.tal->P3[sp], -P.Ek_half[sp] * v2in);  // removal in the mover (part_expmover.f90:91-95)
             P.VX[slot] = __int_as_float(HOLE_NAN);
+            if (P.ss_map)   // collisions.f90:931: the removed particle, at the incident's (ix, iy)
+                atomicAdd(P.ss_map + (size_t)(2 * sp + 1) * P.ss_nn + ((P.X[slot] >> P.S) + 1) +
+                              (long long)((P.Y[slot] >> P.S) + 1) * P.ss_W, 1u);
             atomicAdd(&P.cnt->n_dead[sp], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
         }
@@ -362,6 +370,9 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             const long long t = tslot[tt];  // a charged target that is not a byproduct dies (:921-930)
             atomicAdd(&P.tal->P3[tt], -P.Ek_half[tt] * v2f(P.TVX[tt][t], P.TVY[tt][t], P.TVZ[tt][t]));
             P.TVX[tt][t] = __int_as_float(HOLE_NAN);
+            if (P.ss_map)
+                atomicAdd(P.ss_map + (size_t)(2 * tt + 1) * P.ss_nn + ((P.X[slot] >> P.S) + 1) +
+                              (long long)((P.Y[slot] >> P.S) + 1) * P.ss_W, 1u);
             atomicAdd(&P.cnt->n_dead[tt], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[tt], (unsigned long long)-1ll);
         }
@@ -576,6 +587,7 @@ int mcc_collide(lepic_ctx *c, int it) {
         memset(&P, 0, sizeof(P));
         bool claims = false;   // a charged target species of this incident gets DSMC claims
         P.sp = s; P.ntype = g.ntype;
+        P.ss_map = c->ss_map; P.ss_nn = c->nn; P.ss_W = g.nx + 3;
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
         for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
         P.cnt = c->dcnt;

@@ -32,6 +32,7 @@ struct PushP {
     float scx, scy, scz;       // rotation, k2 = 2 k1 / (1 + k1^2 |B|^2)
     const uint8_t *cellwall;
     unsigned long long *acc;
+    unsigned int *ss_sink;     // this species' ss2D sink counts (null: not accumulated)
     const WorkItem *items;
     DevCounters *cnt;
     int sp;
@@ -210,6 +211,12 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     if (GEN && !is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
     if (is_lost) {
         lost++;
+        if (P.ss_sink) {   // ss2D sink at the node nearest the loss point (part_expmover.f90:327-332)
+            const long long hf = 1ll << (P.S - 1);
+            const int ixw = min(max((int)((Xn + hf) >> P.S) + 1, 0), P.nx + 1);
+            const int iyw = min(max((int)((Yn + hf) >> P.S) + 1, 0), P.ny + 1);
+            atomicAdd(P.ss_sink + ixw + (long long)iyw * P.W, 1u);
+        }
         // the slot becomes a hole that keeps its loss for the tallies (lepic_internal.cuh,
         // loss_hole_tally): X = the loss cell's node, Y = the new vx, VY, VZ = the new vy, vz,
         // VX = a NaN whose payload marks a fresh wall loss (1) or another loss (2)
@@ -450,6 +457,7 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         }
         P.cellwall = c->cellwall;
         P.acc = B.acc;
+        P.ss_sink = c->ss_map ? c->ss_map + (size_t)(2 * s + 1) * c->nn : nullptr;
         P.items = B.items;
         P.cnt = c->dcnt;
         P.sp = s;

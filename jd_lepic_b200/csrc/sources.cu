@@ -422,6 +422,8 @@ struct InjP {
     uint32_t *X[LEPIC_MAXSP], *Y[LEPIC_MAXSP];
     float *VX[LEPIC_MAXSP], *VY[LEPIC_MAXSP], *VZ[LEPIC_MAXSP];
     unsigned long long *acc[LEPIC_MAXSP];
+    unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
+    long long ss_nn;
     uint32_t it, k0, k1;
 };
 
@@ -545,6 +547,8 @@ __global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
         const float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
         P.X[s][slot] = Xf; P.Y[s][slot] = Yf;
         P.VX[s][slot] = fvx; P.VY[s][slot] = fvy; P.VZ[s][slot] = fvz;
+        if (P.ss_map)   // part_injection.f90:205: the source at the particle's (ix, iy)
+            atomicAdd(P.ss_map + (size_t)(2 * s) * P.ss_nn + ix + (long long)iy * P.W, 1u);
         // deposit (the injected particle is in this step's np)
         uint64_t w[4];
         inj_cic(P.S, Xf, Yf, w);
@@ -590,6 +594,8 @@ struct EmitP {
     uint32_t *X[2], *Y[2];
     float *VX[2], *VY[2], *VZ[2];
     long long max_attempts_extra;
+    unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
+    long long ss_nn;
     uint32_t it, k0, k1;
 };
 
@@ -631,7 +637,7 @@ __global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
     for (long long base = 0; s_tot < Nh && base < max_att; base += EMIT_THREADS) {
         const long long a = base + threadIdx.x;
         bool wall = false, lh = false, rh = false;
-        int q = 0;
+        int q = 0, eix = 0, eiy = 0;   // the attempt's node (ix, iy)
         double x = P.xg1, y = 0.0, th = pi / 2.0;
         if (a < max_att) {
             const U4 r = philox4x32_10(U4{(uint32_t)a, (uint32_t)(a >> 32), TAG_FXP, P.it}, P.k0, P.k1);
@@ -648,6 +654,7 @@ __global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
             if (P.chamfer && ((y <= h2 && y > P.y1c) || (y > h2 && fabs(P.ymax - y) > P.y1c)))
                 th = y > h2 ? pi / 2.0 + P.th_c : P.th_c;
             const int ix = (int)(x / P.dx) + 1, iy = (int)(y / P.dy) + 1;
+            eix = ix; eiy = iy;
             if (ix >= 1 && ix <= P.nx + 1 && iy >= 1 && iy <= P.ny + 1) {  // INT truncates toward 0
                 const int32_t *b = P.bcnd;
                 const long long m = ix + (long long)iy * P.W;
@@ -667,6 +674,8 @@ __global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
         const long long idx0 = (j - s_tot) - idx1;      // accepted before it with qe == 0
         if (acc && j < Nh) {
             const long long slot = s_start[qe] + s_n[qe] + (qe ? idx1 : idx0);
+            if (P.ss_map)   // part_flux_emitter.f90:175: the source at the attempt's (ix, iy)
+                atomicAdd(P.ss_map + (size_t)(2 * P.sp[qe]) * P.ss_nn + eix + (long long)eiy * P.W, 1u);
             const U4 v = philox4x32_10(U4{(uint32_t)j, (uint32_t)(j >> 32), TAG_FXV, P.it}, P.k0, P.k1);
             const double vt = P.vt[qe];
             const double vx = dir * vt * sqrt(-log(1.0 - u01(v.x)));
@@ -949,6 +958,7 @@ static int run_injection(lepic_ctx *c, int it) {
         P.acc[sp] = B.acc;
     }
     P.cellwall = c->cellwall;
+    P.ss_map = c->ss_map; P.ss_nn = c->nn;
     P.phi = c->phi;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);
@@ -996,6 +1006,7 @@ static int run_emitter(lepic_ctx *c, int it) {
         P.VX[q] = B.VX[B.cur]; P.VY[q] = B.VY[B.cur]; P.VZ[q] = B.VZ[B.cur];
     }
     P.bcnd = c->bcnd;
+    P.ss_map = c->ss_map; P.ss_nn = c->nn;
     P.max_attempts_extra = 65536;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);

@@ -59,7 +59,8 @@ void o_part_moments(const o_cfg *c, int size_na, int ptype, const double *vxp, i
 
 /* calc_avg for ptype: npg is that species' np(0:nx+2, 0:ny+2); data_pavg(7, na1+1, na2+1,
  * ntype) accumulates (utils.f90:176-262; the ss2D columns 6, 7 are not formed) */
-void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const double *p_mts, double *data_pavg) {
+void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const double *p_mts, double *data_pavg,
+                const double *ss_src, const double *ss_sink) {
     const int na1 = c->nx / size_na, na2 = c->ny / size_na;
     const int64_t ncell = (int64_t)(na1 + 3) * (na2 + 3);
     const int64_t nodes = (int64_t)(na1 + 1) * (na2 + 1);
@@ -78,5 +79,10 @@ void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const
             double Tp = 0.0;
             if (np_ > 0) Tp = c->mass[ptype] / c->qe * (1.0 / 3.0) * (p1 / np_ - (jx * jx + jy * jy + jz * jz) / (np_ * np_));
             if (Tp > 0) d[1] += Tp;
+            if (ss_src) { /* utils.f90:200-204, plt_src = 0: counts times Nm/Vc at the fine node */
+                const double k = c->Nm[ptype] / (c->dx * c->dy * c->zmax);
+                d[5] += ss_src[ixf + (int64_t)iyf * W] * k;
+                d[6] += ss_sink[ixf + (int64_t)iyf * W] * k;
+            }
         }
 }

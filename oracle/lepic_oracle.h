@@ -222,7 +222,9 @@ int o_part_flux_emitter_ctr(const o_cfg *c, const o_emit *e, const int32_t *bcnd
 void o_part_moments(const o_cfg *c, int size_na, int ptype, const double *vxp, int64_t n, const double *kq,
                     double *p_mts);
 /* calc_avg (utils.f90:133-266) for one species: npg its np(0:nx+2, 0:ny+2); accumulates
- * data_pavg(7, na1+1, na2+1, ntype). */
-void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const double *p_mts, double *data_pavg);
+ * data_pavg(7, na1+1, na2+1, ntype).  ss_src, ss_sink (nullable): the species' ss2D counts on
+ * the (nx+3)(ny+3) nodes for the source/sink columns (plt_src = 0). */
+void o_calc_avg(const o_cfg *c, int size_na, int ptype, const double *npg, const double *p_mts, double *data_pavg,
+                const double *ss_src, const double *ss_sink);
 
 #endif

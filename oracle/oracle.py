@@ -160,7 +160,7 @@ def lib() -> C.CDLL:
         L.o_part_flux_emitter_ctr.argtypes = [C.POINTER(OCfg), C.POINTER(OEmit), _IP, C.c_uint64, C.c_int32, C.c_int,
                                               C.POINTER(_DP), _LP, _LP, _LP, _DP, _LP]
         L.o_part_moments.argtypes = [C.POINTER(OCfg), C.c_int, C.c_int, _DP, C.c_int64, _DP, _DP]
-        L.o_calc_avg.argtypes = [C.POINTER(OCfg), C.c_int, C.c_int, _DP, _DP, _DP]
+        L.o_calc_avg.argtypes = [C.POINTER(OCfg), C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP]
         _lib = L
     return _lib
 
@@ -535,6 +535,11 @@ def part_moments(cfg, size_na, ptype, vxp, kq):
     return p
 
 
-def calc_avg(cfg, size_na, ptype, npg, p_mts, data_pavg):
-    """data_pavg: (ntype, na2+1, na1+1, 7) array, accumulated in place."""
-    lib().o_calc_avg(C.byref(cfg), size_na, ptype, dp(np.ascontiguousarray(npg)), dp(p_mts), dp(data_pavg))
+def calc_avg(cfg, size_na, ptype, npg, p_mts, data_pavg, ss=None):
+    """data_pavg: (ntype, na2+1, na1+1, 7) array, accumulated in place; ss: the species'
+    (2, ny+3, nx+3) source and sink counts (or None)."""
+    src = sink = None
+    if ss is not None:
+        src, sink = (np.ascontiguousarray(ss[k], dtype=np.float64) for k in (0, 1))
+    lib().o_calc_avg(C.byref(cfg), size_na, ptype, dp(np.ascontiguousarray(npg)), dp(p_mts), dp(data_pavg),
+                     dp(src), dp(sink))
