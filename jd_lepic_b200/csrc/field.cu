@@ -74,20 +74,23 @@ int field_np_grid(lepic_ctx *c, int ptype, double *d_out) {
 
 // ---------------------------------------------------------------------------------------
 // Efield.f90:1-128.
-// Pass 1 (:19-34): central differences at nodes with bcnd <= 0.
+// Pass 1 (:19-34): central differences at nodes with bcnd <= 0, into the scratch field E;
+// every other node (walls, ghosts) takes the current field's value, which the reference's
+// in/out Ei holds there when the wall pass reads it.
 __global__ void k_efield_interior(int nx, int ny, double h1, double h2, const double *phi,
-                                  const int8_t *bc, double2 *E) {
+                                  const int8_t *bc, const double2 *Ecur, double2 *E) {
     const int W = nx + 3;
-    const long long tot = (long long)(nx + 1) * (ny + 1);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x) {
-        int ix = (int)(t % (nx + 1)) + 1, iy = (int)(t / (nx + 1)) + 1;
-        long long n = ix + (long long)iy * W;
-        if (bc[n] <= 0) {
+    const long long nn = (long long)(nx + 3) * (ny + 3);
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn;
+         n += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(n % W), iy = (int)(n / W);
+        if (ix >= 1 && ix <= nx + 1 && iy >= 1 && iy <= ny + 1 && bc[n] <= 0) {
             double2 e;
             e.x = -(phi[n + 1] - phi[n - 1]) / (2.0 * h1);
             e.y = -(phi[n + W] - phi[n - W]) / (2.0 * h2);
             E[n] = e;
+        } else {
+            E[n] = Ecur[n];
         }
     }
 }
@@ -151,11 +154,10 @@ __global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *
 
 int field_calc_efield(lepic_ctx *c) {
     const int nx = c->cfg.nx, ny = c->cfg.ny;
-    long long tot = (long long)(nx + 1) * (ny + 1);
-    int grid = (int)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16);
-    // E (FP64) lives in Ed[0..nn); the second half is the wall-pass output.
-    double2 *E0 = c->Ed, *E1 = c->Ed + c->nn;
-    k_efield_interior<<<grid, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, E0);
+    int grid = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
+    // E (FP64) lives in Ed[0..nn); the second half holds pass 1, which the wall pass reads
+    double2 *E0 = c->Ed + c->nn, *E1 = c->Ed;
+    k_efield_interior<<<grid, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, E1, E0);
     if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the passes test the labels, as Efield.f90:43-82 does
         for (int part = 0; part < 2; part++)
             k_efield_nmn_pbc<<<div_up(std::max(nx, ny) + 2, 256), 256, 0, c->stream>>>(nx, ny, c->cfg.dy,
@@ -163,6 +165,5 @@ int field_calc_efield(lepic_ctx *c) {
     int grid2 = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
     k_efield_walls<<<grid2, 256, 0, c->stream>>>(nx, ny, c->bc8, E0, E1, c->Ef);
     LCUDA(cudaGetLastError());
-    LCUDA(cudaMemcpyAsync(E0, E1, sizeof(double2) * c->nn, cudaMemcpyDeviceToDevice, c->stream));
     return LEPIC_OK;
 }
