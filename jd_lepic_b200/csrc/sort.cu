@@ -151,15 +151,27 @@ __global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long c = gw; c < nchunks; c += nw) {
         const long long c1 = min((c + 1) * SCATTER_CHUNK, n);
-        for (long long i0 = c * SCATTER_CHUNK; i0 < c1; i0 += 32) {
-            const long long i = i0 + lane;
-            const int key = (i < c1) ? keys[i] : -1;
-            const unsigned m = __match_any_sync(0xffffffffu, key);
-            const int leader = __ffs(m) - 1;
-            int base = 0;
-            if (key >= 0 && (int)lane == leader) base = atomicAdd(&cursor[key], __popc(m));
-            base = __shfl_sync(m, base, leader);
-            if (key >= 0) perm[base + __popc(m & ((1u << lane) - 1u))] = (int)i;
+        // four 32-slot steps at a time: their atomics are in flight together (issued in step
+        // order, so a key that runs across steps still receives ascending positions)
+        for (long long i0 = c * SCATTER_CHUNK; i0 < c1; i0 += 4 * 32) {
+            int key[4], base[4];
+            unsigned m[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const long long i = i0 + 32 * u + lane;
+                key[u] = (i < c1) ? keys[i] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                m[u] = __match_any_sync(0xffffffffu, key[u]);
+                base[u] = 0;
+                if (key[u] >= 0 && (int)lane == __ffs(m[u]) - 1) base[u] = atomicAdd(&cursor[key[u]], __popc(m[u]));
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int b = __shfl_sync(m[u], base[u], __ffs(m[u]) - 1);
+                if (key[u] >= 0) perm[b + __popc(m[u] & ((1u << lane) - 1u))] = (int)(i0 + 32 * u + lane);
+            }
         }
     }
 }
