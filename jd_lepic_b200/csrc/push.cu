@@ -10,9 +10,12 @@
 //            2^44) accumulated in a shared-memory uint64 window around the CTA's sort tile
 //            (plus a halo for particles that drifted since the sort); anything outside the
 //            window goes straight to the global uint64 grid.  Integer sums are associative,
-//            so the density is bit-reproducible whatever the atomic order.
+//            so the density is bit-reproducible whatever the atomic order.  A thread keeps a
+//            run of particles in one cell as its moments (count, sum fx, sum fy, sum fx fy)
+//            where those give the weights exactly, and adds each run once.
 // Work is dispensed dynamically: the sort's per-tile items first, then fixed-size chunks of
-// the unsorted tail (particles created by collisions since the sort).
+// the unsorted tail (particles created by collisions since the sort); each CTA prefetches its
+// next iteration of the stream into L2 with bulk copies.
 //
 // Roofline: 40 B per particle-step of algorithmic HBM traffic (X,Y,VX,VY,VZ read+write).
 #include <algorithm>
