@@ -27,8 +27,15 @@
 
 struct KeyP {
     int S, nx, ny, tw, th, ntx;
+    int twl, thl;   // log2 of tw and th when both are powers of two, else -1
 };
+// sort_cell_key, with shifts in place of the two divisions for power-of-two tiles (the same key)
 __device__ __forceinline__ int cell_key(const KeyP &K, uint32_t X, uint32_t Y) {
+    if (K.twl >= 0) {
+        const int cx = min(max((int)(X >> K.S), 0), K.nx - 1), cy = min(max((int)(Y >> K.S), 0), K.ny - 1);
+        const int tx = cx >> K.twl, ty = cy >> K.thl;
+        return (((ty * K.ntx + tx) << K.thl) + (cy & (K.th - 1))) * K.tw + (cx & (K.tw - 1));
+    }
     return sort_cell_key((int)(X >> K.S), (int)(Y >> K.S), K.nx, K.ny, K.tw, K.th, K.ntx);
 }
 
@@ -344,7 +351,9 @@ __global__ void k_items(const int *offsets, int ntiles, int keys_per_tile, WorkI
 int sort_species(lepic_ctx *c, int sp) {
     SpeciesBuf &B = c->sp[sp];
     const int cur = B.cur, nxt = 1 - cur;
-    KeyP K{c->S, c->cfg.nx, c->cfg.ny, c->tw, c->th, c->ntx};
+    auto log2_or = [](int v) { int l = 0; while ((1 << l) < v) l++; return (1 << l) == v ? l : -1; };
+    KeyP K{c->S, c->cfg.nx, c->cfg.ny, c->tw, c->th, c->ntx, log2_or(c->tw), log2_or(c->th)};
+    if (K.twl < 0 || K.thl < 0) K.twl = K.thl = -1;
     const long long nk = c->nkeys;
     int grid = c->num_sms * 8;
     LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
