@@ -365,9 +365,19 @@ int lepic_gpu_calc_avg(lepic_ctx *ctx);
 /* Reads data_pavg(7, na1+1, na2+1, ntype) and phi_avg(3, 0:nx+2, 0:ny+2) (each nullable) and
  * the sample count cnt_avg; reset != 0 zeroes them afterwards (main.f90:1290-1296). */
 int lepic_gpu_get_avg(lepic_ctx *ctx, double *data_pavg, double *phi_avg, int32_t *cnt_avg, int32_t reset);
-/* Reads the current ss2D(2, 0:nx+2, 0:ny+2, ntype) counts (one rank; synchronises).  Replaces
- * the host's copy of ss2D between calc_avg calls (main.f90:90, 209, 242, 931). */
+/* Reads the current ss2D(2, 0:nx+2, 0:ny+2, ntype) (one rank; synchronises): the counts with
+ * plt_src = 0, the densities of the last sample with plt_src = 1.  Replaces the host's copy of
+ * ss2D (main.f90:90, 209, 242, 921-931). */
 int lepic_gpu_get_source_maps(lepic_ctx *ctx, double *ss2D);
+/* plt_src (read_input.f90:113-117, a negative k_eps0 in the deck): 0 (default) counts made and
+ * removed macroparticles; 1 makes each averaging sample (lepic_gpu_calc_avg or the step's
+ * sample) first run collisions with flag_diag = 1 (collisions.f90:268-299, 546-600, 649): every
+ * particle through the collision frequencies of its reactions, no collision performed, the
+ * ionization, dissociation and charge-exchange frequencies times Nm/Vc deposited with CIC
+ * weights as source (charged byproducts) and sink (charged reactants that do not survive)
+ * densities, which calc_avg adds to data_pavg(6:7, ...) as they are (utils.f90:205-209); the
+ * region tallies cnt_col count that pass too, as the reference's do. */
+int lepic_gpu_set_source_option(lepic_ctx *ctx, int32_t plt_src);
 
 /* Loss, power and collision tallies, cumulative since the context was created or the last
  * reset: part_mover's p_mac and P_loss(1) (part_expmover.f90:316-427), collisions' P_loss(3)

@@ -40,6 +40,7 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
     F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed); F(c->Ef);
+    F(c->ss_diag);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
@@ -643,7 +644,7 @@ extern "C" int lepic_gpu_part_sorting(lepic_ctx *c, int32_t ptype, int32_t *plis
 
 extern "C" int lepic_gpu_collisions(lepic_ctx *c, int32_t it, lepic_mcc_stats *st) {
     if (!c) return LEPIC_EINVAL;
-    int r = mcc_collide(c, it);
+    int r = mcc_collide(c, it, false);
     if (r != LEPIC_OK) return r;
     if (st) return lepic_gpu_get_mcc_stats(c, st);
     return LEPIC_OK;
@@ -669,7 +670,7 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
             if ((r = sort_species(c, s)) != LEPIC_OK) return r;
     if ((r = avg_step(c, it)) != LEPIC_OK) return r;  // main.f90:906-949
     if (it > 1 && g.ns_coll > 0 && it % g.ns_coll == 1)
-        if ((r = mcc_collide(c, it)) != LEPIC_OK) return r;
+        if ((r = mcc_collide(c, it, false)) != LEPIC_OK) return r;
     if ((r = sources_before_push(c, it)) != LEPIC_OK) return r;
     if ((r = push_deposit(c, it, true)) != LEPIC_OK) return r;
     return sources_after_push(c, it);

@@ -135,6 +135,7 @@ struct AvgP {
     double m_over_qe;
     const unsigned int *ss_src, *ss_sink;   // this species' ss2D counts (plt_src = 0)
     double k_ss;                            // Nm / Vc, Vc = dx dy zmax (utils.f90:168, 200-204)
+    const double *ssd_src, *ssd_sink;       // this species' ss2D densities (plt_src = 1), or null
 };
 
 __global__ void k_calc_avg(AvgP P) {
@@ -155,9 +156,14 @@ __global__ void k_calc_avg(AvgP P) {
         double Tp = 0.0;
         if (np_ > 0) Tp = P.m_over_qe * (1.0 / 3.0) * (p1 / np_ - (jx * jx + jy * jy + jz * jz) / (np_ * np_));
         if (Tp > 0) d[1] += Tp;  // :251 (corners, few particles)
-        const long long f = ixf + (long long)iyf * (P.R.nx + 3);   // sour_avg, sink_avg (:200-204)
-        d[5] += (double)P.ss_src[f] * P.k_ss;
-        d[6] += (double)P.ss_sink[f] * P.k_ss;
+        const long long f = ixf + (long long)iyf * (P.R.nx + 3);   // sour_avg, sink_avg (:200-209)
+        if (P.ssd_src) {
+            d[5] += P.ssd_src[f];
+            d[6] += P.ssd_sink[f];
+        } else {
+            d[5] += (double)P.ss_src[f] * P.k_ss;
+            d[6] += (double)P.ss_sink[f] * P.k_ss;
+        }
     }
 }
 
@@ -212,9 +218,14 @@ extern "C" int lepic_gpu_set_avg(lepic_ctx *c, int32_t size_na, int32_t navg) {
     return LEPIC_OK;
 }
 
-int avg_sample(lepic_ctx *c) {
+int avg_sample(lepic_ctx *c, int it) {
     AvgState *A = avg_state(c);
     const lepic_config &g = c->cfg;
+    if (c->plt_src == 1) {   // main.f90:921-927: ss2D from the collision frequencies of this state
+        LCUDA(cudaMemsetAsync(c->ss_diag, 0, sizeof(double) * 2 * g.ntype * c->nn, c->stream));
+        const int r = mcc_collide(c, it, true);
+        if (r != LEPIC_OK) return r;
+    }
     LCUDA(cudaMemsetAsync(A->p_mts, 0, sizeof(double) * 4 * A->ncell * g.ntype, c->stream));
     for (int s = 0; s < g.ntype; s++) {
         SpeciesBuf &B = c->sp[s];
@@ -245,11 +256,13 @@ int avg_sample(lepic_ctx *c) {
         P.ss_src = c->ss_map + (size_t)(2 * s) * c->nn;
         P.ss_sink = c->ss_map + (size_t)(2 * s + 1) * c->nn;
         P.k_ss = g.Nm[s] / (g.dx * g.dy * g.zmax);
+        P.ssd_src = c->plt_src == 1 ? c->ss_diag + (size_t)(2 * s) * c->nn : nullptr;
+        P.ssd_sink = c->plt_src == 1 ? c->ss_diag + (size_t)(2 * s + 1) * c->nn : nullptr;
         k_calc_avg<<<(int)std::min<long long>(div_up(nodes, 256), (long long)c->num_sms * 8), 256, 0, c->stream>>>(P);
         LCUDA(cudaGetLastError());
     }
     // main.f90:931: the counts start again after each sample
-    LCUDA(cudaMemsetAsync(c->ss_map, 0, sizeof(unsigned int) * 2 * g.ntype * c->nn, c->stream));
+    if (c->plt_src == 0) LCUDA(cudaMemsetAsync(c->ss_map, 0, sizeof(unsigned int) * 2 * g.ntype * c->nn, c->stream));
     k_phi_avg<<<(int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 8), 256, 0, c->stream>>>(
         c->phi, c->Ed, c->nn, A->phi_avg);
     LCUDA(cudaGetLastError());
@@ -259,7 +272,22 @@ int avg_sample(lepic_ctx *c) {
 
 extern "C" int lepic_gpu_calc_avg(lepic_ctx *c) {
     if (!c || !avg_state(c)) return LEPIC_EINVAL;
-    return avg_sample(c);
+    return avg_sample(c, 0x40000000 + avg_state(c)->cnt);   // the diagnostic pass's draws: a stream per sample
+}
+
+extern "C" int lepic_gpu_set_source_option(lepic_ctx *c, int32_t plt_src) {
+    if (!c || (plt_src != 0 && plt_src != 1)) return LEPIC_EINVAL;
+    if (plt_src == 1 && !c->ss_diag) {
+        if (cudaMalloc((void **)&c->ss_diag, sizeof(double) * 2 * c->cfg.ntype * c->nn) != cudaSuccess) {
+            c->last_err = "set_source_option: cudaMalloc failed";
+            return LEPIC_ENOMEM;
+        }
+        LCUDA(cudaMemsetAsync(c->ss_diag, 0, sizeof(double) * 2 * c->cfg.ntype * c->nn, c->stream));
+    }
+    if (plt_src == 0 && c->ss_map)
+        LCUDA(cudaMemsetAsync(c->ss_map, 0, sizeof(unsigned int) * 2 * c->cfg.ntype * c->nn, c->stream));
+    c->plt_src = plt_src;
+    return lepic_gpu_sync(c);
 }
 
 extern "C" int lepic_gpu_get_avg(lepic_ctx *c, double *data_pavg, double *phi_avg, int32_t *cnt_avg, int32_t reset) {
@@ -283,6 +311,16 @@ extern "C" int lepic_gpu_get_source_maps(lepic_ctx *c, double *ss2D) {
     if (!c->ss_map) { c->last_err = "source maps need lepic_gpu_set_avg"; return LEPIC_EINVAL; }
     const int nt = c->cfg.ntype;
     const long long nn = c->nn;
+    if (c->plt_src == 1) {   // the densities of the last sample's diagnostic pass
+        std::vector<double> h((size_t)2 * nt * nn);
+        LCUDA(cudaMemcpyAsync(h.data(), c->ss_diag, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        int r = lepic_gpu_sync(c);
+        if (r) return r;
+        for (int s = 0; s < nt; s++)
+            for (long long n = 0; n < nn; n++)
+                for (int k = 0; k < 2; k++) ss2D[k + 2 * (n + nn * s)] = h[(size_t)(2 * s + k) * nn + n];
+        return LEPIC_OK;
+    }
     std::vector<unsigned int> h((size_t)2 * nt * nn);
     LCUDA(cudaMemcpyAsync(h.data(), c->ss_map, sizeof(unsigned int) * h.size(), cudaMemcpyDeviceToHost, c->stream));
     int r = lepic_gpu_sync(c);
@@ -296,7 +334,7 @@ extern "C" int lepic_gpu_get_source_maps(lepic_ctx *c, double *ss2D) {
 int avg_step(lepic_ctx *c, int it) {
     AvgState *A = avg_state(c);
     if (!A || A->navg < 1 || it % A->navg != 1) return LEPIC_OK;
-    return avg_sample(c);
+    return avg_sample(c, it);
 }
 
 // ---------------------------------------------------------------------------------------

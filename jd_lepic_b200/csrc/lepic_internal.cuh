@@ -173,6 +173,10 @@ struct lepic_ctx {
     // + node], k = 0 source, 1 sink; accumulated between averaging samples while averaging is
     // configured (null otherwise)
     unsigned int *ss_map = nullptr;
+    // plt_src (read_input.f90:113-117): 0 counts made/removed macroparticles in ss_map; 1 fills
+    // ss_diag (FP64, same layout) at each averaging sample from the collision frequencies
+    int plt_src = 0;
+    double *ss_diag = nullptr;
     // counters
     DevCounters *dcnt = nullptr;
     TallyDev *tally = nullptr;
@@ -319,7 +323,6 @@ int mg_residual_stats(lepic_ctx *c);
 int mg_mixed_solve(lepic_ctx *c, double eps);
 int push_deposit(lepic_ctx *c, int it, bool move);
 int sort_species(lepic_ctx *c, int ptype);
-int mcc_collide(lepic_ctx *c, int it);
 int particles_load(lepic_ctx *c, const lepic_load_spec *spec);
 int particles_put(lepic_ctx *c, int ptype, const double *vxp, long long n);
 int particles_get(lepic_ctx *c, int ptype, double *vxp, long long cap, long long *n_out);
@@ -327,6 +330,9 @@ int sources_before_push(lepic_ctx *c, int it);
 int sources_after_push(lepic_ctx *c, int it);
 void sources_free(lepic_ctx *c);
 int avg_step(lepic_ctx *c, int it);
+int mcc_collide(lepic_ctx *c, int it, bool diag = false);
+// the ss2D counts the kernels add to (null unless averaging is set up with plt_src = 0)
+static inline unsigned int *ss_counts(const lepic_ctx *c) { return c->plt_src == 0 ? c->ss_map : nullptr; }
 void avg_free(lepic_ctx *c);
 
 #define LCUDA(call)                                                                     \

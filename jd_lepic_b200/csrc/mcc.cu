@@ -31,6 +31,9 @@ struct MccP {
     unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
     long long ss_nn;
     int ss_W;
+    int diag;               // collisions' flag_diag: frequencies into ss_diag, no collision
+    double *ss_diag;        // ss2D with plt_src = 1, [(2 sp + k) nn + node]
+    double nm_vc[LEPIC_MAXSP];   // Nm / Vc per species
     uint32_t *X, *Y;
     float *VX, *VY, *VZ;
     Product *prod[LEPIC_MAXSP];
@@ -142,13 +145,47 @@ __device__ __forceinline__ double sigma_at(const MccP &P, int c, double E) {
     return sL + (E - EL) * (sR - sL) / (ER - EL);
 }
 
+// plt_src = 1 (collisions.f90:546-600): reaction c of the incident in `slot` at frequency k2
+// (1/s) adds k2 Nm/Vc, with the incident's CIC weights, to the source of every charged byproduct
+// other than the incident's and the target's species and to the sink of a charged reactant
+// that is not among the byproducts; elastic and excitation reactions (types 1, 3) add nothing.
+__device__ void diag_source_sink(const MccP &P, long long slot, int c, int sp, int tt, double k2) {
+    const int *ci = P.col_info + c * 10;
+    const int n_re = ci[0], n_by = ci[1], rt = ci[2 + n_re + n_by];
+    if (rt == 1 || rt == 3) return;
+    const uint32_t X = P.X[slot], Y = P.Y[slot], mask = (1u << P.S) - 1u;
+    const double inv = 1.0 / (double)(1u << P.S);
+    const double px = 1.0 - (double)(X & mask) * inv, py = 1.0 - (double)(Y & mask) * inv;  // (ix h - x)/h
+    const double w[4] = {px * py, (1.0 - px) * py, (1.0 - px) * (1.0 - py), px * (1.0 - py)};
+    const long long n00 = ((X >> P.S) + 1) + (long long)((Y >> P.S) + 1) * P.ss_W;
+    const long long nd[4] = {n00, n00 + 1, n00 + P.ss_W + 1, n00 + P.ss_W};
+    bool inc_kept = false, tgt_kept = false;
+    for (int ib = 0; ib < n_by; ib++) {
+        const int bt = ci[2 + n_re + ib];
+        if (P.charge[bt] != 0.0 && bt != sp && bt != tt) {
+            double *m = P.ss_diag + (size_t)(2 * bt) * P.ss_nn;
+            const double k1 = P.nm_vc[bt] * k2;
+            for (int q = 0; q < 4; q++) atomicAdd(m + nd[q], w[q] * k1);
+        }
+        if (bt == sp) inc_kept = true;
+        if (bt == tt) tgt_kept = true;
+    }
+    for (int i_re = 0; i_re < 2; i_re++) {
+        const int bt = i_re == 0 ? sp : tt;
+        if ((i_re == 0 ? inc_kept : tgt_kept) || P.charge[bt] == 0.0) continue;
+        double *m = P.ss_diag + (size_t)(2 * bt + 1) * P.ss_nn;
+        const double k1 = P.nm_vc[bt] * k2;
+        for (int q = 0; q < 4; q++) atomicAdd(m + nd[q], w[q] * k1);
+    }
+}
+
 __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsigned int *n_cand_local) {
     float fvx = P.VX[slot];
     if (isnan(fvx)) return;
     (*n_cand_local)++;
     const int sp = P.sp;
     Rng R;
-    R.ctr = U4{(uint32_t)slot, P.it, (uint32_t)sp | 0x4D430000u, 0u};
+    R.ctr = U4{(uint32_t)slot, P.it, (uint32_t)sp | 0x4D430000u, (uint32_t)P.diag};  // the diagnostic pass: own stream
     R.k0 = P.k0; R.k1 = P.k1; R.used = 4;
     const double vx1 = fvx, vy1 = P.VY[slot], vz1 = P.VZ[slot];
     const double mp = fabs(P.mass[sp]);
@@ -185,7 +222,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
                 // the target particle (:339-403) if this candidate holds its claim, and the
                 // target density at the incident's cell (:524-528)
                 long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
-                if (t >= 0 && (P.claim[tt][t] != (int)slot || isnan(P.TVX[tt][t]))) t = -1;
+                if (t >= 0 && ((!P.diag && P.claim[tt][t] != (int)slot) || isnan(P.TVX[tt][t]))) t = -1;
                 tslot[tt] = t;
                 a = b = z = 0.0;
                 if (t >= 0) { a = P.TVX[tt][t]; b = P.TVY[tt][t]; z = P.TVZ[tt][t]; }
@@ -213,7 +250,9 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             atomicAdd(&P.tal->cnt_col[0][c][rg], nu[q] * nu_max);
             atomicAdd(&P.tal->cnt_col[1][c][rg], 1.0);
         }
+        if (P.diag) diag_source_sink(P, slot, c, sp, tt, nu[q] * nu_max);
     }
+    if (P.diag) return;   // collisions.f90:649: flag_diag makes every event a null collision
     // :619 indexx: reactions ordered by ascending nu (straight insertion, stable); the order
     // decides the outcome when sum(nu) > 1, i.e. when nu_max was capped (main.f90:494-495)
     int order[MCC_MAX_REACTIONS];
@@ -433,6 +472,16 @@ __global__ void __launch_bounds__(MCC_THREADS) k_mcc(MccP P, const int *cand) {
     if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&P.cnt->n_cand[P.sp], (unsigned long long)ncand);
 }
 
+// collisions(..., flag_diag = 1) of collisions.f90:268-299: every particle of the species
+// through the collision frequencies, no collision performed
+__global__ void __launch_bounds__(MCC_THREADS) k_mcc_diag(MccP P) {
+    const long long n = P.cnt->n_slots[P.sp];
+    const double nu_max = step_nu_max(P);
+    unsigned int unused = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        collide_one(P, i, nu_max, &unused);
+}
+
 // DSMC claims: every candidate of this step picks its charged targets as collide_one will and
 // claims them with the smallest incident slot, so that a target takes part in one collision
 // of the step (the winner is independent of the order the threads run in).
@@ -533,7 +582,7 @@ __global__ void k_region_np(RhoParams R, int n_rg, int iyl, int iyr, const int *
     }
 }
 
-int mcc_collide(lepic_ctx *c, int it) {
+int mcc_collide(lepic_ctx *c, int it, bool diag) {
     if (!c->has_xs) return LEPIC_OK;
     if (c->n_rg > 0) {
         RhoParams R = rho_params(c);
@@ -587,7 +636,9 @@ int mcc_collide(lepic_ctx *c, int it) {
         memset(&P, 0, sizeof(P));
         bool claims = false;   // a charged target species of this incident gets DSMC claims
         P.sp = s; P.ntype = g.ntype;
-        P.ss_map = c->ss_map; P.ss_nn = c->nn; P.ss_W = g.nx + 3;
+        P.ss_map = diag ? nullptr : ss_counts(c); P.ss_nn = c->nn; P.ss_W = g.nx + 3;
+        P.diag = diag ? 1 : 0; P.ss_diag = c->ss_diag;
+        for (int t = 0; t < g.ntype; t++) P.nm_vc[t] = g.Nm[t] / (g.dx * g.dy * g.zmax);
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
         for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
         P.cnt = c->dcnt;
@@ -631,6 +682,11 @@ int mcc_collide(lepic_ctx *c, int it) {
                 }
             }
         }
+        if (diag) {
+            k_mcc_diag<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P);
+            LCUDA(cudaGetLastError());
+            continue;
+        }
         // candidates (the sort's key buffer holds the list: one int per slot at most)
         LCUDA(cudaMemsetAsync(&c->dcnt->n_cand_list, 0, sizeof(unsigned int), c->stream));
         k_mcc_select<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P, c->keys);
@@ -642,6 +698,7 @@ int mcc_collide(lepic_ctx *c, int it) {
         k_mcc<<<c->num_sms * 8, MCC_THREADS, 0, c->stream>>>(P, c->keys);
         LCUDA(cudaGetLastError());
     }
+    if (diag) return LEPIC_OK;
     for (int t = 0; t < g.ntype; t++) {
         SpeciesBuf &B = c->sp[t];
         k_mcc_commit<<<1, 1024, 0, c->stream>>>(t, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],

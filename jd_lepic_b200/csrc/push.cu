@@ -460,7 +460,7 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         }
         P.cellwall = c->cellwall;
         P.acc = B.acc;
-        P.ss_sink = c->ss_map ? c->ss_map + (size_t)(2 * s + 1) * c->nn : nullptr;
+        P.ss_sink = ss_counts(c) ? ss_counts(c) + (size_t)(2 * s + 1) * c->nn : nullptr;
         P.items = B.items;
         P.cnt = c->dcnt;
         P.sp = s;

@@ -958,7 +958,7 @@ static int run_injection(lepic_ctx *c, int it) {
         P.acc[sp] = B.acc;
     }
     P.cellwall = c->cellwall;
-    P.ss_map = c->ss_map; P.ss_nn = c->nn;
+    P.ss_map = ss_counts(c); P.ss_nn = c->nn;
     P.phi = c->phi;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);
@@ -1006,7 +1006,7 @@ static int run_emitter(lepic_ctx *c, int it) {
         P.VX[q] = B.VX[B.cur]; P.VY[q] = B.VY[B.cur]; P.VZ[q] = B.VZ[B.cur];
     }
     P.bcnd = c->bcnd;
-    P.ss_map = c->ss_map; P.ss_nn = c->nn;
+    P.ss_map = ss_counts(c); P.ss_nn = c->nn;
     P.max_attempts_extra = 65536;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);

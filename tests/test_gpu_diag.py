@@ -198,3 +198,43 @@ def test_source_maps_count_collision_products(gpu_lib):
         assert np.all(cells[m[0, ..., 0] > 0])
     finally:
         sim.close()
+
+
+def test_source_option_collision_frequencies(gpu_lib):
+    """plt_src = 1 (collisions with flag_diag, collisions.f90:546-600): each 100 eV electron adds
+    its ionization frequency n sigma v times Nm/Vc to the Ar+ source with CIC weights; the
+    electron is not a source (it is the incident) and nothing is a sink (the electron survives,
+    the target is a neutral); calc_avg takes the densities as they are."""
+    import math
+    case = configs.case0(ppc=8, nx=NX, ny=NX)
+    E = dk.energy_grid(1e3, 50)
+    sig = 2.0e-20
+    case.deck_text = dk.write_deck("[Ar+]", 39.95, 0.03, "[Ar]", 0.0258,
+                                   [("[e]+[Ar]->[e]+[e]+[Ar+]", "IONIZATION", 15.76, E, dk.sigma_constant(E, sig))])
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    sp = species_params(case, d)
+    sim = GpuSimulation(case)
+    try:
+        p = sim.get_particles(0)
+        v = math.sqrt(2 * 100 * dk.QE / 9.10938e-31)
+        p[:, 3:] = 0.0
+        p[:, 4] = np.float32(v)
+        sim.put_particles(0, p)
+        sim.check(sim.lib.lepic_gpu_set_avg(sim.ctx, 1, 0), "set_avg")
+        sim.check(sim.lib.lepic_gpu_set_source_option(sim.ctx, 1), "set_source_option")
+        n_before = sim.push_stats()["np_tot"]
+        sim.check(sim.lib.lepic_gpu_calc_avg(sim.ctx), "calc_avg")
+        m = get_maps(sim)
+        assert sim.push_stats()["np_tot"] == n_before          # no collision performed
+        vc = case.dx * case.dy * case.zmax
+        vf = float(np.float32(v))
+        expect = len(p) * case.ngas * sig * vf * sp.Nm[1] / vc
+        assert m[1, ..., 0].sum() == pytest.approx(expect, rel=1e-5)
+        assert np.all(m[0, ..., 0] == 0.0) and np.all(m[..., 1] == 0.0)
+        data, _, _ = get_avg(sim, 1)
+        close(data[1, ..., 5], m[1, 1:NX + 2, 1:NX + 2, 0], 1e-14)
+        # back to counting: the maps start from zero
+        sim.check(sim.lib.lepic_gpu_set_source_option(sim.ctx, 0), "set_source_option")
+        assert np.all(get_maps(sim) == 0.0)
+    finally:
+        sim.close()
