@@ -3,7 +3,7 @@
 // previous potential) to a correction of the potential, trained online on the pairs the
 // solver itself produces.  The solver (FP64 conjugate gradients with the FP32 V-cycle) then
 // refines the corrected potential to the same residual as always, so it stays both the
-// fallback and the judge.  No counterpart in the reference, whose solve starts from the
+// fallback and the arbiter of the answer.  No counterpart in the reference, whose solve starts from the
 // previous step's potential (iterative_solver.f90:1-69, called at main.f90:829).
 //
 // Tensor-core path: every convolution (forward, and the input gradient as a forward
