@@ -229,6 +229,7 @@ PROTOTYPES = {
     "lepic_gpu_get_avg": (C.c_int, [_VP, _DP, _DP, C.POINTER(C.c_int32), C.c_int32]),
     "lepic_gpu_get_source_maps": (C.c_int, [_VP, _DP]),
     "lepic_gpu_set_source_option": (C.c_int, [_VP, C.c_int32]),
+    "lepic_gpu_set_warm_start": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_cnn_configure": (C.c_int, [_VP, C.POINTER(LepicCnnConfig)]),
     "lepic_gpu_cnn_stats": (C.c_int, [_VP, C.POINTER(LepicCnnStats)]),
     "lepic_gpu_cnn_net": (_VP, [_VP]),

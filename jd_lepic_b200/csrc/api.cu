@@ -40,7 +40,7 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
     F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed); F(c->Ef);
-    F(c->ss_diag);
+    F(c->ss_diag); F(c->phi_hist);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
@@ -588,8 +588,9 @@ extern "C" int lepic_gpu_dens_red(lepic_ctx *c, double *np_red_out, double *np_m
 }
 
 static int solve(lepic_ctx *c, double eps, int mode) {
+    if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps, true);
+    c->have_hist = 0;   // any other solver: the next mixed solve starts from its answer as it is
     if (mode == LEPIC_POISSON_FP64_MG) return mg_solve(c, eps, 0);
-    if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps);
     if (mode == 2) return mg_solve(c, eps, 2);
     if (mode == LEPIC_POISSON_LEARNED) return learned_solve(c, eps);
     c->last_err = "unknown Poisson mode";
@@ -697,10 +698,25 @@ extern "C" int lepic_gpu_get_grid(lepic_ctx *c, int32_t which, double *out) {
     return LEPIC_OK;
 }
 
+extern "C" int lepic_gpu_set_warm_start(lepic_ctx *c, int32_t mode) {
+    if (!c || (mode != 0 && mode != 1)) return LEPIC_EINVAL;
+    if (mode == 1 && !c->phi_hist) {
+        if (cudaMalloc((void **)&c->phi_hist, sizeof(double) * c->nn) != cudaSuccess) {
+            c->last_err = "set_warm_start: cudaMalloc failed";
+            return LEPIC_ENOMEM;
+        }
+    }
+    c->warm_xtrap = mode;
+    c->have_hist = 0;
+    return LEPIC_OK;
+}
+
 extern "C" int lepic_gpu_set_grid(lepic_ctx *c, int32_t which, const double *in) {
     if (!c || !in) return LEPIC_EINVAL;
-    if (which == LEPIC_GRID_PHI)
+    if (which == LEPIC_GRID_PHI) {
         LCUDA(cudaMemcpyAsync(c->phi, in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
+        c->have_hist = 0;   // a potential from elsewhere: the next solve starts from it as it is
+    }
     else if (which == LEPIC_GRID_RHS)
         LCUDA(cudaMemcpyAsync(c->rhs, in, sizeof(double) * (c->cfg.nx + 1) * (c->cfg.ny + 1), cudaMemcpyHostToDevice,
                               c->stream));

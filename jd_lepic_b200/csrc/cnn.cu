@@ -1426,7 +1426,7 @@ static int learn_train(lepic_ctx *c, LearnState *L, int steps) {
 // Poisson solve with the learned warm start: predict, keep the prediction only if it lowers
 // the residual, refine with the mixed-precision CG, then learn from the solved pair.
 int learned_solve(lepic_ctx *c, double eps) {
-    if (c->cfg.flag_pbc || c->cfg.flag_nmn) return mg_mixed_solve(c, eps); // same scope as the CG
+    if (c->cfg.flag_pbc || c->cfg.flag_nmn) return mg_mixed_solve(c, eps, false); // same scope as the CG
     int r = learn_init(c);
     if (r) return r;
     LearnState *L = (LearnState *)c->learn;
@@ -1449,7 +1449,7 @@ int learned_solve(lepic_ctx *c, double eps) {
     k_prep_sigma<<<1, 256, 0, c->stream>>>(L->partial, g, count, L->scal + 2);
     k_accept<<<grid_for(c->nn, 256, c->num_sms), 256, 0, c->stream>>>(P, L->scal, L->uprev, c->phi, L->accepted);
     LCUDA(cudaGetLastError());
-    r = mg_mixed_solve(c, eps);
+    r = mg_mixed_solve(c, eps, false);   // from the network's start, not an extrapolation
     if (r) return r;
     L->st.solves++;
     const bool train = L->cfg.enable_training &&

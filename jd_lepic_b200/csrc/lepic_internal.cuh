@@ -146,6 +146,10 @@ struct lepic_ctx {
     double *partials = nullptr;
     int mg_grid = 0, mg_grid_mixed = 0;
     double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;  // finest-level CG vectors
+    // warm start of the mixed solve: 1 extrapolates 2 phi_(n-1) - phi_(n-2) from the inputs of
+    // the last two solves (phi_hist holds the previous input, have_hist says it is valid)
+    int warm_xtrap = 0, have_hist = 0;
+    double *phi_hist = nullptr;
     // collisions
     bool has_xs = false;
     bool dsmc = false;             // a reaction has a charged target (collisions.f90:339-418)
@@ -320,7 +324,7 @@ int field_np_grid(lepic_ctx *c, int ptype, double *d_out);
 int mg_solve(lepic_ctx *c, double eps, int mode);
 int mg_init(lepic_ctx *c);
 int mg_residual_stats(lepic_ctx *c);
-int mg_mixed_solve(lepic_ctx *c, double eps);
+int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap);   // xtrap: the warm start may extrapolate
 int push_deposit(lepic_ctx *c, int it, bool move);
 int sort_species(lepic_ctx *c, int ptype);
 int particles_load(lepic_ctx *c, const lepic_load_spec *spec);

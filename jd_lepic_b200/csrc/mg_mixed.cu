@@ -777,9 +777,26 @@ __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
     }
 }
 
-int mg_mixed_solve(lepic_ctx *c, double eps) {
+// The extrapolated warm start: at the unknowns u = 2 u - u_prev, where u is this solve's
+// input (the last solution) and u_prev the previous solve's input; u_prev <- u in the same
+// pass.  Dirichlet nodes keep their values.
+__global__ void k_warm_xtrap(double *u, double *hist, const int8_t *bc, long long nn, int have) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn; t += (long long)gridDim.x * blockDim.x) {
+        const double cur = u[t];
+        const double prev = hist[t];
+        hist[t] = cur;
+        if (have && bc[t] <= 0) u[t] = 2.0 * cur - prev;
+    }
+}
+
+int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the CG operator is symmetric only with Dirichlet rows
         return mg_solve(c, eps, 2);
+    if (xtrap && c->warm_xtrap) {
+        k_warm_xtrap<<<c->num_sms * 8, 256, 0, c->stream>>>(c->phi, c->phi_hist, c->bc8, c->nn, c->have_hist);
+        LCUDA(cudaGetLastError());
+        c->have_hist = 1;
+    }
     MXP P;
     memset(&P, 0, sizeof(P));
     const double eps0 = c->cfg.eps0;

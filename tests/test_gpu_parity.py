@@ -226,6 +226,40 @@ def test_mg_mixed_precision_reaches_1e8(gpu_lib, idx, n):
     s.close()
 
 
+def test_warm_start_extrapolation(gpu_lib):
+    """lepic_gpu_set_warm_start(1): a rhs that changes linearly from step to step has a linear
+    solution, so 2 phi_(n-1) - phi_(n-2) is almost the answer: fewer CG iterations than from
+    phi_(n-1), the same tolerance on the true residual and the same potential."""
+    case = configs.case4(ppc=2, nx=256, ny=256)
+    s = sim_for(case)
+    try:
+        cfg = oracle_cfg(case, s)
+        base = _perturbed_rhs(s, case)
+        i = np.arange(case.nx + 1)
+        j = np.arange(case.ny + 1)
+        X, Y = np.meshgrid(i / case.nx, j / case.ny)
+        step = 2.0e-4 * np.sin(math.pi * X) * np.sin(2 * math.pi * Y)
+        s.check(s.lib.lepic_gpu_set_warm_start(s.ctx, 1), "set_warm_start")
+        phis, cyc = [], []
+        for n in range(5):
+            set_rhs(s, base + n * step)
+            st = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR)   # from the device's last solution
+            assert st["res_l2_rel"] <= 1e-8
+            cyc.append(st["cycles"])
+            phis.append(s.grid(capi.GRID_PHI))
+        assert O.l2_residual(cfg, phis[4], base + 4 * step, case.bcnd) <= 1e-8
+        # the last step again, from phi_3 as it is
+        s.check(s.lib.lepic_gpu_set_warm_start(s.ctx, 0), "set_warm_start")
+        s.set_phi(phis[3])
+        st = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR)
+        assert st["res_l2_rel"] <= 1e-8
+        assert cyc[4] < st["cycles"], (cyc, st["cycles"])
+        plain = s.grid(capi.GRID_PHI)
+        assert np.abs(phis[4] - plain).max() <= 1e-5 * np.abs(plain).max()
+    finally:
+        s.close()
+
+
 def test_sort_reference_order_exact(gpu_lib):
     case = configs.case0(ppc=20, nx=64, ny=64)
     s = sim_for(case, tile=None)  # the reference's row-major cell order
