@@ -205,7 +205,9 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         LCUDA(cudaMemset(L.e32b, 0, sizeof(float) * nnl));
         LCUDA(cudaMemset(L.r32, 0, sizeof(float) * (L.nx + 1) * (L.ny + 1)));
     }
-    LALLOC(c->partials, (size_t)c->num_sms * 32);
+    // grid-wide sums: up to 3 values x 2 halves per CTA of a cooperative grid of at most 8 CTAs
+    // of 256 threads per SM
+    LALLOC(c->partials, (size_t)c->num_sms * 48);
     LALLOC(c->cg_r, nn); LALLOC(c->cg_p, nn); LALLOC(c->cg_ap, nn);
     LCUDA(cudaMemset(c->cg_r, 0, sizeof(double) * nn));
     LCUDA(cudaMemset(c->cg_p, 0, sizeof(double) * nn));

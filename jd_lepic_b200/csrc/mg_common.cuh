@@ -86,6 +86,39 @@ __device__ __forceinline__ bool team_sum(const BigTeam &T, double v, double *out
     __syncthreads();
     return true;
 }
+// N sums behind one grid barrier.  Sum v of half h sits at partials + (2 v + h) * gridDim.x, so
+// value 0 uses team_sum's layout and a CTA that runs ahead into any later sum (the other half)
+// writes none of the slots still being read; `partials` holds 2 N * gridDim.x doubles.  Each
+// sum is reduced in the same fixed order as team_sum's.
+template <int N>
+__device__ __forceinline__ bool team_sums(const BigTeam &T, const double (&v)[N], double (&out)[N]) {
+    double b[N];
+#pragma unroll
+    for (int q = 0; q < N; q++) b[q] = block_sum(v[q]);
+    const unsigned h = T.phase & 1;
+    T.phase++;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < N; q++) T.partials[(2 * q + h) * gridDim.x + blockIdx.x] = b[q];
+    }
+    if (!T.sync()) return false;
+    __shared__ double s_tot[N];
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int q = 0; q < N; q++) {
+            const volatile double *part = T.partials + (2 * q + h) * gridDim.x;
+            double a = 0.0;
+            for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) a = a + part[i];
+            for (int o = 16; o > 0; o >>= 1) a = a + __shfl_xor_sync(0xffffffffu, a, o);
+            if (threadIdx.x == 0) s_tot[q] = a;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N; q++) out[q] = s_tot[q];
+    __syncthreads();
+    return true;
+}
 __device__ __forceinline__ bool team_sum(const SmallTeam &, double v, double *out) {
     *out = block_sum(v);
     return true;

@@ -548,34 +548,45 @@ __device__ __forceinline__ void walk_batch(Walk2 &w, int W, int *t, int *n, bool
 }
 
 // r = b - A u at unknowns (bcnd <= 0), zero elsewhere; r32 = (float) r; e = 0 (all nodes);
-// returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum
-__device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double *l1) {
+// returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum.  With B0 the same walk also
+// forms ||b0||^2 over bcnd == -1 nodes, b0 = b minus the wall terms of A u (the norm the
+// stopping test scales by), and the three sums share one grid barrier.
+template <bool B0>
+__device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double *l1, double *bb = nullptr) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
     const double aw = L.awd, an = L.and_, ac = L.acd;
-    double a = 0.0, s1 = 0.0;
+    double a = 0.0, s1 = 0.0, s0 = 0.0;
     Walk2 w(B.rank(), B.size(), nx + 1, ny + 1);
     while (w.ok()) {
         int t[FB5], n[FB5];
         bool v[FB5];
         walk_batch<FB5>(w, W, t, n, v);
-        int bc[FB5];
-        double bb[FB5], uc[FB5], uw[FB5], ue[FB5], us[FB5], un[FB5];
+        int bc[FB5], bw[FB5], be[FB5], bs[FB5], bn[FB5];
+        double bb_[FB5], uc[FB5], uw[FB5], ue[FB5], us[FB5], un[FB5];
         const double *u = L.u;
 #pragma unroll
         for (int k = 0; k < FB5; k++) {
-            bc[k] = v[k] ? L.bc[n[k]] : 1;
-            bb[k] = L.b[t[k]];
-            uc[k] = u[n[k]]; uw[k] = u[n[k] - 1 + (v[k] ? 0 : 1)]; ue[k] = u[n[k] + 1];
-            us[k] = v[k] ? u[n[k] - W] : 0.0; un[k] = u[n[k] + W];
+            const int m = n[k];
+            const int mw = v[k] ? m - 1 : m + 1, ms = v[k] ? m - W : m;
+            bc[k] = v[k] ? L.bc[m] : 1;
+            bb_[k] = L.b[t[k]];
+            uc[k] = u[m]; uw[k] = u[mw]; ue[k] = u[m + 1];
+            us[k] = v[k] ? u[ms] : 0.0; un[k] = u[m + W];
+            if (B0) { bw[k] = L.bc[mw]; be[k] = L.bc[m + 1]; bs[k] = L.bc[ms]; bn[k] = L.bc[m + W]; }
         }
 #pragma unroll
         for (int k = 0; k < FB5; k++) {
             if (!v[k]) continue;
             double r = 0.0;
             if (bc[k] <= 0) {
-                r = bb[k] - (aw * uw[k] + an * un[k] + an * us[k] + aw * ue[k] + ac * uc[k]);
+                r = bb_[k] - (aw * uw[k] + an * un[k] + an * us[k] + aw * ue[k] + ac * uc[k]);
                 if (bc[k] == -1) { a += r * r; s1 += fabs(r); }
+            }
+            if (B0 && bc[k] == -1) {
+                const double d = bb_[k] - ((bw[k] > 0 ? aw * uw[k] : 0.0) + (bn[k] > 0 ? an * un[k] : 0.0) +
+                                           (bs[k] > 0 ? an * us[k] : 0.0) + (be[k] > 0 ? aw * ue[k] : 0.0));
+                s0 += d * d;
             }
             P.r64[n[k]] = r;
             L.r[t[k]] = (float)r;
@@ -586,8 +597,16 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
         L.e[t] = 0.0f;
         if (w2.k == 0 || w2.j == 0 || w2.k == nx + 2 || w2.j == ny + 2) P.r64[t] = 0.0;
     }
-    if (!team_sum(B, a, rr)) return false;
-    return team_sum(B, s1, l1);
+    if (B0) {
+        double out[3];
+        if (!team_sums<3>(B, {a, s1, s0}, out)) return false;
+        *rr = out[0]; *l1 = out[1]; *bb = out[2];
+    } else {
+        double out[2];
+        if (!team_sums<2>(B, {a, s1}, out)) return false;
+        *rr = out[0]; *l1 = out[1];
+    }
+    return true;
 }
 
 // z = e (FP32 cycle output): returns r.z
@@ -700,46 +719,11 @@ __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *
     return team_sum(B, a, rr);
 }
 
-template <class Team>
-__device__ bool b0_norm(const Team &T, const MXL &L, double *bb) {
-    const int nx = L.nx, ny = L.ny, W = nx + 3;
-    const double aw = L.awd, an = L.and_;
-    double b = 0.0;
-    Walk2 w(T.rank(), T.size(), nx + 1, ny + 1);
-    while (w.ok()) {
-        int t[FB5], n[FB5];
-        bool v[FB5];
-        walk_batch<FB5>(w, W, t, n, v);
-        const double *u = L.u;
-        const int8_t *bc = L.bc;
-        int b0[FB5], bw[FB5], be[FB5], bs[FB5], bn[FB5];
-        double bv[FB5], uw[FB5], ue[FB5], us[FB5], un[FB5];
-#pragma unroll
-        for (int k = 0; k < FB5; k++) {
-            const int m = n[k];
-            const int ms = v[k] ? m - W : m, mw = v[k] ? m - 1 : m;
-            b0[k] = v[k] ? bc[m] : 1;
-            bw[k] = bc[mw]; be[k] = bc[m + 1]; bs[k] = bc[ms]; bn[k] = bc[m + W];
-            bv[k] = L.b[t[k]];
-            uw[k] = u[mw]; ue[k] = u[m + 1]; us[k] = u[ms]; un[k] = u[m + W];
-        }
-#pragma unroll
-        for (int k = 0; k < FB5; k++) {
-            if (b0[k] != -1) continue;
-            double d = bv[k] - ((bw[k] > 0 ? aw * uw[k] : 0.0) + (bn[k] > 0 ? an * un[k] : 0.0) +
-                                (bs[k] > 0 ? an * us[k] : 0.0) + (be[k] > 0 ? aw * ue[k] : 0.0));
-            b += d * d;
-        }
-    }
-    return team_sum(T, b, bb);
-}
-
 __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
     BigTeam B{P.cnt, P.partials};
     double bb = 0.0, rr = 0.0, l1 = 0.0, rz = 0.0, pap = 0.0;
-    if (!b0_norm(B, P.L[0], &bb)) return;
+    if (!true_residual<true>(B, P, &rr, &l1, &bb)) return;
     const double b0 = sqrt(bb), tol = P.eps * b0;
-    if (!true_residual(B, P, &rr, &l1)) return;
     int it = 0, restarts = 0;
     bool conv = sqrt(rr) <= tol;
     bool first = true;
@@ -757,13 +741,13 @@ __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
         if (!update_ur(B, P, alpha, &rr)) return;
         it++;
         if (sqrt(rr) <= tol) {               // confirm on the true residual
-            if (!true_residual(B, P, &rr, &l1)) return;
+            if (!true_residual<false>(B, P, &rr, &l1)) return;
             conv = sqrt(rr) <= tol;
             if (!conv) { first = true; restarts++; }
         }
     }
     if (!conv) {
-        if (!true_residual(B, P, &rr, &l1)) return;
+        if (!true_residual<false>(B, P, &rr, &l1)) return;
         conv = sqrt(rr) <= tol;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
