@@ -819,12 +819,16 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
         P.soff_b[l] = (int)off; off += ((nn + 15) / 16) * 16;
     }
     P.Ls = Ls;
-    P.omega = 1.0f;
-    // three sweeps before and after the coarse correction: a warm 2048^2 solve needs 3 CG
-    // iterations instead of 5 with two, and an iteration costs 1.3x as much
+    // two over-relaxed sweeps (omega 1.15) before and after the coarse correction; the reverse
+    // colour order after it keeps the cycle a symmetric preconditioner.  Measured at 2048^2
+    // over 100 steps from the extrapolated start (2 iterations): 1.32 ms per solve against
+    // 1.37 with three plain sweeps; two plain sweeps need a third iteration in some steps, and
+    // omega 1.3 in others.  From phi_(n-1) alone: 4 iterations, against 5 with two plain
+    // sweeps and 4 with three.
     // two sweeps each way on the coarsest level (3^2 nodes at 2048^2): eight gave the same
     // iteration counts and residuals and cost CTA 0's 28 more barriers per cycle
-    P.nu1 = 3; P.nu2 = 3; P.nuc = 2; P.max_iter = 200;
+    P.omega = 1.15f;
+    P.nu1 = 2; P.nu2 = 2; P.nuc = 2; P.max_iter = 200;
     if (const char *e = getenv("LEPIC_MX_NUC")) P.nuc = atoi(e);
     if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
     if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
