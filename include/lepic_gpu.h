@@ -231,16 +231,22 @@ int lepic_gpu_deposit_grid(lepic_ctx *ctx, int32_t ptype, void **acc);
  * and handed out by its own (or another framework's) allocator, or code where the implicit
  * synchronisation of an allocation is not allowed.  The caller passes device pointers it
  * owns: X, Y (n fixed-point positions with `shift` fractional bits, as
- * lepic_gpu_particle_arrays returns them), VX (may be NULL; NaN marks a hole), kq
+ * lepic_gpu_particle_arrays returns them), VX (NaN marks a hole left by a lost particle), kq
  * ((nx+3)*(ny+3) node factors), and np_out ((nx+3)*(ny+3) doubles) which receives
  * np = kq * k1 * sum of CIC weights, k1 = Nm / (dx*dy*zmax) -- the np grid of
  * charge_deposition (part_expmover.f90:520-610), identical to the context path.
+ * A hole's X and Y do not hold a position, so VX may be NULL only when every one of the n
+ * slots is a live particle (freshly loaded or put, or compacted by lepic_gpu_part_sorting);
+ * with VX NULL a hole would be deposited as a particle.  A position outside the box
+ * (X >= nx << shift or Y >= ny << shift) is skipped, not deposited and not reported.
  * The temporary uint64 accumulator is a fixed static device array of 2^20 nodes (8 MiB) that
  * every GPU loading the library keeps until exit; larger grids ((nx+3)*(ny+3) > 2^20) are
  * rejected with LEPIC_ECAPACITY.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  All calls on a device share the array and
- * each call clears it first: calls that overlap on the GPU race and must be serialised by the
- * caller.  stream is a cudaStream_t (NULL: the default stream); the call only enqueues work. */
+ * address and the SM count, so make it before any stream capture.  All calls on a device
+ * share the array and each call clears it first: calls that overlap on the GPU race and must
+ * be serialised by the caller.  An error left pending by the caller's earlier CUDA work is
+ * returned as LEPIC_ECUDA (and left pending) before anything is enqueued.
+ * stream is a cudaStream_t (NULL: the default stream); the call only enqueues work. */
 int lepic_gpu_deposit_noalloc(const uint32_t *X, const uint32_t *Y, const float *VX, int64_t n,
                               int32_t nx, int32_t ny, int32_t shift, double k1, const double *kq,
                               double *np_out, void *stream);
