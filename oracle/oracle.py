@@ -220,6 +220,62 @@ def mover(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, flag_dead=None):
     return n.value, t
 
 
+def mover_tagged(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray):
+    """o_part_mover on a copy of vxp whose z holds each particle's index; returns the survivors
+    (compacted in order, part_expmover.f90:496-503) and their indices.  z moves by dt*vz, far
+    below 0.5, so rounding recovers the index."""
+    ref = np.ascontiguousarray(vxp, dtype=np.float64).copy()
+    ref[:, 2] = np.arange(ref.shape[0], dtype=np.float64)
+    n, t = mover(cfg, ptype, Ei, Bi, bcnd, ref)
+    ref = ref[:n].copy()
+    ids = np.rint(ref[:, 2]).astype(np.int64)
+    ref[:, 2] = 0.0
+    return ref, ids, t
+
+
+def align_survivors(got: np.ndarray, ref: np.ndarray, dx: float, dy: float, window: int = 8):
+    """Pairs the device's survivors with the oracle's.  Both are the initial particles minus the
+    lost ones, in the initial order, so they are two subsequences of one sequence that differ
+    only where a particle within a rounding distance of a wall cell is lost on one side.
+    Returns (gi, rj, n_gpu_only, n_ref_only): index arrays of the paired rows and the number of
+    particles kept by one side only.  Two rows pair when their positions agree to 1e-3 of a cell
+    (the parity tolerance is far tighter and is asserted on the pairs by the caller)."""
+    ng, nr = got.shape[0], ref.shape[0]
+    gi, rj = [], []
+    g_only = r_only = 0
+    i = j = 0
+
+    def same(a, b):
+        return abs(got[a, 0] - ref[b, 0]) <= 1e-3 * dx and abs(got[a, 1] - ref[b, 1]) <= 1e-3 * dy
+
+    # vectorised fast path over the common prefix, then a windowed greedy walk at mismatches
+    while i < ng and j < nr:
+        m = min(ng - i, nr - j)
+        ok = (np.abs(got[i:i + m, 0] - ref[j:j + m, 0]) <= 1e-3 * dx) & \
+             (np.abs(got[i:i + m, 1] - ref[j:j + m, 1]) <= 1e-3 * dy)
+        k = int(np.argmin(ok)) if not ok.all() else m
+        gi.extend(range(i, i + k))
+        rj.extend(range(j, j + k))
+        i += k
+        j += k
+        if i >= ng or j >= nr:
+            break
+        for d in range(1, window + 1):       # the device lost ref[j .. j+d-1]
+            if j + d < nr and same(i, j + d):
+                r_only += d
+                j += d
+                break
+            if i + d < ng and same(i + d, j):  # the oracle lost got[i .. i+d-1]
+                g_only += d
+                i += d
+                break
+        else:
+            raise AssertionError(f"device and oracle survivors cannot be aligned at {i}/{j}")
+    g_only += ng - i
+    r_only += nr - j
+    return np.asarray(gi, dtype=np.int64), np.asarray(rj, dtype=np.int64), g_only, r_only
+
+
 def deposit(cfg, ptype, vxp, n, kq, npg):
     lib().o_charge_deposition(C.byref(cfg), ptype, dp(vxp), n, dp(kq), dp(npg))
 
@@ -281,6 +337,29 @@ def l2_residual(cfg, phi, rhs, bcnd):
     Aud = aw * ud[1:-1, :-2] + an * ud[2:, 1:-1] + an * ud[:-2, 1:-1] + aw * ud[1:-1, 2:]
     d = rhs - Aud
     return math.sqrt(float((r[m] ** 2).sum())) / max(math.sqrt(float((d[m] ** 2).sum())), 1e-300)
+
+
+def collisions(cfg, xsh, particles, seed: int, extra: int = 4096):
+    """o_collisions (collisions.f90:1-207, collision_OMP, SCATTER) once on copies of the given
+    per-species particle arrays, the ran2 stream seeded with `seed`.  Returns (rc, arrays after
+    the call with the products appended, the collision tally, flag_dead per species)."""
+    ntype = cfg.ntype
+    bufs, fds = [], []
+    for s in range(ntype):
+        a = np.ascontiguousarray(particles[s], dtype=np.float64)
+        b = np.zeros((a.shape[0] + extra, 6))
+        b[:a.shape[0]] = a
+        bufs.append(b)
+        fds.append(np.zeros(b.shape[0], dtype=np.int8))
+    arrs = (_DP * MAXSP)(*[dp(b) for b in bufs])
+    npt = (C.c_int64 * MAXSP)(*[p.shape[0] for p in particles[:ntype]])
+    cap = (C.c_int64 * MAXSP)(*[b.shape[0] for b in bufs])
+    fdp = (_I8 * MAXSP)(*[f.ctypes.data_as(_I8) for f in fds])
+    t = OMccTally()
+    sd = C.c_int32(seed)
+    rc = lib().o_collisions(C.byref(cfg), C.byref(xsh.xs), arrs, npt, cap, fdp, C.byref(sd), C.byref(t))
+    out = [bufs[s][:npt[s]].copy() for s in range(ntype)]
+    return rc, out, t, [fds[s][:npt[s]].copy() for s in range(ntype)]
 
 
 class OracleSimulation:
