@@ -391,6 +391,12 @@ def run_ours(args):
     if args.nx:
         kw.update(nx=args.nx, ny=args.nx)
     case = configs.make_case(args.config, **kw)
+    # weak scaling with the reference's particle decomposition (load_part.f90:96): the deck's
+    # np_cell grows with the ranks, so Nm = n0 Vc / np_cell shrinks by 1/world, and each rank
+    # loads np_cell n_cell / world particles (one GPU's workload) with its own seed; the int64
+    # all-reduce of rho after each push (calc_rho.f90:71-74) gives every rank the global charge
+    case.ppc *= world
+    case.nproc_mpi = world
     case.seed = case.seed + 7919 * rank
     sim = GpuSimulation(case, tile=(args.tile, args.tile))
     lib, ctx = sim.lib, sim.ctx
@@ -595,7 +601,10 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 particles / f64 Poisson residual",
             "data": "synthetic",
             "config": {"workload": case.name, "grid": [case.nx, case.ny],
-                       "particles_per_species_per_gpu": case.n_particles, "species": sim.sp.ntype,
+                       "particles_per_species_per_gpu": case.n_load, "species": sim.sp.ntype,
+                       "decomposition": (f"particles split over {world} ranks (load_part.f90:96), np_cell "
+                                         f"{case.ppc} in all, Nm = n0 Vc / np_cell, int64 rho all-reduce per step"
+                                         if world > 1 else "one rank"),
                        "particles_avg_per_gpu": n_avg, "poisson": {1: "FP64 CG preconditioned by an FP32 V-cycle, relative L2 residual 1e-8, "
                                       "started from 2 phi_(n-1) - phi_(n-2)",
                                    3: "learned warm start + FP64 CG with the FP32 V-cycle, relative L2 "

@@ -212,6 +212,29 @@ int lepic_gpu_push_deposit(lepic_ctx *ctx, int32_t it, lepic_push_stats *stats);
  * lepic_gpu_set_sources.  eps / mode as lepic_gpu_iterative_solver. */
 int lepic_gpu_step(lepic_ctx *ctx, int32_t it, double eps, int32_t mode);
 
+/* Settings of the solvers and of the cooperative launches.  No counterpart in the reference
+ * (whose solver settings are the constants of iterative_solver.f90 and sors.f90); the defaults
+ * are the measured best on a B200 and nothing else (no environment variable) changes them.
+ * Read the current values with lepic_gpu_get_options, change fields, write them back. */
+typedef struct lepic_options {
+    int32_t mx_nu1, mx_nu2;      /* FP32 V-cycle: sweeps before / after the coarse correction (2, 2)  */
+    int32_t mx_nuc;              /* sweeps each way on the coarsest level (2)                        */
+    float mx_omega;              /* over-relaxation of the FP32 sweeps (1.15)                        */
+    int32_t mx_onchip_bytes;     /* shared memory for the coarse levels CTA 0 runs alone (20480)     */
+    int32_t mx_tiled;            /* 1: fine-level sweeps on shared-memory tiles (default); 0: grid-
+                                    wide half-sweeps -- identical results, for checking the tiles   */
+    int32_t mx_max_iter;         /* CG iterations before LEPIC_ENOTCONV (200)                        */
+    int32_t mg_small_nodes;      /* FP64 V-cycle: levels of at most this many nodes on CTA 0 (4500)  */
+    int32_t ctas_per_sm;         /* CTAs per SM of the cooperative solver kernels (3)                */
+    int32_t barrier_extra;       /* test hook, 0 in use: the solvers' grid barriers wait for this
+                                    many CTAs beyond the launch, so the first wait runs out (after
+                                    about 2 s), the kernel ends and the call returns LEPIC_ETIMEOUT */
+    int64_t fortran_max_subrecord; /* backup writer: subrecord length limit (2^31 - 9, the Intel and
+                                    GNU runtimes' value); smaller values exercise the layout         */
+} lepic_options;
+int lepic_gpu_get_options(lepic_ctx *ctx, lepic_options *out);
+int lepic_gpu_set_options(lepic_ctx *ctx, const lepic_options *in);
+
 /* Copies a device grid (LEPIC_GRID_*) to the host, FP64, in the layouts above. */
 int lepic_gpu_get_grid(lepic_ctx *ctx, int32_t which, double *out);
 /* Sets phi (LEPIC_GRID_PHI) or rhs (LEPIC_GRID_RHS) from the host. */

@@ -181,6 +181,13 @@ class LepicTallies(C.Structure):
 
 _FP = C.POINTER(C.c_float)
 
+
+class LepicOptions(C.Structure):
+    _fields_ = [("mx_nu1", C.c_int32), ("mx_nu2", C.c_int32), ("mx_nuc", C.c_int32), ("mx_omega", C.c_float),
+                ("mx_onchip_bytes", C.c_int32), ("mx_tiled", C.c_int32), ("mx_max_iter", C.c_int32),
+                ("mg_small_nodes", C.c_int32), ("ctas_per_sm", C.c_int32), ("barrier_extra", C.c_int32),
+                ("fortran_max_subrecord", C.c_int64)]
+
 PROTOTYPES = {
     "lepic_gpu_abi_version": (C.c_int32, []),
     "lepic_gpu_create": (C.c_int, [C.POINTER(LepicConfig), _IP, _DP, _DP, C.POINTER(LepicXsTables),
@@ -203,6 +210,8 @@ PROTOTYPES = {
     "lepic_gpu_collisions": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicMccStats)]),
     "lepic_gpu_push_deposit": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicPushStats)]),
     "lepic_gpu_step": (C.c_int, [_VP, C.c_int32, C.c_double, C.c_int32]),
+    "lepic_gpu_get_options": (C.c_int, [_VP, C.POINTER(LepicOptions)]),
+    "lepic_gpu_set_options": (C.c_int, [_VP, C.POINTER(LepicOptions)]),
     "lepic_gpu_get_grid": (C.c_int, [_VP, C.c_int32, _DP]),
     "lepic_gpu_set_grid": (C.c_int, [_VP, C.c_int32, _DP]),
     "lepic_gpu_get_push_stats": (C.c_int, [_VP, C.POINTER(LepicPushStats)]),

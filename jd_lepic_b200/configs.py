@@ -58,11 +58,20 @@ class Case:
     flag_pbc: int = 0
     flag_spec: int = 0
     flag_nmn: int = 0
+    # particle decomposition over MPI ranks (load_part.f90:96): ppc is the deck's np_cell, the
+    # particles per cell of all ranks together, which sets Nm = n0 Vc / np_cell (main.f90:471);
+    # each rank loads NINT(np_cell n_cell / nproc_mpi) of them, and rho is summed over ranks
+    nproc_mpi: int = 1
     extra: dict = field(default_factory=dict)
 
     @property
     def n_particles(self) -> int:
         return self.ppc * self.nx * self.ny
+
+    @property
+    def n_load(self) -> int:
+        """Particles per species that one rank loads (load_part.f90:96, nproc = 1 per rank)."""
+        return int(math.floor(self.n_particles / self.nproc_mpi + 0.5))
 
     def levels(self) -> int:
         if self.ng:

@@ -9,7 +9,7 @@
 #include <vector>
 #include "cnn.cuh"
 
-#define LEPIC_ABI_VERSION 2
+#define LEPIC_ABI_VERSION 3
 
 extern "C" int32_t lepic_gpu_abi_version(void) { return LEPIC_ABI_VERSION; }
 
@@ -283,12 +283,57 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
     return LEPIC_OK;
 }
 
+static lepic_options default_options() {
+    lepic_options o;
+    memset(&o, 0, sizeof(o));
+    o.mx_nu1 = 2; o.mx_nu2 = 2; o.mx_nuc = 2;
+    o.mx_omega = 1.15f;
+    o.mx_onchip_bytes = 20 * 1024;
+    o.mx_tiled = 1;
+    o.mx_max_iter = 200;
+    o.mg_small_nodes = 4500;
+    o.ctas_per_sm = 3;
+    o.barrier_extra = 0;
+    o.fortran_max_subrecord = 2147483639ll;
+    return o;
+}
+
+extern "C" int lepic_gpu_get_options(lepic_ctx *c, lepic_options *out) {
+    if (!c || !out) return LEPIC_EINVAL;
+    *out = c->opt;
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_set_options(lepic_ctx *c, const lepic_options *in) {
+    if (!c || !in) return LEPIC_EINVAL;
+    const lepic_options &o = *in;
+    if (o.mx_nu1 < 1 || o.mx_nu1 > 8 || o.mx_nu2 < 1 || o.mx_nu2 > 8 || o.mx_nuc < 1 || o.mx_nuc > 64 ||
+        !(o.mx_omega > 0.0f && o.mx_omega < 2.0f) || o.mx_onchip_bytes < 0 || o.mx_onchip_bytes > 96 * 1024 ||
+        (o.mx_tiled != 0 && o.mx_tiled != 1) || o.mx_max_iter < 1 || o.mg_small_nodes < 0 || o.ctas_per_sm < 1 ||
+        o.ctas_per_sm > 8 || o.barrier_extra < 0 || o.barrier_extra > 1024 || o.fortran_max_subrecord < 8 ||
+        o.fortran_max_subrecord > 2147483639ll) {
+        c->last_err = "set_options: a value is out of range";
+        return LEPIC_EINVAL;
+    }
+    // the work list of a cooperative launch depends on these: wait for launches in flight
+    LCUDA(cudaStreamSynchronize(c->stream));
+    const bool relaunch = o.ctas_per_sm != c->opt.ctas_per_sm;
+    c->opt = o;
+    if (relaunch) {
+        c->mg_grid_mixed = 0;  // sized again at the next mixed solve
+        int r = mg_init(c);
+        if (r != LEPIC_OK) return r;
+    }
+    return LEPIC_OK;
+}
+
 extern "C" int lepic_gpu_create(const lepic_config *cfg, const int32_t *bcnd, const double *phi_init,
                                 const double *Bi, const lepic_xs_tables *xs, lepic_ctx **out) {
     if (!cfg || !out) return LEPIC_EINVAL;
     *out = nullptr;
     lepic_ctx *c = new (std::nothrow) lepic_ctx();
     if (!c) return LEPIC_ENOMEM;
+    c->opt = default_options();
     int r = create_impl(c, cfg, bcnd, phi_init, Bi, xs);
     if (r != LEPIC_OK) {
         static std::string keep;

@@ -177,14 +177,11 @@ struct RecReader {
     }
 };
 
-static long long max_subrecord() {
-    // test hook: a smaller subrecord limit exercises the multi-subrecord layout
-    const char *e = getenv("LEPIC_FORTRAN_MAX_SUBRECORD");
-    if (e) {
-        long long v = atoll(e);
-        if (v >= 8 && v <= kMaxSub) return v;
-    }
-    return kMaxSub;
+// a smaller subrecord limit (lepic_options::fortran_max_subrecord) exercises the
+// multi-subrecord layout with small files
+static long long max_subrecord(const lepic_ctx *c) {
+    const long long v = c->opt.fortran_max_subrecord;
+    return (v >= 8 && v <= kMaxSub) ? v : kMaxSub;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -250,7 +247,7 @@ extern "C" int lepic_gpu_write_backup(lepic_ctx *c, const char *path, double tim
     if (!f) { c->last_err = std::string("cannot open ") + path; cleanup(); return LEPIC_EINVAL; }
     RecWriter w;
     w.f = f;
-    w.max_sub = max_subrecord();
+    w.max_sub = max_subrecord(c);
     w.begin(8 + 4 + 8);
     w.write(&time, 8); w.write(&gtype, 4); w.write(&Pabs_cor, 8);
     w.end();

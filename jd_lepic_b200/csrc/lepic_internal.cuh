@@ -116,6 +116,7 @@ struct SpeciesBuf {
 
 struct lepic_ctx {
     lepic_config cfg;
+    lepic_options opt;         // solver settings (lepic_gpu_set_options), defaults at create
     int dev = 0, num_sms = 0;
     cudaStream_t stream = nullptr;
     int S = 0;                 // fractional bits of the fixed-point positions

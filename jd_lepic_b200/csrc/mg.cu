@@ -34,6 +34,7 @@ struct MGP {
     int ncycl, pbc, nmn, mode;
     double *partials;
     DevCounters *cnt;
+    unsigned bar_extra;        // lepic_options::barrier_extra
 };
 
 #include "mg_common.cuh"
@@ -250,7 +251,7 @@ __device__ void small_region(const MGP &P, int k, double *res, int *iter) {
 
 // mg.f90:85-225 -- one V-cycle; *res is the L1 residual of the last finest-level sweep
 __device__ bool vcycle(const MGP &P, int k, double *res, int *iter) {
-    BigTeam B{P.cnt, P.partials};
+    BigTeam B{P.cnt, P.partials, P.bar_extra};
     const int ng = P.ng, Ls = P.Ls;
     int ks;
     for (int l = 0; l < Ls && l <= ng - 2; l++) {
@@ -314,7 +315,7 @@ __device__ bool l2_norms(const Team &T, const MGDev &L, double *rr, double *bb) 
 // iterative_solver.f90:18-66.  mode 0: stop on the reference's normalised L1 residual;
 // mode 2: same cycles, stop on ||b-Au||_2/||b-Au_D||_2 <= eps.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_solve(MGP P) {
-    BigTeam B{P.cnt, P.partials};
+    BigTeam B{P.cnt, P.partials, P.bar_extra};
     int iter[LEPIC_MAXLEV];
     for (int i = 0; i < LEPIC_MAXLEV; i++) iter[i] = 0;
     double res = 0.0, res_s = 0.0, rr = 0.0, bb = 0.0;
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_solve(MGP P) {
 
 // Stats only: the L1 and L2 residuals of the current phi.
 __global__ void __launch_bounds__(MG_THREADS) k_mg_stats(MGP P) {
-    BigTeam B{P.cnt, P.partials};
+    BigTeam B{P.cnt, P.partials, P.bar_extra};
     double res = 0.0, rr = 0.0, bb = 0.0;
     if (!residual_l1(B, P.L[0], &res)) return;
     if (!l2_norms(B, P.L[0], &rr, &bb)) return;
@@ -382,8 +383,7 @@ static MGP mg_params(lepic_ctx *c, double eps, int mode) {
         d.u = a.u; d.b = a.b; d.bc = a.bc;
     }
     P.ng = c->nlev;
-    long long small_nodes = 4500;
-    if (const char *e = getenv("LEPIC_MG_SMALL_NODES")) small_nodes = atoll(e);
+    const long long small_nodes = c->opt.mg_small_nodes;
     int Ls = c->nlev;
     for (int l = 0; l < c->nlev; l++)
         if ((long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1) <= small_nodes) { Ls = l; break; }
@@ -397,6 +397,7 @@ static MGP mg_params(lepic_ctx *c, double eps, int mode) {
     P.mode = mode;
     P.partials = c->partials;
     P.cnt = c->dcnt;
+    P.bar_extra = (unsigned)c->opt.barrier_extra;
     return P;
 }
 
@@ -404,9 +405,7 @@ int mg_init(lepic_ctx *c) {
     int occ = 0;
     LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_solve, MG_THREADS, 0));
     if (occ < 1) { c->last_err = "multigrid kernel does not fit on an SM"; return LEPIC_ECUDA; }
-    int per_sm = 3;
-    if (const char *e = getenv("LEPIC_MG_CTAS_PER_SM")) per_sm = atoi(e);
-    c->mg_grid = c->num_sms * std::max(1, std::min(occ, per_sm));
+    c->mg_grid = c->num_sms * std::max(1, std::min(occ, (int)c->opt.ctas_per_sm));
     return LEPIC_OK;
 }
 

@@ -12,10 +12,11 @@
 struct BigTeam {
     DevCounters *c;
     double *partials;          // 2 * gridDim.x doubles
+    unsigned extra = 0;        // CTAs the barrier waits for beyond the launch (a test hook, 0 in use)
     mutable unsigned phase = 0;
     __device__ long long rank() const { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
     __device__ long long size() const { return (long long)gridDim.x * blockDim.x; }
-    __device__ bool sync() const { return grid_barrier(c, gridDim.x); }
+    __device__ bool sync() const { return grid_barrier(c, gridDim.x + extra); }
 };
 struct SmallTeam {
     __device__ long long rank() const { return threadIdx.x; }

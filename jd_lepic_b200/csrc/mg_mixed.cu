@@ -43,6 +43,7 @@ struct MXP {
     double *r64, *p64, *ap64;  // finest-level CG vectors, (nx+3)(ny+3)
     double *partials;
     DevCounters *cnt;
+    unsigned bar_extra;        // lepic_options::barrier_extra
     int soff_e[LEPIC_MAXLEV], soff_r[LEPIC_MAXLEV], soff_b[LEPIC_MAXLEV]; // shared-memory copies
     int smem_bytes;
     int tiled;       // 1: the big levels smooth in shared-memory tiles (temporal blocking)
@@ -488,7 +489,7 @@ __device__ void small_cycle(const MXP &P) {
 
 // one symmetric V-cycle on A e = r32 of level 0, from e = 0 (the caller zeroes e)
 __device__ bool vcycle32(const MXP &P) {
-    BigTeam B{P.cnt, P.partials};
+    BigTeam B{P.cnt, P.partials, P.bar_extra};
     const int ng = P.ng, Ls = P.Ls;
     if (P.tiled) { // Ls <= ng - 1: the small cycle takes the coarse levels
         for (int l = 0; l < Ls; l++) {
@@ -720,7 +721,7 @@ __device__ bool update_ur(const BigTeam &B, const MXP &P, double alpha, double *
 }
 
 __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
-    BigTeam B{P.cnt, P.partials};
+    BigTeam B{P.cnt, P.partials, P.bar_extra};
     double bb = 0.0, rr = 0.0, l1 = 0.0, rz = 0.0, pap = 0.0;
     if (!true_residual<true>(B, P, &rr, &l1, &bb)) return;
     const double b0 = sqrt(bb), tol = P.eps * b0;
@@ -796,8 +797,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     P.ng = c->nlev;
     // the coarsest levels whose e, r and mask fit together in CTA 0's shared-memory budget
     // run on chip; the finer ones use the whole grid
-    long long budget = 20 * 1024;  // levels of 32^2 nodes and coarser (measured best at 2048^2)
-    if (const char *e = getenv("LEPIC_MX_SMEM")) budget = atoll(e);
+    const long long budget = c->opt.mx_onchip_bytes;  // 20 KiB: 32^2 nodes and coarser (best at 2048^2)
     auto level_bytes = [&](int l) {
         const long long nn = (long long)(c->lev[l].nx + 3) * (c->lev[l].ny + 3);
         const long long nr = (long long)(c->lev[l].nx + 1) * (c->lev[l].ny + 1);
@@ -827,12 +827,8 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     // sweeps and 4 with three.
     // two sweeps each way on the coarsest level (3^2 nodes at 2048^2): eight gave the same
     // iteration counts and residuals and cost CTA 0's 28 more barriers per cycle
-    P.omega = 1.15f;
-    P.nu1 = 2; P.nu2 = 2; P.nuc = 2; P.max_iter = 200;
-    if (const char *e = getenv("LEPIC_MX_NUC")) P.nuc = atoi(e);
-    if (const char *e = getenv("LEPIC_MX_OMEGA")) P.omega = (float)atof(e);
-    if (const char *e = getenv("LEPIC_MX_NU1")) P.nu1 = atoi(e);
-    if (const char *e = getenv("LEPIC_MX_NU2")) P.nu2 = atoi(e);
+    P.omega = c->opt.mx_omega;
+    P.nu1 = c->opt.mx_nu1; P.nu2 = c->opt.mx_nu2; P.nuc = c->opt.mx_nuc; P.max_iter = c->opt.mx_max_iter;
     // tiles: region (TX + 2H) x (TY + 2H) with H = 2 nu + 2 (down) or 2 nu (up); e, r (FP32)
     // and the mask per node, sharing the dynamic shared memory with the small cycle
     const int Hmax = 2 * std::max(P.nu1 + 1, P.nu2);
@@ -855,7 +851,7 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     }
     const long long coarse_cap = (long long)((MX_TX + 2 * Hmax) / 2 + 3) * ((MX_TY + 2 * Hmax) / 2 + 3);
     const long long tile_bytes = (long long)P.tile_cap * 9 + coarse_cap * 4 + 16;
-    P.tiled = (Ls <= c->nlev - 1 && Ls >= 1 && !getenv("LEPIC_MX_UNTILED") && tile_bytes <= 64 * 1024) ? 1 : 0;
+    P.tiled = (Ls <= c->nlev - 1 && Ls >= 1 && c->opt.mx_tiled && tile_bytes <= 64 * 1024) ? 1 : 0;
     P.smem_bytes = (int)std::max(off, P.tiled ? tile_bytes : 0ll);
     P.eps = eps;
     P.alpha = fabs((double)(c->cfg.nx + 1) * (c->cfg.ny + 1) * P.L[0].acd);
@@ -864,15 +860,14 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     P.r64 = c->cg_r; P.p64 = c->cg_p; P.ap64 = c->cg_ap;
     P.partials = c->partials;
     P.cnt = c->dcnt;
+    P.bar_extra = (unsigned)c->opt.barrier_extra;
     const size_t smem = (size_t)P.smem_bytes;
     if (c->mg_grid_mixed == 0) {
         LCUDA(cudaFuncSetAttribute(k_mg_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         int occ = 0;
         LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_mixed, MG_THREADS, smem));
         if (occ < 1) { c->last_err = "mixed multigrid kernel does not fit on an SM"; return LEPIC_ECUDA; }
-        int per_sm = 3;
-        if (const char *e = getenv("LEPIC_MG_CTAS_PER_SM")) per_sm = atoi(e);
-        c->mg_grid_mixed = c->num_sms * std::max(1, std::min(occ, per_sm));
+        c->mg_grid_mixed = c->num_sms * std::max(1, std::min(occ, (int)c->opt.ctas_per_sm));
     }
     void *args[] = {&P};
     LCUDA(cudaMemsetAsync(&c->dcnt->bar_count, 0, 3 * sizeof(unsigned int), c->stream));

@@ -84,7 +84,7 @@ class GpuSimulation:
     """One device context running a Case through the C ABI."""
 
     def __init__(self, case: Case, tile=(16, 16), capacity_factor: float = 1.3, load: bool = True,
-                 capacity: int | None = None):
+                 capacity: int | None = None, config: dict | None = None):
         self.lib = capi.load_library()
         self.case = case
         self.deck = dk.read_reactions(case.deck_text, case.ngas)
@@ -111,11 +111,13 @@ class GpuSimulation:
         cfg.ng = case.levels()
         cfg.ncycl = 20000  # main.f90:261
         cfg.omega = 1.4    # iterative_solver.f90:28
-        cap = capacity if capacity is not None else int(case.n_particles * capacity_factor) + 4096
+        cap = capacity if capacity is not None else int(case.n_load * capacity_factor) + 4096
         for s in range(self.sp.ntype):
             cfg.capacity[s] = cap
         cfg.seed = case.seed
         cfg.tile_w, cfg.tile_h = (tile if tile else (0, 0))
+        for k, v in (config or {}).items():   # lepic_config fields set by name (e.g. ncycl)
+            setattr(cfg, k, v)
         self.cfg = cfg
         self._bcnd = np.ascontiguousarray(case.bcnd, dtype=np.int32)
         self._phi0 = np.ascontiguousarray(case.phi0, dtype=np.float64)
@@ -145,7 +147,7 @@ class GpuSimulation:
 
     def load(self, n: int | None = None, seed: int | None = None):
         c = self.case
-        spec = capi.LepicLoadSpec(n if n is not None else c.n_particles, c.profile, 0.0, c.n_peak,
+        spec = capi.LepicLoadSpec(n if n is not None else c.n_load, c.profile, 0.0, c.n_peak,
                                   c.n_floor, c.sigma, seed if seed is not None else c.seed)
         self.check(self.lib.lepic_gpu_load_particles(self.ctx, C.byref(spec)), "load_particles")
         self.check(self.lib.lepic_gpu_charge_deposition(self.ctx), "charge_deposition")
@@ -284,6 +286,20 @@ class GpuSimulation:
         self.check(self.lib.lepic_gpu_read_backup(self.ctx, path.encode(), C.byref(t), C.byref(gt), C.byref(pc)),
                    "read_backup")
         return t.value, gt.value, pc.value
+
+    def options(self) -> capi.LepicOptions:
+        o = capi.LepicOptions()
+        self.check(self.lib.lepic_gpu_get_options(self.ctx, C.byref(o)), "get_options")
+        return o
+
+    def set_options(self, **kw):
+        """Changes solver settings by name (lepic_options fields); returns the previous ones."""
+        old = self.options()
+        o = capi.LepicOptions.from_buffer_copy(old)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        self.check(self.lib.lepic_gpu_set_options(self.ctx, C.byref(o)), "set_options")
+        return old
 
     def stream_ptr(self) -> int:
         return self.lib.lepic_gpu_stream(self.ctx) or 0

@@ -276,6 +276,54 @@ def align_survivors(got: np.ndarray, ref: np.ndarray, dx: float, dy: float, wind
     return np.asarray(gi, dtype=np.int64), np.asarray(rj, dtype=np.int64), g_only, r_only
 
 
+DEP_SHIFT = 44   # the device's accumulators hold CIC weights in units of 2^-44
+
+
+def int_deposit(X, Y, nx: int, ny: int, S: int) -> np.ndarray:
+    """The device's charge accumulator of one species, restated in numpy: uint64 CIC weights of
+    fixed-point positions (cell = X >> S, offset = X & (2^S - 1)), the products of the offsets
+    rounded to 2^-44 (part_expmover.f90:540-575 in integer form), node i + j (nx+3) of
+    np(0:nx+2, 0:ny+2).  Integer sums: any split of the particles over ranks sums to the same
+    grid (calc_rho.f90:71-74)."""
+    X = np.asarray(X, dtype=np.int64)
+    Y = np.asarray(Y, dtype=np.int64)
+    W = nx + 3
+    acc = np.zeros((ny + 3) * W, dtype=np.uint64)
+    mask = (1 << S) - 1
+    fx = (X & mask).astype(np.uint64)
+    fy = (Y & mask).astype(np.uint64)
+    A = np.uint64(1 << S)
+    ax, ay = A - fx, A - fy
+    sh = 2 * S - DEP_SHIFT
+    ix = (X >> S) + 1
+    iy = (Y >> S) + 1
+    for w, ddx, ddy in ((ax * ay, 0, 0), (fx * ay, 1, 0), (fx * fy, 1, 1), (ax * fy, 0, 1)):
+        if sh > 0:
+            w = (w + np.uint64(1 << (sh - 1))) >> np.uint64(sh)
+        elif sh < 0:
+            w = w << np.uint64(-sh)
+        np.add.at(acc, (ix + ddx) + (iy + ddy) * W, w)
+    return acc
+
+
+def np_from_acc(cfg, ptype: int, acc: np.ndarray, kq: np.ndarray) -> np.ndarray:
+    """np(0:nx+2, 0:ny+2) of one species from its accumulator, as the device scales it:
+    kq * (k1 * (acc 2^-44)), k1 = Nm / (dx dy zmax)."""
+    k1 = cfg.Nm[ptype] / (cfg.dx * cfg.dy * cfg.zmax)
+    w = np.asarray(acc, dtype=np.uint64).astype(np.float64) * 5.684341886080802e-14
+    return (np.asarray(kq, dtype=np.float64).ravel() * (k1 * w)).reshape(cfg.ny + 3, cfg.nx + 3)
+
+
+def dens_red(cfg, npg, bcnd):
+    """o_dens_red (calc_rho.f90:134-199): returns (np_red (ntype, ny+3, nx+3), np_mx[ntype])."""
+    ntype = cfg.ntype
+    a = np.ascontiguousarray(npg, dtype=np.float64)
+    out = np.zeros((ntype, cfg.ny + 3, cfg.nx + 3))
+    c = OCfg.from_buffer_copy(cfg)
+    lib().o_dens_red(C.byref(c), dp(a), dp(out), ip(np.ascontiguousarray(bcnd, dtype=np.int32)))
+    return out, np.array(c.np_mx[:ntype])
+
+
 def deposit(cfg, ptype, vxp, n, kq, npg):
     lib().o_charge_deposition(C.byref(cfg), ptype, dp(vxp), n, dp(kq), dp(npg))
 

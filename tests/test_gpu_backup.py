@@ -12,17 +12,12 @@ from jd_lepic_b200.simulation import GpuSimulation
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture
-def small_subrecords(monkeypatch):
-    # 1000-byte subrecords: every particle record of these tests is split
-    monkeypatch.setenv("LEPIC_FORTRAN_MAX_SUBRECORD", "1000")
-
-
-def test_write_then_read_round_trip(gpu_lib, tmp_path, small_subrecords):
+def test_write_then_read_round_trip(gpu_lib, tmp_path):
     case = configs.case0(ppc=4, nx=64, ny=64)
     a = GpuSimulation(case)
     b = GpuSimulation(case, load=False)
     try:
+        a.set_options(fortran_max_subrecord=1000)   # every particle record is split
         a.push(1)                                   # some particles are lost: holes are skipped
         a.deposit()
         path = str(tmp_path / "particles000.bak")
@@ -44,7 +39,7 @@ def test_write_then_read_round_trip(gpu_lib, tmp_path, small_subrecords):
         b.close()
 
 
-def test_read_file_of_two_threads(gpu_lib, tmp_path, small_subrecords):
+def test_read_file_of_two_threads(gpu_lib, tmp_path):
     case = configs.case0(ppc=4, nx=64, ny=64)
     sim = GpuSimulation(case, load=False)
     try:
@@ -123,3 +118,27 @@ def test_slab_layout_put_get(gpu_lib):
             assert np.array_equal(got, np.concatenate([vxp[p, s, :np_tot[p, s]] for p in range(nproc)]))
     finally:
         sim.close()
+
+
+def test_truncated_backup_is_rejected(gpu_lib, tmp_path):
+    """A backup cut short (in the header, inside a particle record, before the last length
+    marker) is refused with LEPIC_EINVAL; the context keeps its particles and stays usable."""
+    case = configs.case0(ppc=2, nx=32, ny=32)
+    a = GpuSimulation(case)
+    b = GpuSimulation(case, load=False)
+    try:
+        full = str(tmp_path / "full.bak")
+        a.write_backup(full, 1.0, 0, 1.0)
+        data = open(full, "rb").read()
+        for cut in (10, 40, len(data) // 2, len(data) - 4, len(data) - 1):
+            p = str(tmp_path / f"cut{cut}.bak")
+            open(p, "wb").write(data[:cut])
+            rc = b.lib.lepic_gpu_read_backup(b.ctx, p.encode(), None, None, None)
+            assert rc == capi.EINVAL, cut
+            assert b.push_stats()["np_tot"] == [0, 0], cut
+        b.read_backup(full)
+        for s in (0, 1):
+            assert np.array_equal(b.get_particles(s), a.get_particles(s))
+    finally:
+        a.close()
+        b.close()

@@ -418,7 +418,7 @@ def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n):
     rhs = _perturbed_rhs(s, case)
     set_rhs(s, rhs)
     tiled = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=case.phi0.copy())
-    monkeypatch.setenv("LEPIC_MX_UNTILED", "1")
+    s.set_options(mx_tiled=0)
     grid = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=case.phi0.copy())
     assert tiled["cycles"] == grid["cycles"]
     assert np.array_equal(tiled["phi"], grid["phi"])
