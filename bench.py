@@ -5,12 +5,14 @@ push+deposit) on the 2048x2048 aperture-plate workload, one B200 per rank.
 
 Prints ONE JSON line (rank 0).  Timing: CUDA events on the library's own stream, barrier +
 synchronize on both sides, max over ranks.  The particle arrays (8.4 GB per species) are far
-larger than L2, so no L2 flush is needed between steps.  Weak scaling for N > 1: every rank
-holds the full per-GPU particle load of the same plasma and the int64 charge accumulators are
-summed with one NCCL all-reduce per step (exact, order-free); Poisson is solved replicated.
+larger than L2, so no L2 flush is needed between steps.  Weak scaling for N > 1: the particles
+are decomposed over the ranks as the reference does (load_part.f90:96), each rank holding one
+GPU's workload at Nm / N, and the int64 charge accumulators are summed with one NCCL
+all-reduce per step (exact, order-free); Poisson is solved replicated.
 
-``--impl reference`` times the CPU restatement of the same routines (OpenMP, all host cores)
-on a bounded sample of the same workload and extrapolates to the full particle count.
+``--impl reference`` runs and times the CPU restatement of the same routines (OpenMP, all host
+cores) on a bounded sample of the same workload: the configuration at its own particles per
+cell on a smaller box (``--cpu-cells``), every phase measured and nothing scaled.
 """
 from __future__ import annotations
 
@@ -113,15 +115,22 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-def cpu_baseline(case, sample_particles: int, steps: int, warmup: int, nthreads: int) -> dict:
-    """CPU restatement (OpenMP, `nthreads`) of the same step on `sample_particles` particles per
-    species with the full grid; the particle part is scaled to the full particle count."""
-    from oracle import oracle as O
-    from jd_lepic_b200.simulation import mean_density
+def sample_case(config: int, cells: int):
+    """The bounded CPU sample of a workload: the same configuration (deck, walls, fields, its own
+    particles per cell) on a box of `cells` cells along x, the aspect ratio kept."""
+    from jd_lepic_b200 import configs
+    full = configs.make_case(config)
+    if cells >= full.nx:
+        return full, full
+    ny = max(16, cells * full.ny // full.nx)
+    return full, configs.make_case(config, nx=cells, ny=ny)
 
-    rng = np.random.default_rng(case.seed)
-    n = sample_particles
-    # positions: uniform or the Gaussian profile by rejection, outside the wall cells
+
+def cpu_particles(case, spp, seed: int) -> dict:
+    """Initial particles of a case for the CPU restatement: the load profile (uniform, or the
+    Gaussian by rejection) outside the wall cells, Maxwellian velocities at vt0."""
+    rng = np.random.default_rng(seed)
+    n = case.n_particles
     L = case.nx * case.dx
     pts = []
     while sum(len(p) for p in pts) < n:
@@ -138,60 +147,47 @@ def cpu_baseline(case, sample_particles: int, steps: int, warmup: int, nthreads:
         wall = (b[iy, ix] >= 1) & (b[iy, ix + 1] >= 1) & (b[iy + 1, ix + 1] >= 1) & (b[iy + 1, ix] >= 1)
         pts.append(np.stack([x[~wall], y[~wall]], 1))
     xy = np.concatenate(pts)[:n]
-    sim = None
     parts = {}
-    from jd_lepic_b200 import deck as dk
-    from jd_lepic_b200.simulation import species_params
-    d = dk.read_reactions(case.deck_text, case.ngas)
-    spp = species_params(case, d)
     for s in range(spp.ntype):
         p = np.zeros((n, 6))
         p[:, :2] = xy
         p[:, 3:] = rng.normal(0, spp.vt0[s] / np.sqrt(2), (n, 3))
         parts[s] = p
-    # the sample carries the full charge: macro-weights scaled by N_full / n
-    sim = O.OracleSimulation(case, nthreads=nthreads, particles=parts, seed=123456)
-    scale = case.n_particles / n
-    for s in range(spp.ntype):
-        sim.cfg.Nm[s] = spp.Nm[s] * scale
-    sim.deposit_all()
-    t_grid, t_part = [], []
-    import ctypes as C
-    for it in range(2, warmup + steps + 2):  # steps without sort/MCC; those are timed below
-        t0 = time.perf_counter()
-        sim.rhs = O.calc_rhs(sim.cfg, sim.npg)
-        rc, _st = O.solve(sim.cfg, sim.phi, sim.rhs, sim.bcnd, sim.ng, case.eps if case.poisson_mode == 0 else 1e-8,
-                          nthreads=nthreads)
-        O.efield(sim.cfg, sim.phi, sim.bcnd, sim.Ei)
-        t1 = time.perf_counter()
-        sim.npg[:] = 0.0
-        for s in range(spp.ntype):
-            nn = C.c_int64(sim.np_tot[s])
-            O.lib().o_push_deposit_omp(C.byref(sim.cfg), s, O.dp(sim.Ei), O.dp(sim.Bi), O.ip(sim.bcnd), O.dp(sim.kq),
-                                       O.dp(sim.vxp[s]), C.byref(nn), sim.flag_dead[s].ctypes.data_as(O._I8),
-                                       O.dp(sim.npg[s]), nthreads)
-            sim.np_tot[s] = nn.value
-        t2 = time.perf_counter()
-        if it > warmup + 1:
-            t_grid.append(t1 - t0)
-            t_part.append(t2 - t1)
+    return parts
+
+
+def cpu_baseline(config: int, cells: int, steps: int, warmup: int, nthreads: int) -> dict:
+    """The step restated on the CPU (the oracle port: FP64, OpenMP over `nthreads` host threads,
+    the reference's loop structure), run and timed as it is on a bounded sample of the workload
+    (sample_case): calc_rhs, the reference's FP64 V-cycles stopped on the same relative L2
+    residual as the device (1e-8; the L1 tolerance of mode-0 configurations), calc_Efield,
+    part_sorting and collisions at their 1-in-10 cadence (main.f90:479-480), the mover and the
+    deposit.  Every phase is measured; nothing is scaled."""
+    from oracle import oracle as O
+    from jd_lepic_b200 import deck as dk
+    from jd_lepic_b200.simulation import species_params
+    full, case = sample_case(config, cells)
+    spp = species_params(case, dk.read_reactions(case.deck_text, case.ngas))
+    sim = O.OracleSimulation(case, nthreads=nthreads, particles=cpu_particles(case, spp, case.seed), seed=123456)
+    l2 = case.poisson_mode != 0
+    eps = 1e-8 if l2 else case.eps
+    it = 1
+    for _ in range(warmup):
+        sim.step(it, eps, l2)
+        it += 1
+    done = 0
     t0 = time.perf_counter()
-    for s in range(spp.ntype):
-        O.sort(sim.cfg, sim.vxp[s], sim.np_tot[s])
-    t_sort = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    sim.collide()
-    t_mcc = time.perf_counter() - t0
-    # per step, with sort and MCC at their 1-in-10 cadence (main.f90:479-480)
-    grid_s = float(np.mean(t_grid))
-    part_s = (float(np.mean(t_part)) + (t_sort + t_mcc) / 10.0) * scale
-    step_s = grid_s + part_s
-    total = case.n_particles * spp.ntype
-    return {"value": total / step_s, "unit": "particle-steps/s", "cores": nthreads, "kind": "port",
-            "step_ms_extrapolated": step_s * 1e3, "grid_ms": grid_s * 1e3, "particle_ms_extrapolated": part_s * 1e3,
-            "sample": (f"{n} particles/species (of {case.n_particles}) on the full {case.nx}x{case.ny} grid, "
-                       f"{steps} steps after {warmup} warm-up; Poisson+E measured on the full grid, "
-                       f"particle phases scaled by {scale:.1f}")}
+    for _ in range(steps):
+        done += sum(sim.np_tot)
+        sim.step(it, eps, l2)
+        it += 1
+    t = time.perf_counter() - t0
+    return {"value": done / t, "unit": "particle-steps/s", "cores": nthreads, "kind": "port",
+            "ms_per_step": t / steps * 1e3,
+            "sample": (f"{full.name} at its {case.ppc} particles per cell on a {case.nx}x{case.ny}-cell box "
+                       f"({case.n_particles} particles per species; the full workload is {full.nx}x{full.ny}, "
+                       f"{full.n_particles} per species): {steps} steps after {warmup}, every phase measured, "
+                       f"Poisson to {'relative L2 ' if l2 else 'L1 '}{eps:g}")}
 
 
 def host_threads() -> int:
@@ -207,20 +203,19 @@ def run_reference(args):
     if rank != 0:
         return 0
     from jd_lepic_b200 import configs
-    case = configs.make_case(args.config)
+    full = configs.make_case(args.config)
     nt = host_threads()
-    sample = args.cpu_sample
     t0 = time.perf_counter()
-    # each step is a bounded sample; at most 20 timed steps keep the run within minutes
-    cb = cpu_baseline(case, sample, min(args.steps, 20), min(args.warmup, 3), nt)
+    cb = cpu_baseline(args.config, args.cpu_cells, args.steps, args.warmup, nt)
     wall = time.perf_counter() - t0
     line = {"metric": "particle-steps/s per PIC step (push+deposit+MCC+sort+Poisson to 1e-8)",
             "value": cb["value"], "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": cb["step_ms_extrapolated"], "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": case.name, "particles_per_species": case.n_particles, "grid": [case.nx, case.ny],
-                       "poisson": "reference multigrid (FP64, L1 criterion) on the CPU"},
+            "config": {"workload": full.name, "particles_per_species": full.n_particles, "grid": [full.nx, full.ny],
+                       "poisson": "the reference's multigrid (FP64) on the CPU, relative L2 residual 1e-8",
+                       "sample": cb["sample"]},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -580,7 +575,7 @@ def run_ours(args):
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(case, args.cpu_sample, 3, 1, host_threads())
+        cb = cpu_baseline(args.config, args.cpu_cells, 5, 2, host_threads())
     line = None
     if rank == 0:
         # kernels of this library launched in the timed steps (memsets/copies not counted):
@@ -640,7 +635,8 @@ def main():
     ap.add_argument("--config", type=int, default=4)
     ap.add_argument("--mode", type=int, default=1)
     ap.add_argument("--tile", type=int, default=16)
-    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--cpu-cells", type=int, default=512,
+                    help="cells along x of the CPU baseline's sample box (the workload's ppc kept)")
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell (profiling runs)")
     ap.add_argument("--nx", type=int, default=0, help="override the grid to nx x nx cells (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

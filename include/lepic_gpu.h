@@ -36,7 +36,9 @@ extern "C" {
 #define LEPIC_EDIVERGED (-5)  /* Poisson residual grew 10x: iterative_solver.f90:42-50  */
 #define LEPIC_ETIMEOUT (-6)   /* a bounded device-side wait gave up                     */
 #define LEPIC_ERANGE (-7)     /* Pmax > 1 (collisions.f90:119-123) or a bad cell index  */
-#define LEPIC_ENOTCONV (-8)   /* ncycl V-cycles without reaching eps                    */
+#define LEPIC_ENOTCONV (-8)   /* ncycl V-cycles (mixed: the CG cap) without reaching eps;
+                                 phi holds the last iterate, with which the reference's
+                                 iterative_solver.f90:56 goes on: a host may continue       */
 #define LEPIC_ENOKERNEL (-9)  /* the library was not built for this GPU                 */
 
 #define LEPIC_MAXSP 8   /* species (charged + neutral)  */

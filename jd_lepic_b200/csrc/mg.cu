@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_solve(MGP P) {
     int k = 1;
     if (P.mode == 2 && !l2_norms(B, P.L[0], &rr, &bb)) return;
     const double b0 = sqrt(bb);
+    bool conv = false;
     for (;;) {
         if (!vcycle(P, k, &res, iter)) return;
         res = res / P.alpha;
@@ -332,7 +333,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_solve(MGP P) {
             if (blockIdx.x == 0 && threadIdx.x == 0) set_err(P.cnt, LERR_DIVERGED, 500);
             return; // every CTA takes the same decision
         }
-        bool conv;
         if (P.mode == 2) {
             if (!l2_norms(B, P.L[0], &rr, &bb)) return;
             conv = sqrt(rr) <= P.eps * b0;
@@ -344,6 +344,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_solve(MGP P) {
     }
     if (!l2_norms(B, P.L[0], &rr, &bb)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // ncycl cycles without reaching eps: the reference goes on with this potential
+        // (iterative_solver.f90:56); the call reports it and phi holds the last cycle's result
+        if (!conv) set_err(P.cnt, LERR_NOTCONV, 501);
         double ktot = 0.0;
         for (int i = 1; i <= P.ng; i++) ktot = ktot + (double)iter[i - 1] / pow(2.0, 2 * (i - 1));
         P.cnt->mg_cycles = k;

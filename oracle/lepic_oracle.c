@@ -513,8 +513,33 @@ static double mg_vcycle(const o_cfg *c, mg_level *L, int ng, double omega, doubl
     return res;
 }
 
+/* ||b - A u||_2 and ||b - A u_D||_2 over the bcnd == -1 nodes (u_D: the walls' values only),
+ * the relative residual the device's mixed and L2 modes stop on */
+static void l2_norms(const o_cfg *c, const double *u, const double *b, const int32_t *bcnd, double *rr,
+                     double *dd, int nt) {
+    const int nx = c->nx, ny = c->ny;
+    const double aw = c->eps0 / (c->dx * c->dx), an = c->eps0 / (c->dy * c->dy);
+    const double ac = -(an + an + aw + aw);
+    double sr = 0.0, sd = 0.0;
+#pragma omp parallel for num_threads(nt) reduction(+ : sr, sd) schedule(static)
+    for (int iy = 1; iy <= ny + 1; iy++)
+        for (int ix = 1; ix <= nx + 1; ix++) {
+            const int64_t n = NODE(ix, iy, nx);
+            if (bcnd[n] != -1) continue;
+            const int64_t W = nx + 3;
+            const double bb = b[RHS(ix, iy, nx)];
+            const double r = bb - (aw * u[n - 1] + an * u[n + W] + an * u[n - W] + aw * u[n + 1] + ac * u[n]);
+            const double d = bb - ((bcnd[n - 1] > 0 ? aw * u[n - 1] : 0.0) + (bcnd[n + W] > 0 ? an * u[n + W] : 0.0) +
+                                   (bcnd[n - W] > 0 ? an * u[n - W] : 0.0) + (bcnd[n + 1] > 0 ? aw * u[n + 1] : 0.0));
+            sr += r * r;
+            sd += d * d;
+        }
+    *rr = sqrt(sr);
+    *dd = sqrt(sd);
+}
+
 static int solver_impl(const o_cfg *c, double *u, const double *b, const int32_t *bcnd, int ng,
-                       int ncycl, double eps, o_solve_stats *st, int nt) {
+                       int ncycl, double eps, o_solve_stats *st, int nt, int l2) {
     const int nx = c->nx, ny = c->ny;
     mg_level L[16];
     memset(L, 0, sizeof(L));
@@ -534,12 +559,20 @@ static int solver_impl(const o_cfg *c, double *u, const double *b, const int32_t
     double ktot = 0.0, res = 0.0, res_s = 0.0;
     const double omega = 1.4;
     int k = 1, rc = 0, sweeps = 0;
+    double rr = 0.0, b0 = 0.0;
+    if (l2) l2_norms(c, u, b, bcnd, &rr, &b0, nt);
     for (;;) { /* :33-66 */
         res = mg_vcycle(c, L, ng, omega, alpha * eps, k, &ktot, &sweeps, nt);
         res = res / alpha;
         if (k == 1) res_s = res;
         else if (fabs(res / res_s) > 10.0) { rc = -1; break; }
-        if (res <= eps || k == ncycl) break;
+        int conv = res <= eps;
+        if (l2) {
+            double dd;
+            l2_norms(c, u, b, bcnd, &rr, &dd, nt);
+            conv = rr <= eps * b0;
+        }
+        if (conv || k == ncycl) break;
         k = k + 1;
     }
     for (int l = 1; l < ng; l++) { free(L[l].u); free(L[l].b); free(L[l].bc); }
@@ -549,12 +582,17 @@ static int solver_impl(const o_cfg *c, double *u, const double *b, const int32_t
 
 int o_iterative_solver(const o_cfg *c, double *u, const double *b, const int32_t *bcnd, int ng,
                        int ncycl, double eps, o_solve_stats *st) {
-    return solver_impl(c, u, b, bcnd, ng, ncycl, eps, st, 1);
+    return solver_impl(c, u, b, bcnd, ng, ncycl, eps, st, 1, 0);
 }
 
 int o_iterative_solver_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
                            int ng, int ncycl, double eps, o_solve_stats *st, int nthreads) {
-    return solver_impl(c, u, b, bcnd, ng, ncycl, eps, st, nthreads < 1 ? 1 : nthreads);
+    return solver_impl(c, u, b, bcnd, ng, ncycl, eps, st, nthreads < 1 ? 1 : nthreads, 0);
+}
+
+int o_iterative_solver_l2_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
+                              int ng, int ncycl, double eps, o_solve_stats *st, int nthreads) {
+    return solver_impl(c, u, b, bcnd, ng, ncycl, eps, st, nthreads < 1 ? 1 : nthreads, 1);
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -653,10 +691,27 @@ void o_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy, doub
     }
 }
 
-/* collisions.f90:1-207 and collision_OMP :209-1040, one thread, neutral targets */
-int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
-                 int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t) {
+/* collisions.f90:339-403: the target of species tt for the incident in 1-based cell ici of the
+ * reference's row-major numbering: the incident's cell, else the first non-empty of ici+1,
+ * ici-1, ici+nx, ici-nx (the linear index, which wraps rows at the box edges) inside 1..pl_max;
+ * returns the cell (0: none) */
+static int dsmc_cell(const int32_t *plist, int ici, int nx, int pl_max) {
+    const int cand[5] = {ici, ici + 1, ici - 1, ici + nx, ici - nx};
+    for (int k = 0; k < 5; k++) {
+        const int ict = cand[k];
+        if (ict <= 0 || ict > pl_max) continue;
+        if (plist[ict] - plist[ict - 1] > 0) return ict;
+    }
+    return 0;
+}
+
+/* collisions.f90:1-207 and collision_OMP :209-1040, one thread (nproc = 1); charged targets
+ * (DSMC, :339-418, :524-528, :767-797, :908-935, :942-1000) when d gives the targets' Plist */
+int o_collisions_dsmc(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
+                      int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t, const o_dsmc *d) {
     const double pi = c->pi, qe = c->qe, dt = c->dt;
+    const int pl_max = c->nx + c->nx * c->ny + 1;
+    const int64_t nn = (int64_t)(c->nx + 3) * (c->ny + 3);
     int64_t Nc[O_MAXSP] = {0}, np_add[O_MAXSP] = {0};
     int sav_ttype[O_MAXCOL];
     for (int i = 0; i < O_MAXCOL; i++) sav_ttype[i] = -1;
@@ -697,6 +752,11 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
             double *P = vxp[p] + 6 * ip;
             double vx[2], vy[2], vz[2];
             vx[0] = P[3]; vy[0] = P[4]; vz[0] = P[5];
+            const int ixc = (int)(P[0] / c->dx) + 1, iyc = (int)(P[1] / c->dy) + 1; /* :286-292 */
+            const int ici = (ixc - 1) + c->nx * (iyc - 1) + 1;
+            int flag_err[O_MAXSP] = {0};
+            int64_t sav_it[O_MAXSP];
+            for (int q = 0; q < O_MAXSP; q++) sav_it[q] = -1;
             int flag_ttype[O_MAXSP] = {0};
             double vr[O_MAXSP] = {0}, Ekr[O_MAXSP] = {0}, mu[O_MAXSP] = {0};
             double vx_cm[O_MAXSP] = {0}, vy_cm[O_MAXSP] = {0}, vz_cm[O_MAXSP] = {0};
@@ -705,7 +765,20 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
             for (int icol = 0; icol < xs->p_ncol[p]; icol++) {
                 int ind_col = xs->sig_list[p * O_MAXCOL + icol];
                 int ttype = sav_ttype[ind_col];
+                const int charged = c->charge[ttype] != 0.0;
+                if (charged && (!d || !d->plist[ttype])) continue; /* no target list: not restated */
+                if (flag_err[ttype]) continue;                      /* :333 */
                 if (flag_ttype[ttype] == 0) {
+                    if (charged) { /* :339-418: the target particle and its velocity */
+                        const int ict = dsmc_cell(d->plist[ttype], ici, c->nx, pl_max);
+                        if (ict == 0) { flag_err[ttype] = 1; continue; }
+                        const double r = o_ran2(iseed);
+                        const int64_t it1 = (int64_t)((double)d->plist[ttype][ict] * (1.0 - r) +
+                                                      (double)d->plist[ttype][ict - 1] * r + 1.0);
+                        sav_it[ttype] = it1 - 1;
+                        const double *T = vxp[ttype] + 6 * (it1 - 1);
+                        vx[1] = T[3]; vy[1] = T[4]; vz[1] = T[5];
+                    } else {
                     double rr[2];
                     rr[0] = o_ran2(iseed); rr[1] = o_ran2(iseed);
                     o_load_gauss(&vx[1], &vy[1], c->vt0[ttype], rr);
@@ -715,6 +788,7 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
                     } else {
                         vz[1] = vz_sav;
                         vz_sav = 0.0;
+                    }
                     }
                     const double mt = fabs(c->mass[ttype]);
                     mu[ttype] = mp * mt / (mp + mt);
@@ -744,6 +818,11 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
                         double sig_L = sg[ipt - 1], sig_R = sg[ipt];
                         double sig_p = sig_L + (Ekr[ttype] - Ek_L) * (sig_R - sig_L) / (Ek_R - Ek_L);
                         double np_t = c->np_mx[ttype];
+                        if (charged) { /* :524-528, the four nodes of the incident's cell */
+                            const double *g = d->np_red + ttype * nn;
+                            np_t = 0.25 * (g[NODE(ixc, iyc, c->nx)] + g[NODE(ixc + 1, iyc, c->nx)] +
+                                           g[NODE(ixc, iyc + 1, c->nx)] + g[NODE(ixc + 1, iyc + 1, c->nx)]);
+                        }
                         nu[icol] = np_t * sig_p * vr[ttype] / nu_max_OMP;
                         sum_nu = sum_nu + nu[icol];
                         sort_arr[icol] = nu[icol];
@@ -819,6 +898,7 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
                     if (iby == 0 && bt == p) { ib = ip; opt_add = 0; flag_add[0] = 0; }
                     if (rt == 1 || rt == 3) {
                         if (bt == p) ib = ip;
+                        if (bt == ttype && bt != p) ib = sav_it[ttype]; /* :794-797 the target scatters too */
                         opt_add = 0;
                         flag_add[0] = 0; flag_add[1] = 0;
                     }
@@ -830,7 +910,7 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
                         B[0] = P[0]; B[1] = P[1]; B[2] = P[2];
                         flag_add[n_re + iby] = 1;
                     }
-                    if (ib < 0) continue; /* a charged target's slot (DSMC) is not restated */
+                    if (ib < 0) continue; /* neither the incident, its target nor a new particle */
                     double vbx = 0, vby = 0, vbz = 0;
                     if (opt_scat == 1) {
                         double cos_th = cos(th), sin_th = sin(th);
@@ -871,18 +951,23 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
                 for (int ire = 0; ire < n_re; ire++) { /* :908-935 */
                     int ct = ci[2 + ire];
                     if (c->mass[ct] <= 0) { flag_add[ire] = 0; continue; }
-                    if (flag_add[ire] == -1 && ct == p && flag_dead && flag_dead[p]) flag_dead[p][ip] = 1;
+                    if (flag_add[ire] == -1 && flag_dead && flag_dead[ct]) {
+                        if (ct == p) flag_dead[p][ip] = 1;
+                        else if (ct == ttype && sav_it[ttype] >= 0) flag_dead[ct][sav_it[ttype]] = 1;
+                    }
                 }
             } else { /* :942-1000 charge exchange */
                 for (int iby = 0; iby < n_by; iby++) {
                     int bt = ci[2 + n_re + iby];
                     if (c->mass[bt] <= 0) continue;
                     int ind_ce;
-                    if (bt == p) ind_ce = 1;
-                    else continue; /* a charged target's slot (DSMC) is not restated */
+                    double *B;
+                    if (bt == p) { ind_ce = 1; B = P; }
+                    else if (sav_it[ttype] >= 0) { ind_ce = 2; B = vxp[bt] + 6 * sav_it[ttype]; }
+                    else continue;
                     ind_ce = ind_ce + 1;
                     if (ind_ce == 3) ind_ce = 1;
-                    P[3] = vx[ind_ce - 1]; P[4] = vy[ind_ce - 1]; P[5] = vz[ind_ce - 1];
+                    B[3] = vx[ind_ce - 1]; B[4] = vy[ind_ce - 1]; B[5] = vz[ind_ce - 1];
                 }
             }
         }
@@ -892,6 +977,11 @@ int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const 
         if (t) t->n_add[p] += np_add[p];
     }
     return 0;
+}
+
+int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
+                 int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t) {
+    return o_collisions_dsmc(c, xs, vxp, np_tot, cap, flag_dead, iseed, t, NULL);
 }
 
 /* ------------------------------------------------------------------------------------ */

@@ -132,6 +132,19 @@ void o_indexx(int n, const double *arr, int *indx);
 int o_collisions(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
                  int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t);
 
+/* The same with charged targets (DSMC, collisions.f90:339-418, 524-528, 767-797, 908-935,
+ * 942-1000): plist[tt] is Plist(0:pl_max) of target species tt's array as o_part_sorting leaves
+ * it (NULL: reactions on tt are skipped, as o_collisions does), np_red the dens_red grids
+ * (ntype node grids); c->np_mx[tt] must hold dens_red's maximum for nu_max.  A target scatters
+ * in elastic and excitation events, takes the incident's velocity in charge exchange and is
+ * flagged dead when it is a reactant that is not a byproduct. */
+typedef struct {
+    const int32_t *plist[O_MAXSP];
+    const double *np_red;
+} o_dsmc;
+int o_collisions_dsmc(o_cfg *c, const o_xs *xs, double **vxp, int64_t *np_tot, const int64_t *cap,
+                      int8_t **flag_dead, int32_t *iseed, o_mcc_tally *t, const o_dsmc *d);
+
 /* SCATTER, collisions.f90:1042-1070 */
 void o_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy, double vz,
                double costheta, double phi);
@@ -144,6 +157,10 @@ void o_push_deposit_omp(const o_cfg *c, int ptype, const double *Ei, const doubl
                         int8_t *flag_dead, double *npg, int nthreads);
 int o_iterative_solver_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
                            int ng, int ncycl, double eps, o_solve_stats *st, int nthreads);
+/* The same V-cycles stopped on ||b - A u||_2 <= eps ||b - A u_D||_2 (bcnd == -1 nodes), the
+ * criterion of the device's mixed and L2 solves, for a CPU baseline of the same tolerance. */
+int o_iterative_solver_l2_omp(const o_cfg *c, double *u, const double *b, const int32_t *bcnd,
+                              int ng, int ncycl, double eps, o_solve_stats *st, int nthreads);
 
 /* ---- particle sources: e_heating.f90, part_injection.f90 ----------------------------------
  * Two forms of each routine.  The plain form restates the reference's draw order from one

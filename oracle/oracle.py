@@ -91,6 +91,10 @@ class OEmit(C.Structure):
     ]
 
 
+class ODsmc(C.Structure):
+    _fields_ = [("plist", C.POINTER(C.c_int32) * MAXSP), ("np_red", C.POINTER(C.c_double))]
+
+
 class OSolveStats(C.Structure):
     _fields_ = [("k", C.c_int), ("ktot", C.c_double), ("res", C.c_double), ("sweeps_fine", C.c_int)]
 
@@ -123,6 +127,9 @@ def lib() -> C.CDLL:
         L.o_iterative_solver_omp.restype = C.c_int
         L.o_iterative_solver_omp.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP, C.c_int, C.c_int, C.c_double,
                                              C.POINTER(OSolveStats), C.c_int]
+        L.o_iterative_solver_l2_omp.restype = C.c_int
+        L.o_iterative_solver_l2_omp.argtypes = [C.POINTER(OCfg), _DP, _DP, _IP, C.c_int, C.c_int, C.c_double,
+                                                C.POINTER(OSolveStats), C.c_int]
         L.o_sor_rb.restype = C.c_int
         L.o_sor_rb.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _DP, _DP, _IP, _DP,
                                C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
@@ -134,6 +141,10 @@ def lib() -> C.CDLL:
         L.o_collisions.restype = C.c_int
         L.o_collisions.argtypes = [C.POINTER(OCfg), C.POINTER(OXs), C.POINTER(_DP), _LP, _LP,
                                    C.POINTER(_I8), C.POINTER(C.c_int32), C.POINTER(OMccTally)]
+        L.o_collisions_dsmc.restype = C.c_int
+        L.o_collisions_dsmc.argtypes = [C.POINTER(OCfg), C.POINTER(OXs), C.POINTER(_DP), _LP, _LP,
+                                        C.POINTER(_I8), C.POINTER(C.c_int32), C.POINTER(OMccTally),
+                                        C.POINTER(ODsmc)]
         L.o_scatter.argtypes = [_DP, _DP, _DP, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.o_push_deposit_omp.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _DP, _LP, _I8, _DP,
                                          C.c_int]
@@ -347,9 +358,14 @@ def efield(cfg, phi, bcnd, Ei=None):
     return Ei
 
 
-def solve(cfg, phi, rhs, bcnd, ng, eps, ncycl=20000, nthreads=1):
+def solve(cfg, phi, rhs, bcnd, ng, eps, ncycl=20000, nthreads=1, l2=False):
+    """iterative_solver on phi in place; eps is the reference's normalised L1 tolerance, or with
+    l2 the relative L2 residual ||b - A u|| / ||b - A u_D|| the device's L2 modes stop on."""
     st = OSolveStats()
-    if nthreads > 1:
+    if l2:
+        rc = lib().o_iterative_solver_l2_omp(C.byref(cfg), dp(phi), dp(rhs), ip(bcnd), ng, ncycl, eps, C.byref(st),
+                                             max(1, nthreads))
+    elif nthreads > 1:
         rc = lib().o_iterative_solver_omp(C.byref(cfg), dp(phi), dp(rhs), ip(bcnd), ng, ncycl, eps, C.byref(st),
                                           nthreads)
     else:
@@ -387,10 +403,13 @@ def l2_residual(cfg, phi, rhs, bcnd):
     return math.sqrt(float((r[m] ** 2).sum())) / max(math.sqrt(float((d[m] ** 2).sum())), 1e-300)
 
 
-def collisions(cfg, xsh, particles, seed: int, extra: int = 4096):
+def collisions(cfg, xsh, particles, seed: int, extra: int = 4096, plists=None, np_red=None):
     """o_collisions (collisions.f90:1-207, collision_OMP, SCATTER) once on copies of the given
     per-species particle arrays, the ran2 stream seeded with `seed`.  Returns (rc, arrays after
-    the call with the products appended, the collision tally, flag_dead per species)."""
+    the call with the products appended, the collision tally, flag_dead per species).
+    With plists ({species: Plist of its array as sort() returns it}) and np_red (dens_red's
+    (ntype, ny+3, nx+3) grids; cfg.np_mx must hold their maxima) charged targets take part
+    (o_collisions_dsmc, collisions.f90:339-418)."""
     ntype = cfg.ntype
     bufs, fds = [], []
     for s in range(ntype):
@@ -405,7 +424,17 @@ def collisions(cfg, xsh, particles, seed: int, extra: int = 4096):
     fdp = (_I8 * MAXSP)(*[f.ctypes.data_as(_I8) for f in fds])
     t = OMccTally()
     sd = C.c_int32(seed)
-    rc = lib().o_collisions(C.byref(cfg), C.byref(xsh.xs), arrs, npt, cap, fdp, C.byref(sd), C.byref(t))
+    if plists is None:
+        rc = lib().o_collisions(C.byref(cfg), C.byref(xsh.xs), arrs, npt, cap, fdp, C.byref(sd), C.byref(t))
+    else:
+        keep = [np.ascontiguousarray(plists[s], dtype=np.int32) for s in sorted(plists)]
+        red = np.ascontiguousarray(np_red, dtype=np.float64)
+        d = ODsmc()
+        for s, a in zip(sorted(plists), keep):
+            d.plist[s] = ip(a)
+        d.np_red = dp(red)
+        rc = lib().o_collisions_dsmc(C.byref(cfg), C.byref(xsh.xs), arrs, npt, cap, fdp, C.byref(sd), C.byref(t),
+                                     C.byref(d))
     out = [bufs[s][:npt[s]].copy() for s in range(ntype)]
     return rc, out, t, [fds[s][:npt[s]].copy() for s in range(ntype)]
 
@@ -454,11 +483,11 @@ class OracleSimulation:
         for s in range(self.sp.ntype):
             deposit(self.cfg, s, self.vxp[s], self.np_tot[s], self.kq, self.npg[s])
 
-    def step(self, it: int, eps: float | None = None):
+    def step(self, it: int, eps: float | None = None, l2: bool = False):
         case = self.case
         eps = case.eps if eps is None else eps
         self.rhs = calc_rhs(self.cfg, self.npg)
-        rc, self.solve_stats = solve(self.cfg, self.phi, self.rhs, self.bcnd, self.ng, eps, nthreads=self.nt)
+        rc, self.solve_stats = solve(self.cfg, self.phi, self.rhs, self.bcnd, self.ng, eps, nthreads=self.nt, l2=l2)
         if rc != 0:
             raise RuntimeError("oracle Poisson solve diverged")
         efield(self.cfg, self.phi, self.bcnd, self.Ei)

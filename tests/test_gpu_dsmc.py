@@ -74,3 +74,64 @@ def test_dsmc_with_neutral_background_in_the_step(gpu_lib):
         assert st["np_tot"][1] == n0[1] - st["n_lost"][1]      # elastic: no ion created or killed
     finally:
         sim.close()
+
+
+def test_dsmc_statistics_match_the_oracle(gpu_lib):
+    """The same electrons and ions through the device's DSMC and the oracle's restatement of the
+    reference's (o_collisions_dsmc: the target drawn from the incident's cell of the sorted ion
+    array, or its neighbours; the target density the mean of dens_red at the cell's four nodes;
+    both partners scattered in the centre-of-mass frame), over K independent draws.  The device
+    adds one rule: a target claimed by two candidates of one step serves the one of the smaller
+    slot, the other has no target.  With about 0.27 candidates per cell among 100 ions that
+    removes about 0.27 / (2 * 100) = 0.13 % of the collisions, far inside the 4-sigma bound
+    on the per-draw Poisson counts compared here; the post-collision energies of both species
+    must pass a two-sample KS test at p > 0.01."""
+    from scipy.stats import ks_2samp
+    from oracle import oracle as O
+    case = dsmc_case()
+    sim = GpuSimulation(case)
+    try:
+        sp = sim.sp
+        base = [sim.get_particles(s) for s in (0, 1)]
+        cfg = O.make_cfg(case, sp)
+        xsh = O.XsHolder(sim.xs)
+        # the oracle's inputs: ions sorted in the reference's order, dens_red of the np grids
+        ions = base[1].copy()
+        plist = O.sort(cfg, ions, ions.shape[0])
+        npg = np.stack([sim.grid(capi.GRID_NP + s) for s in (0, 1)])
+        red, mx = O.dens_red(cfg, npg, case.bcnd)
+        cfg.np_mx[1] = mx[1]
+        K = 10
+        g_coll = o_coll = 0
+        gE, oE, gI, oI = [], [], [], []
+        for k in range(K):
+            sim.put_particles(0, base[0])
+            sim.put_particles(1, base[1])
+            sim.deposit()
+            sim.sort(0)
+            sim.sort(1)
+            b = [sim.get_particles(s) for s in (0, 1)]
+            m0 = sim.mcc_stats()["n_coll"][0]
+            mc = sim.collide(11 + 10 * k)
+            a = [sim.get_particles(s) for s in (0, 1)]
+            n = mc["n_coll"][0] - m0
+            g_coll += n
+            ch = [np.any(a[s][:, 3:] != b[s][:, 3:], axis=1) for s in (0, 1)]
+            assert ch[0].sum() == ch[1].sum() == n
+            gE.append(0.5 * sp.mass[0] * (a[0][ch[0], 3:] ** 2).sum(axis=1) / dk.QE)
+            gI.append(0.5 * sp.mass[1] * (a[1][ch[1], 3:] ** 2).sum(axis=1) / dk.QE)
+            rc, oa, tal, _ = O.collisions(cfg, xsh, [base[0], ions], seed=17 + 7919 * k, plists={1: plist},
+                                          np_red=red)
+            assert rc == 0
+            o_coll += tal.n_coll[0]
+            ce = np.any(oa[0][:, 3:] != base[0][:, 3:], axis=1)
+            ci = np.any(oa[1][:, 3:] != ions[:, 3:], axis=1)
+            oE.append(0.5 * sp.mass[0] * (oa[0][ce, 3:] ** 2).sum(axis=1) / dk.QE)
+            oI.append(0.5 * sp.mass[1] * (oa[1][ci, 3:] ** 2).sum(axis=1) / dk.QE)
+        assert g_coll > 1000 and o_coll > 1000
+        assert abs(g_coll - o_coll) <= 4 * math.sqrt(g_coll + o_coll), (g_coll, o_coll)
+        pe = ks_2samp(np.concatenate(gE), np.concatenate(oE)).pvalue
+        pi = ks_2samp(np.concatenate(gI), np.concatenate(oI)).pvalue
+        assert pe > 0.01 and pi > 0.01, (pe, pi)
+    finally:
+        sim.close()

@@ -221,3 +221,58 @@ def test_mcc_rate_constant_cross_section(oracle_lib):
     expect = n * nu * 10 * case.dt
     got = t.n_coll[0]
     assert abs(got - expect) < 5 * math.sqrt(expect)
+
+
+def test_oracle_dsmc_pairs_conserve_and_targets_come_from_the_cell():
+    """o_collisions_dsmc on electron-ion elastic scattering (a charged target): every collision
+    changes one electron and one ion of the electron's cell (or a neighbour), and the pair
+    keeps its momentum and kinetic energy."""
+    import math
+    from jd_lepic_b200 import configs, deck as dk
+    from jd_lepic_b200.simulation import species_params
+    from oracle import oracle as O
+    case = configs.case0(ppc=100, nx=32, ny=32)
+    case.deck_text = dk.argon_dsmc_deck()
+    d = dk.read_reactions(case.deck_text, case.ngas)
+    sp = species_params(case, d)
+    cfg = O.make_cfg(case, sp)
+    xsh = O.XsHolder(dk.ordering(d))
+    rng = np.random.default_rng(5)
+    n = case.n_particles
+    parts = []
+    for s in (0, 1):
+        p = np.zeros((n, 6))
+        p[:, 0] = rng.uniform(0, case.nx * case.dx, n)
+        p[:, 1] = rng.uniform(0, case.ny * case.dy, n)
+        p[:, 3:] = rng.normal(0, sp.vt0[s] / math.sqrt(2), (n, 3))
+        parts.append(p)
+    plist = O.sort(cfg, parts[1], n)
+    kq = O.kq_of(case.bcnd)
+    npg = np.zeros((2, case.ny + 3, case.nx + 3))
+    for s in (0, 1):
+        O.deposit(cfg, s, parts[s], n, kq, npg[s])
+    red, mx = O.dens_red(cfg, npg, case.bcnd)
+    cfg.np_mx[1] = mx[1]
+    rc, out, tal, _ = O.collisions(cfg, xsh, parts, seed=3, plists={1: plist}, np_red=red)
+    assert rc == 0
+    nc = tal.n_coll[0]
+    assert nc > 50 and tal.n_add[0] == tal.n_add[1] == 0
+    ce = np.flatnonzero(np.any(out[0][:, 3:] != parts[0][:, 3:], axis=1))
+    ci = np.flatnonzero(np.any(out[1][:, 3:] != parts[1][:, 3:], axis=1))
+    # picks with replacement can hit one particle twice: a few changed particles fewer
+    assert nc - 3 <= ce.size <= nc and nc - 3 <= ci.size <= nc
+    dP = sp.mass[0] * (out[0][:, 3:] - parts[0][:, 3:]).sum(axis=0) + \
+        sp.mass[1] * (out[1][:, 3:] - parts[1][:, 3:]).sum(axis=0)
+    pe = sp.mass[0] * np.linalg.norm(parts[0][ce, 3:], axis=1).sum()
+    assert np.abs(dP).max() <= 1e-9 * pe
+    dE = sum(0.5 * sp.mass[s] * ((out[s][:, 3:] ** 2).sum() - (parts[s][:, 3:] ** 2).sum()) for s in (0, 1))
+    Ee = 0.5 * sp.mass[0] * (parts[0][ce, 3:] ** 2).sum()
+    assert abs(dE) <= 1e-9 * Ee
+    # each changed ion sits in the cell of some changed electron or next to it
+    cell = lambda p: ((p[:, 0] / case.dx).astype(int), (p[:, 1] / case.dy).astype(int))
+    ex, ey = cell(out[0][ce])
+    ix, iy = cell(out[1][ci])
+    near = np.zeros(ci.size, dtype=bool)
+    for k in range(ci.size):
+        near[k] = np.any(np.abs(ex - ix[k]) + np.abs(ey - iy[k]) <= 1) or np.any((ey == iy[k] + 1) | (ey == iy[k] - 1))
+    assert near.all()
