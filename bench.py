@@ -571,6 +571,20 @@ def run_ours(args):
     ne1 = sum(ps.np_tot[:sim.sp.ntype])
     e2e_value = 0.5 * (ne0 + ne1) * e2e_steps * world / e2e_s
 
+    # the deposit alone (charge_deposition over the same particles, as after a load or restart):
+    # how much of the fused push+deposit the deposit is; it reads X, Y and VX (the hole test)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(5):
+        sim.check(lib.lepic_gpu_charge_deposition(ctx), "charge_deposition")
+    b.record(stream)
+    torch.cuda.synchronize()
+    dep_ms = a.elapsed_time(b) / 5
+    n_now = sum(sim.push_stats()["np_tot"])
+    deposit_only = {"ms": dep_ms, "particles": n_now, "achieved_gbs": 12.0 * n_now / (dep_ms * 1e-3) / 1e9,
+                    "algorithmic_bytes_per_particle": 12, "kernels": "k_push_deposit<MOVE=false> per species"}
     src = sources_measure(args, sim, lib, ctx, stream, it, case) if not args.no_sources else None
 
     cb = None
@@ -607,6 +621,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (particle arrays 8.4 GB/species)",
                        "sort_every": 10, "mcc_every": 10, "tile": args.tile},
             "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()},
+            "deposit_alone": deposit_only,
             "poisson_compare": pois,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,

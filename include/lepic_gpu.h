@@ -226,6 +226,9 @@ typedef struct lepic_options {
     int32_t mx_tiled;            /* 1: fine-level sweeps on shared-memory tiles (default); 0: grid-
                                     wide half-sweeps -- identical results, for checking the tiles   */
     int32_t mx_max_iter;         /* CG iterations before LEPIC_ENOTCONV (200)                        */
+    int32_t mx_coarse_direct;    /* 1: the on-chip levels' top level (at most 2048 unknowns) solved
+                                    exactly by its precomputed inverse, applied by every CTA
+                                    (default); 0: CTA 0 cycles through the on-chip levels         */
     int32_t mg_small_nodes;      /* FP64 V-cycle: levels of at most this many nodes on CTA 0 (4500)  */
     int32_t ctas_per_sm;         /* CTAs per SM of the cooperative solver kernels (3)                */
     int32_t barrier_extra;       /* test hook, 0 in use: the solvers' grid barriers wait for this

@@ -185,6 +185,7 @@ _FP = C.POINTER(C.c_float)
 class LepicOptions(C.Structure):
     _fields_ = [("mx_nu1", C.c_int32), ("mx_nu2", C.c_int32), ("mx_nuc", C.c_int32), ("mx_omega", C.c_float),
                 ("mx_onchip_bytes", C.c_int32), ("mx_tiled", C.c_int32), ("mx_max_iter", C.c_int32),
+                ("mx_coarse_direct", C.c_int32),
                 ("mg_small_nodes", C.c_int32), ("ctas_per_sm", C.c_int32), ("barrier_extra", C.c_int32),
                 ("fortran_max_subrecord", C.c_int64)]
 

@@ -53,7 +53,7 @@ static void free_all(lepic_ctx *c) {
         F(c->lev[l].e32); F(c->lev[l].e32b); F(c->lev[l].r32);
     }
     F(c->partials);
-    F(c->cg_r); F(c->cg_p); F(c->cg_ap);
+    F(c->cg_r); F(c->cg_p); F(c->cg_ap); F(c->mx_cinv); F(c->mx_cidx);
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
     F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac); F(c->sigv_mx_d); F(c->nu_max_d);
     if (c->hcnt) cudaFreeHost(c->hcnt);
@@ -291,6 +291,7 @@ static lepic_options default_options() {
     o.mx_onchip_bytes = 20 * 1024;
     o.mx_tiled = 1;
     o.mx_max_iter = 200;
+    o.mx_coarse_direct = 1;
     o.mg_small_nodes = 4500;
     o.ctas_per_sm = 3;
     o.barrier_extra = 0;
@@ -309,7 +310,8 @@ extern "C" int lepic_gpu_set_options(lepic_ctx *c, const lepic_options *in) {
     const lepic_options &o = *in;
     if (o.mx_nu1 < 1 || o.mx_nu1 > 8 || o.mx_nu2 < 1 || o.mx_nu2 > 8 || o.mx_nuc < 1 || o.mx_nuc > 64 ||
         !(o.mx_omega > 0.0f && o.mx_omega < 2.0f) || o.mx_onchip_bytes < 0 || o.mx_onchip_bytes > 96 * 1024 ||
-        (o.mx_tiled != 0 && o.mx_tiled != 1) || o.mx_max_iter < 1 || o.mg_small_nodes < 0 || o.ctas_per_sm < 1 ||
+        (o.mx_tiled != 0 && o.mx_tiled != 1) || o.mx_max_iter < 1 ||
+        (o.mx_coarse_direct != 0 && o.mx_coarse_direct != 1) || o.mg_small_nodes < 0 || o.ctas_per_sm < 1 ||
         o.ctas_per_sm > 8 || o.barrier_extra < 0 || o.barrier_extra > 1024 || o.fortran_max_subrecord < 8 ||
         o.fortran_max_subrecord > 2147483639ll) {
         c->last_err = "set_options: a value is out of range";

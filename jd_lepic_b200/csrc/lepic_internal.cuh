@@ -147,6 +147,11 @@ struct lepic_ctx {
     double *partials = nullptr;
     int mg_grid = 0, mg_grid_mixed = 0;
     double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;  // finest-level CG vectors
+    // exact solve of the mixed cycle's on-chip top level: the inverse of that level's operator
+    // (FP32, cn x cn, symmetric) and, per unknown, its node and right-hand-side indices
+    float *mx_cinv = nullptr;
+    int *mx_cidx = nullptr;         // [2 cn]: node index, then r index
+    int mx_cn = 0, mx_clev = -1;
     // warm start of the mixed solve: 1 extrapolates 2 phi_(n-1) - phi_(n-2) from the inputs of
     // the last two solves (phi_hist holds the previous input, have_hist says it is valid)
     int warm_xtrap = 0, have_hist = 0;

@@ -20,7 +20,9 @@
 // cycle (~60 B/node); the coarsest levels that fit together in about 96 KB (e, r and mask)
 // run on CTA 0 out of its shared memory.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
+#include <vector>
 #include "mg_common.cuh"
 
 struct MXL {
@@ -49,6 +51,11 @@ struct MXP {
     int tiled;       // 1: the big levels smooth in shared-memory tiles (temporal blocking)
     int tile_cap;    // nodes a tile region may hold
     int tx[LEPIC_MAXLEV], ty[LEPIC_MAXLEV];   // tile size per level
+    // exact solve of level Ls (instead of CTA 0's cycle through levels Ls..ng-1): e = M r over
+    // the level's cn unknowns, M the inverse of its operator (FP32, cn x cn)
+    const float *cinv;
+    const int *cidx;           // node index of each unknown, then its r index
+    int cn;
 };
 
 template <class Team>
@@ -487,6 +494,30 @@ __device__ void small_cycle(const MXP &P) {
     __syncthreads();
 }
 
+// level Ls solved exactly: e = M r, one row of M per warp across the whole grid (a fixed
+// summation order per row, whatever the launch); e is zero at every other node of the level
+__device__ void coarse_direct(const MXP &P) {
+    const MXL &L = P.L[P.Ls];
+    const int nn = (L.nx + 3) * (L.ny + 3);
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+    const int n = P.cn;
+    const int *ridx = P.cidx + n;
+    for (int k = gw; k < n; k += nw) {
+        const float *row = P.cinv + (size_t)k * n;
+        float a = 0.0f;
+        for (int j = lane; j < n; j += 32) a = fmaf(row[j], L.r[ridx[j]], a);
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) L.e[P.cidx[k]] = a;
+    }
+    const int W = L.nx + 3;
+    for (int t = (int)(blockIdx.x * (long long)blockDim.x + threadIdx.x); t < nn; t += (int)(gridDim.x * blockDim.x)) {
+        const int i = t % W, j = t / W;
+        if (i == 0 || j == 0 || i == L.nx + 2 || j == L.ny + 2 || L.bc[t] > 0) L.e[t] = 0.0f;
+    }
+}
+
 // one symmetric V-cycle on A e = r32 of level 0, from e = 0 (the caller zeroes e)
 __device__ bool vcycle32(const MXP &P) {
     BigTeam B{P.cnt, P.partials, P.bar_extra};
@@ -496,7 +527,8 @@ __device__ bool vcycle32(const MXP &P) {
             tiled_down(B, P, l);
             if (!B.sync()) return false;
         }
-        if (blockIdx.x == 0) small_cycle(P);
+        if (P.cn) coarse_direct(P);
+        else if (blockIdx.x == 0) small_cycle(P);
         if (!B.sync()) return false;
         for (int l = Ls - 1; l >= 0; l--) {
             tiled_up(B, P, l);
@@ -511,7 +543,8 @@ __device__ bool vcycle32(const MXP &P) {
     }
     int top;
     if (Ls <= ng - 1) {
-        if (blockIdx.x == 0) small_cycle(P);
+        if (P.cn) coarse_direct(P);
+        else if (blockIdx.x == 0) small_cycle(P);
         if (!B.sync()) return false;
         top = Ls;
     } else {
@@ -774,6 +807,88 @@ __global__ void k_warm_xtrap(double *u, double *hist, const int8_t *bc, long lon
     }
 }
 
+// The inverse of level l's operator on its unknowns (nodes with bcnd <= 0 inside the level):
+// B = -A is symmetric positive definite (the 5-point stencil with the walls' zero correction),
+// factored by a Cholesky decomposition within its band (unknowns in row order: the band is one
+// row of the level), then B^-1 column by column; M = A^-1 = -B^-1 is kept in FP32.  Computed once
+// per level on the host (at most 2048 unknowns: ~0.1 s), then reused by every solve.
+static int coarse_inverse(lepic_ctx *c, int l) {
+    if (c->mx_clev == l) return LEPIC_OK;
+    c->mx_clev = l;
+    c->mx_cn = 0;
+    const MGLevel &L = c->lev[l];
+    const int W = L.nx + 3, nn = W * (L.ny + 3);
+    std::vector<int8_t> bc((size_t)nn);
+    LCUDA(cudaMemcpy(bc.data(), L.bc, (size_t)nn, cudaMemcpyDeviceToHost));
+    std::vector<int> id((size_t)nn, -1), node, ridx;
+    for (int j = 1; j <= L.ny + 1; j++)
+        for (int i = 1; i <= L.nx + 1; i++) {
+            const int t = i + j * W;
+            if (bc[t] > 0) continue;
+            id[t] = (int)node.size();
+            node.push_back(t);
+            ridx.push_back((i - 1) + (j - 1) * (L.nx + 1));
+        }
+    const int n = (int)node.size();
+    if (n == 0 || n > 2048) return LEPIC_OK;   // the CTA-0 cycle stays
+    const double aw = c->cfg.eps0 / (L.hx * L.hx), an = c->cfg.eps0 / (L.hy * L.hy);
+    std::vector<double> Bm((size_t)n * n, 0.0), G((size_t)n * n, 0.0);
+    int bw = 0;
+    for (int k = 0; k < n; k++) {
+        const int t = node[k];
+        Bm[(size_t)k * n + k] = 2.0 * aw + 2.0 * an;
+        const int nb[4] = {t - 1, t + 1, t - W, t + W};
+        const double cf[4] = {aw, aw, an, an};
+        for (int q = 0; q < 4; q++) {
+            const int m = id[nb[q]];
+            if (m >= 0) {
+                Bm[(size_t)k * n + m] = -cf[q];
+                bw = std::max(bw, std::abs(m - k));
+            }
+        }
+    }
+    for (int j = 0; j < n; j++) {   // G lower triangular, zero below the band
+        double d = Bm[(size_t)j * n + j];
+        for (int k = std::max(0, j - bw); k < j; k++) d -= G[(size_t)j * n + k] * G[(size_t)j * n + k];
+        if (!(d > 0.0)) return LEPIC_OK;   // not positive definite: the CTA-0 cycle stays
+        const double gjj = std::sqrt(d);
+        G[(size_t)j * n + j] = gjj;
+        for (int i = j + 1; i <= std::min(n - 1, j + bw); i++) {
+            double s = Bm[(size_t)i * n + j];
+            for (int k = std::max(0, i - bw); k < j; k++) s -= G[(size_t)i * n + k] * G[(size_t)j * n + k];
+            G[(size_t)i * n + j] = s / gjj;
+        }
+    }
+    std::vector<float> M((size_t)n * n);
+    std::vector<double> y((size_t)n), xv((size_t)n);
+    for (int col = 0; col < n; col++) {
+        for (int i = 0; i < col; i++) y[i] = 0.0;
+        for (int i = col; i < n; i++) {   // G y = e_col
+            double s = i == col ? 1.0 : 0.0;
+            for (int k = std::max(col, i - bw); k < i; k++) s -= G[(size_t)i * n + k] * y[k];
+            y[i] = s / G[(size_t)i * n + i];
+        }
+        for (int i = n - 1; i >= 0; i--) {   // G^T x = y
+            double s = y[i];
+            for (int k = i + 1; k <= std::min(n - 1, i + bw); k++) s -= G[(size_t)k * n + i] * xv[k];
+            xv[i] = s / G[(size_t)i * n + i];
+        }
+        for (int i = 0; i < n; i++) M[(size_t)i * n + col] = (float)(-xv[i]);
+    }
+    if (c->mx_cinv) { cudaFree(c->mx_cinv); c->mx_cinv = nullptr; }
+    if (c->mx_cidx) { cudaFree(c->mx_cidx); c->mx_cidx = nullptr; }
+    if (cudaMalloc((void **)&c->mx_cinv, sizeof(float) * (size_t)n * n) != cudaSuccess ||
+        cudaMalloc((void **)&c->mx_cidx, sizeof(int) * 2 * (size_t)n) != cudaSuccess) {
+        c->last_err = "mixed solver: cudaMalloc of the coarse inverse failed";
+        return LEPIC_ENOMEM;
+    }
+    LCUDA(cudaMemcpy(c->mx_cinv, M.data(), sizeof(float) * (size_t)n * n, cudaMemcpyHostToDevice));
+    LCUDA(cudaMemcpy(c->mx_cidx, node.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+    LCUDA(cudaMemcpy(c->mx_cidx + n, ridx.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+    c->mx_cn = n;
+    return LEPIC_OK;
+}
+
 int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the CG operator is symmetric only with Dirichlet rows
         return mg_solve(c, eps, 2);
@@ -819,6 +934,12 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
         P.soff_b[l] = (int)off; off += ((nn + 15) / 16) * 16;
     }
     P.Ls = Ls;
+    P.cn = 0;
+    if (c->opt.mx_coarse_direct && Ls >= 1 && Ls <= c->nlev - 1) {
+        const int r = coarse_inverse(c, Ls);
+        if (r != LEPIC_OK) return r;
+        if (c->mx_cn > 0 && c->mx_clev == Ls) { P.cinv = c->mx_cinv; P.cidx = c->mx_cidx; P.cn = c->mx_cn; }
+    }
     // two over-relaxed sweeps (omega 1.15) before and after the coarse correction; the reverse
     // colour order after it keeps the cycle a symmetric preconditioner.  Measured at 2048^2
     // over 100 steps from the extrapolated start (2 iterations): 1.32 ms per solve against

@@ -423,3 +423,59 @@ def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n):
     assert tiled["cycles"] == grid["cycles"]
     assert np.array_equal(tiled["phi"], grid["phi"])
     s.close()
+
+
+def test_push_fast_particles_through_the_queues(gpu_lib):
+    """Particles that leave their cell every step (1-3 cells per step), unsorted and sorted: the
+    push's general-move and single-deposit queues fill up and fall back to working in place;
+    every particle both sides keep still matches the FP64 oracle, and the density its FP64
+    deposition."""
+    case = configs.case0(ppc=4, nx=64, ny=64)
+    s = sim_for(case, capacity=200000)
+    try:
+        rng = np.random.default_rng(11)
+        n = 120000
+        p = np.zeros((n, 6))
+        p[:, 0] = rng.uniform(0.05, 0.95, n) * case.nx * case.dx
+        p[:, 1] = rng.uniform(0.05, 0.95, n) * case.ny * case.dy
+        v = rng.uniform(1.0, 3.0, n) * case.dx / case.dt
+        th = rng.uniform(0, 2 * math.pi, n)
+        p[:, 3], p[:, 4] = v * np.cos(th), v * np.sin(th)
+        p[:, 5] = rng.normal(0, 1e5, n)
+        s.put_particles(0, p)
+        s.set_phi(smooth_phi(case))
+        E = s.efield()
+        cfg = oracle_cfg(case, s)
+        kq = O.kq_of(case.bcnd)
+        for it, sort_first in ((1, False), (2, True)):
+            if sort_first:
+                s.sort(0)
+            p0 = s.get_particles(0)
+            s.push(it)
+            got = s.get_particles(0)
+            assert assert_push_matches(case, s, cfg, 0, E, p0, got) > 0.8 * p0.shape[0]
+            npg = np.zeros((case.ny + 3, case.nx + 3))
+            O.deposit(cfg, 0, got, got.shape[0], kq, npg)
+            assert np.abs(s.grid(capi.GRID_NP + 0) - npg).max() <= 1e-12 * np.abs(npg).max()
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("direct", [0, 1])
+def test_mixed_coarse_solve_both_ways(gpu_lib, direct):
+    """The mixed cycle's on-chip levels either solved exactly through the precomputed inverse of
+    their top level (the default) or cycled by CTA 0: both preconditioners are symmetric, both
+    solves reach 1e-8 on the true FP64 residual and give the FP64 multigrid's potential."""
+    case = configs.case4(ppc=2, nx=512, ny=512)
+    s = sim_for(case)
+    try:
+        s.set_options(mx_coarse_direct=direct)
+        rhs = _perturbed_rhs(s, case)
+        set_rhs(s, rhs)
+        st = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=case.phi0.copy())
+        cfg = oracle_cfg(case, s)
+        assert O.l2_residual(cfg, st["phi"], rhs, case.bcnd) <= 1e-8
+        ref = s.solve(eps=1e-12, mode=capi.POISSON_FP64_MG_L2, phi=case.phi0.copy())["phi"]
+        assert np.abs(st["phi"] - ref).max() <= 1e-5 * np.abs(ref).max()
+    finally:
+        s.close()
