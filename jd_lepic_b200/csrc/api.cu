@@ -47,7 +47,7 @@ static void free_all(lepic_ctx *c) {
         for (int k = 0; k < 2; k++) { F(B.X[k]); F(B.Y[k]); F(B.VX[k]); F(B.VY[k]); F(B.VZ[k]); }
         F(B.acc); F(B.items); F(B.prod); F(B.cell_off); F(B.claim);
     }
-    F(c->keys); F(c->perm); F(c->skey); F(c->seglist); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
+    F(c->keys); F(c->perm); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
     for (int l = 0; l < c->nlev; l++) {
         if (l > 0) { F(c->lev[l].u); F(c->lev[l].b); F(c->lev[l].bc); }
         F(c->lev[l].e32); F(c->lev[l].e32b); F(c->lev[l].r32);
@@ -163,10 +163,9 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         LALLOC(B.prod, B.prod_cap);
     }
     c->scratch_cap = maxcap;
-    LALLOC(c->keys, maxcap); LALLOC(c->perm, maxcap); LALLOC(c->skey, maxcap);
+    LALLOC(c->keys, maxcap); LALLOC(c->perm, maxcap);
     LALLOC(c->counts, c->nkeys + 1); LALLOC(c->offsets, c->nkeys + 1); LALLOC(c->cursor, c->nkeys + 1);
     LALLOC(c->blocksums, (c->nkeys + 2047) / 2048 + 1); LALLOC(c->bigseg, c->nkeys + 1);
-    LALLOC(c->seglist, c->nkeys + 1);
     // multigrid levels (level 0 shares phi, rhs and the mask)
     c->nlev = g.ng;
     std::vector<int8_t> prev = bc8;

@@ -49,7 +49,6 @@ struct DevCounters {
     int n_items[LEPIC_MAXSP];
     unsigned int prod_count[LEPIC_MAXSP]; // products waiting for the ordered append
     int n_big;                            // sort: segments too long for one warp
-    int n_seg;                            // sort: segments the scatter left out of order
     unsigned int n_cand_list;             // collisions: candidates of the species being treated
     int err;
     int err_where;
@@ -140,8 +139,6 @@ struct lepic_ctx {
     SpeciesBuf sp[LEPIC_MAXSP];
     // sort scratch
     int *keys = nullptr, *perm = nullptr, *counts = nullptr, *offsets = nullptr;
-    int *skey = nullptr;          // the key of each output position (written by the scatter)
-    int *seglist = nullptr;       // keys whose segment the scatter left out of order
     int *cursor = nullptr, *blocksums = nullptr, *bigseg = nullptr;
     long long scratch_cap = 0;
     // multigrid

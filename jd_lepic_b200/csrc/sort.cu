@@ -5,10 +5,9 @@
 //   1. keys + histogram        (warp-aggregated atomics on the per-key counts)
 //   2. exclusive scan           (three-phase, fixed order)
 //   3. scatter of slot indices  (atomics; each warp takes a contiguous chunk in slot order, so
-//                               a key comes out of order only where it straddles chunks), with
-//                               the key of each output position
-//   4. one pass over the output finds the segments left out of order (a slot index above its
-//      successor's within one key); only those are sorted (bitonic, ascending) -> stable again
+//                               a key comes out of order only where it straddles chunks)
+//   4. per-key segment sort of the slot indices (bitonic, ascending; segments already in
+//      order are skipped) -> stable again
 //   5. gather of the 5 SoA fields into the other buffer, holes dropped
 //   6. push work list: per tile, chunks of CHUNK particles
 // so the result is bit-identical to the reference's, independent of thread timing.
@@ -151,7 +150,7 @@ __global__ void k_scan_final(const int *counts, long long n, const int *blocksum
 // the slots of a key reach their segment in ascending order; only a key whose slots straddle
 // chunks can come out of order (the segment sort below checks every segment and sorts those).
 #define SCATTER_CHUNK 1024
-__global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *cursor, int *perm, int *skey) {
+__global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *cursor, int *perm) {
     const long long n = cnt->n_slots[sp];
     const unsigned lane = threadIdx.x & 31;
     const long long nchunks = (n + SCATTER_CHUNK - 1) / SCATTER_CHUNK;
@@ -178,11 +177,7 @@ __global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int b = __shfl_sync(m[u], base[u], __ffs(m[u]) - 1);
-                if (key[u] >= 0) {
-                    const int pos = b + __popc(m[u] & ((1u << lane) - 1u));
-                    perm[pos] = (int)(i0 + 32 * u + lane);
-                    skey[pos] = key[u];
-                }
+                if (key[u] >= 0) perm[b + __popc(m[u] & ((1u << lane) - 1u))] = (int)(i0 + 32 * u + lane);
             }
         }
     }
@@ -212,29 +207,13 @@ __device__ __forceinline__ void warp_sort64(int &v0, int &v1, int lane) {
     }
 }
 
-// the segments the scatter left out of order: position j and j + 1 hold one key and slot
-// indices in descending order.  Each such key is listed once (its histogram count, no longer
-// needed after the scan, becomes the "listed" mark).
-__global__ void k_segcheck(const int *perm, const int *skey, const int *offsets, long long nkeys, int *mark,
-                           int *seglist, DevCounters *cnt) {
-    const long long n = offsets[nkeys];
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j + 1 < n;
-         j += (long long)gridDim.x * blockDim.x) {
-        const int k = skey[j];
-        if (k == skey[j + 1] && perm[j] > perm[j + 1] && atomicExch(&mark[k], -1) != -1)
-            seglist[atomicAdd(&cnt->n_seg, 1)] = k;
-    }
-}
-
-__global__ void k_segsort_warp(const int *offsets, const int *seglist, int *perm, int *bigseg,
+__global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, int *bigseg,
                                DevCounters *cnt) {
     __shared__ int buf[SORT_THREADS / 32][SEG_WARP_MAX];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long nseg = cnt->n_seg;
-    for (long long q = gw; q < nseg; q += nw) {
-        const long long k = seglist[q];
+    for (long long k = gw; k < nkeys; k += nw) {
         int s0 = offsets[k], s1 = offsets[k + 1], n = s1 - s0;
         if (n <= 1) continue;
         if (n <= 64) {   // the common case: in registers, no shared memory
@@ -378,7 +357,7 @@ int sort_species(lepic_ctx *c, int sp) {
     const long long nk = c->nkeys;
     int grid = c->num_sms * 8;
     LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
-    LCUDA(cudaMemsetAsync(&c->dcnt->n_big, 0, 2 * sizeof(int), c->stream));   // n_big, n_seg
+    LCUDA(cudaMemsetAsync(&c->dcnt->n_big, 0, sizeof(int), c->stream));
     k_keys_hist<<<grid, SORT_THREADS, 0, c->stream>>>(K, B.X[cur], B.Y[cur], B.VX[cur], B.VY[cur], B.VZ[cur],
                                                         c->bcnd, c->tally, c->dcnt, sp, c->keys, c->counts);
     int nb = div_up(nk, SCAN_ITEMS);
@@ -386,10 +365,8 @@ int sort_species(lepic_ctx *c, int sp) {
     k_scan_top<<<1, 1024, 0, c->stream>>>(c->blocksums, nb);
     k_scan_final<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums, c->offsets);
     LCUDA(cudaMemcpyAsync(c->cursor, c->offsets, sizeof(int) * nk, cudaMemcpyDeviceToDevice, c->stream));
-    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, c->dcnt, sp, c->cursor, c->perm, c->skey);
-    k_segcheck<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->skey, c->offsets, nk, c->counts, c->seglist,
-                                                     c->dcnt);
-    k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, c->seglist, c->perm, c->bigseg, c->dcnt);
+    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, c->dcnt, sp, c->cursor, c->perm);
+    k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, nk, c->perm, c->bigseg, c->dcnt);
     k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, c->perm, c->bigseg, c->dcnt);
     k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
                                                    B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt], B.VX[nxt],
