@@ -462,6 +462,13 @@ int lepic_gpu_write_backup(lepic_ctx *ctx, const char *path, double time, int32_
  * deposits every species into np (restart_OMP).  time, gtype, Pabs_cor (nullable) receive the
  * header.  LEPIC_ECAPACITY if the particles do not fit (restart.f90:117-121). */
 int lepic_gpu_read_backup(lepic_ctx *ctx, const char *path, double *time, int32_t *gtype, double *Pabs_cor);
+/* The restart's particle duplication (restart.f90:115-129): with |np_dup| > 1 every species'
+ * particles are followed by |np_dup| - 1 copies of themselves, then deposited into np
+ * (restart_OMP).  LEPIC_ECAPACITY if |np_dup| times the occupied slots exceeds the capacity
+ * (restart.f90:117-121).  The reference's external restart (flag_restart = 2, SAV_DATA) reads
+ * several files into one rank: call lepic_gpu_read_backup once per file (each appends), then
+ * this. */
+int lepic_gpu_duplicate_particles(lepic_ctx *ctx, int32_t np_dup);
 
 /* ---- learned warm start of the Poisson solve (no counterpart in the reference) ----------
  * Mode LEPIC_POISSON_LEARNED of lepic_gpu_iterative_solver: a 4-level convolutional network

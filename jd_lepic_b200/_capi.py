@@ -232,6 +232,7 @@ PROTOTYPES = {
     "lepic_gpu_source_tallies": (C.c_int, [_VP, C.POINTER(LepicSourceTally), C.c_int32]),
     "lepic_gpu_write_backup": (C.c_int, [_VP, C.c_char_p, C.c_double, C.c_int32, C.c_double]),
     "lepic_gpu_read_backup": (C.c_int, [_VP, C.c_char_p, _DP, C.POINTER(C.c_int32), _DP]),
+    "lepic_gpu_duplicate_particles": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_set_avg": (C.c_int, [_VP, C.c_int32, C.c_int32]),
     "lepic_gpu_set_regions": (C.c_int, [_VP, C.c_int32, _DP, _DP, C.c_double, C.c_double]),
     "lepic_gpu_get_tallies": (C.c_int, [_VP, C.POINTER(LepicTallies), C.c_int32]),

@@ -386,3 +386,49 @@ extern "C" int lepic_gpu_read_backup(lepic_ctx *c, const char *path, double *tim
     if (r != LEPIC_OK) return r;
     return lepic_gpu_charge_deposition(c);  // restart_OMP: np of the loaded particles
 }
+
+// ---------------------------------------------------------------------------------------
+// restart.f90:115-129: |np_dup| - 1 copies of every slot appended after the occupied slots
+// (copy i of slot k at i * n + k).  A copied hole stays a plain hole (a loss record is tallied
+// once, from the original).
+__global__ void k_duplicate(long long n, int copies, uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ) {
+    const long long tot = n * (long long)copies;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long k = t % n, d = n + t;
+        const float vx = VX[k];
+        X[d] = X[k]; Y[d] = Y[k];
+        VX[d] = isnan(vx) ? __int_as_float(HOLE_NAN) : vx;
+        VY[d] = VY[k]; VZ[d] = VZ[k];
+    }
+}
+
+extern "C" int lepic_gpu_duplicate_particles(lepic_ctx *c, int32_t np_dup) {
+    if (!c) return LEPIC_EINVAL;
+    const int dup = np_dup < 0 ? -np_dup : np_dup;
+    if (dup <= 1) return LEPIC_OK;
+    int r = lepic_gpu_sync(c);
+    if (r != LEPIC_OK) return r;
+    const lepic_config &g = c->cfg;
+    for (int s = 0; s < g.ntype; s++)   // restart.f90:117-121
+        if ((long long)dup * c->hcnt->n_slots[s] > c->sp[s].cap) {
+            c->last_err = "|np_dup| * np_tot exceeds the particle capacity (restart.f90:117-121)";
+            return LEPIC_ECAPACITY;
+        }
+    for (int s = 0; s < g.ntype; s++) {
+        SpeciesBuf &B = c->sp[s];
+        const long long n = c->hcnt->n_slots[s];
+        if (n > 0) {
+            const long long tot = n * (dup - 1);
+            k_duplicate<<<(unsigned)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16), 256, 0,
+                          c->stream>>>(n, dup - 1, B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur]);
+            LCUDA(cudaGetLastError());
+        }
+        const long long slots = n * dup, alive = c->hcnt->n_alive[s] * dup;
+        LCUDA(cudaMemcpyAsync(&c->dcnt->n_slots[s], &slots, sizeof(slots), cudaMemcpyHostToDevice, c->stream));
+        LCUDA(cudaMemcpyAsync(&c->dcnt->n_alive[s], &alive, sizeof(alive), cudaMemcpyHostToDevice, c->stream));
+        LCUDA(cudaStreamSynchronize(c->stream));   // the host values above are locals
+    }
+    r = lepic_gpu_sync(c);
+    if (r != LEPIC_OK) return r;
+    return lepic_gpu_charge_deposition(c);  // restart_OMP: np of every particle
+}

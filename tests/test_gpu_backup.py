@@ -142,3 +142,43 @@ def test_truncated_backup_is_rejected(gpu_lib, tmp_path):
     finally:
         a.close()
         b.close()
+
+
+def test_external_restart_from_two_files_then_duplication(gpu_lib, tmp_path):
+    """The reference's external restart (restart.f90:66-108): one rank reads several backup
+    files, appending each; then np_dup (:115-129) follows every species' particles with
+    |np_dup| - 1 copies of themselves, and the density is deposited from all of them."""
+    from oracle import oracle as O
+    case = configs.case0(ppc=2, nx=32, ny=32)
+    a = GpuSimulation(case)
+    b = GpuSimulation(case, load=False, capacity=6 * case.n_particles)
+    try:
+        p1 = str(tmp_path / "particles000.bak")
+        p2 = str(tmp_path / "particles001.bak")
+        a.write_backup(p1)
+        a.push(1)
+        a.deposit()
+        a.write_backup(p2)
+        live = [np.concatenate([FR.read_backup(p, 2)[4][s][0] for p in (p1, p2)]) for s in (0, 1)]
+        b.read_backup(p1)
+        b.read_backup(p2)
+        for s in (0, 1):
+            assert np.array_equal(b.get_particles(s), live[s])
+        with pytest.raises(capi.LepicError) as e:
+            b.check(b.lib.lepic_gpu_duplicate_particles(b.ctx, 7), "duplicate")
+        assert e.value.code == capi.ECAPACITY
+        b.check(b.lib.lepic_gpu_duplicate_particles(b.ctx, -3), "duplicate")
+        cfg = O.make_cfg(case, b.sp)
+        kq = O.kq_of(case.bcnd)
+        for s in (0, 1):
+            got = b.get_particles(s)
+            assert np.array_equal(got, np.concatenate([live[s]] * 3))
+            assert b.push_stats()["np_tot"][s] == 3 * len(live[s])
+            npg = np.zeros((case.ny + 3, case.nx + 3))
+            O.deposit(cfg, s, got, got.shape[0], kq, npg)
+            assert np.abs(b.grid(capi.GRID_NP + s) - npg).max() <= 1e-12 * np.abs(npg).max()
+        b.step(1)                                   # the context runs on
+        b.sync()
+    finally:
+        a.close()
+        b.close()
