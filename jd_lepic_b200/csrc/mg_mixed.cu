@@ -202,8 +202,8 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
 // One grid barrier per level and direction instead of one per half-sweep.  Tiles read their
 // halo from one buffer and write their result to the other (e -> e2 down, e2 -> e up), so a
 // tile never sees a neighbour's finished values.
-#define MX_TX 64     // the largest tile; coarser levels use 32 x 16 or 16 x 8 (host choice)
-#define MX_TY 32
+#define MX_TX 64     // the largest tile (the host chooses each level's tile, up to 64 x 64)
+#define MX_TY 64
 
 struct Region {
     int i0, j0, i1, j1;      // tile interior [i0, i1) x [j0, j1) (updatable nodes)
@@ -953,24 +953,34 @@ int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap) {
     // tiles: region (TX + 2H) x (TY + 2H) with H = 2 nu + 2 (down) or 2 nu (up); e, r (FP32)
     // and the mask per node, sharing the dynamic shared memory with the small cycle
     const int Hmax = 2 * std::max(P.nu1 + 1, P.nu2);
-    P.tile_cap = (MX_TX + 2 * Hmax) * (MX_TY + 2 * Hmax);
+    auto region_bytes = [&](int tx, int ty) {
+        const long long cap = (long long)(tx + 2 * Hmax) * (ty + 2 * Hmax);
+        const long long cc = (long long)((tx + 2 * Hmax) / 2 + 3) * ((ty + 2 * Hmax) / 2 + 3);
+        return cap * 9 + cc * 4 + 16;
+    };
+    const int cap_tx = MX_TX, cap_ty = region_bytes(MX_TX, MX_TY) <= 64 * 1024 ? MX_TY : MX_TY / 2;
+    P.tile_cap = (cap_tx + 2 * Hmax) * (cap_ty + 2 * Hmax);
     {
-        // per level the largest tile that still gives every CTA of the grid a tile: on the
-        // coarse levels a small tile is a short dependency chain for the CTA that holds it
-        const int grid_est = c->mg_grid_mixed > 0 ? c->mg_grid_mixed : c->num_sms * 3;
+        // per level the tile that ends the pass soonest: the tiles go round the grid's CTAs, so
+        // a pass lasts (rounds) x (one tile's region, halo included, plus a fixed latency per
+        // tile: a tile is a chain of dependent loads and block barriers); 561 tiles on 444
+        // CTAs, for instance, take two rounds where 442 slightly larger ones take one
+        const int grid_est = c->mg_grid_mixed > 0 ? c->mg_grid_mixed : c->num_sms * c->opt.ctas_per_sm;
         for (int l = 0; l < c->nlev; l++) {
-            int tx = MX_TX, ty = MX_TY;
-            while (tx > 16) {
-                const long long nt = (long long)((c->lev[l].nx + 1 + tx - 1) / tx) * ((c->lev[l].ny + 1 + ty - 1) / ty);
-                if (nt >= grid_est) break;
-                tx /= 2;
-                ty /= 2;
-            }
-            P.tx[l] = tx;
-            P.ty[l] = ty;
+            long long best = -1;
+            int btx = 16, bty = 8;
+            for (int tx = 16; tx <= cap_tx; tx += 16)
+                for (int ty = 8; ty <= cap_ty; ty += 4) {
+                    const long long nt = (long long)((c->lev[l].nx + 1 + tx - 1) / tx) * ((c->lev[l].ny + 1 + ty - 1) / ty);
+                    const long long rounds = (nt + grid_est - 1) / grid_est;
+                    const long long cost = rounds * ((long long)(tx + 2 * Hmax) * (ty + 2 * Hmax) + 1000);
+                    if (best < 0 || cost < best) { best = cost; btx = tx; bty = ty; }
+                }
+            P.tx[l] = btx;
+            P.ty[l] = bty;
         }
     }
-    const long long coarse_cap = (long long)((MX_TX + 2 * Hmax) / 2 + 3) * ((MX_TY + 2 * Hmax) / 2 + 3);
+    const long long coarse_cap = (long long)((cap_tx + 2 * Hmax) / 2 + 3) * ((cap_ty + 2 * Hmax) / 2 + 3);
     const long long tile_bytes = (long long)P.tile_cap * 9 + coarse_cap * 4 + 16;
     P.tiled = (Ls <= c->nlev - 1 && Ls >= 1 && c->opt.mx_tiled && tile_bytes <= 64 * 1024) ? 1 : 0;
     P.smem_bytes = (int)std::max(off, P.tiled ? tile_bytes : 0ll);
