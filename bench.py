@@ -515,11 +515,13 @@ def run_ours(args):
     # then both solvers from the previous phi as it is (set_phi forgets the history); a mixed
     # solve first, untimed, when the time loop used another mode: a context's first mixed solve
     # also factors the coarse level's operator (once, on the host)
-    if mode != capi.POISSON_MIXED_IR:
-        sim.set_phi(phi_save)
-        sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, capi.POISSON_MIXED_IR, None), "solver")
+    for m in (capi.POISSON_MIXED_IR, capi.POISSON_FP64_PCG):
+        if m != mode:
+            sim.set_phi(phi_save)
+            sim.check(lib.lepic_gpu_iterative_solver(ctx, None, eps, m, None), "solver")
     for start, phi0 in (("warm", phi_save), ("cold", phi_cold)):
-        for name, m in (("fp64_mg", capi.POISSON_FP64_MG_L2), ("mixed_pcg", capi.POISSON_MIXED_IR)):
+        for name, m in (("fp64_mg", capi.POISSON_FP64_MG_L2), ("mixed_pcg", capi.POISSON_MIXED_IR),
+                        ("fp64_pcg", capi.POISSON_FP64_PCG)):
             sim.set_phi(phi0)
             st = capi.LepicSolveStats()
             a = torch.cuda.Event(enable_timing=True)
@@ -533,6 +535,8 @@ def run_ours(args):
     sim.set_phi(phi_save)
     for start in ("warm", "cold"):
         pois[f"speedup_{start}"] = pois[f"fp64_mg_{start}"]["ms"] / pois[f"mixed_pcg_{start}"]["ms"]
+        # the same CG with an FP64 cycle: what the FP32 cycle alone gains
+        pois[f"speedup_precision_{start}"] = pois[f"fp64_pcg_{start}"]["ms"] / pois[f"mixed_pcg_{start}"]["ms"]
     if "mixed_pcg_extrapolated" in pois:
         pois["speedup_warm_extrapolated"] = pois["fp64_mg_warm"]["ms"] / pois["mixed_pcg_extrapolated"]["ms"]
 

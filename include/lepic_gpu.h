@@ -49,6 +49,8 @@ extern "C" {
 #define LEPIC_POISSON_MIXED_IR 1  /* FP64 CG preconditioned by an FP32 V-cycle            */
 #define LEPIC_POISSON_FP64_MG_L2 2 /* mode 0's V-cycles, stopped on the L2 relative residual */
 #define LEPIC_POISSON_LEARNED 3   /* mode 1 started from the learned network's prediction   */
+#define LEPIC_POISSON_FP64_PCG 4  /* mode 1 with its V-cycle in FP64: the same algorithm, so that
+                                     modes 4 and 1 compare the precision alone                  */
 
 /* Grid selectors for lepic_gpu_get_grid / lepic_gpu_set_grid */
 #define LEPIC_GRID_PHI 0      /* phi(0:nx+2,0:ny+2)                     */

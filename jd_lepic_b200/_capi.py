@@ -34,6 +34,7 @@ POISSON_FP64_MG = 0
 POISSON_MIXED_IR = 1
 POISSON_FP64_MG_L2 = 2
 POISSON_LEARNED = 3
+POISSON_FP64_PCG = 4
 
 GRID_PHI = 0
 GRID_RHS = 1

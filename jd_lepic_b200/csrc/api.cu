@@ -51,9 +51,10 @@ static void free_all(lepic_ctx *c) {
     for (int l = 0; l < c->nlev; l++) {
         if (l > 0) { F(c->lev[l].u); F(c->lev[l].b); F(c->lev[l].bc); }
         F(c->lev[l].e32); F(c->lev[l].e32b); F(c->lev[l].r32);
+        F(c->lev[l].e64); F(c->lev[l].e64b); F(c->lev[l].r64);
     }
     F(c->partials);
-    F(c->cg_r); F(c->cg_p); F(c->cg_ap); F(c->mx_cinv); F(c->mx_cidx);
+    F(c->cg_r); F(c->cg_p); F(c->cg_ap); F(c->mx_cinv); F(c->mx_cinv64); F(c->mx_cidx);
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
     F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac); F(c->sigv_mx_d); F(c->nu_max_d);
     if (c->hcnt) cudaFreeHost(c->hcnt);
@@ -323,6 +324,7 @@ extern "C" int lepic_gpu_set_options(lepic_ctx *c, const lepic_options *in) {
     c->opt = o;
     if (relaunch) {
         c->mg_grid_mixed = 0;  // sized again at the next mixed solve
+        c->mg_grid_mixed64 = 0;
         int r = mg_init(c);
         if (r != LEPIC_OK) return r;
     }
@@ -638,6 +640,7 @@ extern "C" int lepic_gpu_dens_red(lepic_ctx *c, double *np_red_out, double *np_m
 
 static int solve(lepic_ctx *c, double eps, int mode) {
     if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps, true);
+    if (mode == LEPIC_POISSON_FP64_PCG) return mg_mixed_solve(c, eps, true, true);
     c->have_hist = 0;   // any other solver: the next mixed solve starts from its answer as it is
     if (mode == LEPIC_POISSON_FP64_MG) return mg_solve(c, eps, 0);
     if (mode == 2) return mg_solve(c, eps, 2);

@@ -98,6 +98,8 @@ struct MGLevel {
     float *e32;      // mixed precision correction (nx+3)(ny+3)
     float *e32b;     // the pre-smoothed correction of the tiled V-cycle (ping-pong partner)
     float *r32;      // mixed precision right-hand side (nx+1)(ny+1)
+    double *e64, *e64b, *r64;  // the same three in FP64 for the FP64-cycle comparison (mode 4),
+                               // allocated at its first use
 };
 
 struct SpeciesBuf {
@@ -145,11 +147,12 @@ struct lepic_ctx {
     MGLevel lev[LEPIC_MAXLEV];
     int nlev = 0;
     double *partials = nullptr;
-    int mg_grid = 0, mg_grid_mixed = 0;
+    int mg_grid = 0, mg_grid_mixed = 0, mg_grid_mixed64 = 0;
     double *cg_r = nullptr, *cg_p = nullptr, *cg_ap = nullptr;  // finest-level CG vectors
     // exact solve of the mixed cycle's on-chip top level: the inverse of that level's operator
     // (FP32, cn x cn, symmetric) and, per unknown, its node and right-hand-side indices
     float *mx_cinv = nullptr;
+    double *mx_cinv64 = nullptr;    // the same inverse in FP64 (mode 4's cycle)
     int *mx_cidx = nullptr;         // [2 cn]: node index, then r index
     int mx_cn = 0, mx_clev = -1;
     // warm start of the mixed solve: 1 extrapolates 2 phi_(n-1) - phi_(n-2) from the inputs of
@@ -330,7 +333,8 @@ int field_np_grid(lepic_ctx *c, int ptype, double *d_out);
 int mg_solve(lepic_ctx *c, double eps, int mode);
 int mg_init(lepic_ctx *c);
 int mg_residual_stats(lepic_ctx *c);
-int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap);   // xtrap: the warm start may extrapolate
+// xtrap: the warm start may extrapolate; fp64: the V-cycle in FP64 (mode 4) instead of FP32
+int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap, bool fp64 = false);
 int push_deposit(lepic_ctx *c, int it, bool move);
 int sort_species(lepic_ctx *c, int ptype);
 int particles_load(lepic_ctx *c, const lepic_load_spec *spec);

@@ -233,14 +233,15 @@ def test_mg_fp64_matches_oracle(gpu_lib, n, eps):
     s.close()
 
 
+@pytest.mark.parametrize("mode", [capi.POISSON_MIXED_IR, capi.POISSON_FP64_PCG])
 @pytest.mark.parametrize("idx,n", [(2, 64), (2, 256), (4, 256), (4, 512)])
-def test_mg_mixed_precision_reaches_1e8(gpu_lib, idx, n):
+def test_mg_mixed_precision_reaches_1e8(gpu_lib, idx, n, mode):
     case = configs.case2(ppc=2, nx=n, ny=n // 2) if idx == 2 else configs.case4(ppc=2, nx=n, ny=n)
     s = sim_for(case)
     rhs = _perturbed_rhs(s, case)
     set_rhs(s, rhs)
     phi0 = case.phi0.copy()
-    st = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=phi0)
+    st = s.solve(eps=1e-8, mode=mode, phi=phi0)
     cfg = oracle_cfg(case, s)
     res = O.l2_residual(cfg, st["phi"], rhs, case.bcnd)
     assert res <= 1e-8, res
@@ -407,8 +408,9 @@ def test_config_shapes_run(gpu_lib, idx):
     s.close()
 
 
+@pytest.mark.parametrize("mode", [capi.POISSON_MIXED_IR, capi.POISSON_FP64_PCG])
 @pytest.mark.parametrize("idx,n", [(4, 512), (2, 256), (4, 2048)])
-def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n):
+def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n, mode):
     """The shared-memory tiles of the mixed solver's V-cycle (all half-sweeps of a stage on a
     tile plus halo, then the restriction / after the prolongation) give exactly the values of
     the grid-wide half-sweeps: same iterations, bit-identical potential.  At 2048^2 every CTA
@@ -417,9 +419,9 @@ def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n):
     s = sim_for(case)
     rhs = _perturbed_rhs(s, case)
     set_rhs(s, rhs)
-    tiled = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=case.phi0.copy())
+    tiled = s.solve(eps=1e-8, mode=mode, phi=case.phi0.copy())
     s.set_options(mx_tiled=0)
-    grid = s.solve(eps=1e-8, mode=capi.POISSON_MIXED_IR, phi=case.phi0.copy())
+    grid = s.solve(eps=1e-8, mode=mode, phi=case.phi0.copy())
     assert tiled["cycles"] == grid["cycles"]
     assert np.array_equal(tiled["phi"], grid["phi"])
     s.close()
