@@ -451,6 +451,28 @@ int lepic_gpu_set_regions(lepic_ctx *ctx, int32_t n_rg, const double *xl_rg, con
  * afterwards (main.f90:1296-1300). */
 int lepic_gpu_get_tallies(lepic_ctx *ctx, lepic_tallies *out, int32_t reset);
 
+/* ---- the 3rd virtual dimension of the 2.5D model (hz >= 0) ------------------------------
+ * read_input.f90:158-162 and part_expmover.f90:216-219, 269-309, 400-421: each particle keeps
+ * z in [0, zmax] (zmax = lepic_config.zmax, the deck's length in the 3rd dimension); electrons
+ * and negative ions reaching z <= 0 or z >= zmax are lost through the end plates when
+ * 0.5 m vz^2 / qe >= phi(ix,iy) - phi0, else reflected (vz -> -vz, z -> 0.02 or 0.98 zmax);
+ * positive ions are lost with probability hz 2 uB / zmax * dt per step, uB the Bohm speed on the
+ * averaging grid (main.f90:950-960: sqrt(qe Te / m) from the averaged electron temperature,
+ * formed after each averaging sample of the device, or set by the host).  Such a loss has no
+ * wall label (p_mac's igrid 0) and adds Nm q phi at the loss point to P_loss(1).  The
+ * particles already loaded get z = rnd zmax; loads, injections and emissions draw z as the
+ * reference does, collision products take their parent's z, and put/get, backups and sorts
+ * carry it. */
+typedef struct lepic_zloss_config {
+    double hz;           /* h = ns/<n> of the deck; < 0: no 3rd-dimension losses (the default) */
+    double phi0;         /* end-plate potential [V] (read_input.f90:158)                      */
+    int32_t size_na;     /* the uB grid: na = n / size_na (read_input.f90:109-111)            */
+} lepic_zloss_config;
+int lepic_gpu_set_zloss(lepic_ctx *ctx, const lepic_zloss_config *cfg);
+/* uB(na1+1, na2+1, ntype) [m/s] in Fortran order (main.f90:197), from the host (e.g. after an
+ * MPI reduction of the averages); the device's averaging samples overwrite it. */
+int lepic_gpu_set_bohm_speed(lepic_ctx *ctx, const double *uB);
+
 /* ---- particle backup (main.f90:1102-1139, restart.f90:48-149) ---------------------------
  * The reference's particlesNNN.bak: Fortran unformatted sequential records (4-byte length
  * markers; records over 2^31-9 bytes split into subrecords as the Intel and GNU runtimes do):

@@ -183,6 +183,10 @@ class LepicTallies(C.Structure):
 _FP = C.POINTER(C.c_float)
 
 
+class LepicZlossConfig(C.Structure):
+    _fields_ = [("hz", C.c_double), ("phi0", C.c_double), ("size_na", C.c_int32)]
+
+
 class LepicOptions(C.Structure):
     _fields_ = [("mx_nu1", C.c_int32), ("mx_nu2", C.c_int32), ("mx_nuc", C.c_int32), ("mx_omega", C.c_float),
                 ("mx_onchip_bytes", C.c_int32), ("mx_tiled", C.c_int32), ("mx_max_iter", C.c_int32),
@@ -234,6 +238,8 @@ PROTOTYPES = {
     "lepic_gpu_write_backup": (C.c_int, [_VP, C.c_char_p, C.c_double, C.c_int32, C.c_double]),
     "lepic_gpu_read_backup": (C.c_int, [_VP, C.c_char_p, _DP, C.POINTER(C.c_int32), _DP]),
     "lepic_gpu_duplicate_particles": (C.c_int, [_VP, C.c_int32]),
+    "lepic_gpu_set_zloss": (C.c_int, [_VP, C.POINTER(LepicZlossConfig)]),
+    "lepic_gpu_set_bohm_speed": (C.c_int, [_VP, _DP]),
     "lepic_gpu_set_avg": (C.c_int, [_VP, C.c_int32, C.c_int32]),
     "lepic_gpu_set_regions": (C.c_int, [_VP, C.c_int32, _DP, _DP, C.c_double, C.c_double]),
     "lepic_gpu_get_tallies": (C.c_int, [_VP, C.POINTER(LepicTallies), C.c_int32]),

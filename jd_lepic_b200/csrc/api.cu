@@ -40,11 +40,11 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
     F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed); F(c->Ef);
-    F(c->ss_diag); F(c->phi_hist);
+    F(c->ss_diag); F(c->phi_hist); F(c->uB);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
-        for (int k = 0; k < 2; k++) { F(B.X[k]); F(B.Y[k]); F(B.VX[k]); F(B.VY[k]); F(B.VZ[k]); }
+        for (int k = 0; k < 2; k++) { F(B.X[k]); F(B.Y[k]); F(B.VX[k]); F(B.VY[k]); F(B.VZ[k]); F(B.Z[k]); }
         F(B.acc); F(B.items); F(B.prod); F(B.cell_off); F(B.claim);
     }
     F(c->keys); F(c->perm); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
@@ -398,15 +398,17 @@ int particles_put(lepic_ctx *c, int sp, const double *vxp, long long n) {
     const double sx = (double)(1u << c->S) / g.dx, sy = (double)(1u << c->S) / g.dy;
     const long long xl = (long long)g.nx << c->S, yl = (long long)g.ny << c->S;
     std::vector<uint32_t> X(n), Y(n);
-    std::vector<float> VX(n), VY(n), VZ(n);
+    std::vector<float> VX(n), VY(n), VZ(n), Z(B.Z[0] ? n : 0);
     for (long long k = 0; k < n; k++) {
         const double *p = vxp + 6 * k;
         long long xi = llround(p[0] * sx), yi = llround(p[1] * sy);
         if (xi < 0 || xi >= xl || yi < 0 || yi >= yl) { c->last_err = "particle outside the box"; return LEPIC_EINVAL; }
         X[k] = (uint32_t)xi; Y[k] = (uint32_t)yi;
         VX[k] = (float)p[3]; VY[k] = (float)p[4]; VZ[k] = (float)p[5];
+        if (B.Z[0]) Z[k] = (float)p[2];
     }
     const int cur = B.cur;
+    if (n > 0 && B.Z[0]) LCUDA(cudaMemcpyAsync(B.Z[cur], Z.data(), 4 * n, cudaMemcpyHostToDevice, c->stream));
     if (n > 0) {
         LCUDA(cudaMemcpyAsync(B.X[cur], X.data(), 4 * n, cudaMemcpyHostToDevice, c->stream));
         LCUDA(cudaMemcpyAsync(B.Y[cur], Y.data(), 4 * n, cudaMemcpyHostToDevice, c->stream));
@@ -431,8 +433,9 @@ int particles_get(lepic_ctx *c, int sp, double *vxp, long long cap, long long *n
     SpeciesBuf &B = c->sp[sp];
     const long long ns = c->hcnt->n_slots[sp];
     std::vector<uint32_t> X(ns), Y(ns);
-    std::vector<float> VX(ns), VY(ns), VZ(ns);
+    std::vector<float> VX(ns), VY(ns), VZ(ns), Z(B.Z[0] ? ns : 0);
     const int cur = B.cur;
+    if (ns > 0 && B.Z[0]) LCUDA(cudaMemcpy(Z.data(), B.Z[cur], 4 * ns, cudaMemcpyDeviceToHost));
     if (ns > 0) {
         LCUDA(cudaMemcpy(X.data(), B.X[cur], 4 * ns, cudaMemcpyDeviceToHost));
         LCUDA(cudaMemcpy(Y.data(), B.Y[cur], 4 * ns, cudaMemcpyDeviceToHost));
@@ -447,7 +450,7 @@ int particles_get(lepic_ctx *c, int sp, double *vxp, long long cap, long long *n
         if (std::isnan(VX[i])) continue;
         if (vxp && k < cap) {
             double *p = vxp + 6 * k;
-            p[0] = (double)X[i] * ux; p[1] = (double)Y[i] * uy; p[2] = 0.0;
+            p[0] = (double)X[i] * ux; p[1] = (double)Y[i] * uy; p[2] = B.Z[0] ? (double)Z[i] : 0.0;
             p[3] = VX[i]; p[4] = VY[i]; p[5] = VZ[i];
         }
         k++;
@@ -466,6 +469,8 @@ struct LoadP {
     const uint8_t *cellwall;
     uint32_t *X[LEPIC_MAXSP], *Y[LEPIC_MAXSP];
     float *VX[LEPIC_MAXSP], *VY[LEPIC_MAXSP], *VZ[LEPIC_MAXSP];
+    float *Z[LEPIC_MAXSP];     // null without the 3rd dimension
+    double zmax;
     double vt[LEPIC_MAXSP];
     uint32_t k0, k1;
     DevCounters *cnt;
@@ -501,6 +506,10 @@ __global__ void k_load(LoadP P) {
             sincos(2.0 * pi * u01(r.w), &sz, &cz);
             P.X[s][i] = X; P.Y[s][i] = Y;
             P.VX[s][i] = (float)(vp * cs); P.VY[s][i] = (float)(vp * sn); P.VZ[s][i] = (float)(vpz * cz);
+            if (P.Z[s]) {   // z = rnd zmax, one z for the sample (load_part.f90:108, 141-143)
+                const U4 q = philox4x32_10(U4{(uint32_t)i, 0u, 0x5A504F53u, (uint32_t)(i >> 32)}, P.k0, P.k1);
+                P.Z[s][i] = (float)(u01(q.x) * P.zmax);
+            }
         }
     }
 }
@@ -523,10 +532,12 @@ int particles_load(lepic_ctx *c, const lepic_load_spec *sp) {
     for (int s = 0; s < g.ntype; s++) {
         SpeciesBuf &B = c->sp[s];
         P.X[s] = B.X[B.cur]; P.Y[s] = B.Y[B.cur]; P.VX[s] = B.VX[B.cur]; P.VY[s] = B.VY[B.cur]; P.VZ[s] = B.VZ[B.cur];
+        P.Z[s] = B.Z[B.cur];
         // vt0 = sqrt(2kT/m); load_gauss draws each component with sigma = vt0/sqrt(2)
         P.vt[s] = g.vt0[s];
     }
     P.k0 = (uint32_t)sp->seed; P.k1 = (uint32_t)(sp->seed >> 32) ^ 0x1234567u;
+    P.zmax = g.zmax;
     P.cnt = c->dcnt;
     k_load<<<c->num_sms * 8, 256, 0, c->stream>>>(P);
     LCUDA(cudaGetLastError());

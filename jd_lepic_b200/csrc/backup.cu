@@ -48,8 +48,9 @@ __global__ void k_live_counts(const float *VX, long long n, int *counts) {
 // packs the live particles of blocks [b0, b0 + nb) into out (vxp(6, .) from offset
 // off[b] - off[b0] of block b), in slot order
 __global__ void __launch_bounds__(BK_BLOCK) k_pack(const uint32_t *X, const uint32_t *Y, const float *VX,
-                                                  const float *VY, const float *VZ, long long n, long long b0,
-                                                  const long long *off, double ux, double uy, double *out) {
+                                                  const float *VY, const float *VZ, const float *Z, long long n,
+                                                  long long b0, const long long *off, double ux, double uy,
+                                                  double *out) {
     __shared__ int wsum[BK_BLOCK / 32];
     const long long b = b0 + blockIdx.x;
     const long long i = b * BK_BLOCK + threadIdx.x;
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(BK_BLOCK) k_pack(const uint32_t *X, const uint
     double *p = out + 6 * o;
     p[0] = (double)X[i] * ux;   // as lepic_gpu_get_particles
     p[1] = (double)Y[i] * uy;
-    p[2] = 0.0;
+    p[2] = Z ? (double)Z[i] : 0.0;   // z: the 3rd dimension's, else 0
     p[3] = vx;
     p[4] = VY[i];
     p[5] = VZ[i];
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(BK_BLOCK) k_pack(const uint32_t *X, const uint
 // unpacks n FP64 particles into the slots from dst (as lepic_gpu_put_particles); a particle
 // outside the box raises LERR_RANGE and becomes a hole
 __global__ void k_unpack(const double *in, long long n, long long dst, double sx, double sy, long long xl,
-                         long long yl, uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ,
+                         long long yl, uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, float *Z,
                          DevCounters *cnt) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const double *p = in + 6 * k;
@@ -88,6 +89,7 @@ __global__ void k_unpack(const double *in, long long n, long long dst, double sx
         }
         X[s] = (uint32_t)xi; Y[s] = (uint32_t)yi;
         VX[s] = (float)p[3]; VY[s] = (float)p[4]; VZ[s] = (float)p[5];
+        if (Z) Z[s] = (float)p[2];
     }
 }
 
@@ -270,7 +272,8 @@ extern "C" int lepic_gpu_write_backup(lepic_ctx *c, const char *path, double tim
             const long long bn = std::min(blocks_per_chunk, nb - b0);
             const long long cnt = offs[s][b0 + bn] - offs[s][b0];
             k_pack<<<(unsigned)bn, BK_BLOCK, 0, c->stream>>>(B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur],
-                                                             B.VZ[B.cur], n, b0, d_off, ux, uy, d_out);
+                                                             B.VZ[B.cur], B.Z[B.cur], n, b0, d_off, ux, uy,
+                                                             d_out);
             BK_CUDA(cudaGetLastError());
             if (pend == k) {  // the buffer this chunk goes to is still being written: finish it
                 w.write(h_buf[k], pend_bytes[k]);
@@ -361,7 +364,7 @@ extern "C" int lepic_gpu_read_backup(lepic_ctx *c, const char *path, double *tim
                 if (cudaMemcpyAsync(d_in, h_in, 48 * m, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) { ok = false; break; }
                 k_unpack<<<(unsigned)std::min<long long>(div_up(m, 256), (long long)c->num_sms * 8), 256, 0, c->stream>>>(
                     d_in, m, base + k0, sx, sy, xl, yl, B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur],
-                    c->dcnt);
+                    B.Z[B.cur], c->dcnt);
                 if (cudaStreamSynchronize(c->stream) != cudaSuccess) { ok = false; break; }
             }
             ok = ok && rd.end();
@@ -391,7 +394,8 @@ extern "C" int lepic_gpu_read_backup(lepic_ctx *c, const char *path, double *tim
 // restart.f90:115-129: |np_dup| - 1 copies of every slot appended after the occupied slots
 // (copy i of slot k at i * n + k).  A copied hole stays a plain hole (a loss record is tallied
 // once, from the original).
-__global__ void k_duplicate(long long n, int copies, uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ) {
+__global__ void k_duplicate(long long n, int copies, uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ,
+                            float *Z) {
     const long long tot = n * (long long)copies;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
         const long long k = t % n, d = n + t;
@@ -399,6 +403,7 @@ __global__ void k_duplicate(long long n, int copies, uint32_t *X, uint32_t *Y, f
         X[d] = X[k]; Y[d] = Y[k];
         VX[d] = isnan(vx) ? __int_as_float(HOLE_NAN) : vx;
         VY[d] = VY[k]; VZ[d] = VZ[k];
+        if (Z) Z[d] = Z[k];
     }
 }
 
@@ -420,7 +425,8 @@ extern "C" int lepic_gpu_duplicate_particles(lepic_ctx *c, int32_t np_dup) {
         if (n > 0) {
             const long long tot = n * (dup - 1);
             k_duplicate<<<(unsigned)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16), 256, 0,
-                          c->stream>>>(n, dup - 1, B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur]);
+                          c->stream>>>(n, dup - 1, B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur],
+                                       B.Z[B.cur]);
             LCUDA(cudaGetLastError());
         }
         const long long slots = n * dup, alive = c->hcnt->n_alive[s] * dup;

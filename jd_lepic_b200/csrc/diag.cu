@@ -267,7 +267,7 @@ int avg_sample(lepic_ctx *c, int it) {
         c->phi, c->Ed, c->nn, A->phi_avg);
     LCUDA(cudaGetLastError());
     A->cnt++;
-    return LEPIC_OK;
+    return zloss_after_avg(c, A->data, A->na1, A->na2, A->size_na, A->cnt);   // main.f90:950-960
 }
 
 extern "C" int lepic_gpu_calc_avg(lepic_ctx *c) {
@@ -392,7 +392,7 @@ extern "C" int lepic_gpu_get_tallies(lepic_ctx *c, lepic_tallies *out, int32_t r
             out->P_w[s][l] = Ek * h->v2_loss[s][l];
             lost += out->P_w[s][l];
         }
-        out->P_loss[0][s] = lost + P_src[s];
+        out->P_loss[0][s] = lost + P_src[s] + h->P1z[s];
         out->P_loss[1][s] = s == 0 ? P_heat : 0.0;
         out->P_loss[2][s] = h->P3[s];
         out->P_loss[3][s] = P_inj[s];

@@ -34,7 +34,7 @@ struct Product {            // a particle created by a collision, before its ord
     unsigned long long key; // parent slot * 8 + byproduct index (unique, orders the append)
     uint32_t X, Y;
     float vx, vy, vz;
-    int pad;
+    float z;                // the parent's z (collisions.f90:813; 0 without the 3rd dimension)
 };
 
 struct DevCounters {
@@ -66,6 +66,7 @@ struct TallyDev {
     double v2_loss[LEPIC_MAXSP][LEPIC_MAXLABEL];     // sum of v^2 [m^2/s^2]
     double P3[LEPIC_MAXSP];                           // collisions' energy change [J]
     double cnt_col[3][LEPIC_MAXCOL][LEPIC_MAXRG];
+    double P1z[LEPIC_MAXSP];                          // P_loss(1)'s Nm q phi of 3rd-dimension losses [J]
     double inv_np_rg[LEPIC_MAXSP][LEPIC_MAXRG];       // 1/np_tot_rg of the current collision step
 };
 
@@ -107,6 +108,7 @@ struct SpeciesBuf {
     int *claim = nullptr;      // DSMC: the incident slot that holds each target slot
     uint32_t *X[2], *Y[2];
     float *VX[2], *VY[2], *VZ[2];
+    float *Z[2] = {nullptr, nullptr};   // z [m], kept only with the 3rd-dimension model (hz >= 0)
     int cur;
     long long cap;
     unsigned long long *acc;   // deposit accumulator, one node grid
@@ -178,6 +180,14 @@ struct lepic_ctx {
     void *learn = nullptr;
     double phi_scale = 1.0;        // max |phi| of the initial potential (network input scale)
     long long n_unknown = 0;       // nodes with bcnd <= 0
+    // the 3rd virtual dimension of the 2.5D model (part_expmover.f90:269-309), when hz >= 0:
+    // z kept per particle (SpeciesBuf::Z), electrons and negative ions lost through the end
+    // plates when their z-energy exceeds phi - phi0 (else reflected), positive ions lost at the
+    // rate hz 2 uB / zmax with uB the Bohm speed on the averaging grid
+    int zloss = 0;
+    double hz = 0.0, phi0_end = 0.0;
+    int za1 = 0, za2 = 0, zsize_na = 1;   // the uB grid: na = n / size_na, (na1+1)(na2+1) nodes
+    float *uB = nullptr;                  // [ptype][(na1+1)(na2+1)], m/s
     // particle sources (sources.cu), created by lepic_gpu_set_sources
     void *src = nullptr;
     // averaging diagnostics (diag.cu), created by lepic_gpu_set_avg
@@ -333,6 +343,8 @@ int field_np_grid(lepic_ctx *c, int ptype, double *d_out);
 int mg_solve(lepic_ctx *c, double eps, int mode);
 int mg_init(lepic_ctx *c);
 int mg_residual_stats(lepic_ctx *c);
+// the Bohm speed map of the 3rd-dimension model from an averaging sample (zloss.cu)
+int zloss_after_avg(lepic_ctx *c, const double *data, int na1, int na2, int size_na, int cnt);
 // xtrap: the warm start may extrapolate; fp64: the V-cycle in FP64 (mode 4) instead of FP32
 int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap, bool fp64 = false);
 int push_deposit(lepic_ctx *c, int it, bool move);

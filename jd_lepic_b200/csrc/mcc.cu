@@ -36,6 +36,7 @@ struct MccP {
     double nm_vc[LEPIC_MAXSP];   // Nm / Vc per species
     uint32_t *X, *Y;
     float *VX, *VY, *VZ;
+    const float *Z;             // the incident species' z (3rd dimension), null without it
     Product *prod[LEPIC_MAXSP];
     int prod_cap[LEPIC_MAXSP];
     DevCounters *cnt;
@@ -385,7 +386,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
                 pr.key = (unsigned long long)slot * 8ull + (unsigned long long)ib;
                 pr.X = X; pr.Y = Y;
                 pr.vx = (float)vbx; pr.vy = (float)vby; pr.vz = (float)vbz;
-                pr.pad = 0;
+                pr.z = P.Z ? P.Z[slot] : 0.0f;   // collisions.f90:813: the incident's z
                 P.prod[bt][k] = pr;
             } else {
                 set_err(P.cnt, LERR_CAPACITY, 200);
@@ -529,7 +530,7 @@ __global__ void k_nu_max(NuMaxP P) {
 
 // Ordered append of one species' products after its occupied slots (single CTA).
 __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long long *sortbuf,
-                             uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, long long cap,
+                             uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, float *Z, long long cap,
                              DevCounters *cnt) {
     __shared__ unsigned long long sm[4096];
     int n = (int)min(cnt->prod_count[sp], (unsigned int)prod_cap);
@@ -548,6 +549,7 @@ __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long 
         const Product &p = prod[(int)(a[q] & 0xFFFFFFull)];
         long long s = base + q;
         X[s] = p.X; Y[s] = p.Y; VX[s] = p.vx; VY[s] = p.vy; VZ[s] = p.vz;
+        if (Z) Z[s] = p.z;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -640,6 +642,7 @@ int mcc_collide(lepic_ctx *c, int it, bool diag) {
         P.diag = diag ? 1 : 0; P.ss_diag = c->ss_diag;
         for (int t = 0; t < g.ntype; t++) P.nm_vc[t] = g.Nm[t] / (g.dx * g.dy * g.zmax);
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+        P.Z = B.Z[B.cur];
         for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
         P.cnt = c->dcnt;
         P.nu_max = c->nu_max[s];
@@ -702,7 +705,7 @@ int mcc_collide(lepic_ctx *c, int it, bool diag) {
     for (int t = 0; t < g.ntype; t++) {
         SpeciesBuf &B = c->sp[t];
         k_mcc_commit<<<1, 1024, 0, c->stream>>>(t, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],
-                                                B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.cap, c->dcnt);
+                                                B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.Z[B.cur], B.cap, c->dcnt);
         LCUDA(cudaGetLastError());
     }
     return LEPIC_OK;

@@ -46,6 +46,16 @@ struct PushP {
     uint32_t step_key;
     int tw, th, ntx, M, WX, WY, win;
     long long xlim, ylim;      // nx<<S, ny<<S
+    // the 3rd dimension (zloss.cu): z per slot, its length, the end plates' potential and
+    // phi for the electrons' test, the ions' loss factor hz 2 dt / zmax and the uB map
+    float *Z;                  // null: no 3rd-dimension model
+    int zneg, za1, zsize;
+    float zmax, dtf, nu_fac;
+    double phi0, m_over_2qe, nmq;
+    const double *phi;
+    const float *uB;
+    TallyDev *tal;
+    uint32_t zk0, zk1, it;
 };
 
 #define PUSH_G 4    // consecutive slots per thread: one 16-byte vector per array
@@ -244,6 +254,44 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     return true;
 }
 
+// The 3rd virtual dimension (part_expmover.f90:216-219, 269-309, 400-421) for a particle that
+// the wall test kept, at its new cell (ix, iy): z moves with the new vz; electrons and negative
+// ions leaving [0, zmax] are lost if 0.5 m vz^2 / qe >= phi(ix,iy) - phi0, else reflected; a
+// positive ion is lost with probability hz 2 uB / zmax dt.  A lost particle's slot becomes a
+// hole holding an igrid-0 loss record; P_loss(1) also takes Nm q phi at the loss point.
+__device__ __forceinline__ bool zstep(const PushP &P, int i, uint32_t &X, uint32_t &Y, float &vx, float &vy,
+                                      float &vz, int ix, int iy, unsigned int &lost) {
+    float z = P.Z[i] + P.dtf * vz;   // :219
+    bool gone = false;
+    if (P.zneg) {
+        if (z <= 0.0f || z >= P.zmax) {                                   // :276-292
+            const double Eki = P.m_over_2qe * (double)vz * (double)vz;
+            if (Eki >= P.phi[ix + (long long)iy * P.W] - P.phi0) gone = true;
+            else { vz = -vz; z = z <= 0.0f ? 0.02f * P.zmax : 0.98f * P.zmax; }
+        }
+    } else {                                                              // :294-307
+        const int ixc = P.zsize == 1 ? ix : (int)(X >> P.S) / P.zsize + 1;
+        const int iyc = P.zsize == 1 ? iy : (int)(Y >> P.S) / P.zsize + 1;
+        const float ub = P.uB[(ixc - 1) + (long long)(iyc - 1) * (P.za1 + 1)];
+        const uint32_t u = philox4x32_10(U4{(uint32_t)i, P.it, 0x5A4C4F53u, (uint32_t)P.sp}, P.zk0, P.zk1).x;
+        if (u01(u) <= (double)(P.nu_fac * ub)) gone = true;
+    }
+    P.Z[i] = z;
+    if (!gone) return true;
+    // Nm q phi at the loss point, the bilinear phi of the cell (:400-421)
+    const uint32_t mask = (1u << P.S) - 1u;
+    const double px = 1.0 - (double)(X & mask) * (double)P.inv2S, py = 1.0 - (double)(Y & mask) * (double)P.inv2S;
+    const long long n00 = ix + (long long)iy * P.W;
+    const double phip = px * py * P.phi[n00] + (1.0 - px) * py * P.phi[n00 + 1] +
+                        (1.0 - px) * (1.0 - py) * P.phi[n00 + P.W + 1] + px * (1.0 - py) * P.phi[n00 + P.W];
+    atomicAdd(&P.tal->P1z[P.sp], P.nmq * phip);
+    lost++;
+    X = (uint32_t)n00;
+    Y = __float_as_uint(vx);
+    vx = __int_as_float(LOSS_NAN_OTHER);
+    return false;
+}
+
 // Each thread takes PUSH_G consecutive slots per iteration (one 16-byte vector load and store
 // per array): after the sort consecutive particles mostly share a cell, so the deposit
 // accumulates runs of equal cells in registers and adds each run to the accumulators once.
@@ -330,6 +378,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                     int ix, iy;   // the deposit cell INT(x/h)+1 (x >= 0)
                     if (MOVE) {
                         alive = move_regs<BMODE, GEN>(P, i, X[p], Y[p], vx[p], vy[p], vz[p], cnt, lost, ix, iy);
+                        if (GEN && alive && P.Z) alive = zstep(P, i, X[p], Y[p], vx[p], vy[p], vz[p], ix, iy, lost);
                     } else {
                         alive = !isnan(vx[p]);
                         ix = (int)(X[p] >> P.S) + 1;
@@ -480,7 +529,24 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         if (!P.win) smem = 0;
         P.xlim = (long long)g.nx << c->S;
         P.ylim = (long long)g.ny << c->S;
-        const bool gen = P.pbc || P.nmn || P.negion_nmn;
+        if (c->zloss && B.Z[0]) {
+            P.Z = B.Z[B.cur];
+            P.zneg = g.charge[s] < 0.0 ? 1 : 0;
+            P.za1 = c->za1; P.zsize = c->zsize_na;
+            P.zmax = (float)g.zmax;
+            P.dtf = (float)g.dt;
+            P.nu_fac = (float)(c->hz * 2.0 / g.zmax * g.dt);
+            P.phi0 = c->phi0_end;
+            P.m_over_2qe = 0.5 * g.mass[s] / g.qe;
+            P.nmq = g.Nm[s] * g.charge[s];
+            P.phi = c->phi;
+            P.uB = c->uB + (size_t)s * (c->za1 + 1) * (c->za2 + 1);
+            P.tal = c->tally;
+            P.zk0 = (uint32_t)g.seed; P.zk1 = (uint32_t)(g.seed >> 32) ^ 0x5A10C5u;
+            P.it = (uint32_t)it;
+        }
+        // the boundary options and the 3rd dimension take the general mover for every particle
+        const bool gen = P.pbc || P.nmn || P.negion_nmn || P.Z;
         int r;
         if (bmode == 1) r = launch_b<1>(c, P, smem, gen, move);
         else if (bmode == 2) r = launch_b<2>(c, P, smem, gen, move);

@@ -271,7 +271,8 @@ __global__ void k_segsort_big(const int *offsets, int *perm, const int *bigseg, 
 // gathers, 16-byte stores (the slot arrays are allocated in whole groups of 8)
 __global__ void k_gather(const int *perm, const int *offsets, long long nkeys, const uint32_t *X,
                          const uint32_t *Y, const float *VX, const float *VY, const float *VZ,
-                         uint32_t *X2, uint32_t *Y2, float *VX2, float *VY2, float *VZ2) {
+                         uint32_t *X2, uint32_t *Y2, float *VX2, float *VY2, float *VZ2, const float *Z,
+                         float *Z2) {
     const long long n = offsets[nkeys];
     const long long ng = (n + 3) / 4;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ng;
@@ -289,10 +290,12 @@ __global__ void k_gather(const int *perm, const int *offsets, long long nkeys, c
             *reinterpret_cast<float4 *>(VX2 + j) = a;
             *reinterpret_cast<float4 *>(VY2 + j) = b;
             *reinterpret_cast<float4 *>(VZ2 + j) = c;
+            if (Z) *reinterpret_cast<float4 *>(Z2 + j) = make_float4(Z[p.x], Z[p.y], Z[p.z], Z[p.w]);
         } else {
             for (long long q = j; q < n; q++) {
                 const int i = perm[q];
                 X2[q] = X[i]; Y2[q] = Y[i]; VX2[q] = VX[i]; VY2[q] = VY[i]; VZ2[q] = VZ[i];
+                if (Z) Z2[q] = Z[i];
             }
         }
     }
@@ -370,7 +373,7 @@ int sort_species(lepic_ctx *c, int sp) {
     k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, c->perm, c->bigseg, c->dcnt);
     k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
                                                    B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt], B.VX[nxt],
-                                                   B.VY[nxt], B.VZ[nxt]);
+                                                   B.VY[nxt], B.VZ[nxt], B.Z[cur], B.Z[nxt]);
     k_items<<<1, 1024, 0, c->stream>>>(c->offsets, c->ntiles, c->tw * c->th, B.items, B.max_items,
                                        c->dcnt, sp, nk);
     LCUDA(cudaGetLastError());

@@ -421,6 +421,8 @@ struct InjP {
     const double *phi;
     uint32_t *X[LEPIC_MAXSP], *Y[LEPIC_MAXSP];
     float *VX[LEPIC_MAXSP], *VY[LEPIC_MAXSP], *VZ[LEPIC_MAXSP];
+    float *Z[LEPIC_MAXSP];  // the 3rd dimension's z (null without it)
+    double zmax;
     unsigned long long *acc[LEPIC_MAXSP];
     unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
     long long ss_nn;
@@ -547,6 +549,10 @@ __global__ void __launch_bounds__(INJ_THREADS) k_inject(InjP P, double *part) {
         const float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
         P.X[s][slot] = Xf; P.Y[s][slot] = Yf;
         P.VX[s][slot] = fvx; P.VY[s][slot] = fvy; P.VZ[s][slot] = fvz;
+        if (P.Z[s]) {   // z = rnd zmax (part_injection.f90:129)
+            const U4 zq = philox4x32_10(U4{(uint32_t)j, (uint32_t)s, 0x495A504Fu, P.it}, P.k0, P.k1);
+            P.Z[s][slot] = (float)(u01(zq.x) * P.zmax);
+        }
         if (P.ss_map)   // part_injection.f90:205: the source at the particle's (ix, iy)
             atomicAdd(P.ss_map + (size_t)(2 * s) * P.ss_nn + ix + (long long)iy * P.W, 1u);
         // deposit (the injected particle is in this step's np)
@@ -593,6 +599,8 @@ struct EmitP {
     const int32_t *bcnd;
     uint32_t *X[2], *Y[2];
     float *VX[2], *VY[2], *VZ[2];
+    float *Z[2];            // the 3rd dimension's z (null without it)
+    double zmax;
     long long max_attempts_extra;
     unsigned int *ss_map;   // ss2D counts (null: not accumulated), see lepic_ctx::ss_map
     long long ss_nn;
@@ -699,6 +707,10 @@ __global__ void __launch_bounds__(EMIT_THREADS) k_emit(EmitP P) {
                 P.X[qe][slot] = (uint32_t)min((long long)fx, xl);
                 P.Y[qe][slot] = (uint32_t)min((long long)fy, yl);
                 P.VX[qe][slot] = fvx; P.VY[qe][slot] = fvy; P.VZ[qe][slot] = fvz;
+                if (P.Z[qe]) {   // z_inj = zmax (1 - rnd), moved with vz (part_flux_emitter.f90:139, 207)
+                    const U4 zq = philox4x32_10(U4{(uint32_t)slot, (uint32_t)qe, 0x455A504Fu, P.it}, P.k0, P.k1);
+                    P.Z[qe][slot] = (float)(P.zmax * (1.0 - u01(zq.x)) + vz * dt_tmp);
+                }
             }
         }
         // the created particles of this round per species: those with j < Nh
@@ -955,11 +967,13 @@ static int run_injection(lepic_ctx *c, int it) {
         SpeciesBuf &B = c->sp[sp];
         P.X[sp] = B.X[B.cur]; P.Y[sp] = B.Y[B.cur];
         P.VX[sp] = B.VX[B.cur]; P.VY[sp] = B.VY[B.cur]; P.VZ[sp] = B.VZ[B.cur];
+        P.Z[sp] = B.Z[B.cur];
         P.acc[sp] = B.acc;
     }
     P.cellwall = c->cellwall;
     P.ss_map = ss_counts(c); P.ss_nn = c->nn;
     P.phi = c->phi;
+    P.zmax = g.zmax;
     P.it = (uint32_t)it;
     keys(s, &P.k0, &P.k1);
     k_inject<<<INJ_BLOCKS, INJ_THREADS, 0, c->stream>>>(P, S->part);
@@ -1004,7 +1018,9 @@ static int run_emitter(lepic_ctx *c, int it) {
         SpeciesBuf &B = c->sp[sp];
         P.X[q] = B.X[B.cur]; P.Y[q] = B.Y[B.cur];
         P.VX[q] = B.VX[B.cur]; P.VY[q] = B.VY[B.cur]; P.VZ[q] = B.VZ[B.cur];
+        P.Z[q] = B.Z[B.cur];
     }
+    P.zmax = g.zmax;
     P.bcnd = c->bcnd;
     P.ss_map = ss_counts(c); P.ss_nn = c->nn;
     P.max_attempts_extra = 65536;

@@ -287,6 +287,17 @@ class GpuSimulation:
                    "read_backup")
         return t.value, gt.value, pc.value
 
+    def set_zloss(self, hz: float, phi0: float = 0.0, size_na: int = 1):
+        """The 3rd virtual dimension (hz >= 0 in the deck): z kept per particle, end-plate and
+        Bohm losses in the mover (part_expmover.f90:269-309)."""
+        z = capi.LepicZlossConfig(hz, phi0, size_na)
+        self.check(self.lib.lepic_gpu_set_zloss(self.ctx, C.byref(z)), "set_zloss")
+
+    def set_bohm_speed(self, uB: np.ndarray):
+        """uB(na1+1, na2+1, ntype) in Fortran order: a (ntype, na2+1, na1+1) array."""
+        a = np.ascontiguousarray(uB, dtype=np.float64)
+        self.check(self.lib.lepic_gpu_set_bohm_speed(self.ctx, _dp(a)), "set_bohm_speed")
+
     def options(self) -> capi.LepicOptions:
         o = capi.LepicOptions()
         self.check(self.lib.lepic_gpu_get_options(self.ctx, C.byref(o)), "get_options")

@@ -52,6 +52,12 @@ static void check_outofbounds(int *ix, int *iy, int nx, int ny) {
 void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
                   const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
                   o_push_tally *t) {
+    o_part_mover_z(c, ptype, Ei, Bi, bcnd, vxp, np_tot, flag_dead, t, NULL);
+}
+
+void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                    const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                    o_push_tally *t, const o_zloss *zl) {
     const int nx = c->nx, ny = c->ny;
     const double h1 = c->dx, h2 = c->dy, dt = c->dt;
     const double amu = 1.66053886e-27;
@@ -136,8 +142,41 @@ void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
             flag_lost = 1;
         else if (c->charge[ptype] < 0 && c->mass[ptype] >= amu && xp < 0.0 && c->flag_nmn == 1)
             flag_lost = 3;
+        else if (zl) { /* :269-309 the 3rd virtual dimension */
+            if (c->charge[ptype] < 0) {
+                if (zp <= 0.0 || zp >= c->zmax) {
+                    const double Eki = 0.5 * c->mass[ptype] * vz * vz / c->qe;
+                    if (Eki >= zl->phi[NODE(ix, iy, nx)] - zl->phi0) flag_lost = 2;
+                    else {
+                        vz = -vz;
+                        zp = zp <= 0.0 ? 0.02 * c->zmax : 0.98 * c->zmax;
+                    }
+                }
+            } else {
+                int ixc = ix, iyc = iy;
+                if (zl->size_na != 1) {
+                    ixc = (int)(xp / (zl->size_na * h1)) + 1;
+                    iyc = (int)(yp / (zl->size_na * h2)) + 1;
+                }
+                /* the device's draw: Philox keyed by (slot, step, tag, species); the product
+                   nu_3D dt in FP32, as the device forms it */
+                const float p = zl->nu_fac * zl->uB[(ixc - 1) + (int64_t)(iyc - 1) * (zl->na1 + 1)];
+                uint32_t ctr[4] = {(uint32_t)i, zl->it, 0x5A4C4F53u, (uint32_t)ptype}, out[4];
+                o_philox4x32_10(ctr, zl->k0, zl->k1, out);
+                if (o_u01(out[0]) <= (double)p) flag_lost = 2;
+            }
+        }
         if (flag_lost >= 1) { /* :314-427 */
             np_lost++;
+            if (t && flag_lost == 2) { /* :400-421 Nm q phi at the loss point */
+                const double px2 = ((int)(xp / h1) + 1) * h1, py2 = ((int)(yp / h2) + 1) * h2;
+                const int jx = (int)(xp / h1) + 1, jy = (int)(yp / h2) + 1;
+                const double qx = (px2 - xp) / h1, qy = (py2 - yp) / h2;
+                const double phip = qx * qy * zl->phi[NODE(jx, jy, nx)] + (1.0 - qx) * qy * zl->phi[NODE(jx + 1, jy, nx)] +
+                                    (1.0 - qx) * (1.0 - qy) * zl->phi[NODE(jx + 1, jy + 1, nx)] +
+                                    qx * (1.0 - qy) * zl->phi[NODE(jx, jy + 1, nx)];
+                t->P1z += c->Nm[ptype] * c->charge[ptype] * phip;
+            }
             if (t) {
                 t->n_lost++;
                 int igrid = flag_lost == 1 ? bcnd[NODE(ix, iy, nx)] : 0;

@@ -65,7 +65,20 @@ typedef struct {
                              loss (part_expmover.f90:338), 0 for the other losses; labels
                              above 15 in the last                                   */
     double v2_loss[16];   /* sum of the lost particles' v^2 per igrid (P_w / 0.5 Nm m) */
+    double P1z;           /* P_loss(1)'s Nm q phi of 3rd-dimension losses (:400-421)      */
 } o_push_tally;
+
+/* the 3rd virtual dimension (hz >= 0; part_expmover.f90:269-309): z in vxp[2] moves with vz;
+ * c->zmax is its length.  Positive ions draw from the device's counter stream (slot index i of
+ * the input array, step it, key k0 k1) against nu_fac * uB, nu_fac = hz 2 dt / zmax in FP32. */
+typedef struct {
+    double phi0;
+    const double *phi;      /* phi(0:nx+2, 0:ny+2)                          */
+    const float *uB;        /* this species' uB(na1+1, na2+1)               */
+    int na1, size_na;
+    float nu_fac;
+    uint32_t k0, k1, it;
+} o_zloss;
 
 typedef struct {
     int64_t n_cand[O_MAXSP];              /* Nc per species                 */
@@ -87,6 +100,10 @@ void o_load_gauss(double *vx, double *vy, double vt, const double rnd[2]);
 void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
                   const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
                   o_push_tally *t);
+/* the same with the 3rd-dimension model when zl is not NULL */
+void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                    const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                    o_push_tally *t, const o_zloss *zl);
 
 /* part_expmover.f90:520-610 -- adds into npg (caller zeroes it). */
 void o_charge_deposition(const o_cfg *c, int ptype, const double *vxp, int64_t np_tot,

@@ -60,7 +60,13 @@ class OXs(C.Structure):
 
 class OPushTally(C.Structure):
     _fields_ = [("n_lost", C.c_int64), ("n_dead", C.c_int64), ("n_loss", C.c_int64 * 16),
-                ("v2_loss", C.c_double * 16)]
+                ("v2_loss", C.c_double * 16), ("P1z", C.c_double)]
+
+
+class OZloss(C.Structure):
+    _fields_ = [("phi0", C.c_double), ("phi", C.POINTER(C.c_double)), ("uB", C.POINTER(C.c_float)),
+                ("na1", C.c_int), ("size_na", C.c_int), ("nu_fac", C.c_float),
+                ("k0", C.c_uint32), ("k1", C.c_uint32), ("it", C.c_uint32)]
 
 
 class OMccTally(C.Structure):
@@ -116,6 +122,8 @@ def lib() -> C.CDLL:
         L.o_load_gauss.argtypes = [_DP, _DP, C.c_double, _DP]
         L.o_part_mover.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _LP, _I8,
                                    C.POINTER(OPushTally)]
+        L.o_part_mover_z.argtypes = [C.POINTER(OCfg), C.c_int, _DP, _DP, _IP, _DP, _LP, _I8,
+                                     C.POINTER(OPushTally), C.POINTER(OZloss)]
         L.o_charge_deposition.argtypes = [C.POINTER(OCfg), C.c_int, _DP, C.c_int64, _DP, _DP]
         L.o_np_periodic.argtypes = [C.POINTER(OCfg), _DP, _IP]
         L.o_calc_rhs.argtypes = [C.POINTER(OCfg), _DP, _DP]
@@ -228,6 +236,26 @@ def mover(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, flag_dead=None):
     t = OPushTally()
     fd = flag_dead.ctypes.data_as(_I8) if flag_dead is not None else None
     lib().o_part_mover(C.byref(cfg), ptype, dp(Ei), dp(Bi), ip(bcnd), dp(vxp), C.byref(n), fd, C.byref(t))
+    return n.value, t
+
+
+def zloss_keys(seed: int):
+    """The device's key of the 3rd-dimension draws (push.cu, zstep)."""
+    return int(seed) & 0xFFFFFFFF, ((int(seed) >> 32) ^ 0x5A10C5) & 0xFFFFFFFF
+
+
+def mover_z(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, phi, phi0, uB, na1, size_na, hz, seed, it):
+    """o_part_mover_z on vxp (n, 6) in place (z in column 2); uB: this species' (na2+1, na1+1)
+    map.  Returns (n survivors, tally)."""
+    n = C.c_int64(vxp.shape[0])
+    t = OPushTally()
+    phi_a = np.ascontiguousarray(phi, dtype=np.float64)
+    ub = np.ascontiguousarray(uB, dtype=np.float32)
+    k0, k1 = zloss_keys(seed)
+    z = OZloss(phi0, dp(phi_a), ub.ctypes.data_as(C.POINTER(C.c_float)), na1, size_na,
+               float(np.float32(hz * 2.0 / cfg.zmax * cfg.dt)), k0, k1, it)
+    lib().o_part_mover_z(C.byref(cfg), ptype, dp(Ei), dp(Bi), ip(bcnd), dp(vxp), C.byref(n), None, C.byref(t),
+                         C.byref(z))
     return n.value, t
 
 

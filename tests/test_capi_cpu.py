@@ -48,7 +48,8 @@ def test_struct_layouts_match_c():
                "lepic_mcc_stats": _capi.LepicMccStats, "lepic_load_spec": _capi.LepicLoadSpec,
                "lepic_cnn_config": _capi.LepicCnnConfig, "lepic_cnn_stats": _capi.LepicCnnStats,
                "lepic_source_config": _capi.LepicSourceConfig, "lepic_source_tally": _capi.LepicSourceTally,
-               "lepic_tallies": _capi.LepicTallies, "lepic_options": _capi.LepicOptions}
+               "lepic_tallies": _capi.LepicTallies, "lepic_options": _capi.LepicOptions,
+               "lepic_zloss_config": _capi.LepicZlossConfig}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -276,3 +276,44 @@ def test_oracle_dsmc_pairs_conserve_and_targets_come_from_the_cell():
     for k in range(ci.size):
         near[k] = np.any(np.abs(ex - ix[k]) + np.abs(ey - iy[k]) <= 1) or np.any((ey == iy[k] + 1) | (ey == iy[k] - 1))
     assert near.all()
+
+
+def test_oracle_third_dimension_model():
+    """o_part_mover_z (part_expmover.f90:269-309): an electron crossing an end plate with more
+    z-energy than phi - phi0 is lost, with less it is reflected to 0.02 / 0.98 zmax with vz
+    reversed; ions are lost at the rate hz 2 uB / zmax dt."""
+    import math
+    from jd_lepic_b200 import configs, deck as dk
+    from jd_lepic_b200.simulation import species_params
+    from oracle import oracle as O
+    case = configs.case0(ppc=1, nx=16, ny=16)
+    case.zmax = 0.01
+    sp = species_params(case, dk.read_reactions(case.deck_text, case.ngas))
+    cfg = O.make_cfg(case, sp)
+    E = np.zeros((case.ny + 3, case.nx + 3, 2))
+    phi = np.full((case.ny + 3, case.nx + 3), 5.0)
+    me = sp.mass[0]
+    v = lambda eV: math.sqrt(2 * eV * dk.QE / me)
+    p = np.zeros((4, 6))
+    p[:, 0] = p[:, 1] = 8.3 * case.dx
+    p[0, 2], p[0, 5] = 1e-9, -v(7.0)                # 7 eV >= 5 - (-1): lost
+    p[1, 2], p[1, 5] = 1e-9, -v(5.0)                # 5 eV < 6: reflected at 0.02 zmax
+    p[2, 2], p[2, 5] = case.zmax - 1e-9, v(3.0)     # reflected at 0.98 zmax
+    p[3, 2], p[3, 5] = 0.5 * case.zmax, v(50.0)     # stays inside
+    n, t = O.mover_z(cfg, 0, E, None, case.bcnd, p, phi, -1.0, np.zeros((17, 17), np.float32), 16, 1, 1.0, 1, 1)
+    assert n == 3 and t.n_loss[0] == 1
+    assert p[0, 2] == pytest.approx(0.02 * case.zmax) and p[0, 5] == pytest.approx(v(5.0))
+    assert p[1, 2] == pytest.approx(0.98 * case.zmax) and p[1, 5] == pytest.approx(-v(3.0))
+    assert p[2, 2] == pytest.approx(0.5 * case.zmax + case.dt * v(50.0))
+    assert t.P1z == pytest.approx(sp.Nm[0] * sp.charge[0] * 5.0)
+    rng = np.random.default_rng(1)
+    m = 20000
+    ions = np.zeros((m, 6))
+    ions[:, 0] = rng.uniform(1, 15, m) * case.dx
+    ions[:, 1] = rng.uniform(1, 15, m) * case.dy
+    ions[:, 2] = 0.5 * case.zmax
+    uB = np.full((17, 17), 3000.0, np.float32)
+    hz = 5e4
+    n, _ = O.mover_z(cfg, 1, E, None, case.bcnd, ions, phi, 0.0, uB, 16, 1, hz, 1, 3)
+    expect = m * hz * 2 * 3000.0 / case.zmax * case.dt
+    assert abs((m - n) - expect) < 5 * math.sqrt(expect)
