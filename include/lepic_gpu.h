@@ -151,7 +151,8 @@ int lepic_gpu_destroy(lepic_ctx *ctx);
 
 /* The context's CUDA stream (a cudaStream_t). */
 void *lepic_gpu_stream(lepic_ctx *ctx);
-/* Waits for the context's stream and reports any device-side error flag as a code. */
+/* Waits for the context's stream and the asynchronous downloads, and reports any device-side
+ * error flag as a code. */
 int lepic_gpu_sync(lepic_ctx *ctx);
 /* Text of the last error of this context (valid until the next call). */
 const char *lepic_gpu_last_error(lepic_ctx *ctx);
@@ -190,6 +191,14 @@ int lepic_gpu_dens_red(lepic_ctx *ctx, double *np_red_out, double *np_mx_out);
  * ||b-Au||/||b|| for mode 1.  stats (nullable) forces a sync. */
 int lepic_gpu_iterative_solver(lepic_ctx *ctx, double *phi_inout, double eps, int32_t mode,
                                lepic_solve_stats *stats);
+/* The same solve with its two copies split and the download overlapped: phi_in (nullable) is
+ * uploaded before the solve (after any download into host memory still in flight), and phi_out
+ * (nullable, may be the same array) receives the solution asynchronously -- the call returns
+ * without waiting, the copy runs beside the kernels enqueued next (E field, push), and phi_out
+ * is filled once a call that synchronises the context returns (lepic_gpu_sync, or any call with
+ * an output pointer or stats).  The host must not read or write phi_out before that. */
+int lepic_gpu_iterative_solver_async(lepic_ctx *ctx, const double *phi_in, double *phi_out, double eps,
+                                     int32_t mode);
 /* Warm start of the mixed-precision solve (mode 1): 0 (default) starts from the input phi, as
  * iterative_solver does with its in/out u; 1 starts from the linear extrapolation
  * 2 phi_(n-1) - phi_(n-2) of the inputs of this and the previous solve, for a time loop in
@@ -244,6 +253,10 @@ int lepic_gpu_set_options(lepic_ctx *ctx, const lepic_options *in);
 
 /* Copies a device grid (LEPIC_GRID_*) to the host, FP64, in the layouts above. */
 int lepic_gpu_get_grid(lepic_ctx *ctx, int32_t which, double *out);
+/* The same for LEPIC_GRID_PHI, _RHS and _EI without waiting: the grid as it is after the work
+ * enqueued so far is copied beside the work enqueued next; out is filled once a call that
+ * synchronises the context returns (as for lepic_gpu_iterative_solver_async's phi_out). */
+int lepic_gpu_get_grid_async(lepic_ctx *ctx, int32_t which, double *out);
 /* Sets phi (LEPIC_GRID_PHI) or rhs (LEPIC_GRID_RHS) from the host. */
 int lepic_gpu_set_grid(lepic_ctx *ctx, int32_t which, const double *in);
 /* Live particles per species and the cumulative counters. */
@@ -472,6 +485,42 @@ int lepic_gpu_set_zloss(lepic_ctx *ctx, const lepic_zloss_config *cfg);
 /* uB(na1+1, na2+1, ntype) [m/s] in Fortran order (main.f90:197), from the host (e.g. after an
  * MPI reduction of the averages); the device's averaging samples overwrite it. */
 int lepic_gpu_set_bohm_speed(lepic_ctx *ctx, const double *uB);
+
+/* ---- dielectric walls (generate_boundary.f90:149-152, part_expmover.f90:340-350,
+ * main.f90:756-809) ------------------------------------------------------------------------
+ * dtype[label] (LEPIC_MAXLABEL entries, labels above the last in the last): 1 for a wall label
+ * drawn as dielectric, else 0; Ca its capacitance [F/m^2].  A wall loss on a dielectric label
+ * (or under one) leaves Nm q on the label's rows iy and iy+1 of the loss cell, split by the loss
+ * point's y; once per step before the Poisson solve (lepic_gpu_step does it, or call
+ * lepic_gpu_dielectric_update) the label's wall nodes of rows 2..ny (every row with the periodic
+ * option) take phi += kd dq(label, iy) / (Ca dy), kd = 2 on rows 1 and ny+1, and the charge
+ * starts again from zero.  A multi-rank host sums the charges over its ranks first, as
+ * main.f90:771-772 does (get, all-reduce, set, then lepic_gpu_dielectric_update before the
+ * solve; lepic_gpu_step then finds nothing left to add). */
+int lepic_gpu_set_dielectrics(lepic_ctx *ctx, const int32_t *dtype, double Ca);
+int lepic_gpu_dielectric_update(lepic_ctx *ctx);
+/* the charge collected since the last update, dq(0:ny+2, label) as [label][ny+3] [C] */
+int lepic_gpu_get_dielectric_charge(lepic_ctx *ctx, double *dq);
+/* replaces it (a multi-rank host: the sum over ranks, main.f90:771-772, before the update) */
+int lepic_gpu_set_dielectric_charge(lepic_ctx *ctx, const double *dq);
+
+/* ---- secondary emission (read_input.f90:164-184, generate_boundary.f90:119-122,
+ * part_expmover.f90:354-392) -----------------------------------------------------------------
+ * A positive ion lost on the wall label igrid_sec emits INT(gam_sec) electrons, one more with
+ * probability gam_sec - INT(gam_sec), at (xg_sec, y, z) of its loss point with
+ * vx = -SIGN(1, vx_ion) vt sqrt(-ln(1-r)), (vy, vz) Maxwellian, vt = sqrt(2 qe THm / m_e); they
+ * are appended to the electrons after the push (in the order of their ions' slots) and are in
+ * that step's density.  Each adds 0.5 Nm m (vx^2 + vz^2 + vz^2) to the electrons' P_loss(4),
+ * the reference's sum.  The draws come from the counter stream keyed by (seed, step, species,
+ * slot, electron).  gam_sec = 0 switches it off; 0 <= gam_sec < 8. */
+typedef struct lepic_secondary_config {
+    double gam_sec;            /* emission coefficient                                     */
+    int32_t igrid_sec;         /* the emitting wall label (ABS of the deck's value), >= 1  */
+    int32_t pad;
+    double xg_sec;             /* x of the emitting grid [m]                               */
+    double THm;                /* the electrons' temperature [eV]                          */
+} lepic_secondary_config;
+int lepic_gpu_set_secondary(lepic_ctx *ctx, const lepic_secondary_config *sec);
 
 /* ---- particle backup (main.f90:1102-1139, restart.f90:48-149) ---------------------------
  * The reference's particlesNNN.bak: Fortran unformatted sequential records (4-byte length

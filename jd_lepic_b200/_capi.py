@@ -187,6 +187,11 @@ class LepicZlossConfig(C.Structure):
     _fields_ = [("hz", C.c_double), ("phi0", C.c_double), ("size_na", C.c_int32)]
 
 
+class LepicSecondaryConfig(C.Structure):
+    _fields_ = [("gam_sec", C.c_double), ("igrid_sec", C.c_int32), ("pad", C.c_int32), ("xg_sec", C.c_double),
+                ("THm", C.c_double)]
+
+
 class LepicOptions(C.Structure):
     _fields_ = [("mx_nu1", C.c_int32), ("mx_nu2", C.c_int32), ("mx_nuc", C.c_int32), ("mx_omega", C.c_float),
                 ("mx_onchip_bytes", C.c_int32), ("mx_tiled", C.c_int32), ("mx_max_iter", C.c_int32),
@@ -211,6 +216,8 @@ PROTOTYPES = {
     "lepic_gpu_calc_rhs": (C.c_int, [_VP, _DP]),
     "lepic_gpu_dens_red": (C.c_int, [_VP, _DP, _DP]),
     "lepic_gpu_iterative_solver": (C.c_int, [_VP, _DP, C.c_double, C.c_int32, C.POINTER(LepicSolveStats)]),
+    "lepic_gpu_iterative_solver_async": (C.c_int, [_VP, _DP, _DP, C.c_double, C.c_int32]),
+    "lepic_gpu_get_grid_async": (C.c_int, [_VP, C.c_int32, _DP]),
     "lepic_gpu_calc_efield": (C.c_int, [_VP, _DP]),
     "lepic_gpu_part_sorting": (C.c_int, [_VP, C.c_int32, _IP]),
     "lepic_gpu_collisions": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicMccStats)]),
@@ -239,7 +246,12 @@ PROTOTYPES = {
     "lepic_gpu_read_backup": (C.c_int, [_VP, C.c_char_p, _DP, C.POINTER(C.c_int32), _DP]),
     "lepic_gpu_duplicate_particles": (C.c_int, [_VP, C.c_int32]),
     "lepic_gpu_set_zloss": (C.c_int, [_VP, C.POINTER(LepicZlossConfig)]),
+    "lepic_gpu_set_secondary": (C.c_int, [_VP, C.POINTER(LepicSecondaryConfig)]),
     "lepic_gpu_set_bohm_speed": (C.c_int, [_VP, _DP]),
+    "lepic_gpu_set_dielectrics": (C.c_int, [_VP, _IP, C.c_double]),
+    "lepic_gpu_dielectric_update": (C.c_int, [_VP]),
+    "lepic_gpu_get_dielectric_charge": (C.c_int, [_VP, _DP]),
+    "lepic_gpu_set_dielectric_charge": (C.c_int, [_VP, _DP]),
     "lepic_gpu_set_avg": (C.c_int, [_VP, C.c_int32, C.c_int32]),
     "lepic_gpu_set_regions": (C.c_int, [_VP, C.c_int32, _DP, _DP, C.c_double, C.c_double]),
     "lepic_gpu_get_tallies": (C.c_int, [_VP, C.POINTER(LepicTallies), C.c_int32]),

@@ -36,7 +36,7 @@ SOURCES = {
     "sources.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "backup.cu": [],
-    "zloss.cu": [],
+    "walls.cu": [],
 }
 
 

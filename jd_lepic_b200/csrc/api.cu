@@ -9,7 +9,7 @@
 #include <vector>
 #include "cnn.cuh"
 
-#define LEPIC_ABI_VERSION 3
+#define LEPIC_ABI_VERSION 4
 
 extern "C" int32_t lepic_gpu_abi_version(void) { return LEPIC_ABI_VERSION; }
 
@@ -40,7 +40,7 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
     F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed); F(c->Ef);
-    F(c->ss_diag); F(c->phi_hist); F(c->uB);
+    F(c->ss_diag); F(c->phi_hist); F(c->uB); F(c->dq); F(c->rf_ev); F(c->sec_ev); F(c->ev_count);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
@@ -58,6 +58,10 @@ static void free_all(lepic_ctx *c) {
     F(c->sig_Er); F(c->sig); F(c->Eth); F(c->col_info); F(c->prod_sort);
     F(c->dcnt); F(c->tally); F(c->rg_scratch); F(c->rg_kfac); F(c->sigv_mx_d); F(c->nu_max_d);
     if (c->hcnt) cudaFreeHost(c->hcnt);
+    if (c->cstream) { cudaStreamSynchronize(c->cstream); cudaStreamDestroy(c->cstream); }
+    if (c->ev_snap) cudaEventDestroy(c->ev_snap);
+    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+    F(c->snap);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -364,10 +368,16 @@ extern "C" int lepic_gpu_destroy(lepic_ctx *c) {
 extern "C" void *lepic_gpu_stream(lepic_ctx *c) { return c ? (void *)c->stream : nullptr; }
 extern "C" const char *lepic_gpu_last_error(lepic_ctx *c) { return c ? c->last_err.c_str() : "no context"; }
 
-// Reads the device counters; maps a raised device error to a status (then clears it).
+// Reads the device counters; maps a raised device error to a status (then clears it).  A
+// download still in flight on the copy stream is completed first: every call that
+// synchronises the context leaves the host arrays of the asynchronous downloads filled.
 static int sync_counters(lepic_ctx *c) {
     LCUDA(cudaMemcpyAsync(c->hcnt, c->dcnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, c->stream));
     LCUDA(cudaStreamSynchronize(c->stream));
+    if (c->copy_pending) {
+        LCUDA(cudaEventSynchronize(c->ev_copied));
+        c->copy_pending = 0;
+    }
     int e = c->hcnt->err;
     if (e) {
         int where = c->hcnt->err_where;
@@ -660,11 +670,74 @@ static int solve(lepic_ctx *c, double eps, int mode) {
     return LEPIC_EINVAL;
 }
 
+// An upload from a host array must not overtake a download into the same array that is still
+// in flight: the context's stream waits for the copy stream's last download first.
+static int wait_downloads(lepic_ctx *c) {
+    if (c->copy_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
+    return LEPIC_OK;
+}
+
+// Enqueues the download of `bytes` from the device array `src` into the host array `out`
+// without waiting for it: a device-to-device snapshot on the context's stream (ordered after
+// the work that produced src, ~10 us for a 2049^2 potential), then the device-to-host copy of the
+// snapshot on the copy stream, where it runs beside the kernels enqueued next.  The snapshot is
+// reused by the next download only after this one has completed.
+static int download_async(lepic_ctx *c, void *out, const void *src, size_t bytes) {
+    if (!c->cstream) {
+        LCUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+    }
+    if (c->snap_bytes < bytes) {
+        int r = sync_counters(c);   // no copy may still read the old snapshot
+        if (r != LEPIC_OK) return r;
+        if (c->snap) cudaFree(c->snap);
+        c->snap = nullptr;
+        c->snap_bytes = 0;
+        if (cudaMalloc(&c->snap, bytes) != cudaSuccess) { c->last_err = "download snapshot: cudaMalloc failed"; return LEPIC_ENOMEM; }
+        c->snap_bytes = bytes;
+    }
+    int r = wait_downloads(c);
+    if (r != LEPIC_OK) return r;
+    LCUDA(cudaMemcpyAsync(c->snap, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    LCUDA(cudaEventRecord(c->ev_snap, c->stream));
+    LCUDA(cudaStreamWaitEvent(c->cstream, c->ev_snap, 0));
+    LCUDA(cudaMemcpyAsync(out, c->snap, bytes, cudaMemcpyDeviceToHost, c->cstream));
+    LCUDA(cudaEventRecord(c->ev_copied, c->cstream));
+    c->copy_pending = 1;
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_iterative_solver_async(lepic_ctx *c, const double *phi_in, double *phi_out, double eps,
+                                                int32_t mode) {
+    if (!c || !(eps > 0)) return LEPIC_EINVAL;
+    int r;
+    if (phi_in) {
+        if ((r = wait_downloads(c)) != LEPIC_OK) return r;
+        LCUDA(cudaMemcpyAsync(c->phi, phi_in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
+    }
+    if ((r = solve(c, eps, mode)) != LEPIC_OK) return r;
+    if (phi_out) return download_async(c, phi_out, c->phi, sizeof(double) * c->nn);
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_get_grid_async(lepic_ctx *c, int32_t which, double *out) {
+    if (!c || !out) return LEPIC_EINVAL;
+    if (which == LEPIC_GRID_PHI) return download_async(c, out, c->phi, sizeof(double) * c->nn);
+    if (which == LEPIC_GRID_RHS)
+        return download_async(c, out, c->rhs, sizeof(double) * (c->cfg.nx + 1) * (c->cfg.ny + 1));
+    if (which == LEPIC_GRID_EI) return download_async(c, out, c->Ed, sizeof(double2) * c->nn);
+    return LEPIC_EINVAL;
+}
+
 extern "C" int lepic_gpu_iterative_solver(lepic_ctx *c, double *phi_inout, double eps, int32_t mode,
                                           lepic_solve_stats *st) {
     if (!c || !(eps > 0)) return LEPIC_EINVAL;
-    if (phi_inout)
+    if (phi_inout) {
+        int r = wait_downloads(c);
+        if (r != LEPIC_OK) return r;
         LCUDA(cudaMemcpyAsync(c->phi, phi_inout, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
+    }
     int r = solve(c, eps, mode);
     if (r != LEPIC_OK) return r;
     if (phi_inout)
@@ -726,6 +799,7 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
     if (!c) return LEPIC_EINVAL;
     const lepic_config &g = c->cfg;
     int r;
+    if (c->dq && (r = dielectric_update(c)) != LEPIC_OK) return r;   // main.f90:756-809
     if ((r = field_calc_rhs(c)) != LEPIC_OK) return r;
     if ((r = solve(c, eps, mode)) != LEPIC_OK) return r;
     if ((r = field_calc_efield(c)) != LEPIC_OK) return r;
@@ -776,6 +850,7 @@ extern "C" int lepic_gpu_set_warm_start(lepic_ctx *c, int32_t mode) {
 
 extern "C" int lepic_gpu_set_grid(lepic_ctx *c, int32_t which, const double *in) {
     if (!c || !in) return LEPIC_EINVAL;
+    if (wait_downloads(c) != LEPIC_OK) return LEPIC_ECUDA;
     if (which == LEPIC_GRID_PHI) {
         LCUDA(cudaMemcpyAsync(c->phi, in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
         c->have_hist = 0;   // a potential from elsewhere: the next solve starts from it as it is

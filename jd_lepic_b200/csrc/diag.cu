@@ -392,10 +392,10 @@ extern "C" int lepic_gpu_get_tallies(lepic_ctx *c, lepic_tallies *out, int32_t r
             out->P_w[s][l] = Ek * h->v2_loss[s][l];
             lost += out->P_w[s][l];
         }
-        out->P_loss[0][s] = lost + P_src[s] + h->P1z[s];
+        out->P_loss[0][s] = lost + P_src[s] + h->P1z[s] + h->P1r[s];
         out->P_loss[1][s] = s == 0 ? P_heat : 0.0;
         out->P_loss[2][s] = h->P3[s];
-        out->P_loss[3][s] = P_inj[s];
+        out->P_loss[3][s] = P_inj[s] + h->P4r[s];
     }
     memcpy(out->cnt_col, h->cnt_col, sizeof(out->cnt_col));
     out->n_rg = c->n_rg;

@@ -37,6 +37,15 @@ struct Product {            // a particle created by a collision, before its ord
     float z;                // the parent's z (collisions.f90:813; 0 without the 3rd dimension)
 };
 
+// A wall event the push records for a follow-up kernel (push.cu): refluxing (a = the fixed-point
+// x <= 0 the move reached, (u, v, w) = the velocity before) or secondary emission (a = the
+// fixed-point y of the ion's loss point, u = the ion's vx, w = its z there).
+struct WallEvent {
+    int slot;
+    int a;
+    float u, v, w;
+};
+
 struct DevCounters {
     long long n_slots[LEPIC_MAXSP];    // occupied slots (sorted region + appended tail)
     long long n_sorted[LEPIC_MAXSP];   // end of the region the work list covers
@@ -49,6 +58,7 @@ struct DevCounters {
     int n_items[LEPIC_MAXSP];
     unsigned int prod_count[LEPIC_MAXSP]; // products waiting for the ordered append
     int n_big;                            // sort: segments too long for one warp
+    unsigned int scatter_next;            // sort: the scatter's work-unit dispenser
     unsigned int n_cand_list;             // collisions: candidates of the species being treated
     int err;
     int err_where;
@@ -67,6 +77,8 @@ struct TallyDev {
     double P3[LEPIC_MAXSP];                           // collisions' energy change [J]
     double cnt_col[3][LEPIC_MAXCOL][LEPIC_MAXRG];
     double P1z[LEPIC_MAXSP];                          // P_loss(1)'s Nm q phi of 3rd-dimension losses [J]
+    double P1r[LEPIC_MAXSP];                          // P_loss(1): refluxed particles' energy before [J]
+    double P4r[LEPIC_MAXSP];                          // P_loss(4): refluxed and secondary particles' energy [J]
     double inv_np_rg[LEPIC_MAXSP][LEPIC_MAXRG];       // 1/np_tot_rg of the current collision step
 };
 
@@ -123,6 +135,13 @@ struct lepic_ctx {
     lepic_options opt;         // solver settings (lepic_gpu_set_options), defaults at create
     int dev = 0, num_sms = 0;
     cudaStream_t stream = nullptr;
+    // downloads overlapped with the following work (lepic_gpu_iterative_solver_async,
+    // lepic_gpu_get_grid_async): a device snapshot of the grid, copied to the host on cstream
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_copied = nullptr;
+    void *snap = nullptr;
+    size_t snap_bytes = 0;
+    int copy_pending = 0;
     int S = 0;                 // fractional bits of the fixed-point positions
     long long nn = 0;          // nodes (nx+3)(ny+3)
     int tw = 0, th = 0, ntx = 0, nty = 0, ntiles = 0;
@@ -188,6 +207,20 @@ struct lepic_ctx {
     double hz = 0.0, phi0_end = 0.0;
     int za1 = 0, za2 = 0, zsize_na = 1;   // the uB grid: na = n / size_na, (na1+1)(na2+1) nodes
     float *uB = nullptr;                  // [ptype][(na1+1)(na2+1)], m/s
+    // dielectric walls (part_expmover.f90:340-350, main.f90:756-809): per wall label its type
+    // (1: dielectric), the capacitance Ca [F/m^2], and the charge collected per label and row
+    // since the last update, dq[label][0..ny+2] (null: no dielectrics)
+    int32_t dtype[LEPIC_MAXLABEL] = {0};
+    // secondary emission by positive ions (lepic_gpu_set_secondary): label, coefficient,
+    // the emitting grid's x [m] and the electrons' temperature [eV]
+    int sec_label = 0;
+    double sec_gam = 0.0, sec_xg = 0.0, sec_THm = 0.0;
+    // the push's wall events (refluxing, emission) and their counts, allocated when first needed
+    WallEvent *rf_ev = nullptr, *sec_ev = nullptr;
+    unsigned int *ev_count = nullptr;
+    int ev_cap = 0;
+    double Ca = 0.0;
+    double *dq = nullptr;
     // particle sources (sources.cu), created by lepic_gpu_set_sources
     void *src = nullptr;
     // averaging diagnostics (diag.cu), created by lepic_gpu_set_avg
@@ -234,6 +267,16 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
     return c;
 }
 __device__ __forceinline__ double u01(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
+
+// load_gauss.f90:16-39 from two counter draws: vp = vt sqrt(-ln(1-r1)), th = 2 pi r2
+__device__ __forceinline__ void gauss_pair(double vt, uint32_t a, uint32_t b, double *x, double *y) {
+    const double pi = 3.141592653589793;
+    const double vp = vt * sqrt(-log(1.0 - u01(a)));
+    double s, co;
+    sincos(2.0 * pi * u01(b), &s, &co);
+    *x = vp * co;
+    *y = vp * s;
+}
 
 // 32-bit integer mix (MurmurHash3 finaliser), used for the stochastic rounding of moves.
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
@@ -343,8 +386,17 @@ int field_np_grid(lepic_ctx *c, int ptype, double *d_out);
 int mg_solve(lepic_ctx *c, double eps, int mode);
 int mg_init(lepic_ctx *c);
 int mg_residual_stats(lepic_ctx *c);
-// the Bohm speed map of the 3rd-dimension model from an averaging sample (zloss.cu)
+// the Bohm speed map of the 3rd-dimension model from an averaging sample (walls.cu)
 int zloss_after_avg(lepic_ctx *c, const double *data, int na1, int na2, int size_na, int cnt);
+// refluxing at x = 0 (sources.cu): true when the sources' opt_inj is +-4 and the Neumann option
+// is on; then the species' shifted-flux parameters (part_injection.f90:34-47, :267-290)
+bool sources_reflux(const lepic_ctx *c, int sp, double *vb, double *fmax, double *vt, double *sin_thB,
+                    double *cos_thB);
+// the ordered append of a species' waiting products (mcc.cu); mcc: count them as collision
+// products (n_add)
+int commit_products(lepic_ctx *c, int sp, bool mcc);
+// the dielectric walls' potential from the charge they collected (walls.cu, main.f90:756-809)
+int dielectric_update(lepic_ctx *c);
 // xtrap: the warm start may extrapolate; fp64: the V-cycle in FP64 (mode 4) instead of FP32
 int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap, bool fp64 = false);
 int push_deposit(lepic_ctx *c, int it, bool move);

@@ -531,7 +531,7 @@ __global__ void k_nu_max(NuMaxP P) {
 // Ordered append of one species' products after its occupied slots (single CTA).
 __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long long *sortbuf,
                              uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, float *Z, long long cap,
-                             DevCounters *cnt) {
+                             DevCounters *cnt, int mcc) {
     __shared__ unsigned long long sm[4096];
     int n = (int)min(cnt->prod_count[sp], (unsigned int)prod_cap);
     if (n == 0) return;
@@ -555,7 +555,7 @@ __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long 
     if (threadIdx.x == 0) {
         cnt->n_slots[sp] = base + m;
         cnt->n_alive[sp] += m;
-        cnt->n_add[sp] += (unsigned long long)m;
+        if (mcc) cnt->n_add[sp] += (unsigned long long)m;
         cnt->prod_count[sp] = 0;
     }
 }
@@ -703,10 +703,17 @@ int mcc_collide(lepic_ctx *c, int it, bool diag) {
     }
     if (diag) return LEPIC_OK;
     for (int t = 0; t < g.ntype; t++) {
-        SpeciesBuf &B = c->sp[t];
-        k_mcc_commit<<<1, 1024, 0, c->stream>>>(t, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],
-                                                B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.Z[B.cur], B.cap, c->dcnt);
-        LCUDA(cudaGetLastError());
+        int r = commit_products(c, t, true);
+        if (r != LEPIC_OK) return r;
     }
+    return LEPIC_OK;
+}
+
+int commit_products(lepic_ctx *c, int sp, bool mcc) {
+    SpeciesBuf &B = c->sp[sp];
+    k_mcc_commit<<<1, 1024, 0, c->stream>>>(sp, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],
+                                            B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.Z[B.cur], B.cap, c->dcnt,
+                                            mcc ? 1 : 0);
+    LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }

@@ -46,7 +46,7 @@ struct PushP {
     uint32_t step_key;
     int tw, th, ntx, M, WX, WY, win;
     long long xlim, ylim;      // nx<<S, ny<<S
-    // the 3rd dimension (zloss.cu): z per slot, its length, the end plates' potential and
+    // the 3rd dimension (walls.cu): z per slot, its length, the end plates' potential and
     // phi for the electrons' test, the ions' loss factor hz 2 dt / zmax and the uB map
     float *Z;                  // null: no 3rd-dimension model
     int zneg, za1, zsize;
@@ -56,23 +56,54 @@ struct PushP {
     const float *uB;
     TallyDev *tal;
     uint32_t zk0, zk1, it;
+    // dielectric walls: the charge a wall loss leaves on its label's rows (null: none)
+    double *dq;
+    const int32_t *bcnd;
+    int32_t dtype[LEPIC_MAXLABEL];
+    // refluxing at x = 0 (opt_inj = +-4 with the Neumann option) and secondary emission by
+    // positive ions on one wall label: the push only records the event (k_reflux and
+    // k_sec_emit below do the draws after the species' push)
+    int reflux, sec_label;
+    WallEvent *rf_ev, *sec_ev;
+    unsigned int *ev_count;    // [0] reflux events, [1] emission events
+    int ev_cap;
 };
+
+#define TAG_SECN 0x5345434Eu      // secondary emission: the number of electrons
+#define TAG_SECV 0x53454356u      // secondary emission: one electron's velocity
+#define TAG_RFX 0x52465831u       // refluxing: flux attempt
+#define TAG_RFX2 0x52465832u      // refluxing: the position draw of an attempt
+#define REFLUX_MAX_ATTEMPTS 4096
 
 #define PUSH_G 4    // consecutive slots per thread: one 16-byte vector per array
 
 // CIC weights of one particle: exact integer products of the fixed-point offsets, scaled to
 // 2^LEPIC_DEP_SHIFT, for (ix,iy) (ix+1,iy) (ix+1,iy+1) (ix,iy+1)
-__device__ __forceinline__ void cic_weights(const PushP &P, uint32_t X, uint32_t Y, uint64_t *w) {
-    const uint32_t mask = (1u << P.S) - 1u;
-    const uint32_t A = 1u << P.S;
+__device__ __forceinline__ void cic_weights_s(int S, uint32_t X, uint32_t Y, uint64_t *w) {
+    const uint32_t mask = (1u << S) - 1u;
+    const uint32_t A = 1u << S;
     const uint32_t fx = X & mask, fy = Y & mask, ax = A - fx, ay = A - fy;
     w[0] = (uint64_t)ax * ay; w[1] = (uint64_t)fx * ay; w[2] = (uint64_t)fx * fy; w[3] = (uint64_t)ax * fy;
-    const int sh = 2 * P.S - LEPIC_DEP_SHIFT;
+    const int sh = 2 * S - LEPIC_DEP_SHIFT;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if (sh > 0) w[k] = (w[k] + (1ull << (sh - 1))) >> sh;
         else if (sh < 0) w[k] <<= -sh;
     }
+}
+__device__ __forceinline__ void cic_weights(const PushP &P, uint32_t X, uint32_t Y, uint64_t *w) {
+    cic_weights_s(P.S, X, Y, w);
+}
+
+// one particle's weights added to the global accumulators of its cell's four nodes
+__device__ __forceinline__ void deposit_global(unsigned long long *acc, int S, int W, uint32_t X, uint32_t Y) {
+    uint64_t w[4];
+    cic_weights_s(S, X, Y, w);
+    unsigned long long *q = acc + ((X >> S) + 1) + (long long)((Y >> S) + 1) * W;
+    atomicAdd(q, (unsigned long long)w[0]);
+    atomicAdd(q + 1, (unsigned long long)w[1]);
+    atomicAdd(q + W + 1, (unsigned long long)w[2]);
+    atomicAdd(q + W, (unsigned long long)w[3]);
 }
 
 // The node weights of a run from its moments: n particles with offsets fx, fy summed as
@@ -230,6 +261,26 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
             const int iyw = min(max((int)((Yn + hf) >> P.S) + 1, 0), P.ny + 1);
             atomicAdd(P.ss_sink + ixw + (long long)iyw * P.W, 1u);
         }
+        if (GEN && P.dq && P.cellwall[ixn + iyn * (P.nx + 2)] != 0) {
+            // dielectric charging (part_expmover.f90:340-350): Nm q split by the loss point's y
+            // between the rows iy and iy+1 of the loss cell's label, when that label or the
+            // one above is a dielectric
+            const int lab = min(max(P.bcnd[ixn + iyn * P.W], 0), LEPIC_MAXLABEL - 1);
+            const int up = min(max(P.bcnd[ixn + (iyn + 1) * P.W], 0), LEPIC_MAXLABEL - 1);
+            if (max(P.dtype[lab], P.dtype[up]) == 1) {
+                const double py = (double)iyn - (double)Yn * (double)P.inv2S;   // (iy h - y)/h
+                double *row = P.dq + (long long)lab * (P.ny + 3);
+                atomicAdd(row + iyn, P.nmq * py);
+                atomicAdd(row + iyn + 1, P.nmq * (1.0 - py));
+            }
+        }
+        if (GEN && P.sec_label && P.cellwall[ixn + iyn * (P.nx + 2)] != 0 && P.bcnd[ixn + iyn * P.W] == P.sec_label) {
+            // secondary emission: the event, drawn by k_sec_emit after this push
+            const unsigned int e = atomicAdd(P.ev_count + 1, 1u);
+            if (e < (unsigned int)P.ev_cap)
+                P.sec_ev[e] = WallEvent{i, (int)min(max(Yn, 0ll), P.ylim - 1), ux0, uy0, P.Z ? P.Z[i] + P.dtf * uz0 : 0.0f};
+            else set_err(cnt, LERR_CAPACITY, 102);
+        }
         // the slot becomes a hole that keeps its loss for the tallies (lepic_internal.cuh,
         // loss_hole_tally): X = the loss cell's node, Y = the new vx, VY, VZ = the new vy, vz,
         // VX = a NaN whose payload marks a fresh wall loss (1) or another loss (2)
@@ -240,7 +291,22 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         vx = __int_as_float(wall ? LOSS_NAN_WALL : LOSS_NAN_OTHER);
         return false;
     }
-    if (GEN && P.nmn && Xn <= 0) { Xn = -Xn; ux0 = -ux0; } // :454-459
+    if (GEN && P.nmn && Xn <= 0) { // :454-459 specular reflection, or :445-470 refluxing
+        if (P.reflux) {
+            // the event (slot, x <= 0, the velocity before) for k_reflux, which draws the new
+            // state, writes it and deposits it: the particle is stored as it is and not deposited
+            const unsigned int e = atomicAdd(P.ev_count, 1u);
+            if (e < (unsigned int)P.ev_cap) {
+                P.rf_ev[e] = WallEvent{i, (int)max(Xn, -2147483647ll), ux0, uy0, uz0};
+                X = 0u;
+                Y = (uint32_t)min(max(Yn, 0ll), P.ylim - 1);
+                vx = ux0; vy = uy0; vz = uz0;
+                return false;
+            }
+            set_err(cnt, LERR_CAPACITY, 103);
+        }
+        Xn = -Xn; ux0 = -ux0;
+    }
     if (Xn < 0 || Xn >= P.xlim || Yn < 0 || Yn >= P.ylim) {
         set_err(cnt, LERR_RANGE, 100);
         Xn = min(max(Xn, 0ll), P.xlim - 1);
@@ -484,12 +550,146 @@ static int launch_b(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
                                       : launch_m<BMODE, false>(c, P, smem, gen, move);
 }
 
+// Refluxing (part_expmover.f90:445-470), one thread per event of this species' push: vx from
+// the shifted-Maxwellian flux about vb cos(th_B) by acceptance-rejection against fmax
+// (shifted_maxwellian_flux, part_injection.f90:239-265), (vy, vz) from load_gauss with
+// vy += vb sin(th_B), x = vx r dt; an attempt whose x falls outside [0, xmax] is drawn again.
+// The draws come from the counter stream keyed by (slot, attempt, species, step).  P_loss(1)
+// takes 0.5 Nm m v^2 before, P_loss(4) after; the particle is written and deposited.  With the
+// 3rd dimension its z moves by dt vz (its end-plate test is not taken in this step).  If no
+// attempt is kept the particle is reflected as without refluxing and the call reports ERANGE.
+struct RefluxP {
+    const WallEvent *ev;
+    const unsigned int *count;
+    int cap, sp, S, W;
+    uint32_t *X;
+    const uint32_t *Y;
+    float *VX, *VY, *VZ, *Z;
+    unsigned long long *acc;
+    TallyDev *tal;
+    DevCounters *cnt;
+    double vbx, vby, vt, fmax, dt, xmax, sx, ekf;
+    float dtf;
+    long long xlim;
+    uint32_t k0, k1, it;
+};
+
+__global__ void k_reflux(RefluxP R) {
+    const int n = (int)min(*R.count, (unsigned int)R.cap);
+    const double vm = fmax(0.0, R.vbx - 4.0 * R.vt), vp = R.vbx + 4.0 * R.vt;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const WallEvent E = R.ev[e];
+        const int i = E.slot;
+        double ux = E.u, uy = E.v, uz = E.w;
+        long long Xn = -(long long)E.a;       // the specular reflection, if no attempt is kept
+        bool got = false;
+        for (uint32_t a = 0; a < REFLUX_MAX_ATTEMPTS && !got; a++) {
+            const uint32_t c1 = (a << 3) | (uint32_t)R.sp;
+            const U4 f = philox4x32_10(U4{(uint32_t)i, c1, TAG_RFX, R.it}, R.k0, R.k1);
+            const double v = vm + u01(f.x) * (vp - vm);
+            const double fv = v * exp(-(v - R.vbx) * (v - R.vbx) / (R.vt * R.vt));
+            if (u01(f.y) > fv / R.fmax) continue;
+            double vy, vz;
+            gauss_pair(R.vt, f.z, f.w, &vy, &vz);
+            vy += R.vby;
+            const U4 g = philox4x32_10(U4{(uint32_t)i, c1, TAG_RFX2, R.it}, R.k0, R.k1);
+            const double x = v * (u01(g.x) * R.dt);
+            if (x < 0.0 || x > R.xmax) continue;
+            atomicAdd(&R.tal->P1r[R.sp], R.ekf * (ux * ux + uy * uy + uz * uz));
+            atomicAdd(&R.tal->P4r[R.sp], R.ekf * (v * v + vy * vy + vz * vz));
+            Xn = min((long long)(x * R.sx), R.xlim - 1);   // truncation: the cell is INT(x/h)
+            ux = v; uy = vy; uz = vz;
+            got = true;
+        }
+        if (!got) {
+            set_err(R.cnt, LERR_RANGE, 104);
+            Xn = min(Xn, R.xlim - 1);
+            ux = -ux;
+        }
+        const uint32_t X = (uint32_t)Xn;
+        R.X[i] = X;
+        R.VX[i] = (float)ux; R.VY[i] = (float)uy; R.VZ[i] = (float)uz;
+        if (R.Z) R.Z[i] = R.Z[i] + R.dtf * E.w;
+        deposit_global(R.acc, R.S, R.W, X, R.Y[i]);   // the deposit the push left out
+    }
+}
+
+// Secondary emission (part_expmover.f90:354-392), one thread per event of a positive ion
+// species' push: INT(gam) electrons, one more with probability gam - INT(gam), at
+// (xg_sec, y, z) of the loss point with vx = -SIGN(1, vx_ion) vt sqrt(-ln(1-r)) and (vy, vz)
+// from load_gauss at the emission temperature; each adds 0.5 Nm m (vx^2 + vz^2 + vz^2) to the
+// electrons' P_loss(4) (the reference's sum: vz taken twice, vy not).  The draws come from the
+// counter stream keyed by (slot, step, species, electron); the electrons wait in the electrons'
+// product list (key slot * 8 + k) for the ordered append after the push and are deposited now:
+// they are in this step's density, as in the reference, where the deposition follows the movers.
+struct SecP {
+    const WallEvent *ev;
+    const unsigned int *count;
+    int cap, sp, S, W;
+    double gam, vt, ekf0;
+    uint32_t X;
+    Product *prod;
+    unsigned int *prod_count;
+    int prod_cap;
+    unsigned long long *acc0;
+    TallyDev *tal;
+    DevCounters *cnt;
+    uint32_t k0, k1, it;
+};
+
+__global__ void k_sec_emit(SecP Q) {
+    const int n = (int)min(*Q.count, (unsigned int)Q.cap);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const WallEvent E = Q.ev[e];
+        const int i = E.slot;
+        const U4 r = philox4x32_10(U4{(uint32_t)i, Q.it, TAG_SECN, (uint32_t)Q.sp}, Q.k0, Q.k1);
+        int m = (int)Q.gam;
+        if (u01(r.x) <= Q.gam - (double)m) m++;
+        if (m == 0) continue;
+        const unsigned int base = atomicAdd(Q.prod_count, (unsigned int)m);
+        const uint32_t Y = (uint32_t)E.a;
+        const double sgn = E.u >= 0.0f ? 1.0 : -1.0;
+        for (int k = 0; k < m; k++) {
+            const U4 v = philox4x32_10(U4{(uint32_t)i, Q.it, TAG_SECV, ((uint32_t)Q.sp << 8) | (uint32_t)k}, Q.k0, Q.k1);
+            const double vx = -sgn * Q.vt * sqrt(-log(1.0 - u01(v.x)));
+            double vy, vz;
+            gauss_pair(Q.vt, v.y, v.z, &vy, &vz);
+            if (base + k >= (unsigned int)Q.prod_cap) { set_err(Q.cnt, LERR_CAPACITY, 105); continue; }
+            atomicAdd(&Q.tal->P4r[0], Q.ekf0 * (vx * vx + vz * vz + vz * vz));
+            Product pr;
+            pr.key = (unsigned long long)i * 8ull + (unsigned long long)k;
+            pr.X = Q.X; pr.Y = Y;
+            pr.vx = (float)vx; pr.vy = (float)vy; pr.vz = (float)vz;
+            pr.z = E.w;
+            Q.prod[base + k] = pr;
+            deposit_global(Q.acc0, Q.S, Q.W, Q.X, Y);
+        }
+    }
+}
+
+// the event lists of the push, allocated when a wall model first needs them
+static int wall_events(lepic_ctx *c) {
+    if (c->ev_count) return LEPIC_OK;
+    long long cap = 65536;
+    for (int s = 0; s < c->cfg.ntype; s++) cap = std::max(cap, c->sp[s].cap / 64);
+    cap = std::min(cap, (long long)1 << 26);
+    if (cudaMalloc((void **)&c->rf_ev, sizeof(WallEvent) * cap) != cudaSuccess ||
+        cudaMalloc((void **)&c->sec_ev, sizeof(WallEvent) * cap) != cudaSuccess ||
+        cudaMalloc((void **)&c->ev_count, 2 * sizeof(unsigned int)) != cudaSuccess) {
+        c->last_err = "wall events: cudaMalloc failed";
+        return LEPIC_ENOMEM;
+    }
+    c->ev_cap = (int)cap;
+    return LEPIC_OK;
+}
+
 int push_deposit(lepic_ctx *c, int it, bool move) {
     const lepic_config &g = c->cfg;
     for (int s = 0; s < g.ntype; s++)
         LCUDA(cudaMemsetAsync(c->sp[s].acc, 0, sizeof(unsigned long long) * c->nn, c->stream));
     LCUDA(cudaMemsetAsync(c->dcnt->work_next, 0, sizeof(c->dcnt->work_next), c->stream));
     const double amu = 1.66053886e-27;
+    bool any_sec = false;
     for (int s = 0; s < g.ntype; s++) {
         SpeciesBuf &B = c->sp[s];
         PushP P;
@@ -529,6 +729,44 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         if (!P.win) smem = 0;
         P.xlim = (long long)g.nx << c->S;
         P.ylim = (long long)g.ny << c->S;
+        P.nmq = g.Nm[s] * g.charge[s];
+        P.bcnd = c->bcnd;
+        P.tal = c->tally;
+        P.zk0 = (uint32_t)g.seed; P.zk1 = (uint32_t)(g.seed >> 32) ^ 0x5A10C5u;
+        P.it = (uint32_t)it;
+        if (c->dq) {
+            P.dq = c->dq;
+            for (int l = 0; l < LEPIC_MAXLABEL; l++) P.dtype[l] = c->dtype[l];
+        }
+        // refluxing and secondary emission: the push records events, drawn after it
+        RefluxP R;
+        memset(&R, 0, sizeof(R));
+        SecP Q;
+        memset(&Q, 0, sizeof(Q));
+        {
+            double vb, fm, vt, sn, cs;
+            if (move && sources_reflux(c, s, &vb, &fm, &vt, &sn, &cs)) {
+                P.reflux = 1;
+                R.vbx = vb * cs; R.vby = vb * sn; R.vt = vt; R.fmax = fm;
+                R.dt = g.dt; R.xmax = g.nx * g.dx; R.sx = (double)(1u << c->S) / g.dx;
+                R.ekf = 0.5 * g.Nm[s] * g.mass[s];
+            }
+        }
+        if (move && c->sec_label > 0 && c->sec_gam > 0.0 && g.charge[s] > 0.0) {
+            P.sec_label = c->sec_label;
+            Q.gam = c->sec_gam;
+            Q.vt = std::sqrt(2.0 * g.qe * std::fabs(c->sec_THm) / std::fabs(g.mass[0]));
+            Q.ekf0 = 0.5 * g.Nm[0] * g.mass[0];
+            Q.X = (uint32_t)std::min<long long>((long long)(c->sec_xg / g.dx * (double)(1u << c->S)),
+                                                ((long long)g.nx << c->S) - 1);
+            any_sec = true;
+        }
+        if (P.reflux || P.sec_label) {
+            int r = wall_events(c);
+            if (r != LEPIC_OK) return r;
+            LCUDA(cudaMemsetAsync(c->ev_count, 0, 2 * sizeof(unsigned int), c->stream));
+            P.rf_ev = c->rf_ev; P.sec_ev = c->sec_ev; P.ev_count = c->ev_count; P.ev_cap = c->ev_cap;
+        }
         if (c->zloss && B.Z[0]) {
             P.Z = B.Z[B.cur];
             P.zneg = g.charge[s] < 0.0 ? 1 : 0;
@@ -538,20 +776,35 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
             P.nu_fac = (float)(c->hz * 2.0 / g.zmax * g.dt);
             P.phi0 = c->phi0_end;
             P.m_over_2qe = 0.5 * g.mass[s] / g.qe;
-            P.nmq = g.Nm[s] * g.charge[s];
             P.phi = c->phi;
             P.uB = c->uB + (size_t)s * (c->za1 + 1) * (c->za2 + 1);
-            P.tal = c->tally;
-            P.zk0 = (uint32_t)g.seed; P.zk1 = (uint32_t)(g.seed >> 32) ^ 0x5A10C5u;
-            P.it = (uint32_t)it;
         }
-        // the boundary options and the 3rd dimension take the general mover for every particle
-        const bool gen = P.pbc || P.nmn || P.negion_nmn || P.Z;
+        // the boundary options, the 3rd dimension and the wall models take the general mover
+        const bool gen = P.pbc || P.nmn || P.negion_nmn || P.Z || P.dq || P.reflux || P.sec_label;
         int r;
         if (bmode == 1) r = launch_b<1>(c, P, smem, gen, move);
         else if (bmode == 2) r = launch_b<2>(c, P, smem, gen, move);
         else r = launch_b<0>(c, P, smem, gen, move);
         if (r != LEPIC_OK) return r;
+        const int eg = c->num_sms * 2;
+        if (P.reflux) {
+            R.ev = c->rf_ev; R.count = c->ev_count; R.cap = c->ev_cap; R.sp = s; R.S = c->S; R.W = P.W;
+            R.X = P.X; R.Y = P.Y; R.VX = P.VX; R.VY = P.VY; R.VZ = P.VZ; R.Z = P.Z; R.acc = B.acc;
+            R.tal = c->tally; R.cnt = c->dcnt; R.dtf = (float)g.dt; R.xlim = P.xlim;
+            R.k0 = P.zk0; R.k1 = P.zk1; R.it = P.it;
+            k_reflux<<<eg, 128, 0, c->stream>>>(R);
+            LCUDA(cudaGetLastError());
+        }
+        if (P.sec_label) {
+            SpeciesBuf &E = c->sp[0];
+            Q.ev = c->sec_ev; Q.count = c->ev_count + 1; Q.cap = c->ev_cap; Q.sp = s; Q.S = c->S; Q.W = P.W;
+            Q.prod = E.prod; Q.prod_count = &c->dcnt->prod_count[0]; Q.prod_cap = E.prod_cap; Q.acc0 = E.acc;
+            Q.tal = c->tally; Q.cnt = c->dcnt; Q.k0 = P.zk0; Q.k1 = P.zk1; Q.it = P.it;
+            k_sec_emit<<<eg, 128, 0, c->stream>>>(Q);
+            LCUDA(cudaGetLastError());
+        }
     }
+    // the secondary electrons of this push, appended in the order of their ions' slots
+    if (any_sec) return commit_products(c, 0, false);
     return LEPIC_OK;
 }

@@ -127,16 +127,6 @@ static Region make_region(const lepic_source_config &s, const lepic_config &g, i
 
 static SrcState *state(lepic_ctx *c) { return (SrcState *)c->src; }
 
-__device__ __forceinline__ void gauss_pair(double vt, uint32_t a, uint32_t b, double *x, double *y) {
-    // load_gauss.f90:16-39: vp = vt sqrt(-ln(1-r1)), th = 2 pi r2
-    const double pi = 3.141592653589793;
-    const double vp = vt * sqrt(-log(1.0 - u01(a)));
-    double s, co;
-    sincos(2.0 * pi * u01(b), &s, &co);
-    *x = vp * co;
-    *y = vp * s;
-}
-
 // one CTA's sums of NV values per thread (in shared memory, column = thread), reduced by a
 // fixed tree and written to the CTA's partial row
 template <int NT>
@@ -1145,4 +1135,23 @@ int sources_reset_power(lepic_ctx *c) {
     LCUDA(cudaMemsetAsync(&S->d->P_heat, 0, sizeof(double), c->stream));
     LCUDA(cudaMemsetAsync(S->d->P_inj, 0, sizeof(double) * 2 * LEPIC_MAXSP, c->stream));  // P_inj, P_src
     return LEPIC_OK;
+}
+
+bool sources_reflux(const lepic_ctx *c, int sp, double *vb, double *fmax, double *vt, double *sin_thB,
+                    double *cos_thB) {
+    const SrcState *S = (const SrcState *)c->src;
+    const lepic_config &g = c->cfg;
+    if (!S || std::abs(S->cfg.opt_inj) != 4 || g.flag_nmn != 1) return false;
+    // part_injection.f90:34-47 (electrons: a half-Maxwellian flux with the Neumann option) and
+    // init_shifted_maxwellian_flux (:267-290)
+    double b = std::sqrt(2.0 * g.qe * S->cfg.THm / std::fabs(g.mass[sp]));
+    if (sp == 0) b = 0.0;
+    const double v0 = g.vt0[sp];
+    const double vmax = (b + std::sqrt(b * b + 2.0 * v0 * v0)) / 2.0;
+    *vb = b;
+    *fmax = vmax * std::exp(-(vmax - b) * (vmax - b) / (v0 * v0));
+    *vt = v0;
+    *sin_thB = std::sin(S->cfg.th_B);
+    *cos_thB = std::cos(S->cfg.th_B);
+    return true;
 }

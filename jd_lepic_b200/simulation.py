@@ -298,6 +298,29 @@ class GpuSimulation:
         a = np.ascontiguousarray(uB, dtype=np.float64)
         self.check(self.lib.lepic_gpu_set_bohm_speed(self.ctx, _dp(a)), "set_bohm_speed")
 
+    def set_secondary(self, gam_sec: float, igrid_sec: int, xg_sec: float, THm: float):
+        """Secondary electrons from positive ions lost on wall label igrid_sec
+        (part_expmover.f90:354-392); gam_sec = 0 switches it off."""
+        q = capi.LepicSecondaryConfig(gam_sec, igrid_sec, 0, xg_sec, THm)
+        self.check(self.lib.lepic_gpu_set_secondary(self.ctx, C.byref(q)), "set_secondary")
+
+    def set_dielectrics(self, dtype, Ca: float):
+        """Dielectric wall labels (dtype[label] = 1; part_expmover.f90:340-350, main.f90:756-809)
+        and their capacitance Ca [F/m^2]; all zeros switch the model off."""
+        d = np.zeros(capi.MAXLABEL, dtype=np.int32)
+        d[:len(dtype)] = dtype
+        self.check(self.lib.lepic_gpu_set_dielectrics(self.ctx, d.ctypes.data_as(C.POINTER(C.c_int32)), Ca),
+                   "set_dielectrics")
+
+    def dielectric_update(self):
+        self.check(self.lib.lepic_gpu_dielectric_update(self.ctx), "dielectric_update")
+
+    def dielectric_charge(self) -> np.ndarray:
+        """The charge collected on the dielectric labels since the last update: (MAXLABEL, ny+3) [C]."""
+        q = np.zeros((capi.MAXLABEL, self.case.ny + 3))
+        self.check(self.lib.lepic_gpu_get_dielectric_charge(self.ctx, _dp(q)), "get_dielectric_charge")
+        return q
+
     def options(self) -> capi.LepicOptions:
         o = capi.LepicOptions()
         self.check(self.lib.lepic_gpu_get_options(self.ctx, C.byref(o)), "get_options")

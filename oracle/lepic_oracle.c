@@ -58,6 +58,25 @@ void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
 void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
                     const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
                     o_push_tally *t, const o_zloss *zl) {
+    o_part_mover_zd(c, ptype, Ei, Bi, bcnd, vxp, np_tot, flag_dead, t, zl, NULL);
+}
+
+static int o_label(int l) { return l < 0 ? 0 : (l > 15 ? 15 : l); }
+
+void o_part_mover_zd(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                     const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                     o_push_tally *t, const o_zloss *zl, const o_dielec *dl) {
+    o_part_mover_x(c, ptype, Ei, Bi, bcnd, vxp, np_tot, flag_dead, t, zl, dl, NULL);
+}
+
+#define O_TAG_SECN 0x5345434Eu
+#define O_TAG_SECV 0x53454356u
+#define O_TAG_RFX 0x52465831u
+#define O_TAG_RFX2 0x52465832u
+
+void o_part_mover_x(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                    const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                    o_push_tally *t, const o_zloss *zl, const o_dielec *dl, o_wallx *wx) {
     const int nx = c->nx, ny = c->ny;
     const double h1 = c->dx, h2 = c->dy, dt = c->dt;
     const double amu = 1.66053886e-27;
@@ -168,6 +187,40 @@ void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *B
         }
         if (flag_lost >= 1) { /* :314-427 */
             np_lost++;
+            if (dl && flag_lost == 1) { /* :337-350 dielectric charging */
+                const int igrid = o_label(bcnd[NODE(ix, iy, nx)]);
+                const int up = o_label(bcnd[NODE(ix, iy + 1, nx)]);
+                int dt_tmp = dl->dtype[igrid];
+                if (dl->dtype[up] > dt_tmp) dt_tmp = dl->dtype[up];
+                if (dt_tmp == 1) {
+                    const double k3 = c->Nm[ptype] * c->charge[ptype];
+                    const double py = (iy * h2 - yp) / h2;
+                    dl->dq[(int64_t)igrid * (ny + 3) + iy] += k3 * py;
+                    dl->dq[(int64_t)igrid * (ny + 3) + iy + 1] += k3 * (1.0 - py);
+                }
+            }
+            if (wx && wx->sec_label > 0 && flag_lost == 1 && c->charge[ptype] > 0 &&
+                bcnd[NODE(ix, iy, nx)] == wx->sec_label) { /* :354-392 secondary emission */
+                uint32_t ctr[4] = {(uint32_t)i, wx->it, O_TAG_SECN, (uint32_t)ptype}, r[4];
+                o_philox4x32_10(ctr, wx->k0, wx->k1, r);
+                int n_sec = (int)wx->gam_sec;
+                if (o_u01(r[0]) <= wx->gam_sec - n_sec) n_sec++;
+                for (int k = 0; k < n_sec; k++) {
+                    uint32_t cv[4] = {(uint32_t)i, wx->it, O_TAG_SECV, ((uint32_t)ptype << 8) | (uint32_t)k}, v[4];
+                    o_philox4x32_10(cv, wx->k0, wx->k1, v);
+                    const double sgn = vx >= 0.0 ? 1.0 : -1.0; /* SIGN(1.d0, vpx_new) */
+                    const double vxs = -sgn * wx->vt_sec * sqrt(-log(1.0 - o_u01(v[0])));
+                    double vys, vzs;
+                    const double g[2] = {o_u01(v[1]), o_u01(v[2])};
+                    o_load_gauss(&vys, &vzs, wx->vt_sec, g);
+                    if (wx->n_sec < wx->sec_cap) {
+                        double *q = wx->sec_out + 6 * wx->n_sec;
+                        q[0] = wx->xg_sec; q[1] = yp; q[2] = zp; q[3] = vxs; q[4] = vys; q[5] = vzs;
+                    }
+                    wx->n_sec++;
+                    wx->P4sec += 0.5 * wx->Nm0 * wx->m0 * (vxs * vxs + vzs * vzs + vzs * vzs);
+                }
+            }
             if (t && flag_lost == 2) { /* :400-421 Nm q phi at the loss point */
                 const double px2 = ((int)(xp / h1) + 1) * h1, py2 = ((int)(yp / h2) + 1) * h2;
                 const int jx = (int)(xp / h1) + 1, jy = (int)(yp / h2) + 1;
@@ -187,14 +240,58 @@ void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *B
             }
             continue;
         }
-        if (c->flag_nmn == 1 && xp <= 0.0) { /* :454-459 specular reflection */
-            xp = -xp;
-            vx = -vx;
+        if (c->flag_nmn == 1 && xp <= 0.0) {
+            int done = 0;
+            if (wx && wx->reflux) { /* :445-470 refluxing */
+                const double vbx = wx->vb * wx->cos_thB;
+                const double vm = vbx - 4.0 * wx->vt > 0.0 ? vbx - 4.0 * wx->vt : 0.0, vpm = vbx + 4.0 * wx->vt;
+                const double xmax = nx * h1;
+                for (uint32_t a = 0; a < 4096 && !done; a++) {
+                    uint32_t cf[4] = {(uint32_t)i, (a << 3) | (uint32_t)ptype, O_TAG_RFX, wx->it}, f[4];
+                    o_philox4x32_10(cf, wx->k0, wx->k1, f);
+                    const double v = vm + o_u01(f[0]) * (vpm - vm);
+                    const double fv = v * exp(-(v - vbx) * (v - vbx) / (wx->vt * wx->vt));
+                    if (o_u01(f[1]) > fv / wx->fmax) continue;
+                    double vyn, vzn;
+                    const double g[2] = {o_u01(f[2]), o_u01(f[3])};
+                    o_load_gauss(&vyn, &vzn, wx->vt, g);
+                    vyn += wx->vb * wx->sin_thB;
+                    uint32_t cg[4] = {(uint32_t)i, (a << 3) | (uint32_t)ptype, O_TAG_RFX2, wx->it}, gg[4];
+                    o_philox4x32_10(cg, wx->k0, wx->k1, gg);
+                    const double xn = v * (o_u01(gg[0]) * dt);
+                    if (xn < 0.0 || xn > xmax) continue;
+                    const double ek = 0.5 * c->Nm[ptype] * c->mass[ptype];
+                    wx->P1r += ek * (vx * vx + vy * vy + vz * vz);
+                    wx->P4r += ek * (v * v + vyn * vyn + vzn * vzn);
+                    xp = xn; vx = v; vy = vyn; vz = vzn;
+                    done = 1;
+                }
+            }
+            if (!done) { /* :454-459 specular reflection */
+                xp = -xp;
+                vx = -vx;
+            }
         }
         double *q = vxp + 6 * (i - np_lost); /* :496-503 */
         q[0] = xp; q[1] = yp; q[2] = zp; q[3] = vx; q[4] = vy; q[5] = vz;
     }
     *np_tot = n - np_lost; /* :513 */
+}
+
+/* main.f90:756-809 with nproc = 1 and one MPI rank */
+void o_dielectric_update(const o_cfg *c, double *phi, const int32_t *bcnd, const int32_t *dtype,
+                         double *dq, double Ca) {
+    const int nx = c->nx, ny = c->ny;
+    const int iyl = c->flag_pbc == 1 ? 0 : 2, iyr = c->flag_pbc == 1 ? ny + 2 : ny;
+    for (int iy = iyl; iy <= iyr; iy++) {
+        const double kd = (iy == 1 || iy == ny + 1) ? 2.0 : 1.0; /* :763 half cell */
+        for (int ix = 0; ix <= nx + 2; ix++) {
+            const int igrid = bcnd[NODE(ix, iy, nx)];
+            if (igrid >= 1 && dtype[o_label(igrid)] == 1)
+                phi[NODE(ix, iy, nx)] += kd * dq[(int64_t)o_label(igrid) * (ny + 3) + iy] / (Ca * c->dy);
+        }
+    }
+    for (int64_t k = 0; k < 16 * (int64_t)(ny + 3); k++) dq[k] = 0.0; /* :776 */
 }
 
 /* part_expmover.f90:520-610 (heating tally not restated) */

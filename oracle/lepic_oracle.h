@@ -95,8 +95,8 @@ void o_load_gauss(double *vx, double *vy, double vt, const double rnd[2]);
 
 /* part_expmover.f90:1-517 (E gather, Boris/leap-frog, move, y wrap, wall loss,
  * Neumann reflection, flag_dead removal, order-preserving compaction).
- * Not restated: 3rd-dimension loss model (hz >= 0), dielectric charging, secondary
- * emission, refluxing (opt_inj = 4), phase-space and power tallies. */
+ * The 3rd-dimension model, dielectric charging, refluxing and secondary emission are in
+ * o_part_mover_z / _zd / _x below; not restated: the phase-space tally. */
 void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
                   const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
                   o_push_tally *t);
@@ -104,6 +104,40 @@ void o_part_mover(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
 void o_part_mover_z(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
                     const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
                     o_push_tally *t, const o_zloss *zl);
+
+/* dielectric walls (part_expmover.f90:340-350): dtype[label] for labels 0..15 (larger labels in
+ * the last), dq[label * (ny+3) + iy] the collected charge summed over species. */
+typedef struct {
+    const int32_t *dtype;
+    double *dq;
+} o_dielec;
+/* o_part_mover_z that also adds wall losses on dielectric labels to dl->dq when dl is not NULL */
+void o_part_mover_zd(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                     const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                     o_push_tally *t, const o_zloss *zl, const o_dielec *dl);
+/* refluxing (part_expmover.f90:445-470) and secondary emission (:354-392), drawn from the
+ * device's counter streams (slot i of the input array, step it, key k0 k1) so that the two agree
+ * particle by particle. */
+typedef struct {
+    int reflux;                 /* opt_inj = +-4 with flag_nmn: re-draw at x <= 0           */
+    double vb, fmax, vt, sin_thB, cos_thB;
+    int sec_label;              /* emitting wall label of this positive species (0: none)   */
+    double gam_sec, vt_sec, xg_sec, Nm0, m0;
+    double *sec_out;            /* (x, y, z, vx, vy, vz) per electron, in emission order    */
+    int64_t sec_cap, n_sec;
+    uint32_t k0, k1, it;
+    double P1r, P4r, P4sec;     /* P_loss(1) and (4) of this species' refluxing; (4) of the
+                                   electrons from the emission                               */
+} o_wallx;
+/* o_part_mover_zd with the two branches when wx is not NULL */
+void o_part_mover_x(const o_cfg *c, int ptype, const double *Ei, const double *Bi,
+                    const int32_t *bcnd, double *vxp, int64_t *np_tot, int8_t *flag_dead,
+                    o_push_tally *t, const o_zloss *zl, const o_dielec *dl, o_wallx *wx);
+
+/* main.f90:756-809 on one rank: phi += kd dq / (Ca dy) on the dielectric labels' wall nodes,
+ * kd = 2 on rows 1 and ny+1, rows 2..ny (0..ny+2 with flag_pbc); dq is zeroed. */
+void o_dielectric_update(const o_cfg *c, double *phi, const int32_t *bcnd, const int32_t *dtype,
+                         double *dq, double Ca);
 
 /* part_expmover.f90:520-610 -- adds into npg (caller zeroes it). */
 void o_charge_deposition(const o_cfg *c, int ptype, const double *vxp, int64_t np_tot,

@@ -259,6 +259,64 @@ def mover_z(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, phi, phi0, uB, na1, size_
     return n.value, t
 
 
+class ODielec(C.Structure):
+    _fields_ = [("dtype", C.POINTER(C.c_int32)), ("dq", C.POINTER(C.c_double))]
+
+
+def mover_dielec(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, dtype):
+    """o_part_mover_zd on vxp (n, 6) in place with dielectric labels dtype (16 entries); returns
+    (n survivors, tally, dq (16, ny+3))."""
+    n = C.c_int64(vxp.shape[0])
+    t = OPushTally()
+    dt = np.ascontiguousarray(dtype, dtype=np.int32)
+    dq = np.zeros((16, cfg.ny + 3))
+    d = ODielec(dt.ctypes.data_as(C.POINTER(C.c_int32)), dp(dq))
+    lib().o_part_mover_zd(C.byref(cfg), ptype, dp(Ei), dp(Bi), ip(bcnd), dp(vxp), C.byref(n), None, C.byref(t),
+                          None, C.byref(d))
+    return n.value, t, dq
+
+
+class OWallx(C.Structure):
+    _fields_ = [("reflux", C.c_int), ("vb", C.c_double), ("fmax", C.c_double), ("vt", C.c_double),
+                ("sin_thB", C.c_double), ("cos_thB", C.c_double), ("sec_label", C.c_int),
+                ("gam_sec", C.c_double), ("vt_sec", C.c_double), ("xg_sec", C.c_double), ("Nm0", C.c_double),
+                ("m0", C.c_double), ("sec_out", C.POINTER(C.c_double)), ("sec_cap", C.c_int64),
+                ("n_sec", C.c_int64), ("k0", C.c_uint32), ("k1", C.c_uint32), ("it", C.c_uint32),
+                ("P1r", C.c_double), ("P4r", C.c_double), ("P4sec", C.c_double)]
+
+
+def mover_wallx(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray, seed: int, it: int, reflux=None, secondary=None,
+                sec_cap: int = 1 << 20):
+    """o_part_mover_x on vxp (n, 6) in place with the device's counter streams.
+    reflux: dict(vb, fmax, vt, th_B); secondary: dict(label, gam, vt, xg, Nm0, m0).
+    Returns (n survivors, tally, wallx struct, emitted electrons (m, 6))."""
+    n = C.c_int64(vxp.shape[0])
+    t = OPushTally()
+    w = OWallx()
+    out = np.zeros((sec_cap, 6))
+    k0, k1 = zloss_keys(seed)
+    w.k0, w.k1, w.it = k0, k1, it
+    if reflux:
+        w.reflux = 1
+        w.vb, w.fmax, w.vt = reflux["vb"], reflux["fmax"], reflux["vt"]
+        w.sin_thB, w.cos_thB = math.sin(reflux["th_B"]), math.cos(reflux["th_B"])
+    if secondary:
+        w.sec_label, w.gam_sec, w.vt_sec = secondary["label"], secondary["gam"], secondary["vt"]
+        w.xg_sec, w.Nm0, w.m0 = secondary["xg"], secondary["Nm0"], secondary["m0"]
+    w.sec_out = dp(out)
+    w.sec_cap = sec_cap
+    lib().o_part_mover_x(C.byref(cfg), ptype, dp(Ei), dp(Bi), ip(bcnd), dp(vxp), C.byref(n), None, C.byref(t),
+                         None, None, C.byref(w))
+    return n.value, t, w, out[:min(w.n_sec, sec_cap)].copy()
+
+
+def dielectric_update(cfg, phi: np.ndarray, bcnd, dtype, dq: np.ndarray, Ca: float):
+    """o_dielectric_update: phi (ny+3, nx+3) and dq (16, ny+3) in place."""
+    dt = np.ascontiguousarray(dtype, dtype=np.int32)
+    lib().o_dielectric_update(C.byref(cfg), dp(phi), ip(bcnd), dt.ctypes.data_as(C.POINTER(C.c_int32)), dp(dq),
+                              C.c_double(Ca))
+
+
 def mover_tagged(cfg, ptype, Ei, Bi, bcnd, vxp: np.ndarray):
     """o_part_mover on a copy of vxp whose z holds each particle's index; returns the survivors
     (compacted in order, part_expmover.f90:496-503) and their indices.  z moves by dt*vz, far

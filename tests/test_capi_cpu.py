@@ -39,7 +39,7 @@ def test_ctypes_prototypes_cover_header():
 
 def test_abi_version_without_gpu(lib):
     lib.lepic_gpu_abi_version.restype = C.c_int32
-    assert lib.lepic_gpu_abi_version() == 3
+    assert lib.lepic_gpu_abi_version() == 4
 
 
 def test_struct_layouts_match_c():
@@ -49,7 +49,8 @@ def test_struct_layouts_match_c():
                "lepic_cnn_config": _capi.LepicCnnConfig, "lepic_cnn_stats": _capi.LepicCnnStats,
                "lepic_source_config": _capi.LepicSourceConfig, "lepic_source_tally": _capi.LepicSourceTally,
                "lepic_tallies": _capi.LepicTallies, "lepic_options": _capi.LepicOptions,
-               "lepic_zloss_config": _capi.LepicZlossConfig}
+               "lepic_zloss_config": _capi.LepicZlossConfig,
+               "lepic_secondary_config": _capi.LepicSecondaryConfig}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

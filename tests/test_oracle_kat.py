@@ -317,3 +317,38 @@ def test_oracle_third_dimension_model():
     n, _ = O.mover_z(cfg, 1, E, None, case.bcnd, ions, phi, 0.0, uB, 16, 1, hz, 1, 3)
     expect = m * hz * 2 * 3000.0 / case.zmax * case.dt
     assert abs((m - n) - expect) < 5 * math.sqrt(expect)
+
+
+def test_oracle_dielectric_charging():
+    """o_part_mover_zd / o_dielectric_update (part_expmover.f90:340-350, main.f90:756-809): an
+    electron lost in the left wall at y = (iy - 0.25) h leaves 0.25 Nm q on row iy and 0.75 on
+    row iy+1 of the wall's label; the update adds kd dq / (Ca dy) to that label's wall nodes of
+    rows 2..ny (kd = 2 on rows 1 and ny+1) and clears dq.  A conductor label collects nothing."""
+    case = configs.case0(ppc=1, nx=16, ny=16)
+    case.bcnd = configs.box_mask(16, 16, label_left=2, label_right=3)
+    cfg, sp = cfg_for(case)
+    E = np.zeros((case.ny + 3, case.nx + 3, 2))
+    dtype = np.zeros(16, np.int32)
+    dtype[2] = 1
+    p = np.zeros((3, 6))
+    p[0, 0], p[0, 1], p[0, 3] = 0.5 * case.dx, 6.75 * case.dy, -1.0 * case.dx / case.dt  # -> x < 0: cell ix 0
+    p[1, 0], p[1, 1], p[1, 3] = (case.nx - 0.5) * case.dx, 5.5 * case.dy, case.dx / case.dt  # right: a conductor
+    p[2, 0], p[2, 1] = 8.0 * case.dx, 8.0 * case.dy                                          # stays
+    n, t, dq = O.mover_dielec(cfg, 0, E, None, case.bcnd, p, dtype)
+    nmq = sp.Nm[0] * sp.charge[0]
+    assert n == 1 and t.n_lost == 2
+    iy = 7                                           # floor(6.75) + 1
+    assert dq[2, iy] == pytest.approx(0.25 * nmq) and dq[2, iy + 1] == pytest.approx(0.75 * nmq)
+    assert np.count_nonzero(dq) == 2
+    phi = np.zeros((case.ny + 3, case.nx + 3))
+    Ca = 1e-7
+    O.dielectric_update(cfg, phi, case.bcnd, dtype, dq, Ca)
+    assert not dq.any()
+    col = phi[:, 0]
+    assert col[iy] == pytest.approx(0.25 * nmq / (Ca * case.dy))
+    assert col[iy + 1] == pytest.approx(0.75 * nmq / (Ca * case.dy))
+    assert np.count_nonzero(phi) == 4                # columns 0 and 1 of label 2, two rows
+    # a loss on row 1 (the half cell) doubles, but the row lies outside 2..ny: nothing moves
+    dq[2, 1] = nmq
+    O.dielectric_update(cfg, phi, case.bcnd, dtype, dq, Ca)
+    assert np.count_nonzero(phi) == 4
