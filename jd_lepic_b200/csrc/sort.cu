@@ -4,8 +4,9 @@
 // ic = (ix-1) + nx*(iy-1) + 1, original order kept inside a cell.  Here:
 //   1. keys + histogram        (warp-aggregated atomics on the per-key counts)
 //   2. exclusive scan           (three-phase, fixed order)
-//   3. scatter of slot indices  (atomics; each warp takes a contiguous chunk in slot order, so
-//                               a key comes out of order only where it straddles chunks)
+//   3. scatter of slot indices  (atomics; each warp takes one old tile's slots, or a chunk of the
+//                               appended tail, in slot order, so a key comes out of order only
+//                               where it receives particles from another tile or the tail)
 //   4. per-key segment sort of the slot indices (bitonic, ascending; segments already in
 //      order are skipped) -> stable again
 //   5. gather of the 5 SoA fields into the other buffer, holes dropped
@@ -24,6 +25,7 @@
 #define PUSH_CHUNK 16384
 #define SEG_WARP_MAX 256
 #define SEG_BLOCK_MAX 8192
+#define SEG_CHECK_STEPS 4
 
 struct KeyP {
     int S, nx, ny, tw, th, ntx;
@@ -146,38 +148,65 @@ __global__ void k_scan_final(const int *counts, long long n, const int *blocksum
     }
 }
 
-// Each warp scatters a contiguous chunk of SCATTER_CHUNK slots in slot order, so inside a chunk
-// the slots of a key reach their segment in ascending order; only a key whose slots straddle
-// chunks can come out of order (the segment sort below checks every segment and sorts those).
+// Each warp scatters one work unit in slot order: a work item of the previous sort (the slots of
+// one old tile, or a part of it) or a SCATTER_CHUNK-slot chunk of the tail appended since.  A
+// particle that changed cell inside its old tile is met by the same warp in slot order as the
+// particles of its new cell, so its position comes out in stable order; only a cell that
+// receives particles from another work unit (a neighbouring tile, the tail) can come out of
+// order, and the segment sort below checks every segment and sorts those.  (Fixed 1024-slot
+// chunks cut every tile into pieces, so a particle moving to the next row of cells reached
+// another chunk and nearly every electron cell needed the segment sort.)  Units are dispensed
+// dynamically: the items' sizes follow the density.
 #define SCATTER_CHUNK 1024
-__global__ void k_scatter(const int *keys, const DevCounters *cnt, int sp, int *cursor, int *perm) {
+#define SCATTER_STEPS 8
+__global__ void k_scatter(const int *keys, const WorkItem *items, DevCounters *cnt, int sp, int *cursor, int *perm) {
     const long long n = cnt->n_slots[sp];
+    const long long ns = min(cnt->n_sorted[sp], n);
+    const int ni = cnt->n_items[sp];
+    const long long units = ni + (n - ns + SCATTER_CHUNK - 1) / SCATTER_CHUNK;
     const unsigned lane = threadIdx.x & 31;
-    const long long nchunks = (n + SCATTER_CHUNK - 1) / SCATTER_CHUNK;
-    const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long c = gw; c < nchunks; c += nw) {
-        const long long c1 = min((c + 1) * SCATTER_CHUNK, n);
-        // four 32-slot steps at a time: their atomics are in flight together (issued in step
-        // order, so a key that runs across steps still receives ascending positions)
-        for (long long i0 = c * SCATTER_CHUNK; i0 < c1; i0 += 4 * 32) {
-            int key[4], base[4];
-            unsigned m[4];
+    for (;;) {
+        long long u = 0;
+        if (lane == 0) u = (long long)atomicAdd(&cnt->scatter_next, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= units) break;
+        long long c0, c1;
+        if (u < ni) {
+            const WorkItem w = items[u];
+            c0 = w.start;
+            c1 = min((long long)w.end, ns);
+        } else {
+            c0 = ns + (u - ni) * SCATTER_CHUNK;
+            c1 = min(c0 + SCATTER_CHUNK, n);
+        }
+        // SCATTER_STEPS 32-slot steps at a time: their atomics are in flight together (issued in
+        // step order, so a key that runs across steps still receives ascending positions), and the
+        // next iteration's keys are loaded before this one's atomics
+        int nk[SCATTER_STEPS];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const long long i = i0 + 32 * u + lane;
-                key[u] = (i < c1) ? keys[i] : -1;
+        for (int v = 0; v < SCATTER_STEPS; v++) {
+            const long long i = c0 + 32 * v + lane;
+            nk[v] = (i < c1) ? keys[i] : -1;
+        }
+        for (long long i0 = c0; i0 < c1; i0 += SCATTER_STEPS * 32) {
+            int key[SCATTER_STEPS], base[SCATTER_STEPS];
+            unsigned m[SCATTER_STEPS];
+#pragma unroll
+            for (int v = 0; v < SCATTER_STEPS; v++) {
+                key[v] = nk[v];
+                const long long i = i0 + SCATTER_STEPS * 32 + 32 * v + lane;
+                nk[v] = (i < c1) ? keys[i] : -1;
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                m[u] = __match_any_sync(0xffffffffu, key[u]);
-                base[u] = 0;
-                if (key[u] >= 0 && (int)lane == __ffs(m[u]) - 1) base[u] = atomicAdd(&cursor[key[u]], __popc(m[u]));
+            for (int v = 0; v < SCATTER_STEPS; v++) {
+                m[v] = __match_any_sync(0xffffffffu, key[v]);
+                base[v] = 0;
+                if (key[v] >= 0 && (int)lane == __ffs(m[v]) - 1) base[v] = atomicAdd(&cursor[key[v]], __popc(m[v]));
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int b = __shfl_sync(m[u], base[u], __ffs(m[u]) - 1);
-                if (key[u] >= 0) perm[b + __popc(m[u] & ((1u << lane) - 1u))] = (int)(i0 + 32 * u + lane);
+            for (int v = 0; v < SCATTER_STEPS; v++) {
+                const int b = __shfl_sync(m[v], base[v], __ffs(m[v]) - 1);
+                if (key[v] >= 0) perm[b + __popc(m[v] & ((1u << lane) - 1u))] = (int)(i0 + 32 * v + lane);
             }
         }
     }
@@ -207,45 +236,71 @@ __device__ __forceinline__ void warp_sort64(int &v0, int &v1, int lane) {
     }
 }
 
+// A warp takes 32 consecutive segments: one coalesced load of their bounds, then one pass over
+// their slot lists in 32-wide steps that marks each segment holding a descending adjacent pair
+// (the segment of a position is found by a binary search over the 32 bounds held in the lanes);
+// only the marked segments are sorted: up to 64 slots in registers, up to SEG_WARP_MAX in the
+// warp's shared memory, longer ones listed for k_segsort_big.  (One segment per warp, each with
+// its own dependent loads of bounds and slots, was latency-bound on the segments in order.)
 __global__ void k_segsort_warp(const int *offsets, long long nkeys, int *perm, int *bigseg,
                                DevCounters *cnt) {
     __shared__ int buf[SORT_THREADS / 32][SEG_WARP_MAX];
+    const unsigned full = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long k = gw; k < nkeys; k += nw) {
-        int s0 = offsets[k], s1 = offsets[k + 1], n = s1 - s0;
-        if (n <= 1) continue;
-        if (n <= 64) {   // the common case: in registers, no shared memory
-            int v0 = lane < n ? perm[s0 + lane] : INT_MAX;
-            int v1 = lane + 32 < n ? perm[s0 + lane + 32] : INT_MAX;
-            // already ascending (the chunked scatter leaves most segments so): nothing to do
-            const int n0 = __shfl_down_sync(0xffffffffu, v0, 1), n1 = __shfl_down_sync(0xffffffffu, v1, 1);
-            const int f1 = __shfl_sync(0xffffffffu, v1, 0);
-            const bool ok = (lane == 31 ? v0 <= f1 : v0 <= n0) && (lane == 31 || v1 <= n1);
-            if (__all_sync(0xffffffffu, ok)) continue;
-            warp_sort64(v0, v1, lane);
-            if (lane < n) perm[s0 + lane] = v0;
-            if (lane + 32 < n) perm[s0 + lane + 32] = v1;
-            continue;
-        }
-        bool sorted = true;
-        for (int q = lane; q + 1 < n; q += 32)
-            if (perm[s0 + q] > perm[s0 + q + 1]) sorted = false;
-        if (__all_sync(0xffffffffu, sorted)) continue;
-        if (n > SEG_WARP_MAX) {
-            if (lane == 0) {
-                int slot = atomicAdd(&cnt->n_big, 1);
-                bigseg[slot] = (int)k;
+    const long long ngroups = (nkeys + 31) / 32;
+    for (long long gi = gw; gi < ngroups; gi += nw) {
+        const long long k = gi * 32 + lane;
+        const int s0 = offsets[k < nkeys ? k : nkeys];
+        const int s1 = offsets[k < nkeys ? k + 1 : nkeys];
+        const int S0 = __shfl_sync(full, s0, 0), S1 = __shfl_sync(full, s1, 31);
+        unsigned dirty = 0;
+        for (int q0 = S0; q0 < S1 - 1; q0 += 32 * SEG_CHECK_STEPS) {   // the pairs (q, q+1)
+            int a[SEG_CHECK_STEPS], b[SEG_CHECK_STEPS];
+#pragma unroll
+            for (int u = 0; u < SEG_CHECK_STEPS; u++) {   // every step's loads in flight together
+                const int q = q0 + 32 * u + lane;
+                a[u] = 0; b[u] = 0;
+                if (q < S1 - 1) { a[u] = perm[q]; b[u] = perm[q + 1]; }
             }
-            continue;
+            unsigned mark = 0;
+#pragma unroll
+            for (int u = 0; u < SEG_CHECK_STEPS; u++) {
+                const int q = q0 + 32 * u + lane;
+                int lo = 0;                                // the last lane whose segment starts at or before q
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int sv = __shfl_sync(full, s0, lo + st);
+                    if (sv <= q) lo += st;
+                }
+                const int e = __shfl_sync(full, s1, lo);
+                if (q < S1 - 1 && a[u] > b[u] && q + 1 < e) mark |= 1u << lo;
+            }
+            dirty |= __reduce_or_sync(full, mark);
         }
-        int *a = buf[warp];
-        for (int q = lane; q < n; q += 32) a[q] = perm[s0 + q];
-        __syncwarp();
-        bitonic_sort(a, n, lane, 32, WarpSync());
-        for (int q = lane; q < n; q += 32) perm[s0 + q] = a[q];
-        __syncwarp();
+        while (dirty) {
+            const int l = __ffs(dirty) - 1;
+            dirty &= dirty - 1;
+            const int t0 = __shfl_sync(full, s0, l), n = __shfl_sync(full, s1, l) - t0;
+            if (n <= 64) {   // in registers
+                int v0 = lane < n ? perm[t0 + lane] : INT_MAX;
+                int v1 = lane + 32 < n ? perm[t0 + lane + 32] : INT_MAX;
+                warp_sort64(v0, v1, lane);
+                if (lane < n) perm[t0 + lane] = v0;
+                if (lane + 32 < n) perm[t0 + lane + 32] = v1;
+            } else if (n <= SEG_WARP_MAX) {
+                int *a = buf[warp];
+                for (int q = lane; q < n; q += 32) a[q] = perm[t0 + q];
+                __syncwarp();
+                bitonic_sort(a, n, lane, 32, WarpSync());
+                for (int q = lane; q < n; q += 32) perm[t0 + q] = a[q];
+                __syncwarp();
+            } else if (lane == 0) {
+                const int slot = atomicAdd(&cnt->n_big, 1);
+                bigseg[slot] = (int)(gi * 32 + l);
+            }
+        }
     }
 }
 
@@ -361,6 +416,7 @@ int sort_species(lepic_ctx *c, int sp) {
     int grid = c->num_sms * 8;
     LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
     LCUDA(cudaMemsetAsync(&c->dcnt->n_big, 0, sizeof(int), c->stream));
+    LCUDA(cudaMemsetAsync(&c->dcnt->scatter_next, 0, sizeof(unsigned int), c->stream));
     k_keys_hist<<<grid, SORT_THREADS, 0, c->stream>>>(K, B.X[cur], B.Y[cur], B.VX[cur], B.VY[cur], B.VZ[cur],
                                                         c->bcnd, c->tally, c->dcnt, sp, c->keys, c->counts);
     int nb = div_up(nk, SCAN_ITEMS);
@@ -368,7 +424,7 @@ int sort_species(lepic_ctx *c, int sp) {
     k_scan_top<<<1, 1024, 0, c->stream>>>(c->blocksums, nb);
     k_scan_final<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums, c->offsets);
     LCUDA(cudaMemcpyAsync(c->cursor, c->offsets, sizeof(int) * nk, cudaMemcpyDeviceToDevice, c->stream));
-    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, c->dcnt, sp, c->cursor, c->perm);
+    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, B.items, c->dcnt, sp, c->cursor, c->perm);
     k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, nk, c->perm, c->bigseg, c->dcnt);
     k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, c->perm, c->bigseg, c->dcnt);
     k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
