@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_PARTICLE_STEP = 40  # X, Y, VX, VY, VZ read + written by the fused push/deposit
+PERM_BYTES_PER_PARTICLE = 4   # the push after a sort also reads the sort's permutation
 
 
 def peaks():
@@ -493,7 +494,9 @@ def run_ours(args):
     n_avg = 0.5 * (n_start + n_end)
     value = n_avg * args.steps * world / (total_ms * 1e-3)
     push_ms = phases["push_deposit"] / args.steps
-    bytes_per_launch = BYTES_PER_PARTICLE_STEP * n_avg
+    # the push after each sort reads the pending permutation too (lepic_options.sort_defer = 1)
+    n_sort_pushes = sum(1 for k in range(first_timed, first_timed + args.steps) if k % 10 == 1)
+    bytes_per_launch = (BYTES_PER_PARTICLE_STEP + PERM_BYTES_PER_PARTICLE * n_sort_pushes / args.steps) * n_avg
     peak, peak_kind = peaks()
     achieved = bytes_per_launch / (push_ms * 1e-3) / 1e9
     tpp = profiled_traffic_per_particle()
@@ -640,6 +643,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": "k_push_deposit (both species, incl. accumulator clears)",
+                         "algorithmic_bytes_per_particle": bytes_per_launch / n_avg,
                          "traffic": (tpp * n_avg if tpp else None)},
             "cpu_baseline": ({k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")} if cb else None),
             "e2e": {"value": e2e_value, "unit": "particle-steps/s",

@@ -247,6 +247,11 @@ typedef struct lepic_options {
                                     about 2 s), the kernel ends and the call returns LEPIC_ETIMEOUT */
     int64_t fortran_max_subrecord; /* backup writer: subrecord length limit (2^31 - 9, the Intel and
                                     GNU runtimes' value); smaller values exercise the layout         */
+    int32_t sort_defer;          /* 1 (default): a sort leaves its permutation pending and the next
+                                    push moves the records as it writes them (one pass over them
+                                    fewer; every other call that reads them moves them first);
+                                    0: the sort moves them itself -- the same order and results  */
+    int32_t pad;
 } lepic_options;
 int lepic_gpu_get_options(lepic_ctx *ctx, lepic_options *out);
 int lepic_gpu_set_options(lepic_ctx *ctx, const lepic_options *in);

@@ -197,7 +197,7 @@ class LepicOptions(C.Structure):
                 ("mx_onchip_bytes", C.c_int32), ("mx_tiled", C.c_int32), ("mx_max_iter", C.c_int32),
                 ("mx_coarse_direct", C.c_int32),
                 ("mg_small_nodes", C.c_int32), ("ctas_per_sm", C.c_int32), ("barrier_extra", C.c_int32),
-                ("fortran_max_subrecord", C.c_int64)]
+                ("fortran_max_subrecord", C.c_int64), ("sort_defer", C.c_int32), ("pad", C.c_int32)]
 
 PROTOTYPES = {
     "lepic_gpu_abi_version": (C.c_int32, []),

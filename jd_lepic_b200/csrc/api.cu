@@ -45,7 +45,7 @@ static void free_all(lepic_ctx *c) {
     for (int s = 0; s < LEPIC_MAXSP; s++) {
         SpeciesBuf &B = c->sp[s];
         for (int k = 0; k < 2; k++) { F(B.X[k]); F(B.Y[k]); F(B.VX[k]); F(B.VY[k]); F(B.VZ[k]); F(B.Z[k]); }
-        F(B.acc); F(B.items); F(B.prod); F(B.cell_off); F(B.claim);
+        F(B.acc); F(B.items); F(B.prod); F(B.cell_off); F(B.claim); F(B.pind);
     }
     F(c->keys); F(c->perm); F(c->counts); F(c->offsets); F(c->cursor); F(c->blocksums); F(c->bigseg);
     for (int l = 0; l < c->nlev; l++) {
@@ -301,6 +301,7 @@ static lepic_options default_options() {
     o.ctas_per_sm = 3;
     o.barrier_extra = 0;
     o.fortran_max_subrecord = 2147483639ll;
+    o.sort_defer = 1;
     return o;
 }
 
@@ -318,7 +319,7 @@ extern "C" int lepic_gpu_set_options(lepic_ctx *c, const lepic_options *in) {
         (o.mx_tiled != 0 && o.mx_tiled != 1) || o.mx_max_iter < 1 ||
         (o.mx_coarse_direct != 0 && o.mx_coarse_direct != 1) || o.mg_small_nodes < 0 || o.ctas_per_sm < 1 ||
         o.ctas_per_sm > 8 || o.barrier_extra < 0 || o.barrier_extra > 1024 || o.fortran_max_subrecord < 8 ||
-        o.fortran_max_subrecord > 2147483639ll) {
+        o.fortran_max_subrecord > 2147483639ll || (o.sort_defer != 0 && o.sort_defer != 1)) {
         c->last_err = "set_options: a value is out of range";
         return LEPIC_EINVAL;
     }
@@ -565,6 +566,7 @@ int particles_load(lepic_ctx *c, const lepic_load_spec *sp) {
 
 extern "C" int lepic_gpu_put_particles(lepic_ctx *c, int32_t ptype, const double *vxp, int64_t n) {
     if (!c || ptype < 0 || ptype >= c->cfg.ntype || (n > 0 && !vxp)) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return particles_put(c, ptype, vxp, n);
 }
 // The reference's own particle array vxp(6, nmax, ntype, nproc) with np_tot(ntype, nproc): a
@@ -574,6 +576,7 @@ extern "C" int lepic_gpu_put_particles(lepic_ctx *c, int32_t ptype, const double
 extern "C" int lepic_gpu_put_particles_slabs(lepic_ctx *c, const double *vxp, const int32_t *np_tot, int64_t nmax,
                                              int32_t ntype, int32_t nproc) {
     if (!c || !vxp || !np_tot || nmax < 0 || ntype != c->cfg.ntype || nproc < 1) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     for (int s = 0; s < ntype; s++) {
         long long n = 0;
         for (int p = 0; p < nproc; p++) {
@@ -598,6 +601,7 @@ extern "C" int lepic_gpu_put_particles_slabs(lepic_ctx *c, const double *vxp, co
 extern "C" int lepic_gpu_get_particles_slabs(lepic_ctx *c, double *vxp, int32_t *np_tot, int64_t nmax,
                                              int32_t ntype, int32_t nproc) {
     if (!c || !vxp || !np_tot || nmax < 0 || ntype != c->cfg.ntype || nproc < 1) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     for (int s = 0; s < ntype; s++) {
         long long n = 0;
         int r = particles_get(c, s, nullptr, 0, &n);
@@ -620,6 +624,7 @@ extern "C" int lepic_gpu_get_particles_slabs(lepic_ctx *c, double *vxp, int32_t 
 
 extern "C" int lepic_gpu_get_particles(lepic_ctx *c, int32_t ptype, double *vxp, int64_t cap, int64_t *n_out) {
     if (!c || ptype < 0 || ptype >= c->cfg.ntype) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     long long n = 0;
     int r = particles_get(c, ptype, vxp, cap, &n);
     if (n_out) *n_out = n;
@@ -627,6 +632,7 @@ extern "C" int lepic_gpu_get_particles(lepic_ctx *c, int32_t ptype, double *vxp,
 }
 extern "C" int lepic_gpu_load_particles(lepic_ctx *c, const lepic_load_spec *spec) {
     if (!c || !spec || spec->n_samples < 0) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return particles_load(c, spec);
 }
 
@@ -767,7 +773,9 @@ extern "C" int lepic_gpu_calc_efield(lepic_ctx *c, double *Ei_out) {
 
 extern "C" int lepic_gpu_part_sorting(lepic_ctx *c, int32_t ptype, int32_t *plist_out) {
     if (!c || ptype < 0 || ptype >= c->cfg.ntype) return LEPIC_EINVAL;
-    int r = sort_species(c, ptype);
+    // the records move into sorted order in the next push (or, before any other call that reads
+    // them, at that call's start): the same order, one pass over the records fewer
+    int r = sort_species(c, ptype, c->opt.sort_defer == 1 && !push_needs_general(c, ptype));
     if (r != LEPIC_OK || !plist_out) return r;
     const int nx = c->cfg.nx, ny = c->cfg.ny;
     const long long pl_max = (long long)nx + (long long)nx * ny + 1;
@@ -795,6 +803,12 @@ extern "C" int lepic_gpu_push_deposit(lepic_ctx *c, int32_t it, lepic_push_stats
     return LEPIC_OK;
 }
 
+// an error inside lepic_gpu_step: the records of a pending permutation are moved first
+static int settle(lepic_ctx *c, int r) {
+    materialize_all(c);
+    return r;
+}
+
 extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode) {
     if (!c) return LEPIC_EINVAL;
     const lepic_config &g = c->cfg;
@@ -803,14 +817,19 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
     if ((r = field_calc_rhs(c)) != LEPIC_OK) return r;
     if ((r = solve(c, eps, mode)) != LEPIC_OK) return r;
     if ((r = field_calc_efield(c)) != LEPIC_OK) return r;
+    // The sort leaves its permutation pending for the species the fast mover pushes (as
+    // lepic_gpu_part_sorting does): the collisions read and write through it and the push moves
+    // the records into sorted order as it writes them, which saves the sort's gather (44 B per
+    // particle).  Whatever else would read the records in between moves them first.
     if (g.nsort > 0 && it % g.nsort == 1)
         for (int s = 0; s < g.ntype; s++)
-            if ((r = sort_species(c, s)) != LEPIC_OK) return r;
-    if ((r = avg_step(c, it)) != LEPIC_OK) return r;  // main.f90:906-949
+            if ((r = sort_species(c, s, c->opt.sort_defer == 1 && !push_needs_general(c, s))) != LEPIC_OK)
+                return settle(c, r);
+    if ((r = avg_step(c, it)) != LEPIC_OK) return settle(c, r);  // main.f90:906-949
     if (it > 1 && g.ns_coll > 0 && it % g.ns_coll == 1)
-        if ((r = mcc_collide(c, it, false)) != LEPIC_OK) return r;
-    if ((r = sources_before_push(c, it)) != LEPIC_OK) return r;
-    if ((r = push_deposit(c, it, true)) != LEPIC_OK) return r;
+        if ((r = mcc_collide(c, it, false)) != LEPIC_OK) return settle(c, r);
+    if ((r = sources_before_push(c, it)) != LEPIC_OK) return settle(c, r);
+    if ((r = push_deposit(c, it, true)) != LEPIC_OK) return settle(c, r);
     return sources_after_push(c, it);
 }
 
@@ -900,6 +919,7 @@ extern "C" int lepic_gpu_deposit_grid(lepic_ctx *c, int32_t ptype, void **acc) {
 extern "C" int lepic_gpu_particle_arrays(lepic_ctx *c, int32_t ptype, void **X, void **Y, void **VX, void **VY,
                                          void **VZ, int64_t *n_slots, int32_t *shift) {
     if (!c || ptype < 0 || ptype >= c->cfg.ntype) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     SpeciesBuf &B = c->sp[ptype];
     if (X) *X = B.X[B.cur];
     if (Y) *Y = B.Y[B.cur];

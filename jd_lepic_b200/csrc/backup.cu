@@ -189,6 +189,7 @@ static long long max_subrecord(const lepic_ctx *c) {
 // ---------------------------------------------------------------------------------------
 extern "C" int lepic_gpu_write_backup(lepic_ctx *c, const char *path, double time, int32_t gtype, double Pabs_cor) {
     if (!c || !path) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     int r = lepic_gpu_sync(c);
     if (r != LEPIC_OK) return r;
     const lepic_config &g = c->cfg;
@@ -307,6 +308,7 @@ extern "C" int lepic_gpu_write_backup(lepic_ctx *c, const char *path, double tim
 
 extern "C" int lepic_gpu_read_backup(lepic_ctx *c, const char *path, double *time, int32_t *gtype, double *Pabs_cor) {
     if (!c || !path) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     int r = lepic_gpu_sync(c);
     if (r != LEPIC_OK) return r;
     const lepic_config &g = c->cfg;
@@ -409,6 +411,7 @@ __global__ void k_duplicate(long long n, int copies, uint32_t *X, uint32_t *Y, f
 
 extern "C" int lepic_gpu_duplicate_particles(lepic_ctx *c, int32_t np_dup) {
     if (!c) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     const int dup = np_dup < 0 ? -np_dup : np_dup;
     if (dup <= 1) return LEPIC_OK;
     int r = lepic_gpu_sync(c);

@@ -191,6 +191,7 @@ void avg_free(lepic_ctx *c) {
 
 extern "C" int lepic_gpu_set_avg(lepic_ctx *c, int32_t size_na, int32_t navg) {
     if (!c || size_na < 1 || navg < 0) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     const lepic_config &g = c->cfg;
     if (g.nx / size_na < 1 || g.ny / size_na < 1) { c->last_err = "size_na larger than the grid"; return LEPIC_EINVAL; }
     avg_free(c);
@@ -272,6 +273,7 @@ int avg_sample(lepic_ctx *c, int it) {
 
 extern "C" int lepic_gpu_calc_avg(lepic_ctx *c) {
     if (!c || !avg_state(c)) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return avg_sample(c, 0x40000000 + avg_state(c)->cnt);   // the diagnostic pass's draws: a stream per sample
 }
 
@@ -334,6 +336,8 @@ extern "C" int lepic_gpu_get_source_maps(lepic_ctx *c, double *ss2D) {
 int avg_step(lepic_ctx *c, int it) {
     AvgState *A = avg_state(c);
     if (!A || A->navg < 1 || it % A->navg != 1) return LEPIC_OK;
+    const int r = materialize_all(c);   // the moments read the records in sorted order
+    if (r != LEPIC_OK) return r;
     return avg_sample(c, it);
 }
 
@@ -370,6 +374,7 @@ int sources_reset_power(lepic_ctx *c);
 
 extern "C" int lepic_gpu_get_tallies(lepic_ctx *c, lepic_tallies *out, int32_t reset) {
     if (!c || !out) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     for (int s = 0; s < c->cfg.ntype; s++) {
         SpeciesBuf &B = c->sp[s];
         k_loss_scan<<<c->num_sms * 8, 256, 0, c->stream>>>(B.X[B.cur], B.Y[B.cur], B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur],

@@ -59,6 +59,7 @@ struct DevCounters {
     unsigned int prod_count[LEPIC_MAXSP]; // products waiting for the ordered append
     int n_big;                            // sort: segments too long for one warp
     unsigned int scatter_next;            // sort: the scatter's work-unit dispenser
+    long long ind_old[LEPIC_MAXSP];       // sort: the slots occupied before it (pending permutation)
     unsigned int n_cand_list;             // collisions: candidates of the species being treated
     int err;
     int err_where;
@@ -128,7 +129,19 @@ struct SpeciesBuf {
     int max_items;
     Product *prod;             // product list
     int prod_cap;
+    // A sort inside lepic_gpu_step may leave its permutation pending instead of moving the
+    // records: position j of the sorted order is then slot pind[j] of buffer cur for
+    // j < n_sorted, and slot ind_old + (j - n_sorted) for the products appended since (ind_old =
+    // the slots occupied before the sort).  The collisions and the push read and write through
+    // it; the push writes the sorted order into the other buffer and ends the pending state.
+    int *pind = nullptr;
+    bool ind = false;
 };
+
+// the slot of buffer cur that holds position j of a species' sorted order (see SpeciesBuf)
+__device__ __forceinline__ long long ind_slot(const int *pind, long long n_sorted, long long ind_old, long long j) {
+    return pind ? (j < n_sorted ? (long long)pind[j] : ind_old + (j - n_sorted)) : j;
+}
 
 struct lepic_ctx {
     lepic_config cfg;
@@ -400,7 +413,13 @@ int dielectric_update(lepic_ctx *c);
 // xtrap: the warm start may extrapolate; fp64: the V-cycle in FP64 (mode 4) instead of FP32
 int mg_mixed_solve(lepic_ctx *c, double eps, bool xtrap, bool fp64 = false);
 int push_deposit(lepic_ctx *c, int it, bool move);
-int sort_species(lepic_ctx *c, int ptype);
+int sort_species(lepic_ctx *c, int ptype, bool defer = false);
+// moves the records of a pending permutation (the gather a deferred sort left out)
+int materialize_species(lepic_ctx *c, int ptype);
+int materialize_all(lepic_ctx *c);
+// true when the push of species s takes the general mover (boundary options, wall models,
+// the 3rd dimension); such a species' sort is not deferred
+bool push_needs_general(const lepic_ctx *c, int s);
 int particles_load(lepic_ctx *c, const lepic_load_spec *spec);
 int particles_put(lepic_ctx *c, int ptype, const double *vxp, long long n);
 int particles_get(lepic_ctx *c, int ptype, double *vxp, long long cap, long long *n_out);

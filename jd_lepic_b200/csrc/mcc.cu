@@ -68,7 +68,15 @@ struct MccP {
     const double *np_red;
     const double *nu_max_d;   // the device's nu_max of this step (DSMC), else nu_max above
     double ns_coll_dt;
+    // a sort's pending permutation per species (SpeciesBuf::pind), null where there is none:
+    // slots and targets are positions of the sorted order, read and written through it
+    const int *pind[LEPIC_MAXSP];
 };
+
+// the slot of the buffer that holds position j of species s
+__device__ __forceinline__ long long mslot(const MccP &P, int s, long long j) {
+    return ind_slot(P.pind[s], P.cnt->n_sorted[s], P.cnt->ind_old[s], j);
+}
 
 #define TAG_DSMC 0x44534D43u
 
@@ -146,7 +154,7 @@ __device__ __forceinline__ double sigma_at(const MccP &P, int c, double E) {
     return sL + (E - EL) * (sR - sL) / (ER - EL);
 }
 
-// plt_src = 1 (collisions.f90:546-600): reaction c of the incident in `slot` at frequency k2
+// plt_src = 1 (collisions.f90:546-600): reaction c of the incident in `slot` (of the buffer) at frequency k2
 // (1/s) adds k2 Nm/Vc, with the incident's CIC weights, to the source of every charged byproduct
 // other than the incident's and the target's species and to the sink of a charged reactant
 // that is not among the byproducts; elastic and excitation reactions (types 1, 3) add nothing.
@@ -181,27 +189,28 @@ __device__ void diag_source_sink(const MccP &P, long long slot, int c, int sp, i
 }
 
 __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsigned int *n_cand_local) {
-    float fvx = P.VX[slot];
+    const long long st = mslot(P, P.sp, slot);   // where the incident's record is
+    float fvx = P.VX[st];
     if (isnan(fvx)) return;
     (*n_cand_local)++;
     const int sp = P.sp;
     Rng R;
     R.ctr = U4{(uint32_t)slot, P.it, (uint32_t)sp | 0x4D430000u, (uint32_t)P.diag};  // the diagnostic pass: own stream
     R.k0 = P.k0; R.k1 = P.k1; R.used = 4;
-    const double vx1 = fvx, vy1 = P.VY[slot], vz1 = P.VZ[slot];
+    const double vx1 = fvx, vy1 = P.VY[st], vz1 = P.VZ[st];
     const double mp = fabs(P.mass[sp]);
     int rg = -1;
-    if (P.n_rg > 0) rg = region_of(P, (int)(P.X[slot] >> P.S) + 1, (int)(P.Y[slot] >> P.S) + 1);
+    if (P.n_rg > 0) rg = region_of(P, (int)(P.X[st] >> P.S) + 1, (int)(P.Y[st] >> P.S) + 1);
     // per target species: drawn velocity and CM quantities (collision_OMP :336-482)
     double tvx[LEPIC_MAXSP], tvy[LEPIC_MAXSP], tvz[LEPIC_MAXSP], mu[LEPIC_MAXSP], vr[LEPIC_MAXSP];
     double vcx[LEPIC_MAXSP], vcy[LEPIC_MAXSP], vcz[LEPIC_MAXSP];
-    long long tslot[LEPIC_MAXSP];   // the DSMC target of a charged target species (-1: none)
+    long long tslot[LEPIC_MAXSP];   // the DSMC target's record of a charged target species (-1: none)
     double np_t[LEPIC_MAXSP];
 #pragma unroll
     for (int t = 0; t < LEPIC_MAXSP; t++) tslot[t] = -1;
     unsigned drawn = 0;
     int cx = 0, cy = 0;
-    if (P.dsmc) { cx = (int)(P.X[slot] >> P.S); cy = (int)(P.Y[slot] >> P.S); }
+    if (P.dsmc) { cx = (int)(P.X[st] >> P.S); cy = (int)(P.Y[st] >> P.S); }
     double nu[MCC_MAX_REACTIONS];
     double sum_nu = 0.0;
     for (int q = 0; q < P.ncol_sp; q++) {
@@ -222,11 +231,12 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             } else {
                 // the target particle (:339-403) if this candidate holds its claim, and the
                 // target density at the incident's cell (:524-528)
-                long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));
-                if (t >= 0 && ((!P.diag && P.claim[tt][t] != (int)slot) || isnan(P.TVX[tt][t]))) t = -1;
-                tslot[tt] = t;
+                long long t = pick_target(P, tt, cx, cy, dsmc_draw(P, slot, tt));   // a position
+                const long long ts = t >= 0 ? mslot(P, tt, t) : -1;                  // its record
+                if (t >= 0 && ((!P.diag && P.claim[tt][t] != (int)slot) || isnan(P.TVX[tt][ts]))) t = -1;
+                tslot[tt] = t >= 0 ? ts : -1;
                 a = b = z = 0.0;
-                if (t >= 0) { a = P.TVX[tt][t]; b = P.TVY[tt][t]; z = P.TVZ[tt][t]; }
+                if (t >= 0) { a = P.TVX[tt][ts]; b = P.TVY[tt][ts]; z = P.TVZ[tt][ts]; }
                 const long long m = (cx + 1) + (long long)(cy + 1) * P.W + tt * P.nn;
                 np_t[tt] = 0.25 * (P.np_red[m] + P.np_red[m + 1] + P.np_red[m + P.W] + P.np_red[m + P.W + 1]);
             }
@@ -251,7 +261,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             atomicAdd(&P.tal->cnt_col[0][c][rg], nu[q] * nu_max);
             atomicAdd(&P.tal->cnt_col[1][c][rg], 1.0);
         }
-        if (P.diag) diag_source_sink(P, slot, c, sp, tt, nu[q] * nu_max);
+        if (P.diag) diag_source_sink(P, st, c, sp, tt, nu[q] * nu_max);
     }
     if (P.diag) return;   // collisions.f90:649: flag_diag makes every event a null collision
     // :619 indexx: reactions ordered by ascending nu (straight insertion, stable); the order
@@ -277,7 +287,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
     const int tt = ci[2 + n_re - 1];
     atomicAdd(&P.cnt->n_coll[c], 1ull);
     if (rg >= 0) atomicAdd(&P.tal->cnt_col[2][c][rg], P.tal->inv_np_rg[sp][rg]); // :1026-1033
-    const uint32_t X = P.X[slot], Y = P.Y[slot];
+    const uint32_t X = P.X[st], Y = P.Y[st];
     const double v2in = v2f(fvx, (float)vy1, (float)vz1);
     if (rt == 4) { // charge exchange :942-1000: the incident ion takes the neutral's velocity
         for (int ib = 0; ib < n_by; ib++) {
@@ -285,7 +295,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             if (P.mass[bt] <= 0.0) continue;
             if (bt == sp) {
                 const float a = (float)tvx[tt], b = (float)tvy[tt], cz = (float)tvz[tt];
-                P.VX[slot] = a; P.VY[slot] = b; P.VZ[slot] = cz;
+                P.VX[st] = a; P.VY[st] = b; P.VZ[st] = cz;
                 atomicAdd(&P.tal->P3[sp], P.Ek_half[sp] * (v2f(a, b, cz) - v2in)); // :980-983
             } else if (bt == tt && P.charge[tt] != 0.0 && tslot[tt] >= 0) {
                 // a charged target takes the incident's velocity (:955-978)
@@ -376,7 +386,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
         atomicAdd(&P.tal->P3[bt], P.Ek_half[bt] * (v2f((float)vbx, (float)vby, (float)vbz) - (to_incident ? v2in : 0.0)));
         if (to_incident) {
             incident_kept = true;
-            P.VX[slot] = (float)vbx; P.VY[slot] = (float)vby; P.VZ[slot] = (float)vbz;
+            P.VX[st] = (float)vbx; P.VY[st] = (float)vby; P.VZ[st] = (float)vbz;
         } else {
             if (P.ss_map)   // collisions.f90:809: a created particle at the incident's (ix, iy)
                 atomicAdd(P.ss_map + (size_t)(2 * bt) * P.ss_nn + ((X >> P.S) + 1) + (long long)((Y >> P.S) + 1) * P.ss_W, 1u);
@@ -386,7 +396,7 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
                 pr.key = (unsigned long long)slot * 8ull + (unsigned long long)ib;
                 pr.X = X; pr.Y = Y;
                 pr.vx = (float)vbx; pr.vy = (float)vby; pr.vz = (float)vbz;
-                pr.z = P.Z ? P.Z[slot] : 0.0f;   // collisions.f90:813: the incident's z
+                pr.z = P.Z ? P.Z[st] : 0.0f;   // collisions.f90:813: the incident's z
                 P.prod[bt][k] = pr;
             } else {
                 set_err(P.cnt, LERR_CAPACITY, 200);
@@ -399,10 +409,10 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
         if (P.mass[ct] <= 0.0) continue;
         if (ct == sp && !incident_kept && ire == 0) {
             atomicAdd(&P.tal->P3[sp], -P.Ek_half[sp] * v2in);  // removal in the mover (part_expmover.f90:91-95)
-            P.VX[slot] = __int_as_float(HOLE_NAN);
+            P.VX[st] = __int_as_float(HOLE_NAN);
             if (P.ss_map)   // collisions.f90:931: the removed particle, at the incident's (ix, iy)
-                atomicAdd(P.ss_map + (size_t)(2 * sp + 1) * P.ss_nn + ((P.X[slot] >> P.S) + 1) +
-                              (long long)((P.Y[slot] >> P.S) + 1) * P.ss_W, 1u);
+                atomicAdd(P.ss_map + (size_t)(2 * sp + 1) * P.ss_nn + ((P.X[st] >> P.S) + 1) +
+                              (long long)((P.Y[st] >> P.S) + 1) * P.ss_W, 1u);
             atomicAdd(&P.cnt->n_dead[sp], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[sp], (unsigned long long)-1ll);
         }
@@ -411,8 +421,8 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
             atomicAdd(&P.tal->P3[tt], -P.Ek_half[tt] * v2f(P.TVX[tt][t], P.TVY[tt][t], P.TVZ[tt][t]));
             P.TVX[tt][t] = __int_as_float(HOLE_NAN);
             if (P.ss_map)
-                atomicAdd(P.ss_map + (size_t)(2 * tt + 1) * P.ss_nn + ((P.X[slot] >> P.S) + 1) +
-                              (long long)((P.Y[slot] >> P.S) + 1) * P.ss_W, 1u);
+                atomicAdd(P.ss_map + (size_t)(2 * tt + 1) * P.ss_nn + ((P.X[st] >> P.S) + 1) +
+                              (long long)((P.Y[st] >> P.S) + 1) * P.ss_W, 1u);
             atomicAdd(&P.cnt->n_dead[tt], 1ull);
             atomicAdd((unsigned long long *)&P.cnt->n_alive[tt], (unsigned long long)-1ll);
         }
@@ -490,8 +500,9 @@ __global__ void __launch_bounds__(MCC_THREADS) k_mcc_claim(MccP P, const int *ca
     const long long m = P.cnt->n_cand_list;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
         const long long slot = cand[i];
-        if (isnan(P.VX[slot])) continue;
-        const int cx = (int)(P.X[slot] >> P.S), cy = (int)(P.Y[slot] >> P.S);
+        const long long st = mslot(P, P.sp, slot);
+        if (isnan(P.VX[st])) continue;
+        const int cx = (int)(P.X[st] >> P.S), cy = (int)(P.Y[st] >> P.S);
         unsigned done = 0;
         for (int k = 0; k < P.ncol_sp; k++) {
             const int *ci = P.col_info + P.cols[k] * 10;
@@ -531,7 +542,7 @@ __global__ void k_nu_max(NuMaxP P) {
 // Ordered append of one species' products after its occupied slots (single CTA).
 __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long long *sortbuf,
                              uint32_t *X, uint32_t *Y, float *VX, float *VY, float *VZ, float *Z, long long cap,
-                             DevCounters *cnt, int mcc) {
+                             DevCounters *cnt, int mcc, int ind) {
     __shared__ unsigned long long sm[4096];
     int n = (int)min(cnt->prod_count[sp], (unsigned int)prod_cap);
     if (n == 0) return;
@@ -539,10 +550,13 @@ __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long 
     for (int q = threadIdx.x; q < n; q += blockDim.x) a[q] = (prod[q].key << 24) | (unsigned long long)q;
     __syncthreads();
     bitonic_sort(a, n, threadIdx.x, blockDim.x, BlockSync());
-    const long long base = cnt->n_slots[sp];
+    // positions n_slots.. of the sorted order; with a pending permutation their records go after
+    // the slots the buffer held before the sort
+    const long long pos = cnt->n_slots[sp];
+    const long long base = ind ? cnt->ind_old[sp] + (pos - cnt->n_sorted[sp]) : pos;
     int m = n;
     if (base + m > cap) {
-        m = (int)(cap - base);
+        m = (int)max(cap - base, 0ll);
         if (threadIdx.x == 0) set_err(cnt, LERR_CAPACITY, 201);
     }
     for (int q = threadIdx.x; q < m; q += blockDim.x) {
@@ -553,7 +567,7 @@ __global__ void k_mcc_commit(int sp, Product *prod, int prod_cap, unsigned long 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        cnt->n_slots[sp] = base + m;
+        cnt->n_slots[sp] = pos + m;
         cnt->n_alive[sp] += m;
         if (mcc) cnt->n_add[sp] += (unsigned long long)m;
         cnt->prod_count[sp] = 0;
@@ -643,6 +657,7 @@ int mcc_collide(lepic_ctx *c, int it, bool diag) {
         for (int t = 0; t < g.ntype; t++) P.nm_vc[t] = g.Nm[t] / (g.dx * g.dy * g.zmax);
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
         P.Z = B.Z[B.cur];
+        for (int t = 0; t < g.ntype; t++) P.pind[t] = c->sp[t].ind ? c->sp[t].pind : nullptr;
         for (int t = 0; t < g.ntype; t++) { P.prod[t] = c->sp[t].prod; P.prod_cap[t] = c->sp[t].prod_cap; }
         P.cnt = c->dcnt;
         P.nu_max = c->nu_max[s];
@@ -713,7 +728,7 @@ int commit_products(lepic_ctx *c, int sp, bool mcc) {
     SpeciesBuf &B = c->sp[sp];
     k_mcc_commit<<<1, 1024, 0, c->stream>>>(sp, B.prod, B.prod_cap, c->prod_sort, B.X[B.cur], B.Y[B.cur],
                                             B.VX[B.cur], B.VY[B.cur], B.VZ[B.cur], B.Z[B.cur], B.cap, c->dcnt,
-                                            mcc ? 1 : 0);
+                                            mcc ? 1 : 0, B.ind ? 1 : 0);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }

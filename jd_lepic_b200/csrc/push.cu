@@ -28,6 +28,11 @@ struct PushP {
     int nx, ny, S, W;
     uint32_t *X, *Y;
     float *VX, *VY, *VZ;
+    // a sort's pending permutation (IND): position j is read from record
+    // ind_slot(pind, n_sorted, ind_old, j) of these arrays and written to X..VZ above at j
+    const uint32_t *Xi, *Yi;
+    const float *VXi, *VYi, *VZi;
+    const int *pind;
     const float4 *E;           // node pairs: (Ex, Ey)[n], (Ex, Ey)[n+1]
     const float4 *B;
     float Bcx, Bcy, Bcz;
@@ -364,13 +369,14 @@ __device__ __forceinline__ bool zstep(const PushP &P, int i, uint32_t &X, uint32
 // A work item's range is rounded down to multiples of 8 slots at both ends, so consecutive items
 // still tile the slot array exactly; particles a rounded range takes from a neighbouring
 // tile reach the global grid when they fall outside the window.
-template <int BMODE, bool GEN, bool MOVE, bool MOM>
+template <int BMODE, bool GEN, bool MOVE, bool MOM, bool IND>
 __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
     __shared__ unsigned int s_lost;
     DevCounters *cnt = P.cnt;
     const long long n_slots = cnt->n_slots[P.sp], n_sorted = cnt->n_sorted[P.sp];
+    const long long ind_old = IND ? cnt->ind_old[P.sp] : 0;
     const int n_items = cnt->n_items[P.sp];
     const long long tail0 = n_sorted & ~7ll;
     for (;;) {
@@ -411,16 +417,48 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                 const int bn = base + PUSH_G * PUSH_THREADS;
                 if (bn < end) {
                     const uint32_t nb = (uint32_t)((min(PUSH_G * PUSH_THREADS, end - bn) + 7) & ~7) * 4u;
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.X + bn), "r"(nb) : "memory");
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.Y + bn), "r"(nb) : "memory");
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VX + bn), "r"(nb) : "memory");
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VY + bn), "r"(nb) : "memory");
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VZ + bn), "r"(nb) : "memory");
+                    if (!IND) {
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.X + bn), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.Y + bn), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VX + bn), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VY + bn), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VZ + bn), "r"(nb) : "memory");
+                    } else if (bn < n_sorted) {
+                        // the permutation of the next iteration, and the records from where it starts
+                        // (the permutation is close to a shift inside a tile)
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.pind + bn), "r"(nb) : "memory");
+                        const long long s0 = (long long)P.pind[bn] & ~3ll;
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.Xi + s0), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.Yi + s0), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VXi + s0), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VYi + s0), "r"(nb) : "memory");
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(P.VZi + s0), "r"(nb) : "memory");
+                    }
                 }
             }
             uint32_t X[PUSH_G], Y[PUSH_G];
             float vx[PUSH_G], vy[PUSH_G], vz[PUSH_G];
-            if (grp_ok) {   // storage is whole groups of 8: the last, partial group is masked below
+            if (grp_ok && IND) {
+                // position j of the sorted order from its record in the input buffer
+                int sl[PUSH_G];
+                if (g + PUSH_G <= n_sorted) {
+                    const int4 pm = *reinterpret_cast<const int4 *>(P.pind + g);
+                    sl[0] = pm.x; sl[1] = pm.y; sl[2] = pm.z; sl[3] = pm.w;
+                } else {
+#pragma unroll
+                    for (int p = 0; p < PUSH_G; p++) sl[p] = (int)ind_slot(P.pind, n_sorted, ind_old, (long long)(g + p));
+                }
+#pragma unroll
+                for (int p = 0; p < PUSH_G; p++) {
+                    if (g + p < end) {
+                        const int s = sl[p];
+                        X[p] = __ldg(P.Xi + s); Y[p] = __ldg(P.Yi + s);
+                        vx[p] = __ldg(P.VXi + s); vy[p] = __ldg(P.VYi + s); vz[p] = __ldg(P.VZi + s);
+                    } else {
+                        X[p] = 0u; Y[p] = 0u; vx[p] = __int_as_float(HOLE_NAN); vy[p] = 0.0f; vz[p] = 0.0f;
+                    }
+                }
+            } else if (grp_ok) {   // storage is whole groups of 8: the last, partial group is masked below
                 const uint4 x0 = *reinterpret_cast<const uint4 *>(P.X + g);
                 const uint4 y0 = *reinterpret_cast<const uint4 *>(P.Y + g);
                 const float4 a0 = *reinterpret_cast<const float4 *>(P.VX + g);
@@ -521,33 +559,35 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     }
 }
 
-template <int BMODE, bool GEN, bool MOVE, bool MOM>
+template <int BMODE, bool GEN, bool MOVE, bool MOM, bool IND>
 static int launch_one(lepic_ctx *c, PushP &P, size_t smem) {
     static bool attr_set[64] = {false};
     if (!attr_set[c->dev & 63]) {
-        LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE, MOM>,
+        LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE, MOM, IND>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         attr_set[c->dev & 63] = true;
     }
     int occ = 0;
-    LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE, MOM>, PUSH_THREADS,
-                                                        smem));
-    k_push_deposit<BMODE, GEN, MOVE, MOM><<<c->num_sms * std::max(1, occ), PUSH_THREADS, smem, c->stream>>>(P);
+    LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE, MOM, IND>,
+                                                        PUSH_THREADS, smem));
+    k_push_deposit<BMODE, GEN, MOVE, MOM, IND><<<c->num_sms * std::max(1, occ), PUSH_THREADS, smem, c->stream>>>(P);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
 }
 
+// ind: the fast mover reading through a pending permutation (only without the general mover)
 template <int BMODE, bool MOM>
-static int launch_m(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
-    if (!move) return launch_one<BMODE, false, false, MOM>(c, P, smem);
-    return gen ? launch_one<BMODE, true, true, MOM>(c, P, smem) : launch_one<BMODE, false, true, MOM>(c, P, smem);
+static int launch_m(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move, bool ind) {
+    if (!move) return launch_one<BMODE, false, false, MOM, false>(c, P, smem);
+    if (gen) return launch_one<BMODE, true, true, MOM, false>(c, P, smem);
+    return ind ? launch_one<BMODE, false, true, MOM, true>(c, P, smem) : launch_one<BMODE, false, true, MOM, false>(c, P, smem);
 }
 
 // moments deposit where the weights are exact (2S <= LEPIC_DEP_SHIFT, grids of 1024 and up)
 template <int BMODE>
-static int launch_b(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move) {
-    return 2 * P.S <= LEPIC_DEP_SHIFT ? launch_m<BMODE, true>(c, P, smem, gen, move)
-                                      : launch_m<BMODE, false>(c, P, smem, gen, move);
+static int launch_b(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move, bool ind) {
+    return 2 * P.S <= LEPIC_DEP_SHIFT ? launch_m<BMODE, true>(c, P, smem, gen, move, ind)
+                                      : launch_m<BMODE, false>(c, P, smem, gen, move, ind);
 }
 
 // Refluxing (part_expmover.f90:445-470), one thread per event of this species' push: vx from
@@ -695,7 +735,20 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         PushP P;
         memset(&P, 0, sizeof(P));
         P.nx = g.nx; P.ny = g.ny; P.S = c->S; P.W = g.nx + 3;
+        // a pending permutation: the fast mover reads through it and writes the sorted order into
+        // the other buffer; anything else moves the records first
+        if (B.ind && (!move || push_needs_general(c, s))) {
+            const int r = materialize_species(c, s);
+            if (r != LEPIC_OK) return r;
+        }
+        const bool ind = B.ind;
         P.X = B.X[B.cur]; P.Y = B.Y[B.cur]; P.VX = B.VX[B.cur]; P.VY = B.VY[B.cur]; P.VZ = B.VZ[B.cur];
+        if (ind) {
+            P.Xi = P.X; P.Yi = P.Y; P.VXi = P.VX; P.VYi = P.VY; P.VZi = P.VZ;
+            P.pind = B.pind;
+            const int o = 1 - B.cur;
+            P.X = B.X[o]; P.Y = B.Y[o]; P.VX = B.VX[o]; P.VY = B.VY[o]; P.VZ = B.VZ[o];
+        }
         P.E = c->Ef; P.B = c->Bf;
         int bmode = g.flag_B;
         if (g.flag_B_pos == 1 && g.charge[s] > 0.0) bmode = 0; // :185
@@ -782,10 +835,14 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         // the boundary options, the 3rd dimension and the wall models take the general mover
         const bool gen = P.pbc || P.nmn || P.negion_nmn || P.Z || P.dq || P.reflux || P.sec_label;
         int r;
-        if (bmode == 1) r = launch_b<1>(c, P, smem, gen, move);
-        else if (bmode == 2) r = launch_b<2>(c, P, smem, gen, move);
-        else r = launch_b<0>(c, P, smem, gen, move);
+        if (bmode == 1) r = launch_b<1>(c, P, smem, gen, move, ind);
+        else if (bmode == 2) r = launch_b<2>(c, P, smem, gen, move, ind);
+        else r = launch_b<0>(c, P, smem, gen, move, ind);
         if (r != LEPIC_OK) return r;
+        if (ind) {   // the sorted order now sits in the other buffer
+            B.cur = 1 - B.cur;
+            B.ind = false;
+        }
         const int eg = c->num_sms * 2;
         if (P.reflux) {
             R.ev = c->rf_ev; R.count = c->ev_count; R.cap = c->ev_cap; R.sp = s; R.S = c->S; R.W = P.W;
@@ -807,4 +864,11 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
     // the secondary electrons of this push, appended in the order of their ions' slots
     if (any_sec) return commit_products(c, 0, false);
     return LEPIC_OK;
+}
+
+bool push_needs_general(const lepic_ctx *c, int s) {
+    const lepic_config &g = c->cfg;
+    double vb, fm, vt, sn, cs;
+    return g.flag_pbc || g.flag_nmn || (c->zloss && c->sp[s].Z[0]) || c->dq ||
+           sources_reflux(c, s, &vb, &fm, &vt, &sn, &cs) || (c->sec_label > 0 && c->sec_gam > 0.0 && g.charge[s] > 0.0);
 }

@@ -399,6 +399,7 @@ __global__ void k_items(const int *offsets, int ntiles, int keys_per_tile, WorkI
         int nitems = carry;
         if (nitems > max_items) { set_err(cnt, LERR_CAPACITY, 300); nitems = max_items; }
         long long total = offsets[nkeys];
+        cnt->ind_old[sp] = cnt->n_slots[sp];
         cnt->n_items[sp] = nitems;
         cnt->n_slots[sp] = total;
         cnt->n_sorted[sp] = total;
@@ -406,12 +407,25 @@ __global__ void k_items(const int *offsets, int ntiles, int keys_per_tile, WorkI
     }
 }
 
-int sort_species(lepic_ctx *c, int sp) {
+int sort_species(lepic_ctx *c, int sp, bool defer) {
     SpeciesBuf &B = c->sp[sp];
     const int cur = B.cur, nxt = 1 - cur;
     auto log2_or = [](int v) { int l = 0; while ((1 << l) < v) l++; return (1 << l) == v ? l : -1; };
     KeyP K{c->S, c->cfg.nx, c->cfg.ny, c->tw, c->th, c->ntx, log2_or(c->tw), log2_or(c->th)};
     if (K.twl < 0 || K.thl < 0) K.twl = K.thl = -1;
+    if (B.ind) {   // a permutation still pending: move its records first
+        int r = materialize_species(c, sp);
+        if (r != LEPIC_OK) return r;
+        return sort_species(c, sp, defer);
+    }
+    if (defer && B.Z[0]) defer = false;   // the push that ends the pending state does not carry z
+    if (defer && !B.pind) {
+        if (cudaMalloc((void **)&B.pind, sizeof(int) * (size_t)std::max(B.cap, 8ll)) != cudaSuccess) {
+            c->last_err = "sort: cudaMalloc of the pending permutation failed";
+            return LEPIC_ENOMEM;
+        }
+    }
+    int *perm = defer ? B.pind : c->perm;
     const long long nk = c->nkeys;
     int grid = c->num_sms * 8;
     LCUDA(cudaMemsetAsync(c->counts, 0, sizeof(int) * (nk + 1), c->stream));
@@ -424,18 +438,53 @@ int sort_species(lepic_ctx *c, int sp) {
     k_scan_top<<<1, 1024, 0, c->stream>>>(c->blocksums, nb);
     k_scan_final<<<nb, SORT_THREADS, 0, c->stream>>>(c->counts, nk, c->blocksums, c->offsets);
     LCUDA(cudaMemcpyAsync(c->cursor, c->offsets, sizeof(int) * nk, cudaMemcpyDeviceToDevice, c->stream));
-    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, B.items, c->dcnt, sp, c->cursor, c->perm);
-    k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, nk, c->perm, c->bigseg, c->dcnt);
-    k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, c->perm, c->bigseg, c->dcnt);
-    k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(c->perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
-                                                   B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt], B.VX[nxt],
-                                                   B.VY[nxt], B.VZ[nxt], B.Z[cur], B.Z[nxt]);
+    k_scatter<<<grid, SORT_THREADS, 0, c->stream>>>(c->keys, B.items, c->dcnt, sp, c->cursor, perm);
+    k_segsort_warp<<<grid, SORT_THREADS, 0, c->stream>>>(c->offsets, nk, perm, c->bigseg, c->dcnt);
+    k_segsort_big<<<c->num_sms, 512, 0, c->stream>>>(c->offsets, perm, c->bigseg, c->dcnt);
+    if (!defer)
+        k_gather<<<grid, SORT_THREADS, 0, c->stream>>>(perm, c->offsets, nk, B.X[cur], B.Y[cur], B.VX[cur],
+                                                       B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt], B.VX[nxt],
+                                                       B.VY[nxt], B.VZ[nxt], B.Z[cur], B.Z[nxt]);
     k_items<<<1, 1024, 0, c->stream>>>(c->offsets, c->ntiles, c->tw * c->th, B.items, B.max_items,
                                        c->dcnt, sp, nk);
     LCUDA(cudaGetLastError());
     // the cell lists of this order (sorting.f90's Plist) for the DSMC target search
     if (B.cell_off)
         LCUDA(cudaMemcpyAsync(B.cell_off, c->offsets, sizeof(int) * (nk + 1), cudaMemcpyDeviceToDevice, c->stream));
+    if (defer) B.ind = true;   // the records stay in buffer cur until the push
+    else B.cur = nxt;
+    return LEPIC_OK;
+}
+
+// the gather of a pending permutation over every position of the sorted order, the products
+// appended since included; holes are carried as they are (the next sort drops them)
+__global__ void k_gather_ind(const int *pind, const DevCounters *cnt, int sp, const uint32_t *X, const uint32_t *Y,
+                             const float *VX, const float *VY, const float *VZ, uint32_t *X2, uint32_t *Y2,
+                             float *VX2, float *VY2, float *VZ2) {
+    const long long n = cnt->n_slots[sp], ns = cnt->n_sorted[sp], old = cnt->ind_old[sp];
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const long long i = ind_slot(pind, ns, old, j);
+        X2[j] = X[i]; Y2[j] = Y[i]; VX2[j] = VX[i]; VY2[j] = VY[i]; VZ2[j] = VZ[i];
+    }
+}
+
+int materialize_species(lepic_ctx *c, int sp) {
+    SpeciesBuf &B = c->sp[sp];
+    if (!B.ind) return LEPIC_OK;
+    const int cur = B.cur, nxt = 1 - cur;
+    k_gather_ind<<<c->num_sms * 8, SORT_THREADS, 0, c->stream>>>(B.pind, c->dcnt, sp, B.X[cur], B.Y[cur], B.VX[cur],
+                                                                  B.VY[cur], B.VZ[cur], B.X[nxt], B.Y[nxt],
+                                                                  B.VX[nxt], B.VY[nxt], B.VZ[nxt]);
+    LCUDA(cudaGetLastError());
     B.cur = nxt;
+    B.ind = false;
+    return LEPIC_OK;
+}
+
+int materialize_all(lepic_ctx *c) {
+    for (int s = 0; s < c->cfg.ntype; s++) {
+        const int r = materialize_species(c, s);
+        if (r != LEPIC_OK) return r;
+    }
     return LEPIC_OK;
 }

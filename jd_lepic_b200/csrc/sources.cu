@@ -842,6 +842,7 @@ extern "C" int lepic_gpu_set_sources(lepic_ctx *c, const lepic_source_config *cf
 
 extern "C" int lepic_gpu_set_heating(lepic_ctx *c, const double *vt, int32_t n_icp, double Pabs_cor) {
     if (!c || !vt || !state(c)) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     SrcState *S = state(c);
     if (n_icp != S->cfg.n_icp) { c->last_err = "set_heating: n_icp differs from the source config"; return LEPIC_EINVAL; }
     for (int b = 0; b < n_icp; b++)
@@ -1032,21 +1033,25 @@ static int te_update(lepic_ctx *c) {
 
 extern "C" int lepic_gpu_eheating(lepic_ctx *c, int32_t it) {
     if (!c || !state(c) || !state(c)->cfg.flag_heat) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return run_heating(c, it);
 }
 
 extern "C" int lepic_gpu_part_injection(lepic_ctx *c, int32_t it) {
     if (!c || !state(c) || !state(c)->cfg.flag_inj) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return run_injection(c, it);
 }
 
 extern "C" int lepic_gpu_flux_emitter(lepic_ctx *c, int32_t it) {
     if (!c || !state(c) || !(state(c)->cfg.js > 0.0)) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return run_emitter(c, it);
 }
 
 extern "C" int lepic_gpu_heating_tally(lepic_ctx *c) {
     if (!c || !state(c)) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     return run_tally(c);
 }
 
@@ -1092,6 +1097,8 @@ extern "C" int lepic_gpu_source_tallies(lepic_ctx *c, lepic_source_tally *out, i
 int sources_before_push(lepic_ctx *c, int it) {
     SrcState *S = state(c);
     if (!S || !S->cfg.flag_heat || it % S->cfg.ns_heat != 0) return LEPIC_OK;
+    const int rm = materialize_all(c);   // the heating reads the records in sorted order
+    if (rm != LEPIC_OK) return rm;
     const lepic_source_config &s = S->cfg;
     if (s.te_update && s.Pabs[0] > 0.0 && !s.flag_inj) {
         int r;

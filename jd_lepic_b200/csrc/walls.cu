@@ -49,6 +49,7 @@ int zloss_after_avg(lepic_ctx *c, const double *data, int na1, int na2, int size
 
 extern "C" int lepic_gpu_set_zloss(lepic_ctx *c, const lepic_zloss_config *z) {
     if (!c || !z) return LEPIC_EINVAL;
+    if (const int rm = materialize_all(c)) return rm;   // records of a pending sort moved first
     const lepic_config &g = c->cfg;
     if (z->hz < 0.0) {   // the reference's "no losses in the 3rd dimension" (read_input.f90:162)
         c->zloss = 0;
