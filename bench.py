@@ -554,8 +554,9 @@ def run_ours(args):
         it = learned_compare(args, sim, lib, ctx, capi, stream, it, eps, pois, one_step)
 
     # end to end through the C ABI with host buffers: phi exchanged with pinned host memory
-    # every step (the Fortran host's array: uploaded before the solve, downloaded after it on
-    # the copy stream beside the E field and the push) and the particle counters read back
+    # every step (the Fortran host's array: downloaded after the solve and uploaded again as the
+    # next solve's input, both on the copy stream beside the E field and the push) and the
+    # particle counters read back
     e2e_steps = min(args.steps, 10)
     nn = (case.nx + 3) * (case.ny + 3)
     phi_host = torch.empty(nn, dtype=torch.float64, pin_memory=True)
@@ -567,15 +568,18 @@ def run_ours(args):
         dist.barrier()
     w0 = time.perf_counter()
     ne0 = n_end
-    for _ in range(e2e_steps):
+    sim.check(lib.lepic_gpu_stage_solver_input(ctx, php), "stage")   # the first step's input
+    for k in range(e2e_steps):
         sim.check(lib.lepic_gpu_calc_rhs(ctx, None), "calc_rhs")
-        sim.check(lib.lepic_gpu_iterative_solver_async(ctx, php, php, eps, mode), "solver")
+        sim.check(lib.lepic_gpu_iterative_solver_async(ctx, None, php, eps, mode), "solver")
         sim.check(lib.lepic_gpu_calc_efield(ctx, None), "efield")
         if it % 10 == 1:
             for s in range(sim.sp.ntype):
                 sim.check(lib.lepic_gpu_part_sorting(ctx, s, None), "sort")
         if it > 1 and it % 10 == 1:
             sim.check(lib.lepic_gpu_collisions(ctx, it, None), "collisions")
+        if k + 1 < e2e_steps:   # the next step's input, uploaded beside the push
+            sim.check(lib.lepic_gpu_stage_solver_input(ctx, php), "stage")
         sim.check(lib.lepic_gpu_push_deposit(ctx, it, C.byref(ps)), "push")
         reduce_rho()
         it += 1

@@ -199,6 +199,16 @@ int lepic_gpu_iterative_solver(lepic_ctx *ctx, double *phi_inout, double eps, in
  * an output pointer or stats).  The host must not read or write phi_out before that. */
 int lepic_gpu_iterative_solver_async(lepic_ctx *ctx, const double *phi_in, double *phi_out, double eps,
                                      int32_t mode);
+/* Stages the next solve's phi input now, on the copy stream: the host array is copied into phi
+ * after the work enqueued so far (the E field that reads phi) and after the copy stream's earlier
+ * copies (a download into the same array), beside the kernels enqueued next (the push); the next
+ * call that reads or writes phi waits for it.  It is the phi_in of the next
+ * lepic_gpu_iterative_solver[_async] call (which then passes NULL), moved off the critical path:
+ * a host that keeps phi on its side every step calls
+ *   solve_async(NULL, phi) -> efield -> [sort, collisions] -> stage_solver_input(phi) -> push
+ * and every step still copies phi both ways.  phi_in must stay unchanged until a call that
+ * synchronises the context returns. */
+int lepic_gpu_stage_solver_input(lepic_ctx *ctx, const double *phi_in);
 /* Warm start of the mixed-precision solve (mode 1): 0 (default) starts from the input phi, as
  * iterative_solver does with its in/out u; 1 starts from the linear extrapolation
  * 2 phi_(n-1) - phi_(n-2) of the inputs of this and the previous solve, for a time loop in

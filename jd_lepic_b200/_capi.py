@@ -218,6 +218,7 @@ PROTOTYPES = {
     "lepic_gpu_iterative_solver": (C.c_int, [_VP, _DP, C.c_double, C.c_int32, C.POINTER(LepicSolveStats)]),
     "lepic_gpu_iterative_solver_async": (C.c_int, [_VP, _DP, _DP, C.c_double, C.c_int32]),
     "lepic_gpu_get_grid_async": (C.c_int, [_VP, C.c_int32, _DP]),
+    "lepic_gpu_stage_solver_input": (C.c_int, [_VP, _DP]),
     "lepic_gpu_calc_efield": (C.c_int, [_VP, _DP]),
     "lepic_gpu_part_sorting": (C.c_int, [_VP, C.c_int32, _IP]),
     "lepic_gpu_collisions": (C.c_int, [_VP, C.c_int32, C.POINTER(LepicMccStats)]),

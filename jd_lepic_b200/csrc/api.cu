@@ -665,7 +665,16 @@ extern "C" int lepic_gpu_dens_red(lepic_ctx *c, double *np_red_out, double *np_m
     return LEPIC_OK;
 }
 
+// The context's stream waits for the copy stream's last copy: an upload from a host array
+// must not overtake a download into it, and the work that reads or writes phi must not overtake
+// a staged upload into phi (lepic_gpu_stage_solver_input).
+int wait_copies(lepic_ctx *c) {
+    if (c->copy_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
+    return LEPIC_OK;
+}
+
 static int solve(lepic_ctx *c, double eps, int mode) {
+    if (const int r = wait_copies(c)) return r;
     if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps, true);
     if (mode == LEPIC_POISSON_FP64_PCG) return mg_mixed_solve(c, eps, true, true);
     c->have_hist = 0;   // any other solver: the next mixed solve starts from its answer as it is
@@ -676,24 +685,14 @@ static int solve(lepic_ctx *c, double eps, int mode) {
     return LEPIC_EINVAL;
 }
 
-// An upload from a host array must not overtake a download into the same array that is still
-// in flight: the context's stream waits for the copy stream's last download first.
-static int wait_downloads(lepic_ctx *c) {
-    if (c->copy_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
-    return LEPIC_OK;
-}
-
 // Enqueues the download of `bytes` from the device array `src` into the host array `out`
 // without waiting for it: a device-to-device snapshot on the context's stream (ordered after
 // the work that produced src, ~10 us for a 2049^2 potential), then the device-to-host copy of the
 // snapshot on the copy stream, where it runs beside the kernels enqueued next.  The snapshot is
 // reused by the next download only after this one has completed.
+static int copy_stream(lepic_ctx *c);
 static int download_async(lepic_ctx *c, void *out, const void *src, size_t bytes) {
-    if (!c->cstream) {
-        LCUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
-        LCUDA(cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming));
-        LCUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
-    }
+    if (const int r = copy_stream(c)) return r;
     if (c->snap_bytes < bytes) {
         int r = sync_counters(c);   // no copy may still read the old snapshot
         if (r != LEPIC_OK) return r;
@@ -703,7 +702,7 @@ static int download_async(lepic_ctx *c, void *out, const void *src, size_t bytes
         if (cudaMalloc(&c->snap, bytes) != cudaSuccess) { c->last_err = "download snapshot: cudaMalloc failed"; return LEPIC_ENOMEM; }
         c->snap_bytes = bytes;
     }
-    int r = wait_downloads(c);
+    int r = wait_copies(c);
     if (r != LEPIC_OK) return r;
     LCUDA(cudaMemcpyAsync(c->snap, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
     LCUDA(cudaEventRecord(c->ev_snap, c->stream));
@@ -714,12 +713,37 @@ static int download_async(lepic_ctx *c, void *out, const void *src, size_t bytes
     return LEPIC_OK;
 }
 
+// the copy stream and its events, created with the first overlapped copy
+static int copy_stream(lepic_ctx *c) {
+    if (!c->cstream) {
+        LCUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+    }
+    return LEPIC_OK;
+}
+
+extern "C" int lepic_gpu_stage_solver_input(lepic_ctx *c, const double *phi_in) {
+    if (!c || !phi_in) return LEPIC_EINVAL;
+    int r = copy_stream(c);
+    if (r != LEPIC_OK) return r;
+    // after the work enqueued so far (the E field that reads phi) and after the copy stream's
+    // earlier copies (a download into phi_in), then the copy into phi; the next work that reads
+    // or writes phi waits for it
+    LCUDA(cudaEventRecord(c->ev_snap, c->stream));
+    LCUDA(cudaStreamWaitEvent(c->cstream, c->ev_snap, 0));
+    LCUDA(cudaMemcpyAsync(c->phi, phi_in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->cstream));
+    LCUDA(cudaEventRecord(c->ev_copied, c->cstream));
+    c->copy_pending = 1;
+    return LEPIC_OK;
+}
+
 extern "C" int lepic_gpu_iterative_solver_async(lepic_ctx *c, const double *phi_in, double *phi_out, double eps,
                                                 int32_t mode) {
     if (!c || !(eps > 0)) return LEPIC_EINVAL;
     int r;
     if (phi_in) {
-        if ((r = wait_downloads(c)) != LEPIC_OK) return r;
+        if ((r = wait_copies(c)) != LEPIC_OK) return r;
         LCUDA(cudaMemcpyAsync(c->phi, phi_in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
     }
     if ((r = solve(c, eps, mode)) != LEPIC_OK) return r;
@@ -740,7 +764,7 @@ extern "C" int lepic_gpu_iterative_solver(lepic_ctx *c, double *phi_inout, doubl
                                           lepic_solve_stats *st) {
     if (!c || !(eps > 0)) return LEPIC_EINVAL;
     if (phi_inout) {
-        int r = wait_downloads(c);
+        int r = wait_copies(c);
         if (r != LEPIC_OK) return r;
         LCUDA(cudaMemcpyAsync(c->phi, phi_inout, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
     }
@@ -835,6 +859,7 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
 
 extern "C" int lepic_gpu_get_grid(lepic_ctx *c, int32_t which, double *out) {
     if (!c || !out) return LEPIC_EINVAL;
+    if (const int r = wait_copies(c)) return r;   // a staged upload into phi
     const long long nn = c->nn;
     if (which == LEPIC_GRID_PHI) {
         LCUDA(cudaMemcpyAsync(out, c->phi, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
@@ -869,7 +894,7 @@ extern "C" int lepic_gpu_set_warm_start(lepic_ctx *c, int32_t mode) {
 
 extern "C" int lepic_gpu_set_grid(lepic_ctx *c, int32_t which, const double *in) {
     if (!c || !in) return LEPIC_EINVAL;
-    if (wait_downloads(c) != LEPIC_OK) return LEPIC_ECUDA;
+    if (wait_copies(c) != LEPIC_OK) return LEPIC_ECUDA;
     if (which == LEPIC_GRID_PHI) {
         LCUDA(cudaMemcpyAsync(c->phi, in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
         c->have_hist = 0;   // a potential from elsewhere: the next solve starts from it as it is

@@ -417,6 +417,8 @@ int sort_species(lepic_ctx *c, int ptype, bool defer = false);
 // moves the records of a pending permutation (the gather a deferred sort left out)
 int materialize_species(lepic_ctx *c, int ptype);
 int materialize_all(lepic_ctx *c);
+// the context's stream waits for the copies in flight on the copy stream (api.cu)
+int wait_copies(lepic_ctx *c);
 // true when the push of species s takes the general mover (boundary options, wall models,
 // the 3rd dimension); such a species' sort is not deferred
 bool push_needs_general(const lepic_ctx *c, int s);
