@@ -613,17 +613,20 @@ def run_ours(args):
         cb = cpu_baseline(args.config, args.cpu_cells, 5, 2, host_threads())
     line = None
     if rank == 0:
-        # kernels of this library launched in the timed steps (memsets/copies not counted):
-        # rhs 1, Poisson 1 (cooperative), E field 2, push 1 per species; a sort step adds 9 per
-        # species, a collision step 1 k_mcc per colliding species + 1 commit per species
+        # kernels of this library launched in the timed steps (memsets/copies not counted), as
+        # the ncu launch list shows them: rhs 1, the warm start's extrapolation 1 (mixed mode),
+        # Poisson 1 (cooperative), E field 2, push 1 per species; a sort step adds 8 per species
+        # (keys, three scan passes, scatter, two segment passes, work items; the records move in
+        # the push), a collision step the selection and the collisions per colliding species
+        # and the product commit per species
         n_mcc = sum(1 for s in range(sim.sp.ntype) if sim.xs.p_ncol[s] > 0)
         launches = 0
         for t in range(first_timed, first_timed + args.steps):
-            launches += 1 + 1 + 2 + sim.sp.ntype
+            launches += 1 + (1 if mode == capi.POISSON_MIXED_IR else 0) + 1 + 2 + sim.sp.ntype
             if t % 10 == 1:
-                launches += 9 * sim.sp.ntype
+                launches += 8 * sim.sp.ntype
             if t > 1 and t % 10 == 1:
-                launches += n_mcc + sim.sp.ntype
+                launches += 2 * n_mcc + sim.sp.ntype
         line = {
             "metric": "particle-steps/s per PIC step (push+deposit+MCC+sort+Poisson to 1e-8)",
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
