@@ -60,7 +60,8 @@ static void free_all(lepic_ctx *c) {
     if (c->hcnt) cudaFreeHost(c->hcnt);
     if (c->cstream) { cudaStreamSynchronize(c->cstream); cudaStreamDestroy(c->cstream); }
     if (c->ev_snap) cudaEventDestroy(c->ev_snap);
-    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+    if (c->ev_down) cudaEventDestroy(c->ev_down);
+    if (c->ev_up) cudaEventDestroy(c->ev_up);
     F(c->snap);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -375,9 +376,13 @@ extern "C" const char *lepic_gpu_last_error(lepic_ctx *c) { return c ? c->last_e
 static int sync_counters(lepic_ctx *c) {
     LCUDA(cudaMemcpyAsync(c->hcnt, c->dcnt, sizeof(DevCounters), cudaMemcpyDeviceToHost, c->stream));
     LCUDA(cudaStreamSynchronize(c->stream));
-    if (c->copy_pending) {
-        LCUDA(cudaEventSynchronize(c->ev_copied));
-        c->copy_pending = 0;
+    if (c->down_pending) {
+        LCUDA(cudaEventSynchronize(c->ev_down));
+        c->down_pending = 0;
+    }
+    if (c->up_pending) {
+        LCUDA(cudaEventSynchronize(c->ev_up));
+        c->up_pending = 0;
     }
     int e = c->hcnt->err;
     if (e) {
@@ -665,16 +670,25 @@ extern "C" int lepic_gpu_dens_red(lepic_ctx *c, double *np_red_out, double *np_m
     return LEPIC_OK;
 }
 
-// The context's stream waits for the copy stream's last copy: an upload from a host array
-// must not overtake a download into it, and the work that reads or writes phi must not overtake
-// a staged upload into phi (lepic_gpu_stage_solver_input).
-int wait_copies(lepic_ctx *c) {
-    if (c->copy_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
+// The context's stream waits for copies on the copy stream: the work that reads or writes phi
+// for a staged upload into phi (lepic_gpu_stage_solver_input); an upload from a host array, and
+// the reuse of the download snapshot, for the last download (into that array, out of the
+// snapshot).  A download alone holds up nothing else: the E field and the push run beside it.
+int wait_upload(lepic_ctx *c) {
+    if (c->up_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_up, 0));
     return LEPIC_OK;
+}
+static int wait_download(lepic_ctx *c) {
+    if (c->down_pending) LCUDA(cudaStreamWaitEvent(c->stream, c->ev_down, 0));
+    return LEPIC_OK;
+}
+static int wait_copies(lepic_ctx *c) {
+    if (const int r = wait_upload(c)) return r;
+    return wait_download(c);
 }
 
 static int solve(lepic_ctx *c, double eps, int mode) {
-    if (const int r = wait_copies(c)) return r;
+    if (const int r = wait_upload(c)) return r;
     if (mode == LEPIC_POISSON_MIXED_IR) return mg_mixed_solve(c, eps, true);
     if (mode == LEPIC_POISSON_FP64_PCG) return mg_mixed_solve(c, eps, true, true);
     c->have_hist = 0;   // any other solver: the next mixed solve starts from its answer as it is
@@ -708,8 +722,8 @@ static int download_async(lepic_ctx *c, void *out, const void *src, size_t bytes
     LCUDA(cudaEventRecord(c->ev_snap, c->stream));
     LCUDA(cudaStreamWaitEvent(c->cstream, c->ev_snap, 0));
     LCUDA(cudaMemcpyAsync(out, c->snap, bytes, cudaMemcpyDeviceToHost, c->cstream));
-    LCUDA(cudaEventRecord(c->ev_copied, c->cstream));
-    c->copy_pending = 1;
+    LCUDA(cudaEventRecord(c->ev_down, c->cstream));
+    c->down_pending = 1;
     return LEPIC_OK;
 }
 
@@ -718,7 +732,8 @@ static int copy_stream(lepic_ctx *c) {
     if (!c->cstream) {
         LCUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
         LCUDA(cudaEventCreateWithFlags(&c->ev_snap, cudaEventDisableTiming));
-        LCUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_down, cudaEventDisableTiming));
+        LCUDA(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
     }
     return LEPIC_OK;
 }
@@ -733,8 +748,8 @@ extern "C" int lepic_gpu_stage_solver_input(lepic_ctx *c, const double *phi_in) 
     LCUDA(cudaEventRecord(c->ev_snap, c->stream));
     LCUDA(cudaStreamWaitEvent(c->cstream, c->ev_snap, 0));
     LCUDA(cudaMemcpyAsync(c->phi, phi_in, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->cstream));
-    LCUDA(cudaEventRecord(c->ev_copied, c->cstream));
-    c->copy_pending = 1;
+    LCUDA(cudaEventRecord(c->ev_up, c->cstream));
+    c->up_pending = 1;
     return LEPIC_OK;
 }
 
@@ -859,7 +874,7 @@ extern "C" int lepic_gpu_step(lepic_ctx *c, int32_t it, double eps, int32_t mode
 
 extern "C" int lepic_gpu_get_grid(lepic_ctx *c, int32_t which, double *out) {
     if (!c || !out) return LEPIC_EINVAL;
-    if (const int r = wait_copies(c)) return r;   // a staged upload into phi
+    if (const int r = wait_upload(c)) return r;   // a staged upload into phi
     const long long nn = c->nn;
     if (which == LEPIC_GRID_PHI) {
         LCUDA(cudaMemcpyAsync(out, c->phi, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));

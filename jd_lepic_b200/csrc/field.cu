@@ -153,7 +153,7 @@ __global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *
 }
 
 int field_calc_efield(lepic_ctx *c) {
-    if (const int r = wait_copies(c)) return r;   // a staged upload into phi
+    if (const int r = wait_upload(c)) return r;   // a staged upload into phi
     const int nx = c->cfg.nx, ny = c->cfg.ny;
     int grid = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
     // E (FP64) lives in Ed[0..nn); the second half holds pass 1, which the wall pass reads

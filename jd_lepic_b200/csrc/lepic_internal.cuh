@@ -151,10 +151,11 @@ struct lepic_ctx {
     // downloads overlapped with the following work (lepic_gpu_iterative_solver_async,
     // lepic_gpu_get_grid_async): a device snapshot of the grid, copied to the host on cstream
     cudaStream_t cstream = nullptr;
-    cudaEvent_t ev_snap = nullptr, ev_copied = nullptr;
+    cudaEvent_t ev_snap = nullptr;
+    cudaEvent_t ev_down = nullptr, ev_up = nullptr;   // after the last download / upload into phi
     void *snap = nullptr;
     size_t snap_bytes = 0;
-    int copy_pending = 0;
+    int down_pending = 0, up_pending = 0;
     int S = 0;                 // fractional bits of the fixed-point positions
     long long nn = 0;          // nodes (nx+3)(ny+3)
     int tw = 0, th = 0, ntx = 0, nty = 0, ntiles = 0;
@@ -417,8 +418,9 @@ int sort_species(lepic_ctx *c, int ptype, bool defer = false);
 // moves the records of a pending permutation (the gather a deferred sort left out)
 int materialize_species(lepic_ctx *c, int ptype);
 int materialize_all(lepic_ctx *c);
-// the context's stream waits for the copies in flight on the copy stream (api.cu)
-int wait_copies(lepic_ctx *c);
+// the context's stream waits for a staged upload into phi still in flight (api.cu): every
+// reader and writer of phi calls it
+int wait_upload(lepic_ctx *c);
 // true when the push of species s takes the general mover (boundary options, wall models,
 // the 3rd dimension); such a species' sort is not deferred
 bool push_needs_general(const lepic_ctx *c, int s);

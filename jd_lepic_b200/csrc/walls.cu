@@ -134,7 +134,7 @@ __global__ void k_dielectric(double *phi, const int32_t *bcnd, const double *dq,
 }
 
 int dielectric_update(lepic_ctx *c) {
-    if (const int r = wait_copies(c)) return r;   // a staged upload into phi
+    if (const int r = wait_upload(c)) return r;   // a staged upload into phi
     const lepic_config &g = c->cfg;
     Dtype dt;
     for (int l = 0; l < LEPIC_MAXLABEL; l++) dt.v[l] = c->dtype[l];
