@@ -48,7 +48,7 @@ struct PushP {
     float cdx, cdy;            // dt * 2^S / dx
     float inv2S;               // 2^-S
     int pbc, spec, nmn, negion_nmn;
-    uint32_t step_key;
+    uint32_t step_key, step_key2;
     int tw, th, ntx, M, WX, WY, win;
     long long xlim, ylim;      // nx<<S, ny<<S
     // the 3rd dimension (walls.cu): z per slot, its length, the end plates' potential and
@@ -160,14 +160,16 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     // gather at the old position: ix = INT(x/h)+1, px = (ix*h - x)/h
     const int cx = (int)(X >> P.S), cy = (int)(Y >> P.S);
     const float fx = (float)(X & mask) * inv2S, fy = (float)(Y & mask) * inv2S;
-    const float px = 1.0f - fx, py = 1.0f - fy;
-    const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
     const int n00 = (cx + 1) + (cy + 1) * P.W;
     const float4 r0 = __ldg(P.E + n00), r1 = __ldg(P.E + n00 + P.W);   // nodes n00, +1 and +W, +W+1
     // the wall byte of the current cell, fetched with the field (independent of the move)
     const bool wall_now = !GEN && __ldg(P.cellwall + (cx + 1) + (cy + 1) * (P.nx + 2)) != 0;
-    const float Ex = k00 * r0.x + k10 * r0.z + k11 * r1.z + k01 * r1.x;
-    const float Ey = k00 * r0.y + k10 * r0.w + k11 * r1.w + k01 * r1.y;
+    // bilinear in lerp form: along x on the rows iy and iy+1, then along y (the CIC weights
+    // (1-fx)(1-fy), fx(1-fy), fx fy, (1-fx) fy of the four nodes, in six operations per component)
+    const float ax = fmaf(fx, r0.z - r0.x, r0.x), bx = fmaf(fx, r1.z - r1.x, r1.x);
+    const float ay = fmaf(fx, r0.w - r0.y, r0.y), by = fmaf(fx, r1.w - r1.y, r1.y);
+    const float Ex = fmaf(fy, bx - ax, ax);
+    const float Ey = fmaf(fy, by - ay, ay);
     const float k1 = P.k1;
     bool mag = false;
     float Bx = 0.f, By = 0.f, Bz = 0.f;
@@ -178,6 +180,8 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         if (b00.w > 1.e-5f) {
             const float4 b10 = __ldg(P.B + n00 + 1), b11 = __ldg(P.B + n00 + P.W + 1);
             const float4 b01 = __ldg(P.B + n00 + P.W);
+            const float px = 1.0f - fx, py = 1.0f - fy;
+            const float k00 = px * py, k10 = fx * py, k11 = fx * fy, k01 = px * fy;
             Bx = k00 * b00.x + k10 * b10.x + k11 * b11.x + k01 * b01.x;
             By = k00 * b00.y + k10 * b10.y + k11 * b11.y + k01 * b01.y;
             Bz = k00 * b00.z + k10 * b10.z + k11 * b11.z + k01 * b01.z;
@@ -217,13 +221,13 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         return false;
     }
     // move (:216-217) in fixed-point units: the displacement rounded stochastically,
-    // floor(d + u) with u uniform on [0, 1) in steps of 2^-16 (one integer hash of slot and
-    // step), which rounds up with probability frac(d) and so moves slow particles unbiased
-    uint32_t h = (uint32_t)i * 0x9E3779B1u ^ P.step_key;
-    h = (h ^ (h >> 16)) * 0x7FEB352Du;
-    h ^= h >> 15;
-    const float ux = (float)(h & 0xFFFFu) * (1.0f / 65536.0f);
-    const float uy = (float)(h >> 16) * (1.0f / 65536.0f);
+    // floor(d + u) with u uniform on [0, 1) in steps of 2^-16 (the top 16 bits of a
+    // multiplicative hash of the slot and a per-step key, one per axis), which rounds up with
+    // probability frac(d) and so moves slow particles unbiased
+    const uint32_t hx = ((uint32_t)i ^ P.step_key) * 0x9E3779B1u;
+    const uint32_t hy = ((uint32_t)i ^ P.step_key2) * 0x85EBCA77u;
+    const float ux = (float)(hx >> 16) * (1.0f / 65536.0f);
+    const float uy = (float)(hy >> 16) * (1.0f / 65536.0f);
     const int dX = __float2int_rd(fmaf(ux0, P.cdx, ux));
     const int dY = __float2int_rd(fmaf(uy0, P.cdy, uy));
     if (!GEN) {
@@ -773,6 +777,7 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         P.pbc = g.flag_pbc; P.spec = g.flag_spec; P.nmn = g.flag_nmn;
         P.negion_nmn = (g.charge[s] < 0 && g.mass[s] >= amu && g.flag_nmn == 1) ? 1 : 0;
         P.step_key = (uint32_t)(g.seed * 0x2545F491ull) ^ ((uint32_t)it * 0x27D4EB2Fu) ^ ((uint32_t)s * 0x165667B1u);
+        P.step_key2 = (uint32_t)(g.seed * 0x94D049BBull) ^ ((uint32_t)it * 0xC2B2AE3Du) ^ ((uint32_t)s * 0x9E3779B9u);
         P.tw = c->tw; P.th = c->th; P.ntx = c->ntx;
         P.M = 3;
         P.WX = c->tw + 1 + 2 * P.M;
