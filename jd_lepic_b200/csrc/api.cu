@@ -440,6 +440,7 @@ int particles_put(lepic_ctx *c, int sp, const double *vxp, long long n) {
     v = 0;
     LCUDA(cudaMemcpy(&c->dcnt->n_sorted[sp], &v, sizeof(v), cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(&c->dcnt->n_items[sp], &zero, sizeof(int), cudaMemcpyHostToDevice));
+    B.ordered = false;
     return LEPIC_OK;
 }
 
@@ -565,6 +566,7 @@ int particles_load(lepic_ctx *c, const lepic_load_spec *sp) {
         LCUDA(cudaMemcpyAsync(&c->dcnt->n_sorted[s], &z, sizeof(z), cudaMemcpyHostToDevice, c->stream));
         LCUDA(cudaMemcpyAsync(&c->dcnt->n_items[s], &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
         LCUDA(cudaStreamSynchronize(c->stream));
+        c->sp[s].ordered = false;
     }
     return sync_counters(c);
 }

@@ -383,6 +383,7 @@ extern "C" int lepic_gpu_read_backup(lepic_ctx *c, const char *path, double *tim
         LCUDA(cudaMemcpy(&c->dcnt->n_sorted[s], &zero, sizeof(zero), cudaMemcpyHostToDevice));
         int zi = 0;
         LCUDA(cudaMemcpy(&c->dcnt->n_items[s], &zi, sizeof(int), cudaMemcpyHostToDevice));
+        c->sp[s].ordered = false;
     }
     if (time) *time = t;
     if (gtype) *gtype = gt;

@@ -136,6 +136,10 @@ struct SpeciesBuf {
     // it; the push writes the sorted order into the other buffer and ends the pending state.
     int *pind = nullptr;
     bool ind = false;
+    // the slots are in the order of a sort (false after a put, a load or a restart): only then
+    // is a sort's permutation close to the identity, so that the push can read through it
+    // without scattered loads; the first sort after a load moves the records itself
+    bool ordered = false;
 };
 
 // the slot of buffer cur that holds position j of a species' sorted order (see SpeciesBuf)

@@ -419,6 +419,7 @@ int sort_species(lepic_ctx *c, int sp, bool defer) {
         return sort_species(c, sp, defer);
     }
     if (defer && B.Z[0]) defer = false;   // the push that ends the pending state does not carry z
+    if (!B.ordered) defer = false;         // a random order: the gather streams, the push would not
     if (defer && !B.pind) {
         if (cudaMalloc((void **)&B.pind, sizeof(int) * (size_t)std::max(B.cap, 8ll)) != cudaSuccess) {
             c->last_err = "sort: cudaMalloc of the pending permutation failed";
@@ -453,6 +454,7 @@ int sort_species(lepic_ctx *c, int sp, bool defer) {
         LCUDA(cudaMemcpyAsync(B.cell_off, c->offsets, sizeof(int) * (nk + 1), cudaMemcpyDeviceToDevice, c->stream));
     if (defer) B.ind = true;   // the records stay in buffer cur until the push
     else B.cur = nxt;
+    B.ordered = true;
     return LEPIC_OK;
 }
 
