@@ -39,7 +39,7 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
-    F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed); F(c->Ef);
+    F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed_base); F(c->Ef);
     F(c->ss_diag); F(c->phi_hist); F(c->uB); F(c->dq); F(c->rf_ev); F(c->sec_ev); F(c->ev_count);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
@@ -132,7 +132,8 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         LCUDA(cudaMemcpy(c->Bf, bf.data(), sizeof(float4) * nn, cudaMemcpyHostToDevice));
     }
     LALLOC(c->phi, nn); LALLOC(c->rhs, (size_t)(nx + 1) * (ny + 1));
-    LALLOC(c->Ed, 2 * nn); LALLOC(c->Ef, nn);
+    LALLOC(c->Ed_base, 2 * nn); LALLOC(c->Ef, nn);
+    c->Ed = c->Ed_base;
     LALLOC(c->npd, nn); LALLOC(c->np_red, (size_t)g.ntype * nn); LALLOC(c->np_mx, LEPIC_MAXSP);
     LCUDA(cudaMemcpy(c->phi, phi_init, sizeof(double) * nn, cudaMemcpyHostToDevice));
     {
@@ -145,7 +146,7 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         c->n_unknown = cnt;
     }
     LCUDA(cudaMemset(c->rhs, 0, sizeof(double) * (nx + 1) * (ny + 1)));
-    LCUDA(cudaMemset(c->Ed, 0, sizeof(double2) * 2 * nn));
+    LCUDA(cudaMemset(c->Ed_base, 0, sizeof(double2) * 2 * nn));
     LCUDA(cudaMemset(c->Ef, 0, sizeof(float4) * nn));
     // particles
     long long maxcap = 0;

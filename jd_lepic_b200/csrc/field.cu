@@ -9,14 +9,15 @@
 #include "rho.cuh"
 
 // calc_rho.f90:37-77: rhs(ix,iy) = -sum_ptype charge(ptype)*np(ix,iy,ptype)
+// one node per thread: the column from the thread, the row from blockIdx.y (no division)
 __global__ void k_calc_rhs(RhoParams P, double *rhs) {
-    const long long tot = (long long)(P.nx + 1) * (P.ny + 1);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
-         t += (long long)gridDim.x * blockDim.x) {
-        int ix = (int)(t % (P.nx + 1)) + 1, iy = (int)(t / (P.nx + 1)) + 1;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > P.nx) return;
+    for (int j = blockIdx.y; j <= P.ny; j += gridDim.y) {   // gridDim.y <= 65535
+        const int ix = k + 1, iy = j + 1;
         double r = 0.0;
         for (int s = 0; s < P.ntype; s++) r = r - P.charge[s] * np_val(P, s, ix, iy);
-        rhs[t] = r;
+        rhs[k + (long long)j * (P.nx + 1)] = r;
     }
 }
 
@@ -48,8 +49,7 @@ __global__ void k_np_grid(RhoParams P, int s, double *out) {
 
 int field_calc_rhs(lepic_ctx *c) {
     RhoParams P = rho_params(c);
-    long long tot = (long long)(c->cfg.nx + 1) * (c->cfg.ny + 1);
-    int grid = (int)std::min<long long>(div_up(tot, 256), (long long)c->num_sms * 16);
+    const dim3 grid(div_up(c->cfg.nx + 1, 256), std::min(c->cfg.ny + 1, 65535));
     k_calc_rhs<<<grid, 256, 0, c->stream>>>(P, c->rhs);
     LCUDA(cudaGetLastError());
     return LEPIC_OK;
@@ -152,12 +152,70 @@ __global__ void k_efield_walls(int nx, int ny, const int8_t *bc, const double2 *
     }
 }
 
+// Both passes in one for decks without the periodic and Neumann options: a wall node takes the
+// pass-1 values of its neighbours recomputed from phi (the same operations, so the same bits),
+// and the result goes to the other half of the field buffer, so that every node reads the
+// previous field where pass 1 would have copied it.
+__device__ __forceinline__ double2 efield_pass1(int nx, int ny, double h1, double h2, const double *phi,
+                                                const int8_t *bc, const double2 *Ecur, int mx, int my, int W) {
+    const int m = mx + my * W;
+    if (mx >= 1 && mx <= nx + 1 && my >= 1 && my <= ny + 1 && bc[m] <= 0) {
+        double2 e;
+        e.x = -(phi[m + 1] - phi[m - 1]) / (2.0 * h1);
+        e.y = -(phi[m + W] - phi[m - W]) / (2.0 * h2);
+        return e;
+    }
+    return Ecur[m];
+}
+// one node per thread: the column from the thread, the row from blockIdx.y (no division)
+__global__ void k_efield_fused(int nx, int ny, double h1, double h2, const double *phi, const int8_t *bc,
+                               const double2 *Ecur, double2 *Eout, float4 *Ef) {
+    const int W = nx + 3;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= W) return;
+    for (int iy = blockIdx.y; iy < ny + 3; iy += gridDim.y) {   // gridDim.y <= 65535
+    const int n = ix + iy * W;
+    double2 e;
+    if (ix >= 1 && ix <= nx + 1 && iy >= 1 && iy <= ny + 1 && bc[n] >= 1) {   // pass 2 at a wall
+        e.x = 0.0;
+        e.y = 0.0;
+        if (bc[n + 1] <= 0)
+            e.x = 2.0 * efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix + 1, iy, W).x -
+                  (ix + 2 <= nx + 2 ? efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix + 2, iy, W).x : 0.0);
+        if (bc[n - 1] <= 0)
+            e.x = 2.0 * efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix - 1, iy, W).x -
+                  (ix >= 2 ? efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix - 2, iy, W).x : 0.0);
+        if (bc[n + W] <= 0)
+            e.y = 2.0 * efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix, iy + 1, W).y -
+                  (iy + 2 <= ny + 2 ? efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix, iy + 2, W).y : 0.0);
+        if (bc[n - W] <= 0)
+            e.y = 2.0 * efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix, iy - 1, W).y -
+                  (iy >= 2 ? efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix, iy - 2, W).y : 0.0);
+    } else {
+        e = efield_pass1(nx, ny, h1, h2, phi, bc, Ecur, ix, iy, W);
+    }
+    Eout[n] = e;
+    const float2 f = make_float2((float)e.x, (float)e.y);
+    float2 *half = reinterpret_cast<float2 *>(Ef);
+    half[2 * (long long)n] = f;
+    if (n > 0) half[2 * (long long)n - 1] = f;
+    }
+}
+
 int field_calc_efield(lepic_ctx *c) {
     if (const int r = wait_upload(c)) return r;   // a staged upload into phi
     const int nx = c->cfg.nx, ny = c->cfg.ny;
     int grid = (int)std::min<long long>(div_up(c->nn, 256), (long long)c->num_sms * 16);
-    // E (FP64) lives in Ed[0..nn); the second half holds pass 1, which the wall pass reads
-    double2 *E0 = c->Ed + c->nn, *E1 = c->Ed;
+    if (!c->cfg.flag_pbc && !c->cfg.flag_nmn) {
+        double2 *other = c->Ed == c->Ed_base ? c->Ed_base + c->nn : c->Ed_base;
+        const dim3 g2(div_up(nx + 3, 256), std::min(ny + 3, 65535));
+        k_efield_fused<<<g2, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, c->Ed, other, c->Ef);
+        LCUDA(cudaGetLastError());
+        c->Ed = other;
+        return LEPIC_OK;
+    }
+    // E (FP64) lives in the current half; the other half holds pass 1, which the wall pass reads
+    double2 *E0 = c->Ed == c->Ed_base ? c->Ed_base + c->nn : c->Ed_base, *E1 = c->Ed;
     k_efield_interior<<<grid, 256, 0, c->stream>>>(nx, ny, c->cfg.dx, c->cfg.dy, c->phi, c->bc8, E1, E0);
     if (c->cfg.flag_pbc || c->cfg.flag_nmn) // the passes test the labels, as Efield.f90:43-82 does
         for (int part = 0; part < 2; part++)

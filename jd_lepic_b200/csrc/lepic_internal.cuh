@@ -172,7 +172,8 @@ struct lepic_ctx {
     float4 *Bf = nullptr;
     // dynamic grids
     double *phi = nullptr, *rhs = nullptr;
-    double2 *Ed = nullptr;
+    double2 *Ed = nullptr;       // the current FP64 field: one half of Ed_base (nn each)
+    double2 *Ed_base = nullptr;  // 2 nn: the field and the pass buffer of calc_Efield
     float4 *Ef = nullptr;         // gather copy in node pairs: (Ex, Ey)[n], (Ex, Ey)[n+1]
     double *npd = nullptr;        // FP64 np grids (ntype), filled on demand
     double *np_red = nullptr;
