@@ -39,7 +39,7 @@ static int dalloc(lepic_ctx *c, T **p, size_t count) {
 
 static void free_all(lepic_ctx *c) {
     auto F = [](void *p) { if (p) cudaFree(p); };
-    F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed_base); F(c->Ef);
+    F(c->bcnd); F(c->bc8); F(c->cellwall); F(c->cellwall_w); F(c->kq); F(c->Bf); F(c->phi); F(c->rhs); F(c->Ed_base); F(c->Ef);
     F(c->ss_diag); F(c->phi_hist); F(c->uB); F(c->dq); F(c->rf_ev); F(c->sec_ev); F(c->ev_count);
     F(c->npd); F(c->np_red); F(c->np_mx);
     for (int s = 0; s < LEPIC_MAXSP; s++) {
@@ -113,16 +113,19 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
         kq[n] = (b != -1) ? 2.0 : 1.0; // main.f90:334-344
     }
     std::vector<uint8_t> cw((size_t)(nx + 2) * (ny + 2));
+    std::vector<uint8_t> cww((size_t)W * (ny + 2), 0);   // the same with the node rows' stride
     for (int iy = 0; iy <= ny + 1; iy++)
         for (int ix = 0; ix <= nx + 1; ix++) {
             bool wall = bcnd[ix + iy * W] >= 1 && bcnd[ix + 1 + iy * W] >= 1 && bcnd[ix + 1 + (iy + 1) * W] >= 1 &&
                         bcnd[ix + (iy + 1) * W] >= 1;
             cw[ix + (size_t)iy * (nx + 2)] = wall ? 1 : 0;
+            cww[ix + (size_t)iy * W] = wall ? 1 : 0;
         }
-    LALLOC(c->bcnd, nn); LALLOC(c->bc8, nn); LALLOC(c->cellwall, cw.size()); LALLOC(c->kq, nn);
+    LALLOC(c->bcnd, nn); LALLOC(c->bc8, nn); LALLOC(c->cellwall, cw.size()); LALLOC(c->cellwall_w, cww.size()); LALLOC(c->kq, nn);
     LCUDA(cudaMemcpy(c->bcnd, bcnd, sizeof(int32_t) * nn, cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(c->bc8, bc8.data(), nn, cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(c->cellwall, cw.data(), cw.size(), cudaMemcpyHostToDevice));
+    LCUDA(cudaMemcpy(c->cellwall_w, cww.data(), cww.size(), cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(c->kq, kq.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
     if (g.flag_B == 2) {
         std::vector<float4> bf(nn);

@@ -168,6 +168,7 @@ struct lepic_ctx {
     int32_t *bcnd = nullptr;
     int8_t *bc8 = nullptr;
     uint8_t *cellwall = nullptr;   // (nx+2)(ny+2) cells, 1 = all corners are walls
+    uint8_t *cellwall_w = nullptr; // the same flags at [ix + iy (nx+3)], the node index of the cell's corner
     double *kq = nullptr;
     float4 *Bf = nullptr;
     // dynamic grids

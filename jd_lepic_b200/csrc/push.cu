@@ -38,7 +38,7 @@ struct PushP {
     float Bcx, Bcy, Bcz;
     float tcx, tcy, tcz;       // constant field (BMODE 1): t = k1 B and s = k2 B of the Boris
     float scx, scy, scz;       // rotation, k2 = 2 k1 / (1 + k1^2 |B|^2)
-    const uint8_t *cellwall;
+    const uint8_t *cellwall;   // cell flags at [ix + iy W] (1: all four corners are walls)
     unsigned long long *acc;
     unsigned int *ss_sink;     // this species' ss2D sink counts (null: not accumulated)
     const WorkItem *items;
@@ -50,6 +50,8 @@ struct PushP {
     int pbc, spec, nmn, negion_nmn;
     uint32_t step_key, step_key2;
     int tw, th, ntx, M, WX, WY, win;
+    unsigned WX1, WY1;         // WX - 1, WY - 1
+    int mom_up, mom_sup;       // LEPIC_DEP_SHIFT - 2S and LEPIC_DEP_SHIFT - S (moments deposit)
     long long xlim, ylim;      // nx<<S, ny<<S
     // the 3rd dimension (walls.cu): z per slot, its length, the end plates' potential and
     // phi for the electrons' test, the ions' loss factor hz 2 dt / zmax and the uB map
@@ -115,27 +117,28 @@ __device__ __forceinline__ void deposit_global(unsigned long long *acc, int S, i
 // sx = sum fx, sy = sum fy, sxy = sum fx fy give sum (A-fx)(A-fy), sum fx (A-fy), sum fx fy,
 // sum (A-fx) fy (A = 2^S).  Used when 2S <= LEPIC_DEP_SHIFT: every product is then exact and
 // only shifted up, so the run's weights equal the sum of its particles' cic_weights bit for
-// bit, for two 32-bit adds, one 32x32 product and one 64-bit add per particle.
+// bit, for two 32-bit adds, one 32x32 product and one 64-bit add per particle.  The shift up
+// by 2^(LEPIC_DEP_SHIFT - 2S) is applied to the three moments before the differences (a shift
+// distributes over sums modulo 2^64), and n 2^(2S) shifted up is n 2^LEPIC_DEP_SHIFT.
 __device__ __forceinline__ void mom_weights(const PushP &P, uint32_t n, uint32_t sx, uint32_t sy, uint64_t sxy,
                                             uint64_t *w) {
-    const int S = P.S;
-    const uint64_t Asx = (uint64_t)sx << S, Asy = (uint64_t)sy << S;
-    w[2] = sxy;
-    w[1] = Asx - sxy;
-    w[3] = Asy - sxy;
-    w[0] = ((uint64_t)n << (2 * S)) - Asx - Asy + sxy;
-    const int up = LEPIC_DEP_SHIFT - 2 * S;
-#pragma unroll
-    for (int k = 0; k < 4; k++) w[k] <<= up;
+    const uint64_t c2 = sxy << P.mom_up;
+    const uint64_t ax = (uint64_t)sx << P.mom_sup, ay = (uint64_t)sy << P.mom_sup;
+    w[2] = c2;
+    w[1] = ax - c2;
+    w[3] = ay - c2;
+    w[0] = ((uint64_t)n << LEPIC_DEP_SHIFT) - ax - ay + c2;
 }
 
-// the four accumulators of cell (ix, iy): the CTA's shared-memory window or the global grid
-__device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win, int ox, int oy, bool use_win,
+// the four accumulators of cell (ix, iy): the CTA's shared-memory window when the cell's four
+// nodes lie in it (window-relative cell 0 <= lx < WX - 1, 0 <= ly < WY - 1; an item without a
+// window has its origin far away), else the global grid
+__device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win, int ox, int oy,
                                          int ix, int iy, const uint64_t *w) {
     const int lx = ix - ox, ly = iy - oy;
     unsigned long long *q;
     int row;
-    if (use_win && lx >= 0 && lx + 1 < P.WX && ly >= 0 && ly + 1 < P.WY) {
+    if ((unsigned)lx < P.WX1 && (unsigned)ly < P.WY1) {
         q = win + lx + ly * P.WX;
         row = P.WX;
     } else {
@@ -146,6 +149,29 @@ __device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win
     atomicAdd(q + 1, (unsigned long long)w[1]);
     atomicAdd(q + row + 1, (unsigned long long)w[2]);
     atomicAdd(q + row, (unsigned long long)w[3]);
+}
+
+// a run's moments added to cell (ix, iy) as node weights (mom_weights), each weight formed
+// just before its atomic so that few 64-bit values are live at once
+__device__ __forceinline__ void add_run(const PushP &P, unsigned long long *win, int ox, int oy, int ix, int iy,
+                                        uint32_t n, uint32_t sx, uint32_t sy, uint64_t sxy) {
+    const int lx = ix - ox, ly = iy - oy;
+    unsigned long long *q;
+    int row;
+    if ((unsigned)lx < P.WX1 && (unsigned)ly < P.WY1) {
+        q = win + lx + ly * P.WX;
+        row = P.WX;
+    } else {
+        q = P.acc + ix + (long long)iy * P.W;
+        row = P.W;
+    }
+    const uint64_t c2 = sxy << P.mom_up;
+    atomicAdd(q + row + 1, (unsigned long long)c2);
+    const uint64_t ax = (uint64_t)sx << P.mom_sup;
+    atomicAdd(q + 1, (unsigned long long)(ax - c2));
+    const uint64_t ay = (uint64_t)sy << P.mom_sup;
+    atomicAdd(q + row, (unsigned long long)(ay - c2));
+    atomicAdd(q, (unsigned long long)(((uint64_t)n << LEPIC_DEP_SHIFT) - ax - ay + c2));
 }
 
 // part_mover for one particle in registers; returns false for a hole or a particle lost in
@@ -163,7 +189,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     const int n00 = (cx + 1) + (cy + 1) * P.W;
     const float4 r0 = __ldg(P.E + n00), r1 = __ldg(P.E + n00 + P.W);   // nodes n00, +1 and +W, +W+1
     // the wall byte of the current cell, fetched with the field (independent of the move)
-    const bool wall_now = !GEN && __ldg(P.cellwall + (cx + 1) + (cy + 1) * (P.nx + 2)) != 0;
+    const bool wall_now = !GEN && __ldg(P.cellwall + n00) != 0;
     // bilinear in lerp form: along x on the rows iy and iy+1, then along y (the CIC weights
     // (1-fx)(1-fy), fx(1-fy), fx fy, (1-fx) fy of the four nodes, in six operations per component)
     const float ax = fmaf(fx, r0.z - r0.x, r0.x), bx = fmaf(fx, r1.z - r1.x, r1.x);
@@ -221,15 +247,16 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         return false;
     }
     // move (:216-217) in fixed-point units: the displacement rounded stochastically,
-    // floor(d + u) with u uniform on [0, 1) in steps of 2^-16 (the top 16 bits of a
-    // multiplicative hash of the slot and a per-step key, one per axis), which rounds up with
-    // probability frac(d) and so moves slow particles unbiased
+    // floor(d + u) with u uniform on [0, 1) in steps of 2^-23, which rounds up with probability
+    // frac(d) and so moves slow particles unbiased.  u comes from a multiplicative hash of the
+    // slot and a per-step key, one per axis: its low 23 bits (an odd multiplier permutes the
+    // residues mod 2^23) as the mantissa of 1 + u, so floor(d + 1 + u) - 1 needs no conversion
     const uint32_t hx = ((uint32_t)i ^ P.step_key) * 0x9E3779B1u;
     const uint32_t hy = ((uint32_t)i ^ P.step_key2) * 0x85EBCA77u;
-    const float ux = (float)(hx >> 16) * (1.0f / 65536.0f);
-    const float uy = (float)(hy >> 16) * (1.0f / 65536.0f);
-    const int dX = __float2int_rd(fmaf(ux0, P.cdx, ux));
-    const int dY = __float2int_rd(fmaf(uy0, P.cdy, uy));
+    const float ux = __uint_as_float((hx & 0x007FFFFFu) | 0x3F800000u);
+    const float uy = __uint_as_float((hy & 0x007FFFFFu) | 0x3F800000u);
+    const int dX = (int)((uint32_t)__float2int_rd(fmaf(ux0, P.cdx, ux)) - 1u);
+    const int dY = (int)((uint32_t)__float2int_rd(fmaf(uy0, P.cdy, uy)) - 1u);
     if (!GEN) {
         // a particle that stays in its cell (the common case) and whose cell is not a wall cell
         // is neither lost nor out of range (a wrap of the 32-bit sum always changes the cell)
@@ -260,7 +287,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
     int ixn = (int)(Xn >> P.S) + 1, iyn = (int)(Yn >> P.S) + 1;
     ixn = min(max(ixn, 0), P.nx + 1);
     iyn = min(max(iyn, 0), P.ny + 1);
-    bool is_lost = P.cellwall[ixn + iyn * (P.nx + 2)] != 0;
+    bool is_lost = P.cellwall[ixn + iyn * P.W] != 0;
     if (GEN && !is_lost && P.negion_nmn && Xn < 0) is_lost = true; // :261-266
     if (is_lost) {
         lost++;
@@ -270,7 +297,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
             const int iyw = min(max((int)((Yn + hf) >> P.S) + 1, 0), P.ny + 1);
             atomicAdd(P.ss_sink + ixw + (long long)iyw * P.W, 1u);
         }
-        if (GEN && P.dq && P.cellwall[ixn + iyn * (P.nx + 2)] != 0) {
+        if (GEN && P.dq && P.cellwall[ixn + iyn * P.W] != 0) {
             // dielectric charging (part_expmover.f90:340-350): Nm q split by the loss point's y
             // between the rows iy and iy+1 of the loss cell's label, when that label or the
             // one above is a dielectric
@@ -283,7 +310,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
                 atomicAdd(row + iyn + 1, P.nmq * (1.0 - py));
             }
         }
-        if (GEN && P.sec_label && P.cellwall[ixn + iyn * (P.nx + 2)] != 0 && P.bcnd[ixn + iyn * P.W] == P.sec_label) {
+        if (GEN && P.sec_label && P.cellwall[ixn + iyn * P.W] != 0 && P.bcnd[ixn + iyn * P.W] == P.sec_label) {
             // secondary emission: the event, drawn by k_sec_emit after this push
             const unsigned int e = atomicAdd(P.ev_count + 1, 1u);
             if (e < (unsigned int)P.ev_cap)
@@ -293,7 +320,7 @@ __device__ __forceinline__ bool move_regs(const PushP &P, int i, uint32_t &X, ui
         // the slot becomes a hole that keeps its loss for the tallies (lepic_internal.cuh,
         // loss_hole_tally): X = the loss cell's node, Y = the new vx, VY, VZ = the new vy, vz,
         // VX = a NaN whose payload marks a fresh wall loss (1) or another loss (2)
-        const bool wall = !GEN || P.cellwall[ixn + iyn * (P.nx + 2)] != 0;
+        const bool wall = !GEN || P.cellwall[ixn + iyn * P.W] != 0;
         X = (uint32_t)(ixn + iyn * P.W);
         Y = __float_as_uint(ux0);
         vy = uy0; vz = uz0;
@@ -400,7 +427,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
         const int tile = s_tile;
         if (tile == -2) break;
         const bool use_win = P.win && tile >= 0;
-        int ox = 0, oy = 0;
+        int ox = 1 << 30, oy = 1 << 30;   // no window: every cell is outside it
         if (use_win) {
             int tx = tile % P.ntx, ty = tile / P.ntx;
             ox = tx * P.tw + 1 - P.M;
@@ -498,11 +525,8 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                         const uint32_t fx = X[p] & fmask, fy = Y[p] & fmask;
                         const uint64_t fxy = (uint64_t)fx * fy;
                         if (key != rkey) {
-                            if (rkey >= 0) {
-                                uint64_t w[4];
-                                mom_weights(P, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3], w);
-                                add_cell(P, win, ox, oy, use_win, rix, riy, w);
-                            }
+                            if (rkey >= 0)
+                                add_run(P, win, ox, oy, rix, riy, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3]);
                             rkey = key; rix = ix; riy = iy;
                             rw[0] = 1; rw[1] = fx; rw[2] = fy; rw[3] = fxy;
                         } else {
@@ -513,7 +537,7 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
                     uint64_t w[4];
                     cic_weights(P, X[p], Y[p], w);
                     if (key != rkey) {
-                        if (rkey >= 0) add_cell(P, win, ox, oy, use_win, rix, riy, rw);
+                        if (rkey >= 0) add_cell(P, win, ox, oy, rix, riy, rw);
                         rkey = key; rix = ix; riy = iy;
                         rw[0] = w[0]; rw[1] = w[1]; rw[2] = w[2]; rw[3] = w[3];
                     } else {
@@ -534,11 +558,9 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
             // reduction measured 16 % slower on the whole push, a segmented shuffle scan 4 %)
             if (rkey >= 0) {
                 if (MOM) {
-                    uint64_t w[4];
-                    mom_weights(P, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3], w);
-                    add_cell(P, win, ox, oy, use_win, rix, riy, w);
+                    add_run(P, win, ox, oy, rix, riy, (uint32_t)rw[0], (uint32_t)rw[1], (uint32_t)rw[2], rw[3]);
                 } else {
-                    add_cell(P, win, ox, oy, use_win, rix, riy, rw);
+                    add_cell(P, win, ox, oy, rix, riy, rw);
                 }
             }
         }
@@ -764,7 +786,7 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
             P.tcx = k1f * P.Bcx; P.tcy = k1f * P.Bcy; P.tcz = k1f * P.Bcz;
             P.scx = k2 * P.Bcx; P.scy = k2 * P.Bcy; P.scz = k2 * P.Bcz;
         }
-        P.cellwall = c->cellwall;
+        P.cellwall = c->cellwall_w;
         P.acc = B.acc;
         P.ss_sink = ss_counts(c) ? ss_counts(c) + (size_t)(2 * s + 1) * c->nn : nullptr;
         P.items = B.items;
@@ -774,6 +796,8 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         P.cdx = (float)(g.dt * (double)(1u << c->S) / g.dx);
         P.cdy = (float)(g.dt * (double)(1u << c->S) / g.dy);
         P.inv2S = 1.0f / (float)(1u << c->S);
+        P.mom_up = LEPIC_DEP_SHIFT - 2 * c->S;
+        P.mom_sup = LEPIC_DEP_SHIFT - c->S;
         P.pbc = g.flag_pbc; P.spec = g.flag_spec; P.nmn = g.flag_nmn;
         P.negion_nmn = (g.charge[s] < 0 && g.mass[s] >= amu && g.flag_nmn == 1) ? 1 : 0;
         P.step_key = (uint32_t)(g.seed * 0x2545F491ull) ^ ((uint32_t)it * 0x27D4EB2Fu) ^ ((uint32_t)s * 0x165667B1u);
@@ -782,6 +806,8 @@ int push_deposit(lepic_ctx *c, int it, bool move) {
         P.M = 3;
         P.WX = c->tw + 1 + 2 * P.M;
         P.WY = c->th + 1 + 2 * P.M;
+        P.WX1 = (unsigned)(P.WX - 1);
+        P.WY1 = (unsigned)(P.WY - 1);
         size_t smem = sizeof(unsigned long long) * (size_t)P.WX * P.WY;
         P.win = smem <= 64 * 1024 ? 1 : 0;
         if (!P.win) smem = 0;
