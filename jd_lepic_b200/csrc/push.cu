@@ -113,23 +113,6 @@ __device__ __forceinline__ void deposit_global(unsigned long long *acc, int S, i
     atomicAdd(q + W, (unsigned long long)w[3]);
 }
 
-// The node weights of a run from its moments: n particles with offsets fx, fy summed as
-// sx = sum fx, sy = sum fy, sxy = sum fx fy give sum (A-fx)(A-fy), sum fx (A-fy), sum fx fy,
-// sum (A-fx) fy (A = 2^S).  Used when 2S <= LEPIC_DEP_SHIFT: every product is then exact and
-// only shifted up, so the run's weights equal the sum of its particles' cic_weights bit for
-// bit, for two 32-bit adds, one 32x32 product and one 64-bit add per particle.  The shift up
-// by 2^(LEPIC_DEP_SHIFT - 2S) is applied to the three moments before the differences (a shift
-// distributes over sums modulo 2^64), and n 2^(2S) shifted up is n 2^LEPIC_DEP_SHIFT.
-__device__ __forceinline__ void mom_weights(const PushP &P, uint32_t n, uint32_t sx, uint32_t sy, uint64_t sxy,
-                                            uint64_t *w) {
-    const uint64_t c2 = sxy << P.mom_up;
-    const uint64_t ax = (uint64_t)sx << P.mom_sup, ay = (uint64_t)sy << P.mom_sup;
-    w[2] = c2;
-    w[1] = ax - c2;
-    w[3] = ay - c2;
-    w[0] = ((uint64_t)n << LEPIC_DEP_SHIFT) - ax - ay + c2;
-}
-
 // the four accumulators of cell (ix, iy): the CTA's shared-memory window when the cell's four
 // nodes lie in it (window-relative cell 0 <= lx < WX - 1, 0 <= ly < WY - 1; an item without a
 // window has its origin far away), else the global grid
@@ -151,8 +134,14 @@ __device__ __forceinline__ void add_cell(const PushP &P, unsigned long long *win
     atomicAdd(q + row, (unsigned long long)w[3]);
 }
 
-// a run's moments added to cell (ix, iy) as node weights (mom_weights), each weight formed
-// just before its atomic so that few 64-bit values are live at once
+// A run's moments added to cell (ix, iy) as node weights: n particles with offsets fx, fy
+// summed as sx = sum fx, sy = sum fy, sxy = sum fx fy give sum (A-fx)(A-fy), sum fx (A-fy),
+// sum fx fy, sum (A-fx) fy (A = 2^S).  Used when 2S <= LEPIC_DEP_SHIFT: every product is then
+// exact and only shifted up, so the run's weights equal the sum of its particles' cic_weights
+// bit for bit, for two 32-bit adds, one 32x32 product and one 64-bit add per particle.  The
+// shift up by 2^(LEPIC_DEP_SHIFT - 2S) is applied to the moments before the differences (a
+// shift distributes over sums modulo 2^64); n 2^(2S) shifted up is n 2^LEPIC_DEP_SHIFT.  Each
+// weight is formed just before its atomic, so that few 64-bit values are live at once.
 __device__ __forceinline__ void add_run(const PushP &P, unsigned long long *win, int ox, int oy, int ix, int iy,
                                         uint32_t n, uint32_t sx, uint32_t sy, uint64_t sxy) {
     const int lx = ix - ox, ly = iy - oy;
