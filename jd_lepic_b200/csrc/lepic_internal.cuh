@@ -66,7 +66,8 @@ struct DevCounters {
     // multigrid results
     int mg_cycles, mg_sweeps_fine;
     double mg_res_l1, mg_ktot, mg_res_l2, mg_b_l2;
-    unsigned int bar_count, bar_gen;      // grid barrier of the cooperative kernels
+    unsigned long long bar_arrived;       // grid barrier of the cooperative kernels: arrivals
+                                          // since the launch (zeroed before each launch)
     int abort_flag;                       // set to end every wait of a cooperative kernel
 };
 
@@ -321,29 +322,34 @@ __device__ __forceinline__ int ld_volatile_i32(const int *p) {
     asm volatile("ld.volatile.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+// Each CTA adds one arrival to a counter that only grows during the launch (zeroed before it):
+// the arrivals of barrier k are the values k nblocks .. (k + 1) nblocks - 1 (no CTA arrives at
+// barrier k + 1 before barrier k is complete), so a CTA reads its barrier from the value its
+// atomic returns and waits until the counter reaches the end of that barrier.  With no reset
+// between barriers one atomic and one acquire poll are on the critical path (1.8 us per
+// barrier over 444 CTAs on B200, against 2.8 us for a count-and-generation barrier, measured
+// by a standalone probe).
 __device__ __forceinline__ bool grid_barrier(DevCounters *c, unsigned int nblocks) {
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned int g = ld_acquire_u32(&c->bar_gen);
         __threadfence();
-        unsigned int arrived = atomicAdd(&c->bar_count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&c->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&c->bar_gen, 1u);
-        } else {
-            long long t0 = clock64();
-            while (ld_acquire_u32(&c->bar_gen) == g) {
-                if (ld_volatile_i32(&c->abort_flag) != 0) { ok = 0; break; }
-                if (clock64() - t0 > 4000000000LL) {
-                    set_err(c, LERR_TIMEOUT, 900);
-                    atomicExch(&c->abort_flag, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+        const unsigned long long nb = nblocks;
+        const unsigned long long target = (atomicAdd(&c->bar_arrived, 1ull) / nb + 1) * nb;
+        long long t0 = clock64();
+        while (ld_acquire_u64(&c->bar_arrived) < target) {
+            if (ld_volatile_i32(&c->abort_flag) != 0) { ok = 0; break; }
+            if (clock64() - t0 > 4000000000LL) {
+                set_err(c, LERR_TIMEOUT, 900);
+                atomicExch(&c->abort_flag, 1);
+                ok = 0;
+                break;
             }
         }
         __threadfence();

@@ -414,7 +414,7 @@ int mg_init(lepic_ctx *c) {
 
 static int launch_coop(lepic_ctx *c, void *fn, int grid, MGP &P) {
     void *args[] = {&P};
-    LCUDA(cudaMemsetAsync(&c->dcnt->bar_count, 0, 3 * sizeof(unsigned int), c->stream));
+    LCUDA(cudaMemsetAsync(&c->dcnt->bar_arrived, 0, sizeof(unsigned long long) + sizeof(int), c->stream));
     LCUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(MG_THREADS), args, 0, c->stream));
     return LEPIC_OK;
 }

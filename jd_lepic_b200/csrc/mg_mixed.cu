@@ -266,7 +266,7 @@ static int mixed_launch(lepic_ctx *c, double eps, int *grid_cache) {
         *grid_cache = c->num_sms * std::max(1, std::min(occ, (int)c->opt.ctas_per_sm));
     }
     void *args[] = {&P};
-    LCUDA(cudaMemsetAsync(&c->dcnt->bar_count, 0, 3 * sizeof(unsigned int), c->stream));
+    LCUDA(cudaMemsetAsync(&c->dcnt->bar_arrived, 0, sizeof(unsigned long long) + sizeof(int), c->stream));
     LCUDA(cudaLaunchCooperativeKernel(Mx::kernel(), dim3(*grid_cache), dim3(MG_THREADS), args, smem, c->stream));
     return LEPIC_OK;
 }
