@@ -216,61 +216,55 @@ __device__ __forceinline__ Region make_region(const MXL &L, int tile, int TX, in
     return g;
 }
 
-#define MX_BATCH 4   // elements per thread whose loads are all issued before their stores
+#define MX_BATCH 4   // mask bytes per thread whose loads are all issued before their stores
+
+// one element global -> shared by an asynchronous copy (no register staging); completed by
+// cp_async_wait before the CTA barrier that publishes the region
+__device__ __forceinline__ void cp_async_elem(R *dst, const R *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(R) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // e (from e_src, or zeros when e_src is null), mask and (at updatable nodes) r of the region
-// into shared memory, MX_BATCH elements per thread per round with all loads issued first
+// into shared memory: e and r by asynchronous copies, all issued before the mask's loads
+// (MX_BATCH bytes per thread in flight); the caller waits (cp_async_wait) before its barrier
 __device__ __forceinline__ void region_load(const MXL &L, const R *e_src, const Region &g) {
     const int W = L.nx + 3;
+    for (Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH); w.ok(); w.next()) {
+        const int i = g.ri0 + w.k, j = g.rj0 + w.j;
+        const int q = w.flat();
+        if (e_src) cp_async_elem(g.e + q, e_src + i + j * W);
+        else g.e[q] = R(0.0);
+        if (i >= 1 && i <= L.nx + 1 && j >= 1 && j <= L.ny + 1) cp_async_elem(g.r + q, L.r + (i - 1) + (j - 1) * (L.nx + 1));
+        else g.r[q] = R(0.0);
+    }
     Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH);
     while (w.ok()) {
         int q[MX_BATCH];
-        R ev[MX_BATCH], rv[MX_BATCH];
         int bv[MX_BATCH];
 #pragma unroll
         for (int u = 0; u < MX_BATCH; u++) {
             q[u] = -1;
             if (w.ok()) {
-                const int i = g.ri0 + w.k, j = g.rj0 + w.j;
-                const int n = i + j * W;
                 q[u] = w.flat();
-                ev[u] = e_src ? e_src[n] : R(0.0);
-                bv[u] = L.bc[n];
-                rv[u] = (i >= 1 && i <= L.nx + 1 && j >= 1 && j <= L.ny + 1) ? L.r[(i - 1) + (j - 1) * (L.nx + 1)]
-                                                                              : R(0.0);
+                bv[u] = L.bc[(g.ri0 + w.k) + (g.rj0 + w.j) * W];
                 w.next();
             }
         }
 #pragma unroll
         for (int u = 0; u < MX_BATCH; u++)
-            if (q[u] >= 0) {
-                g.e[q[u]] = ev[u];
-                g.b[q[u]] = (int8_t)bv[u];
-                g.r[q[u]] = rv[u];
-            }
+            if (q[u] >= 0) g.b[q[u]] = (int8_t)bv[u];
     }
 }
 
-// the coarse nodes (ci0.., cj0..) the prolongation of the region reads, into g.ce
+// the coarse nodes (ci0.., cj0..) the prolongation of the region reads, into g.ce, by
+// asynchronous copies (the caller waits)
 __device__ __forceinline__ void coarse_load(const MXL &C, const Region &g, int ci0, int cj0, int CW, int CH) {
     const int W2 = C.nx + 3;
-    Walk2 w(threadIdx.x, blockDim.x, CW, CH);
-    while (w.ok()) {
-        int q[MX_BATCH];
-        R v[MX_BATCH];
-#pragma unroll
-        for (int u = 0; u < MX_BATCH; u++) {
-            q[u] = -1;
-            if (w.ok()) {
-                q[u] = w.flat();
-                v[u] = C.e[(ci0 + w.k) + (cj0 + w.j) * W2];
-                w.next();
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < MX_BATCH; u++)
-            if (q[u] >= 0) g.ce[q[u]] = v[u];
-    }
+    for (Walk2 w(threadIdx.x, blockDim.x, CW, CH); w.ok(); w.next())
+        cp_async_elem(g.ce + w.flat(), C.e + (ci0 + w.k) + (cj0 + w.j) * W2);
 }
 
 // the tile (and, for a tile on the border, the ghost nodes beside it) from shared memory to
@@ -334,6 +328,7 @@ __device__ void tiled_down(const BigTeam &, const MXP &P, int l) {
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const Region g = make_region(F, tile, TX, TY, H, mx_smem, P.tile_cap);
         region_load(F, nullptr, g);   // every level of the cycle starts from e = 0
+        cp_async_wait();
         __syncthreads();
         for (int h = 0; h < K; h++) {
             region_half_sweep(F, g, h, h & 1, P.omega);
@@ -383,6 +378,7 @@ __device__ void tiled_up(const BigTeam &, const MXP &P, int l) {
         const int ci1 = min((g.ri0 + g.RW + 1) / 2, C.nx + 2), cj1 = min((g.rj0 + g.RH + 1) / 2, C.ny + 2);
         const int CW = ci1 - ci0 + 1, CH = cj1 - cj0 + 1;
         coarse_load(C, g, ci0, cj0, CW, CH);
+        cp_async_wait();
         __syncthreads();
         // prolong32 written per fine node: each fine node (i, j), 0 <= i <= nx+1, 0 <= j <= ny+1,
         // takes the correction of the one coarse node prolong32 assigns it, in the same order
