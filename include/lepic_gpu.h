@@ -154,7 +154,8 @@ void *lepic_gpu_stream(lepic_ctx *ctx);
 /* Waits for the context's stream and the asynchronous downloads, and reports any device-side
  * error flag as a code. */
 int lepic_gpu_sync(lepic_ctx *ctx);
-/* Text of the last error of this context (valid until the next call). */
+/* Text of the last error of this context (valid until the next call); with ctx NULL, the
+ * reason of the last failed lepic_gpu_create. */
 const char *lepic_gpu_last_error(lepic_ctx *ctx);
 
 /* Uploads n particles of one charged species, AoS FP64 as vxp(6,n) (z is not kept).

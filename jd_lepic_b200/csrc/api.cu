@@ -121,7 +121,8 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
             cw[ix + (size_t)iy * (nx + 2)] = wall ? 1 : 0;
             cww[ix + (size_t)iy * W] = wall ? 1 : 0;
         }
-    LALLOC(c->bcnd, nn); LALLOC(c->bc8, nn); LALLOC(c->cellwall, cw.size()); LALLOC(c->cellwall_w, cww.size()); LALLOC(c->kq, nn);
+    // the masks are 16 bytes longer: the mixed solver's tiles read them in whole words
+    LALLOC(c->bcnd, nn); LALLOC(c->bc8, nn + 16); LALLOC(c->cellwall, cw.size()); LALLOC(c->cellwall_w, cww.size()); LALLOC(c->kq, nn);
     LCUDA(cudaMemcpy(c->bcnd, bcnd, sizeof(int32_t) * nn, cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(c->bc8, bc8.data(), nn, cudaMemcpyHostToDevice));
     LCUDA(cudaMemcpy(c->cellwall, cw.data(), cw.size(), cudaMemcpyHostToDevice));
@@ -204,7 +205,7 @@ static int create_impl(lepic_ctx *c, const lepic_config *cfg, const int32_t *bcn
             cur[L.nx + 2] = prev[nxf + 2];
             cur[(L.ny + 2) * W2] = prev[(nyf + 2) * Wf];
             cur[L.nx + 2 + (L.ny + 2) * W2] = prev[nxf + 2 + (nyf + 2) * Wf];
-            LALLOC(L.u, nnl); LALLOC(L.b, (size_t)(L.nx + 1) * (L.ny + 1)); LALLOC(L.bc, nnl);
+            LALLOC(L.u, nnl); LALLOC(L.b, (size_t)(L.nx + 1) * (L.ny + 1)); LALLOC(L.bc, nnl + 16);
             LCUDA(cudaMemset(L.u, 0, sizeof(double) * nnl));
             LCUDA(cudaMemset(L.b, 0, sizeof(double) * (L.nx + 1) * (L.ny + 1)));
             LCUDA(cudaMemcpy(L.bc, cur.data(), nnl, cudaMemcpyHostToDevice));
@@ -341,6 +342,9 @@ extern "C" int lepic_gpu_set_options(lepic_ctx *c, const lepic_options *in) {
     return LEPIC_OK;
 }
 
+// the reason of the last failed lepic_gpu_create (lepic_gpu_last_error(NULL))
+static std::string g_create_err = "no context";
+
 extern "C" int lepic_gpu_create(const lepic_config *cfg, const int32_t *bcnd, const double *phi_init,
                                 const double *Bi, const lepic_xs_tables *xs, lepic_ctx **out) {
     if (!cfg || !out) return LEPIC_EINVAL;
@@ -350,8 +354,7 @@ extern "C" int lepic_gpu_create(const lepic_config *cfg, const int32_t *bcnd, co
     c->opt = default_options();
     int r = create_impl(c, cfg, bcnd, phi_init, Bi, xs);
     if (r != LEPIC_OK) {
-        static std::string keep;
-        keep = c->last_err;
+        g_create_err = "lepic_gpu_create: " + c->last_err;
         free_all(c);
         delete c;
         return r;
@@ -372,7 +375,7 @@ extern "C" int lepic_gpu_destroy(lepic_ctx *c) {
 }
 
 extern "C" void *lepic_gpu_stream(lepic_ctx *c) { return c ? (void *)c->stream : nullptr; }
-extern "C" const char *lepic_gpu_last_error(lepic_ctx *c) { return c ? c->last_err.c_str() : "no context"; }
+extern "C" const char *lepic_gpu_last_error(lepic_ctx *c) { return c ? c->last_err.c_str() : g_create_err.c_str(); }
 
 // Reads the device counters; maps a raised device error to a status (then clears it).  A
 // download still in flight on the copy stream is completed first: every call that

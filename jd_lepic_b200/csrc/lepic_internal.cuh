@@ -430,6 +430,7 @@ int sort_species(lepic_ctx *c, int ptype, bool defer = false);
 // moves the records of a pending permutation (the gather a deferred sort left out)
 int materialize_species(lepic_ctx *c, int ptype);
 int materialize_all(lepic_ctx *c);
+int push_preload_ind(lepic_ctx *c, int s);
 // the context's stream waits for a staged upload into phi still in flight (api.cu): every
 // reader and writer of phi calls it
 int wait_upload(lepic_ctx *c);

@@ -219,13 +219,13 @@ static int mixed_launch(lepic_ctx *c, double eps, int *grid_cache) {
     // mask per node, sharing the dynamic shared memory with the small cycle
     const int Hmax = 2 * std::max(P.nu1 + 1, P.nu2);
     auto region_bytes = [&](int tx, int ty) {
-        const long long cap = ((long long)(tx + 2 * Hmax) * (ty + 2 * Hmax) + 15) / 16 * 16;
+        const long long cap = ((long long)((tx + 2 * Hmax + 3) & ~3) * (ty + 2 * Hmax) + 15) / 16 * 16;
         const long long cc = (long long)((tx + 2 * Hmax) / 2 + 3) * ((ty + 2 * Hmax) / 2 + 3);
         return cap * (2 * rs + 1) + cc * rs + 16;
     };
     int cap_tx = MX_TX, cap_ty = MX_TY;
     while (cap_ty > 8 && region_bytes(cap_tx, cap_ty) > 64 * 1024) cap_ty /= 2;
-    P.tile_cap = ((cap_tx + 2 * Hmax) * (cap_ty + 2 * Hmax) + 15) / 16 * 16;
+    P.tile_cap = (((cap_tx + 2 * Hmax + 3) & ~3) * (cap_ty + 2 * Hmax) + 15) / 16 * 16;   // rows padded to 4
     {
         // per level the tile that ends the pass soonest: the tiles go round the grid's CTAs, so
         // a pass lasts (rounds) x (one tile's region, halo included, plus a fixed latency per

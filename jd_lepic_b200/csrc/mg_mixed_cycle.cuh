@@ -187,11 +187,12 @@ __device__ void prolong32(const Team &T, const MXL &C, const MXL &F) {
 struct Region {
     int i0, j0, i1, j1;      // tile interior [i0, i1) x [j0, j1) (updatable nodes)
     int ri0, rj0, RW, RH;    // region origin and size (clamped to the node array)
+    int RP;                  // row pitch in shared memory: RW rounded up to a multiple of 4
     int H;
     R *e, *r;
     int8_t *b;
     R *ce;               // the coarse nodes the region's prolongation reads
-    __device__ __forceinline__ int at(int i, int j) const { return (i - ri0) + (j - rj0) * RW; }
+    __device__ __forceinline__ int at(int i, int j) const { return (i - ri0) + (j - rj0) * RP; }
 };
 
 __device__ __forceinline__ Region make_region(const MXL &L, int tile, int TX, int TY, int H, unsigned char *smem,
@@ -209,6 +210,7 @@ __device__ __forceinline__ Region make_region(const MXL &L, int tile, int TX, in
     g.rj0 = max(g.j0 - H, 0);
     g.RW = min(g.i1 + H, nx + 3) - g.ri0;
     g.RH = min(g.j1 + H, ny + 3) - g.rj0;
+    g.RP = (g.RW + 3) & ~3;
     g.e = (R *)smem;
     g.r = g.e + cap;
     g.b = (int8_t *)(g.r + cap);
@@ -228,34 +230,37 @@ __device__ __forceinline__ void cp_async_elem(R *dst, const R *src) {
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // e (from e_src, or zeros when e_src is null), mask and (at updatable nodes) r of the region
-// into shared memory: e and r by asynchronous copies, all issued before the mask's loads
-// (MX_BATCH bytes per thread in flight); the caller waits (cp_async_wait) before its barrier
+// into shared memory: e and r by asynchronous copies, all issued before the mask's loads; the
+// caller waits (cp_async_wait) before its barrier.  The mask moves in 32-bit words: a shared
+// row starts on a word (the pitch is a multiple of 4), the global row anywhere, so each word
+// is two aligned global words and a funnel shift (the masks are allocated 16 bytes longer for
+// the words past a row's end).
 __device__ __forceinline__ void region_load(const MXL &L, const R *e_src, const Region &g) {
     const int W = L.nx + 3;
     for (Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH); w.ok(); w.next()) {
         const int i = g.ri0 + w.k, j = g.rj0 + w.j;
-        const int q = w.flat();
+        const int q = w.k + w.j * g.RP;
         if (e_src) cp_async_elem(g.e + q, e_src + i + j * W);
         else g.e[q] = R(0.0);
         if (i >= 1 && i <= L.nx + 1 && j >= 1 && j <= L.ny + 1) cp_async_elem(g.r + q, L.r + (i - 1) + (j - 1) * (L.nx + 1));
         else g.r[q] = R(0.0);
     }
-    Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH);
-    while (w.ok()) {
-        int q[MX_BATCH];
-        int bv[MX_BATCH];
-#pragma unroll
-        for (int u = 0; u < MX_BATCH; u++) {
-            q[u] = -1;
-            if (w.ok()) {
-                q[u] = w.flat();
-                bv[u] = L.bc[(g.ri0 + w.k) + (g.rj0 + w.j) * W];
-                w.next();
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < MX_BATCH; u++)
-            if (q[u] >= 0) g.b[q[u]] = (int8_t)bv[u];
+    const int wpr = g.RP >> 2;
+    const uint32_t *bw = reinterpret_cast<const uint32_t *>(L.bc);
+    uint32_t *sb = reinterpret_cast<uint32_t *>(g.b);
+    Walk2 w(threadIdx.x, blockDim.x, wpr, g.RH);
+    while (w.ok()) {   // two words per thread in flight
+        const int q0 = w.k + w.j * wpr;
+        const int gs0 = g.ri0 + (g.rj0 + w.j) * W + 4 * w.k;   // the word's first byte
+        w.next();
+        const bool two = w.ok();
+        const int q1 = two ? w.k + w.j * wpr : q0;
+        const int gs1 = two ? g.ri0 + (g.rj0 + w.j) * W + 4 * w.k : gs0;
+        if (two) w.next();
+        const uint32_t a0 = __ldg(bw + (gs0 >> 2)), b0 = __ldg(bw + (gs0 >> 2) + 1);
+        const uint32_t a1 = __ldg(bw + (gs1 >> 2)), b1 = __ldg(bw + (gs1 >> 2) + 1);
+        sb[q0] = __funnelshift_r(a0, b0, (gs0 & 3) * 8);
+        sb[q1] = __funnelshift_r(a1, b1, (gs1 & 3) * 8);
     }
 }
 
@@ -289,7 +294,7 @@ __device__ __forceinline__ void region_half_sweep(const MXL &L, const Region &g,
     const int lo_j = max(g.j0 - g.H + h + 1, 1), hi_j = min(g.j1 + g.H - h - 1, ny + 2);
     if (lo_i >= hi_i || lo_j >= hi_j) return;
     const int hw = (hi_i - lo_i + 1) / 2 + 1;
-    const int RW = g.RW;
+    const int RW = g.RP;   // the row pitch
     for (Walk2 w(threadIdx.x, blockDim.x, hw, hi_j - lo_j); w.ok(); w.next()) {
         const int j = lo_j + w.j;
         int i = lo_i + 2 * w.k;
@@ -312,7 +317,7 @@ __device__ __forceinline__ void region_half_sweep(const MXL &L, const Region &g,
 // getres32 on the region (no Neumann column: the CG path has no Neumann or periodic decks)
 __device__ __forceinline__ R region_res(const MXL &L, const Region &g, int i, int j) {
     const R aw = L.aw, ae = L.aw, an = L.an, as = L.an, ac = L.ac;
-    const int q = g.at(i, j), RW = g.RW;
+    const int q = g.at(i, j), RW = g.RP;
     return g.r[q] - (aw * g.e[q - 1] + ae * g.e[q + 1] + an * g.e[q + RW] + as * g.e[q - RW] + ac * g.e[q]);
 }
 
@@ -385,7 +390,7 @@ __device__ void tiled_up(const BigTeam &, const MXP &P, int l) {
         for (Walk2 w(threadIdx.x, blockDim.x, g.RW, g.RH); w.ok(); w.next()) {
             const int i = g.ri0 + w.k, j = g.rj0 + w.j;
             if (i > nx + 1 || j > ny + 1) continue;
-            const int q = w.flat();
+            const int q = w.k + w.j * g.RP;
             if (g.b[q] > 0) continue;
             const int i2 = (i + 2) / 2, j2 = (j + 2) / 2;    // the coarse node whose stencil holds (i, j)
             const R *e = g.ce + (i2 - ci0) + (j2 - cj0) * CW;

@@ -574,14 +574,22 @@ __global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
     }
 }
 
+// the kernel's dynamic shared-memory limit, set once per device (this also loads the kernel)
 template <int BMODE, bool GEN, bool MOVE, bool MOM, bool IND>
-static int launch_one(lepic_ctx *c, PushP &P, size_t smem) {
+static int set_push_attr(lepic_ctx *c) {
     static bool attr_set[64] = {false};
     if (!attr_set[c->dev & 63]) {
         LCUDA(cudaFuncSetAttribute(k_push_deposit<BMODE, GEN, MOVE, MOM, IND>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         attr_set[c->dev & 63] = true;
     }
+    return LEPIC_OK;
+}
+
+template <int BMODE, bool GEN, bool MOVE, bool MOM, bool IND>
+static int launch_one(lepic_ctx *c, PushP &P, size_t smem) {
+    const int ra = set_push_attr<BMODE, GEN, MOVE, MOM, IND>(c);
+    if (ra != LEPIC_OK) return ra;
     int occ = 0;
     LCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push_deposit<BMODE, GEN, MOVE, MOM, IND>,
                                                         PUSH_THREADS, smem));
@@ -596,6 +604,23 @@ static int launch_m(lepic_ctx *c, PushP &P, size_t smem, bool gen, bool move, bo
     if (!move) return launch_one<BMODE, false, false, MOM, false>(c, P, smem);
     if (gen) return launch_one<BMODE, true, true, MOM, false>(c, P, smem);
     return ind ? launch_one<BMODE, false, true, MOM, true>(c, P, smem) : launch_one<BMODE, false, true, MOM, false>(c, P, smem);
+}
+
+// The mover that reads through a pending permutation, configured (and so loaded) ahead of its
+// first launch: the first sort of a species that may leave its permutation pending calls this,
+// so that the first push after a deferred sort pays no kernel loading.
+template <int BMODE>
+static int preload_ind_b(lepic_ctx *c) {
+    return 2 * c->S <= LEPIC_DEP_SHIFT ? set_push_attr<BMODE, false, true, true, true>(c)
+                                       : set_push_attr<BMODE, false, true, false, true>(c);
+}
+int push_preload_ind(lepic_ctx *c, int s) {
+    const lepic_config &g = c->cfg;
+    int bmode = g.flag_B;
+    if (g.flag_B_pos == 1 && g.charge[s] > 0.0) bmode = 0; // as push_deposit
+    if (bmode == 1) return preload_ind_b<1>(c);
+    if (bmode == 2) return preload_ind_b<2>(c);
+    return preload_ind_b<0>(c);
 }
 
 // moments deposit where the weights are exact (2S <= LEPIC_DEP_SHIFT, grids of 1024 and up)

@@ -420,11 +420,17 @@ int sort_species(lepic_ctx *c, int sp, bool defer) {
     }
     if (defer && B.Z[0]) defer = false;   // the push that ends the pending state does not carry z
     if (!B.ordered) defer = false;         // a random order: the gather streams, the push would not
-    if (defer && !B.pind) {
+    if ((defer || c->opt.sort_defer == 1) && !B.pind) {
+        // at the species' first sort, deferred or not (after a load the first one is not): the
+        // permutation's buffer and the mover that reads through it are ready before the time
+        // loop, whose first deferred sort would otherwise allocate (a device-wide wait while
+        // the driver maps and clears 4 B per slot) and whose next push would load a kernel
         if (cudaMalloc((void **)&B.pind, sizeof(int) * (size_t)std::max(B.cap, 8ll)) != cudaSuccess) {
             c->last_err = "sort: cudaMalloc of the pending permutation failed";
             return LEPIC_ENOMEM;
         }
+        const int r = push_preload_ind(c, sp);
+        if (r != LEPIC_OK) return r;
     }
     int *perm = defer ? B.pind : c->perm;
     const long long nk = c->nkeys;

@@ -135,7 +135,8 @@ class GpuSimulation:
         rc = self.lib.lepic_gpu_create(C.byref(cfg), _ip(self._bcnd), _dp(self._phi0), _dp(self._Bi),
                                        C.byref(xs), C.byref(self.ctx))
         if rc != 0:
-            raise capi.LepicError(rc, "lepic_gpu_create", "")
+            msg = self.lib.lepic_gpu_last_error(None)
+            raise capi.LepicError(rc, "lepic_gpu_create", msg.decode() if msg else "")
         if load:
             self.load()
 
