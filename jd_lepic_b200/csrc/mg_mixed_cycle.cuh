@@ -564,8 +564,9 @@ __device__ __forceinline__ void walk_batch(Walk2 &w, int W, int *t, int *n, bool
 // r = b - A u at unknowns (bcnd <= 0), zero elsewhere; r32 = (R) r; e = 0 (all nodes);
 // returns ||r||^2 over bcnd == -1 nodes and the reference's L1 sum.  With B0 the same walk also
 // forms ||b0||^2 over bcnd == -1 nodes, b0 = b minus the wall terms of A u (the norm the
-// stopping test scales by), and the three sums share one grid barrier.
-template <bool B0>
+// stopping test scales by), and the three sums share one grid barrier.  Without WRITE only the
+// sums are formed (the convergence check: r, r32 and e stay as they are).
+template <bool B0, bool WRITE = true>
 __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double *l1, double *bb = nullptr) {
     const MXL &L = P.L[0];
     const int nx = L.nx, ny = L.ny, W = nx + 3;
@@ -602,14 +603,18 @@ __device__ bool true_residual(const BigTeam &B, const MXP &P, double *rr, double
                                            (bs[k] > 0 ? an * us[k] : 0.0) + (be[k] > 0 ? aw * ue[k] : 0.0));
                 s0 += d * d;
             }
-            P.r64[n[k]] = r;
-            L.r[t[k]] = (R)r;
+            if (WRITE) {
+                P.r64[n[k]] = r;
+                L.r[t[k]] = (R)r;
+            }
         }
     }
-    for (Walk2 w2(B.rank(), B.size(), W, ny + 3); w2.ok(); w2.next()) {
-        const int t = w2.flat();
-        L.e[t] = R(0.0);
-        if (w2.k == 0 || w2.j == 0 || w2.k == nx + 2 || w2.j == ny + 2) P.r64[t] = 0.0;
+    if (WRITE) {
+        for (Walk2 w2(B.rank(), B.size(), W, ny + 3); w2.ok(); w2.next()) {
+            const int t = w2.flat();
+            L.e[t] = R(0.0);
+            if (w2.k == 0 || w2.j == 0 || w2.k == nx + 2 || w2.j == ny + 2) P.r64[t] = 0.0;
+        }
     }
     if (B0) {
         double out[3];
@@ -754,14 +759,18 @@ __global__ void __launch_bounds__(MG_THREADS, 3) k_mg_mixed(MXP P) {
         if (!(alpha > 0.0) || !isfinite(alpha)) break; // no descent: stop and report
         if (!update_ur(B, P, alpha, &rr)) return;
         it++;
-        if (sqrt(rr) <= tol) {               // confirm on the true residual
-            if (!true_residual<false>(B, P, &rr, &l1)) return;
+        if (sqrt(rr) <= tol) {               // confirm on the true residual (its sums only)
+            if (!true_residual<false, false>(B, P, &rr, &l1)) return;
             conv = sqrt(rr) <= tol;
-            if (!conv) { first = true; restarts++; }
+            if (!conv) {                     // restart from the true residual
+                if (!true_residual<false>(B, P, &rr, &l1)) return;
+                first = true;
+                restarts++;
+            }
         }
     }
     if (!conv) {
-        if (!true_residual<false>(B, P, &rr, &l1)) return;
+        if (!true_residual<false, false>(B, P, &rr, &l1)) return;
         conv = sqrt(rr) <= tol;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
