@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <thread>
 #include <vector>
 #include "mg_common.cuh"
 
@@ -49,11 +50,13 @@ __global__ void k_warm_xtrap(double *u, double *hist, const int8_t *bc, long lon
     }
 }
 
+#define MX_DIRECT_MAX 2048   // unknowns of the exactly solved level (33^2 nodes fit)
+
 // The inverse of level l's operator on its unknowns (nodes with bcnd <= 0 inside the level):
 // B = -A is symmetric positive definite (the 5-point stencil with the walls' zero correction),
 // factored by a Cholesky decomposition within its band (unknowns in row order: the band is one
 // row of the level), then B^-1 column by column; M = A^-1 = -B^-1 is kept in FP32 (and in FP64
-// for mode 4's cycle).  Computed once per level on the host (at most 2048 unknowns: ~0.1 s),
+// for mode 4's cycle).  Computed once per level on the host (at most MX_DIRECT_MAX unknowns),
 // then reused by every solve.
 static int coarse_inverse(lepic_ctx *c, int l) {
     if (c->mx_clev == l) return LEPIC_OK;
@@ -73,7 +76,7 @@ static int coarse_inverse(lepic_ctx *c, int l) {
             ridx.push_back((i - 1) + (j - 1) * (L.nx + 1));
         }
     const int n = (int)node.size();
-    if (n == 0 || n > 2048) return LEPIC_OK;   // the CTA-0 cycle stays
+    if (n == 0 || n > MX_DIRECT_MAX) return LEPIC_OK;   // the CTA-0 cycle stays
     const double aw = c->cfg.eps0 / (L.hx * L.hx), an = c->cfg.eps0 / (L.hy * L.hy);
     std::vector<double> Bm((size_t)n * n, 0.0), G((size_t)n * n, 0.0);
     int bw = 0;
@@ -104,23 +107,34 @@ static int coarse_inverse(lepic_ctx *c, int l) {
     }
     std::vector<float> M((size_t)n * n);
     std::vector<double> M64((size_t)n * n);
-    std::vector<double> y((size_t)n), xv((size_t)n);
-    for (int col = 0; col < n; col++) {
-        for (int i = 0; i < col; i++) y[i] = 0.0;
-        for (int i = col; i < n; i++) {   // G y = e_col
-            double s = i == col ? 1.0 : 0.0;
-            for (int k = std::max(col, i - bw); k < i; k++) s -= G[(size_t)i * n + k] * y[k];
-            y[i] = s / G[(size_t)i * n + i];
+    // the columns are independent: host threads take every nth one
+    auto columns = [&](int first, int stride) {
+        std::vector<double> y((size_t)n), xv((size_t)n);
+        for (int col = first; col < n; col += stride) {
+            for (int i = 0; i < col; i++) y[i] = 0.0;
+            for (int i = col; i < n; i++) {   // G y = e_col
+                double s = i == col ? 1.0 : 0.0;
+                for (int k = std::max(col, i - bw); k < i; k++) s -= G[(size_t)i * n + k] * y[k];
+                y[i] = s / G[(size_t)i * n + i];
+            }
+            for (int i = n - 1; i >= 0; i--) {   // G^T x = y
+                double s = y[i];
+                for (int k = i + 1; k <= std::min(n - 1, i + bw); k++) s -= G[(size_t)k * n + i] * xv[k];
+                xv[i] = s / G[(size_t)i * n + i];
+            }
+            for (int i = 0; i < n; i++) {
+                M[(size_t)i * n + col] = (float)(-xv[i]);
+                M64[(size_t)i * n + col] = -xv[i];
+            }
         }
-        for (int i = n - 1; i >= 0; i--) {   // G^T x = y
-            double s = y[i];
-            for (int k = i + 1; k <= std::min(n - 1, i + bw); k++) s -= G[(size_t)k * n + i] * xv[k];
-            xv[i] = s / G[(size_t)i * n + i];
-        }
-        for (int i = 0; i < n; i++) {
-            M[(size_t)i * n + col] = (float)(-xv[i]);
-            M64[(size_t)i * n + col] = -xv[i];
-        }
+    };
+    const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < 512 || nth == 1) {
+        columns(0, 1);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; t++) pool.emplace_back(columns, t, nth);
+        for (auto &th : pool) th.join();
     }
     if (c->mx_cinv) { cudaFree(c->mx_cinv); c->mx_cinv = nullptr; }
     if (c->mx_cinv64) { cudaFree(c->mx_cinv64); c->mx_cinv64 = nullptr; }
