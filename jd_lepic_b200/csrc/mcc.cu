@@ -2,10 +2,11 @@
 // :209-1040) for neutral targets, every ns_coll steps.
 //
 // The reference draws Nc = N*Pmax particles with replacement from one Park-Miller stream.
-// Here every slot draws its own uniform from Philox4x32-10 keyed by (seed, step, species,
-// slot): the slot is a candidate when u < Pmax = nu_max*ns_coll*dt, so the expected number of
-// candidates and the per-particle collision probability sum(nu)*ns_coll*dt are the same, and
-// every result is reproducible run to run.  A candidate then follows collision_OMP exactly:
+// Here every slot is a candidate with probability Pmax = nu_max*ns_coll*dt, independently (a
+// Bernoulli trial per slot, drawn as geometric gaps between candidates from Philox4x32-10
+// keyed by seed, step, species and slot chunk), so the expected number of candidates and the
+// per-particle collision probability sum(nu)*ns_coll*dt are the same, and every result is
+// reproducible run to run.  A candidate then follows collision_OMP exactly:
 // Maxwellian target velocity (load_gauss), centre-of-mass kinematics, cross section by
 // interval search on the union energy grid with linear interpolation, nu/nu_max per reaction,
 // one uniform against the cumulative sum, and the reaction outcome (energy- and momentum-
@@ -17,9 +18,9 @@
 // a second kernel sorts each list by key and appends it after the occupied slots, so the
 // particle order after a collision step is deterministic.
 //
-// Roofline: the selection pass generates one Philox block per 4 slots and reads nothing (it
-// writes the candidate list); only candidates (N*Pmax, about 0.3 % of particles) read and
-// write their 20 B record, one candidate per thread.
+// Roofline: the selection pass draws one uniform per candidate (twice: count, then write)
+// and reads nothing (it writes the candidate list); only candidates (N*Pmax, about 0.3 % of
+// particles) read and write their 20 B record, one candidate per thread.
 #include <algorithm>
 #include "rho.cuh"
 
@@ -433,26 +434,47 @@ __device__ void collide_one(const MccP &P, long long slot, double nu_max, unsign
 // nu_max (charged targets: it depends on the densities, collisions.f90:98-117)
 __device__ __forceinline__ double step_nu_max(const MccP &P) { return P.dsmc ? P.nu_max_d[P.sp] : P.nu_max; }
 
-// Selection: every slot's uniform against Pmax (one Philox block per 4 slots); the candidates
-// are compacted into a list (one atomic per warp).  The list's order does not matter: every
-// draw of a collision is keyed by its slot, a DSMC target goes to the smallest claiming slot,
-// and products are sorted before they are appended.
+// Selection: every slot is a candidate with probability Pmax, independently of the others (a
+// Bernoulli trial per slot), drawn as the geometric gaps between candidates: a thread walks a
+// chunk of SEL_CHUNK slots, each gap floor(log u / log(1 - Pmax)) slots long, so that the
+// random numbers number the candidates (Pmax is ~0.3 %) instead of the slots.  The uniforms
+// come from Philox4x32-10 keyed by (chunk, draw, step, species); P(gap >= k) = (1 - Pmax)^k
+// to the 2^-32 grain of u.  The walk runs twice, counting and then writing, so that each warp
+// takes its place in the list with one atomic.  The list's order does not matter: every draw
+// of a collision is keyed by its slot, a DSMC target goes to the smallest claiming slot, and
+// products are sorted before they are appended.
+#define SEL_CHUNK 4096
+
+__device__ __forceinline__ int select_walk(const MccP &P, long long ch, long long lo, long long hi, double lq,
+                                           bool all, int *out) {
+    long long pos = lo - 1;
+    int cnt = 0;
+    U4 r{0u, 0u, 0u, 0u};
+    for (uint32_t k = 0;; k++) {
+        if ((k & 3u) == 0u)
+            r = philox4x32_10(U4{(uint32_t)ch, k >> 2, P.it, (uint32_t)P.sp | 0x53470000u}, P.k0, P.k1);
+        const uint32_t v = (k & 3u) == 0u ? r.x : (k & 3u) == 1u ? r.y : (k & 3u) == 2u ? r.z : r.w;
+        const double g = all ? 0.0 : floor(log(u01(v)) / lq);
+        if (g >= (double)(hi - 1 - pos)) break;   // the next candidate lies beyond the chunk
+        pos += (long long)g + 1;
+        if (out) out[cnt] = (int)pos;
+        cnt++;
+    }
+    return cnt;
+}
+
 __global__ void __launch_bounds__(MCC_THREADS) k_mcc_select(MccP P, int *cand) {
     const long long n = P.cnt->n_slots[P.sp];
     const double Pmax = P.dsmc ? step_nu_max(P) * P.ns_coll_dt : P.Pmax;
+    const bool any = Pmax > 0.0, all = Pmax >= 1.0;
+    const double lq = any && !all ? log1p(-Pmax) : -1.0;
     const unsigned lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x * 4;
-    for (long long base0 = blockIdx.x * (long long)blockDim.x * 4; base0 < n; base0 += stride) {  // uniform trip count
-        const long long base = base0 + 4 * (long long)threadIdx.x;
-        unsigned mask = 0;
-        if (base < n) {
-            const U4 r = philox4x32_10(U4{(uint32_t)(base >> 2), P.it, (uint32_t)P.sp | 0x53450000u, 0u}, P.k0, P.k1);
-            const uint32_t v[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (base + q < n && u01(v[q]) < Pmax) mask |= 1u << q;
-        }
-        const int c = __popc(mask);
+    const long long nchunk = (n + SEL_CHUNK - 1) / SEL_CHUNK;
+    for (long long c0 = blockIdx.x * (long long)blockDim.x; c0 < nchunk; c0 += (long long)gridDim.x * blockDim.x) {
+        const long long ch = c0 + threadIdx.x;   // every lane takes the same trip count
+        const long long lo = ch * SEL_CHUNK, hi = min(lo + SEL_CHUNK, n);
+        const bool mine = ch < nchunk && any;
+        const int c = mine ? select_walk(P, ch, lo, hi, lq, all, nullptr) : 0;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -463,10 +485,7 @@ __global__ void __launch_bounds__(MCC_THREADS) k_mcc_select(MccP P, int *cand) {
         unsigned wbase = 0;
         if (lane == 31 && total) wbase = atomicAdd(&P.cnt->n_cand_list, (unsigned)total);
         wbase = __shfl_sync(0xffffffffu, wbase, 31);
-        const long long off = (long long)wbase + incl - c;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-            if ((mask >> q) & 1u) cand[off + __popc(mask & ((1u << q) - 1u))] = (int)(base + q);
+        if (mine && c) select_walk(P, ch, lo, hi, lq, all, cand + (long long)wbase + incl - c);
     }
 }
 

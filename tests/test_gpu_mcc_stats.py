@@ -1,8 +1,9 @@
 """Null-collision MCC of the 5-reaction argon deck on the B200 against the oracle's collisions
 (collisions.f90:1-207, collision_OMP :209-1040), matched statistically.
 
-The two sides draw different random numbers: the device selects each slot with its own
-Philox draw against Pmax (a Bernoulli trial per slot), the reference picks Nc = N Pmax
+The two sides draw different random numbers: the device selects each slot with probability
+Pmax (a Bernoulli trial per slot, drawn as geometric gaps between candidates from Philox
+counter streams), the reference picks Nc = N Pmax
 particles with replacement from one Park-Miller stream (collisions.f90:92-157, 273-283).  The
 expected number of candidates, the per-particle collision probability and every outcome
 distribution are the same, and that is what these tests check:
