@@ -21,7 +21,7 @@
 #include <algorithm>
 #include "lepic_internal.cuh"
 
-#define PUSH_THREADS 256
+#define PUSH_THREADS 128
 #define PUSH_CHUNK 16384
 
 struct PushP {
@@ -390,7 +390,7 @@ __device__ __forceinline__ bool zstep(const PushP &P, int i, uint32_t &X, uint32
 // still tile the slot array exactly; particles a rounded range takes from a neighbouring
 // tile reach the global grid when they fall outside the window.
 template <int BMODE, bool GEN, bool MOVE, bool MOM, bool IND>
-__global__ void __launch_bounds__(PUSH_THREADS, 4) k_push_deposit(PushP P) {
+__global__ void __launch_bounds__(PUSH_THREADS, 8) k_push_deposit(PushP P) {
     extern __shared__ unsigned long long win[];
     __shared__ int s_tile, s_start, s_end;
     __shared__ unsigned int s_lost;
