@@ -624,14 +624,16 @@ def run_ours(args):
     if rank == 0:
         # kernels of this library launched in the timed steps (memsets/copies not counted), as
         # the ncu launch list shows them: rhs 1, the warm start's extrapolation 1 (mixed mode),
-        # Poisson 1 (cooperative), E field 2, push 1 per species; a sort step adds 8 per species
+        # Poisson 1 (cooperative), E field 1 (4 with the periodic or Neumann option), push 1 per
+        # species; a sort step adds 8 per species
         # (keys, three scan passes, scatter, two segment passes, work items; the records move in
         # the push), a collision step the selection and the collisions per colliding species
         # and the product commit per species
         n_mcc = sum(1 for s in range(sim.sp.ntype) if sim.xs.p_ncol[s] > 0)
+        e_launches = 4 if (case.flag_pbc or case.flag_nmn) else 1
         launches = 0
         for t in range(first_timed, first_timed + args.steps):
-            launches += 1 + (1 if mode == capi.POISSON_MIXED_IR else 0) + 1 + 2 + sim.sp.ntype
+            launches += 1 + (1 if mode == capi.POISSON_MIXED_IR else 0) + 1 + e_launches + sim.sp.ntype
             if t % 10 == 1:
                 launches += 8 * sim.sp.ntype
             if t > 1 and t % 10 == 1:
