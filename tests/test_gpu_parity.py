@@ -428,10 +428,9 @@ def test_mixed_tiled_smoother_matches_grid_sweeps(gpu_lib, monkeypatch, idx, n, 
 
 
 def test_push_fast_particles_through_the_queues(gpu_lib):
-    """Particles that leave their cell every step (1-3 cells per step), unsorted and sorted: the
-    push's general-move and single-deposit queues fill up and fall back to working in place;
-    every particle both sides keep still matches the FP64 oracle, and the density its FP64
-    deposition."""
+    """Particles that leave their cell every step (1-3 cells per step), unsorted and sorted, so
+    that every particle takes the push's cell-change path: every particle both sides keep still
+    matches the FP64 oracle, and the density its FP64 deposition."""
     case = configs.case0(ppc=4, nx=64, ny=64)
     s = sim_for(case, capacity=200000)
     try:
